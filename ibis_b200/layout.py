@@ -1,0 +1,280 @@
+"""Structure-of-arrays layout of the hourly-step state on the device.
+
+Every per-cell quantity is stored as one or more *planes*: a plane is a
+contiguous run of ``ld`` values (``ld`` >= number of cells, a multiple of 32 so
+that each plane starts 128-byte aligned).  A field with a trailing dimension of
+``k`` (soil layers, bands, plant-type slots ...) occupies ``k`` consecutive
+planes, layer-major, so thread ``i`` of a warp reads element ``i`` of a plane
+and every load is coalesced.
+
+The planes are grouped into five buffers by how the step uses them:
+
+``PROG``   prognostic state: read at the start of a step, written at its end
+``STAT``   per-cell static inputs (soil texture, vegetation structure): read only
+``FORC``   hourly forcing (the ``atm`` leaves the step assumes are set)
+``DIAG``   diagnostics the step writes but never reads (optional)
+``ACC``    per-step accumulators of the day loop (optional; Kahan-compensated
+           in the FP32 kernels, so each accumulator plane has a twin holding
+           its running compensation)
+
+Each field names the leaf of the reference ``IBISState`` it mirrors
+(``python-port/ibis/state/*.py``), so host code can move data between the
+reference's pytree and these buffers without a lookup table of its own.  The
+C header ``include/ibis_layout.h`` is generated from this table by
+:func:`header_text` and checked against it by the test suite.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+NSOILAY = 6
+NBEDROCK = 3
+NSNOLAY = 3
+NPFT = 12
+NBAND = 2
+
+
+@dataclass(frozen=True)
+class Field:
+    name: str          # C-side name (upper-cased in the header)
+    leaf: str          # reference pytree leaf, e.g. "soil.tsoi"
+    k: int = 1         # number of planes (trailing dimension)
+
+
+PROG = (
+    Field("tsoi", "soil.tsoi", NSOILAY),
+    Field("wsoi", "soil.wsoi", NSOILAY),
+    Field("wisoi", "soil.wisoi", NSOILAY),
+    Field("tg", "soil.tg"),
+    Field("wpud", "soil.wpud"),
+    Field("wipud", "soil.wipud"),
+    Field("tsoi_deep", "soil.tsoi_deep", NBEDROCK),
+    Field("fi", "snow.fi"),
+    Field("tsno", "snow.tsno", NSNOLAY),
+    Field("hsno", "snow.hsno", NSNOLAY),
+    Field("ti", "snow.ti"),
+    Field("tlsub", "snow.tlsub"),
+    Field("tu", "canopy.tu"),
+    Field("ts", "canopy.ts"),
+    Field("tl", "canopy.tl"),
+    Field("t12", "canopy.t12"),
+    Field("t34", "canopy.t34"),
+    Field("q12", "canopy.q12"),
+    Field("q34", "canopy.q34"),
+    Field("wliqu", "canopy.wliqu"),
+    Field("wliqs", "canopy.wliqs"),
+    Field("wliql", "canopy.wliql"),
+    Field("wsnou", "canopy.wsnou"),
+    Field("wsnos", "canopy.wsnos"),
+    Field("wsnol", "canopy.wsnol"),
+    Field("ci_upper", "canopy.ci_upper", 2),
+    Field("gs_upper", "canopy.gs_upper", 2),
+    Field("cs_upper", "canopy.cs_upper", 2),
+    Field("ci_lower", "canopy.ci_lower", 3),
+    Field("gs_lower", "canopy.gs_lower", 3),
+    Field("cs_lower", "canopy.cs_lower", 3),
+    Field("a10scalparamu", "canopy.a10scalparamu"),
+    Field("a10daylightu", "canopy.a10daylightu"),
+    Field("a10scalparaml", "canopy.a10scalparaml"),
+    Field("a10daylightl", "canopy.a10daylightl"),
+    Field("firefac", "vegetation.firefac"),
+    Field("nytimes", "vegetation.nytimes"),
+    Field("nfirestep", "vegetation.nfirestep"),
+    Field("sdry", "vegetation.sdry"),
+    Field("nfirestep_vpd", "vegetation.nfirestep_vpd"),
+    Field("sdry_vpd", "vegetation.sdry_vpd"),
+)
+
+STAT = (
+    Field("poros", "soil.poros", NSOILAY),
+    Field("hydraul", "soil.hydraul", NSOILAY),
+    Field("suction", "soil.suction", NSOILAY),
+    Field("bex", "soil.bex", NSOILAY),
+    Field("sfield", "soil.sfield", NSOILAY),
+    Field("swilt", "soil.swilt", NSOILAY),
+    Field("sand", "soil.sand", NSOILAY),
+    Field("clay", "soil.clay", NSOILAY),
+    Field("csoi", "soil.csoi", NSOILAY),
+    Field("rhosoi", "soil.rhosoi", NSOILAY),
+    Field("albsav", "soil.albsav"),
+    Field("albsan", "soil.albsan"),
+    Field("z0soi", "soil.z0soi"),
+    Field("lai", "vegetation.lai", 2),
+    Field("sai", "vegetation.sai", 2),
+    Field("ztop", "vegetation.ztop", 2),
+    Field("zbot", "vegetation.zbot", 2),
+    Field("fu", "vegetation.fu"),
+    Field("fl", "vegetation.fl"),
+    Field("frac", "vegetation.frac", NPFT),
+    Field("exist", "vegetation.exist", NPFT),
+    Field("cbiow", "vegetation.cbiow", NPFT),
+    Field("cbior", "vegetation.cbior", NPFT),
+    Field("sapfrac", "vegetation.sapfrac"),
+    Field("tco2mic", "vegetation.tco2mic"),
+    Field("f_inund", "methane.f_inund"),
+)
+
+FORC = (
+    Field("ta", "atm.ta"),
+    Field("qa", "atm.qa"),
+    Field("ua", "atm.ua"),
+    Field("psurf", "atm.psurf"),
+    Field("coszen", "atm.coszen"),
+    Field("solad", "atm.solad", NBAND),
+    Field("solai", "atm.solai", NBAND),
+    Field("fira", "atm.fira"),
+    Field("raina", "atm.raina"),
+    Field("snowa", "atm.snowa"),
+)
+
+DIAG = (
+    Field("an_upper", "canopy.an_upper", 2),
+    Field("ag_upper", "canopy.ag_upper", 2),
+    Field("an_lower", "canopy.an_lower", 3),
+    Field("ag_lower", "canopy.ag_lower", 3),
+    Field("fwetu", "canopy.fwetu"),
+    Field("fwets", "canopy.fwets"),
+    Field("fwetl", "canopy.fwetl"),
+    Field("rliqu", "canopy.rliqu"),
+    Field("rliqs", "canopy.rliqs"),
+    Field("rliql", "canopy.rliql"),
+    Field("solu", "canopy.solu"),
+    Field("sols", "canopy.sols"),
+    Field("soll", "canopy.soll"),
+    Field("solg", "canopy.solg"),
+    Field("soli", "canopy.soli"),
+    Field("firu", "canopy.firu"),
+    Field("firs", "canopy.firs"),
+    Field("firl", "canopy.firl"),
+    Field("firg", "canopy.firg"),
+    Field("firi", "canopy.firi"),
+    Field("firb", "canopy.firb"),
+    Field("asurd", "canopy.asurd", NBAND),
+    Field("asuri", "canopy.asuri", NBAND),
+    Field("topparu", "canopy.topparu"),
+    Field("topparl", "canopy.topparl"),
+    Field("scalcoefu", "canopy.scalcoefu", 4),
+    Field("scalcoefl", "canopy.scalcoefl", 4),
+    Field("fsenu", "canopy.fsenu"),
+    Field("fsens", "canopy.fsens"),
+    Field("fsenl", "canopy.fsenl"),
+    Field("fseng", "canopy.fseng"),
+    Field("fseni", "canopy.fseni"),
+    Field("fvapg", "canopy.fvapg"),
+    Field("fvapi", "canopy.fvapi"),
+    Field("raing", "canopy.raing"),
+    Field("snowg", "canopy.snowg"),
+    Field("rhoa", "canopy.rhoa"),
+    Field("consoi", "soil.consoi", NSOILAY),
+    Field("hflo", "soil.hflo", NSOILAY + 1),
+    Field("heatg", "soil.heatg"),
+    Field("hvasug", "soil.hvasug"),
+    Field("qglif", "soil.qglif", 4),
+    Field("stresstu", "soil.stresstu"),
+    Field("stresstl", "soil.stresstl"),
+    Field("stressu", "soil.stressu", NSOILAY),
+    Field("stressl", "soil.stressl", NSOILAY),
+    Field("porosflo", "soil.porosflo", NSOILAY),
+    Field("heati", "snow.heati"),
+    Field("hvasui", "snow.hvasui"),
+    Field("ginvap", "hydrology.ginvap"),
+    Field("gsuvap", "hydrology.gsuvap"),
+    Field("gtrans", "hydrology.gtrans"),
+    Field("gtransu", "hydrology.gtransu"),
+    Field("gtransl", "hydrology.gtransl"),
+    Field("grunof", "hydrology.grunof"),
+    Field("gdrain", "hydrology.gdrain"),
+    Field("gadjust", "hydrology.gadjust"),
+    Field("wtot", "hydrology.wtot"),
+    Field("raing_avg", "hydrology.raing_avg"),
+    Field("traing_avg", "hydrology.traing_avg"),
+    Field("fhtop_soil", "hydrology.fhtop_soil"),
+    Field("rainl", "hydrology.rainl"),
+    Field("snowl", "hydrology.snowl"),
+    Field("trainl", "hydrology.trainl"),
+    Field("tsnowl", "hydrology.tsnowl"),
+    Field("sflo_bot", "hydrology.sflo_bot"),
+    Field("fhtop_snow", "hydrology.fhtop_snow"),
+)
+
+ACC = (
+    Field("adrain", "summary.adrain"),
+    Field("adsnow", "summary.adsnow"),
+    Field("adaet", "summary.adaet"),
+    Field("a10ancub", "summary.a10ancub"),
+    Field("a10ancls", "summary.a10ancls"),
+    Field("a10ancl3", "summary.a10ancl3"),
+    Field("a10ancl4", "summary.a10ancl4"),
+    Field("aynpp", "summary.aynpp", NPFT),
+    Field("aynpptot", "summary.aynpptot"),
+    Field("aygpptot", "summary.aygpptot"),
+    Field("aytrunof", "summary.aytrunof"),
+    Field("aytdrain", "summary.aytdrain"),
+    Field("ch4", "acc.ch4_day"),
+    Field("tsoi_mean", "acc.tsoi_day", NSOILAY),
+    Field("wsoi_mean", "acc.wsoi_day", NSOILAY),
+    Field("wisoi_mean", "acc.wisoi_day", NSOILAY),
+    Field("tg_mean", "acc.tg_day"),
+)
+
+GROUPS = {"PROG": PROG, "STAT": STAT, "FORC": FORC, "DIAG": DIAG, "ACC": ACC}
+
+
+def offsets(group):
+    """name -> (first plane, number of planes) for one buffer group."""
+    out, p = {}, 0
+    for f in group:
+        out[f.name] = (p, f.k)
+        p += f.k
+    return out
+
+
+def nplanes(group):
+    return sum(f.k for f in group)
+
+
+N_PROG = nplanes(PROG)
+N_STAT = nplanes(STAT)
+N_FORC = nplanes(FORC)
+N_DIAG = nplanes(DIAG)
+N_ACC = nplanes(ACC)
+
+OFF = {g: offsets(v) for g, v in GROUPS.items()}
+
+
+def leading_dim(ncell: int) -> int:
+    """Plane stride for ``ncell`` cells: rounded up to 32 values (128 bytes in FP32)."""
+    return max(32, (ncell + 31) // 32 * 32)
+
+
+def header_text() -> str:
+    lines = [
+        "/* Generated from ibis_b200/layout.py by header_text(); do not edit by hand.",
+        " *",
+        " * Plane indices of the structure-of-arrays buffers of the hourly step.",
+        " * Element (plane p, cell i) of a buffer with leading dimension ld lives at",
+        " * buf[p * ld + i].  Forcing for a run of nstep hours is nstep consecutive",
+        " * FORC blocks: step s, plane p, cell i at forc[(s * IBIS_FORC_COUNT + p) * ld + i].",
+        " * The ACC buffer holds IBIS_ACC_COUNT value planes followed by the same",
+        " * number of Kahan compensation planes.",
+        " */",
+        "#ifndef IBIS_LAYOUT_H",
+        "#define IBIS_LAYOUT_H",
+        "",
+    ]
+    for g, fields in GROUPS.items():
+        lines.append(f"/* {g} */")
+        lines.append("enum {")
+        for f in fields:
+            off = OFF[g][f.name][0]
+            suffix = f"  /* {f.leaf}, {f.k} planes */" if f.k > 1 else f"  /* {f.leaf} */"
+            lines.append(f"    IBIS_{g}_{f.name.upper()} = {off},{suffix}")
+        lines.append(f"    IBIS_{g}_COUNT = {nplanes(fields)}")
+        lines.append("};")
+        lines.append("")
+    lines.append("#endif /* IBIS_LAYOUT_H */")
+    return "\n".join(lines) + "\n"
+
+
+if __name__ == "__main__":
+    print(header_text(), end="")

@@ -1,0 +1,197 @@
+"""Scalar and small-table parameters of the hourly step.
+
+One flat, all-``double`` record mirrors every parameter the reference's
+``timestep_body`` (``python-port/ibis/timestepping/loops.py:234``) and the
+per-step accumulators of ``_run_day_inner._step_body``
+(``python-port/ibis/timestepping/loops_gswp3.py:115-320``) read from
+``PhysicalConstants``, ``SimParams`` and its sub-modules, plus the static
+fields of ``SnowState``.  Defaults are the reference's defaults (the F77
+branches of ``configs/params/default.yaml``; ``rhosoi_val``/``csoi_mineral_val``
+from ``io/soil_init.py``).
+
+The record is passed by value to the kernels (it lands in the constant bank);
+the C declaration ``IbisParams`` in ``include/ibis_layout.h`` is generated from
+:data:`PARAM_FIELDS` so host and device agree on the layout.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field, fields
+from typing import Sequence
+
+import numpy as np
+
+from . import layout as L
+
+# (name, count, default) -- count > 1 is a fixed-size table
+PARAM_FIELDS: list[tuple[str, int, object]] = [
+    # --- PhysicalConstants (constants.py:16-80)
+    ("stef", 1, 5.67e-8), ("vonk", 1, 0.4), ("grav", 1, 9.80616), ("tmelt", 1, 273.16),
+    ("hvap", 1, 2.5104e6), ("hfus", 1, 0.3336e6), ("hsub", 1, 2.5104e6 + 0.3336e6),
+    ("ch2o", 1, 4.218e3), ("cice", 1, 2.106e3), ("cair", 1, 1.00464e3), ("cvap", 1, 1.81e3),
+    ("rair", 1, 287.04), ("rvap", 1, 461.0), ("cappa", 1, 287.04 / 1.00464e3),
+    ("rhow", 1, 1.0e3), ("epsilon", 1, 1.0e-7),
+    # --- time step (s) and atmospheric CO2 (mol/mol)
+    ("dtime", 1, 3600.0), ("co2conc", 1, 350.0e-6),
+    # --- SnowState static fields (state/snow.py:33-39)
+    ("z0sno", 1, 0.0005), ("rhos", 1, 250.0), ("consno", 1, 0.20), ("hsnotop", 1, 0.05),
+    ("hsnomin", 1, 0.15), ("fimin", 1, 0.00004), ("fimax", 1, 1.00),
+    # --- VegRadParams (radiation.py:32-56), [band][story] with story 0 = lower
+    ("rhoveg", 4, (0.10, 0.10, 0.60, 0.40)), ("tauveg", 4, (0.07, 0.05, 0.25, 0.20)),
+    ("oriev", 2, (0.5, 0.0)), ("orieh", 2, (0.0, 0.0)),
+    ("omegasno", 2, (0.9, 0.7)),
+    # --- CanopyParams (canopy_exchange.py:68-84)
+    ("cleaf", 1, 0.01), ("cstem", 1, 0.01), ("cgrass", 1, 0.01),
+    ("dleaf", 2, (0.10, 0.10)), ("dstem", 2, (0.10, 0.10)),
+    ("alaiml", 1, 8.0), ("alaimu", 1, 8.0), ("chu", 1, 8436.0), ("chs", 1, 2.109e5),
+    ("chl", 1, 8436.0), ("soil_beta_power", 1, 1.0),
+    # --- InterceptionParams (interception.py:31-45)
+    ("wliqumax", 1, 0.20), ("wliqsmax", 1, 0.40), ("wliqlmax", 1, 0.20),
+    ("wsnoumax", 1, 2.00), ("wsnosmax", 1, 4.00), ("wsnolmax", 1, 2.00),
+    ("tdripu", 1, 7200.0), ("tdrips", 1, 7200.0), ("tdripl", 1, 7200.0),
+    ("tblowu", 1, 43200.0), ("tblows", 1, 43200.0), ("tblowl", 1, 43200.0),
+    ("fmax", 1, 0.25),
+    # --- StomataParams (stomata.py:33-161); Ball-Berry groups [broadleaf, conifer, shrub, C4, C3]
+    ("tau15", 1, 4500.0), ("kc15", 1, 1.5e-4), ("ko15", 1, 0.25), ("cimax", 1, 2000.0e-6),
+    ("o2conc", 1, 0.209), ("alpha3", 1, 0.080), ("theta3", 1, 0.950), ("beta3", 1, 0.990),
+    ("alpha4", 1, 0.050), ("theta4", 1, 0.970), ("beta4", 1, 0.800),
+    ("gamma", 5, (0.015, 0.015, 0.015, 0.030, 0.015)),
+    ("coefm", 5, (10.0, 6.0, 9.0, 4.0, 9.0)),
+    ("coefb", 5, (0.010, 0.010, 0.010, 0.040, 0.010)),
+    ("gsmin", 5, (1e-5, 1e-5, 1e-5, 1e-5, 1e-5)),
+    ("vmax_pft", 12, (65e-6, 65e-6, 40e-6, 30e-6, 30e-6, 25e-6,
+                      30e-6, 30e-6, 27.5e-6, 27.5e-6, 15e-6, 25e-6)),
+    ("stressfac", 1, -5.0), ("cap_kn", 1, 0.15),
+    # --- soil constants of SimParams (loops.py:92-111)
+    ("wpudmax", 1, 10.0), ("zwpmax", 1, 0.5), ("bperm", 1, 0.04),
+    ("rhosoi_val", 1, 2650.0 * 0.99 + 1300.0 * 0.01), ("csoi_mineral_val", 1, 870.0 * 0.99 + 1920.0 * 0.01),
+    # --- column geometry: soil layer thicknesses (io/soil_init.py:17), root fractions [layer][lower, upper]
+    ("hsoi", 6, (0.10, 0.15, 0.25, 0.50, 1.00, 2.00)),
+    ("froot", 12, (0.0,) * 12),
+    # --- BedrockParams (bedrock.py:35-66)
+    ("hsoi_bed", 3, (2.0, 2.0, 4.0)), ("consoi_bed", 1, 3.0), ("rhosoi_bed", 1, 2700.0),
+    ("csoi_bed", 1, 740.74074074074076),
+    # --- FireParams used per step (fire.py:205-360)
+    ("d_crit", 1, 0.5), ("vpd_ref", 1, 3.0), ("d_crit_vpd", 1, 0.33),
+    # --- physical clamps read from the environment at trace time (loops.py:665, 1143)
+    ("flux_max", 1, 2000.0), ("t_max_dev", 1, 40.0),
+    # --- MethaneParams (bgc/methane.py:19-91)
+    ("sat_crit", 1, 0.95), ("z_max", 1, 4.0), ("r_ch4", 1, 0.23), ("q10p", 1, 1.60),
+    ("t_ref", 1, 295.15), ("z_wt_max", 1, 0.30), ("z_wt_ref", 1, 0.50), ("z_tau", 1, 0.50),
+    ("tau_oxid", 1, 0.10),
+    # --- BGCParams respiration used by the NPP accumulator (io/parameters.py:248-259)
+    ("rwood", 12, (0.0125,) * 12), ("rroot", 12, (1.25,) * 12), ("rgrowth", 12, (0.30,) * 12),
+    ("ndaypy", 1, 365.0),
+]
+
+#: Compile-time switches carried in ``IbisParams.flags``.
+FLAG_BEDROCK = 1 << 0          # soil.tsoi_deep present: 9-layer heat solve (bedrock.py:88)
+FLAG_H2O_CONSISTENT = 1 << 1   # SimParams.h2o_consistent_weights (soil_physics.py:263)
+FLAG_SUNSHADE_U = 1 << 2       # StomataParams.sunshade_u (stomata.py:140)
+FLAG_SUNSHADE_L = 1 << 3       # StomataParams.sunshade_l
+FLAG_ACC = 1 << 4              # advance the day-loop accumulators (loops_gswp3.py:161-302)
+FLAG_CH4 = 1 << 5              # per-step wetland CH4 into the day accumulator (loops_gswp3.py:307-314)
+FLAG_SOIL_MEANS = 1 << 6       # per-step day means of tsoi/wsoi/wisoi/tg (loops_gswp3.py:316-318)
+FLAG_DIAG = 1 << 7             # write the DIAG buffer
+FLAG_KAHAN = 1 << 8            # compensated accumulation (FP32 kernels)
+
+KNOWN_FLAGS = (FLAG_BEDROCK | FLAG_H2O_CONSISTENT | FLAG_SUNSHADE_U | FLAG_SUNSHADE_L | FLAG_ACC
+               | FLAG_CH4 | FLAG_SOIL_MEANS | FLAG_DIAG | FLAG_KAHAN)
+
+# Default root profile (lower, upper) used by the synthetic columns; the reference keeps froot as a
+# state leaf vegetation.froot of shape (nsoilay, 2) shared by every cell.
+DEFAULT_FROOT = np.array([[0.25, 0.15], [0.25, 0.15], [0.20, 0.20],
+                          [0.15, 0.20], [0.10, 0.15], [0.05, 0.15]])
+
+
+def _ctypes_struct():
+    flds = []
+    for name, n, _ in PARAM_FIELDS:
+        flds.append((name, ctypes.c_double * n if n > 1 else ctypes.c_double))
+    flds.append(("flags", ctypes.c_uint32))
+    flds.append(("_pad", ctypes.c_uint32))
+    return type("IbisParams", (ctypes.Structure,), {"_fields_": flds})
+
+
+IbisParamsC = _ctypes_struct()
+
+
+class StepParams:
+    """Mutable parameter record with the reference defaults.
+
+    Attribute names follow the reference (``params.stomata_params.coefm`` is
+    ``coefm`` here, ``consts.tmelt`` is ``tmelt``).  ``flags`` holds the
+    compile-time switches (``FLAG_*``).
+    """
+
+    def __init__(self, **overrides):
+        for name, n, default in PARAM_FIELDS:
+            val = np.array(default, dtype=np.float64) if n > 1 else float(default)
+            object.__setattr__(self, name, val)
+        self.froot = DEFAULT_FROOT.reshape(-1).copy()
+        self.flags = FLAG_BEDROCK | FLAG_ACC | FLAG_CH4 | FLAG_KAHAN
+        for k, v in overrides.items():
+            setattr(self, k, v)
+
+    def __setattr__(self, key, value):
+        spec = {n: c for n, c, _ in PARAM_FIELDS}
+        if key == "flags":
+            value = int(value)
+            if value & ~KNOWN_FLAGS:
+                raise ValueError(f"unknown flag bits 0x{value & ~KNOWN_FLAGS:x}")
+        elif key in spec:
+            if spec[key] > 1:
+                arr = np.array(value, dtype=np.float64).reshape(-1)
+                if arr.size != spec[key]:
+                    raise ValueError(f"{key} needs {spec[key]} values, got {arr.size}")
+                value = arr
+            else:
+                value = float(value)
+        else:
+            raise AttributeError(f"no parameter named {key!r}")
+        object.__setattr__(self, key, value)
+
+    # convenience views
+    @property
+    def froot2(self) -> np.ndarray:
+        """Root fractions as (nsoilay, 2) [lower, upper], like ``vegetation.froot``."""
+        return np.asarray(self.froot).reshape(L.NSOILAY, 2)
+
+    def has(self, flag: int) -> bool:
+        return bool(self.flags & flag)
+
+    def copy(self) -> "StepParams":
+        out = StepParams()
+        for name, n, _ in PARAM_FIELDS:
+            v = getattr(self, name)
+            object.__setattr__(out, name, v.copy() if n > 1 else v)
+        out.flags = self.flags
+        return out
+
+    def to_c(self):
+        s = IbisParamsC()
+        for name, n, _ in PARAM_FIELDS:
+            v = getattr(self, name)
+            if n > 1:
+                getattr(s, name)[:] = [float(x) for x in v]
+            else:
+                setattr(s, name, float(v))
+        s.flags = self.flags
+        return s
+
+
+def header_struct_text() -> str:
+    lines = ["/* Parameter record of the hourly step (all double; passed by value). */",
+             "typedef struct IbisParams {"]
+    for name, n, _ in PARAM_FIELDS:
+        lines.append(f"    double {name}[{n}];" if n > 1 else f"    double {name};")
+    lines.append("    unsigned int flags;   /* IBIS_FLAG_* */")
+    lines.append("    unsigned int _pad;")
+    lines.append("} IbisParams;")
+    lines.append("")
+    for nm, val in [("BEDROCK", FLAG_BEDROCK), ("H2O_CONSISTENT", FLAG_H2O_CONSISTENT),
+                    ("SUNSHADE_U", FLAG_SUNSHADE_U), ("SUNSHADE_L", FLAG_SUNSHADE_L),
+                    ("ACC", FLAG_ACC), ("CH4", FLAG_CH4), ("SOIL_MEANS", FLAG_SOIL_MEANS),
+                    ("DIAG", FLAG_DIAG), ("KAHAN", FLAG_KAHAN)]:
+        lines.append(f"#define IBIS_FLAG_{nm} {val}u")
+    return "\n".join(lines) + "\n"

@@ -1,0 +1,316 @@
+/* Generated from ibis_b200/layout.py by header_text(); do not edit by hand.
+ *
+ * Plane indices of the structure-of-arrays buffers of the hourly step.
+ * Element (plane p, cell i) of a buffer with leading dimension ld lives at
+ * buf[p * ld + i].  Forcing for a run of nstep hours is nstep consecutive
+ * FORC blocks: step s, plane p, cell i at forc[(s * IBIS_FORC_COUNT + p) * ld + i].
+ * The ACC buffer holds IBIS_ACC_COUNT value planes followed by the same
+ * number of Kahan compensation planes.
+ */
+#ifndef IBIS_LAYOUT_H
+#define IBIS_LAYOUT_H
+
+/* PROG */
+enum {
+    IBIS_PROG_TSOI = 0,  /* soil.tsoi, 6 planes */
+    IBIS_PROG_WSOI = 6,  /* soil.wsoi, 6 planes */
+    IBIS_PROG_WISOI = 12,  /* soil.wisoi, 6 planes */
+    IBIS_PROG_TG = 18,  /* soil.tg */
+    IBIS_PROG_WPUD = 19,  /* soil.wpud */
+    IBIS_PROG_WIPUD = 20,  /* soil.wipud */
+    IBIS_PROG_TSOI_DEEP = 21,  /* soil.tsoi_deep, 3 planes */
+    IBIS_PROG_FI = 24,  /* snow.fi */
+    IBIS_PROG_TSNO = 25,  /* snow.tsno, 3 planes */
+    IBIS_PROG_HSNO = 28,  /* snow.hsno, 3 planes */
+    IBIS_PROG_TI = 31,  /* snow.ti */
+    IBIS_PROG_TLSUB = 32,  /* snow.tlsub */
+    IBIS_PROG_TU = 33,  /* canopy.tu */
+    IBIS_PROG_TS = 34,  /* canopy.ts */
+    IBIS_PROG_TL = 35,  /* canopy.tl */
+    IBIS_PROG_T12 = 36,  /* canopy.t12 */
+    IBIS_PROG_T34 = 37,  /* canopy.t34 */
+    IBIS_PROG_Q12 = 38,  /* canopy.q12 */
+    IBIS_PROG_Q34 = 39,  /* canopy.q34 */
+    IBIS_PROG_WLIQU = 40,  /* canopy.wliqu */
+    IBIS_PROG_WLIQS = 41,  /* canopy.wliqs */
+    IBIS_PROG_WLIQL = 42,  /* canopy.wliql */
+    IBIS_PROG_WSNOU = 43,  /* canopy.wsnou */
+    IBIS_PROG_WSNOS = 44,  /* canopy.wsnos */
+    IBIS_PROG_WSNOL = 45,  /* canopy.wsnol */
+    IBIS_PROG_CI_UPPER = 46,  /* canopy.ci_upper, 2 planes */
+    IBIS_PROG_GS_UPPER = 48,  /* canopy.gs_upper, 2 planes */
+    IBIS_PROG_CS_UPPER = 50,  /* canopy.cs_upper, 2 planes */
+    IBIS_PROG_CI_LOWER = 52,  /* canopy.ci_lower, 3 planes */
+    IBIS_PROG_GS_LOWER = 55,  /* canopy.gs_lower, 3 planes */
+    IBIS_PROG_CS_LOWER = 58,  /* canopy.cs_lower, 3 planes */
+    IBIS_PROG_A10SCALPARAMU = 61,  /* canopy.a10scalparamu */
+    IBIS_PROG_A10DAYLIGHTU = 62,  /* canopy.a10daylightu */
+    IBIS_PROG_A10SCALPARAML = 63,  /* canopy.a10scalparaml */
+    IBIS_PROG_A10DAYLIGHTL = 64,  /* canopy.a10daylightl */
+    IBIS_PROG_FIREFAC = 65,  /* vegetation.firefac */
+    IBIS_PROG_NYTIMES = 66,  /* vegetation.nytimes */
+    IBIS_PROG_NFIRESTEP = 67,  /* vegetation.nfirestep */
+    IBIS_PROG_SDRY = 68,  /* vegetation.sdry */
+    IBIS_PROG_NFIRESTEP_VPD = 69,  /* vegetation.nfirestep_vpd */
+    IBIS_PROG_SDRY_VPD = 70,  /* vegetation.sdry_vpd */
+    IBIS_PROG_COUNT = 71
+};
+
+/* STAT */
+enum {
+    IBIS_STAT_POROS = 0,  /* soil.poros, 6 planes */
+    IBIS_STAT_HYDRAUL = 6,  /* soil.hydraul, 6 planes */
+    IBIS_STAT_SUCTION = 12,  /* soil.suction, 6 planes */
+    IBIS_STAT_BEX = 18,  /* soil.bex, 6 planes */
+    IBIS_STAT_SFIELD = 24,  /* soil.sfield, 6 planes */
+    IBIS_STAT_SWILT = 30,  /* soil.swilt, 6 planes */
+    IBIS_STAT_SAND = 36,  /* soil.sand, 6 planes */
+    IBIS_STAT_CLAY = 42,  /* soil.clay, 6 planes */
+    IBIS_STAT_CSOI = 48,  /* soil.csoi, 6 planes */
+    IBIS_STAT_RHOSOI = 54,  /* soil.rhosoi, 6 planes */
+    IBIS_STAT_ALBSAV = 60,  /* soil.albsav */
+    IBIS_STAT_ALBSAN = 61,  /* soil.albsan */
+    IBIS_STAT_Z0SOI = 62,  /* soil.z0soi */
+    IBIS_STAT_LAI = 63,  /* vegetation.lai, 2 planes */
+    IBIS_STAT_SAI = 65,  /* vegetation.sai, 2 planes */
+    IBIS_STAT_ZTOP = 67,  /* vegetation.ztop, 2 planes */
+    IBIS_STAT_ZBOT = 69,  /* vegetation.zbot, 2 planes */
+    IBIS_STAT_FU = 71,  /* vegetation.fu */
+    IBIS_STAT_FL = 72,  /* vegetation.fl */
+    IBIS_STAT_FRAC = 73,  /* vegetation.frac, 12 planes */
+    IBIS_STAT_EXIST = 85,  /* vegetation.exist, 12 planes */
+    IBIS_STAT_CBIOW = 97,  /* vegetation.cbiow, 12 planes */
+    IBIS_STAT_CBIOR = 109,  /* vegetation.cbior, 12 planes */
+    IBIS_STAT_SAPFRAC = 121,  /* vegetation.sapfrac */
+    IBIS_STAT_TCO2MIC = 122,  /* vegetation.tco2mic */
+    IBIS_STAT_F_INUND = 123,  /* methane.f_inund */
+    IBIS_STAT_COUNT = 124
+};
+
+/* FORC */
+enum {
+    IBIS_FORC_TA = 0,  /* atm.ta */
+    IBIS_FORC_QA = 1,  /* atm.qa */
+    IBIS_FORC_UA = 2,  /* atm.ua */
+    IBIS_FORC_PSURF = 3,  /* atm.psurf */
+    IBIS_FORC_COSZEN = 4,  /* atm.coszen */
+    IBIS_FORC_SOLAD = 5,  /* atm.solad, 2 planes */
+    IBIS_FORC_SOLAI = 7,  /* atm.solai, 2 planes */
+    IBIS_FORC_FIRA = 9,  /* atm.fira */
+    IBIS_FORC_RAINA = 10,  /* atm.raina */
+    IBIS_FORC_SNOWA = 11,  /* atm.snowa */
+    IBIS_FORC_COUNT = 12
+};
+
+/* DIAG */
+enum {
+    IBIS_DIAG_AN_UPPER = 0,  /* canopy.an_upper, 2 planes */
+    IBIS_DIAG_AG_UPPER = 2,  /* canopy.ag_upper, 2 planes */
+    IBIS_DIAG_AN_LOWER = 4,  /* canopy.an_lower, 3 planes */
+    IBIS_DIAG_AG_LOWER = 7,  /* canopy.ag_lower, 3 planes */
+    IBIS_DIAG_FWETU = 10,  /* canopy.fwetu */
+    IBIS_DIAG_FWETS = 11,  /* canopy.fwets */
+    IBIS_DIAG_FWETL = 12,  /* canopy.fwetl */
+    IBIS_DIAG_RLIQU = 13,  /* canopy.rliqu */
+    IBIS_DIAG_RLIQS = 14,  /* canopy.rliqs */
+    IBIS_DIAG_RLIQL = 15,  /* canopy.rliql */
+    IBIS_DIAG_SOLU = 16,  /* canopy.solu */
+    IBIS_DIAG_SOLS = 17,  /* canopy.sols */
+    IBIS_DIAG_SOLL = 18,  /* canopy.soll */
+    IBIS_DIAG_SOLG = 19,  /* canopy.solg */
+    IBIS_DIAG_SOLI = 20,  /* canopy.soli */
+    IBIS_DIAG_FIRU = 21,  /* canopy.firu */
+    IBIS_DIAG_FIRS = 22,  /* canopy.firs */
+    IBIS_DIAG_FIRL = 23,  /* canopy.firl */
+    IBIS_DIAG_FIRG = 24,  /* canopy.firg */
+    IBIS_DIAG_FIRI = 25,  /* canopy.firi */
+    IBIS_DIAG_FIRB = 26,  /* canopy.firb */
+    IBIS_DIAG_ASURD = 27,  /* canopy.asurd, 2 planes */
+    IBIS_DIAG_ASURI = 29,  /* canopy.asuri, 2 planes */
+    IBIS_DIAG_TOPPARU = 31,  /* canopy.topparu */
+    IBIS_DIAG_TOPPARL = 32,  /* canopy.topparl */
+    IBIS_DIAG_SCALCOEFU = 33,  /* canopy.scalcoefu, 4 planes */
+    IBIS_DIAG_SCALCOEFL = 37,  /* canopy.scalcoefl, 4 planes */
+    IBIS_DIAG_FSENU = 41,  /* canopy.fsenu */
+    IBIS_DIAG_FSENS = 42,  /* canopy.fsens */
+    IBIS_DIAG_FSENL = 43,  /* canopy.fsenl */
+    IBIS_DIAG_FSENG = 44,  /* canopy.fseng */
+    IBIS_DIAG_FSENI = 45,  /* canopy.fseni */
+    IBIS_DIAG_FVAPG = 46,  /* canopy.fvapg */
+    IBIS_DIAG_FVAPI = 47,  /* canopy.fvapi */
+    IBIS_DIAG_RAING = 48,  /* canopy.raing */
+    IBIS_DIAG_SNOWG = 49,  /* canopy.snowg */
+    IBIS_DIAG_RHOA = 50,  /* canopy.rhoa */
+    IBIS_DIAG_CONSOI = 51,  /* soil.consoi, 6 planes */
+    IBIS_DIAG_HFLO = 57,  /* soil.hflo, 7 planes */
+    IBIS_DIAG_HEATG = 64,  /* soil.heatg */
+    IBIS_DIAG_HVASUG = 65,  /* soil.hvasug */
+    IBIS_DIAG_QGLIF = 66,  /* soil.qglif, 4 planes */
+    IBIS_DIAG_STRESSTU = 70,  /* soil.stresstu */
+    IBIS_DIAG_STRESSTL = 71,  /* soil.stresstl */
+    IBIS_DIAG_STRESSU = 72,  /* soil.stressu, 6 planes */
+    IBIS_DIAG_STRESSL = 78,  /* soil.stressl, 6 planes */
+    IBIS_DIAG_POROSFLO = 84,  /* soil.porosflo, 6 planes */
+    IBIS_DIAG_HEATI = 90,  /* snow.heati */
+    IBIS_DIAG_HVASUI = 91,  /* snow.hvasui */
+    IBIS_DIAG_GINVAP = 92,  /* hydrology.ginvap */
+    IBIS_DIAG_GSUVAP = 93,  /* hydrology.gsuvap */
+    IBIS_DIAG_GTRANS = 94,  /* hydrology.gtrans */
+    IBIS_DIAG_GTRANSU = 95,  /* hydrology.gtransu */
+    IBIS_DIAG_GTRANSL = 96,  /* hydrology.gtransl */
+    IBIS_DIAG_GRUNOF = 97,  /* hydrology.grunof */
+    IBIS_DIAG_GDRAIN = 98,  /* hydrology.gdrain */
+    IBIS_DIAG_GADJUST = 99,  /* hydrology.gadjust */
+    IBIS_DIAG_WTOT = 100,  /* hydrology.wtot */
+    IBIS_DIAG_RAING_AVG = 101,  /* hydrology.raing_avg */
+    IBIS_DIAG_TRAING_AVG = 102,  /* hydrology.traing_avg */
+    IBIS_DIAG_FHTOP_SOIL = 103,  /* hydrology.fhtop_soil */
+    IBIS_DIAG_RAINL = 104,  /* hydrology.rainl */
+    IBIS_DIAG_SNOWL = 105,  /* hydrology.snowl */
+    IBIS_DIAG_TRAINL = 106,  /* hydrology.trainl */
+    IBIS_DIAG_TSNOWL = 107,  /* hydrology.tsnowl */
+    IBIS_DIAG_SFLO_BOT = 108,  /* hydrology.sflo_bot */
+    IBIS_DIAG_FHTOP_SNOW = 109,  /* hydrology.fhtop_snow */
+    IBIS_DIAG_COUNT = 110
+};
+
+/* ACC */
+enum {
+    IBIS_ACC_ADRAIN = 0,  /* summary.adrain */
+    IBIS_ACC_ADSNOW = 1,  /* summary.adsnow */
+    IBIS_ACC_ADAET = 2,  /* summary.adaet */
+    IBIS_ACC_A10ANCUB = 3,  /* summary.a10ancub */
+    IBIS_ACC_A10ANCLS = 4,  /* summary.a10ancls */
+    IBIS_ACC_A10ANCL3 = 5,  /* summary.a10ancl3 */
+    IBIS_ACC_A10ANCL4 = 6,  /* summary.a10ancl4 */
+    IBIS_ACC_AYNPP = 7,  /* summary.aynpp, 12 planes */
+    IBIS_ACC_AYNPPTOT = 19,  /* summary.aynpptot */
+    IBIS_ACC_AYGPPTOT = 20,  /* summary.aygpptot */
+    IBIS_ACC_AYTRUNOF = 21,  /* summary.aytrunof */
+    IBIS_ACC_AYTDRAIN = 22,  /* summary.aytdrain */
+    IBIS_ACC_CH4 = 23,  /* acc.ch4_day */
+    IBIS_ACC_TSOI_MEAN = 24,  /* acc.tsoi_day, 6 planes */
+    IBIS_ACC_WSOI_MEAN = 30,  /* acc.wsoi_day, 6 planes */
+    IBIS_ACC_WISOI_MEAN = 36,  /* acc.wisoi_day, 6 planes */
+    IBIS_ACC_TG_MEAN = 42,  /* acc.tg_day */
+    IBIS_ACC_COUNT = 43
+};
+
+/* Parameter record of the hourly step (all double; passed by value). */
+typedef struct IbisParams {
+    double stef;
+    double vonk;
+    double grav;
+    double tmelt;
+    double hvap;
+    double hfus;
+    double hsub;
+    double ch2o;
+    double cice;
+    double cair;
+    double cvap;
+    double rair;
+    double rvap;
+    double cappa;
+    double rhow;
+    double epsilon;
+    double dtime;
+    double co2conc;
+    double z0sno;
+    double rhos;
+    double consno;
+    double hsnotop;
+    double hsnomin;
+    double fimin;
+    double fimax;
+    double rhoveg[4];
+    double tauveg[4];
+    double oriev[2];
+    double orieh[2];
+    double omegasno[2];
+    double cleaf;
+    double cstem;
+    double cgrass;
+    double dleaf[2];
+    double dstem[2];
+    double alaiml;
+    double alaimu;
+    double chu;
+    double chs;
+    double chl;
+    double soil_beta_power;
+    double wliqumax;
+    double wliqsmax;
+    double wliqlmax;
+    double wsnoumax;
+    double wsnosmax;
+    double wsnolmax;
+    double tdripu;
+    double tdrips;
+    double tdripl;
+    double tblowu;
+    double tblows;
+    double tblowl;
+    double fmax;
+    double tau15;
+    double kc15;
+    double ko15;
+    double cimax;
+    double o2conc;
+    double alpha3;
+    double theta3;
+    double beta3;
+    double alpha4;
+    double theta4;
+    double beta4;
+    double gamma[5];
+    double coefm[5];
+    double coefb[5];
+    double gsmin[5];
+    double vmax_pft[12];
+    double stressfac;
+    double cap_kn;
+    double wpudmax;
+    double zwpmax;
+    double bperm;
+    double rhosoi_val;
+    double csoi_mineral_val;
+    double hsoi[6];
+    double froot[12];
+    double hsoi_bed[3];
+    double consoi_bed;
+    double rhosoi_bed;
+    double csoi_bed;
+    double d_crit;
+    double vpd_ref;
+    double d_crit_vpd;
+    double flux_max;
+    double t_max_dev;
+    double sat_crit;
+    double z_max;
+    double r_ch4;
+    double q10p;
+    double t_ref;
+    double z_wt_max;
+    double z_wt_ref;
+    double z_tau;
+    double tau_oxid;
+    double rwood[12];
+    double rroot[12];
+    double rgrowth[12];
+    double ndaypy;
+    unsigned int flags;   /* IBIS_FLAG_* */
+    unsigned int _pad;
+} IbisParams;
+
+#define IBIS_FLAG_BEDROCK 1u
+#define IBIS_FLAG_H2O_CONSISTENT 2u
+#define IBIS_FLAG_SUNSHADE_U 4u
+#define IBIS_FLAG_SUNSHADE_L 8u
+#define IBIS_FLAG_ACC 16u
+#define IBIS_FLAG_CH4 32u
+#define IBIS_FLAG_SOIL_MEANS 64u
+#define IBIS_FLAG_DIAG 128u
+#define IBIS_FLAG_KAHAN 256u
+
+#endif /* IBIS_LAYOUT_H */

@@ -1,0 +1,268 @@
+"""Generate golden fixtures by running the REFERENCE's own hourly step.
+
+The reference (UW-GCRL/ibis, ``python-port/``) is JAX + Equinox code and
+neither is installed here, so this script puts a small NumPy-backed stand-in
+for ``jax``/``jax.numpy``/``equinox`` (``tests/golden/jaxshim``) first on
+``sys.path`` and imports the reference package unmodified from
+``/root/reference/python-port``.  It then runs, in float64:
+
+* ``ibis.timestepping.loops.timestep_body`` hour by hour, recording the state
+  it returns (prognostic and diagnostic leaves), and
+* ``ibis.timestepping.loops_gswp3._run_day_inner`` for one day with the
+  wetland-CH4 and soil-mean accumulators on, with its weather generator
+  ``diurnal`` replaced by the synthetic forcing and its per-step float32 cast
+  replaced by the identity (the float64 reference run),
+
+on seeded synthetic columns from ``ibis_b200.synth``, and writes the inputs
+and outputs to ``tests/golden/<case>.npz``.  The fixtures travel with the
+repository; this script only runs where ``/root/reference`` exists.
+
+Usage:  python tests/golden/make_golden.py [--check]
+"""
+from __future__ import annotations
+
+import argparse
+import dataclasses
+import os
+import sys
+import types
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+REF = "/root/reference/python-port"
+
+os.environ.pop("IBIS_FLUX_MAX", None)
+os.environ.pop("IBIS_T_MAX_DEV", None)
+sys.path.insert(0, os.path.join(HERE, "jaxshim"))
+sys.path.insert(0, REF)
+sys.path.insert(0, REPO)
+
+import jax.numpy as jnp  # noqa: E402  (the NumPy stand-in)
+import equinox as eqx  # noqa: E402
+from ibis.constants import get_constants  # noqa: E402
+from ibis.dimensions import GridConfig  # noqa: E402
+from ibis.state.model_state import create_ibis_state  # noqa: E402
+from ibis.timestepping import loops, loops_gswp3  # noqa: E402
+from ibis.physics.bedrock import BedrockParams  # noqa: E402
+from ibis.bgc.methane import MethaneParams  # noqa: E402
+
+from ibis_b200 import layout as L  # noqa: E402
+from ibis_b200 import synth  # noqa: E402
+from ibis_b200.params import (StepParams, FLAG_BEDROCK, FLAG_H2O_CONSISTENT, FLAG_SUNSHADE_U,  # noqa: E402
+                              FLAG_SUNSHADE_L, FLAG_ACC, FLAG_CH4, FLAG_SOIL_MEANS)
+
+
+def _a(x):
+    return jnp.asarray(np.asarray(x, dtype=np.float64))
+
+
+def reference_state(wl):
+    """IBISState (float64) holding the workload's prognostic and static fields."""
+    n = wl.ncell
+    bed = bool(wl.params.flags & FLAG_BEDROCK)
+    st = create_ibis_state(GridConfig(nlon=2, nlat=1, npoi=n, nbedrock=3 if bed else 0))
+    P, S = wl.prog, wl.stat
+    hsoi = np.zeros(L.NSOILAY + 1)
+    hsoi[:L.NSOILAY] = wl.params.hsoi
+    soil_fields = {f.leaf.split(".")[1]: f.name for f in L.PROG + L.STAT if f.leaf.startswith("soil.")}
+    if not bed:
+        soil_fields.pop("tsoi_deep")
+    src = {**S, **P}
+    soil = st.soil
+    for leaf, name in soil_fields.items():
+        soil = dataclasses.replace(soil, **{leaf: _a(src[name])})
+    soil = dataclasses.replace(soil, hsoi=_a(hsoi))
+    snow = st.snow
+    for f in L.PROG:
+        if f.leaf.startswith("snow."):
+            snow = dataclasses.replace(snow, **{f.leaf.split(".")[1]: _a(P[f.name])})
+    can = st.canopy
+    for f in L.PROG:
+        if f.leaf.startswith("canopy."):
+            can = dataclasses.replace(can, **{f.leaf.split(".")[1]: _a(P[f.name])})
+    veg = st.vegetation
+    for f in L.PROG + L.STAT:
+        if f.leaf.startswith("vegetation.") and f.name != "nytimes":
+            veg = dataclasses.replace(veg, **{f.leaf.split(".")[1]: _a(src[f.name])})
+    veg = dataclasses.replace(veg, nytimes=_a(P["nytimes"][0]), froot=_a(wl.params.froot2))
+    atm = dataclasses.replace(st.atm, co2conc=float(wl.params.co2conc))
+    return dataclasses.replace(st, soil=soil, snow=snow, canopy=can, vegetation=veg, atm=atm)
+
+
+def reference_params(wl):
+    p = wl.params
+    sp = loops.default_sim_params(wl.ncell)
+    stom = dataclasses.replace(
+        sp.stomata_params, coefm=_a(p.coefm), coefb=_a(p.coefb), gamma=_a(p.gamma), gsmin=_a(p.gsmin),
+        vmax_pft=_a(p.vmax_pft), stressfac=float(p.stressfac),
+        sunshade_u=bool(p.flags & FLAG_SUNSHADE_U), sunshade_l=bool(p.flags & FLAG_SUNSHADE_L))
+    canp = sp.canopy._replace(soil_beta_power=float(p.soil_beta_power))
+    ip = sp.interception._replace(wliqumax=float(p.wliqumax), wliqsmax=float(p.wliqsmax),
+                                  wliqlmax=float(p.wliqlmax), fmax=float(p.fmax))
+    meth = MethaneParams(r_ch4=float(p.r_ch4), q10p=float(p.q10p), z_tau=float(p.z_tau),
+                         tau_oxid=float(p.tau_oxid), z_wt_max=float(p.z_wt_max))
+    bgc = dataclasses.replace(sp.bgc_params, rwood=_a(p.rwood), rroot=_a(p.rroot), rgrowth=_a(p.rgrowth))
+    return dataclasses.replace(
+        sp, stomata_params=stom, canopy=canp, interception=ip, methane=meth, bgc_params=bgc,
+        latitude=_a(np.deg2rad(wl.latitude)),
+        bedrock=BedrockParams() if p.flags & FLAG_BEDROCK else None,
+        h2o_consistent_weights=bool(p.flags & FLAG_H2O_CONSISTENT))
+
+
+def set_forcing(st, F):
+    atm = st.atm
+    for f in L.FORC:
+        atm = dataclasses.replace(atm, **{f.leaf.split(".")[1]: _a(F[f.name])})
+    return dataclasses.replace(st, atm=atm)
+
+
+def get(obj, path):
+    for part in path.split("."):
+        obj = getattr(obj, part)
+    return np.asarray(obj, dtype=np.float64)
+
+
+def snapshot(st):
+    out = {}
+    for f in L.PROG:
+        if f.name == "tsoi_deep" and st.soil.tsoi_deep is None:
+            continue
+        v = get(st, f.leaf)
+        out["prog." + f.name] = np.broadcast_to(v, (st.soil.tg.shape[0],) + v.shape[1:]) if f.name == "nytimes" else v
+    for f in L.DIAG:
+        out["diag." + f.name] = get(st, f.leaf)
+    return out
+
+
+def run_steps(wl, record):
+    consts = get_constants()
+    params = reference_params(wl)
+    st = reference_state(wl)
+    snaps = {}
+    for h in range(wl.nhour):
+        st = set_forcing(st, wl.forcing_at(h))
+        st = loops.timestep_body(st, consts, params, float(wl.params.dtime))
+        if (h + 1) in record:
+            snaps[h + 1] = snapshot(st)
+    return snaps
+
+
+def run_day_accumulators(wl):
+    """_run_day_inner over 24 hourly steps with CH4 and soil means on."""
+    assert wl.nhour == 24
+    consts = get_constants()
+    params = reference_params(wl)
+    st = reference_state(wl)
+    F = wl.forc
+
+    def fake_diurnal(time, jday, dw, lat, plens, startp, endp, key, dtime, nband=2):
+        h = int(round(float(time) / float(dtime)))
+        hw = types.SimpleNamespace(coszen=_a(F["coszen"][h]), ta=_a(F["ta"][h]), qa=_a(F["qa"][h]),
+                                   ua=_a(F["ua"][h]), solad=_a(F["solad"][h]), solai=_a(F["solai"][h]),
+                                   raina=_a(F["raina"][h]), snowa=_a(F["snowa"][h]), fira=_a(F["fira"][h]))
+        return key, hw
+
+    saved = (loops_gswp3.diurnal, loops_gswp3._cast_tree_f32)
+    loops_gswp3.diurnal = fake_diurnal
+    loops_gswp3._cast_tree_f32 = lambda tree: tree
+    try:
+        dw = types.SimpleNamespace(psurf=_a(F["psurf"][0]))
+        n = wl.ncell
+        z = _a(np.zeros(n))
+        key = jnp.asarray(np.array([0, 1], dtype=np.uint32))
+        st_out, _, acc = loops_gswp3._run_day_inner(
+            st, consts, params, dw, _a(F["fira"][0]), z, z, z, jnp.asarray(np.int32(wl.start_doy)), key,
+            float(wl.params.dtime), ch4=(_a(wl.stat["f_inund"]), params.methane, None), soil_means=True)
+    finally:
+        loops_gswp3.diurnal, loops_gswp3._cast_tree_f32 = saved
+    out = snapshot(st_out)
+    for f in L.ACC:
+        if f.leaf.startswith("summary."):
+            out["acc." + f.name] = get(st_out, f.leaf)
+    out["acc.ch4"] = np.asarray(acc[0], dtype=np.float64)
+    out["acc.tsoi_mean"] = np.asarray(acc[1], dtype=np.float64)
+    out["acc.wsoi_mean"] = np.asarray(acc[2], dtype=np.float64)
+    out["acc.wisoi_mean"] = np.asarray(acc[3], dtype=np.float64)
+    out["acc.tg_mean"] = np.asarray(acc[4], dtype=np.float64)
+    return out
+
+
+def pack_inputs(wl):
+    d = {}
+    for k, v in wl.prog.items():
+        d["in.prog." + k] = v
+    for k, v in wl.stat.items():
+        d["in.stat." + k] = v
+    for k, v in wl.forc.items():
+        d["in.forc." + k] = v
+    from ibis_b200.params import PARAM_FIELDS
+    for name, _, _ in PARAM_FIELDS:
+        d["in.param." + name] = np.asarray(getattr(wl.params, name), dtype=np.float64)
+    d["in.param.flags"] = np.asarray(wl.params.flags, dtype=np.int64)
+    d["in.latitude"] = wl.latitude
+    d["in.start_doy"] = np.asarray(wl.start_doy)
+    return d
+
+
+CASES = {
+    # 16 cells incl. bare/snowpack/frozen/flooded/polar-night/desert columns, bedrock, one day with accumulators
+    "day_mixed": dict(ncell=16, nhour=24, seed=11, edge_cases=True, record=(1, 2, 6, 24), day=True),
+    # soil column without bedrock, consistent soil-water weights
+    "nobedrock": dict(ncell=8, nhour=6, seed=12, edge_cases=True, record=(1, 6), bedrock=False,
+                      flags_on=FLAG_H2O_CONSISTENT),
+    # sunlit/shaded two-big-leaf canopies on both stories
+    "sunshade": dict(ncell=8, nhour=6, seed=13, edge_cases=True, record=(1, 6),
+                     flags_on=FLAG_SUNSHADE_U | FLAG_SUNSHADE_L),
+    # perturbed calibration parameters (the 31-parameter vector) and a soil-evaporation exponent
+    "perturbed": dict(ncell=8, nhour=6, seed=14, edge_cases=False, record=(1, 6), perturb=True),
+}
+
+
+def build_case(name, spec):
+    wl = synth.make_workload(spec["ncell"], spec["nhour"], seed=spec["seed"], edge_cases=spec["edge_cases"],
+                             bedrock=spec.get("bedrock", True))
+    wl.params.flags = wl.params.flags | spec.get("flags_on", 0)
+    if spec.get("day"):
+        wl.params.flags = wl.params.flags | FLAG_ACC | FLAG_CH4 | FLAG_SOIL_MEANS
+        # the day loop takes one longwave value per day (GSWP3 rlds): make the forcing match
+        wl.forc["fira"][:] = wl.forc["fira"][0][None, :]
+    if spec.get("perturb"):
+        rng = np.random.Generator(np.random.PCG64(spec["seed"] + 1000))
+        f = lambda v: np.asarray(v) * np.exp(rng.uniform(np.log(0.5), np.log(1.5), size=np.shape(v)))
+        p = wl.params
+        p.vmax_pft, p.coefm = f(p.vmax_pft), f(p.coefm)
+        p.stressfac, p.soil_beta_power = f(p.stressfac), 2.0
+        p.wliqumax, p.wliqsmax, p.wliqlmax, p.fmax = f(p.wliqumax), f(p.wliqsmax), f(p.wliqlmax), f(p.fmax)
+        p.r_ch4, p.q10p, p.z_tau, p.tau_oxid, p.z_wt_max = (f(p.r_ch4), f(p.q10p), f(p.z_tau), f(p.tau_oxid),
+                                                            f(p.z_wt_max))
+        p.rwood, p.rroot, p.rgrowth = (np.full(12, f(p.rwood[0])), np.full(12, f(p.rroot[0])),
+                                        np.full(12, f(p.rgrowth[0])))
+    return wl
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--only", default=None)
+    args = ap.parse_args()
+    for name, spec in CASES.items():
+        if args.only and name != args.only:
+            continue
+        wl = build_case(name, spec)
+        out = pack_inputs(wl)
+        snaps = run_steps(wl, set(spec["record"]))
+        for h, s in snaps.items():
+            for k, v in s.items():
+                out[f"out.{h}.{k}"] = v
+        if spec.get("day"):
+            for k, v in run_day_accumulators(wl).items():
+                out[f"day.{k}"] = v
+        out["meta.record"] = np.asarray(spec["record"])
+        path = os.path.join(HERE, f"{name}.npz")
+        np.savez_compressed(path, **out)
+        print(f"wrote {path}: {len(out)} arrays, {os.path.getsize(path)} bytes")
+
+
+if __name__ == "__main__":
+    main()
