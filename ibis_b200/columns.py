@@ -1,0 +1,131 @@
+"""Device-resident column state and the launch of the hourly-step kernels.
+
+A :class:`Columns` owns the structure-of-arrays buffers of ``ncell`` columns on
+one GPU (torch tensors are used only as device allocations) and advances them
+through the C ABI of ``include/ibis_b200.h``.  Forcing for ``nstep`` hours is a
+``(nstep, IBIS_FORC_COUNT, ld)`` device tensor; the whole run executes in one
+launch, so prognostic state stays in registers across the hours.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import layout as L
+from . import lib as _lib
+from . import synth
+from .params import StepParams, FLAG_DIAG, FLAG_ACC, FLAG_CH4, FLAG_SOIL_MEANS
+
+INT_MAX = 2 ** 31 - 1
+_ACC_FLAGS = FLAG_ACC | FLAG_CH4 | FLAG_SOIL_MEANS
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else ctypes.c_void_p(0)
+
+
+class Columns:
+    """``ncell`` IBIS columns resident on ``device`` in FP32 (default) or FP64."""
+
+    def __init__(self, ncell: int, dtype=torch.float32, device="cuda", diag: bool = False, acc: bool = True):
+        if dtype not in (torch.float32, torch.float64):
+            raise ValueError("dtype must be torch.float32 or torch.float64")
+        self.ncell = int(ncell)
+        self.ld = L.leading_dim(self.ncell)
+        self.dtype = dtype
+        dev = torch.device(device)
+        if dev.type != "cuda":
+            raise ValueError("Columns live on a CUDA device; there is no host implementation")
+        if dev.index is None:
+            dev = torch.device("cuda", torch.cuda.current_device())
+        self.device = dev
+        kw = dict(dtype=dtype, device=self.device)
+        self.prog = torch.zeros((L.N_PROG, self.ld), **kw)
+        self.stat = torch.zeros((L.N_STAT, self.ld), **kw)
+        self.diag = torch.zeros((L.N_DIAG, self.ld), **kw) if diag else None
+        self.acc = torch.zeros((2 * L.N_ACC, self.ld), **kw) if acc else None
+        self.status = torch.tensor([0, INT_MAX], dtype=torch.int32, device=self.device)
+        self._np_dtype = np.float32 if dtype == torch.float32 else np.float64
+        self._fn = _lib.load().ibis_step_f32 if dtype == torch.float32 else _lib.load().ibis_step_f64
+
+    # -------------------------------------------------------------- transfer
+    @classmethod
+    def from_host(cls, prog: dict, stat: dict, dtype=torch.float32, device="cuda", diag=False, acc=True):
+        n = prog["tg"].shape[0]
+        c = cls(n, dtype=dtype, device=device, diag=diag, acc=acc)
+        c.set_prog(prog)
+        c.set_stat(stat)
+        return c
+
+    def set_prog(self, prog: dict):
+        a = synth.to_planes("PROG", prog, self.ld, self._np_dtype)
+        self.prog.copy_(torch.from_numpy(a))
+
+    def set_stat(self, stat: dict):
+        a = synth.to_planes("STAT", stat, self.ld, self._np_dtype)
+        self.stat.copy_(torch.from_numpy(a))
+
+    def forcing(self, forc: dict, h0: int = 0, h1: int | None = None) -> torch.Tensor:
+        """Device forcing tensor (nstep, IBIS_FORC_COUNT, ld) for hours [h0, h1)."""
+        a = synth.forcing_planes(forc, self.ld, h0, h1, self._np_dtype)
+        return torch.from_numpy(a).to(self.device)
+
+    def prog_host(self) -> dict:
+        return synth.from_planes("PROG", self.prog.cpu().numpy(), self.ncell)
+
+    def diag_host(self) -> dict:
+        if self.diag is None:
+            raise ValueError("diagnostics were not allocated")
+        return synth.from_planes("DIAG", self.diag.cpu().numpy(), self.ncell)
+
+    def acc_host(self, compensated: bool = True) -> dict:
+        """Accumulators; with ``compensated`` the Kahan terms are folded in."""
+        if self.acc is None:
+            raise ValueError("accumulators were not allocated")
+        a = self.acc.cpu().numpy().astype(np.float64)
+        v = a[:L.N_ACC]
+        if compensated:
+            v = v - a[L.N_ACC:]
+        return synth.from_planes("ACC", v, self.ncell)
+
+    def reset_acc(self):
+        if self.acc is not None:
+            self.acc.zero_()
+
+    def reset_status(self):
+        self.status.copy_(torch.tensor([0, INT_MAX], dtype=torch.int32))
+
+    def nonfinite(self):
+        """(flag, first cell) of the non-finite detector."""
+        s = self.status.cpu().numpy()
+        return bool(s[0] & 1), int(s[1])
+
+    # -------------------------------------------------------------- compute
+    def run(self, forc: torch.Tensor, params: StepParams, nstep: int | None = None, stream=None):
+        """Advance the columns ``nstep`` hours with forcing ``forc`` (asynchronous)."""
+        if forc.dtype != self.dtype or forc.device != self.device:
+            raise ValueError("forcing must have the Columns' dtype and device")
+        if forc.dim() != 3 or forc.shape[1] != L.N_FORC or forc.shape[2] != self.ld:
+            raise ValueError(f"forcing must be (nstep, {L.N_FORC}, {self.ld})")
+        if not forc.is_contiguous():
+            raise ValueError("forcing must be contiguous")
+        nstep = forc.shape[0] if nstep is None else int(nstep)
+        if nstep > forc.shape[0]:
+            raise ValueError("nstep exceeds the forcing provided")
+        flags = params.flags
+        if self.diag is None:
+            flags &= ~FLAG_DIAG
+        else:
+            flags |= FLAG_DIAG
+        if self.acc is None:
+            flags &= ~_ACC_FLAGS
+        p = params.to_c()
+        p.flags = flags
+        if stream is None:
+            stream = torch.cuda.current_stream(self.device)
+        rc = self._fn(_ptr(self.prog), _ptr(self.stat), _ptr(forc), _ptr(self.diag), _ptr(self.acc), self.ncell,
+                      self.ld, nstep, ctypes.byref(p), _ptr(self.status), ctypes.c_void_p(stream.cuda_stream))
+        _lib.check(rc, "ibis_step")
+        return self

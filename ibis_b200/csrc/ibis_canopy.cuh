@@ -1,0 +1,480 @@
+// Photosynthesis / stomatal conductance and the 9x9 canopy energy-vapour solve.
+// Reference: python-port/ibis/physics/stomata.py and canopy_exchange.py:470-811.
+#pragma once
+#include "ibis_column.cuh"
+
+namespace ibis {
+
+// ---------------------------------------------------------------------------
+// stomata (stomata.py:198-1080)
+// ---------------------------------------------------------------------------
+
+template <typename R>
+__device__ __forceinline__ R colimit(R j1, R j2, R theta) {
+    R b = j1 + j2;
+    R c = j1 * j2;
+    R disc = mx(b * b - R(4.0) * theta * c, R(0.0));
+    R q = R(0.5) * (b + sq(disc)) + R(1.0e-15);
+    return mn(q / theta, c / q);
+}
+
+template <typename R>
+__device__ __forceinline__ void c3_rate(R& ag, R& an, R par, R ci, R vmax, R gst, R kc, R ko, R rdark,
+                                        const DevParams<R>& P) {
+    R je = par * R(4.59e-06) * P.alpha3 * (ci - gst) / (ci + R(2.0) * gst);
+    R jc = vmax * (ci - gst) / (ci + kc * (R(1.0) + P.o2conc / ko));
+    R js = vmax / R(2.2);
+    ag = colimit(colimit(je, jc, P.theta3), js, P.beta3);
+    an = ag - rdark;
+}
+
+template <typename R>
+__device__ __forceinline__ void c4_rate(R& ag, R& an, R par, R ci, R vmax, R rdark, const DevParams<R>& P) {
+    R je = par * R(4.59e-06) * P.alpha4;
+    R ji = R(18.0e3) * vmax * ci;
+    ag = colimit(colimit(je, vmax, P.theta4), ji, P.beta4);
+    an = ag - rdark;
+}
+
+template <typename R>
+struct Kin { R kc, ko, gst, vm3, vm4; };
+
+template <typename R>
+__device__ __forceinline__ Kin<R> kinetics(R tleaf, const DevParams<R>& P) {
+    Kin<R> k;
+    R rw = R(3.47e-03) - R(1.0) / tleaf;
+    R tau = P.tau15 * ex(R(-4500.0) * rw);
+    k.kc = P.kc15 * ex(R(6000.0) * rw);
+    k.ko = P.ko15 * ex(R(1500.0) * rw);
+    k.gst = P.o2conc / (R(2.0) * tau);
+    R tc = tleaf - R(273.16);
+    R base = ex(R(3500.0) * rw);
+    R hot = R(1.0) + ex(R(0.40) * (tc - R(50.0)));
+    k.vm3 = base / ((R(1.0) + ex(R(0.40) * (R(5.0) - tc))) * hot);
+    k.vm4 = base / ((R(1.0) + ex(R(0.40) * (R(10.0) - tc))) * hot);
+    return k;
+}
+
+template <typename R>
+__device__ __forceinline__ void ball_berry(R& cs, R& gs, R& ci, R an, R gb, R rh, R m, R b0, R stress, R gmin,
+                                           R cmin, R imin, const DevParams<R>& P) {
+    R csn = mx(cmin, R(0.5) * (cs + P.co2conc - an / gb));
+    R gsn = R(0.5) * (gs + m * an * rh / csn + b0 * stress);
+    gsn = mx(gsn, mx(gmin, b0 * stress));
+    ci = clip(R(0.5) * (ci + csn - R(1.6) * an / gsn), imin, P.cimax);
+    cs = csn;
+    gs = gsn;
+}
+
+// canopy_scaling, F77 denominator k*LAI (stomata.py:442-512)
+template <typename R>
+__device__ __forceinline__ R light_scaling(R toppar, R k, R h, const R (&sc)[4], R lai, R sai, R& a10s, R& a10d,
+                                           const DevParams<R>& P) {
+    R ext = (k * sc[0] + h * sc[1] - h * sc[2]) / mx(sc[3], P.epsilon);
+    ext = clip(ext, R(0.1), R(10.0));
+    R pxai = ext * (lai + sai);
+    R plai = ext * lai;
+    bool has = plai > R(0.0);
+    bool day = toppar > R(10.0);
+    R sday = (R(1.0) - ex(-pxai)) / mx(plai, P.epsilon);
+    R snight = a10s / mx(a10d, P.epsilon);
+    if (has && day) {
+        a10s = P.zweight * a10s + (R(1.0) - P.zweight) * sday * toppar;
+        a10d = P.zweight * a10d + (R(1.0) - P.zweight) * toppar;
+    }
+    return has ? (day ? sday : snight) : R(0.0);
+}
+
+// integral of exp(-a x) over [0, plai] (stomata.py:436-441)
+template <typename R>
+__device__ __forceinline__ R e1(R a, R plai) {
+    R x = a * plai;
+    if (fabs((double)x) < 1.0e-5) return plai * (R(1.0) - R(0.5) * x);
+    return -em1(-x) / a;
+}
+
+template <typename R>
+struct SunShade { R psun, psha, vsun, vsha; };
+
+// sunshade_canopy (stomata.py:395-427)
+template <typename R>
+__device__ __forceinline__ SunShade<R> sunshade(const R (&sc)[4], R dbeam, R k, R h, R lai, R sai,
+                                                const DevParams<R>& P) {
+    R plai = mx(lai + sai, P.epsilon);
+    R fl = lai > R(0.0) ? lai / plai : R(0.0);
+    R ek = e1(k, plai), e2k = e1(R(2.0) * k, plai);
+    R tot = mx(sc[0] * ek + sc[1] * e1(h, plai) + sc[2] * e1(-h, plai), R(0.0));
+    R sun = sc[0] * e2k + sc[1] * e1(k + h, plai) + sc[2] * e1(k - h, plai) + dbeam * (ek - e2k);
+    sun = clip(sun, R(0.0), tot);
+    SunShade<R> s;
+    s.psun = sun * fl;
+    s.psha = (tot - sun) * fl;
+    s.vsun = fl * e1(P.cap_kn * fl + k, plai);
+    s.vsha = mx(fl * e1(P.cap_kn * fl, plai) - s.vsun, R(0.0));
+    return s;
+}
+
+template <typename R>
+__device__ __forceinline__ R total_conductance(R s, R g) {
+    return R(1.0) / (R(1.0) / s + R(1.0 / 0.029) / g);
+}
+
+template <typename R>
+struct Stom {
+    R an_u[2], ag_u[2], an_l[3], ag_l[3];
+    R tcub, tcuc, tcls, tcl3, tcl4;
+};
+
+// One pass of stomata over the five big leaves.  Updates the carried ci/gs/cs
+// and a10 running means in `c`.  SUN_U/SUN_L select the sunlit/shaded canopy.
+template <typename R, bool SUN_U, bool SUN_L>
+__device__ __forceinline__ void stomata(Stom<R>& o, Col<R>& c, R tu, R tl, R t12, R t34, R q12, R q34, R su,
+                                        R sl, R ps, const Rad<R>& Rd, R fwetu, R fwetl, const Stat<R>& S,
+                                        R stresstu, R stresstl, const DevParams<R>& P) {
+    const R eps = P.epsilon;
+    const R lai0 = S(IBIS_STAT_LAI, 0), lai1 = S(IBIS_STAT_LAI, 1);
+    const R sai0 = S(IBIS_STAT_SAI, 0), sai1 = S(IBIS_STAT_SAI, 1);
+    // ---------------- upper canopy: broadleaf (group 0) and conifer (group 1)
+    {
+        Kin<R> K = kinetics(tu, P);
+        R gmn = R(1.05) * K.gst;
+        R gb = clip(su * R(25.5), R(0.1), R(10.0));
+        R rh = mx(R(0.30), q12 / mx(qsat(esat(t12), ps), eps));
+        R vn[2];
+        vn[0] = S(IBIS_STAT_EXIST, 0) > R(0.5) ? P.vmax_pft[0]
+              : (S(IBIS_STAT_EXIST, 2) > R(0.5) ? P.vmax_pft[2] : P.vmax_pft[4]);
+        vn[1] = S(IBIS_STAT_EXIST, 3) > R(0.5) ? P.vmax_pft[3] : P.vmax_pft[5];
+        SunShade<R> ss;
+        if (SUN_U) ss = sunshade(Rd.scu, Rd.dbeamu, Rd.termu6, Rd.termu7, lai1, sai1, P);
+        R ag[2], an[2];
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            R ci = clip(c.ci_u[j], gmn, P.cimax);
+            R vmax = vn[j] * K.vm3 * stresstu;
+            R rd = P.gamma[j] * vn[j] * K.vm3;
+            c3_rate(ag[j], an[j], Rd.topparu, ci, vmax, K.gst, K.kc, K.ko, rd, P);
+            R bb = an[j];
+            if (SUN_U) {
+                R ags, ans, agh, anh;
+                c3_rate(ags, ans, ss.psun, ci, vmax * ss.vsun, K.gst, K.kc, K.ko, rd * ss.vsun, P);
+                c3_rate(agh, anh, ss.psha, ci, vmax * ss.vsha, K.gst, K.kc, K.ko, rd * ss.vsha, P);
+                R inv = lai1 > R(0.0) ? R(1.0) / mx(lai1, R(1.0e-6)) : R(0.0);
+                ag[j] = (ags + agh) * inv;
+                an[j] = (ans + anh) * inv;
+                bb = an[j];
+            }
+            c.ci_u[j] = ci;
+            ball_berry(c.cs_u[j], c.gs_u[j], c.ci_u[j], bb, gb, rh, P.coefm[j], P.coefb[j], stresstu, P.gsmin[j],
+                       gmn, gmn, P);
+        }
+        R scale = light_scaling(Rd.topparu, Rd.termu6, Rd.termu7, Rd.scu, lai1, sai1, c.a10su, c.a10du, P);
+        R tcs[2];
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            R agc = ag[j], anc = an[j];
+            if (!SUN_U) { agc = ag[j] * scale; anc = an[j] * scale; }
+            R csc = mx(gmn, P.co2conc - anc / gb);
+            R gsc = mx(mx(P.gsmin[j], P.coefb[j] * stresstu), P.coefm[j] * anc * rh / csc + P.coefb[j] * stresstu);
+            tcs[j] = total_conductance(su, gsc);
+            o.ag_u[j] = agc * (R(1.0) - fwetu);
+            o.an_u[j] = anc * (R(1.0) - fwetu);
+        }
+        o.tcub = tcs[0];
+        o.tcuc = tcs[1];
+    }
+    // ---------------- lower canopy: shrub (group 2, C3), C3 grass (group 4), C4 grass (group 3)
+    {
+        Kin<R> K = kinetics(tl, P);
+        R gmn = R(1.05) * K.gst;
+        R gb = clip(sl * R(25.5), R(0.1), R(10.0));
+        R rh = mx(R(0.30), q34 / mx(qsat(esat(t34), ps), eps));
+        SunShade<R> ss;
+        if (SUN_L) ss = sunshade(Rd.scl, Rd.dbeaml, Rd.terml6, Rd.terml7, lai0, sai0, P);
+        const int grp[3] = {2, 4, 3};
+        R ag[3], an[3];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const bool c4 = (j == 2);
+            const int g = grp[j];
+            R vn = j == 0 ? P.vmax_pft[8] : (j == 1 ? P.vmax_pft[11] : P.vmax_pft[10]);
+            R ci = clip(c.ci_l[j], c4 ? R(0.0) : gmn, P.cimax);
+            R vm = c4 ? K.vm4 : K.vm3;
+            R vmax = vn * vm * stresstl;
+            R rd = P.gamma[g] * vn * vm;
+            if (c4) c4_rate(ag[j], an[j], Rd.topparl, ci, vmax, rd, P);
+            else c3_rate(ag[j], an[j], Rd.topparl, ci, vmax, K.gst, K.kc, K.ko, rd, P);
+            R bb = an[j];
+            if (SUN_L) {
+                R ags, ans, agh, anh;
+                if (c4) {
+                    c4_rate(ags, ans, ss.psun, ci, vmax * ss.vsun, rd * ss.vsun, P);
+                    c4_rate(agh, anh, ss.psha, ci, vmax * ss.vsha, rd * ss.vsha, P);
+                } else {
+                    c3_rate(ags, ans, ss.psun, ci, vmax * ss.vsun, K.gst, K.kc, K.ko, rd * ss.vsun, P);
+                    c3_rate(agh, anh, ss.psha, ci, vmax * ss.vsha, K.gst, K.kc, K.ko, rd * ss.vsha, P);
+                }
+                R inv = lai0 > R(0.0) ? R(1.0) / mx(lai0, R(1.0e-6)) : R(0.0);
+                ag[j] = (ags + agh) * inv;
+                an[j] = (ans + anh) * inv;
+                bb = an[j];
+            }
+            c.ci_l[j] = ci;
+            ball_berry(c.cs_l[j], c.gs_l[j], c.ci_l[j], bb, gb, rh, P.coefm[g], P.coefb[g], stresstl, P.gsmin[g],
+                       c4 ? R(1.0e-8) : gmn, c4 ? R(0.0) : gmn, P);
+        }
+        R scale = light_scaling(Rd.topparl, Rd.terml6, Rd.terml7, Rd.scl, lai0, sai0, c.a10sl, c.a10dl, P);
+        R tcs[3];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const bool c4 = (j == 2);
+            const int g = grp[j];
+            R agc = ag[j], anc = an[j];
+            if (!SUN_L) { agc = ag[j] * scale; anc = an[j] * scale; }
+            R csc = mx(c4 ? R(1.0e-8) : gmn, P.co2conc - anc / gb);
+            R gsc = mx(mx(P.gsmin[g], P.coefb[g] * stresstl), P.coefm[g] * anc * rh / csc + P.coefb[g] * stresstl);
+            tcs[j] = total_conductance(sl, gsc);
+            o.ag_l[j] = agc * (R(1.0) - fwetl);
+            o.an_l[j] = anc * (R(1.0) - fwetl);
+        }
+        o.tcls = tcs[0];
+        o.tcl3 = tcs[1];
+        o.tcl4 = tcs[2];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// turvap: 9x9 implicit canopy / air / ground / snow system (canopy_exchange.py:470-811)
+// Always double.  Unknowns: tu ts tl t12 t34 q12 q34 tg ti.
+// ---------------------------------------------------------------------------
+
+// Structural nonzeros of the system after fill-in by no-pivot elimination in row
+// order.  Updates that would multiply a structural zero leave their target
+// unchanged in IEEE arithmetic, so skipping them reproduces the dense
+// elimination (canopy_exchange.py:26-61) exactly.
+__device__ constexpr bool kNZ[9][9] = {
+    {1, 0, 0, 1, 0, 1, 0, 0, 0}, {0, 1, 0, 1, 0, 1, 0, 0, 0}, {0, 0, 1, 0, 1, 0, 1, 0, 0},
+    {1, 1, 0, 1, 1, 1, 0, 0, 0}, {0, 0, 1, 1, 1, 1, 1, 1, 1}, {1, 1, 0, 1, 1, 1, 1, 1, 1},
+    {0, 0, 1, 0, 1, 1, 1, 1, 1}, {0, 0, 0, 0, 1, 1, 1, 1, 1}, {0, 0, 0, 0, 1, 1, 1, 1, 1}};
+
+__device__ __forceinline__ void gauss9(double (&A)[9][9], double (&b)[9], double (&x)[9]) {
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+#pragma unroll
+        for (int i = p + 1; i < 9; ++i) {
+            if (kNZ[i][p]) {
+                double f = A[i][p] / A[p][p];
+#pragma unroll
+                for (int j = p + 1; j < 9; ++j)
+                    if (kNZ[p][j]) A[i][j] = A[i][j] - f * A[p][j];
+                b[i] = b[i] - f * b[p];
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 8; i >= 0; --i) {
+        double s = 0.0;
+#pragma unroll
+        for (int j = i + 1; j < 9; ++j)
+            if (kNZ[i][j]) s = s + A[i][j] * x[j];
+        x[i] = (b[i] - s) / A[i][i];
+    }
+}
+
+// Inputs of turvap that do not change across the three passes.
+template <typename R>
+struct TvFixed {
+    double xu, xs, xl, fi, chux, chsx, chlx, cog, coi, zirg, ziri;
+    double wliqu, wliqs, wliql, wsnou, wsnos, wsnol;
+    double rliqu, rliqs, rliql, fwetu, fwets, fwetl;
+    double hvasug, hvasui, tsoi0, tsno0;
+    double zwtot, swilt0, suction0, bex0;
+    double fradu, frads, fradl, pfluxu, pfluxs, pfluxl;
+    double solg, soli, firg, firi, firb;
+    double lai1, lai0, lsl0, fu, fl;
+    double frac[12];
+};
+
+template <typename R>
+struct TvOut {
+    double fsenu, fsens, fsenl, fseng, fseni;
+    double fvapuw, fvaput, fvaps, fvaplw, fvaplt, fvapg, fvapi;
+    double firg, firi, firb, ginvap, gsuvap, gtrans;
+};
+
+struct Sat64 { double q, dq; };
+
+__device__ __forceinline__ Sat64 sat64(double t, double ps) {
+    double e = esat(t);
+    Sat64 s;
+    s.q = qsat(e, ps);
+    s.dq = fmin(dqsat(t, s.q, e), s.q * 0.1);
+    return s;
+}
+
+template <typename R>
+__device__ __forceinline__ void turvap(double (&W)[9], TvOut<R>& o, const double (&old)[5], const Trans<R>& T,
+                                       double cp, double tfac, double wu, double ws, double wl, double wg,
+                                       double wi, const TvFixed<R>& X, const Stom<R>& st, double ta, double qa,
+                                       double ps, const DevParams<R>& P) {
+    const double eps = (double)P.epsilon, dt = (double)P.dtime;
+    const double tmelt = (double)P.tmelt, hvap = (double)P.hvap, hsub = (double)P.hsub;
+    const double ch2o = (double)P.ch2o, cice = (double)P.cice, cvap = (double)P.cvap;
+    const double tu = wu * W[0] + (1.0 - wu) * old[0];
+    const double ts = ws * W[1] + (1.0 - ws) * old[1];
+    const double tl = wl * W[2] + (1.0 - wl) * old[2];
+    const double tg = wg * W[7] + (1.0 - wg) * old[3];
+    const double ti = wi * W[8] + (1.0 - wi) * old[4];
+    const double t34 = W[4], q12 = W[5], q34 = W[6];
+    const Sat64 Su = sat64(tu, ps), Ss = sat64(ts, ps), Sl = sat64(tl, ps), Sg = sat64(tg, ps), Si = sat64(ti, ps);
+    const double qu = Su.q, dqu = Su.dq, qs = Ss.q, dqs = Ss.dq, ql = Sl.q, dql = Sl.dq;
+    const double qg = Sg.q, dqg = Sg.dq, qi = Si.q, dqi = Si.dq;
+
+    // soil-surface humidity factor (canopy_exchange.py:532-572)
+    const double psig = -(double)P.grav * X.suction0 * pow(X.zwtot, -X.bex0);
+    const double hfac = exp(psig / ((double)P.rvap * tg));
+    const double hfac2 = q34 / fmax(qg, eps);
+    double betaw = clip((X.zwtot - X.swilt0) / fmax(1.0 - X.swilt0, eps), 0.0, 1.0);
+    if ((double)P.soil_beta_power != 1.0) betaw = pow(betaw, (double)P.soil_beta_power);
+    const double e34 = esat(t34);
+    const double qs1 = qsat(e34, ps);
+    const double dqs1 = dqsat(t34, qs1, e34);
+    const double xden = cp + ((double)P.zir * cube(t34)) / (double)T.sg;
+    const double bfac = hvap * dqs1 / xden;
+    const double betas = betaw / (1.0 + bfac * (1.0 - betaw));
+    double qgfac = (betas > 0.0) ? betas * hfac + (1.0 - betas) * hfac2 : hfac2;
+    const double qeps = 1.0e-10;
+    if (q34 > qg + qeps) qgfac = 1.0;
+    const double fwux = (q12 > qu + qeps) ? 1.0 : X.fwetu;
+    const double fwsx = (q12 > qs + qeps) ? 1.0 : X.fwets;
+    const double fwlx = (q34 > ql + qeps) ? 1.0 : X.fwetl;
+
+    // vapour conductances (canopy_exchange.py:587-618)
+    const double su = T.su, ss = T.ss, sl = T.sl, sg = T.sg, si = T.si, cu = T.cu, cl = T.cl;
+    const double tb = st.tcub, tc = st.tcuc;
+    const double* fr = X.frac;
+    const double suw = fmin(fwux * su, 0.8 * (X.wliqu + X.wsnou) / fmax(dt * (qu - q12), eps));
+    const double sut = fmax(0.0, (1.0 - fwux) * 0.5 * (tb * fr[0] + tb * fr[1] + tb * fr[2] + tc * fr[3]
+                                                      + tb * fr[4] + tc * fr[5] + tb * fr[6] + tb * fr[7]));
+    const double hvu = hvap + cvap * (ta - tmelt) - ch2o * (tu - tmelt);
+    const double hsu = hsub + cvap * (ta - tmelt) - cice * (tu - tmelt);
+    const double suh = suw * (X.rliqu * hvu + (1.0 - X.rliqu) * hsu) + sut * hvu;
+    const double ssw = fmin(fwsx * ss, 0.8 * (X.wliqs + X.wsnos) / fmax(dt * (qs - q12), eps));
+    const double ssh = ssw * (X.rliqs * (hvap + cvap * (ta - tmelt) - ch2o * (ts - tmelt))
+                              + (1.0 - X.rliqs) * (hsub + cvap * (ta - tmelt) - cice * (ts - tmelt)));
+    const double slw = fmin(fwlx * sl, 0.8 * (X.wliql + X.wsnol) / fmax(dt * (ql - q34), eps));
+    const double tls = st.tcls, tl3 = st.tcl3, tl4 = st.tcl4;
+    const double slt0 = fmax(0.0, (1.0 - fwlx) * 0.5 * (tls * fr[8] + tls * fr[9] + tl4 * fr[10] + tl3 * fr[11]));
+    const double slt = slt0 * X.lai0 / fmax(X.lsl0, eps);
+    const double hvl = hvap + cvap * (ta - tmelt) - ch2o * (tl - tmelt);
+    const double slh = slw * (X.rliql * hvl + (1.0 - X.rliql) * (hsub + cvap * (ta - tmelt) - cice * (tl - tmelt)))
+                     + slt * hvl;
+
+    // matrix and right-hand side (canopy_exchange.py:620-682)
+    double A[9][9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i)
+#pragma unroll
+        for (int j = 0; j < 9; ++j) A[i][j] = 0.0;
+    double b[9];
+    const double rdt = 1.0 / dt;
+    const double fi = X.fi;
+    double r2 = su * cp;
+    A[0][0] = X.chux * rdt + wu * r2 + wu * suh * dqu;
+    A[0][3] = -r2;
+    A[0][5] = -suh;
+    b[0] = old[0] * X.chux * rdt - (1.0 - wu) * r2 * tu - suh * (qu - wu * dqu * tu) + X.fradu - X.pfluxu;
+    r2 = ss * cp;
+    A[1][1] = X.chsx * rdt + ws * r2 + ws * ssh * dqs;
+    A[1][3] = -r2;
+    A[1][5] = -ssh;
+    b[1] = old[1] * X.chsx * rdt - (1.0 - ws) * r2 * ts - ssh * (qs - ws * dqs * ts) + X.frads - X.pfluxs;
+    r2 = sl * cp;
+    A[2][2] = X.chlx * rdt + wl * r2 + wl * slh * dql;
+    A[2][4] = -r2;
+    A[2][6] = -slh;
+    b[2] = old[2] * X.chlx * rdt - (1.0 - wl) * r2 * tl - slh * (ql - wl * dql * tl) + X.fradl - X.pfluxl;
+    const double ru = X.xu * su, rs = X.xs * ss;
+    A[3][0] = -wu * ru;
+    A[3][1] = -ws * rs;
+    A[3][3] = cu + cl + ru + rs;
+    A[3][4] = -cl;
+    b[3] = cu * ta * tfac + (1.0 - wu) * ru * tu + (1.0 - ws) * rs * ts;
+    const double rl = X.xl * sl, ri = fi * si;
+    A[4][2] = -wl * rl;
+    A[4][3] = -cl;
+    A[4][4] = cl + rl + (1.0 - fi) * sg + ri;
+    A[4][7] = -wg * (1.0 - fi) * sg;
+    A[4][8] = -wi * ri;
+    b[4] = (1.0 - wl) * rl * tl + (1.0 - wg) * (1.0 - fi) * sg * tg + (1.0 - wi) * ri * ti;
+    const double ruq = X.xu * (suw + sut), rsq = X.xs * ssw;
+    A[5][0] = -wu * ruq * dqu;
+    A[5][1] = -ws * rsq * dqs;
+    A[5][5] = cu + cl + ruq + rsq;
+    A[5][6] = -cl;
+    b[5] = cu * qa + ruq * (qu - wu * dqu * tu) + rsq * (qs - ws * dqs * ts);
+    const double rlq = X.xl * (slw + slt), rgq = (1.0 - fi) * sg;
+    A[6][2] = -wl * rlq * dql;
+    A[6][5] = -cl;
+    A[6][6] = cl + rlq + rgq + fi * si;
+    A[6][7] = -wg * rgq * qgfac * dqg;
+    A[6][8] = -wi * fi * si * dqi;
+    b[6] = rlq * (ql - wl * dql * tl) + rgq * qgfac * (qg - wg * dqg * tg) + fi * si * (qi - wi * dqi * ti);
+    double r1 = sg * cp;
+    r2 = sg * X.hvasug;
+    A[7][4] = -r1;
+    A[7][6] = -r2;
+    A[7][7] = r1 + r2 * qgfac * dqg + X.cog + X.zirg;
+    b[7] = -r2 * qgfac * (qg - dqg * tg) + X.cog * X.tsoi0 + X.solg + X.firg + X.zirg * old[3];
+    r1 = si * cp;
+    r2 = si * X.hvasui;
+    A[8][4] = -r1;
+    A[8][6] = -r2;
+    A[8][8] = r1 + r2 * dqi + X.coi + X.ziri;
+    b[8] = -r2 * (qi - dqi * ti) + X.coi * X.tsno0 + X.soli + X.firi + X.ziri * old[4];
+
+    // bare cells: canopy rows pinned to the air (canopy_exchange.py:684-732)
+    if ((X.xu + X.xs + X.xl) < eps) {
+#pragma unroll
+        for (int i = 0; i < 7; ++i) {
+#pragma unroll
+            for (int j = 0; j < 9; ++j) A[i][j] = (i == j) ? 1.0 : 0.0;
+        }
+        const double ttf = ta * tfac;
+#pragma unroll
+        for (int i = 0; i < 5; ++i) b[i] = ttf;
+        b[5] = qa;
+        b[6] = qa;
+        b[7] = b[7] + ((X.fradu - X.pfluxu) * X.xu + (X.frads - X.pfluxs) * X.xs + (X.fradl - X.pfluxl) * X.xl);
+    }
+
+    double v[9];
+    gauss9(A, b, v);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) W[i] = v[i];
+    const double nu = v[0], ns = v[1], nl = v[2], n12 = v[3], n34 = v[4], nq12 = v[5], nq34 = v[6];
+    const double ng = v[7], ni = v[8];
+
+    // flux diagnostics (canopy_exchange.py:746-795)
+    o.fsenu = cp * su * (wu * nu + (1.0 - wu) * tu - n12);
+    o.fsens = cp * ss * (ws * ns + (1.0 - ws) * ts - n12);
+    o.fsenl = cp * sl * (wl * nl + (1.0 - wl) * tl - n12);
+    o.fseng = cp * sg * (wg * ng + (1.0 - wg) * tg - n34);
+    o.fseni = cp * si * (wi * ni + (1.0 - wi) * ti - n34);
+    const double quav = qu + wu * dqu * (nu - tu);
+    o.fvapuw = suw * (quav - nq12);
+    o.fvaput = fmax(0.0, sut * (quav - nq12));
+    o.fvaps = ssw * (qs + ws * dqs * (ns - ts) - nq12);
+    const double qlav = ql + wl * dql * (nl - tl);
+    o.fvaplw = slw * (qlav - nq34);
+    o.fvaplt = fmax(0.0, slt0 * (qlav - nq34));
+    o.fvapg = sg * (qgfac * (qg + wg * dqg * (ng - tg)) - nq34);
+    o.fvapi = si * (qi + wi * dqi * (ni - ti) - nq34);
+    o.firg = X.firg - wg * X.zirg * (ng - old[3]);
+    o.firi = X.firi - wi * X.ziri * (ni - old[4]);
+    o.firb = X.firb + (1.0 - fi) * wg * X.zirg * (ng - old[3]) + fi * wi * X.ziri * (ni - old[4]);
+    o.ginvap = o.fvapuw * X.xu + o.fvaps * X.xs + o.fvaplw * X.xl;
+    o.gsuvap = o.fvapg * (1.0 - fi) + o.fvapi * fi;
+    o.gtrans = o.fvaput * 2.0 * X.lai1 * X.fu + o.fvaplt * 2.0 * X.lai0 * X.fl * (1.0 - fi);
+}
+
+}  // namespace ibis

@@ -1,0 +1,395 @@
+// Snow, soil (+ thermal-only bedrock) column solves, fire counters and wetland CH4.
+// Reference: python-port/ibis/physics/snow_physics.py, soil_physics.py,
+// bedrock.py, fire.py (per-step part) and bgc/methane.py.
+#pragma once
+#include "ibis_column.cuh"
+
+namespace ibis {
+
+// Thomas algorithm (solvers.py:17-83) on N unknowns held in registers.
+template <typename T, int N>
+__device__ __forceinline__ void thomas(const T (&lo)[N], const T (&di)[N], const T (&up)[N], const T (&r)[N],
+                                       T (&x)[N]) {
+    T gam[N];
+    T alp = T(1.0) / di[0];
+    gam[0] = up[0] * alp;
+    x[0] = r[0] * alp;
+#pragma unroll
+    for (int k = 1; k < N - 1; ++k) {
+        alp = T(1.0) / (di[k] - lo[k] * gam[k - 1]);
+        gam[k] = up[k] * alp;
+        x[k] = (r[k] - lo[k] * x[k - 1]) * alp;
+    }
+    x[N - 1] = (r[N - 1] - lo[N - 1] * x[N - 2]) / (di[N - 1] - lo[N - 1] * gam[N - 2]);
+#pragma unroll
+    for (int k = N - 2; k >= 0; --k) x[k] = x[k] - gam[k] * x[k + 1];
+}
+
+// ---------------------------------------------------------------------------
+// snowheat (snow_physics.py:109-229): snow layers + one buried-vegetation node
+// ---------------------------------------------------------------------------
+template <typename R>
+__device__ __forceinline__ void snow_heat(R (&tsno)[NS], R& tlsub, R& sflo_bot, R fhtop, R xl, R fi,
+                                          const R (&hsno)[NS], R hsoi0, R consoi0, R tsoi0, const DevParams<R>& P) {
+    const R conbur = R(2.0), hfake = R(0.01);
+    R con[NS + 2];
+    const R rs = R(0.5) / P.consno;
+    con[0] = R(0.0);
+#pragma unroll
+    for (int k = 1; k < NS; ++k) con[k] = R(1.0) / (mx(hsno[k - 1], hfake) * rs + mx(hsno[k], hfake) * rs);
+    con[NS] = R(1.0) / (mx(hsno[NS - 1], hfake) * rs + R(0.5) * xl / conbur);
+    con[NS + 1] = R(1.0) / (xl * (R(0.5) / conbur) + R(0.5) * hsoi0 / mx(consoi0, R(1e-12)));
+    R lo[NS + 1], di[NS + 1], up[NS + 1], r[NS + 1], tn[NS + 1];
+    const R rdt = P.dtime / (P.rhos * P.cice);
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+        R dt = rdt / mx(hsno[k], hfake);
+        lo[k] = -dt * con[k];
+        di[k] = R(1.0) + dt * (con[k] + con[k + 1]);
+        up[k] = -dt * con[k + 1];
+        r[k] = tsno[k];
+        if (k == 0) r[k] = r[k] + dt * fhtop;
+    }
+    R dti = xl * P.chl / P.dtime;
+    lo[NS] = -con[NS];
+    di[NS] = dti + (con[NS] + con[NS + 1]);
+    up[NS] = R(0.0);
+    r[NS] = dti * tlsub + con[NS + 1] * tsoi0;
+    thomas(lo, di, up, r, tn);
+    R s = fhtop;
+    const R rh = P.rhos * P.cice / P.dtime;
+#pragma unroll
+    for (int k = 0; k < NS; ++k) s = s - rh * hsno[k] * (tn[k] - tsno[k]);
+    sflo_bot = s - xl * (P.chl / P.dtime) * (tn[NS] - tlsub);
+    if (fi > R(0.0)) {
+#pragma unroll
+        for (int k = 0; k < NS; ++k) tsno[k] = tn[k];
+        tlsub = tn[NS];
+    }
+}
+
+// vadapt (snow_physics.py:27-106)
+template <typename R>
+__device__ __forceinline__ void readapt_layers(R (&h)[NS], R (&t)[NS], R htop, R eps) {
+    R zold[NS + 1];
+    zold[0] = R(0.0);
+#pragma unroll
+    for (int k = 0; k < NS; ++k) zold[k + 1] = zold[k] + h[k];
+    R ht = zold[NS];
+    if (!(ht > eps)) return;
+    bool thick = ht >= R(NS) * htop;
+    R h1 = thick ? (ht - htop) / R(NS - 1) : mx(ht / R(NS), eps);
+    R hn[NS];
+#pragma unroll
+    for (int k = 0; k < NS; ++k) hn[k] = h1;
+    hn[0] = thick ? htop : h1;
+    R znew[NS + 1];
+    znew[0] = R(0.0);
+#pragma unroll
+    for (int k = 0; k < NS; ++k) znew[k + 1] = znew[k] + hn[k];
+    R tn[NS];
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+        R acc = R(0.0);
+#pragma unroll
+        for (int ko = 0; ko < NS; ++ko) {
+            R ov = mx(mn(zold[ko + 1], znew[k + 1]) - mx(zold[ko], znew[k]), R(0.0));
+            acc = acc + t[ko] * ov;
+        }
+        tn[k] = acc / mx(hn[k], eps);
+    }
+#pragma unroll
+    for (int k = 0; k < NS; ++k) { h[k] = hn[k]; t[k] = tn[k]; }
+}
+
+// ---------------------------------------------------------------------------
+// soilh2o (soil_physics.py:196-373), always double
+// ---------------------------------------------------------------------------
+template <typename R>
+__device__ __forceinline__ void soil_water(double (&w)[NL], double& wpud, double (&wflo)[NL + 1],
+                                           const double (&wisoi)[NL], const double (&poros)[NL],
+                                           const double (&pflo)[NL], const Stat<R>& S, double fwtop, double fwpud,
+                                           const DevParams<R>& P) {
+    const double dmin = 1e-9;
+    const double dtime = (double)P.dtime, rhow = (double)P.rhow, eps = (double)P.epsilon;
+    const bool consistent = (P.flags & IBIS_FLAG_H2O_CONSISTENT) != 0;
+    double e[NL + 1], f[NL + 1], g[NL + 1];
+    e[0] = f[0] = g[0] = 0.0;
+    f[NL] = g[NL] = 0.0;
+    double hyd_prev = (double)S(IBIS_STAT_HYDRAUL, 0);
+    double suc_prev = (double)S(IBIS_STAT_SUCTION, 0);
+    double bex_prev = (double)S(IBIS_STAT_BEX, 0);
+#pragma unroll
+    for (int k = 1; k < NL; ++k) {
+        const double hyd = (double)S(IBIS_STAT_HYDRAUL, k);
+        const double suc = (double)S(IBIS_STAT_SUCTION, k);
+        const double bex = (double)S(IBIS_STAT_BEX, k);
+        const double hm = P.sw_hm[k], wp = P.sw_wp[k], wm = P.sw_wm[k];
+        double a = wm * hyd_prev + wp * hyd;
+        double b = wm * hyd_prev * suc_prev * bex_prev + wp * hyd * suc * bex;
+        double zb = wm * bex_prev + wp * bex;
+        int nb = (int)floor(zb + 0.5);
+        int m = 2 * nb + 3;
+        int nn = nb + 2;
+        double ws = consistent ? wp * w[k - 1] + wm * w[k] : wm * w[k - 1] + wp * w[k];
+        double wa = fmin(ws, 1.0);
+        double bwn1 = b * ipow(wa, nn - 1);
+        double bwn = bwn1 * wa;
+        if (bwn < dmin) bwn1 = 0.0;
+        bwn = fmax(bwn, dmin);
+        double dw = (w[k] - w[k - 1]) / hm;
+        double wam1 = ipow(wa, m - 1);
+        double ek = (-1.0 + (double)m) * a * (wam1 * wa) + ((0.0 * bwn) - (double)nn * bwn1 * wa) * dw;
+        double fk = (double)(-m) * a * wam1 + (double)nn * bwn1 * dw;
+        double zi = fmax(0.0, 1.0 - fmax(wisoi[k - 1], wisoi[k]));
+        zi = zi * zi;
+        e[k] = zi * ek;
+        f[k] = zi * fk;
+        g[k] = zi * bwn;
+        hyd_prev = hyd; suc_prev = suc; bex_prev = bex;
+    }
+    {
+        double wab = fmin(w[NL - 1], 1.0);
+        int mb = 2 * (int)floor(bex_prev + 0.5) + 3;
+        double zi = fmax(0.0, 1.0 - wisoi[NL - 1]);
+        e[NL] = (zi * zi) * (-hyd_prev * ipow(wab, mb) * (double)P.bperm);
+    }
+    double lo[NL], di[NL], up[NL], r[NL], wn[NL];
+#pragma unroll
+    for (int k = 0; k < NL; ++k) {
+        const double h = (double)P.hsoi[k];
+        const double dt = dtime / fmax(pflo[k] * h, 1e-30);
+        const double hm = P.sw_hb[k];
+        const int km1 = k > 0 ? k - 1 : 0;
+        double d1 = dt * (f[k] * 0.5 * h / hm - g[k] / hm);
+        double rk = w[k] + dt * (e[k + 1] - e[k]);
+        if (k == 0) {
+            rk = rk + dt * (fwtop + fwpud) / rhow;
+            d1 = 0.0;
+        }
+        double d2, d3;
+        if (k < NL - 1) {
+            const double hp = P.sw_hp[k];
+            d2 = 1.0 + dt * (-f[k + 1] * 0.5 * (double)P.hsoi[k + 1] / hp + f[k] * 0.5 * (double)P.hsoi[km1] / hm
+                             + g[k + 1] / hp + g[k] / hm);
+            d3 = dt * (-f[k + 1] * 0.5 * h / hp - g[k + 1] / hp);
+        } else {
+            d2 = 1.0 + dt * (-f[k + 1] + f[k] * 0.5 * (double)P.hsoi[km1] / hm + g[k] / hm);
+            d3 = 0.0;
+        }
+        lo[k] = d1; di[k] = d2; up[k] = d3; r[k] = rk;
+    }
+    thomas(lo, di, up, r, wn);
+    wflo[NL] = -rhow * e[NL];
+    double fsq = 0.0;
+#pragma unroll
+    for (int k = NL - 1; k >= 0; --k) {
+        double zz = rhow * poros[k] * fmax(eps, 1.0 - wisoi[k]) * (double)P.hsoi[k];
+        double wk = wn[k] + dtime * fsq / zz;
+        double fsn = fmax(wk - 1.0, 0.0) * zz / dtime;
+        wk = fmin(wk, 1.0);
+        wflo[k] = wflo[k + 1] + (wk - w[k]) * zz / dtime;
+        wn[k] = wk;
+        fsq = fsn;
+    }
+    wpud = fmax(wpud + (fsq - fwpud) * dtime, 0.0);
+    wflo[0] = wflo[0] + fsq - fwpud;
+#pragma unroll
+    for (int k = 0; k < NL; ++k) w[k] = wn[k];
+}
+
+// ---------------------------------------------------------------------------
+// soilheat / soilheat_with_bedrock (soil_physics.py:385-490, bedrock.py:88-153)
+// NT = 6 (no bedrock) or 9; the first NL layers carry water.
+// ---------------------------------------------------------------------------
+template <typename R, int NT>
+__device__ __forceinline__ void soil_heat(R (&t)[NT], R (&hflo)[NL + 1], const R (&owsoi)[NL], const R (&wsoi)[NL],
+                                          const R (&wisoi)[NL], const R (&poros)[NL], const R (&consoi)[NL],
+                                          const R (&csoi)[NL], const R (&rhosoi)[NL], R c0pud0, R c1pud0, R fhtop,
+                                          const R (&wflo)[NL + 1], const DevParams<R>& P) {
+    R h[NT], con[NT + 1], whf[NT + 1], c0[NT], c1[NT];
+#pragma unroll
+    for (int k = 0; k < NT; ++k) h[k] = k < NL ? P.hsoi[k] : P.hsoi_bed[k - NL];
+    auto cons = [&](int k) -> R { return k < NL ? consoi[k] : P.consoi_bed; };
+    con[0] = R(0.0);
+    con[NT] = R(0.0);
+    whf[0] = wflo[0] * P.ch2o * t[0];
+#pragma unroll
+    for (int k = 1; k < NT; ++k) {
+        con[k] = R(1.0) / (R(0.5) * (h[k - 1] / mx(cons(k - 1), R(1e-12)) + h[k] / mx(cons(k), R(1e-12))));
+        if (k < NL) {
+            R tav = (h[k] * t[k - 1] + h[k - 1] * t[k]) / (h[k - 1] + h[k]);
+            whf[k] = wflo[k] * P.ch2o * tav;
+        }
+    }
+    R drain = wflo[NL] * P.ch2o * t[NL - 1];
+#pragma unroll
+    for (int k = NL; k <= NT; ++k) whf[k] = drain;
+#pragma unroll
+    for (int k = 0; k < NT; ++k) {
+        if (k < NL) {
+            R r1 = (R(1.0) - poros[k]) * csoi[k] * rhosoi[k];
+            R r2 = poros[k] * (R(1.0) - wisoi[k]) * P.ch2o * P.rhow;
+            R r3 = poros[k] * wisoi[k] * P.cice * P.rhow;
+            R pud0 = k == 0 ? c0pud0 : R(0.0);
+            R pud1 = k == 0 ? c1pud0 : R(0.0);
+            c0[k] = pud0 + (r1 + r2 * owsoi[k] + r3) * h[k];
+            c1[k] = pud1 + (r1 + r2 * wsoi[k] + r3) * h[k];
+        } else {
+            // bedrock: zero porosity and water, so (1-0) csoi rho plus 0 * 0 terms (bedrock.py:132-150)
+            R r1 = (R(1.0) - R(0.0)) * P.csoi_bed * P.rhosoi_bed;
+            R v = R(0.0) + (r1 + R(0.0) * R(0.0) + R(0.0)) * h[k];
+            c0[k] = v;
+            c1[k] = v;
+        }
+    }
+    R lo[NT], di[NT], up[NT], r[NT], tn[NT];
+#pragma unroll
+    for (int k = 0; k < NT; ++k) {
+        R rw = P.dtime / c1[k];
+        lo[k] = -rw * con[k];
+        di[k] = R(1.0) + rw * (con[k] + con[k + 1]);
+        up[k] = -rw * con[k + 1];
+        r[k] = (c0[k] / c1[k]) * t[k] + rw * (whf[k] - whf[k + 1]);
+        if (k == 0) r[k] = r[k] + (P.dtime / c1[k]) * fhtop;
+    }
+    thomas(lo, di, up, r, tn);
+    R s = fhtop;
+    hflo[0] = s;
+#pragma unroll
+    for (int k = 0; k < NT; ++k) {
+        s = s - (c1[k] * tn[k] - c0[k] * t[k]) / P.dtime;
+        if (k < NL) hflo[k + 1] = s;
+    }
+#pragma unroll
+    for (int k = 0; k < NT; ++k) t[k] = tn[k];
+}
+
+// wadjust (soil_physics.py:147-189); returns the mass adjustment rate
+template <typename R>
+__device__ __forceinline__ R water_bounds(R (&w)[NL], R (&i)[NL], const R (&poros)[NL], const DevParams<R>& P) {
+    const R eps = P.epsilon;
+    R tot = R(0.0);
+#pragma unroll
+    for (int k = 0; k < NL; ++k) {
+        R z0 = P.hsoi[k] * poros[k] * P.rhow * ((R(1.0) - i[k]) * w[k] + i[k]);
+        R ww = w[k] < eps ? R(0.0) : w[k];
+        R ii = i[k] < eps ? R(0.0) : i[k];
+        ww = mn(R(1.0), ww);
+        ii = mn(R(1.0), ii);
+        if (ii >= R(1.0) - eps) ww = R(0.0);
+        R z1 = P.hsoi[k] * poros[k] * P.rhow * ((R(1.0) - ii) * ww + ii);
+        tot = tot + (z1 - z0);
+        w[k] = ww;
+        i[k] = ii;
+    }
+    return tot / P.dtime;
+}
+
+// freeze_thaw (soil_physics.py:497-564)
+template <typename R>
+__device__ __forceinline__ void phase_change(R (&t)[NL], R (&w)[NL], R (&i)[NL], R (&pflo)[NL], const R (&poros)[NL],
+                                             const R (&csoi)[NL], const R (&rhosoi)[NL], R c1pud0,
+                                             const DevParams<R>& P) {
+    const R eps = P.epsilon;
+#pragma unroll
+    for (int k = 0; k < NL; ++k) {
+        R zp = mx(poros[k], eps);
+        R c1 = k == 0 ? c1pud0 : R(0.0);
+        R rw = c1 / (P.rhow * P.hsoi[k]) + (R(1.0) - zp) * csoi[k] * rhosoi[k] / P.rhow;
+        R chav = rw + zp * (R(1.0) - i[k]) * w[k] * P.ch2o + zp * i[k] * P.cice;
+        R zw = mn(R(1.0), w[k]);
+        R dh = chav * (P.tmelt - t[k]);
+        R dw = mn(zp * (R(1.0) - i[k]) * zw, mx(R(0.0), dh / P.hfus));
+        R ik = i[k] + dw / zp;
+        R wk = w[k] - (dw / zp) * (R(1.0) - zw) / mx(eps, R(1.0) - ik);
+        chav = rw + zp * (R(1.0) - ik) * wk * P.ch2o + zp * ik * P.cice;
+        R tk = P.tmelt - (dh - P.hfus * dw) / chav;
+        dh = chav * (tk - P.tmelt);
+        dw = mn(zp * ik, mx(R(0.0), dh / P.hfus));
+        ik = ik - dw / zp;
+        wk = wk + (dw / zp) * (R(1.0) - wk) / mx(eps, R(1.0) - ik);
+        chav = rw + zp * (R(1.0) - ik) * wk * P.ch2o + zp * ik * P.cice;
+        t[k] = P.tmelt + (dh - P.hfus * dw) / chav;
+        w[k] = wk;
+        i[k] = ik;
+        pflo[k] = poros[k] * mx(eps, R(1.0) - ik);
+    }
+}
+
+// puddle_freeze_thaw (soil_physics.py:567-615)
+template <typename R>
+__device__ __forceinline__ void puddle_phase(R& t0, R& wpud, R& wipud, R poros0, R w0, R i0, R csoi0, R rho0,
+                                             const DevParams<R>& P) {
+    R rw = ((R(1.0) - poros0) * csoi0 * rho0 + poros0 * (R(1.0) - i0) * w0 * P.ch2o * P.rhow
+            + poros0 * i0 * P.cice * P.rhow) * P.hsoi[0];
+    R chav = P.ch2o * wpud + P.cice * wipud + rw;
+    R dh = chav * (P.tmelt - t0);
+    R dw = mn(wpud, mx(R(0.0), dh / P.hfus));
+    wipud = wipud + dw;
+    wpud = wpud - dw;
+    chav = P.ch2o * wpud + P.cice * wipud + rw;
+    t0 = P.tmelt - (dh - P.hfus * dw) / chav;
+    dh = chav * (t0 - P.tmelt);
+    dw = mn(wipud, mx(R(0.0), dh / P.hfus));
+    wipud = wipud - dw;
+    wpud = wpud + dw;
+    chav = P.ch2o * wpud + P.cice * wipud + rw;
+    t0 = P.tmelt + (dh - P.hfus * dw) / chav;
+    wpud = mx(wpud, R(0.0));
+    wipud = mx(wipud, R(0.0));
+}
+
+// fire counters (fire.py:88-140, 340-366, 470-514, 583-604)
+template <typename R>
+__device__ __forceinline__ void fire_counters(Col<R>& c, R swilt0, const Forc<R>& F, const DevParams<R>& P) {
+    R nyt = c.nytimes + R(1.0);
+    R water = c.wisoi[0] + (R(1.0) - c.wisoi[0]) * c.wsoi[0];
+    R frac = (water - swilt0) / (R(1.0) - swilt0);
+    R fd = mn(R(1.0), mx(R(0.0), R(-2.0) * (frac - R(0.5))));
+    R nn = mx(nyt, R(1.0));
+    c.firefac = ((nn - R(1.0)) * c.firefac + fd) / nn;
+    c.nytimes = nyt;
+    R hit = fd > P.d_crit ? R(1.0) : R(0.0);
+    c.nfirestep = c.nfirestep + hit;
+    c.sdry = c.sdry + fd * hit;
+    R eact = F.qa * F.ps / (R(0.622) + R(0.378) * F.qa);
+    R vpd = mx(esat(F.ta) - eact, R(0.0)) / R(1000.0);
+    R fl = clip(vpd / P.vpd_ref, R(0.0), R(1.0));
+    hit = fl > P.d_crit_vpd ? R(1.0) : R(0.0);
+    c.nfirestep_vpd = c.nfirestep_vpd + hit;
+    c.sdry_vpd = c.sdry_vpd + fl * hit;
+}
+
+// methane_flux (methane.py:233-383), kgC m-2 d-1
+template <typename R>
+__device__ __forceinline__ R methane(R f_inund, R rh, const R (&t)[NL], const R (&w)[NL], const R (&i)[NL],
+                                     const DevParams<R>& P) {
+    R acc = R(0.0);
+#pragma unroll
+    for (int k = 0; k < NL; ++k) {
+        R th = clip(w[k] * (R(1.0) - i[k]) + i[k], R(0.0), R(1.0));
+        acc = acc + th * P.ch4_wtop[k];
+    }
+    R ttop = acc / P.ch4_wtot;
+    R wet = clip(ttop / mx(P.sat_crit, R(1e-6)), R(0.0), R(1.0));
+    R zwt = P.z_wt_max * (R(1.0) - wet);
+    R tt = R(0.0), tw = R(0.0);
+#pragma unroll
+    for (int k = 0; k < NL; ++k) {
+        R below = P.hsoi_bot[k] - mx(zwt, P.hsoi_top[k]);
+        R an = clip(below / P.hsoi[k], R(0.0), R(1.0)) * P.hsoi[k];
+        R th = t[k] >= R(273.15) ? an : R(0.0);
+        tt = tt + th;
+        tw = tw + th * t[k];
+    }
+    R tth = tt > R(1e-12) ? tw / mx(tt, R(1e-12)) : t[0];
+    R zp = mx(zwt, R(0.0));
+    R rha = mx(rh, R(0.0)) * ex(-zp / mx(P.z_tau, R(1e-6)));
+    R q10 = pw(P.q10p, (tth - P.t_ref) / R(10.0));
+    R prod = mx(rha, R(0.0)) * P.r_ch4 * q10 * (tth >= R(273.15) ? R(1.0) : R(0.0));
+    R area = clip(mx(f_inund, R(0.0)), R(0.0), R(1.0));
+    return area * prod * ex(-zp / mx(P.tau_oxid, R(1e-6)));
+}
+
+}  // namespace ibis

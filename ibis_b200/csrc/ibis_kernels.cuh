@@ -1,0 +1,227 @@
+// Kernels and host-side launch helpers of the hourly step (included by one
+// translation unit per precision: ibis_step_f32.cu and ibis_step_f64.cu).
+#pragma once
+#include <errno.h>
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include "ibis_step.cuh"
+
+namespace ibis {
+
+constexpr int kBlock = 128;
+
+template <typename R>
+__device__ __forceinline__ void load_col(Col<R>& c, const R* __restrict__ p, int ld) {
+    auto g = [&](int plane) { return p[(size_t)plane * ld]; };
+#pragma unroll
+    for (int k = 0; k < NL; ++k) {
+        c.tsoi[k] = g(IBIS_PROG_TSOI + k);
+        c.wsoi[k] = g(IBIS_PROG_WSOI + k);
+        c.wisoi[k] = g(IBIS_PROG_WISOI + k);
+    }
+    c.tg = g(IBIS_PROG_TG); c.wpud = g(IBIS_PROG_WPUD); c.wipud = g(IBIS_PROG_WIPUD);
+#pragma unroll
+    for (int k = 0; k < NB; ++k) c.tsoi_deep[k] = g(IBIS_PROG_TSOI_DEEP + k);
+    c.fi = g(IBIS_PROG_FI);
+#pragma unroll
+    for (int k = 0; k < NS; ++k) { c.tsno[k] = g(IBIS_PROG_TSNO + k); c.hsno[k] = g(IBIS_PROG_HSNO + k); }
+    c.ti = g(IBIS_PROG_TI); c.tlsub = g(IBIS_PROG_TLSUB);
+    c.tu = g(IBIS_PROG_TU); c.ts = g(IBIS_PROG_TS); c.tl = g(IBIS_PROG_TL);
+    c.t12 = g(IBIS_PROG_T12); c.t34 = g(IBIS_PROG_T34); c.q12 = g(IBIS_PROG_Q12); c.q34 = g(IBIS_PROG_Q34);
+    c.wliqu = g(IBIS_PROG_WLIQU); c.wliqs = g(IBIS_PROG_WLIQS); c.wliql = g(IBIS_PROG_WLIQL);
+    c.wsnou = g(IBIS_PROG_WSNOU); c.wsnos = g(IBIS_PROG_WSNOS); c.wsnol = g(IBIS_PROG_WSNOL);
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+        c.ci_u[j] = g(IBIS_PROG_CI_UPPER + j); c.gs_u[j] = g(IBIS_PROG_GS_UPPER + j); c.cs_u[j] = g(IBIS_PROG_CS_UPPER + j);
+    }
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        c.ci_l[j] = g(IBIS_PROG_CI_LOWER + j); c.gs_l[j] = g(IBIS_PROG_GS_LOWER + j); c.cs_l[j] = g(IBIS_PROG_CS_LOWER + j);
+    }
+    c.a10su = g(IBIS_PROG_A10SCALPARAMU); c.a10du = g(IBIS_PROG_A10DAYLIGHTU);
+    c.a10sl = g(IBIS_PROG_A10SCALPARAML); c.a10dl = g(IBIS_PROG_A10DAYLIGHTL);
+    c.firefac = g(IBIS_PROG_FIREFAC); c.nytimes = g(IBIS_PROG_NYTIMES); c.nfirestep = g(IBIS_PROG_NFIRESTEP);
+    c.sdry = g(IBIS_PROG_SDRY); c.nfirestep_vpd = g(IBIS_PROG_NFIRESTEP_VPD); c.sdry_vpd = g(IBIS_PROG_SDRY_VPD);
+}
+
+template <typename R>
+__device__ __forceinline__ R store_col(const Col<R>& c, R* __restrict__ p, int ld) {
+    R sum = R(0.0);
+    auto s = [&](int plane, R v) { p[(size_t)plane * ld] = v; sum = sum + v; };
+#pragma unroll
+    for (int k = 0; k < NL; ++k) {
+        s(IBIS_PROG_TSOI + k, c.tsoi[k]); s(IBIS_PROG_WSOI + k, c.wsoi[k]); s(IBIS_PROG_WISOI + k, c.wisoi[k]);
+    }
+    s(IBIS_PROG_TG, c.tg); s(IBIS_PROG_WPUD, c.wpud); s(IBIS_PROG_WIPUD, c.wipud);
+#pragma unroll
+    for (int k = 0; k < NB; ++k) s(IBIS_PROG_TSOI_DEEP + k, c.tsoi_deep[k]);
+    s(IBIS_PROG_FI, c.fi);
+#pragma unroll
+    for (int k = 0; k < NS; ++k) { s(IBIS_PROG_TSNO + k, c.tsno[k]); s(IBIS_PROG_HSNO + k, c.hsno[k]); }
+    s(IBIS_PROG_TI, c.ti); s(IBIS_PROG_TLSUB, c.tlsub);
+    s(IBIS_PROG_TU, c.tu); s(IBIS_PROG_TS, c.ts); s(IBIS_PROG_TL, c.tl);
+    s(IBIS_PROG_T12, c.t12); s(IBIS_PROG_T34, c.t34); s(IBIS_PROG_Q12, c.q12); s(IBIS_PROG_Q34, c.q34);
+    s(IBIS_PROG_WLIQU, c.wliqu); s(IBIS_PROG_WLIQS, c.wliqs); s(IBIS_PROG_WLIQL, c.wliql);
+    s(IBIS_PROG_WSNOU, c.wsnou); s(IBIS_PROG_WSNOS, c.wsnos); s(IBIS_PROG_WSNOL, c.wsnol);
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+        s(IBIS_PROG_CI_UPPER + j, c.ci_u[j]); s(IBIS_PROG_GS_UPPER + j, c.gs_u[j]); s(IBIS_PROG_CS_UPPER + j, c.cs_u[j]);
+    }
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        s(IBIS_PROG_CI_LOWER + j, c.ci_l[j]); s(IBIS_PROG_GS_LOWER + j, c.gs_l[j]); s(IBIS_PROG_CS_LOWER + j, c.cs_l[j]);
+    }
+    s(IBIS_PROG_A10SCALPARAMU, c.a10su); s(IBIS_PROG_A10DAYLIGHTU, c.a10du);
+    s(IBIS_PROG_A10SCALPARAML, c.a10sl); s(IBIS_PROG_A10DAYLIGHTL, c.a10dl);
+    s(IBIS_PROG_FIREFAC, c.firefac); s(IBIS_PROG_NYTIMES, c.nytimes); s(IBIS_PROG_NFIRESTEP, c.nfirestep);
+    s(IBIS_PROG_SDRY, c.sdry); s(IBIS_PROG_NFIRESTEP_VPD, c.nfirestep_vpd); s(IBIS_PROG_SDRY_VPD, c.sdry_vpd);
+    return sum;
+}
+
+template <typename R>
+__device__ __forceinline__ Forc<R> load_forc(const R* __restrict__ f, int ld) {
+    Forc<R> F;
+    auto g = [&](int plane) { return __ldg(f + (size_t)plane * ld); };
+    F.ta = g(IBIS_FORC_TA); F.qa = g(IBIS_FORC_QA); F.ua = g(IBIS_FORC_UA); F.ps = g(IBIS_FORC_PSURF);
+    F.cosz = g(IBIS_FORC_COSZEN);
+    F.sd[0] = g(IBIS_FORC_SOLAD); F.sd[1] = g(IBIS_FORC_SOLAD + 1);
+    F.si[0] = g(IBIS_FORC_SOLAI); F.si[1] = g(IBIS_FORC_SOLAI + 1);
+    F.fira = g(IBIS_FORC_FIRA); F.rain = g(IBIS_FORC_RAINA); F.snow = g(IBIS_FORC_SNOWA);
+    return F;
+}
+
+// Status word written by the kernels: [0] bit 0 = a column left the step with a
+// non-finite prognostic value; [1] = smallest such cell index (INT_MAX if none).
+template <typename R, int NT, bool SU, bool SL>
+__global__ void __launch_bounds__(kBlock) hourly_step_kernel(R* __restrict__ prog, const R* __restrict__ stat,
+                                                             const R* __restrict__ forc, R* __restrict__ diag,
+                                                             R* __restrict__ acc, int ncell, int ld, int nstep,
+                                                             long long forc_stride, const DevParams<R> P,
+                                                             int* __restrict__ status) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ncell) return;
+    Col<R> c;
+    load_col(c, prog + i, ld);
+    Stat<R> S{stat + i, ld};
+    Diag<R> D{diag ? diag + i : nullptr, ld};
+    Acc<R> A{acc ? acc + i : nullptr, ld, (P.flags & IBIS_FLAG_KAHAN) != 0};
+#pragma unroll 1
+    for (int s = 0; s < nstep; ++s) {
+        Forc<R> F = load_forc(forc + (size_t)s * forc_stride + i, ld);
+        column_step<R, NT, SU, SL>(c, F, S, D, A, P);
+    }
+    R sum = store_col(c, prog + i, ld);
+    if (status && !finite(sum)) {
+        atomicOr(status, 1);
+        atomicMin(status + 1, i);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+
+template <typename R>
+static DevParams<R> make_dev_params(const IbisParams& h) {
+    DevParams<R> d;
+    memset(&d, 0, sizeof(d));
+#define IBIS_S(name) d.name = (R)h.name;
+#define IBIS_A(name, n) for (int q = 0; q < n; ++q) d.name[q] = (R)h.name[q];
+    IBIS_PARAM_LIST(IBIS_S, IBIS_A)
+#undef IBIS_S
+#undef IBIS_A
+    d.flags = h.flags;
+    d.tfac = (R)(1.0 / pow(0.999, h.cappa));
+    d.vonk2 = (R)pow(h.vonk, 2.0);
+    d.cdmax = (R)(300.0 / (2.0 * h.dtime));
+    d.zweight = (R)exp(-1.0 / (10.0 * 86400.0 / h.dtime));
+    d.wliqmin = (R)(0.001 * (h.dtime / 3600.0) * (h.wliqumax / 0.2));
+    d.wsnomin = (R)(0.001 * (h.dtime / 3600.0) * (h.wsnoumax / 2.0));
+    d.znorm = (R)(1.0 - exp(h.stressfac));
+    d.rdt = (R)(1.0 / h.dtime);
+    d.zir = (R)(4.0 * 0.95 * h.stef);
+    for (int k = 1; k < NL; ++k) {
+        d.sw_hm[k] = 0.5 * (h.hsoi[k - 1] + h.hsoi[k]);
+        d.sw_wp[k] = 0.5 * h.hsoi[k] / d.sw_hm[k];
+        d.sw_wm[k] = 1.0 - d.sw_wp[k];
+    }
+    for (int k = 0; k < NL; ++k) {
+        double hb = k == 0 ? 0.5 * h.hsoi[0] : 0.5 * h.hsoi[k - 1] + 0.5 * h.hsoi[k];
+        d.sw_hb[k] = hb > 1e-30 ? hb : 1e-30;
+        double hp = k < NL - 1 ? 0.5 * (h.hsoi[k] + h.hsoi[k + 1]) : 1.0;
+        d.sw_hp[k] = hp > 1e-30 ? hp : 1e-30;
+    }
+    // respiration tables formed in float32 as the reference does (loops_gswp3.py:185-190)
+    const float per_s = (float)(h.ndaypy * 86400.0), mol = (float)(1000.0 / 12.0);
+    for (int j = 0; j < 12; ++j) {
+        d.rwood_s[j] = (R)(((float)h.rwood[j] / per_s) * mol);
+        d.rroot_s[j] = (R)(((float)h.rroot[j] / per_s) * mol);
+        d.keep[j] = (R)(1.0f - (float)h.rgrowth[j]);
+    }
+    d.ch4_w = (R)(float)(h.dtime / 86400.0);
+    d.rh_conv = (R)(float)(12.0e-3 * 86400.0);
+    double top = 0.0, tot = 0.0;
+    for (int k = 0; k < NL; ++k) {
+        double bot = top + h.hsoi[k];
+        double w = h.z_wt_ref - top;
+        w = w < 0.0 ? 0.0 : (w > h.hsoi[k] ? h.hsoi[k] : w);
+        d.ch4_wtop[k] = (R)w;
+        tot += w;
+        d.hsoi_top[k] = (R)top;
+        d.hsoi_bot[k] = (R)bot;
+        top = bot;
+    }
+    d.ch4_wtot = (R)(tot > 1e-12 ? tot : 1e-12);
+    return d;
+}
+
+template <typename R, int NT, bool SU, bool SL>
+static cudaError_t launch_variant(R* prog, const R* stat, const R* forc, R* diag, R* acc, int ncell, int ld, int nstep,
+                                  long long fstride, const DevParams<R>& P, int* status, cudaStream_t s) {
+    const int grid = (ncell + kBlock - 1) / kBlock;
+    hourly_step_kernel<R, NT, SU, SL><<<grid, kBlock, 0, s>>>(prog, stat, forc, diag, acc, ncell, ld, nstep, fstride,
+                                                              P, status);
+    return cudaGetLastError();
+}
+
+template <typename R>
+static int hourly_step(R* prog, const R* stat, const R* forc, R* diag, R* acc, int ncell, int ld, int nstep,
+                       const IbisParams* hp, int* status, void* stream) {
+    if (!prog || !stat || !forc || !hp) return -EINVAL;
+    if (ncell < 0 || nstep < 0 || ld < ncell || (ld % 32) != 0) return -EINVAL;
+    if (ncell == 0 || nstep == 0) return 0;
+    const unsigned known = IBIS_FLAG_BEDROCK | IBIS_FLAG_H2O_CONSISTENT | IBIS_FLAG_SUNSHADE_U | IBIS_FLAG_SUNSHADE_L |
+                           IBIS_FLAG_ACC | IBIS_FLAG_CH4 | IBIS_FLAG_SOIL_MEANS | IBIS_FLAG_DIAG | IBIS_FLAG_KAHAN;
+    if (hp->flags & ~known) return -EINVAL;
+    if ((hp->flags & (IBIS_FLAG_ACC | IBIS_FLAG_CH4 | IBIS_FLAG_SOIL_MEANS)) && !acc) return -EINVAL;
+    if ((hp->flags & IBIS_FLAG_DIAG) && !diag) return -EINVAL;
+    if (!(hp->dtime > 0.0)) return -EINVAL;
+    DevParams<R> P = make_dev_params<R>(*hp);
+    if (!(hp->flags & IBIS_FLAG_DIAG)) diag = nullptr;
+    if (!(hp->flags & (IBIS_FLAG_ACC | IBIS_FLAG_CH4 | IBIS_FLAG_SOIL_MEANS))) acc = nullptr;
+    const long long fstride = (long long)IBIS_FORC_COUNT * ld;
+    cudaStream_t s = (cudaStream_t)stream;
+    const bool bed = hp->flags & IBIS_FLAG_BEDROCK;
+    const bool su = hp->flags & IBIS_FLAG_SUNSHADE_U;
+    const bool sl = hp->flags & IBIS_FLAG_SUNSHADE_L;
+    cudaError_t e;
+#define IBIS_CASE(NT_, SU_, SL_) \
+    e = launch_variant<R, NT_, SU_, SL_>(prog, stat, forc, diag, acc, ncell, ld, nstep, fstride, P, status, s)
+    if (bed) {
+        if (su) { if (sl) IBIS_CASE(9, true, true); else IBIS_CASE(9, true, false); }
+        else { if (sl) IBIS_CASE(9, false, true); else IBIS_CASE(9, false, false); }
+    } else {
+        if (su) { if (sl) IBIS_CASE(6, true, true); else IBIS_CASE(6, true, false); }
+        else { if (sl) IBIS_CASE(6, false, true); else IBIS_CASE(6, false, false); }
+    }
+#undef IBIS_CASE
+    if (e != cudaSuccess) {
+        fprintf(stderr, "ibis_b200: kernel launch failed: %s\n", cudaGetErrorString(e));
+        return -(int)e - 1000;
+    }
+    return 0;
+}
+
+}  // namespace ibis

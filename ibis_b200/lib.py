@@ -1,0 +1,72 @@
+"""ctypes binding of the in-tree CUDA library (``include/ibis_b200.h``).
+
+The product path has no CPU fallback: :func:`load` raises when the library is
+missing or a symbol is absent, and the callers in this package never fall back
+to a host implementation.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+from .params import IbisParamsC
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(HERE)
+LIB_PATH = os.path.join(HERE, "_lib", "libibis_b200.so")
+
+_c_int_p = ctypes.POINTER(ctypes.c_int)
+_P = ctypes.POINTER(IbisParamsC)
+
+# name -> (restype, argtypes); every function declared in include/*.h
+SIGNATURES = {
+    "ibis_step_f32": (ctypes.c_int, [ctypes.c_void_p] * 5 + [ctypes.c_int] * 3 + [_P, ctypes.c_void_p, ctypes.c_void_p]),
+    "ibis_step_f64": (ctypes.c_int, [ctypes.c_void_p] * 5 + [ctypes.c_int] * 3 + [_P, ctypes.c_void_p, ctypes.c_void_p]),
+}
+
+_lib = None
+
+
+class IbisError(RuntimeError):
+    pass
+
+
+def declared_symbols():
+    """Function names declared in the public headers."""
+    names = []
+    inc = os.path.join(REPO, "include")
+    for f in sorted(os.listdir(inc)):
+        if not f.endswith(".h"):
+            continue
+        with open(os.path.join(inc, f)) as fh:
+            txt = fh.read()
+        names += re.findall(r"^\s*(?:int|void|size_t|const char\s*\*)\s+(ibis_\w+)\s*\(", txt, flags=re.M)
+    return names
+
+
+def load(path: str = LIB_PATH):
+    """Load the CUDA library (build it first with ``python -m ibis_b200.build``)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise IbisError(f"{path} is missing: build it with `python -m ibis_b200.build` (nvcc, sm_100a)")
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name, None)
+        if fn is None:
+            raise IbisError(f"{path} does not export {name}")
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(rc: int, what: str):
+    if rc != 0:
+        if rc == -22:
+            raise IbisError(f"{what}: invalid argument (EINVAL)")
+        if rc <= -1000:
+            raise IbisError(f"{what}: CUDA launch error {-rc - 1000}")
+        raise IbisError(f"{what}: error {rc}")

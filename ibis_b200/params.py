@@ -189,6 +189,12 @@ def header_struct_text() -> str:
     lines.append("    unsigned int _pad;")
     lines.append("} IbisParams;")
     lines.append("")
+    lines.append("/* X-macro over the record: S(name) for scalars, A(name, count) for tables. */")
+    lines.append("#define IBIS_PARAM_LIST(S, A) \\")
+    for name, n, _ in PARAM_FIELDS:
+        lines.append(f"    A({name}, {n}) \\" if n > 1 else f"    S({name}) \\")
+    lines.append("")
+    lines.append("")
     for nm, val in [("BEDROCK", FLAG_BEDROCK), ("H2O_CONSISTENT", FLAG_H2O_CONSISTENT),
                     ("SUNSHADE_U", FLAG_SUNSHADE_U), ("SUNSHADE_L", FLAG_SUNSHADE_L),
                     ("ACC", FLAG_ACC), ("CH4", FLAG_CH4), ("SOIL_MEANS", FLAG_SOIL_MEANS),

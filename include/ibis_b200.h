@@ -1,0 +1,50 @@
+/* C ABI of the B200-native IBIS 3.0 hourly land-surface step.
+ *
+ * The reference exposes this path as one pure function over Equinox pytrees,
+ *     timestep_body(state, consts, params, dtime) -> state
+ * (python-port/ibis/timestepping/loops.py:234-284), scanned by the day loop
+ * _run_day_inner._step_body (python-port/ibis/timestepping/loops_gswp3.py:115-320).
+ * It has no operator, plugin or FFI layer of its own; these entry points are
+ * what an XLA FFI handler or a ctypes/cgo binding of that function calls.
+ *
+ * Conventions
+ *   - All buffer pointers are DEVICE pointers owned by the caller.
+ *   - Buffers are structure-of-arrays "planes" (include/ibis_layout.h):
+ *     element (plane p, cell i) is buf[p * ld + i]; ld >= ncell, ld % 32 == 0.
+ *   - Calls are asynchronous on `stream` (a cudaStream_t; NULL = legacy default).
+ *   - Return 0 on success, -EINVAL for bad arguments, or a value <= -1000
+ *     (-(cudaError_t) - 1000) when the launch itself failed.
+ *   - A column whose state becomes non-finite is data, not an error: the kernel
+ *     sets status[0] |= 1 and status[1] = min(status[1], cell).  `status` may be
+ *     NULL; otherwise it is a device int[2] the caller initialises to {0, INT_MAX}.
+ */
+#ifndef IBIS_B200_H
+#define IBIS_B200_H
+
+#include "ibis_layout.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* nstep hourly steps of timestep_body (+ the day-loop accumulators when the
+ * IBIS_FLAG_ACC / _CH4 / _SOIL_MEANS bits of params->flags are set) on ncell
+ * columns, in FP32 with FP64 canopy and soil-water solves.
+ *   prog   [IBIS_PROG_COUNT][ld]              in/out: prognostic state
+ *   stat   [IBIS_STAT_COUNT][ld]              in: per-cell static inputs
+ *   forc   [nstep][IBIS_FORC_COUNT][ld]       in: hourly forcing (the atm leaves)
+ *   diag   [IBIS_DIAG_COUNT][ld] or NULL      out: last step's diagnostics (IBIS_FLAG_DIAG)
+ *   acc    [2*IBIS_ACC_COUNT][ld] or NULL     in/out: accumulators then Kahan terms
+ * Replaces: timestep_body (loops.py:234) iterated by _step_body (loops_gswp3.py:115). */
+int ibis_step_f32(float* prog, const float* stat, const float* forc, float* diag, float* acc, int ncell, int ld,
+                  int nstep, const IbisParams* params, int* status, void* stream);
+
+/* Same contract in float64 throughout (the float64 run of the reference's step). */
+int ibis_step_f64(double* prog, const double* stat, const double* forc, double* diag, double* acc, int ncell,
+                  int ld, int nstep, const IbisParams* params, int* status, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* IBIS_B200_H */

@@ -303,6 +303,111 @@ typedef struct IbisParams {
     unsigned int _pad;
 } IbisParams;
 
+/* X-macro over the record: S(name) for scalars, A(name, count) for tables. */
+#define IBIS_PARAM_LIST(S, A) \
+    S(stef) \
+    S(vonk) \
+    S(grav) \
+    S(tmelt) \
+    S(hvap) \
+    S(hfus) \
+    S(hsub) \
+    S(ch2o) \
+    S(cice) \
+    S(cair) \
+    S(cvap) \
+    S(rair) \
+    S(rvap) \
+    S(cappa) \
+    S(rhow) \
+    S(epsilon) \
+    S(dtime) \
+    S(co2conc) \
+    S(z0sno) \
+    S(rhos) \
+    S(consno) \
+    S(hsnotop) \
+    S(hsnomin) \
+    S(fimin) \
+    S(fimax) \
+    A(rhoveg, 4) \
+    A(tauveg, 4) \
+    A(oriev, 2) \
+    A(orieh, 2) \
+    A(omegasno, 2) \
+    S(cleaf) \
+    S(cstem) \
+    S(cgrass) \
+    A(dleaf, 2) \
+    A(dstem, 2) \
+    S(alaiml) \
+    S(alaimu) \
+    S(chu) \
+    S(chs) \
+    S(chl) \
+    S(soil_beta_power) \
+    S(wliqumax) \
+    S(wliqsmax) \
+    S(wliqlmax) \
+    S(wsnoumax) \
+    S(wsnosmax) \
+    S(wsnolmax) \
+    S(tdripu) \
+    S(tdrips) \
+    S(tdripl) \
+    S(tblowu) \
+    S(tblows) \
+    S(tblowl) \
+    S(fmax) \
+    S(tau15) \
+    S(kc15) \
+    S(ko15) \
+    S(cimax) \
+    S(o2conc) \
+    S(alpha3) \
+    S(theta3) \
+    S(beta3) \
+    S(alpha4) \
+    S(theta4) \
+    S(beta4) \
+    A(gamma, 5) \
+    A(coefm, 5) \
+    A(coefb, 5) \
+    A(gsmin, 5) \
+    A(vmax_pft, 12) \
+    S(stressfac) \
+    S(cap_kn) \
+    S(wpudmax) \
+    S(zwpmax) \
+    S(bperm) \
+    S(rhosoi_val) \
+    S(csoi_mineral_val) \
+    A(hsoi, 6) \
+    A(froot, 12) \
+    A(hsoi_bed, 3) \
+    S(consoi_bed) \
+    S(rhosoi_bed) \
+    S(csoi_bed) \
+    S(d_crit) \
+    S(vpd_ref) \
+    S(d_crit_vpd) \
+    S(flux_max) \
+    S(t_max_dev) \
+    S(sat_crit) \
+    S(z_max) \
+    S(r_ch4) \
+    S(q10p) \
+    S(t_ref) \
+    S(z_wt_max) \
+    S(z_wt_ref) \
+    S(z_tau) \
+    S(tau_oxid) \
+    A(rwood, 12) \
+    A(rroot, 12) \
+    A(rgrowth, 12) \
+    S(ndaypy) \
+
+
 #define IBIS_FLAG_BEDROCK 1u
 #define IBIS_FLAG_H2O_CONSISTENT 2u
 #define IBIS_FLAG_SUNSHADE_U 4u

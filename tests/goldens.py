@@ -57,7 +57,7 @@ FLOORS = {
     "fvapg": 1e-9, "fvapi": 1e-9, "ginvap": 1e-9, "gsuvap": 1e-9, "gtrans": 1e-9, "gtransu": 1e-9,
     "gtransl": 1e-9, "grunof": 1e-9, "gdrain": 1e-9, "gadjust": 1e-9, "raing": 1e-9, "snowg": 1e-9,
     "rainl": 1e-9, "snowl": 1e-9, "raing_avg": 1e-9, "ch4": 1e-15, "aygpptot": 1e-9, "aynpptot": 1e-9,
-    "aynpp": 1e-9, "a10ancub": 1e-9, "a10ancls": 1e-9, "a10ancl3": 1e-9, "a10ancl4": 1e-9,
+    "aynpp": 1e-9, "hflo": 1.0, "a10ancub": 1e-9, "a10ancls": 1e-9, "a10ancl3": 1e-9, "a10ancl4": 1e-9,
 }
 
 
