@@ -1,0 +1,315 @@
+"""Benchmark of the B200 hourly land-surface step (IBIS 3.0 timestep_body).
+
+Workload (one "step"): one day -- 24 hourly steps of timestep_body plus the
+day-loop accumulators and hourly wetland CH4 -- on 95,333 independent columns
+(the 0.5-degree land-cell count), FP32 structure-of-arrays state, seeded
+synthetic forcing and columns (ibis_b200.synth).  Multi-GPU runs are weak
+scaling: every rank advances its own 95,333 columns with no data-path
+communication (a max-reduce of the timings is the only collective).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Rank 0 prints one JSON line.  ``--impl reference`` times the CPU oracle (the
+reference's algorithm restated in NumPy, float64) on all host cores, because
+the reference's own JAX step cannot run here (no jax/jaxlib/equinox).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+import warnings
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "cell-steps/s at 95,333 cells, ≤1e-4 rel err vs FP64; serve p50/p99 latency"
+NCELL = 95333
+HOURS = 24
+
+
+def _peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _algorithmic_bytes(nhours):
+    """Bytes one cell needs moved per launch of the hourly-step kernel (FP32):
+    prognostic planes read and written, the static planes the step reads, the
+    hourly forcing, and the enabled accumulators with their Kahan terms read
+    and written."""
+    from ibis_b200 import layout as L
+    prog = 2 * L.N_PROG * 4
+    stat_planes = (10 * 6) + 3 + 8 + 2 + 12 + 3 + 10 + 12 + 3   # planes column_step reads
+    acc_planes = 23 + 1                                          # ACC + CH4 value planes
+    acc = 2 * 2 * acc_planes * 4
+    return prog + stat_planes * 4 + acc + nhours * L.N_FORC * 4
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        for line in (self.out or "").strip().splitlines():
+            p = [x.strip() for x in line.split(",")]
+            if len(p) >= 9:
+                rows.append(p)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mxs = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mxs) if mxs else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_baseline_sample(ncell=16384, hours=HOURS, seed=123):
+    """The float64 oracle on one host core over a bounded sample of the workload."""
+    import oracle
+    from ibis_b200 import synth
+    wl = synth.make_workload(ncell, hours, seed=seed)
+    prog = wl.prog
+    acc = oracle.new_acc(ncell)
+    t0 = time.perf_counter()
+    with np.errstate(all="ignore"):
+        for h in range(hours):
+            prog, _, acc = oracle.step(prog, wl.stat, wl.forcing_at(h), wl.params, acc)
+    dt = time.perf_counter() - t0
+    return {"value": ncell * hours / dt, "unit": "cell-steps/s", "cores": 1, "kind": "port",
+            "sample": f"{ncell} cells x {hours} hourly steps of the configs[1] generator, float64 NumPy oracle, "
+                      f"{dt:.1f} s"}
+
+
+# ---------------------------------------------------------------------------- reference arm
+def _oracle_chunk(args):
+    prog, stat, forc, params, hours = args
+    import oracle
+    acc = oracle.new_acc(prog["tg"].shape[0])
+    with np.errstate(all="ignore"):
+        for h in range(hours):
+            prog, _, acc = oracle.step(prog, stat, {k: v[h] for k, v in forc.items()}, params, acc)
+    return prog["tg"].shape[0]
+
+
+def run_reference(args):
+    """The CPU oracle on all host cores (spawned process pool), same metric and config."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    from ibis_b200 import synth
+    warnings.filterwarnings("ignore")
+    cores = os.cpu_count() or 1
+    ncell = min(NCELL, 4000 * cores)
+    wl = synth.make_workload(ncell, HOURS, seed=0)
+    chunks = np.array_split(np.arange(ncell), cores)
+    tasks = []
+    for idx in chunks:
+        if idx.size == 0:
+            continue
+        sl = lambda d: {k: v[idx] for k, v in d.items()}
+        tasks.append((sl(wl.prog), sl(wl.stat), {k: v[:, idx] for k, v in wl.forc.items()}, wl.params, HOURS))
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(processes=len(tasks)) as pool:
+        for _ in range(args.warmup):
+            pool.map(_oracle_chunk, [(t[0], t[1], {k: v[:1] for k, v in t[2].items()}, t[3], 1) for t in tasks])
+        times = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            pool.map(_oracle_chunk, tasks)
+            times.append(time.perf_counter() - t0)
+    ms = 1e3 * float(np.mean(times))
+    v = ncell * HOURS / (ms / 1e3)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "cell-steps/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{ncell} of 95,333 cells x 24 hourly steps per step (bounded sample), "
+                                   "float64 NumPy restatement of the reference step", "ncell": ncell,
+                       "hours_per_step": HOURS},
+            "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": len(tasks), "kind": "port",
+                             "sample": f"{ncell} cells x {HOURS} h per step over {len(tasks)} spawned processes"},
+            "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference's JAX step is not installable here (no jax/jaxlib/equinox wheels); this arm "
+                    "times the oracle port of its algorithm"}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------- our arm
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from ibis_b200 import synth
+    from ibis_b200.columns import Columns
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample()
+
+    wl = synth.make_workload(args.ncell, HOURS, seed=1000 + rank)
+    P = wl.params
+    cols = Columns.from_host(wl.prog, wl.stat, dtype=torch.float32, device=dev, acc=True)
+    forc = cols.forcing(wl.forc)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def day():
+        cols.run(forc, P, stream=stream)
+
+    def day_per_step():
+        for h in range(HOURS):
+            cols.run(forc[h:h + 1], P, stream=stream)
+
+    def timed(fn, k):
+        evs = []
+        for _ in range(k):
+            flush.fill_(1.0)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            evs.append((a, b))
+        torch.cuda.synchronize(dev)
+        return [a.elapsed_time(b) for a, b in evs]
+
+    with ClockSampler(local) as clk:
+        for _ in range(args.warmup):
+            day()
+            day_per_step()
+        torch.cuda.synchronize(dev)
+        barrier()
+        torch.cuda.synchronize(dev)
+        ms = timed(day, args.steps)
+        barrier()
+        torch.cuda.synchronize(dev)
+    ms_step = float(np.sum(ms)) / args.steps
+    ms_plain = float(np.sum(timed(day_per_step, args.steps))) / args.steps
+
+    # end to end through the public API: pinned host forcing in, host state out, copies timed
+    h_forc = torch.from_numpy(synth.forcing_planes(wl.forc, cols.ld)).pin_memory()
+    h_prog = torch.empty_like(cols.prog, device="cpu").pin_memory()
+    d_forc = torch.empty_like(forc)
+
+    def e2e_day():
+        d_forc.copy_(h_forc, non_blocking=True)
+        cols.run(d_forc, P, stream=stream)
+        h_prog.copy_(cols.prog, non_blocking=True)
+
+    e2e_day()
+    ms_e2e = float(np.sum(timed(e2e_day, args.steps))) / args.steps
+
+    nonfinite = cols.nonfinite()
+    if world > 1:
+        t = torch.tensor([ms_step, ms_plain, ms_e2e], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_step, ms_plain, ms_e2e = (float(x) for x in t.cpu())
+    cell_steps = world * args.ncell * HOURS
+    value = cell_steps / (ms_step / 1e3)
+    peak, peak_kind = _peaks()
+    bpl = _algorithmic_bytes(HOURS) * args.ncell
+    achieved = bpl / (ms_step / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(REPO, "profiles", "hourly_step_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            tj = json.load(f)
+        per_cell = tj.get("fused_day_bytes_per_cell")
+        if per_cell:
+            traffic = float(per_cell) * args.ncell
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{args.ncell} cells x 24 hourly steps (one day) per step, FP32 SoA state, "
+                                   "accumulators + hourly CH4 on, one fused launch per day",
+                       "ncell_per_gpu": args.ncell, "hours_per_step": HOURS,
+                       "l2": "flushed between timed steps (256 MiB write, outside the events)",
+                       "parallelism": f"replicas x{world} (independent columns, no collectives)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": peak_kind, "algorithmic_bytes_per_launch": bpl},
+            "per_step_launch": {"value": cell_steps / (ms_plain / 1e3), "ms_per_step": ms_plain,
+                                "launches_per_step": HOURS,
+                                "achieved_gbs": _algorithmic_bytes(1) * args.ncell * HOURS / (ms_plain / 1e3) / 1e9},
+            "e2e": {"value": cell_steps / (ms_e2e / 1e3), "unit": "cell-steps/s",
+                    "h2d_bytes_per_step": int(h_forc.numel() * 4), "d2h_bytes_per_step": int(h_prog.numel() * 4)},
+            "gpu_launches": args.steps,
+            "clocks": clk.summary(),
+            "nonfinite_columns": nonfinite[0],
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ncell", type=int, default=NCELL)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()
