@@ -29,7 +29,8 @@ def _ptr(t):
 class Columns:
     """``ncell`` IBIS columns resident on ``device`` in FP32 (default) or FP64."""
 
-    def __init__(self, ncell: int, dtype=torch.float32, device="cuda", diag: bool = False, acc: bool = True):
+    def __init__(self, ncell: int, dtype=torch.float32, device="cuda", diag: bool = False, acc: bool = True,
+                 mode: str = "fused"):
         if dtype not in (torch.float32, torch.float64):
             raise ValueError("dtype must be torch.float32 or torch.float64")
         self.ncell = int(ncell)
@@ -48,13 +49,30 @@ class Columns:
         self.acc = torch.zeros((2 * L.N_ACC, self.ld), **kw) if acc else None
         self.status = torch.tensor([0, INT_MAX], dtype=torch.int32, device=self.device)
         self._np_dtype = np.float32 if dtype == torch.float32 else np.float64
-        self._fn = _lib.load().ibis_step_f32 if dtype == torch.float32 else _lib.load().ibis_step_f64
+        lib = _lib.load()
+        self._fn = lib.ibis_step_f32 if dtype == torch.float32 else lib.ibis_step_f64
+        self._split = lib.ibis_step_split_f32
+        self.scratch = None
+        self.set_mode(mode)
+
+    def set_mode(self, mode: str):
+        """``fused`` (one kernel per launch) or ``split`` (surface + ground kernels per hour)."""
+        if mode not in ("fused", "split"):
+            raise ValueError("mode must be 'fused' or 'split'")
+        if mode == "split":
+            if self.dtype != torch.float32:
+                raise ValueError("the split form is FP32 only")
+            if self.scratch is None:
+                self.scratch = torch.zeros((_lib.load().ibis_mid_planes(), self.ld), dtype=self.dtype,
+                                           device=self.device)
+        self.mode = mode
 
     # -------------------------------------------------------------- transfer
     @classmethod
-    def from_host(cls, prog: dict, stat: dict, dtype=torch.float32, device="cuda", diag=False, acc=True):
+    def from_host(cls, prog: dict, stat: dict, dtype=torch.float32, device="cuda", diag=False, acc=True,
+                  mode="fused"):
         n = prog["tg"].shape[0]
-        c = cls(n, dtype=dtype, device=device, diag=diag, acc=acc)
+        c = cls(n, dtype=dtype, device=device, diag=diag, acc=acc, mode=mode)
         c.set_prog(prog)
         c.set_stat(stat)
         return c
@@ -125,7 +143,12 @@ class Columns:
         p.flags = flags
         if stream is None:
             stream = torch.cuda.current_stream(self.device)
-        rc = self._fn(_ptr(self.prog), _ptr(self.stat), _ptr(forc), _ptr(self.diag), _ptr(self.acc), self.ncell,
-                      self.ld, nstep, ctypes.byref(p), _ptr(self.status), ctypes.c_void_p(stream.cuda_stream))
+        if self.mode == "split":
+            rc = self._split(_ptr(self.prog), _ptr(self.stat), _ptr(forc), _ptr(self.diag), _ptr(self.acc),
+                             _ptr(self.scratch), self.ncell, self.ld, nstep, ctypes.byref(p), _ptr(self.status),
+                             ctypes.c_void_p(stream.cuda_stream))
+        else:
+            rc = self._fn(_ptr(self.prog), _ptr(self.stat), _ptr(forc), _ptr(self.diag), _ptr(self.acc), self.ncell,
+                          self.ld, nstep, ctypes.byref(p), _ptr(self.status), ctypes.c_void_p(stream.cuda_stream))
         _lib.check(rc, "ibis_step")
         return self

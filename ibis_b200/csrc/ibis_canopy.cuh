@@ -2,6 +2,11 @@
 // Reference: python-port/ibis/physics/stomata.py and canopy_exchange.py:470-811.
 #pragma once
 #include "ibis_column.cuh"
+#include "gauss9_gen.cuh"
+
+#ifndef IBIS_FAST_SAT
+#define IBIS_FAST_SAT 0
+#endif
 
 namespace ibis {
 
@@ -247,51 +252,18 @@ __device__ __forceinline__ void stomata(Stom<R>& o, Col<R>& c, R tu, R tl, R t12
 // Always double.  Unknowns: tu ts tl t12 t34 q12 q34 tg ti.
 // ---------------------------------------------------------------------------
 
-// Structural nonzeros of the system after fill-in by no-pivot elimination in row
-// order.  Updates that would multiply a structural zero leave their target
-// unchanged in IEEE arithmetic, so skipping them reproduces the dense
-// elimination (canopy_exchange.py:26-61) exactly.
-__device__ constexpr bool kNZ[9][9] = {
-    {1, 0, 0, 1, 0, 1, 0, 0, 0}, {0, 1, 0, 1, 0, 1, 0, 0, 0}, {0, 0, 1, 0, 1, 0, 1, 0, 0},
-    {1, 1, 0, 1, 1, 1, 0, 0, 0}, {0, 0, 1, 1, 1, 1, 1, 1, 1}, {1, 1, 0, 1, 1, 1, 1, 1, 1},
-    {0, 0, 1, 0, 1, 1, 1, 1, 1}, {0, 0, 0, 0, 1, 1, 1, 1, 1}, {0, 0, 0, 0, 1, 1, 1, 1, 1}};
-
-__device__ __forceinline__ void gauss9(double (&A)[9][9], double (&b)[9], double (&x)[9]) {
-#pragma unroll
-    for (int p = 0; p < 8; ++p) {
-#pragma unroll
-        for (int i = p + 1; i < 9; ++i) {
-            if (kNZ[i][p]) {
-                double f = A[i][p] / A[p][p];
-#pragma unroll
-                for (int j = p + 1; j < 9; ++j)
-                    if (kNZ[p][j]) A[i][j] = A[i][j] - f * A[p][j];
-                b[i] = b[i] - f * b[p];
-            }
-        }
-    }
-#pragma unroll
-    for (int i = 8; i >= 0; --i) {
-        double s = 0.0;
-#pragma unroll
-        for (int j = i + 1; j < 9; ++j)
-            if (kNZ[i][j]) s = s + A[i][j] * x[j];
-        x[i] = (b[i] - s) / A[i][i];
-    }
-}
-
-// Inputs of turvap that do not change across the three passes.
+// Inputs of turvap that do not change across the three passes (stored in R;
+// widened to double where the system is assembled).
 template <typename R>
 struct TvFixed {
-    double xu, xs, xl, fi, chux, chsx, chlx, cog, coi, zirg, ziri;
-    double wliqu, wliqs, wliql, wsnou, wsnos, wsnol;
-    double rliqu, rliqs, rliql, fwetu, fwets, fwetl;
-    double hvasug, hvasui, tsoi0, tsno0;
-    double zwtot, swilt0, suction0, bex0;
-    double fradu, frads, fradl, pfluxu, pfluxs, pfluxl;
-    double solg, soli, firg, firi, firb;
-    double lai1, lai0, lsl0, fu, fl;
-    double frac[12];
+    R xu, xs, xl, fi, chux, chsx, chlx, cog, coi, zirg, ziri;
+    R wliqu, wliqs, wliql, wsnou, wsnos, wsnol;
+    R rliqu, rliqs, rliql, fwetu, fwets, fwetl;
+    R hvasug, hvasui, tsoi0, tsno0;
+    R zwtot, swilt0, suction0, bex0;
+    R fradu, frads, fradl, pfluxu, pfluxs, pfluxl;
+    R solg, soli, firg, firi, firb;
+    R lai1, lai0, lsl0, fu, fl;
 };
 
 template <typename R>
@@ -303,9 +275,23 @@ struct TvOut {
 
 struct Sat64 { double q, dq; };
 
+// Saturation humidity and its capped derivative at the blended temperature.
+// The float kernels evaluate the Lowe polynomials in R (they carry R-precision
+// inputs anyway) and widen the result; the float64 kernels stay in double.
+template <typename R>
 __device__ __forceinline__ Sat64 sat64(double t, double ps) {
-    double e = esat(t);
     Sat64 s;
+#if IBIS_FAST_SAT
+    if constexpr (sizeof(R) == 4) {
+        const float tf = (float)t, pf = (float)ps;
+        const float e = esat(tf);
+        const float q = qsat(e, pf);
+        s.q = q;
+        s.dq = fminf(dqsat(tf, q, e), q * 0.1f);
+        return s;
+    }
+#endif
+    double e = esat(t);
     s.q = qsat(e, ps);
     s.dq = fmin(dqsat(t, s.q, e), s.q * 0.1);
     return s;
@@ -315,7 +301,7 @@ template <typename R>
 __device__ __forceinline__ void turvap(double (&W)[9], TvOut<R>& o, const double (&old)[5], const Trans<R>& T,
                                        double cp, double tfac, double wu, double ws, double wl, double wg,
                                        double wi, const TvFixed<R>& X, const Stom<R>& st, double ta, double qa,
-                                       double ps, const DevParams<R>& P) {
+                                       double ps, const Stat<R>& S, const DevParams<R>& P) {
     const double eps = (double)P.epsilon, dt = (double)P.dtime;
     const double tmelt = (double)P.tmelt, hvap = (double)P.hvap, hsub = (double)P.hsub;
     const double ch2o = (double)P.ch2o, cice = (double)P.cice, cvap = (double)P.cvap;
@@ -325,15 +311,16 @@ __device__ __forceinline__ void turvap(double (&W)[9], TvOut<R>& o, const double
     const double tg = wg * W[7] + (1.0 - wg) * old[3];
     const double ti = wi * W[8] + (1.0 - wi) * old[4];
     const double t34 = W[4], q12 = W[5], q34 = W[6];
-    const Sat64 Su = sat64(tu, ps), Ss = sat64(ts, ps), Sl = sat64(tl, ps), Sg = sat64(tg, ps), Si = sat64(ti, ps);
+    const Sat64 Su = sat64<R>(tu, ps), Ss = sat64<R>(ts, ps), Sl = sat64<R>(tl, ps), Sg = sat64<R>(tg, ps),
+                Si = sat64<R>(ti, ps);
     const double qu = Su.q, dqu = Su.dq, qs = Ss.q, dqs = Ss.dq, ql = Sl.q, dql = Sl.dq;
     const double qg = Sg.q, dqg = Sg.dq, qi = Si.q, dqi = Si.dq;
 
     // soil-surface humidity factor (canopy_exchange.py:532-572)
-    const double psig = -(double)P.grav * X.suction0 * pow(X.zwtot, -X.bex0);
+    const double psig = -(double)P.grav * (double)X.suction0 * pow((double)X.zwtot, -(double)X.bex0);
     const double hfac = exp(psig / ((double)P.rvap * tg));
     const double hfac2 = q34 / fmax(qg, eps);
-    double betaw = clip((X.zwtot - X.swilt0) / fmax(1.0 - X.swilt0, eps), 0.0, 1.0);
+    double betaw = clip(((double)X.zwtot - (double)X.swilt0) / fmax(1.0 - (double)X.swilt0, eps), 0.0, 1.0);
     if ((double)P.soil_beta_power != 1.0) betaw = pow(betaw, (double)P.soil_beta_power);
     const double e34 = esat(t34);
     const double qs1 = qsat(e34, ps);
@@ -351,7 +338,9 @@ __device__ __forceinline__ void turvap(double (&W)[9], TvOut<R>& o, const double
     // vapour conductances (canopy_exchange.py:587-618)
     const double su = T.su, ss = T.ss, sl = T.sl, sg = T.sg, si = T.si, cu = T.cu, cl = T.cl;
     const double tb = st.tcub, tc = st.tcuc;
-    const double* fr = X.frac;
+    double fr[12];
+#pragma unroll
+    for (int j = 0; j < 12; ++j) fr[j] = (double)S(IBIS_STAT_FRAC, j);
     const double suw = fmin(fwux * su, 0.8 * (X.wliqu + X.wsnou) / fmax(dt * (qu - q12), eps));
     const double sut = fmax(0.0, (1.0 - fwux) * 0.5 * (tb * fr[0] + tb * fr[1] + tb * fr[2] + tc * fr[3]
                                                       + tb * fr[4] + tc * fr[5] + tb * fr[6] + tb * fr[7]));
@@ -364,91 +353,88 @@ __device__ __forceinline__ void turvap(double (&W)[9], TvOut<R>& o, const double
     const double slw = fmin(fwlx * sl, 0.8 * (X.wliql + X.wsnol) / fmax(dt * (ql - q34), eps));
     const double tls = st.tcls, tl3 = st.tcl3, tl4 = st.tcl4;
     const double slt0 = fmax(0.0, (1.0 - fwlx) * 0.5 * (tls * fr[8] + tls * fr[9] + tl4 * fr[10] + tl3 * fr[11]));
-    const double slt = slt0 * X.lai0 / fmax(X.lsl0, eps);
+    const double slt = slt0 * (double)X.lai0 / fmax((double)X.lsl0, eps);
     const double hvl = hvap + cvap * (ta - tmelt) - ch2o * (tl - tmelt);
     const double slh = slw * (X.rliql * hvl + (1.0 - X.rliql) * (hsub + cvap * (ta - tmelt) - cice * (tl - tmelt)))
                      + slt * hvl;
 
     // matrix and right-hand side (canopy_exchange.py:620-682)
-    double A[9][9];
-#pragma unroll
-    for (int i = 0; i < 9; ++i)
-#pragma unroll
-        for (int j = 0; j < 9; ++j) A[i][j] = 0.0;
-    double b[9];
+    Sys9 M;
+    sys9_zero(M);
     const double rdt = 1.0 / dt;
     const double fi = X.fi;
     double r2 = su * cp;
-    A[0][0] = X.chux * rdt + wu * r2 + wu * suh * dqu;
-    A[0][3] = -r2;
-    A[0][5] = -suh;
-    b[0] = old[0] * X.chux * rdt - (1.0 - wu) * r2 * tu - suh * (qu - wu * dqu * tu) + X.fradu - X.pfluxu;
+    M.a00 = X.chux * rdt + wu * r2 + wu * suh * dqu;
+    M.a03 = -r2;
+    M.a05 = -suh;
+    M.b0 = old[0] * X.chux * rdt - (1.0 - wu) * r2 * tu - suh * (qu - wu * dqu * tu) + X.fradu - X.pfluxu;
     r2 = ss * cp;
-    A[1][1] = X.chsx * rdt + ws * r2 + ws * ssh * dqs;
-    A[1][3] = -r2;
-    A[1][5] = -ssh;
-    b[1] = old[1] * X.chsx * rdt - (1.0 - ws) * r2 * ts - ssh * (qs - ws * dqs * ts) + X.frads - X.pfluxs;
+    M.a11 = X.chsx * rdt + ws * r2 + ws * ssh * dqs;
+    M.a13 = -r2;
+    M.a15 = -ssh;
+    M.b1 = old[1] * X.chsx * rdt - (1.0 - ws) * r2 * ts - ssh * (qs - ws * dqs * ts) + X.frads - X.pfluxs;
     r2 = sl * cp;
-    A[2][2] = X.chlx * rdt + wl * r2 + wl * slh * dql;
-    A[2][4] = -r2;
-    A[2][6] = -slh;
-    b[2] = old[2] * X.chlx * rdt - (1.0 - wl) * r2 * tl - slh * (ql - wl * dql * tl) + X.fradl - X.pfluxl;
+    M.a22 = X.chlx * rdt + wl * r2 + wl * slh * dql;
+    M.a24 = -r2;
+    M.a26 = -slh;
+    M.b2 = old[2] * X.chlx * rdt - (1.0 - wl) * r2 * tl - slh * (ql - wl * dql * tl) + X.fradl - X.pfluxl;
     const double ru = X.xu * su, rs = X.xs * ss;
-    A[3][0] = -wu * ru;
-    A[3][1] = -ws * rs;
-    A[3][3] = cu + cl + ru + rs;
-    A[3][4] = -cl;
-    b[3] = cu * ta * tfac + (1.0 - wu) * ru * tu + (1.0 - ws) * rs * ts;
+    M.a30 = -wu * ru;
+    M.a31 = -ws * rs;
+    M.a33 = cu + cl + ru + rs;
+    M.a34 = -cl;
+    M.b3 = cu * ta * tfac + (1.0 - wu) * ru * tu + (1.0 - ws) * rs * ts;
     const double rl = X.xl * sl, ri = fi * si;
-    A[4][2] = -wl * rl;
-    A[4][3] = -cl;
-    A[4][4] = cl + rl + (1.0 - fi) * sg + ri;
-    A[4][7] = -wg * (1.0 - fi) * sg;
-    A[4][8] = -wi * ri;
-    b[4] = (1.0 - wl) * rl * tl + (1.0 - wg) * (1.0 - fi) * sg * tg + (1.0 - wi) * ri * ti;
+    M.a42 = -wl * rl;
+    M.a43 = -cl;
+    M.a44 = cl + rl + (1.0 - fi) * sg + ri;
+    M.a47 = -wg * (1.0 - fi) * sg;
+    M.a48 = -wi * ri;
+    M.b4 = (1.0 - wl) * rl * tl + (1.0 - wg) * (1.0 - fi) * sg * tg + (1.0 - wi) * ri * ti;
     const double ruq = X.xu * (suw + sut), rsq = X.xs * ssw;
-    A[5][0] = -wu * ruq * dqu;
-    A[5][1] = -ws * rsq * dqs;
-    A[5][5] = cu + cl + ruq + rsq;
-    A[5][6] = -cl;
-    b[5] = cu * qa + ruq * (qu - wu * dqu * tu) + rsq * (qs - ws * dqs * ts);
+    M.a50 = -wu * ruq * dqu;
+    M.a51 = -ws * rsq * dqs;
+    M.a55 = cu + cl + ruq + rsq;
+    M.a56 = -cl;
+    M.b5 = cu * qa + ruq * (qu - wu * dqu * tu) + rsq * (qs - ws * dqs * ts);
     const double rlq = X.xl * (slw + slt), rgq = (1.0 - fi) * sg;
-    A[6][2] = -wl * rlq * dql;
-    A[6][5] = -cl;
-    A[6][6] = cl + rlq + rgq + fi * si;
-    A[6][7] = -wg * rgq * qgfac * dqg;
-    A[6][8] = -wi * fi * si * dqi;
-    b[6] = rlq * (ql - wl * dql * tl) + rgq * qgfac * (qg - wg * dqg * tg) + fi * si * (qi - wi * dqi * ti);
+    M.a62 = -wl * rlq * dql;
+    M.a65 = -cl;
+    M.a66 = cl + rlq + rgq + fi * si;
+    M.a67 = -wg * rgq * qgfac * dqg;
+    M.a68 = -wi * fi * si * dqi;
+    M.b6 = rlq * (ql - wl * dql * tl) + rgq * qgfac * (qg - wg * dqg * tg) + fi * si * (qi - wi * dqi * ti);
     double r1 = sg * cp;
     r2 = sg * X.hvasug;
-    A[7][4] = -r1;
-    A[7][6] = -r2;
-    A[7][7] = r1 + r2 * qgfac * dqg + X.cog + X.zirg;
-    b[7] = -r2 * qgfac * (qg - dqg * tg) + X.cog * X.tsoi0 + X.solg + X.firg + X.zirg * old[3];
+    M.a74 = -r1;
+    M.a76 = -r2;
+    M.a77 = r1 + r2 * qgfac * dqg + X.cog + X.zirg;
+    M.b7 = -r2 * qgfac * (qg - dqg * tg) + X.cog * X.tsoi0 + X.solg + X.firg + X.zirg * old[3];
     r1 = si * cp;
     r2 = si * X.hvasui;
-    A[8][4] = -r1;
-    A[8][6] = -r2;
-    A[8][8] = r1 + r2 * dqi + X.coi + X.ziri;
-    b[8] = -r2 * (qi - dqi * ti) + X.coi * X.tsno0 + X.soli + X.firi + X.ziri * old[4];
+    M.a84 = -r1;
+    M.a86 = -r2;
+    M.a88 = r1 + r2 * dqi + X.coi + X.ziri;
+    M.b8 = -r2 * (qi - dqi * ti) + X.coi * X.tsno0 + X.soli + X.firi + X.ziri * old[4];
 
     // bare cells: canopy rows pinned to the air (canopy_exchange.py:684-732)
     if ((X.xu + X.xs + X.xl) < eps) {
-#pragma unroll
-        for (int i = 0; i < 7; ++i) {
-#pragma unroll
-            for (int j = 0; j < 9; ++j) A[i][j] = (i == j) ? 1.0 : 0.0;
-        }
+        M.a00 = 1.0; M.a03 = 0.0; M.a05 = 0.0;
+        M.a11 = 1.0; M.a13 = 0.0; M.a15 = 0.0;
+        M.a22 = 1.0; M.a24 = 0.0; M.a26 = 0.0;
+        M.a30 = 0.0; M.a31 = 0.0; M.a33 = 1.0; M.a34 = 0.0;
+        M.a42 = 0.0; M.a43 = 0.0; M.a44 = 1.0; M.a47 = 0.0; M.a48 = 0.0;
+        M.a50 = 0.0; M.a51 = 0.0; M.a55 = 1.0; M.a56 = 0.0;
+        M.a62 = 0.0; M.a65 = 0.0; M.a66 = 1.0; M.a67 = 0.0; M.a68 = 0.0;
         const double ttf = ta * tfac;
-#pragma unroll
-        for (int i = 0; i < 5; ++i) b[i] = ttf;
-        b[5] = qa;
-        b[6] = qa;
-        b[7] = b[7] + ((X.fradu - X.pfluxu) * X.xu + (X.frads - X.pfluxs) * X.xs + (X.fradl - X.pfluxl) * X.xl);
+        M.b0 = ttf; M.b1 = ttf; M.b2 = ttf; M.b3 = ttf; M.b4 = ttf;
+        M.b5 = qa;
+        M.b6 = qa;
+        M.b7 = M.b7 + ((X.fradu - X.pfluxu) * X.xu + (X.frads - X.pfluxs) * X.xs + (X.fradl - X.pfluxl) * X.xl);
     }
 
     double v[9];
-    gauss9(A, b, v);
+    sys9_solve(M, v);
 #pragma unroll
     for (int i = 0; i < 9; ++i) W[i] = v[i];
     const double nu = v[0], ns = v[1], nl = v[2], n12 = v[3], n34 = v[4], nq12 = v[5], nq34 = v[6];

@@ -8,9 +8,33 @@
 
 #include "ibis_step.cuh"
 
+#ifndef IBIS_BLOCK
+#define IBIS_BLOCK 128
+#endif
+#ifndef IBIS_MIN_BLOCKS
+#define IBIS_MIN_BLOCKS 1
+#endif
+#ifndef IBIS_MIN_BLOCKS_SURF
+#define IBIS_MIN_BLOCKS_SURF 1
+#endif
+#ifndef IBIS_MIN_BLOCKS_GROUND
+#define IBIS_MIN_BLOCKS_GROUND 1
+#endif
+#ifndef IBIS_SMEM_STATE
+#define IBIS_SMEM_STATE 1
+#endif
+
 namespace ibis {
 
-constexpr int kBlock = 128;
+constexpr int kBlock = IBIS_BLOCK;
+
+// FP32 kernels keep each column's prognostic state in shared memory (array of
+// structures: the 71-word stride is odd, so a warp's accesses to one field fall
+// in 32 different banks); that frees registers for the step's temporaries.
+template <typename R>
+struct StateInSmem {
+    static constexpr bool value = IBIS_SMEM_STATE && sizeof(R) == 4;
+};
 
 template <typename R>
 __device__ __forceinline__ void load_col(Col<R>& c, const R* __restrict__ p, int ld) {
@@ -95,14 +119,19 @@ __device__ __forceinline__ Forc<R> load_forc(const R* __restrict__ f, int ld) {
 // Status word written by the kernels: [0] bit 0 = a column left the step with a
 // non-finite prognostic value; [1] = smallest such cell index (INT_MAX if none).
 template <typename R, int NT, bool SU, bool SL>
-__global__ void __launch_bounds__(kBlock) hourly_step_kernel(R* __restrict__ prog, const R* __restrict__ stat,
+__global__ void __launch_bounds__(kBlock, IBIS_MIN_BLOCKS) hourly_step_kernel(R* __restrict__ prog, const R* __restrict__ stat,
                                                              const R* __restrict__ forc, R* __restrict__ diag,
                                                              R* __restrict__ acc, int ncell, int ld, int nstep,
                                                              long long forc_stride, const DevParams<R> P,
                                                              int* __restrict__ status) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ncell) return;
-    Col<R> c;
+    extern __shared__ unsigned char smem_raw[];
+    Col<R> creg;
+    Col<R>* cp;
+    if constexpr (StateInSmem<R>::value) cp = reinterpret_cast<Col<R>*>(smem_raw) + threadIdx.x;
+    else cp = &creg;
+    Col<R>& c = *cp;
     load_col(c, prog + i, ld);
     Stat<R> S{stat + i, ld};
     Diag<R> D{diag ? diag + i : nullptr, ld};
@@ -112,6 +141,61 @@ __global__ void __launch_bounds__(kBlock) hourly_step_kernel(R* __restrict__ pro
         Forc<R> F = load_forc(forc + (size_t)s * forc_stride + i, ld);
         column_step<R, NT, SU, SL>(c, F, S, D, A, P);
     }
+    R sum = store_col(c, prog + i, ld);
+    if (status && !finite(sum)) {
+        atomicOr(status, 1);
+        atomicMin(status + 1, i);
+    }
+}
+
+// Two-kernel form of one hour: the surface phase writes the hand-off values to
+// `mid` (kMidCount planes), the ground phase reads them.  Both phases load the
+// column from `prog` and write back what they change.
+template <typename R, bool SU, bool SL>
+__global__ void __launch_bounds__(kBlock, IBIS_MIN_BLOCKS_SURF) surface_kernel(R* __restrict__ prog, const R* __restrict__ stat,
+                                                                    const R* __restrict__ forc, R* __restrict__ diag,
+                                                                    R* __restrict__ mid, int ncell, int ld,
+                                                                    const DevParams<R> P) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ncell) return;
+    extern __shared__ unsigned char smem_raw[];
+    Col<R> creg;
+    Col<R>* cp;
+    if constexpr (StateInSmem<R>::value) cp = reinterpret_cast<Col<R>*>(smem_raw) + threadIdx.x;
+    else cp = &creg;
+    Col<R>& c = *cp;
+    load_col(c, prog + i, ld);
+    Stat<R> S{stat + i, ld};
+    Diag<R> D{diag ? diag + i : nullptr, ld};
+    Forc<R> F = load_forc(forc + i, ld);
+    Mid<R> M;
+    surface_phase<R, SU, SL>(c, F, S, D, P, M);
+    mid_store(M, mid + i, ld);
+    store_col(c, prog + i, ld);
+}
+
+template <typename R, int NT>
+__global__ void __launch_bounds__(kBlock, IBIS_MIN_BLOCKS_GROUND) ground_kernel(R* __restrict__ prog, const R* __restrict__ stat,
+                                                                   const R* __restrict__ forc, R* __restrict__ diag,
+                                                                   R* __restrict__ acc, const R* __restrict__ mid,
+                                                                   int ncell, int ld, const DevParams<R> P,
+                                                                   int* __restrict__ status) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ncell) return;
+    extern __shared__ unsigned char smem_raw[];
+    Col<R> creg;
+    Col<R>* cp;
+    if constexpr (StateInSmem<R>::value) cp = reinterpret_cast<Col<R>*>(smem_raw) + threadIdx.x;
+    else cp = &creg;
+    Col<R>& c = *cp;
+    load_col(c, prog + i, ld);
+    Stat<R> S{stat + i, ld};
+    Diag<R> D{diag ? diag + i : nullptr, ld};
+    Acc<R> A{acc ? acc + i : nullptr, ld, (P.flags & IBIS_FLAG_KAHAN) != 0};
+    Forc<R> F = load_forc(forc + i, ld);
+    Mid<R> M;
+    mid_load(M, mid + i, ld);
+    ground_phase<R, NT>(c, F, S, D, A, P, M);
     R sum = store_col(c, prog + i, ld);
     if (status && !finite(sum)) {
         atomicOr(status, 1);
@@ -181,14 +265,28 @@ template <typename R, int NT, bool SU, bool SL>
 static cudaError_t launch_variant(R* prog, const R* stat, const R* forc, R* diag, R* acc, int ncell, int ld, int nstep,
                                   long long fstride, const DevParams<R>& P, int* status, cudaStream_t s) {
     const int grid = (ncell + kBlock - 1) / kBlock;
-    hourly_step_kernel<R, NT, SU, SL><<<grid, kBlock, 0, s>>>(prog, stat, forc, diag, acc, ncell, ld, nstep, fstride,
+    const size_t smem = StateInSmem<R>::value ? kBlock * sizeof(Col<R>) : 0;
+    hourly_step_kernel<R, NT, SU, SL><<<grid, kBlock, smem, s>>>(prog, stat, forc, diag, acc, ncell, ld, nstep, fstride,
                                                               P, status);
+    return cudaGetLastError();
+}
+
+template <typename R, int NT, bool SU, bool SL>
+static cudaError_t launch_split(R* prog, const R* stat, const R* forc, R* diag, R* acc, R* mid, int ncell, int ld,
+                                int nstep, long long fstride, const DevParams<R>& P, int* status, cudaStream_t s) {
+    const int grid = (ncell + kBlock - 1) / kBlock;
+    const size_t smem = StateInSmem<R>::value ? kBlock * sizeof(Col<R>) : 0;
+    for (int h = 0; h < nstep; ++h) {
+        const R* f = forc + (size_t)h * fstride;
+        surface_kernel<R, SU, SL><<<grid, kBlock, smem, s>>>(prog, stat, f, diag, mid, ncell, ld, P);
+        ground_kernel<R, NT><<<grid, kBlock, smem, s>>>(prog, stat, f, diag, acc, mid, ncell, ld, P, status);
+    }
     return cudaGetLastError();
 }
 
 template <typename R>
 static int hourly_step(R* prog, const R* stat, const R* forc, R* diag, R* acc, int ncell, int ld, int nstep,
-                       const IbisParams* hp, int* status, void* stream) {
+                       const IbisParams* hp, int* status, void* stream, R* mid = nullptr) {
     if (!prog || !stat || !forc || !hp) return -EINVAL;
     if (ncell < 0 || nstep < 0 || ld < ncell || (ld % 32) != 0) return -EINVAL;
     if (ncell == 0 || nstep == 0) return 0;
@@ -207,8 +305,9 @@ static int hourly_step(R* prog, const R* stat, const R* forc, R* diag, R* acc, i
     const bool su = hp->flags & IBIS_FLAG_SUNSHADE_U;
     const bool sl = hp->flags & IBIS_FLAG_SUNSHADE_L;
     cudaError_t e;
-#define IBIS_CASE(NT_, SU_, SL_) \
-    e = launch_variant<R, NT_, SU_, SL_>(prog, stat, forc, diag, acc, ncell, ld, nstep, fstride, P, status, s)
+#define IBIS_CASE(NT_, SU_, SL_)                                                                                \
+    e = mid ? launch_split<R, NT_, SU_, SL_>(prog, stat, forc, diag, acc, mid, ncell, ld, nstep, fstride, P, status, s) \
+            : launch_variant<R, NT_, SU_, SL_>(prog, stat, forc, diag, acc, ncell, ld, nstep, fstride, P, status, s)
     if (bed) {
         if (su) { if (sl) IBIS_CASE(9, true, true); else IBIS_CASE(9, true, false); }
         else { if (sl) IBIS_CASE(9, false, true); else IBIS_CASE(9, false, false); }

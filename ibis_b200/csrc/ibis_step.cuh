@@ -28,30 +28,61 @@ struct Acc {
     __device__ __forceinline__ R get(int plane) const { return base[(size_t)plane * ld]; }
 };
 
-template <typename R, int NT, bool SUN_U, bool SUN_L>
-__device__ __forceinline__ void column_step(Col<R>& c, const Forc<R>& F, const Stat<R>& S, const Diag<R>& D,
-                                            const Acc<R>& Ac, const DevParams<R>& P) {
-    const R eps = P.epsilon, dt = P.dtime;
-    const R fi = c.fi;
-    const R lai0 = S(IBIS_STAT_LAI, 0), lai1 = S(IBIS_STAT_LAI, 1);
-    const R sai0 = S(IBIS_STAT_SAI, 0), sai1 = S(IBIS_STAT_SAI, 1);
-    const R fu = S(IBIS_STAT_FU), fl = S(IBIS_STAT_FL);
+// Values the surface phase (steps 1-9 of timestep_body) hands to the ground
+// phase (steps 10-12 and the accumulators).  In the fused kernel they stay in
+// registers; the two-kernel form passes them through a scratch buffer of
+// IBIS_MID_COUNT planes.
+template <typename R>
+struct Mid {
+    R heatg, heati, fvapg, fvapi, fvaput, fvaplt, ginvap, gsuvap, gtrans;
+    R raing, traing, snowg, tsnowg, rainl, trainl, snowl, tsnowl;
+    R an_u[2], ag_u[2], an_l[3], ag_l[3];
+};
+constexpr int kMidCount = 27;
 
-    // ---- 1. setsoi (soil_physics.py:37-140)
-    R consoi[NL];
-    R q1, q2, q3, q4, hvasug, hvasui;
-    {
+template <typename R>
+__device__ __forceinline__ void mid_store(const Mid<R>& m, R* __restrict__ p, int ld) {
+    const R v[kMidCount] = {m.heatg, m.heati, m.fvapg, m.fvapi, m.fvaput, m.fvaplt, m.ginvap, m.gsuvap, m.gtrans,
+                            m.raing, m.traing, m.snowg, m.tsnowg, m.rainl, m.trainl, m.snowl, m.tsnowl,
+                            m.an_u[0], m.an_u[1], m.ag_u[0], m.ag_u[1], m.an_l[0], m.an_l[1], m.an_l[2],
+                            m.ag_l[0], m.ag_l[1], m.ag_l[2]};
 #pragma unroll
-        for (int k = 0; k < NL; ++k) {
-            R fs = R(0.01) * S(IBIS_STAT_SAND, k);
-            R fc = R(0.01) * S(IBIS_STAT_CLAY, k);
-            R fsilt = R(1.0) - fs - fc;
-            R por = S(IBIS_STAT_POROS, k);
-            R pliq = por * c.wsoi[k] * (R(1.0) - c.wisoi[k]);
-            R pice = por * c.wisoi[k];
-            R dry = fs * R(0.300) + fsilt * R(0.265) + fc * R(0.250);
-            consoi[k] = dry * pw(R(56.0), pliq) * pw(R(224.0), pice);
-        }
+    for (int q = 0; q < kMidCount; ++q) p[(size_t)q * ld] = v[q];
+}
+
+template <typename R>
+__device__ __forceinline__ void mid_load(Mid<R>& m, const R* __restrict__ p, int ld) {
+    R v[kMidCount];
+#pragma unroll
+    for (int q = 0; q < kMidCount; ++q) v[q] = p[(size_t)q * ld];
+    m.heatg = v[0]; m.heati = v[1]; m.fvapg = v[2]; m.fvapi = v[3]; m.fvaput = v[4]; m.fvaplt = v[5];
+    m.ginvap = v[6]; m.gsuvap = v[7]; m.gtrans = v[8];
+    m.raing = v[9]; m.traing = v[10]; m.snowg = v[11]; m.tsnowg = v[12];
+    m.rainl = v[13]; m.trainl = v[14]; m.snowl = v[15]; m.tsnowl = v[16];
+    m.an_u[0] = v[17]; m.an_u[1] = v[18]; m.ag_u[0] = v[19]; m.ag_u[1] = v[20];
+    m.an_l[0] = v[21]; m.an_l[1] = v[22]; m.an_l[2] = v[23];
+    m.ag_l[0] = v[24]; m.ag_l[1] = v[25]; m.ag_l[2] = v[26];
+}
+
+// setsoi (soil_physics.py:37-140): conductivity of layer k
+template <typename R>
+__device__ __forceinline__ R layer_conductivity(const Col<R>& c, const Stat<R>& S, int k) {
+    R fs = R(0.01) * S(IBIS_STAT_SAND, k);
+    R fc = R(0.01) * S(IBIS_STAT_CLAY, k);
+    R fsilt = R(1.0) - fs - fc;
+    R por = S(IBIS_STAT_POROS, k);
+    R pliq = por * c.wsoi[k] * (R(1.0) - c.wisoi[k]);
+    R pice = por * c.wisoi[k];
+    R dry = fs * R(0.300) + fsilt * R(0.265) + fc * R(0.250);
+    return dry * pw(R(56.0), pliq) * pw(R(224.0), pice);
+}
+
+// setsoi (soil_physics.py:37-140): evaporation source fractions and latent heats
+template <typename R>
+__device__ __forceinline__ void evap_sources(const Col<R>& c, const Forc<R>& F, const DevParams<R>& P, R& q1, R& q2,
+                                             R& q3, R& q4, R& hvasug, R& hvasui) {
+    const R eps = P.epsilon;
+    {
         R pud = c.wpud + c.wipud;
         R zwpud = clip(P.zwpmax * pud / mx(P.wpudmax, eps), R(0.0), P.zwpmax);
         R w0 = c.wsoi[0], i0 = c.wisoi[0];
@@ -69,6 +100,41 @@ __device__ __forceinline__ void column_step(Col<R>& c, const Forc<R>& F, const S
         hvasug = (q1 + q3) * zvap + (q2 + q4) * zsub;
         hvasui = P.hsub + P.cvap * (F.ta - P.tmelt) - P.cice * (c.tsno[0] - P.tmelt);
     }
+}
+
+// drystress (stomata.py:515-562)
+template <typename R>
+__device__ __forceinline__ void soil_stress(const Col<R>& c, const Stat<R>& S, const DevParams<R>& P,
+                                            R (&stressu)[NL], R (&stressl)[NL], R& stresstu, R& stresstl) {
+    stresstu = R(0.0);
+    stresstl = R(0.0);
+#pragma unroll
+    for (int k = 0; k < NL; ++k) {
+        R sw = S(IBIS_STAT_SWILT, k);
+        R awc = clip((c.wsoi[k] * (R(1.0) - c.wisoi[k]) - sw) / mx(S(IBIS_STAT_SFIELD, k) - sw, R(1e-10)), R(0.0), R(1.0));
+        R zw = clip((R(1.0) - ex(P.stressfac * awc)) / P.znorm, R(0.0), R(1.0));
+        stressl[k] = zw * P.froot[2 * k + 0];
+        stressu[k] = zw * P.froot[2 * k + 1];
+        stresstl = stresstl + stressl[k];
+        stresstu = stresstu + stressu[k];
+    }
+}
+
+// Steps 1-9 of timestep_body: soil diagnostics, radiation, interception, the
+// three canopy passes (turcof + stomata + turvap), evaporation of intercepted
+// water, the bare-story reset and the surface fluxes (loops.py:318-674).
+// Leaves tu/ts/tl/tg unclamped in `c` (the ground phase clamps them).
+template <typename R, bool SUN_U, bool SUN_L>
+__device__ __forceinline__ void surface_phase(Col<R>& c, const Forc<R>& F, const Stat<R>& S, const Diag<R>& D,
+                                              const DevParams<R>& P, Mid<R>& M) {
+    const R eps = P.epsilon;
+    const R fi = c.fi;
+    const R lai0 = S(IBIS_STAT_LAI, 0), lai1 = S(IBIS_STAT_LAI, 1);
+    const R sai0 = S(IBIS_STAT_SAI, 0), sai1 = S(IBIS_STAT_SAI, 1);
+    const R fu = S(IBIS_STAT_FU), fl = S(IBIS_STAT_FL);
+    R q1, q2, q3, q4, hvasug, hvasui;
+    evap_sources(c, F, P, q1, q2, q3, q4, hvasug, hvasui);
+    const R consoi0 = layer_conductivity(c, S, 0);
 
     // ---- 2-3. wet fractions and radiation (loops.py:331-354)
     Rad<R> Rd;
@@ -92,31 +158,24 @@ __device__ __forceinline__ void column_step(Col<R>& c, const Forc<R>& F, const S
     Aero<R> A;
     R u2, alogu, alogl;
     aero_geometry(A, u2, alogu, alogl, F, S, fi, P);
-    R stressu[NL], stressl[NL];
-    R stresstu = R(0.0), stresstl = R(0.0);
-#pragma unroll
-    for (int k = 0; k < NL; ++k) {
-        R sw = S(IBIS_STAT_SWILT, k);
-        R awc = clip((c.wsoi[k] * (R(1.0) - c.wisoi[k]) - sw) / mx(S(IBIS_STAT_SFIELD, k) - sw, R(1e-10)), R(0.0), R(1.0));
-        R zw = clip((R(1.0) - ex(P.stressfac * awc)) / P.znorm, R(0.0), R(1.0));
-        stressl[k] = zw * P.froot[2 * k + 0];
-        stressu[k] = zw * P.froot[2 * k + 1];
-        stresstl = stresstl + stressl[k];
-        stresstu = stresstu + stressu[k];
+    R stresstu, stresstl;
+    {
+        R su_[NL], sl_[NL];
+        soil_stress(c, S, P, su_, sl_, stresstu, stresstl);
     }
     TvFixed<R> X;
     const R csoi0 = S(IBIS_STAT_CSOI, 0) > R(0.0) ? S(IBIS_STAT_CSOI, 0) : P.csoi_mineral_val;
     const R rhosoi0 = S(IBIS_STAT_RHOSOI, 0) > R(0.0) ? S(IBIS_STAT_RHOSOI, 0) : P.rhosoi_val;
     R chgx, wlgx, wigx;
     {
-        X.xu = (double)(R(2.0) * lai1 * fu);
-        X.xs = (double)(R(2.0) * sai1 * fu);
-        X.xl = (double)(R(2.0) * (lai0 + sai0) * fl * (R(1.0) - fi));
+        X.xu = R(2.0) * lai1 * fu;
+        X.xs = R(2.0) * sai1 * fu;
+        X.xl = R(2.0) * (lai0 + sai0) * fl * (R(1.0) - fi);
         X.fi = (double)fi;
-        X.cog = (double)(consoi[0] / mx(R(0.5) * P.hsoi[0], eps));
-        X.coi = (double)(P.consno / mx(R(0.5) * mx(c.hsno[0], P.hsnotop), eps));
-        X.zirg = (double)(P.zir * cube(c.tg));
-        X.ziri = (double)(P.zir * cube(c.ti));
+        X.cog = consoi0 / mx(R(0.5) * P.hsoi[0], eps);
+        X.coi = P.consno / mx(R(0.5) * mx(c.hsno[0], P.hsnotop), eps);
+        X.zirg = P.zir * cube(c.tg);
+        X.ziri = P.zir * cube(c.ti);
         const R p0 = S(IBIS_STAT_POROS, 0), w0 = c.wsoi[0], i0 = c.wisoi[0];
         const R rwp = p0 * P.rhow;
         chgx = P.ch2o * c.wpud + P.cice * c.wipud
@@ -125,27 +184,25 @@ __device__ __forceinline__ void column_step(Col<R>& c, const Forc<R>& F, const S
         wigx = c.wipud + rwp * i0 * P.hsoi[0];
         X.wliqu = C.wliqu; X.wliqs = C.wliqs; X.wliql = C.wliql;
         X.wsnou = C.wsnou; X.wsnos = C.wsnos; X.wsnol = C.wsnol;
-        X.chux = (double)(P.chu + P.ch2o * C.wliqu + P.cice * C.wsnou);
-        X.chsx = (double)(P.chs + P.ch2o * C.wliqs + P.cice * C.wsnos);
-        X.chlx = (double)(P.chl + P.ch2o * C.wliql + P.cice * C.wsnol);
+        X.chux = P.chu + P.ch2o * C.wliqu + P.cice * C.wsnou;
+        X.chsx = P.chs + P.ch2o * C.wliqs + P.cice * C.wsnos;
+        X.chlx = P.chl + P.ch2o * C.wliql + P.cice * C.wsnol;
         X.rliqu = rliqu; X.rliqs = rliqs; X.rliql = rliql;
         X.fwetu = fwetu; X.fwets = fwets; X.fwetl = fwetl;
         X.hvasug = hvasug; X.hvasui = hvasui;
         X.tsoi0 = c.tsoi[0]; X.tsno0 = c.tsno[0];
         const R zwp = clip(R(0.5) * (c.wpud + c.wipud) / mx(P.wpudmax, eps), R(0.0), R(0.5));
         const R zws = (R(1.0) - i0) * w0 + i0;
-        X.zwtot = (double)(zwp + (R(1.0) - zwp) * zws);
+        X.zwtot = zwp + (R(1.0) - zwp) * zws;
         X.swilt0 = S(IBIS_STAT_SWILT, 0);
         X.suction0 = S(IBIS_STAT_SUCTION, 0);
         X.bex0 = S(IBIS_STAT_BEX, 0);
-        X.fradu = (double)(lai1 > eps ? (Rd.solu + Rd.firu) / (R(2.0) * lai1) : R(0.0));
-        X.frads = (double)(sai1 > eps ? (Rd.sols + Rd.firs) / (R(2.0) * sai1) : R(0.0));
-        X.fradl = (double)((lai0 + sai0) > eps ? (Rd.soll + Rd.firl) / (R(2.0) * (lai0 + sai0)) : R(0.0));
+        X.fradu = lai1 > eps ? (Rd.solu + Rd.firu) / (R(2.0) * lai1) : R(0.0);
+        X.frads = sai1 > eps ? (Rd.sols + Rd.firs) / (R(2.0) * sai1) : R(0.0);
+        X.fradl = (lai0 + sai0) > eps ? (Rd.soll + Rd.firl) / (R(2.0) * (lai0 + sai0)) : R(0.0);
         X.pfluxu = C.pfluxu; X.pfluxs = C.pfluxs; X.pfluxl = C.pfluxl;
         X.solg = Rd.solg; X.soli = Rd.soli; X.firg = Rd.firg; X.firi = Rd.firi; X.firb = Rd.firb;
-        X.lai1 = lai1; X.lai0 = lai0; X.lsl0 = (double)(lai0 + sai0); X.fu = fu; X.fl = fl;
-#pragma unroll
-        for (int j = 0; j < 12; ++j) X.frac[j] = (double)S(IBIS_STAT_FRAC, j);
+        X.lai1 = lai1; X.lai0 = lai0; X.lsl0 = lai0 + sai0; X.fu = fu; X.fl = fl;
     }
     const double old[5] = {(double)c.tu, (double)c.ts, (double)c.tl, (double)c.tg, (double)c.ti};
     double Wv[9] = {(double)c.tu, (double)c.ts, (double)c.tl, (double)c.t12, (double)c.t34,
@@ -169,11 +226,11 @@ __device__ __forceinline__ void column_step(Col<R>& c, const Forc<R>& F, const S
         R wl = weight_veg(tl, (R)X.chlx, C.wliql, C.wsnol, wprev[2], first, P);
         R wg = weight_veg(tg, chgx, wlgx, wigx, wprev[3], first, P);
         R wi = weight_snow(ti, c.ti, wprev[4], first, P);
-        turvap(Wv, tv, old, T, (double)A.cp, (double)P.tfac, wu, ws, wl, wg, wi, X, st, ta64, qa64, ps64, P);
+        turvap(Wv, tv, old, T, (double)A.cp, (double)P.tfac, wu, ws, wl, wg, wi, X, st, ta64, qa64, ps64, S, P);
         wprev[0] = wu; wprev[1] = ws; wprev[2] = wl; wprev[3] = wg; wprev[4] = wi;
     }
-    R ti_new = mn((R)Wv[8], P.tmelt);
-    R tg_w = (R)Wv[7];
+    const R ti_new = mn((R)Wv[8], P.tmelt);
+    const R tg_w = (R)Wv[7];
 
     // ---- 7-8. evaporation of intercepted water, bare-story reset (loops.py:616-640)
     R tu = (R)Wv[0], ts = (R)Wv[1], tl = (R)Wv[2];
@@ -190,20 +247,89 @@ __device__ __forceinline__ void column_step(Col<R>& c, const Forc<R>& F, const S
 
     // ---- 9. surface fluxes into soil and snow (loops.py:665-674)
     const R fm = P.flux_max;
-    const R fvapg = (R)tv.fvapg, fvapi = (R)tv.fvapi;
-    R heatg = Rd.solg + clip((R)tv.firg, -fm, fm) - clip((R)tv.fseng, -fm, fm) - hvasug * fvapg;
-    R heati = Rd.soli + clip((R)tv.firi, -fm, fm) - clip((R)tv.fseni, -fm, fm) - hvasui * fvapi;
+    M.fvapg = (R)tv.fvapg;
+    M.fvapi = (R)tv.fvapi;
+    M.heatg = Rd.solg + clip((R)tv.firg, -fm, fm) - clip((R)tv.fseng, -fm, fm) - hvasug * M.fvapg;
+    M.heati = Rd.soli + clip((R)tv.firi, -fm, fm) - clip((R)tv.fseni, -fm, fm) - hvasui * M.fvapi;
+    M.fvaput = (R)tv.fvaput;
+    M.fvaplt = (R)tv.fvaplt;
+    M.ginvap = (R)tv.ginvap;
+    M.gsuvap = (R)tv.gsuvap;
+    M.gtrans = (R)tv.gtrans;
+    M.raing = C.raing; M.traing = C.traing; M.snowg = C.snowg; M.tsnowg = C.tsnowg;
+    M.rainl = C.rainl; M.trainl = C.trainl; M.snowl = C.snowl; M.tsnowl = C.tsnowl;
+#pragma unroll
+    for (int j = 0; j < 2; ++j) { M.an_u[j] = st.an_u[j]; M.ag_u[j] = st.ag_u[j]; }
+#pragma unroll
+    for (int j = 0; j < 3; ++j) { M.an_l[j] = st.an_l[j]; M.ag_l[j] = st.ag_l[j]; }
+
+    // canopy state left for the ground phase (tu/ts/tl/tg unclamped)
+    c.tu = tu; c.ts = ts; c.tl = tl; c.tg = tg_w; c.ti = ti_new;
+    c.t12 = (R)Wv[3]; c.t34 = (R)Wv[4]; c.q12 = (R)Wv[5]; c.q34 = (R)Wv[6];
+    c.wliqu = wliqu; c.wliqs = wliqs; c.wliql = wliql;
+    c.wsnou = wsnou; c.wsnos = wsnos; c.wsnol = wsnol;
+
+    // ---- diagnostics of the surface phase (loops.py:1158-1241)
+    if (D.base) {
+#pragma unroll
+        for (int j = 0; j < 2; ++j) { D.put(IBIS_DIAG_AN_UPPER, j, st.an_u[j]); D.put(IBIS_DIAG_AG_UPPER, j, st.ag_u[j]); }
+#pragma unroll
+        for (int j = 0; j < 3; ++j) { D.put(IBIS_DIAG_AN_LOWER, j, st.an_l[j]); D.put(IBIS_DIAG_AG_LOWER, j, st.ag_l[j]); }
+        D.put(IBIS_DIAG_FWETU, fwetu); D.put(IBIS_DIAG_FWETS, fwets); D.put(IBIS_DIAG_FWETL, fwetl);
+        D.put(IBIS_DIAG_RLIQU, rliqu); D.put(IBIS_DIAG_RLIQS, rliqs); D.put(IBIS_DIAG_RLIQL, rliql);
+        D.put(IBIS_DIAG_SOLU, Rd.solu); D.put(IBIS_DIAG_SOLS, Rd.sols); D.put(IBIS_DIAG_SOLL, Rd.soll);
+        D.put(IBIS_DIAG_SOLG, Rd.solg); D.put(IBIS_DIAG_SOLI, Rd.soli);
+        D.put(IBIS_DIAG_FIRU, Rd.firu); D.put(IBIS_DIAG_FIRS, Rd.firs); D.put(IBIS_DIAG_FIRL, Rd.firl);
+        D.put(IBIS_DIAG_FIRG, (R)tv.firg); D.put(IBIS_DIAG_FIRI, (R)tv.firi); D.put(IBIS_DIAG_FIRB, (R)tv.firb);
+#pragma unroll
+        for (int b = 0; b < 2; ++b) { D.put(IBIS_DIAG_ASURD, b, Rd.asurd[b]); D.put(IBIS_DIAG_ASURI, b, Rd.asuri[b]); }
+        D.put(IBIS_DIAG_TOPPARU, Rd.topparu); D.put(IBIS_DIAG_TOPPARL, Rd.topparl);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) { D.put(IBIS_DIAG_SCALCOEFU, j, Rd.scu[j]); D.put(IBIS_DIAG_SCALCOEFL, j, Rd.scl[j]); }
+        D.put(IBIS_DIAG_FSENU, (R)tv.fsenu); D.put(IBIS_DIAG_FSENS, (R)tv.fsens); D.put(IBIS_DIAG_FSENL, (R)tv.fsenl);
+        D.put(IBIS_DIAG_FSENG, (R)tv.fseng); D.put(IBIS_DIAG_FSENI, (R)tv.fseni);
+        D.put(IBIS_DIAG_FVAPG, M.fvapg); D.put(IBIS_DIAG_FVAPI, M.fvapi);
+        D.put(IBIS_DIAG_RAING, C.raing); D.put(IBIS_DIAG_SNOWG, C.snowg); D.put(IBIS_DIAG_RHOA, A.rhoa);
+        D.put(IBIS_DIAG_HVASUG, hvasug); D.put(IBIS_DIAG_HVASUI, hvasui);
+        D.put(IBIS_DIAG_QGLIF, 0, q1); D.put(IBIS_DIAG_QGLIF, 1, q2); D.put(IBIS_DIAG_QGLIF, 2, q3); D.put(IBIS_DIAG_QGLIF, 3, q4);
+        D.put(IBIS_DIAG_HEATI, M.heati);
+        D.put(IBIS_DIAG_GINVAP, M.ginvap); D.put(IBIS_DIAG_GSUVAP, M.gsuvap); D.put(IBIS_DIAG_GTRANS, M.gtrans);
+        D.put(IBIS_DIAG_RAINL, C.rainl); D.put(IBIS_DIAG_SNOWL, C.snowl);
+        D.put(IBIS_DIAG_TRAINL, C.trainl); D.put(IBIS_DIAG_TSNOWL, C.tsnowl);
+    }
+}
+
+// Steps 10-12 of timestep_body -- snow, soil water and heat (+ bedrock),
+// freeze/thaw, the surface-temperature bound -- then the fire counters and the
+// day-loop accumulators (loops.py:676-1275; loops_gswp3.py:161-318).
+template <typename R, int NT>
+__device__ __forceinline__ void ground_phase(Col<R>& c, const Forc<R>& F, const Stat<R>& S, const Diag<R>& D,
+                                             const Acc<R>& Ac, const DevParams<R>& P, const Mid<R>& M) {
+    const R eps = P.epsilon, dt = P.dtime;
+    const R fi = c.fi;
+    const R lai0 = S(IBIS_STAT_LAI, 0), lai1 = S(IBIS_STAT_LAI, 1);
+    const R sai0 = S(IBIS_STAT_SAI, 0);
+    const R fu = S(IBIS_STAT_FU), fl = S(IBIS_STAT_FL);
+    const R tu = c.tu, tl = c.tl;
+    R wliql = c.wliql, wsnol = c.wsnol;
+    R consoi[NL];
+#pragma unroll
+    for (int k = 0; k < NL; ++k) consoi[k] = layer_conductivity(c, S, k);
+    R q1, q2, q3, q4, hvasug_, hvasui_;
+    evap_sources(c, F, P, q1, q2, q3, q4, hvasug_, hvasui_);
+    R stressu[NL], stressl[NL], stresstu, stresstl;
+    soil_stress(c, S, P, stressu, stressl, stresstu, stresstl);
 
     // ---- 10. snow (loops.py:676-848)
     R smelt, zheat, sflo_bot, fhtop_snow;
     {
-        fhtop_snow = heati + C.rainl * (P.ch2o * (C.trainl - P.tmelt) + P.hfus + P.cice * (P.tmelt - c.tsno[0]))
-                   + C.snowl * P.cice * (C.tsnowl - c.tsno[0]);
+        fhtop_snow = M.heati + M.rainl * (P.ch2o * (M.trainl - P.tmelt) + P.hfus + P.cice * (P.tmelt - c.tsno[0]))
+                   + M.snowl * P.cice * (M.tsnowl - c.tsno[0]);
         const R xlb = fl * R(2.0) * (lai0 + sai0);
         R hp[NS];
 #pragma unroll
         for (int k = 0; k < NS; ++k) hp[k] = c.hsno[k];
-        if (fi > R(0.0)) hp[0] = c.hsno[0] + (C.rainl + C.snowl - fvapi) * (P.dtime / P.rhos);
+        if (fi > R(0.0)) hp[0] = c.hsno[0] + (M.rainl + M.snowl - M.fvapi) * (P.dtime / P.rhos);
         R tsh[NS];
 #pragma unroll
         for (int k = 0; k < NS; ++k) tsh[k] = c.tsno[k];
@@ -213,14 +339,14 @@ __device__ __forceinline__ void column_step(Col<R>& c, const Forc<R>& F, const S
 #pragma unroll
         for (int k = 0; k < NS; ++k) ht = ht + hp[k];
         R hts = ht > R(0.0) ? ht : P.hsnomin;
-        R dfi = (R(1.0) - fi) * P.dtime * C.snowg / (P.rhos * hts);
+        R dfi = (R(1.0) - fi) * P.dtime * M.snowg / (P.rhos * hts);
         dfi = mn(dfi, R(1.0) - fi);
         R fi1 = fi + dfi;
         R tm[NS], hm[NS];
         const bool fresh = (fi < eps) && (dfi > R(0.0));
 #pragma unroll
         for (int k = 0; k < NS; ++k) {
-            tm[k] = fi1 > R(0.0) ? (tsh[k] * fi + C.tsnowg * dfi) / mx(fi1, eps) : tsh[k];
+            tm[k] = fi1 > R(0.0) ? (tsh[k] * fi + M.tsnowg * dfi) / mx(fi1, eps) : tsh[k];
             R hinit = k == 0 ? P.hsnotop : (P.hsnomin - P.hsnotop) / R(NS - 1);
             hm[k] = fresh ? hinit : hp[k];
         }
@@ -283,15 +409,17 @@ __device__ __forceinline__ void column_step(Col<R>& c, const Forc<R>& F, const S
 #pragma unroll
         for (int k = 0; k < NS; ++k) { c.hsno[k] = hm[k]; c.tsno[k] = tm[k]; }
         c.tlsub = tlsub;
+        c.wliql = wliql;
+        c.wsnol = wsnol;
     }
-    const R heatg_avg = (R(1.0) - fi) * heatg + fi * sflo_bot + zheat * P.rdt;
-    const R fvapg_avg = clip((R(1.0) - fi) * fvapg, R(-1.0e-3), R(1.0e-3));
-    const R raing_nf = (R(1.0) - fi) * C.raing;
+    const R heatg_avg = (R(1.0) - fi) * M.heatg + fi * sflo_bot + zheat * P.rdt;
+    const R fvapg_avg = clip((R(1.0) - fi) * M.fvapg, R(-1.0e-3), R(1.0e-3));
+    const R raing_nf = (R(1.0) - fi) * M.raing;
     const R smr = smelt * P.rdt;
     const R rsum = raing_nf + smr;
     const bool rzero = rsum < eps;
     const R raing_avg = rzero ? R(0.0) : rsum;
-    const R traing_avg = rzero ? R(0.0) : (raing_nf * C.traing + smr * P.tmelt) / mx(rsum, eps);
+    const R traing_avg = rzero ? R(0.0) : (raing_nf * M.traing + smr * P.tmelt) / mx(rsum, eps);
 
     // ---- 11. soil (loops.py:896-1125)
     R poros[NL], csoi[NL], rhosoi[NL];
@@ -329,8 +457,8 @@ __device__ __forceinline__ void column_step(Col<R>& c, const Forc<R>& F, const S
     if (evap) { wsw[0] = w0a; wisw[0] = i0n; }
 #pragma unroll
     for (int k = 0; k < NL; ++k) pflo[k] = mx(poros[k] * mx(R(1.0) - wisw[k], eps), eps);
-    const R gtransu = (R)tv.fvaput * R(2.0) * lai1 * fu;
-    const R gtransl = (R)tv.fvaplt * R(2.0) * lai0 * fl * (R(1.0) - fi);
+    const R gtransu = M.fvaput * R(2.0) * lai1 * fu;
+    const R gtransl = M.fvaplt * R(2.0) * lai0 * fl * (R(1.0) - fi);
     const R sstu = mx(stresstu, eps), sstl = mx(stresstl, eps);
     R tpt[NT];
 #pragma unroll
@@ -385,37 +513,14 @@ __device__ __forceinline__ void column_step(Col<R>& c, const Forc<R>& F, const S
 
     // ---- 12. surface temperature bound (loops.py:1143-1151)
     const R lo_ = F.ta - P.t_max_dev, hi_ = F.ta + P.t_max_dev;
-    c.tu = clip(tu, lo_, hi_);
-    c.ts = clip(ts, lo_, hi_);
-    c.tl = clip(tl, lo_, hi_);
-    c.tg = clip(tg_w, lo_, hi_);
-    c.ti = ti_new;
-    c.t12 = (R)Wv[3]; c.t34 = (R)Wv[4]; c.q12 = (R)Wv[5]; c.q34 = (R)Wv[6];
-    c.wliqu = wliqu; c.wliqs = wliqs; c.wliql = wliql;
-    c.wsnou = wsnou; c.wsnos = wsnos; c.wsnol = wsnol;
+    c.tu = clip(c.tu, lo_, hi_);
+    c.ts = clip(c.ts, lo_, hi_);
+    c.tl = clip(c.tl, lo_, hi_);
+    c.tg = clip(c.tg, lo_, hi_);
     fire_counters(c, S(IBIS_STAT_SWILT, 0), F, P);
 
-    // ---- diagnostics (loops.py:1158-1241)
+    // ---- diagnostics of the ground phase (loops.py:1158-1241)
     if (D.base) {
-#pragma unroll
-        for (int j = 0; j < 2; ++j) { D.put(IBIS_DIAG_AN_UPPER, j, st.an_u[j]); D.put(IBIS_DIAG_AG_UPPER, j, st.ag_u[j]); }
-#pragma unroll
-        for (int j = 0; j < 3; ++j) { D.put(IBIS_DIAG_AN_LOWER, j, st.an_l[j]); D.put(IBIS_DIAG_AG_LOWER, j, st.ag_l[j]); }
-        D.put(IBIS_DIAG_FWETU, fwetu); D.put(IBIS_DIAG_FWETS, fwets); D.put(IBIS_DIAG_FWETL, fwetl);
-        D.put(IBIS_DIAG_RLIQU, rliqu); D.put(IBIS_DIAG_RLIQS, rliqs); D.put(IBIS_DIAG_RLIQL, rliql);
-        D.put(IBIS_DIAG_SOLU, Rd.solu); D.put(IBIS_DIAG_SOLS, Rd.sols); D.put(IBIS_DIAG_SOLL, Rd.soll);
-        D.put(IBIS_DIAG_SOLG, Rd.solg); D.put(IBIS_DIAG_SOLI, Rd.soli);
-        D.put(IBIS_DIAG_FIRU, Rd.firu); D.put(IBIS_DIAG_FIRS, Rd.firs); D.put(IBIS_DIAG_FIRL, Rd.firl);
-        D.put(IBIS_DIAG_FIRG, (R)tv.firg); D.put(IBIS_DIAG_FIRI, (R)tv.firi); D.put(IBIS_DIAG_FIRB, (R)tv.firb);
-#pragma unroll
-        for (int b = 0; b < 2; ++b) { D.put(IBIS_DIAG_ASURD, b, Rd.asurd[b]); D.put(IBIS_DIAG_ASURI, b, Rd.asuri[b]); }
-        D.put(IBIS_DIAG_TOPPARU, Rd.topparu); D.put(IBIS_DIAG_TOPPARL, Rd.topparl);
-#pragma unroll
-        for (int j = 0; j < 4; ++j) { D.put(IBIS_DIAG_SCALCOEFU, j, Rd.scu[j]); D.put(IBIS_DIAG_SCALCOEFL, j, Rd.scl[j]); }
-        D.put(IBIS_DIAG_FSENU, (R)tv.fsenu); D.put(IBIS_DIAG_FSENS, (R)tv.fsens); D.put(IBIS_DIAG_FSENL, (R)tv.fsenl);
-        D.put(IBIS_DIAG_FSENG, (R)tv.fseng); D.put(IBIS_DIAG_FSENI, (R)tv.fseni);
-        D.put(IBIS_DIAG_FVAPG, fvapg); D.put(IBIS_DIAG_FVAPI, fvapi);
-        D.put(IBIS_DIAG_RAING, C.raing); D.put(IBIS_DIAG_SNOWG, C.snowg); D.put(IBIS_DIAG_RHOA, A.rhoa);
 #pragma unroll
         for (int k = 0; k < NL; ++k) {
             D.put(IBIS_DIAG_CONSOI, k, consoi[k]);
@@ -425,17 +530,12 @@ __device__ __forceinline__ void column_step(Col<R>& c, const Forc<R>& F, const S
         }
 #pragma unroll
         for (int k = 0; k <= NL; ++k) D.put(IBIS_DIAG_HFLO, k, hflo[k]);
-        D.put(IBIS_DIAG_HEATG, heatg_avg); D.put(IBIS_DIAG_HVASUG, hvasug);
-        D.put(IBIS_DIAG_QGLIF, 0, q1); D.put(IBIS_DIAG_QGLIF, 1, q2); D.put(IBIS_DIAG_QGLIF, 2, q3); D.put(IBIS_DIAG_QGLIF, 3, q4);
+        D.put(IBIS_DIAG_HEATG, heatg_avg);
         D.put(IBIS_DIAG_STRESSTU, stresstu); D.put(IBIS_DIAG_STRESSTL, stresstl);
-        D.put(IBIS_DIAG_HEATI, heati); D.put(IBIS_DIAG_HVASUI, hvasui);
-        D.put(IBIS_DIAG_GINVAP, (R)tv.ginvap); D.put(IBIS_DIAG_GSUVAP, (R)tv.gsuvap); D.put(IBIS_DIAG_GTRANS, (R)tv.gtrans);
         D.put(IBIS_DIAG_GTRANSU, gtransu); D.put(IBIS_DIAG_GTRANSL, gtransl); D.put(IBIS_DIAG_GRUNOF, grunof);
         D.put(IBIS_DIAG_GDRAIN, wflo[NL]); D.put(IBIS_DIAG_GADJUST, gadj); D.put(IBIS_DIAG_WTOT, R(0.0));
         D.put(IBIS_DIAG_RAING_AVG, raing_avg); D.put(IBIS_DIAG_TRAING_AVG, traing_avg);
         D.put(IBIS_DIAG_FHTOP_SOIL, fhtop_soil);
-        D.put(IBIS_DIAG_RAINL, C.rainl); D.put(IBIS_DIAG_SNOWL, C.snowl);
-        D.put(IBIS_DIAG_TRAINL, C.trainl); D.put(IBIS_DIAG_TSNOWL, C.tsnowl);
         D.put(IBIS_DIAG_SFLO_BOT, sflo_bot); D.put(IBIS_DIAG_FHTOP_SNOW, fhtop_snow);
     }
 
@@ -457,10 +557,10 @@ __device__ __forceinline__ void column_step(Col<R>& c, const Forc<R>& F, const S
                 bool wood = true;
                 if (j < 8) {
                     const bool con = (j == 3 || j == 5 || j == 7);
-                    an = con ? st.an_u[1] : st.an_u[0];
+                    an = con ? M.an_u[1] : M.an_u[0];
                     lai_ = lai1; cov = fu; sp = sap;
                 } else {
-                    an = j < 10 ? st.an_l[0] : (j == 10 ? st.an_l[2] : st.an_l[1]);
+                    an = j < 10 ? M.an_l[0] : (j == 10 ? M.an_l[2] : M.an_l[1]);
                     lai_ = lai0; cov = fl * smask; sp = R(1.0);
                     wood = j < 10;
                 }
@@ -484,16 +584,16 @@ __device__ __forceinline__ void column_step(Col<R>& c, const Forc<R>& F, const S
             R fb = S(IBIS_STAT_FRAC, 0) + S(IBIS_STAT_FRAC, 1) + S(IBIS_STAT_FRAC, 2) + S(IBIS_STAT_FRAC, 4)
                  + S(IBIS_STAT_FRAC, 6);
             R fcn = S(IBIS_STAT_FRAC, 3) + S(IBIS_STAT_FRAC, 5) + S(IBIS_STAT_FRAC, 7);
-            R gu = (st.ag_u[0] * fb + st.ag_u[1] * fcn) * lai1 * fu;
-            R gl = (st.ag_l[0] * (S(IBIS_STAT_FRAC, 8) + S(IBIS_STAT_FRAC, 9)) + st.ag_l[2] * S(IBIS_STAT_FRAC, 10)
-                    + st.ag_l[1] * S(IBIS_STAT_FRAC, 11)) * lai0 * fl * smask;
+            R gu = (M.ag_u[0] * fb + M.ag_u[1] * fcn) * lai1 * fu;
+            R gl = (M.ag_l[0] * (S(IBIS_STAT_FRAC, 8) + S(IBIS_STAT_FRAC, 9)) + M.ag_l[2] * S(IBIS_STAT_FRAC, 10)
+                    + M.ag_l[1] * S(IBIS_STAT_FRAC, 11)) * lai0 * fl * smask;
             Ac.add(IBIS_ACC_ADRAIN, F.rain * dt);
             Ac.add(IBIS_ACC_ADSNOW, F.snow * dt);
-            Ac.add(IBIS_ACC_ADAET, ((R)tv.ginvap + (R)tv.gsuvap + (R)tv.gtrans) * dt);
-            Ac.add(IBIS_ACC_A10ANCUB, st.an_u[0] * dt);
-            Ac.add(IBIS_ACC_A10ANCLS, st.an_l[0] * dt);
-            Ac.add(IBIS_ACC_A10ANCL3, st.an_l[1] * dt);
-            Ac.add(IBIS_ACC_A10ANCL4, st.an_l[2] * dt);
+            Ac.add(IBIS_ACC_ADAET, (M.ginvap + M.gsuvap + M.gtrans) * dt);
+            Ac.add(IBIS_ACC_A10ANCUB, M.an_u[0] * dt);
+            Ac.add(IBIS_ACC_A10ANCLS, M.an_l[0] * dt);
+            Ac.add(IBIS_ACC_A10ANCL3, M.an_l[1] * dt);
+            Ac.add(IBIS_ACC_A10ANCL4, M.an_l[2] * dt);
             Ac.add(IBIS_ACC_AYNPPTOT, npp);
             Ac.add(IBIS_ACC_AYGPPTOT, (gu + gl) * cf);
             Ac.add(IBIS_ACC_AYTRUNOF, grunof * dt);
@@ -514,6 +614,15 @@ __device__ __forceinline__ void column_step(Col<R>& c, const Forc<R>& F, const S
             Ac.add(IBIS_ACC_TG_MEAN, c.tg * P.ch4_w);
         }
     }
+}
+
+// One full hourly step of a column in one kernel.
+template <typename R, int NT, bool SUN_U, bool SUN_L>
+__device__ __forceinline__ void column_step(Col<R>& c, const Forc<R>& F, const Stat<R>& S, const Diag<R>& D,
+                                            const Acc<R>& Ac, const DevParams<R>& P) {
+    Mid<R> M;
+    surface_phase<R, SUN_U, SUN_L>(c, F, S, D, P, M);
+    ground_phase<R, NT>(c, F, S, D, Ac, P, M);
 }
 
 }  // namespace ibis

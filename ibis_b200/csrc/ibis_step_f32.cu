@@ -7,3 +7,12 @@ extern "C" int ibis_step_f32(float* prog, const float* stat, const float* forc, 
                              int ld, int nstep, const IbisParams* params, int* status, void* stream) {
     return ibis::hourly_step<float>(prog, stat, forc, diag, acc, ncell, ld, nstep, params, status, stream);
 }
+
+extern "C" int ibis_step_split_f32(float* prog, const float* stat, const float* forc, float* diag, float* acc,
+                                   float* scratch, int ncell, int ld, int nstep, const IbisParams* params,
+                                   int* status, void* stream) {
+    if (!scratch) return -EINVAL;
+    return ibis::hourly_step<float>(prog, stat, forc, diag, acc, ncell, ld, nstep, params, status, stream, scratch);
+}
+
+extern "C" int ibis_mid_planes(void) { return ibis::kMidCount; }

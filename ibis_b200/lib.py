@@ -23,6 +23,9 @@ _P = ctypes.POINTER(IbisParamsC)
 SIGNATURES = {
     "ibis_step_f32": (ctypes.c_int, [ctypes.c_void_p] * 5 + [ctypes.c_int] * 3 + [_P, ctypes.c_void_p, ctypes.c_void_p]),
     "ibis_step_f64": (ctypes.c_int, [ctypes.c_void_p] * 5 + [ctypes.c_int] * 3 + [_P, ctypes.c_void_p, ctypes.c_void_p]),
+    "ibis_step_split_f32": (ctypes.c_int, [ctypes.c_void_p] * 6 + [ctypes.c_int] * 3
+                            + [_P, ctypes.c_void_p, ctypes.c_void_p]),
+    "ibis_mid_planes": (ctypes.c_int, []),
 }
 
 _lib = None

@@ -39,6 +39,19 @@ extern "C" {
 int ibis_step_f32(float* prog, const float* stat, const float* forc, float* diag, float* acc, int ncell, int ld,
                   int nstep, const IbisParams* params, int* status, void* stream);
 
+/* Same contract as ibis_step_f32, run as two kernels per hour: a surface
+ * phase (radiation, interception, canopy solve) and a ground phase (snow,
+ * soil, accumulators) that hand ibis_mid_planes() values per cell to each
+ * other through `scratch` [ibis_mid_planes()][ld] (device, caller-owned).
+ * Each kernel needs fewer registers than the fused one; which form is faster
+ * depends on the batch (see ibis_b200/tune.py).
+ * Replaces: timestep_body (loops.py:234) iterated by _step_body (loops_gswp3.py:115). */
+int ibis_step_split_f32(float* prog, const float* stat, const float* forc, float* diag, float* acc, float* scratch,
+                        int ncell, int ld, int nstep, const IbisParams* params, int* status, void* stream);
+
+/* Number of scratch planes ibis_step_split_f32 needs. */
+int ibis_mid_planes(void);
+
 /* Same contract in float64 throughout (the float64 run of the reference's step). */
 int ibis_step_f64(double* prog, const double* stat, const double* forc, double* diag, double* acc, int ncell,
                   int ld, int nstep, const IbisParams* params, int* status, void* stream);

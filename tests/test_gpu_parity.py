@@ -82,3 +82,19 @@ def test_f32_kernel_close_to_oracle(cuda_lib, name):
         np.testing.assert_allclose(got[k], prog[k], rtol=2e-3, atol=0.5, err_msg=k)
     for k in ("wsoi", "wisoi", "fi"):
         np.testing.assert_allclose(got[k], prog[k], rtol=2e-3, atol=2e-3, err_msg=k)
+
+
+@pytest.mark.parametrize("name", ["day_mixed", "sunshade"])
+def test_split_form_matches_fused_form(cuda_lib, name):
+    """The two-kernel form runs the same phases; FP32 results agree to rounding."""
+    c = Case(name)
+    out = {}
+    for mode in ("fused", "split"):
+        cols = Columns.from_host(c.prog, c.stat, dtype=torch.float32, diag=True, acc=True, mode=mode)
+        cols.run(cols.forcing(c.forc), c.params)
+        torch.cuda.synchronize()
+        out[mode] = (cols.prog_host(), cols.acc_host())
+    for k in ("tsoi", "tg", "tu", "tl", "tsno", "ti"):
+        np.testing.assert_allclose(out["split"][0][k], out["fused"][0][k], rtol=1e-4, atol=0.05, err_msg=k)
+    for k in ("wsoi", "wisoi", "fi"):
+        np.testing.assert_allclose(out["split"][0][k], out["fused"][0][k], rtol=1e-3, atol=1e-4, err_msg=k)
