@@ -21,14 +21,19 @@ LIB = os.path.join(OUT_DIR, "libibis_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", os.path.join(REPO, "include")]
 
+# FP32 kernels: fast single-precision math (MUFU exp/log/pow, approximate
+# division and square root, denormals flushed) and FP32 saturation terms inside
+# the FP64 canopy solve.  Their error against the float64 kernels is measured by
+# tests/test_gpu_precision.py.
+F32_FLAGS = ["-use_fast_math", "-DIBIS_FAST_SAT=1"]
+
 # translation unit -> extra flags
 UNITS = {
-    # FP32 kernels: fast single-precision math (MUFU exp/log/pow, approximate
-    # division and square root, denormals flushed), FP32 saturation terms inside
-    # the FP64 canopy solve, and per-kernel occupancy targets.  Their error
-    # against the float64 kernels is measured by tests/test_gpu_precision.py.
-    "ibis_step_f32.cu": ["-use_fast_math", "-DIBIS_FAST_SAT=1", "-DIBIS_MIN_BLOCKS=2",
-                         "-DIBIS_MIN_BLOCKS_SURF=2", "-DIBIS_MIN_BLOCKS_GROUND=3"],
+    "ibis_step_f32.cu": F32_FLAGS,
+    "ibis_f32_inst_a.cu": F32_FLAGS,
+    "ibis_f32_inst_b.cu": F32_FLAGS,
+    "ibis_f32_inst_c.cu": F32_FLAGS,
+    "ibis_f32_inst_d.cu": F32_FLAGS,
     "ibis_step_f64.cu": ["--fmad=false"],
     "ibis_batch.cu": [],
 }

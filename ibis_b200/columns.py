@@ -51,21 +51,32 @@ class Columns:
         self._np_dtype = np.float32 if dtype == torch.float32 else np.float64
         lib = _lib.load()
         self._fn = lib.ibis_step_f32 if dtype == torch.float32 else lib.ibis_step_f64
-        self._split = lib.ibis_step_split_f32
+        self._cfg_fn = lib.ibis_step_config_f32
         self.scratch = None
+        self.config = None
         self.set_mode(mode)
 
     def set_mode(self, mode: str):
-        """``fused`` (one kernel per launch) or ``split`` (surface + ground kernels per hour)."""
-        if mode not in ("fused", "split"):
-            raise ValueError("mode must be 'fused' or 'split'")
-        if mode == "split":
-            if self.dtype != torch.float32:
-                raise ValueError("the split form is FP32 only")
-            if self.scratch is None:
-                self.scratch = torch.zeros((_lib.load().ibis_mid_planes(), self.ld), dtype=self.dtype,
-                                           device=self.device)
-        self.mode = mode
+        """``fused`` (one kernel per launch), ``split`` (surface + ground kernels per hour),
+        or an integer launch configuration (see ``lib.configs()``)."""
+        if isinstance(mode, (int, np.integer)) and not isinstance(mode, bool):
+            cfgs = _lib.configs()
+            if not 0 <= int(mode) < len(cfgs):
+                raise ValueError(f"launch configuration {mode} out of range")
+            cfg = int(mode)
+            form = cfgs[cfg]["form"]
+        elif mode in ("fused", "split"):
+            form = mode
+            cfg = 0 if mode == "fused" else 8
+        else:
+            raise ValueError("mode must be 'fused', 'split' or a configuration index")
+        if self.dtype != torch.float32 and (form == "split" or cfg != 0):
+            raise ValueError("only the default fused form exists in float64")
+        if form == "split" and self.scratch is None:
+            self.scratch = torch.zeros((_lib.load().ibis_mid_planes(), self.ld), dtype=self.dtype,
+                                       device=self.device)
+        self.mode = form
+        self.config = cfg
 
     # -------------------------------------------------------------- transfer
     @classmethod
@@ -143,10 +154,10 @@ class Columns:
         p.flags = flags
         if stream is None:
             stream = torch.cuda.current_stream(self.device)
-        if self.mode == "split":
-            rc = self._split(_ptr(self.prog), _ptr(self.stat), _ptr(forc), _ptr(self.diag), _ptr(self.acc),
-                             _ptr(self.scratch), self.ncell, self.ld, nstep, ctypes.byref(p), _ptr(self.status),
-                             ctypes.c_void_p(stream.cuda_stream))
+        if self.dtype == torch.float32:
+            rc = self._cfg_fn(_ptr(self.prog), _ptr(self.stat), _ptr(forc), _ptr(self.diag), _ptr(self.acc),
+                              _ptr(self.scratch), self.ncell, self.ld, nstep, ctypes.byref(p), _ptr(self.status),
+                              ctypes.c_void_p(stream.cuda_stream), self.config)
         else:
             rc = self._fn(_ptr(self.prog), _ptr(self.stat), _ptr(forc), _ptr(self.diag), _ptr(self.acc), self.ncell,
                           self.ld, nstep, ctypes.byref(p), _ptr(self.status), ctypes.c_void_p(stream.cuda_stream))

@@ -41,10 +41,17 @@ def main():
     out.append("    " + " ".join(f"s.a{i}{j} = 0.0;" for i, j in sorted(nz)))
     out.append("}")
     out.append("")
+    out.append("// Each pivot's reciprocal is formed once and reused by the rows below it and by")
+    out.append("// the back substitution (one division per unknown instead of one per update).")
     out.append("__device__ __forceinline__ void sys9_solve(Sys9& s, double (&x)[9]) {")
     out.append("    double f;")
+    out.append("    double r0, r1, r2, r3, r4, r5, r6, r7, r8;")
+    done = set()
     for p, i, cols in ops:
-        out.append(f"    f = s.a{i}{p} / s.a{p}{p};")
+        if p not in done:
+            out.append(f"    r{p} = 1.0 / s.a{p}{p};")
+            done.add(p)
+        out.append(f"    f = s.a{i}{p} * r{p};")
         for j in cols:
             out.append(f"    s.a{i}{j} = s.a{i}{j} - f * s.a{p}{j};")
         out.append(f"    s.b{i} = s.b{i} - f * s.b{p};")
@@ -53,10 +60,13 @@ def main():
         expr = None
         for j in terms:
             expr = f"s.a{i}{j} * x[{j}]" if expr is None else f"({expr} + s.a{i}{j} * x[{j}])"
+        if i not in done:
+            out.append(f"    r{i} = 1.0 / s.a{i}{i};")
+            done.add(i)
         if expr is None:
-            out.append(f"    x[{i}] = s.b{i} / s.a{i}{i};")
+            out.append(f"    x[{i}] = s.b{i} * r{i};")
         else:
-            out.append(f"    x[{i}] = (s.b{i} - {expr}) / s.a{i}{i};")
+            out.append(f"    x[{i}] = (s.b{i} - {expr}) * r{i};")
     out.append("}")
     out.append("")
     out.append("}  // namespace ibis")

@@ -317,8 +317,15 @@ __device__ __forceinline__ void turvap(double (&W)[9], TvOut<R>& o, const double
     const double qg = Sg.q, dqg = Sg.dq, qi = Si.q, dqi = Si.dq;
 
     // soil-surface humidity factor (canopy_exchange.py:532-572)
-    const double psig = -(double)P.grav * (double)X.suction0 * pow((double)X.zwtot, -(double)X.bex0);
-    const double hfac = exp(psig / ((double)P.rvap * tg));
+    double hfac;
+    if constexpr (sizeof(R) == 4) {
+        // float kernels: the matric-potential factor in float (it scales qg only)
+        const float psig = -P.grav * X.suction0 * powf(X.zwtot, -X.bex0);
+        hfac = (double)expf(psig / (P.rvap * (float)tg));
+    } else {
+        const double psig = -(double)P.grav * (double)X.suction0 * pow((double)X.zwtot, -(double)X.bex0);
+        hfac = exp(psig / ((double)P.rvap * tg));
+    }
     const double hfac2 = q34 / fmax(qg, eps);
     double betaw = clip(((double)X.zwtot - (double)X.swilt0) / fmax(1.0 - (double)X.swilt0, eps), 0.0, 1.0);
     if ((double)P.soil_beta_power != 1.0) betaw = pow(betaw, (double)P.soil_beta_power);

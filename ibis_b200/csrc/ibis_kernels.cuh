@@ -8,25 +8,26 @@
 
 #include "ibis_step.cuh"
 
-#ifndef IBIS_BLOCK
-#define IBIS_BLOCK 128
-#endif
-#ifndef IBIS_MIN_BLOCKS
-#define IBIS_MIN_BLOCKS 1
-#endif
-#ifndef IBIS_MIN_BLOCKS_SURF
-#define IBIS_MIN_BLOCKS_SURF 1
-#endif
-#ifndef IBIS_MIN_BLOCKS_GROUND
-#define IBIS_MIN_BLOCKS_GROUND 1
-#endif
 #ifndef IBIS_SMEM_STATE
 #define IBIS_SMEM_STATE 1
 #endif
 
 namespace ibis {
 
-constexpr int kBlock = IBIS_BLOCK;
+// Launch configurations.  form 0: one fused kernel per launch (all hours in
+// registers/shared memory); form 1: a surface kernel and a ground kernel per
+// hour.  block/minb are the block size and the minimum resident blocks per SM
+// promised to the compiler (__launch_bounds__), i.e. the register budget.
+struct LaunchConfig {
+    int form, block, minb, block2, minb2;
+};
+constexpr LaunchConfig kConfigs[] = {
+    {0, 128, 2, 0, 0}, {0, 64, 4, 0, 0},  {0, 96, 2, 0, 0},    {0, 128, 3, 0, 0},
+    {0, 160, 1, 0, 0}, {0, 192, 1, 0, 0}, {0, 224, 1, 0, 0},   {0, 256, 1, 0, 0},
+    {1, 128, 2, 128, 3}, {1, 256, 1, 256, 2}, {1, 128, 3, 128, 4}};
+constexpr int kNumConfigs = sizeof(kConfigs) / sizeof(kConfigs[0]);
+constexpr int kDefaultFused = 0;
+constexpr int kDefaultSplit = 8;
 
 // FP32 kernels keep each column's prognostic state in shared memory (array of
 // structures: the 71-word stride is odd, so a warp's accesses to one field fall
@@ -118,8 +119,8 @@ __device__ __forceinline__ Forc<R> load_forc(const R* __restrict__ f, int ld) {
 
 // Status word written by the kernels: [0] bit 0 = a column left the step with a
 // non-finite prognostic value; [1] = smallest such cell index (INT_MAX if none).
-template <typename R, int NT, bool SU, bool SL>
-__global__ void __launch_bounds__(kBlock, IBIS_MIN_BLOCKS) hourly_step_kernel(R* __restrict__ prog, const R* __restrict__ stat,
+template <typename R, int NT, bool SU, bool SL, int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) hourly_step_kernel(R* __restrict__ prog, const R* __restrict__ stat,
                                                              const R* __restrict__ forc, R* __restrict__ diag,
                                                              R* __restrict__ acc, int ncell, int ld, int nstep,
                                                              long long forc_stride, const DevParams<R> P,
@@ -151,8 +152,8 @@ __global__ void __launch_bounds__(kBlock, IBIS_MIN_BLOCKS) hourly_step_kernel(R*
 // Two-kernel form of one hour: the surface phase writes the hand-off values to
 // `mid` (kMidCount planes), the ground phase reads them.  Both phases load the
 // column from `prog` and write back what they change.
-template <typename R, bool SU, bool SL>
-__global__ void __launch_bounds__(kBlock, IBIS_MIN_BLOCKS_SURF) surface_kernel(R* __restrict__ prog, const R* __restrict__ stat,
+template <typename R, bool SU, bool SL, int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) surface_kernel(R* __restrict__ prog, const R* __restrict__ stat,
                                                                     const R* __restrict__ forc, R* __restrict__ diag,
                                                                     R* __restrict__ mid, int ncell, int ld,
                                                                     const DevParams<R> P) {
@@ -174,8 +175,8 @@ __global__ void __launch_bounds__(kBlock, IBIS_MIN_BLOCKS_SURF) surface_kernel(R
     store_col(c, prog + i, ld);
 }
 
-template <typename R, int NT>
-__global__ void __launch_bounds__(kBlock, IBIS_MIN_BLOCKS_GROUND) ground_kernel(R* __restrict__ prog, const R* __restrict__ stat,
+template <typename R, int NT, int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) ground_kernel(R* __restrict__ prog, const R* __restrict__ stat,
                                                                    const R* __restrict__ forc, R* __restrict__ diag,
                                                                    R* __restrict__ acc, const R* __restrict__ mid,
                                                                    int ncell, int ld, const DevParams<R> P,
@@ -261,33 +262,94 @@ static DevParams<R> make_dev_params(const IbisParams& h) {
     return d;
 }
 
-template <typename R, int NT, bool SU, bool SL>
-static cudaError_t launch_variant(R* prog, const R* stat, const R* forc, R* diag, R* acc, int ncell, int ld, int nstep,
-                                  long long fstride, const DevParams<R>& P, int* status, cudaStream_t s) {
-    const int grid = (ncell + kBlock - 1) / kBlock;
-    const size_t smem = StateInSmem<R>::value ? kBlock * sizeof(Col<R>) : 0;
-    hourly_step_kernel<R, NT, SU, SL><<<grid, kBlock, smem, s>>>(prog, stat, forc, diag, acc, ncell, ld, nstep, fstride,
-                                                              P, status);
+template <typename R, int NT, bool SU, bool SL, int BLOCK, int MINB>
+cudaError_t launch_fused(R* prog, const R* stat, const R* forc, R* diag, R* acc, int ncell, int ld, int nstep,
+                         long long fstride, const DevParams<R>& P, int* status, cudaStream_t s) {
+    const int grid = (ncell + BLOCK - 1) / BLOCK;
+    const size_t smem = StateInSmem<R>::value ? BLOCK * sizeof(Col<R>) : 0;
+    auto k = hourly_step_kernel<R, NT, SU, SL, BLOCK, MINB>;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k<<<grid, BLOCK, smem, s>>>(prog, stat, forc, diag, acc, ncell, ld, nstep, fstride, P, status);
     return cudaGetLastError();
 }
 
-template <typename R, int NT, bool SU, bool SL>
-static cudaError_t launch_split(R* prog, const R* stat, const R* forc, R* diag, R* acc, R* mid, int ncell, int ld,
-                                int nstep, long long fstride, const DevParams<R>& P, int* status, cudaStream_t s) {
-    const int grid = (ncell + kBlock - 1) / kBlock;
-    const size_t smem = StateInSmem<R>::value ? kBlock * sizeof(Col<R>) : 0;
+template <typename R, int NT, bool SU, bool SL, int B1, int M1, int B2, int M2>
+cudaError_t launch_split(R* prog, const R* stat, const R* forc, R* diag, R* acc, R* mid, int ncell, int ld,
+                         int nstep, long long fstride, const DevParams<R>& P, int* status, cudaStream_t s) {
+    const int g1 = (ncell + B1 - 1) / B1, g2 = (ncell + B2 - 1) / B2;
+    const size_t sm1 = StateInSmem<R>::value ? B1 * sizeof(Col<R>) : 0;
+    const size_t sm2 = StateInSmem<R>::value ? B2 * sizeof(Col<R>) : 0;
+    auto k1 = surface_kernel<R, SU, SL, B1, M1>;
+    auto k2 = ground_kernel<R, NT, B2, M2>;
+    if (sm1 > 48 * 1024) cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
+    if (sm2 > 48 * 1024) cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
     for (int h = 0; h < nstep; ++h) {
         const R* f = forc + (size_t)h * fstride;
-        surface_kernel<R, SU, SL><<<grid, kBlock, smem, s>>>(prog, stat, f, diag, mid, ncell, ld, P);
-        ground_kernel<R, NT><<<grid, kBlock, smem, s>>>(prog, stat, f, diag, acc, mid, ncell, ld, P, status);
+        k1<<<g1, B1, sm1, s>>>(prog, stat, f, diag, mid, ncell, ld, P);
+        k2<<<g2, B2, sm2, s>>>(prog, stat, f, diag, acc, mid, ncell, ld, P, status);
     }
     return cudaGetLastError();
 }
 
+template <typename R, int NT, bool SU, bool SL, int CFG>
+cudaError_t run_config(R* prog, const R* stat, const R* forc, R* diag, R* acc, R* mid, int ncell, int ld, int nstep,
+                       long long fs, const DevParams<R>& P, int* status, cudaStream_t s) {
+    constexpr LaunchConfig C = kConfigs[CFG];
+    if constexpr (C.form == 0)
+        return launch_fused<R, NT, SU, SL, C.block, C.minb>(prog, stat, forc, diag, acc, ncell, ld, nstep, fs, P,
+                                                            status, s);
+    else
+        return launch_split<R, NT, SU, SL, C.block, C.minb, C.block2, C.minb2>(prog, stat, forc, diag, acc, mid,
+                                                                              ncell, ld, nstep, fs, P, status, s);
+}
+
+#define IBIS_RUN_ARGS(R) \
+    R*, const R*, const R*, R*, R*, R*, int, int, int, long long, const DevParams<R>&, int*, cudaStream_t
+
+// Every (variant, configuration) pair the FP32 library instantiates: the F77
+// canopy (no sunlit/shaded split) in every configuration, the sunlit/shaded
+// variants in the two default ones.  X(NT, SU, SL, CFG).
+#define IBIS_F77_CONFIGS(X, NT)                                                                                \
+    X(NT, false, false, 0) X(NT, false, false, 1) X(NT, false, false, 2) X(NT, false, false, 3)                \
+    X(NT, false, false, 4) X(NT, false, false, 5) X(NT, false, false, 6) X(NT, false, false, 7)                \
+    X(NT, false, false, 8) X(NT, false, false, 9) X(NT, false, false, 10)
+#define IBIS_SUN_CONFIGS(X, NT)                                                                                \
+    X(NT, true, false, 0) X(NT, false, true, 0) X(NT, true, true, 0)                                           \
+    X(NT, true, false, 8) X(NT, false, true, 8) X(NT, true, true, 8)
+
+template <typename R, int NT, bool SU, bool SL>
+cudaError_t dispatch_config(int cfg, R* prog, const R* stat, const R* forc, R* diag, R* acc, R* mid, int ncell,
+                            int ld, int nstep, long long fs, const DevParams<R>& P, int* status, cudaStream_t s) {
+#define IBIS_ARGS prog, stat, forc, diag, acc, mid, ncell, ld, nstep, fs, P, status, s
+    if constexpr (sizeof(R) == 8) {
+        return run_config<R, NT, SU, SL, kDefaultFused>(IBIS_ARGS);
+    } else if constexpr (SU || SL) {
+        if (kConfigs[cfg].form == 0) return run_config<R, NT, SU, SL, kDefaultFused>(IBIS_ARGS);
+        return run_config<R, NT, SU, SL, kDefaultSplit>(IBIS_ARGS);
+    } else {
+        switch (cfg) {
+            case 1: return run_config<R, NT, SU, SL, 1>(IBIS_ARGS);
+            case 2: return run_config<R, NT, SU, SL, 2>(IBIS_ARGS);
+            case 3: return run_config<R, NT, SU, SL, 3>(IBIS_ARGS);
+            case 4: return run_config<R, NT, SU, SL, 4>(IBIS_ARGS);
+            case 5: return run_config<R, NT, SU, SL, 5>(IBIS_ARGS);
+            case 6: return run_config<R, NT, SU, SL, 6>(IBIS_ARGS);
+            case 7: return run_config<R, NT, SU, SL, 7>(IBIS_ARGS);
+            case 8: return run_config<R, NT, SU, SL, 8>(IBIS_ARGS);
+            case 9: return run_config<R, NT, SU, SL, 9>(IBIS_ARGS);
+            case 10: return run_config<R, NT, SU, SL, 10>(IBIS_ARGS);
+            default: return run_config<R, NT, SU, SL, 0>(IBIS_ARGS);
+        }
+    }
+#undef IBIS_ARGS
+}
+
 template <typename R>
 static int hourly_step(R* prog, const R* stat, const R* forc, R* diag, R* acc, int ncell, int ld, int nstep,
-                       const IbisParams* hp, int* status, void* stream, R* mid = nullptr) {
+                       const IbisParams* hp, int* status, void* stream, R* mid, int cfg) {
     if (!prog || !stat || !forc || !hp) return -EINVAL;
+    if (cfg < 0 || cfg >= kNumConfigs) return -EINVAL;
+    if (kConfigs[cfg].form == 1 && (!mid || sizeof(R) != 4)) return -EINVAL;
     if (ncell < 0 || nstep < 0 || ld < ncell || (ld % 32) != 0) return -EINVAL;
     if (ncell == 0 || nstep == 0) return 0;
     const unsigned known = IBIS_FLAG_BEDROCK | IBIS_FLAG_H2O_CONSISTENT | IBIS_FLAG_SUNSHADE_U | IBIS_FLAG_SUNSHADE_L |
@@ -305,9 +367,8 @@ static int hourly_step(R* prog, const R* stat, const R* forc, R* diag, R* acc, i
     const bool su = hp->flags & IBIS_FLAG_SUNSHADE_U;
     const bool sl = hp->flags & IBIS_FLAG_SUNSHADE_L;
     cudaError_t e;
-#define IBIS_CASE(NT_, SU_, SL_)                                                                                \
-    e = mid ? launch_split<R, NT_, SU_, SL_>(prog, stat, forc, diag, acc, mid, ncell, ld, nstep, fstride, P, status, s) \
-            : launch_variant<R, NT_, SU_, SL_>(prog, stat, forc, diag, acc, ncell, ld, nstep, fstride, P, status, s)
+#define IBIS_CASE(NT_, SU_, SL_) \
+    e = dispatch_config<R, NT_, SU_, SL_>(cfg, prog, stat, forc, diag, acc, mid, ncell, ld, nstep, fstride, P, status, s)
     if (bed) {
         if (su) { if (sl) IBIS_CASE(9, true, true); else IBIS_CASE(9, true, false); }
         else { if (sl) IBIS_CASE(9, false, true); else IBIS_CASE(9, false, false); }

@@ -1,18 +1,51 @@
 // FP32 production kernels of the hourly step (FP64 islands in the canopy and
-// soil-water solves) and their C-ABI entry point.
+// soil-water solves) and their C-ABI entry points.  The kernel instantiations
+// live in ibis_f32_inst_*.cu so they compile in parallel.
 #include "../../include/ibis_b200.h"
 #include "ibis_kernels.cuh"
 
+namespace ibis {
+#define IBIS_EXTERN(NT, SU, SL, CFG) \
+    extern template cudaError_t run_config<float, NT, SU, SL, CFG>(IBIS_RUN_ARGS(float));
+IBIS_F77_CONFIGS(IBIS_EXTERN, 6)
+IBIS_F77_CONFIGS(IBIS_EXTERN, 9)
+IBIS_SUN_CONFIGS(IBIS_EXTERN, 6)
+IBIS_SUN_CONFIGS(IBIS_EXTERN, 9)
+#undef IBIS_EXTERN
+}  // namespace ibis
+
 extern "C" int ibis_step_f32(float* prog, const float* stat, const float* forc, float* diag, float* acc, int ncell,
                              int ld, int nstep, const IbisParams* params, int* status, void* stream) {
-    return ibis::hourly_step<float>(prog, stat, forc, diag, acc, ncell, ld, nstep, params, status, stream);
+    return ibis::hourly_step<float>(prog, stat, forc, diag, acc, ncell, ld, nstep, params, status, stream, nullptr,
+                                    ibis::kDefaultFused);
 }
 
 extern "C" int ibis_step_split_f32(float* prog, const float* stat, const float* forc, float* diag, float* acc,
                                    float* scratch, int ncell, int ld, int nstep, const IbisParams* params,
                                    int* status, void* stream) {
     if (!scratch) return -EINVAL;
-    return ibis::hourly_step<float>(prog, stat, forc, diag, acc, ncell, ld, nstep, params, status, stream, scratch);
+    return ibis::hourly_step<float>(prog, stat, forc, diag, acc, ncell, ld, nstep, params, status, stream, scratch,
+                                    ibis::kDefaultSplit);
+}
+
+extern "C" int ibis_step_config_f32(float* prog, const float* stat, const float* forc, float* diag, float* acc,
+                                    float* scratch, int ncell, int ld, int nstep, const IbisParams* params,
+                                    int* status, void* stream, int config) {
+    return ibis::hourly_step<float>(prog, stat, forc, diag, acc, ncell, ld, nstep, params, status, stream, scratch,
+                                    config);
 }
 
 extern "C" int ibis_mid_planes(void) { return ibis::kMidCount; }
+
+extern "C" int ibis_num_configs(void) { return ibis::kNumConfigs; }
+
+extern "C" int ibis_config_info(int config, int* form, int* block, int* min_blocks, int* block2, int* min_blocks2) {
+    if (config < 0 || config >= ibis::kNumConfigs) return -EINVAL;
+    const ibis::LaunchConfig& c = ibis::kConfigs[config];
+    if (form) *form = c.form;
+    if (block) *block = c.block;
+    if (min_blocks) *min_blocks = c.minb;
+    if (block2) *block2 = c.block2;
+    if (min_blocks2) *min_blocks2 = c.minb2;
+    return 0;
+}

@@ -6,5 +6,6 @@
 
 extern "C" int ibis_step_f64(double* prog, const double* stat, const double* forc, double* diag, double* acc,
                              int ncell, int ld, int nstep, const IbisParams* params, int* status, void* stream) {
-    return ibis::hourly_step<double>(prog, stat, forc, diag, acc, ncell, ld, nstep, params, status, stream);
+    return ibis::hourly_step<double>(prog, stat, forc, diag, acc, ncell, ld, nstep, params, status, stream, nullptr,
+                                     ibis::kDefaultFused);
 }

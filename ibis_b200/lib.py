@@ -26,7 +26,24 @@ SIGNATURES = {
     "ibis_step_split_f32": (ctypes.c_int, [ctypes.c_void_p] * 6 + [ctypes.c_int] * 3
                             + [_P, ctypes.c_void_p, ctypes.c_void_p]),
     "ibis_mid_planes": (ctypes.c_int, []),
+    "ibis_step_config_f32": (ctypes.c_int, [ctypes.c_void_p] * 6 + [ctypes.c_int] * 3
+                             + [_P, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
+    "ibis_num_configs": (ctypes.c_int, []),
+    "ibis_config_info": (ctypes.c_int, [ctypes.c_int] + [_c_int_p] * 5),
 }
+
+
+def configs():
+    """List of dicts describing the launch configurations of the FP32 kernels."""
+    L = load()
+    out = []
+    for i in range(L.ibis_num_configs()):
+        v = [ctypes.c_int() for _ in range(5)]
+        check(L.ibis_config_info(i, *[ctypes.byref(x) for x in v]), "ibis_config_info")
+        f, b, m, b2, m2 = (x.value for x in v)
+        out.append(dict(id=i, form="fused" if f == 0 else "split", block=b, min_blocks=m, block2=b2,
+                        min_blocks2=m2))
+    return out
 
 _lib = None
 

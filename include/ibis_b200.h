@@ -52,6 +52,20 @@ int ibis_step_split_f32(float* prog, const float* stat, const float* forc, float
 /* Number of scratch planes ibis_step_split_f32 needs. */
 int ibis_mid_planes(void);
 
+/* ibis_step_f32 / ibis_step_split_f32 with an explicit launch configuration
+ * (0 <= config < ibis_num_configs()): the form (fused or two-kernel), block
+ * size and register budget.  `scratch` is required by two-kernel configs and
+ * ignored by fused ones.  ibis_b200/tune.py times them and picks one per batch.
+ * Replaces: timestep_body (loops.py:234) iterated by _step_body (loops_gswp3.py:115). */
+int ibis_step_config_f32(float* prog, const float* stat, const float* forc, float* diag, float* acc, float* scratch,
+                         int ncell, int ld, int nstep, const IbisParams* params, int* status, void* stream,
+                         int config);
+
+/* Launch configurations: count, and the description of one
+ * (form 0 = fused, 1 = two-kernel; block sizes and min resident blocks/SM). */
+int ibis_num_configs(void);
+int ibis_config_info(int config, int* form, int* block, int* min_blocks, int* block2, int* min_blocks2);
+
 /* Same contract in float64 throughout (the float64 run of the reference's step). */
 int ibis_step_f64(double* prog, const double* stat, const double* forc, double* diag, double* acc, int ncell,
                   int ld, int nstep, const IbisParams* params, int* status, void* stream);

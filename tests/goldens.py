@@ -57,8 +57,12 @@ FLOORS = {
     "fvapg": 1e-9, "fvapi": 1e-9, "ginvap": 1e-9, "gsuvap": 1e-9, "gtrans": 1e-9, "gtransu": 1e-9,
     "gtransl": 1e-9, "grunof": 1e-9, "gdrain": 1e-9, "gadjust": 1e-9, "raing": 1e-9, "snowg": 1e-9,
     "rainl": 1e-9, "snowl": 1e-9, "raing_avg": 1e-9, "ch4": 1e-15, "aygpptot": 1e-9, "aynpptot": 1e-9,
-    "aynpp": 1e-9, "hflo": 1.0, "a10ancub": 1e-9, "a10ancls": 1e-9, "a10ancl3": 1e-9, "a10ancl4": 1e-9,
+    "aynpp": 1e-9, "a10ancub": 1e-9, "a10ancls": 1e-9, "a10ancl3": 1e-9, "a10ancl4": 1e-9,
 }
+# energy fluxes (W m-2): an absolute floor of 1 W m-2 for near-zero fluxes
+for _k in ("hflo", "fsenu", "fsens", "fsenl", "fseng", "fseni", "firu", "firs", "firl", "firg", "firi", "firb",
+           "heatg", "heati", "fhtop_soil", "fhtop_snow", "sflo_bot", "solu", "sols", "soll", "solg", "soli"):
+    FLOORS[_k] = 1.0
 
 
 def compare(got: dict, want: dict, rtol: float, default_floor=1e-3, skip=()):
