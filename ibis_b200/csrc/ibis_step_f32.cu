@@ -49,3 +49,45 @@ extern "C" int ibis_config_info(int config, int* form, int* block, int* min_bloc
     if (min_blocks2) *min_blocks2 = c.minb2;
     return 0;
 }
+
+// ---------------------------------------------------------------------------
+// Two-kernel step without any allocation by the caller or the library.
+//
+// Some callers cannot call cudaMalloc at the point where they run the step: an
+// XLA custom-call handler must not allocate behind XLA's allocator, code that
+// runs while a stream is being captured into a CUDA graph cannot allocate, and
+// serving loops that reserve all device memory up front have nothing left to
+// hand out.  For them the hand-off planes of the two-kernel form live in a
+// fixed device array owned by this library, sized for kNoAllocMaxLd cells.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int kNoAllocMaxLd = 32768;   // largest leading dimension (cells, padded to 32) accepted
+constexpr int kMaxDevices = 64;
+// kMidCount planes x kNoAllocMaxLd floats = 3.5 MiB, resident on every GPU that loads the library.
+static __device__ __align__(256) float g_noalloc_mid[ibis::kMidCount * kNoAllocMaxLd];
+float* g_noalloc_ptr[kMaxDevices] = {nullptr};
+}  // namespace
+
+extern "C" int ibis_step_split_noalloc_f32(float* prog, const float* stat, const float* forc, float* diag,
+                                           float* acc, int ncell, int ld, int nstep, const IbisParams* params,
+                                           int* status, void* stream) {
+    if (ld > kNoAllocMaxLd) {
+        fprintf(stderr, "ibis_step_split_noalloc_f32: ld=%d exceeds the built-in scratch (%d cells)\n", ld,
+                kNoAllocMaxLd);
+        return -EINVAL;
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return -ENODEV;
+    if (!g_noalloc_ptr[dev]) {
+        // once per device, with that device current: the device address of the array
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_mid);
+        if (e != cudaSuccess || !p) {
+            fprintf(stderr, "ibis_step_split_noalloc_f32: cudaGetSymbolAddress failed: %s\n", cudaGetErrorString(e));
+            return -(int)e - 1000;
+        }
+        g_noalloc_ptr[dev] = static_cast<float*>(p);
+    }
+    return ibis::hourly_step<float>(prog, stat, forc, diag, acc, ncell, ld, nstep, params, status, stream,
+                                    g_noalloc_ptr[dev], ibis::kDefaultSplit);
+}

@@ -29,6 +29,8 @@ SIGNATURES = {
     "ibis_step_config_f32": (ctypes.c_int, [ctypes.c_void_p] * 6 + [ctypes.c_int] * 3
                              + [_P, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
     "ibis_num_configs": (ctypes.c_int, []),
+    "ibis_step_split_noalloc_f32": (ctypes.c_int, [ctypes.c_void_p] * 5 + [ctypes.c_int] * 3
+                                    + [_P, ctypes.c_void_p, ctypes.c_void_p]),
     "ibis_config_info": (ctypes.c_int, [ctypes.c_int] + [_c_int_p] * 5),
 }
 

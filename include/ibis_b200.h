@@ -66,6 +66,23 @@ int ibis_step_config_f32(float* prog, const float* stat, const float* forc, floa
 int ibis_num_configs(void);
 int ibis_config_info(int config, int* form, int* block, int* min_blocks, int* block2, int* min_blocks2);
 
+/* ibis_step_split_f32 for callers that cannot allocate device memory (an XLA
+ * custom-call handler that must not allocate behind XLA's allocator, code that
+ * runs while a stream is being captured into a CUDA graph, a serving loop that
+ * reserved all memory up front).  No counterpart in the reference: the
+ * hand-off planes live in a fixed array inside this library, sized for at most
+ * 32768 cells (ld <= 32768, 3.5 MiB held on every GPU that loads the library
+ * until the process exits); larger ld returns -EINVAL with a message on stderr.
+ * No cudaMalloc, cudaFree or other allocating call is made.  The first call on
+ * each device looks up the array's device address (cudaGetSymbolAddress), so
+ * make that first call before any stream capture.  Every call on a device
+ * shares the one array and it keeps the last call's contents; the surface
+ * kernel writes every value the ground kernel reads, so nothing needs
+ * clearing, but calls that overlap on the GPU (different streams, or
+ * different host threads) race on it and must be serialised by the caller. */
+int ibis_step_split_noalloc_f32(float* prog, const float* stat, const float* forc, float* diag, float* acc,
+                                int ncell, int ld, int nstep, const IbisParams* params, int* status, void* stream);
+
 /* Same contract in float64 throughout (the float64 run of the reference's step). */
 int ibis_step_f64(double* prog, const double* stat, const double* forc, double* diag, double* acc, int ncell,
                   int ld, int nstep, const IbisParams* params, int* status, void* stream);
