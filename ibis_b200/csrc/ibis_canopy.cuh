@@ -132,10 +132,10 @@ struct Stom {
 
 // One pass of stomata over the five big leaves.  Updates the carried ci/gs/cs
 // and a10 running means in `c`.  SUN_U/SUN_L select the sunlit/shaded canopy.
-template <typename R, bool SUN_U, bool SUN_L>
+template <typename R, bool SUN_U, bool SUN_L, typename Q>
 __device__ __forceinline__ void stomata(Stom<R>& o, Col<R>& c, R tu, R tl, R t12, R t34, R q12, R q34, R su,
                                         R sl, R ps, const Rad<R>& Rd, R fwetu, R fwetl, const Stat<R>& S,
-                                        R stresstu, R stresstl, const DevParams<R>& P) {
+                                        R stresstu, R stresstl, const DevParams<R>& P, const Q& q) {
     const R eps = P.epsilon;
     const R lai0 = S(IBIS_STAT_LAI, 0), lai1 = S(IBIS_STAT_LAI, 1);
     const R sai0 = S(IBIS_STAT_SAI, 0), sai1 = S(IBIS_STAT_SAI, 1);
@@ -146,9 +146,9 @@ __device__ __forceinline__ void stomata(Stom<R>& o, Col<R>& c, R tu, R tl, R t12
         R gb = clip(su * R(25.5), R(0.1), R(10.0));
         R rh = mx(R(0.30), q12 / mx(qsat(esat(t12), ps), eps));
         R vn[2];
-        vn[0] = S(IBIS_STAT_EXIST, 0) > R(0.5) ? P.vmax_pft[0]
-              : (S(IBIS_STAT_EXIST, 2) > R(0.5) ? P.vmax_pft[2] : P.vmax_pft[4]);
-        vn[1] = S(IBIS_STAT_EXIST, 3) > R(0.5) ? P.vmax_pft[3] : P.vmax_pft[5];
+        vn[0] = S(IBIS_STAT_EXIST, 0) > R(0.5) ? q.vmax(0)
+              : (S(IBIS_STAT_EXIST, 2) > R(0.5) ? q.vmax(2) : q.vmax(4));
+        vn[1] = S(IBIS_STAT_EXIST, 3) > R(0.5) ? q.vmax(3) : q.vmax(5);
         SunShade<R> ss;
         if (SUN_U) ss = sunshade(Rd.scu, Rd.dbeamu, Rd.termu6, Rd.termu7, lai1, sai1, P);
         R ag[2], an[2];
@@ -169,7 +169,7 @@ __device__ __forceinline__ void stomata(Stom<R>& o, Col<R>& c, R tu, R tl, R t12
                 bb = an[j];
             }
             c.ci_u[j] = ci;
-            ball_berry(c.cs_u[j], c.gs_u[j], c.ci_u[j], bb, gb, rh, P.coefm[j], P.coefb[j], stresstu, P.gsmin[j],
+            ball_berry(c.cs_u[j], c.gs_u[j], c.ci_u[j], bb, gb, rh, q.coefm(j), P.coefb[j], stresstu, P.gsmin[j],
                        gmn, gmn, P);
         }
         R scale = light_scaling(Rd.topparu, Rd.termu6, Rd.termu7, Rd.scu, lai1, sai1, c.a10su, c.a10du, P);
@@ -179,7 +179,7 @@ __device__ __forceinline__ void stomata(Stom<R>& o, Col<R>& c, R tu, R tl, R t12
             R agc = ag[j], anc = an[j];
             if (!SUN_U) { agc = ag[j] * scale; anc = an[j] * scale; }
             R csc = mx(gmn, P.co2conc - anc / gb);
-            R gsc = mx(mx(P.gsmin[j], P.coefb[j] * stresstu), P.coefm[j] * anc * rh / csc + P.coefb[j] * stresstu);
+            R gsc = mx(mx(P.gsmin[j], P.coefb[j] * stresstu), q.coefm(j) * anc * rh / csc + P.coefb[j] * stresstu);
             tcs[j] = total_conductance(su, gsc);
             o.ag_u[j] = agc * (R(1.0) - fwetu);
             o.an_u[j] = anc * (R(1.0) - fwetu);
@@ -201,7 +201,7 @@ __device__ __forceinline__ void stomata(Stom<R>& o, Col<R>& c, R tu, R tl, R t12
         for (int j = 0; j < 3; ++j) {
             const bool c4 = (j == 2);
             const int g = grp[j];
-            R vn = j == 0 ? P.vmax_pft[8] : (j == 1 ? P.vmax_pft[11] : P.vmax_pft[10]);
+            R vn = j == 0 ? q.vmax(8) : (j == 1 ? q.vmax(11) : q.vmax(10));
             R ci = clip(c.ci_l[j], c4 ? R(0.0) : gmn, P.cimax);
             R vm = c4 ? K.vm4 : K.vm3;
             R vmax = vn * vm * stresstl;
@@ -224,7 +224,7 @@ __device__ __forceinline__ void stomata(Stom<R>& o, Col<R>& c, R tu, R tl, R t12
                 bb = an[j];
             }
             c.ci_l[j] = ci;
-            ball_berry(c.cs_l[j], c.gs_l[j], c.ci_l[j], bb, gb, rh, P.coefm[g], P.coefb[g], stresstl, P.gsmin[g],
+            ball_berry(c.cs_l[j], c.gs_l[j], c.ci_l[j], bb, gb, rh, q.coefm(g), P.coefb[g], stresstl, P.gsmin[g],
                        c4 ? R(1.0e-8) : gmn, c4 ? R(0.0) : gmn, P);
         }
         R scale = light_scaling(Rd.topparl, Rd.terml6, Rd.terml7, Rd.scl, lai0, sai0, c.a10sl, c.a10dl, P);
@@ -236,7 +236,7 @@ __device__ __forceinline__ void stomata(Stom<R>& o, Col<R>& c, R tu, R tl, R t12
             R agc = ag[j], anc = an[j];
             if (!SUN_L) { agc = ag[j] * scale; anc = an[j] * scale; }
             R csc = mx(c4 ? R(1.0e-8) : gmn, P.co2conc - anc / gb);
-            R gsc = mx(mx(P.gsmin[g], P.coefb[g] * stresstl), P.coefm[g] * anc * rh / csc + P.coefb[g] * stresstl);
+            R gsc = mx(mx(P.gsmin[g], P.coefb[g] * stresstl), q.coefm(g) * anc * rh / csc + P.coefb[g] * stresstl);
             tcs[j] = total_conductance(sl, gsc);
             o.ag_l[j] = agc * (R(1.0) - fwetl);
             o.an_l[j] = anc * (R(1.0) - fwetl);
@@ -268,7 +268,7 @@ struct TvFixed {
 
 template <typename R>
 struct TvOut {
-    double fsenu, fsens, fsenl, fseng, fseni;
+    double fsena, fsenu, fsens, fsenl, fseng, fseni;
     double fvapuw, fvaput, fvaps, fvaplw, fvaplt, fvapg, fvapi;
     double firg, firi, firb, ginvap, gsuvap, gtrans;
 };
@@ -301,7 +301,7 @@ template <typename R>
 __device__ __forceinline__ void turvap(double (&W)[9], TvOut<R>& o, const double (&old)[5], const Trans<R>& T,
                                        double cp, double tfac, double wu, double ws, double wl, double wg,
                                        double wi, const TvFixed<R>& X, const Stom<R>& st, double ta, double qa,
-                                       double ps, const Stat<R>& S, const DevParams<R>& P) {
+                                       double ps, const Stat<R>& S, const DevParams<R>& P, double beta_power) {
     const double eps = (double)P.epsilon, dt = (double)P.dtime;
     const double tmelt = (double)P.tmelt, hvap = (double)P.hvap, hsub = (double)P.hsub;
     const double ch2o = (double)P.ch2o, cice = (double)P.cice, cvap = (double)P.cvap;
@@ -328,7 +328,7 @@ __device__ __forceinline__ void turvap(double (&W)[9], TvOut<R>& o, const double
     }
     const double hfac2 = q34 / fmax(qg, eps);
     double betaw = clip(((double)X.zwtot - (double)X.swilt0) / fmax(1.0 - (double)X.swilt0, eps), 0.0, 1.0);
-    if ((double)P.soil_beta_power != 1.0) betaw = pow(betaw, (double)P.soil_beta_power);
+    if (beta_power != 1.0) betaw = pow(betaw, beta_power);
     const double e34 = esat(t34);
     const double qs1 = qsat(e34, ps);
     const double dqs1 = dqsat(t34, qs1, e34);
@@ -448,6 +448,7 @@ __device__ __forceinline__ void turvap(double (&W)[9], TvOut<R>& o, const double
     const double ng = v[7], ni = v[8];
 
     // flux diagnostics (canopy_exchange.py:746-795)
+    o.fsena = cp * cu * (ta * tfac - n12);
     o.fsenu = cp * su * (wu * nu + (1.0 - wu) * tu - n12);
     o.fsens = cp * ss * (ws * ns + (1.0 - ws) * ts - n12);
     o.fsenl = cp * sl * (wl * nl + (1.0 - wl) * tl - n12);

@@ -305,11 +305,11 @@ __device__ __forceinline__ void radiation(Rad<R>& out, const Col<R>& c, const Fo
 // ===========================================================================
 
 template <typename R>
-__device__ __forceinline__ void wet_fraction(R tveg, R wliq, R wsno, R wliqmax, R wsnomax, const DevParams<R>& P,
-                                             R& fwet, R& rliq) {
+__device__ __forceinline__ void wet_fraction(R tveg, R wliq, R wsno, R wliqmax, R wsnomax, R fmax,
+                                             const DevParams<R>& P, R& fwet, R& rliq) {
     R xliq = wliq / mx(wliqmax, R(0.01));
     R xtot = xliq + wsno / mx(wsnomax, R(0.01));
-    fwet = mn(P.fmax, xtot);
+    fwet = mn(fmax, xtot);
     rliq = xliq / mx(xtot, P.epsilon);
     if (fwet == R(0.0)) rliq = (tveg < P.tmelt - R(1.0e-9)) ? R(0.0) : R(1.0);
 }
@@ -349,7 +349,8 @@ struct Surf { R wliq, wsno, pflux, rain, train, snow, tsnow; };
 // steph2o (interception.py:174-260)
 template <typename R>
 __device__ __forceinline__ Surf<R> intercept(R tveg, R wliq, R wsno, R xai, R rain, R train, R snow, R tsnow,
-                                             R tdrip, R tblow, R wliqmax, R wsnomax, const DevParams<R>& P) {
+                                             R tdrip, R tblow, R wliqmax, R wsnomax, R wliqmin,
+                                             const DevParams<R>& P) {
     const R dt = P.dtime, eps = P.epsilon;
     R fint = (xai >= eps) ? (R(1.0) - ex(R(-0.5) * xai)) / xai : R(0.5);
     R rdt = R(1.0) / dt;
@@ -360,7 +361,7 @@ __device__ __forceinline__ Surf<R> intercept(R tveg, R wliq, R wsno, R xai, R ra
     rain = rain * (R(1.0) - xai * fint);
     R x = wliq;
     wliq = mn(wliq, wliqmax);
-    if (wliq < P.wliqmin) wliq = R(0.0);
+    if (wliq < wliqmin) wliq = R(0.0);
     drip = drip + xai * (x - wliq) * rdt;
     R blow = xai * wsno / tblow;
     wsno = wsno * (R(1.0) - dt / tblow);
@@ -394,9 +395,9 @@ struct Casc {
 };
 
 // cascade (interception.py:263-357)
-template <typename R>
+template <typename R, typename Q>
 __device__ __forceinline__ void cascade(Casc<R>& o, const Col<R>& c, const Forc<R>& F, const Stat<R>& S,
-                                        const DevParams<R>& P) {
+                                        const DevParams<R>& P, const Q& q) {
     const R eps = P.epsilon;
     const R fu = S(IBIS_STAT_FU), fl = S(IBIS_STAT_FL);
     R tw = (F.ta > P.tmelt + R(1.0e-9)) ? wet_bulb(F.ta, F.qa, F.ps, P) : P.tmelt;
@@ -404,13 +405,14 @@ __device__ __forceinline__ void cascade(Casc<R>& o, const Col<R>& c, const Forc<
     mix2(rainu, trainu, F.rain, mx(tw, P.tmelt), R(0.0), mx(c.t12, P.tmelt), R(0.0), R(0.0), eps);
     mix2(snowu, tsnowu, F.snow, mn(F.ta, P.tmelt), R(0.0), mn(c.t12, P.tmelt), R(0.0), R(0.0), eps);
     Surf<R> u = intercept(c.tu, c.wliqu, c.wsnou, R(2.0) * S(IBIS_STAT_LAI, 1), rainu, trainu, snowu, tsnowu,
-                          P.tdripu, P.tblowu, P.wliqumax, P.wsnoumax, P);
+                          P.tdripu, P.tblowu, q.wliqumax(), P.wsnoumax, q.wliqmin(), P);
     Surf<R> s = intercept(c.ts, c.wliqs, c.wsnos, R(2.0) * S(IBIS_STAT_SAI, 1), u.rain, u.train, u.snow, u.tsnow,
-                          P.tdrips, P.tblows, P.wliqsmax, P.wsnosmax, P);
+                          P.tdrips, P.tblows, q.wliqsmax(), P.wsnosmax, q.wliqmin(), P);
     mix2(o.rainl, o.trainl, fu * s.rain, s.train, (R(1.0) - fu) * rainu, trainu, R(0.0), mx(c.t34, P.tmelt), eps);
     mix2(o.snowl, o.tsnowl, fu * s.snow, s.tsnow, (R(1.0) - fu) * snowu, tsnowu, R(0.0), mn(c.t34, P.tmelt), eps);
     Surf<R> l = intercept(c.tl, c.wliql, c.wsnol, R(2.0) * (S(IBIS_STAT_LAI, 0) + S(IBIS_STAT_SAI, 0)), o.rainl,
-                          o.trainl, o.snowl, o.tsnowl, P.tdripl, P.tblowl, P.wliqlmax, P.wsnolmax, P);
+                          o.trainl, o.snowl, o.tsnowl, P.tdripl, P.tblowl, q.wliqlmax(), P.wsnolmax,
+                          q.wliqmin(), P);
     mix2(o.raing, o.traing, fl * l.rain, l.train, (R(1.0) - fl) * o.rainl, o.trainl, R(0.0), R(0.0), eps);
     mix2(o.snowg, o.tsnowg, fl * l.snow, l.tsnow, (R(1.0) - fl) * o.snowl, o.tsnowl, R(0.0), R(0.0), eps);
     o.wliqu = u.wliq; o.wliqs = s.wliq; o.wliql = l.wliq;

@@ -1,0 +1,136 @@
+// C-ABI entry points of the calibration-ensemble kernels (ibis_ensemble.cuh).
+// The kernel instantiations live in ibis_ens_inst_*.cu so they compile in
+// parallel.
+#include <stdint.h>
+
+#include "../../include/ibis_b200.h"
+#include "ibis_ensemble.cuh"
+
+namespace ibis {
+#define IBIS_ENS_EXTERN(NT, SU, SL)                                                                          \
+    extern template cudaError_t launch_ensemble<NT, SU, SL>(const EnsArgs&, const DevParams<float>&, int, int, \
+                                                            cudaStream_t);                                     \
+    extern template int ensemble_occupancy<NT, SU, SL>(int);                                                  \
+    extern template cudaError_t launch_ensemble_hours<NT, SU, SL>(const EnsArgs&, const DevParams<float>&, int*, \
+                                                                  int, cudaStream_t);
+IBIS_ENS_VARIANTS(IBIS_ENS_EXTERN, 9)
+IBIS_ENS_VARIANTS(IBIS_ENS_EXTERN, 6)
+#undef IBIS_ENS_EXTERN
+
+namespace {
+
+constexpr unsigned kEnsFlags = IBIS_FLAG_BEDROCK | IBIS_FLAG_H2O_CONSISTENT | IBIS_FLAG_SUNSHADE_U |
+                               IBIS_FLAG_SUNSHADE_L | IBIS_FLAG_ACC | IBIS_FLAG_CH4 | IBIS_FLAG_SOIL_MEANS |
+                               IBIS_FLAG_KAHAN;
+
+// Validate an ensemble description; fills `a`.  Returns 0, or -EINVAL.
+int ens_args(const IbisEnsemble* e, const IbisParams* hp, EnsArgs& a) {
+    if (!e || !hp) return -EINVAL;
+    if (e->nrun < 0 || e->nsite < 0 || e->forc_len < 0) return -EINVAL;
+    if (e->nrun == 0) return 0;
+    if (!e->prog || !e->stat || !e->forc || !e->run_params || !e->run_site || !e->run_forc || !e->run_nstep)
+        return -EINVAL;
+    if (e->nsite < 1 || e->ld_run < e->nrun || e->ld_run % 32 || e->ld_site < e->nsite || e->ld_site % 32)
+        return -EINVAL;
+    if ((uintptr_t)e->forc % 16) return -EINVAL;
+    if (hp->flags & ~kEnsFlags) return -EINVAL;
+    const bool accum = hp->flags & (IBIS_FLAG_ACC | IBIS_FLAG_CH4 | IBIS_FLAG_SOIL_MEANS);
+    if (accum && !e->acc) return -EINVAL;
+    if (e->yearly && (!e->acc || !(hp->flags & IBIS_FLAG_ACC) || e->year_steps <= 0 || e->nyear < 0))
+        return -EINVAL;
+    if (!(hp->dtime > 0.0)) return -EINVAL;
+    a.prog = e->prog;
+    a.acc = accum ? e->acc : nullptr;
+    a.stat = e->stat;
+    a.forc = e->forc;
+    a.run_params = e->run_params;
+    a.run_site = e->run_site;
+    a.run_forc = e->run_forc;
+    a.run_nstep = e->run_nstep;
+    a.order = e->order;
+    a.yearly = e->yearly;
+    a.forc_len = e->forc_len;
+    a.nrun = e->nrun;
+    a.ld_run = e->ld_run;
+    a.nsite = e->nsite;
+    a.ld_site = e->ld_site;
+    a.nyear = e->nyear;
+    a.year_steps = e->year_steps > 0 ? e->year_steps : 1;
+    a.queue = e->queue;
+    a.status = e->status;
+    return 0;
+}
+
+int launch_error(cudaError_t err, const char* what) {
+    if (err == cudaSuccess) return 0;
+    fprintf(stderr, "ibis_b200: %s failed: %s\n", what, cudaGetErrorString(err));
+    return -(int)err - 1000;
+}
+
+// Expands CALL(NT, SU, SL) for the model variant the flags select.
+#define IBIS_BY_VARIANT(flags, CALL)                                                           \
+    (((flags) & IBIS_FLAG_BEDROCK)                                                            \
+         ? (((flags) & IBIS_FLAG_SUNSHADE_U)                                                  \
+                ? (((flags) & IBIS_FLAG_SUNSHADE_L) ? CALL(9, true, true) : CALL(9, true, false))  \
+                : (((flags) & IBIS_FLAG_SUNSHADE_L) ? CALL(9, false, true) : CALL(9, false, false))) \
+         : (((flags) & IBIS_FLAG_SUNSHADE_U)                                                  \
+                ? (((flags) & IBIS_FLAG_SUNSHADE_L) ? CALL(6, true, true) : CALL(6, true, false))  \
+                : (((flags) & IBIS_FLAG_SUNSHADE_L) ? CALL(6, false, true) : CALL(6, false, false))))
+
+}  // namespace
+}  // namespace ibis
+
+using namespace ibis;
+
+extern "C" int ibis_ensemble_occupancy(const IbisParams* params, int block) {
+    if (!params || block < 32 || block > 256 || block % 32) return 0;
+#define IBIS_OCC(NT, SU, SL) ensemble_occupancy<NT, SU, SL>(block)
+    return IBIS_BY_VARIANT(params->flags, IBIS_OCC);
+#undef IBIS_OCC
+}
+
+extern "C" int ibis_ensemble_f32(const IbisEnsemble* ens, const IbisParams* params, int block, void* stream) {
+    EnsArgs a{};
+    int rc = ens_args(ens, params, a);
+    if (rc || ens->nrun == 0) return rc;
+    if (!ens->queue) return -EINVAL;
+    if (block != 0 && (block < 32 || block > 256 || block % 32)) return -EINVAL;
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0)
+        return -ENODEV;
+    const int nitem = (a.nrun + 31) / 32;
+    if (block == 0) {
+        const int w = (nitem + sms - 1) / sms;          // warps per SM that cover every item in one pass
+        block = 32 * (w < 1 ? 1 : (w > 8 ? 8 : w));
+    }
+    const int occ = ibis_ensemble_occupancy(params, block);
+    if (occ <= 0) return -EINVAL;
+    const int per_block = block / 32;
+    int grid = sms * occ;
+    const int need = (nitem + per_block - 1) / per_block;
+    if (need < grid) grid = need;
+    const DevParams<float> P = make_dev_params<float>(*params);
+    cudaStream_t s = (cudaStream_t)stream;
+    rc = launch_error(cudaMemsetAsync(ens->queue, 0, sizeof(int), s), "ensemble queue reset");
+    if (rc) return rc;
+#define IBIS_RUN(NT, SU, SL) launch_ensemble<NT, SU, SL>(a, P, block, grid, s)
+    const cudaError_t err = IBIS_BY_VARIANT(params->flags, IBIS_RUN);
+#undef IBIS_RUN
+    return launch_error(err, "ensemble launch");
+}
+
+extern "C" int ibis_ensemble_hours_f32(const IbisEnsemble* ens, const IbisParams* params, int* hour, int nhour,
+                                       void* stream) {
+    EnsArgs a{};
+    int rc = ens_args(ens, params, a);
+    if (rc || ens->nrun == 0) return rc;
+    if (!hour || nhour < 0) return -EINVAL;
+    if (nhour == 0) return 0;
+    const DevParams<float> P = make_dev_params<float>(*params);
+    cudaStream_t s = (cudaStream_t)stream;
+#define IBIS_RUN(NT, SU, SL) launch_ensemble_hours<NT, SU, SL>(a, P, hour, nhour, s)
+    const cudaError_t err = IBIS_BY_VARIANT(params->flags, IBIS_RUN);
+#undef IBIS_RUN
+    return launch_error(err, "ensemble hourly launch");
+}

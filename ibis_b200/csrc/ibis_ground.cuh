@@ -362,9 +362,9 @@ __device__ __forceinline__ void fire_counters(Col<R>& c, R swilt0, const Forc<R>
 }
 
 // methane_flux (methane.py:233-383), kgC m-2 d-1
-template <typename R>
+template <typename R, typename Q>
 __device__ __forceinline__ R methane(R f_inund, R rh, const R (&t)[NL], const R (&w)[NL], const R (&i)[NL],
-                                     const DevParams<R>& P) {
+                                     const DevParams<R>& P, const Q& q) {
     R acc = R(0.0);
 #pragma unroll
     for (int k = 0; k < NL; ++k) {
@@ -373,7 +373,7 @@ __device__ __forceinline__ R methane(R f_inund, R rh, const R (&t)[NL], const R 
     }
     R ttop = acc / P.ch4_wtot;
     R wet = clip(ttop / mx(P.sat_crit, R(1e-6)), R(0.0), R(1.0));
-    R zwt = P.z_wt_max * (R(1.0) - wet);
+    R zwt = q.z_wt_max() * (R(1.0) - wet);
     R tt = R(0.0), tw = R(0.0);
 #pragma unroll
     for (int k = 0; k < NL; ++k) {
@@ -385,11 +385,11 @@ __device__ __forceinline__ R methane(R f_inund, R rh, const R (&t)[NL], const R 
     }
     R tth = tt > R(1e-12) ? tw / mx(tt, R(1e-12)) : t[0];
     R zp = mx(zwt, R(0.0));
-    R rha = mx(rh, R(0.0)) * ex(-zp / mx(P.z_tau, R(1e-6)));
-    R q10 = pw(P.q10p, (tth - P.t_ref) / R(10.0));
-    R prod = mx(rha, R(0.0)) * P.r_ch4 * q10 * (tth >= R(273.15) ? R(1.0) : R(0.0));
+    R rha = mx(rh, R(0.0)) * ex(-zp / mx(q.z_tau(), R(1e-6)));
+    R q10 = pw(q.q10p(), (tth - P.t_ref) / R(10.0));
+    R prod = mx(rha, R(0.0)) * q.r_ch4() * q10 * (tth >= R(273.15) ? R(1.0) : R(0.0));
     R area = clip(mx(f_inund, R(0.0)), R(0.0), R(1.0));
-    return area * prod * ex(-zp / mx(P.tau_oxid, R(1e-6)));
+    return area * prod * ex(-zp / mx(q.tau_oxid(), R(1e-6)));
 }
 
 }  // namespace ibis

@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) hourly_step_kernel(R* __restrict_
 #pragma unroll 1
     for (int s = 0; s < nstep; ++s) {
         Forc<R> F = load_forc(forc + (size_t)s * forc_stride + i, ld);
-        column_step<R, NT, SU, SL>(c, F, S, D, A, P);
+        column_step<R, NT, SU, SL>(c, F, S, D, A, P, UniformQ<R>{P});
     }
     R sum = store_col(c, prog + i, ld);
     if (status && !finite(sum)) {
@@ -170,7 +170,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) surface_kernel(R* __restrict__ pr
     Diag<R> D{diag ? diag + i : nullptr, ld};
     Forc<R> F = load_forc(forc + i, ld);
     Mid<R> M;
-    surface_phase<R, SU, SL>(c, F, S, D, P, M);
+    surface_phase<R, SU, SL>(c, F, S, D, P, UniformQ<R>{P}, M);
     mid_store(M, mid + i, ld);
     store_col(c, prog + i, ld);
 }
@@ -196,7 +196,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) ground_kernel(R* __restrict__ pro
     Forc<R> F = load_forc(forc + i, ld);
     Mid<R> M;
     mid_load(M, mid + i, ld);
-    ground_phase<R, NT>(c, F, S, D, A, P, M);
+    ground_phase<R, NT>(c, F, S, D, A, P, UniformQ<R>{P}, M);
     R sum = store_col(c, prog + i, ld);
     if (status && !finite(sum)) {
         atomicOr(status, 1);

@@ -36,4 +36,59 @@ struct DevParams {
     R hsoi_top[6], hsoi_bot[6];  // layer tops/bottoms (cumsum of hsoi)
 };
 
+// The parameters a calibration ensemble varies per run (the 31-parameter
+// vector: vmax per plant type, Ball-Berry slopes, soil-stress shape,
+// soil-evaporation exponent, interception capacities, wet fraction cap,
+// wetland-CH4 parameters, maintenance/growth respiration), and the values
+// derived from them.  The physics reads them through one of two sources:
+// UniformQ (one parameter record for every cell) or RunQ (one run's values,
+// 33 words: an odd stride, so a warp reading one field of its 32 runs' records
+// in shared memory touches 32 different banks).
+template <typename R>
+struct UniformQ {
+    const DevParams<R>& P;
+    __device__ __forceinline__ R vmax(int j) const { return P.vmax_pft[j]; }
+    __device__ __forceinline__ R coefm(int g) const { return P.coefm[g]; }
+    __device__ __forceinline__ R stressfac() const { return P.stressfac; }
+    __device__ __forceinline__ R znorm() const { return P.znorm; }
+    __device__ __forceinline__ R beta_power() const { return P.soil_beta_power; }
+    __device__ __forceinline__ R wliqumax() const { return P.wliqumax; }
+    __device__ __forceinline__ R wliqsmax() const { return P.wliqsmax; }
+    __device__ __forceinline__ R wliqlmax() const { return P.wliqlmax; }
+    __device__ __forceinline__ R fmax() const { return P.fmax; }
+    __device__ __forceinline__ R wliqmin() const { return P.wliqmin; }
+    __device__ __forceinline__ R r_ch4() const { return P.r_ch4; }
+    __device__ __forceinline__ R q10p() const { return P.q10p; }
+    __device__ __forceinline__ R z_tau() const { return P.z_tau; }
+    __device__ __forceinline__ R tau_oxid() const { return P.tau_oxid; }
+    __device__ __forceinline__ R z_wt_max() const { return P.z_wt_max; }
+    __device__ __forceinline__ R rwood(int j) const { return P.rwood_s[j]; }
+    __device__ __forceinline__ R rroot(int j) const { return P.rroot_s[j]; }
+    __device__ __forceinline__ R keep(int j) const { return P.keep[j]; }
+};
+
+template <typename R>
+struct RunQ {
+    R vmax_[12], coefm_[5], stressfac_, znorm_, beta_, wliqumax_, wliqsmax_, wliqlmax_, fmax_, wliqmin_;
+    R r_ch4_, q10p_, z_tau_, tau_oxid_, z_wt_max_, rwood_, rroot_, keep_;
+    __device__ __forceinline__ R vmax(int j) const { return vmax_[j]; }
+    __device__ __forceinline__ R coefm(int g) const { return coefm_[g]; }
+    __device__ __forceinline__ R stressfac() const { return stressfac_; }
+    __device__ __forceinline__ R znorm() const { return znorm_; }
+    __device__ __forceinline__ R beta_power() const { return beta_; }
+    __device__ __forceinline__ R wliqumax() const { return wliqumax_; }
+    __device__ __forceinline__ R wliqsmax() const { return wliqsmax_; }
+    __device__ __forceinline__ R wliqlmax() const { return wliqlmax_; }
+    __device__ __forceinline__ R fmax() const { return fmax_; }
+    __device__ __forceinline__ R wliqmin() const { return wliqmin_; }
+    __device__ __forceinline__ R r_ch4() const { return r_ch4_; }
+    __device__ __forceinline__ R q10p() const { return q10p_; }
+    __device__ __forceinline__ R z_tau() const { return z_tau_; }
+    __device__ __forceinline__ R tau_oxid() const { return tau_oxid_; }
+    __device__ __forceinline__ R z_wt_max() const { return z_wt_max_; }
+    __device__ __forceinline__ R rwood(int) const { return rwood_; }
+    __device__ __forceinline__ R rroot(int) const { return rroot_; }
+    __device__ __forceinline__ R keep(int) const { return keep_; }
+};
+
 }  // namespace ibis

@@ -37,15 +37,16 @@ struct Mid {
     R heatg, heati, fvapg, fvapi, fvaput, fvaplt, ginvap, gsuvap, gtrans;
     R raing, traing, snowg, tsnowg, rainl, trainl, snowl, tsnowl;
     R an_u[2], ag_u[2], an_l[3], ag_l[3];
+    R fsena;
 };
-constexpr int kMidCount = 27;
+constexpr int kMidCount = 28;
 
 template <typename R>
 __device__ __forceinline__ void mid_store(const Mid<R>& m, R* __restrict__ p, int ld) {
     const R v[kMidCount] = {m.heatg, m.heati, m.fvapg, m.fvapi, m.fvaput, m.fvaplt, m.ginvap, m.gsuvap, m.gtrans,
                             m.raing, m.traing, m.snowg, m.tsnowg, m.rainl, m.trainl, m.snowl, m.tsnowl,
                             m.an_u[0], m.an_u[1], m.ag_u[0], m.ag_u[1], m.an_l[0], m.an_l[1], m.an_l[2],
-                            m.ag_l[0], m.ag_l[1], m.ag_l[2]};
+                            m.ag_l[0], m.ag_l[1], m.ag_l[2], m.fsena};
 #pragma unroll
     for (int q = 0; q < kMidCount; ++q) p[(size_t)q * ld] = v[q];
 }
@@ -62,6 +63,7 @@ __device__ __forceinline__ void mid_load(Mid<R>& m, const R* __restrict__ p, int
     m.an_u[0] = v[17]; m.an_u[1] = v[18]; m.ag_u[0] = v[19]; m.ag_u[1] = v[20];
     m.an_l[0] = v[21]; m.an_l[1] = v[22]; m.an_l[2] = v[23];
     m.ag_l[0] = v[24]; m.ag_l[1] = v[25]; m.ag_l[2] = v[26];
+    m.fsena = v[27];
 }
 
 // setsoi (soil_physics.py:37-140): conductivity of layer k
@@ -103,8 +105,8 @@ __device__ __forceinline__ void evap_sources(const Col<R>& c, const Forc<R>& F, 
 }
 
 // drystress (stomata.py:515-562)
-template <typename R>
-__device__ __forceinline__ void soil_stress(const Col<R>& c, const Stat<R>& S, const DevParams<R>& P,
+template <typename R, typename Q>
+__device__ __forceinline__ void soil_stress(const Col<R>& c, const Stat<R>& S, const DevParams<R>& P, const Q& q,
                                             R (&stressu)[NL], R (&stressl)[NL], R& stresstu, R& stresstl) {
     stresstu = R(0.0);
     stresstl = R(0.0);
@@ -112,7 +114,7 @@ __device__ __forceinline__ void soil_stress(const Col<R>& c, const Stat<R>& S, c
     for (int k = 0; k < NL; ++k) {
         R sw = S(IBIS_STAT_SWILT, k);
         R awc = clip((c.wsoi[k] * (R(1.0) - c.wisoi[k]) - sw) / mx(S(IBIS_STAT_SFIELD, k) - sw, R(1e-10)), R(0.0), R(1.0));
-        R zw = clip((R(1.0) - ex(P.stressfac * awc)) / P.znorm, R(0.0), R(1.0));
+        R zw = clip((R(1.0) - ex(q.stressfac() * awc)) / q.znorm(), R(0.0), R(1.0));
         stressl[k] = zw * P.froot[2 * k + 0];
         stressu[k] = zw * P.froot[2 * k + 1];
         stresstl = stresstl + stressl[k];
@@ -124,9 +126,9 @@ __device__ __forceinline__ void soil_stress(const Col<R>& c, const Stat<R>& S, c
 // three canopy passes (turcof + stomata + turvap), evaporation of intercepted
 // water, the bare-story reset and the surface fluxes (loops.py:318-674).
 // Leaves tu/ts/tl/tg unclamped in `c` (the ground phase clamps them).
-template <typename R, bool SUN_U, bool SUN_L>
+template <typename R, bool SUN_U, bool SUN_L, typename Q>
 __device__ __forceinline__ void surface_phase(Col<R>& c, const Forc<R>& F, const Stat<R>& S, const Diag<R>& D,
-                                              const DevParams<R>& P, Mid<R>& M) {
+                                              const DevParams<R>& P, const Q& q, Mid<R>& M) {
     const R eps = P.epsilon;
     const R fi = c.fi;
     const R lai0 = S(IBIS_STAT_LAI, 0), lai1 = S(IBIS_STAT_LAI, 1);
@@ -140,19 +142,19 @@ __device__ __forceinline__ void surface_phase(Col<R>& c, const Forc<R>& F, const
     Rad<R> Rd;
     {
         R fwu, fws, fwl, rlu, rls, rll;
-        wet_fraction(c.tu, c.wliqu, c.wsnou, P.wliqumax, P.wsnoumax, P, fwu, rlu);
-        wet_fraction(c.ts, c.wliqs, c.wsnos, P.wliqsmax, P.wsnosmax, P, fws, rls);
-        wet_fraction(c.tl, c.wliql, c.wsnol, P.wliqlmax, P.wsnolmax, P, fwl, rll);
+        wet_fraction(c.tu, c.wliqu, c.wsnou, q.wliqumax(), P.wsnoumax, q.fmax(), P, fwu, rlu);
+        wet_fraction(c.ts, c.wliqs, c.wsnos, q.wliqsmax(), P.wsnosmax, q.fmax(), P, fws, rls);
+        wet_fraction(c.tl, c.wliql, c.wsnol, q.wliqlmax(), P.wsnolmax, q.fmax(), P, fwl, rll);
         radiation(Rd, c, F, S, fwu, fws, fwl, rlu, rls, rll, P);
     }
 
     // ---- 4-5. precipitation cascade and wet fractions after it (loops.py:359-389)
     Casc<R> C;
-    cascade(C, c, F, S, P);
+    cascade(C, c, F, S, P, q);
     R fwetu, fwets, fwetl, rliqu, rliqs, rliql;
-    wet_fraction(c.tu, C.wliqu, C.wsnou, P.wliqumax, P.wsnoumax, P, fwetu, rliqu);
-    wet_fraction(c.ts, C.wliqs, C.wsnos, P.wliqsmax, P.wsnosmax, P, fwets, rliqs);
-    wet_fraction(c.tl, C.wliql, C.wsnol, P.wliqlmax, P.wsnolmax, P, fwetl, rliql);
+    wet_fraction(c.tu, C.wliqu, C.wsnou, q.wliqumax(), P.wsnoumax, q.fmax(), P, fwetu, rliqu);
+    wet_fraction(c.ts, C.wliqs, C.wsnos, q.wliqsmax(), P.wsnosmax, q.fmax(), P, fwets, rliqs);
+    wet_fraction(c.tl, C.wliql, C.wsnol, q.wliqlmax(), P.wsnolmax, q.fmax(), P, fwetl, rliql);
 
     // ---- 6. canopy exchange (loops.py:396-611)
     Aero<R> A;
@@ -161,7 +163,7 @@ __device__ __forceinline__ void surface_phase(Col<R>& c, const Forc<R>& F, const
     R stresstu, stresstl;
     {
         R su_[NL], sl_[NL];
-        soil_stress(c, S, P, su_, sl_, stresstu, stresstl);
+        soil_stress(c, S, P, q, su_, sl_, stresstu, stresstl);
     }
     TvFixed<R> X;
     const R csoi0 = S(IBIS_STAT_CSOI, 0) > R(0.0) ? S(IBIS_STAT_CSOI, 0) : P.csoi_mineral_val;
@@ -220,13 +222,14 @@ __device__ __forceinline__ void surface_phase(Col<R>& c, const Forc<R>& F, const
         Trans<R> T;
         transfer(T, strat, u2, alogu, alogl, A, F, t12, t34, q12, q34, first, P);
         stomata<R, SUN_U, SUN_L>(st, c, tu, tl, t12, t34, q12, q34, T.su, T.sl, F.ps, Rd, fwetu, fwetl, S,
-                                 stresstu, stresstl, P);
+                                 stresstu, stresstl, P, q);
         R wu = weight_veg(tu, (R)X.chux, C.wliqu, C.wsnou, wprev[0], first, P);
         R ws = weight_veg(ts, (R)X.chsx, C.wliqs, C.wsnos, wprev[1], first, P);
         R wl = weight_veg(tl, (R)X.chlx, C.wliql, C.wsnol, wprev[2], first, P);
         R wg = weight_veg(tg, chgx, wlgx, wigx, wprev[3], first, P);
         R wi = weight_snow(ti, c.ti, wprev[4], first, P);
-        turvap(Wv, tv, old, T, (double)A.cp, (double)P.tfac, wu, ws, wl, wg, wi, X, st, ta64, qa64, ps64, S, P);
+        turvap(Wv, tv, old, T, (double)A.cp, (double)P.tfac, wu, ws, wl, wg, wi, X, st, ta64, qa64, ps64, S, P,
+               (double)q.beta_power());
         wprev[0] = wu; wprev[1] = ws; wprev[2] = wl; wprev[3] = wg; wprev[4] = wi;
     }
     const R ti_new = mn((R)Wv[8], P.tmelt);
@@ -256,6 +259,7 @@ __device__ __forceinline__ void surface_phase(Col<R>& c, const Forc<R>& F, const
     M.ginvap = (R)tv.ginvap;
     M.gsuvap = (R)tv.gsuvap;
     M.gtrans = (R)tv.gtrans;
+    M.fsena = (R)tv.fsena;
     M.raing = C.raing; M.traing = C.traing; M.snowg = C.snowg; M.tsnowg = C.tsnowg;
     M.rainl = C.rainl; M.trainl = C.trainl; M.snowl = C.snowl; M.tsnowl = C.tsnowl;
 #pragma unroll
@@ -296,15 +300,16 @@ __device__ __forceinline__ void surface_phase(Col<R>& c, const Forc<R>& F, const
         D.put(IBIS_DIAG_GINVAP, M.ginvap); D.put(IBIS_DIAG_GSUVAP, M.gsuvap); D.put(IBIS_DIAG_GTRANS, M.gtrans);
         D.put(IBIS_DIAG_RAINL, C.rainl); D.put(IBIS_DIAG_SNOWL, C.snowl);
         D.put(IBIS_DIAG_TRAINL, C.trainl); D.put(IBIS_DIAG_TSNOWL, C.tsnowl);
+        D.put(IBIS_DIAG_FSENA, M.fsena);
     }
 }
 
 // Steps 10-12 of timestep_body -- snow, soil water and heat (+ bedrock),
 // freeze/thaw, the surface-temperature bound -- then the fire counters and the
 // day-loop accumulators (loops.py:676-1275; loops_gswp3.py:161-318).
-template <typename R, int NT>
+template <typename R, int NT, typename Q>
 __device__ __forceinline__ void ground_phase(Col<R>& c, const Forc<R>& F, const Stat<R>& S, const Diag<R>& D,
-                                             const Acc<R>& Ac, const DevParams<R>& P, const Mid<R>& M) {
+                                             const Acc<R>& Ac, const DevParams<R>& P, const Q& q, const Mid<R>& M) {
     const R eps = P.epsilon, dt = P.dtime;
     const R fi = c.fi;
     const R lai0 = S(IBIS_STAT_LAI, 0), lai1 = S(IBIS_STAT_LAI, 1);
@@ -318,7 +323,7 @@ __device__ __forceinline__ void ground_phase(Col<R>& c, const Forc<R>& F, const 
     R q1, q2, q3, q4, hvasug_, hvasui_;
     evap_sources(c, F, P, q1, q2, q3, q4, hvasug_, hvasui_);
     R stressu[NL], stressl[NL], stresstu, stresstl;
-    soil_stress(c, S, P, stressu, stressl, stresstu, stresstl);
+    soil_stress(c, S, P, q, stressu, stressl, stresstu, stresstl);
 
     // ---- 10. snow (loops.py:676-848)
     R smelt, zheat, sflo_bot, fhtop_snow;
@@ -567,10 +572,10 @@ __device__ __forceinline__ void ground_phase(Col<R>& c, const Forc<R>& F, const 
                 R g;
                 if (j < 8) g = an * S(IBIS_STAT_FRAC, j) * lai_ * cov;
                 else g = an * S(IBIS_STAT_FRAC, j) * lai_ * fl * smask;
-                R r = P.rroot_s[j] * S(IBIS_STAT_CBIOR, j) * funcb;
-                if (wood) r = (j < 8 ? P.rwood_s[j] * S(IBIS_STAT_CBIOW, j) * sp * funca
-                                     : P.rwood_s[j] * S(IBIS_STAT_CBIOW, j) * funca) + r;
-                R inc = P.keep[j] * (g - r) * cf;
+                R r = q.rroot(j) * S(IBIS_STAT_CBIOR, j) * funcb;
+                if (wood) r = (j < 8 ? q.rwood(j) * S(IBIS_STAT_CBIOW, j) * sp * funca
+                                     : q.rwood(j) * S(IBIS_STAT_CBIOW, j) * funca) + r;
+                R inc = q.keep(j) * (g - r) * cf;
                 if (Ac.kahan) {
                     Ac.add(IBIS_ACC_AYNPP + j, inc);
                     npp = npp + inc;
@@ -598,10 +603,11 @@ __device__ __forceinline__ void ground_phase(Col<R>& c, const Forc<R>& F, const 
             Ac.add(IBIS_ACC_AYGPPTOT, (gu + gl) * cf);
             Ac.add(IBIS_ACC_AYTRUNOF, grunof * dt);
             Ac.add(IBIS_ACC_AYTDRAIN, wflo[NL] * dt);
+            Ac.add(IBIS_ACC_AFSENA, M.fsena * dt);
         }
         if (P.flags & IBIS_FLAG_CH4) {
             R rh = S(IBIS_STAT_TCO2MIC) * P.rh_conv;
-            R flux = methane(S(IBIS_STAT_F_INUND), rh, c.tsoi, c.wsoi, c.wisoi, P);
+            R flux = methane(S(IBIS_STAT_F_INUND), rh, c.tsoi, c.wsoi, c.wisoi, P, q);
             Ac.add(IBIS_ACC_CH4, flux * P.ch4_w);
         }
         if (P.flags & IBIS_FLAG_SOIL_MEANS) {
@@ -617,12 +623,12 @@ __device__ __forceinline__ void ground_phase(Col<R>& c, const Forc<R>& F, const 
 }
 
 // One full hourly step of a column in one kernel.
-template <typename R, int NT, bool SUN_U, bool SUN_L>
+template <typename R, int NT, bool SUN_U, bool SUN_L, typename Q>
 __device__ __forceinline__ void column_step(Col<R>& c, const Forc<R>& F, const Stat<R>& S, const Diag<R>& D,
-                                            const Acc<R>& Ac, const DevParams<R>& P) {
+                                            const Acc<R>& Ac, const DevParams<R>& P, const Q& q) {
     Mid<R> M;
-    surface_phase<R, SUN_U, SUN_L>(c, F, S, D, P, M);
-    ground_phase<R, NT>(c, F, S, D, Ac, P, M);
+    surface_phase<R, SUN_U, SUN_L>(c, F, S, D, P, q, M);
+    ground_phase<R, NT>(c, F, S, D, Ac, P, q, M);
 }
 
 }  // namespace ibis

@@ -7,7 +7,7 @@ that each plane starts 128-byte aligned).  A field with a trailing dimension of
 planes, layer-major, so thread ``i`` of a warp reads element ``i`` of a plane
 and every load is coalesced.
 
-The planes are grouped into five buffers by how the step uses them:
+The planes are grouped into buffers by how the step uses them:
 
 ``PROG``   prognostic state: read at the start of a step, written at its end
 ``STAT``   per-cell static inputs (soil texture, vegetation structure): read only
@@ -16,6 +16,8 @@ The planes are grouped into five buffers by how the step uses them:
 ``ACC``    per-step accumulators of the day loop (optional; Kahan-compensated
            in the FP32 kernels, so each accumulator plane has a twin holding
            its running compensation)
+``RUN``    per-run calibration vector of the ensemble kernels
+``YEARLY`` accumulator totals an ensemble run reports at each year end
 
 Each field names the leaf of the reference ``IBISState`` it mirrors
 (``python-port/ibis/state/*.py``), so host code can move data between the
@@ -195,6 +197,7 @@ DIAG = (
     Field("tsnowl", "hydrology.tsnowl"),
     Field("sflo_bot", "hydrology.sflo_bot"),
     Field("fhtop_snow", "hydrology.fhtop_snow"),
+    Field("fsena", "canopy.fsena"),
 )
 
 ACC = (
@@ -215,9 +218,47 @@ ACC = (
     Field("wsoi_mean", "acc.wsoi_day", NSOILAY),
     Field("wisoi_mean", "acc.wisoi_day", NSOILAY),
     Field("tg_mean", "acc.tg_day"),
+    Field("afsena", "acc.fsena"),
 )
 
-GROUPS = {"PROG": PROG, "STAT": STAT, "FORC": FORC, "DIAG": DIAG, "ACC": ACC}
+# Per-run calibration vector of the ensemble kernels: the step-relevant
+# parameters the reference's tower calibration varies
+# (verify/calibration/fit_carbon.py:253-381, setters of SimParams leaves), 31
+# values.  rwood/rroot/rgrowth are scalars there and apply to all 12 plant
+# types; t_ref of the methane model stays at its SimParams value, as the tower
+# fits hold it.
+RUN = (
+    Field("vmax", "stomata_params.vmax_pft", NPFT),
+    Field("coefm", "stomata_params.coefm", 5),
+    Field("stressfac", "stomata_params.stressfac"),
+    Field("soil_beta_power", "canopy.soil_beta_power"),
+    Field("wliqumax", "interception.wliqumax"),
+    Field("wliqsmax", "interception.wliqsmax"),
+    Field("wliqlmax", "interception.wliqlmax"),
+    Field("fmax", "interception.fmax"),
+    Field("r_ch4", "methane.r_ch4"),
+    Field("q10p", "methane.q10p"),
+    Field("z_tau", "methane.z_tau"),
+    Field("tau_oxid", "methane.tau_oxid"),
+    Field("z_wt_max", "methane.z_wt_max"),
+    Field("rwood", "bgc_params.rwood"),
+    Field("rroot", "bgc_params.rroot"),
+    Field("rgrowth", "bgc_params.rgrowth"),
+)
+
+# Accumulators an ensemble run reports at the end of each year of its record
+# (running totals; the host differences them into per-year sums).
+YEARLY = (
+    Field("aygpptot", "summary.aygpptot"),
+    Field("aynpptot", "summary.aynpptot"),
+    Field("adaet", "summary.adaet"),
+    Field("afsena", "acc.fsena"),
+    Field("aytrunof", "summary.aytrunof"),
+    Field("aytdrain", "summary.aytdrain"),
+    Field("ch4", "acc.ch4_day"),
+)
+
+GROUPS = {"PROG": PROG, "STAT": STAT, "FORC": FORC, "DIAG": DIAG, "ACC": ACC, "RUN": RUN, "YEARLY": YEARLY}
 
 
 def offsets(group):
@@ -238,6 +279,8 @@ N_STAT = nplanes(STAT)
 N_FORC = nplanes(FORC)
 N_DIAG = nplanes(DIAG)
 N_ACC = nplanes(ACC)
+N_RUN = nplanes(RUN)
+N_YEARLY = nplanes(YEARLY)
 
 OFF = {g: offsets(v) for g, v in GROUPS.items()}
 

@@ -16,8 +16,22 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 LIB_PATH = os.path.join(HERE, "_lib", "libibis_b200.so")
 
+
+
+class IbisEnsembleC(ctypes.Structure):
+    """ctypes mirror of ``IbisEnsemble`` (include/ibis_b200.h)."""
+    _fields_ = [("prog", ctypes.c_void_p), ("acc", ctypes.c_void_p), ("stat", ctypes.c_void_p),
+                ("forc", ctypes.c_void_p), ("run_params", ctypes.c_void_p), ("run_site", ctypes.c_void_p),
+                ("run_forc", ctypes.c_void_p), ("run_nstep", ctypes.c_void_p), ("order", ctypes.c_void_p),
+                ("yearly", ctypes.c_void_p), ("forc_len", ctypes.c_longlong), ("nrun", ctypes.c_int),
+                ("ld_run", ctypes.c_int), ("nsite", ctypes.c_int), ("ld_site", ctypes.c_int),
+                ("nyear", ctypes.c_int), ("year_steps", ctypes.c_int), ("queue", ctypes.c_void_p),
+                ("status", ctypes.c_void_p)]
+
+
 _c_int_p = ctypes.POINTER(ctypes.c_int)
 _P = ctypes.POINTER(IbisParamsC)
+_E = ctypes.POINTER(IbisEnsembleC)
 
 # name -> (restype, argtypes); every function declared in include/*.h
 SIGNATURES = {
@@ -32,6 +46,9 @@ SIGNATURES = {
     "ibis_step_split_noalloc_f32": (ctypes.c_int, [ctypes.c_void_p] * 5 + [ctypes.c_int] * 3
                                     + [_P, ctypes.c_void_p, ctypes.c_void_p]),
     "ibis_config_info": (ctypes.c_int, [ctypes.c_int] + [_c_int_p] * 5),
+    "ibis_ensemble_f32": (ctypes.c_int, [_E, _P, ctypes.c_int, ctypes.c_void_p]),
+    "ibis_ensemble_hours_f32": (ctypes.c_int, [_E, _P, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    "ibis_ensemble_occupancy": (ctypes.c_int, [_P, ctypes.c_int]),
 }
 
 

@@ -83,6 +83,59 @@ int ibis_config_info(int config, int* form, int* block, int* min_blocks, int* bl
 int ibis_step_split_noalloc_f32(float* prog, const float* stat, const float* forc, float* diag, float* acc,
                                 int ncell, int ld, int nstep, const IbisParams* params, int* status, void* stream);
 
+/* A calibration ensemble: nrun runs, each one parameter vector at one site
+ * over its own record of hourly forcing.  Per-run buffers use ld_run, per-site
+ * buffers ld_site (both multiples of 32, >= the count).
+ *   prog        [IBIS_PROG_COUNT][ld_run]       in/out: state of every run
+ *   acc         [2*IBIS_ACC_COUNT][ld_run]/NULL in/out: accumulators + Kahan terms
+ *   stat        [IBIS_STAT_COUNT][ld_site]      in: static inputs of every site
+ *   forc        [forc_len][IBIS_FORC_COUNT]     in: hourly forcing records (16-byte aligned)
+ *   run_params  [IBIS_RUN_COUNT][ld_run]        in: calibration vector of every run
+ *   run_site    [nrun]  site of the run; run_forc [nrun] index of its first record
+ *   run_nstep   [nrun]  hours in its record (records run_forc .. run_forc+nstep-1)
+ *   order       [nrun] or NULL: order in which runs are taken (longest first is best)
+ *   yearly      [nyear][IBIS_YEARLY_COUNT][ld_run] or NULL: running totals of the
+ *               IBIS_YEARLY accumulators at the end of each year_steps hours
+ *   queue       device int used as the work counter (reset by the call)
+ *   status      device int[2] as for ibis_step_f32; bit 1 (value 2) flags a run
+ *               whose descriptor is out of range, which is then skipped.
+ * No counterpart in the reference's step API: its calibration harness runs
+ * one site at a time in host worker processes (verify/calibration/site_fit.py:375-436). */
+typedef struct IbisEnsemble {
+    float* prog;
+    float* acc;
+    const float* stat;
+    const float* forc;
+    const float* run_params;
+    const int* run_site;
+    const long long* run_forc;
+    const int* run_nstep;
+    const int* order;
+    float* yearly;
+    long long forc_len;
+    int nrun, ld_run, nsite, ld_site, nyear, year_steps;
+    int* queue;
+    int* status;
+} IbisEnsemble;
+
+/* Every run of the ensemble from its first hour to its last in ONE persistent
+ * launch: grid = SMs x resident blocks of `block` threads (a multiple of 32,
+ * <= 256; 0 picks one from the run count), each warp drawing 32 runs at a time
+ * from the work counter.  params->flags selects the model variants and the
+ * accumulators as for ibis_step_f32 (no diagnostics). */
+int ibis_ensemble_f32(const IbisEnsemble* ens, const IbisParams* params, int block, void* stream);
+
+/* The same runs advanced `nhour` hours in nhour launches (one per hour), from
+ * the hour held in the device int *hour, which the last launch advances by
+ * nhour: a fixed sequence that can be captured once in a CUDA graph and
+ * replayed until every record has ended. */
+int ibis_ensemble_hours_f32(const IbisEnsemble* ens, const IbisParams* params, int* hour, int nhour,
+                            void* stream);
+
+/* Resident blocks per SM of the persistent ensemble kernel at `block` threads,
+ * for the variant params->flags selects (0 when it cannot run). */
+int ibis_ensemble_occupancy(const IbisParams* params, int block);
+
 /* Same contract in float64 throughout (the float64 run of the reference's step). */
 int ibis_step_f64(double* prog, const double* stat, const double* forc, double* diag, double* acc, int ncell,
                   int ld, int nstep, const IbisParams* params, int* status, void* stream);

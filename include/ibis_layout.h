@@ -171,7 +171,8 @@ enum {
     IBIS_DIAG_TSNOWL = 107,  /* hydrology.tsnowl */
     IBIS_DIAG_SFLO_BOT = 108,  /* hydrology.sflo_bot */
     IBIS_DIAG_FHTOP_SNOW = 109,  /* hydrology.fhtop_snow */
-    IBIS_DIAG_COUNT = 110
+    IBIS_DIAG_FSENA = 110,  /* canopy.fsena */
+    IBIS_DIAG_COUNT = 111
 };
 
 /* ACC */
@@ -193,7 +194,41 @@ enum {
     IBIS_ACC_WSOI_MEAN = 30,  /* acc.wsoi_day, 6 planes */
     IBIS_ACC_WISOI_MEAN = 36,  /* acc.wisoi_day, 6 planes */
     IBIS_ACC_TG_MEAN = 42,  /* acc.tg_day */
-    IBIS_ACC_COUNT = 43
+    IBIS_ACC_AFSENA = 43,  /* acc.fsena */
+    IBIS_ACC_COUNT = 44
+};
+
+/* RUN */
+enum {
+    IBIS_RUN_VMAX = 0,  /* stomata_params.vmax_pft, 12 planes */
+    IBIS_RUN_COEFM = 12,  /* stomata_params.coefm, 5 planes */
+    IBIS_RUN_STRESSFAC = 17,  /* stomata_params.stressfac */
+    IBIS_RUN_SOIL_BETA_POWER = 18,  /* canopy.soil_beta_power */
+    IBIS_RUN_WLIQUMAX = 19,  /* interception.wliqumax */
+    IBIS_RUN_WLIQSMAX = 20,  /* interception.wliqsmax */
+    IBIS_RUN_WLIQLMAX = 21,  /* interception.wliqlmax */
+    IBIS_RUN_FMAX = 22,  /* interception.fmax */
+    IBIS_RUN_R_CH4 = 23,  /* methane.r_ch4 */
+    IBIS_RUN_Q10P = 24,  /* methane.q10p */
+    IBIS_RUN_Z_TAU = 25,  /* methane.z_tau */
+    IBIS_RUN_TAU_OXID = 26,  /* methane.tau_oxid */
+    IBIS_RUN_Z_WT_MAX = 27,  /* methane.z_wt_max */
+    IBIS_RUN_RWOOD = 28,  /* bgc_params.rwood */
+    IBIS_RUN_RROOT = 29,  /* bgc_params.rroot */
+    IBIS_RUN_RGROWTH = 30,  /* bgc_params.rgrowth */
+    IBIS_RUN_COUNT = 31
+};
+
+/* YEARLY */
+enum {
+    IBIS_YEARLY_AYGPPTOT = 0,  /* summary.aygpptot */
+    IBIS_YEARLY_AYNPPTOT = 1,  /* summary.aynpptot */
+    IBIS_YEARLY_ADAET = 2,  /* summary.adaet */
+    IBIS_YEARLY_AFSENA = 3,  /* acc.fsena */
+    IBIS_YEARLY_AYTRUNOF = 4,  /* summary.aytrunof */
+    IBIS_YEARLY_AYTDRAIN = 5,  /* summary.aytdrain */
+    IBIS_YEARLY_CH4 = 6,  /* acc.ch4_day */
+    IBIS_YEARLY_COUNT = 7
 };
 
 /* Parameter record of the hourly step (all double; passed by value). */

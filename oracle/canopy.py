@@ -572,6 +572,7 @@ def turvap(W, old, T, A, X, w, I, F, S, wet, stom, R, casc, P):
     v = gauss_nopivot(M, b)
     nu, ns, nl, n12, n34, nq12, nq34, ng, ni = (v[:, i] for i in range(9))
     o = dict(tu=nu, ts=ns, tl=nl, t12=n12, t34=n34, q12=nq12, q34=nq34, tg=ng, ti=ni)
+    o["fsena"] = cp * cu * (ta * A["tfac"] - n12)
     o["fsenu"] = cp * su * (wu * nu + (1.0 - wu) * tu - n12)
     o["fsens"] = cp * ss * (ws * ns + (1.0 - ws) * ts - n12)
     o["fsenl"] = cp * sl * (wl * nl + (1.0 - wl) * tl - n12)

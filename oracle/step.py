@@ -27,7 +27,7 @@ FLAG_SOIL_MEANS = 1 << 6
 
 ACC_FIELDS = {"adrain": 1, "adsnow": 1, "adaet": 1, "a10ancub": 1, "a10ancls": 1, "a10ancl3": 1,
               "a10ancl4": 1, "aynpp": 12, "aynpptot": 1, "aygpptot": 1, "aytrunof": 1, "aytdrain": 1,
-              "ch4": 1, "tsoi_mean": 6, "wsoi_mean": 6, "wisoi_mean": 6, "tg_mean": 1}
+              "ch4": 1, "tsoi_mean": 6, "wsoi_mean": 6, "wisoi_mean": 6, "tg_mean": 1, "afsena": 1}
 
 
 def new_acc(n):
@@ -238,7 +238,7 @@ def step(prog, S, F, P, acc=None):
     D.update({k: wet[k] for k in ("fwetu", "fwets", "fwetl", "rliqu", "rliqs", "rliql")})
     D.update({k: R[k] for k in ("solu", "sols", "soll", "solg", "soli", "firu", "firs", "firl",
                                 "asurd", "asuri", "topparu", "topparl", "scalcoefu", "scalcoefl")})
-    D.update({k: res[k] for k in ("firg", "firi", "firb", "fsenu", "fsens", "fsenl", "fseng", "fseni",
+    D.update({k: res[k] for k in ("firg", "firi", "firb", "fsena", "fsenu", "fsens", "fsenl", "fseng", "fseni",
                                   "fvapg", "fvapi", "ginvap", "gsuvap", "gtrans")})
     D.update(raing=casc["raing"], snowg=casc["snowg"], rhoa=A["rhoa"], consoi=consoi, hflo=hflo, heatg=heatg_avg,
              hvasug=hvasug, qglif=qglif, stresstu=stresstu, stresstl=stresstl, stressu=stressu, stressl=stressl,
@@ -329,6 +329,9 @@ def accumulate(acc, new, D, S, F, P):
     acc["aygpptot"] = acc["aygpptot"] + (gu + gl) * cf
     acc["aytrunof"] = acc["aytrunof"] + D["grunof"] * dt
     acc["aytdrain"] = acc["aytdrain"] + D["gdrain"] * dt
+    # canopy-top sensible heat of turvap (canopy_exchange.py:759), summed like
+    # the other fluxes; the reference's day loop does not keep this sum
+    acc["afsena"] = acc["afsena"] + D["fsena"] * dt
 
 
 def run_steps(prog, S, forcings, P, acc=None):

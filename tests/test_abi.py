@@ -20,3 +20,25 @@ def test_loader_sets_prototypes():
     L = lib.load()
     assert L.ibis_step_f32.restype is ctypes.c_int
     assert len(L.ibis_step_f32.argtypes) == 11
+
+
+def _c_layout(tmp_path, body):
+    import subprocess
+    src = tmp_path / "probe.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "ibis_b200.h"\nint main(void){' + body + 'return 0;}\n')
+    exe = tmp_path / "probe"
+    subprocess.run(["gcc", "-std=c99", "-I", os.path.join(lib.REPO, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
+    return [int(x) for x in out]
+
+
+def test_struct_layouts_match_ctypes(tmp_path):
+    from ibis_b200.params import IbisParamsC
+    E = lib.IbisEnsembleC
+    names = [f[0] for f in E._fields_]
+    body = 'printf("%zu %zu ", sizeof(IbisParams), sizeof(IbisEnsemble));'
+    body += "".join(f'printf("%zu ", offsetof(IbisEnsemble, {n}));' for n in names)
+    got = _c_layout(tmp_path, body)
+    assert got[0] == ctypes.sizeof(IbisParamsC)
+    assert got[1] == ctypes.sizeof(E)
+    assert got[2:] == [getattr(E, n).offset for n in names]

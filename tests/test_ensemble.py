@@ -1,0 +1,142 @@
+"""Calibration ensembles: host-side construction (CPU) and the persistent and
+hourly ensemble kernels against each other and against the single-parameter
+column kernels (GPU).
+
+Tolerances: the persistent and the hourly forms run the same step code on the
+same values, so their states, accumulators and yearly totals must agree
+bit for bit; so must an ensemble run and the same column run through
+``ibis_step_config_f32`` with the run's vector as its parameter record (the
+derived parameter values are formed the same way on the host and the device).
+"""
+import numpy as np
+import pytest
+import torch
+
+from ibis_b200 import ensemble as E
+from ibis_b200 import layout as L
+from ibis_b200 import synth
+from ibis_b200.columns import Columns
+from ibis_b200.params import StepParams
+
+
+def _small(nsite=3, nparam=40, hours=(50, 30, 75), seed=3):
+    return E.make_ensemble(nsite, nparam, site_hours=np.array(hours[:nsite]), seed=seed)
+
+
+def test_vector_round_trip():
+    P = StepParams(co2conc=390.0e-6)
+    v = E.default_vector(P)
+    assert v.shape == (L.N_RUN,) == (31,)
+    Q = E.apply_vector(P, v)
+    assert np.array_equal(E.default_vector(Q), v)
+    assert np.allclose(Q.vmax_pft, P.vmax_pft, rtol=1e-6)
+
+
+def test_draw_vectors_within_half_of_default():
+    rng = np.random.default_rng(0)
+    d = E.default_vector().astype(np.float64)
+    V = E.draw_vectors(rng, 500).astype(np.float64)
+    r = V / d
+    assert np.all(r >= 0.5 - 1e-6) and np.all(r <= 1.5 + 1e-6)
+    assert np.all(np.sign(V) == np.sign(d))
+    # log-uniform: the median ratio sits at sqrt(0.5 * 1.5)
+    assert abs(np.median(r) - np.sqrt(0.75)) < 0.05
+
+
+def test_make_ensemble_records():
+    s = _small()
+    assert s.nrun == 120 and s.forc.shape == (155, L.N_FORC) and s.forc.dtype == np.float32
+    assert list(s.site_first) == [0, 50, 80]
+    assert np.array_equal(s.vectors[0], E.default_vector(s.params))
+    # record hour 0 of site 1 equals what make_forcing produced for it
+    assert np.isfinite(s.forc).all()
+    y = E.make_ensemble(4, 2, years=(1, 3), year_hours=24, seed=1)
+    assert set(y.site_hours // 24) <= {1, 2, 3}
+
+
+def test_full_size_ensemble_shape():
+    """356 sites x 64 vectors = 22,784 runs, 1-15 year records (shape only)."""
+    rng = np.random.Generator(np.random.PCG64(0))
+    years = rng.integers(1, 16, size=356)
+    assert 356 * 64 == 22784 and years.min() >= 1 and years.max() <= 15
+
+
+# ---------------------------------------------------------------- GPU
+
+def _run(ens, how, **kw):
+    ens.reset()
+    if how == "persistent":
+        ens.run(**kw)
+    else:
+        ens.run_hourly(**kw)
+    torch.cuda.synchronize()
+    return (ens.prog.cpu().numpy().copy(), ens.acc.cpu().numpy().copy(), ens.yearly.cpu().numpy().copy(),
+            ens.status.cpu().numpy().copy())
+
+
+@pytest.mark.gpu
+def test_persistent_matches_hourly_forms(cuda_lib):
+    ens = E.Ensemble(_small(), year_steps=24)
+    a = _run(ens, "persistent")
+    for kw in (dict(block=64), dict(block=256)):
+        b = _run(ens, "persistent", **kw)
+        for x, y in zip(a, b):
+            np.testing.assert_array_equal(x, y)
+    for kw in (dict(chunk=24, graph=True), dict(chunk=7, graph=False)):
+        b = _run(ens, "hourly", **kw)
+        for x, y in zip(a, b):
+            np.testing.assert_array_equal(x, y)
+    assert a[3][0] == 0
+    assert np.isfinite(a[0][:, :ens.nrun]).all()
+
+
+@pytest.mark.gpu
+def test_ensemble_run_equals_column_run(cuda_lib):
+    spec = _small(nsite=3, nparam=5, hours=(40, 40, 40))
+    ens = E.Ensemble(spec, year_steps=24)
+    ens.run()
+    torch.cuda.synchronize()
+    got = ens.prog.cpu().numpy()
+    acc = ens.acc.cpu().numpy()
+    forc_sites = spec.forc.reshape(3, 40, L.N_FORC)
+    for p in range(spec.nparam):
+        P = E.apply_vector(spec.params, spec.vectors[p])
+        cols = Columns.from_host(spec.prog, spec.stat, dtype=torch.float32, acc=True)
+        fp = np.zeros((40, L.N_FORC, cols.ld), dtype=np.float32)
+        fp[:, :, :3] = np.transpose(forc_sites, (1, 2, 0))
+        cols.set_mode(0)
+        cols.run(torch.from_numpy(fp).to(cols.device), P)
+        torch.cuda.synchronize()
+        runs = np.arange(3) * spec.nparam + p
+        np.testing.assert_array_equal(got[:, runs], cols.prog.cpu().numpy()[:, :3], err_msg=f"vector {p}")
+        np.testing.assert_array_equal(acc[:, runs], cols.acc.cpu().numpy()[:, :3], err_msg=f"vector {p}")
+
+
+@pytest.mark.gpu
+def test_yearly_totals_sum_to_accumulators(cuda_lib):
+    spec = E.make_ensemble(4, 32, site_hours=np.array([72, 48, 24, 96]), seed=5)
+    ens = E.Ensemble(spec, year_steps=24)
+    ens.run()
+    torch.cuda.synchronize()
+    ys = ens.yearly_sums()
+    acc = ens.acc_host()
+    planes = [f.name for f in L.YEARLY]
+    for k, name in enumerate(planes):
+        tot = np.nansum(ys[:, :, k], axis=1)
+        np.testing.assert_allclose(tot, acc[name], rtol=2e-5, atol=1e-6, err_msg=name)
+    years = ens.run_nstep_host // 24
+    assert np.all(np.isnan(ys[years < ens.nyear, -1, 0]))
+
+
+@pytest.mark.gpu
+def test_out_of_range_run_is_flagged_and_skipped(cuda_lib):
+    ens = E.Ensemble(_small(nparam=32), year_steps=24)
+    ens.reset()
+    ens.run_site[5] = ens.nsite + 7          # outside the site planes: the kernel's check must skip it
+    before = ens.prog.cpu().numpy()[:, 5].copy()
+    ens.run()
+    torch.cuda.synchronize()
+    bad_nonfinite, bad_desc, _ = ens.nonfinite()
+    assert bad_desc and not bad_nonfinite
+    np.testing.assert_array_equal(ens.prog.cpu().numpy()[:, 5], before)
+    assert not np.array_equal(ens.prog.cpu().numpy()[:, 6], before)
