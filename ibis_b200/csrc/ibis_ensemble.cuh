@@ -25,19 +25,21 @@ struct EnsArgs {
     const int* run_site;
     const long long* run_forc;
     const int* run_nstep;
+    const int* run_pos;
     const int* order;
     float* yearly;
     long long forc_len;
     int nrun, ld_run, nsite, ld_site, nyear, year_steps;
+    int nwork;   // entries of order to run (nrun when order is NULL)
     int* queue;
     int* status;
 };
 
 // A run whose descriptor points outside the buffers is flagged (status bit 1)
 // and skipped, so no access leaves the caller's arrays.
-__device__ __forceinline__ bool run_ok(const EnsArgs& e, int r, int site, int nstep, long long first) {
+__device__ __forceinline__ bool run_ok(const EnsArgs& e, int r, int site, int nstep, long long first, int pos) {
     const bool ok = r >= 0 && r < e.nrun && site >= 0 && site < e.nsite && nstep >= 0 && first >= 0 &&
-                    first + nstep <= e.forc_len;
+                    first + nstep <= e.forc_len && pos >= 0;
     if (!ok && e.status) atomicOr(e.status, 2);
     return ok;
 }
@@ -126,7 +128,7 @@ __global__ void __launch_bounds__(256, 1) ensemble_kernel(const EnsArgs e, const
     Col<float>& c = reinterpret_cast<Col<float>*>(smem_raw)[threadIdx.x];
     RunQ<float>& q = reinterpret_cast<RunQ<float>*>(smem_raw + blockDim.x * sizeof(Col<float>))[threadIdx.x];
     const int lane = threadIdx.x & 31;
-    const int nitem = (e.nrun + 31) >> 5;
+    const int nitem = (e.nwork + 31) >> 5;
     const bool kahan = (P.flags & IBIS_FLAG_KAHAN) != 0;
     const Diag<float> D{nullptr, 0};
     for (;;) {
@@ -135,19 +137,21 @@ __global__ void __launch_bounds__(256, 1) ensemble_kernel(const EnsArgs e, const
         item = __shfl_sync(0xffffffffu, item, 0);
         if (item >= nitem) break;
         const int idx = item * 32 + lane;
-        const int r = idx < e.nrun ? (e.order ? __ldg(e.order + idx) : idx) : -1;
+        const int r = idx < e.nwork ? (e.order ? __ldg(e.order + idx) : idx) : -1;
         const bool in = r >= 0 && r < e.nrun;
         const int site = in ? __ldg(e.run_site + r) : -1;
         const int nstep = in ? __ldg(e.run_nstep + r) : 0;
         const long long first = in ? __ldg(e.run_forc + r) : -1;
-        if (idx < e.nrun && run_ok(e, r, site, nstep, first)) {
+        const int pos = in && e.run_pos ? __ldg(e.run_pos + r) : 0;
+        if (idx < e.nwork && run_ok(e, r, site, nstep, first, pos)) {
             const float* f = e.forc + (size_t)first * IBIS_FORC_COUNT;
             load_col(c, e.prog + r, e.ld_run);
             load_run_params(q, e.run_params + r, e.ld_run, P);
             const Stat<float> S{e.stat + site, e.ld_site};
             const Acc<float> A{e.acc ? e.acc + r : nullptr, e.ld_run, kahan};
-            int next_year = e.year_steps;
-            int year = 0;
+            // steps of this call until the run's next year end, and that year's index
+            int next_year = e.year_steps - pos % e.year_steps;
+            int year = pos / e.year_steps;
 #pragma unroll 1
             for (int s = 0; s < nstep; ++s) {
                 const Forc<float> F = load_forc_record(f + (size_t)s * IBIS_FORC_COUNT);
@@ -178,7 +182,8 @@ __global__ void __launch_bounds__(128, 2) ensemble_hour_kernel(const EnsArgs e, 
     if (hour >= nstep) return;
     const int site = __ldg(e.run_site + r);
     const long long first = __ldg(e.run_forc + r);
-    if (!run_ok(e, r, site, nstep, first)) return;
+    const int pos = e.run_pos ? __ldg(e.run_pos + r) : 0;
+    if (!run_ok(e, r, site, nstep, first, pos)) return;
     extern __shared__ unsigned char smem_raw[];
     Col<float>& c = reinterpret_cast<Col<float>*>(smem_raw)[threadIdx.x];
     RunQ<float>& q = reinterpret_cast<RunQ<float>*>(smem_raw + blockDim.x * sizeof(Col<float>))[threadIdx.x];
@@ -188,8 +193,8 @@ __global__ void __launch_bounds__(128, 2) ensemble_hour_kernel(const EnsArgs e, 
     const Acc<float> A{e.acc ? e.acc + r : nullptr, e.ld_run, (P.flags & IBIS_FLAG_KAHAN) != 0};
     const Forc<float> F = load_forc_record(e.forc + (size_t)(first + hour) * IBIS_FORC_COUNT);
     column_step<float, NT, SU, SL>(c, F, S, Diag<float>{nullptr, 0}, A, P, q);
-    if (e.yearly && (hour + 1) % e.year_steps == 0) {
-        const int y = (hour + 1) / e.year_steps - 1;
+    if (e.yearly && (pos + hour + 1) % e.year_steps == 0) {
+        const int y = (pos + hour + 1) / e.year_steps - 1;
         if (y < e.nyear) yearly_snapshot(e, A, r, y);
     }
     flag_nonfinite(e, store_col(c, e.prog + r, e.ld_run), r);
@@ -201,11 +206,21 @@ constexpr int kEnsHourBlock = 128;
 
 inline size_t ens_smem(int block) { return (size_t)block * (sizeof(Col<float>) + sizeof(RunQ<float>)); }
 
+// Both ensemble kernels keep state and parameters in shared memory: ask for the
+// largest shared-memory carveout so the driver never picks a split with fewer
+// resident blocks (the choice is otherwise left to the driver per launch).
+template <typename K>
+cudaError_t ens_attributes(K k, size_t smem) {
+    cudaError_t err = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) return err;
+    return cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+}
+
 template <int NT, bool SU, bool SL>
 cudaError_t launch_ensemble(const EnsArgs& e, const DevParams<float>& P, int block, int grid, cudaStream_t s) {
     auto k = ensemble_kernel<NT, SU, SL>;
     const size_t smem = ens_smem(block);
-    cudaError_t err = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ens_smem(256));
+    cudaError_t err = ens_attributes(k, ens_smem(256));
     if (err != cudaSuccess) return err;
     k<<<grid, block, smem, s>>>(e, P);
     return cudaGetLastError();
@@ -216,10 +231,8 @@ cudaError_t launch_ensemble_hours(const EnsArgs& e, const DevParams<float>& P, i
                                   cudaStream_t s) {
     auto k = ensemble_hour_kernel<NT, SU, SL>;
     const size_t smem = ens_smem(kEnsHourBlock);
-    if (smem > 48 * 1024) {
-        cudaError_t err = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (err != cudaSuccess) return err;
-    }
+    cudaError_t err = ens_attributes(k, smem);
+    if (err != cudaSuccess) return err;
     const int grid = (e.nrun + kEnsHourBlock - 1) / kEnsHourBlock;
     for (int h = 0; h < nhour; ++h) k<<<grid, kEnsHourBlock, smem, s>>>(e, P, hour0, h);
     advance_hour<<<1, 1, 0, s>>>(hour0, nhour);
@@ -231,8 +244,7 @@ template <int NT, bool SU, bool SL>
 int ensemble_occupancy(int block) {
     int n = 0;
     auto k = ensemble_kernel<NT, SU, SL>;
-    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ens_smem(256)) != cudaSuccess)
-        return 0;
+    if (ens_attributes(k, ens_smem(256)) != cudaSuccess) return 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, block, ens_smem(block)) != cudaSuccess) return 0;
     return n;
 }

@@ -26,7 +26,8 @@ constexpr unsigned kEnsFlags = IBIS_FLAG_BEDROCK | IBIS_FLAG_H2O_CONSISTENT | IB
 // Validate an ensemble description; fills `a`.  Returns 0, or -EINVAL.
 int ens_args(const IbisEnsemble* e, const IbisParams* hp, EnsArgs& a) {
     if (!e || !hp) return -EINVAL;
-    if (e->nrun < 0 || e->nsite < 0 || e->forc_len < 0) return -EINVAL;
+    if (e->nrun < 0 || e->nsite < 0 || e->forc_len < 0 || (e->order && (e->norder < 0 || e->norder > e->nrun)))
+        return -EINVAL;
     if (e->nrun == 0) return 0;
     if (!e->prog || !e->stat || !e->forc || !e->run_params || !e->run_site || !e->run_forc || !e->run_nstep)
         return -EINVAL;
@@ -47,6 +48,7 @@ int ens_args(const IbisEnsemble* e, const IbisParams* hp, EnsArgs& a) {
     a.run_site = e->run_site;
     a.run_forc = e->run_forc;
     a.run_nstep = e->run_nstep;
+    a.run_pos = e->run_pos;
     a.order = e->order;
     a.yearly = e->yearly;
     a.forc_len = e->forc_len;
@@ -56,6 +58,7 @@ int ens_args(const IbisEnsemble* e, const IbisParams* hp, EnsArgs& a) {
     a.ld_site = e->ld_site;
     a.nyear = e->nyear;
     a.year_steps = e->year_steps > 0 ? e->year_steps : 1;
+    a.nwork = e->order ? e->norder : e->nrun;
     a.queue = e->queue;
     a.status = e->status;
     return 0;
@@ -99,7 +102,8 @@ extern "C" int ibis_ensemble_f32(const IbisEnsemble* ens, const IbisParams* para
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0)
         return -ENODEV;
-    const int nitem = (a.nrun + 31) / 32;
+    if (a.nwork == 0) return 0;
+    const int nitem = (a.nwork + 31) / 32;
     if (block == 0) {
         const int w = (nitem + sms - 1) / sms;          // warps per SM that cover every item in one pass
         block = 32 * (w < 1 ? 1 : (w > 8 ? 8 : w));

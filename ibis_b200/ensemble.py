@@ -199,10 +199,10 @@ class Ensemble:
         p = lambda t: ctypes.c_void_p(t.data_ptr()) if t is not None else None
         return IbisEnsembleC(prog=p(self.prog), acc=p(self.acc), stat=p(self.stat), forc=p(self.forc),
                              run_params=p(self.run_params), run_site=p(self.run_site), run_forc=p(self.run_forc),
-                             run_nstep=p(self.run_nstep), order=p(self.order), yearly=p(self.yearly),
-                             forc_len=int(self.forc.shape[0]), nrun=self.nrun, ld_run=self.ld_run,
-                             nsite=self.nsite, ld_site=self.ld_site, nyear=self.nyear, year_steps=self.year_steps,
-                             queue=p(self.queue), status=p(self.status))
+                             run_nstep=p(self.run_nstep), run_pos=None, order=p(self.order),
+                             yearly=p(self.yearly), forc_len=int(self.forc.shape[0]), nrun=self.nrun,
+                             ld_run=self.ld_run, nsite=self.nsite, ld_site=self.ld_site, nyear=self.nyear,
+                             year_steps=self.year_steps, norder=self.nrun, queue=p(self.queue), status=p(self.status))
 
     # ------------------------------------------------------------------ runs
     def reset(self):

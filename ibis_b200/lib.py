@@ -22,10 +22,11 @@ class IbisEnsembleC(ctypes.Structure):
     """ctypes mirror of ``IbisEnsemble`` (include/ibis_b200.h)."""
     _fields_ = [("prog", ctypes.c_void_p), ("acc", ctypes.c_void_p), ("stat", ctypes.c_void_p),
                 ("forc", ctypes.c_void_p), ("run_params", ctypes.c_void_p), ("run_site", ctypes.c_void_p),
-                ("run_forc", ctypes.c_void_p), ("run_nstep", ctypes.c_void_p), ("order", ctypes.c_void_p),
-                ("yearly", ctypes.c_void_p), ("forc_len", ctypes.c_longlong), ("nrun", ctypes.c_int),
-                ("ld_run", ctypes.c_int), ("nsite", ctypes.c_int), ("ld_site", ctypes.c_int),
-                ("nyear", ctypes.c_int), ("year_steps", ctypes.c_int), ("queue", ctypes.c_void_p),
+                ("run_forc", ctypes.c_void_p), ("run_nstep", ctypes.c_void_p), ("run_pos", ctypes.c_void_p),
+                ("order", ctypes.c_void_p), ("yearly", ctypes.c_void_p), ("forc_len", ctypes.c_longlong),
+                ("nrun", ctypes.c_int), ("ld_run", ctypes.c_int), ("nsite", ctypes.c_int),
+                ("ld_site", ctypes.c_int), ("nyear", ctypes.c_int), ("year_steps", ctypes.c_int),
+                ("norder", ctypes.c_int), ("queue", ctypes.c_void_p),
                 ("status", ctypes.c_void_p)]
 
 

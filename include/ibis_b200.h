@@ -93,7 +93,12 @@ int ibis_step_split_noalloc_f32(float* prog, const float* stat, const float* for
  *   run_params  [IBIS_RUN_COUNT][ld_run]        in: calibration vector of every run
  *   run_site    [nrun]  site of the run; run_forc [nrun] index of its first record
  *   run_nstep   [nrun]  hours in its record (records run_forc .. run_forc+nstep-1)
- *   order       [nrun] or NULL: order in which runs are taken (longest first is best)
+ *   run_pos     [nrun] or NULL: hours each run completed before this call (its
+ *               records start at run_forc regardless; run_pos only places the
+ *               year ends of the yearly totals), NULL = 0
+ *   order       [norder] or NULL: the runs to advance, in the order they are
+ *               taken (longest first is best); NULL = all nrun runs in index order
+ *   norder      entries of order (ignored when order is NULL)
  *   yearly      [nyear][IBIS_YEARLY_COUNT][ld_run] or NULL: running totals of the
  *               IBIS_YEARLY accumulators at the end of each year_steps hours
  *   queue       device int used as the work counter (reset by the call)
@@ -110,10 +115,11 @@ typedef struct IbisEnsemble {
     const int* run_site;
     const long long* run_forc;
     const int* run_nstep;
+    const int* run_pos;
     const int* order;
     float* yearly;
     long long forc_len;
-    int nrun, ld_run, nsite, ld_site, nyear, year_steps;
+    int nrun, ld_run, nsite, ld_site, nyear, year_steps, norder;
     int* queue;
     int* status;
 } IbisEnsemble;
@@ -128,7 +134,8 @@ int ibis_ensemble_f32(const IbisEnsemble* ens, const IbisParams* params, int blo
 /* The same runs advanced `nhour` hours in nhour launches (one per hour), from
  * the hour held in the device int *hour, which the last launch advances by
  * nhour: a fixed sequence that can be captured once in a CUDA graph and
- * replayed until every record has ended. */
+ * replayed until every record has ended.  Every run r < nrun whose record
+ * covers the hour takes its step (order is not used). */
 int ibis_ensemble_hours_f32(const IbisEnsemble* ens, const IbisParams* params, int* hour, int nhour,
                             void* stream);
 
