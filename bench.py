@@ -50,7 +50,9 @@ def _algorithmic_bytes(nhours):
     and written."""
     from ibis_b200 import layout as L
     prog = 2 * L.N_PROG * 4
-    stat_planes = (10 * 6) + 3 + 8 + 2 + 12 + 3 + 10 + 12 + 3   # planes column_step reads (see DESIGN.md)
+    # static planes the step reads: 10 soil fields x 6 layers, albedos/z0, canopy structure (8),
+    # fu/fl, frac, exist/sapfrac/CH4 inputs, cbiow (10 used), cbior, root weights
+    stat_planes = (10 * 6) + 3 + 8 + 2 + 12 + 3 + 10 + 12 + 3
     acc_planes = 23 + 1                                          # ACC + CH4 value planes
     acc = 2 * 2 * acc_planes * 4
     return prog + stat_planes * 4 + acc + nhours * L.N_FORC * 4
@@ -305,8 +307,109 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_ensemble(args):
+    """The calibration ensemble: 356 sites x 64 parameter vectors (22,784 runs),
+    records of U{1..15} years, one step = every run over its whole record.  The
+    persistent launch is timed; the same runs with one launch per hour (eager and
+    replayed from a CUDA graph) are timed beside it."""
+    import torch
+    from ibis_b200 import ensemble as E
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    t0 = time.time()
+    hours = None if args.record_hours is None else np.full(args.sites, args.record_hours)
+    spec = E.make_ensemble(args.sites, args.params_per_site, years=(1, 15), seed=7, site_hours=hours)
+    gen_s = time.time() - t0
+    ens = E.Ensemble(spec)
+    stream = torch.cuda.current_stream()
+    tuned = ens.tune(blocks=[96, 128, 160, 192, 256]) if args.tune else None
+    block = tuned["best"] if tuned else 0
+
+    def timed(fn, k):
+        out = []
+        for _ in range(k):
+            ens.reset()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+            out.append(a.elapsed_time(b))
+        return out
+
+    with ClockSampler(local) as clk:
+        timed(lambda: ens.run(block=block), args.warmup)
+        ms = timed(lambda: ens.run(block=block), args.steps)
+    nonfinite = ens.nonfinite()
+    ms_graph = timed(lambda: ens.run_hourly(chunk=24, graph=True), 1 + args.steps)[1:]
+    ms_eager = timed(lambda: ens.run_hourly(chunk=24, graph=False), args.steps)
+    cs = ens.cell_steps()
+    m = float(np.mean(ms))
+    line = {
+        "metric": "cell-steps/s, calibration ensemble (persistent launch)", "value": cs / (m / 1e3),
+        "unit": "cell-steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": m,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{args.sites} sites x {args.params_per_site} parameter vectors = {ens.nrun} runs, "
+                               + ("records U{1..15} years of hourly forcing" if hours is None
+                                  else f"records of {args.record_hours} hours")
+                               + ", one step = every run to the end of its record",
+                   "cell_steps_per_step": cs, "longest_record_hours": int(ens.run_nstep_host.max()),
+                   "block": block or "auto", "tuned_ms": tuned["ms"] if tuned else None,
+                   "forcing_gb": ens.forc.numel() * 4 / 1e9, "generation_s": gen_s,
+                   "l2": "inputs (1.2 GB of forcing records) larger than L2"},
+        "hourly_graph": {"value": cs / (float(np.mean(ms_graph)) / 1e3), "ms_per_step": float(np.mean(ms_graph)),
+                         "launches_per_step": int(ens.run_nstep_host.max()),
+                         "note": "one launch per hour, 24-hour CUDA graph replayed"},
+        "hourly_eager": {"value": cs / (float(np.mean(ms_eager)) / 1e3), "ms_per_step": float(np.mean(ms_eager))},
+        "persistent_vs_hourly_graph": float(np.mean(ms_graph)) / m,
+        "gpu_launches": args.steps,
+        "clocks": clk.summary(), "nonfinite_runs": nonfinite[0], "bad_descriptors": nonfinite[1],
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_serve(args):
+    """The request loop: Poisson arrivals (50/s by default) of requests for
+    U{1..64} of 356 resident tower sites, U{1..10} years, one calibration vector
+    each, continuously batched into the resident ensemble; p50/p99 latency."""
+    import torch
+    from ibis_b200 import serve as S
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    t0 = time.time()
+    lib = S.SiteLibrary(args.sites, 10, seed=3)
+    gen_s = time.time() - t0
+    srv = S.Server(lib, budget_bytes=150e9, epoch_hours=args.epoch_hours)
+    srv.serve(S.poisson_requests(np.random.default_rng(1), args.rate, 0.2, args.sites, max_years=1))
+    reqs = S.poisson_requests(np.random.default_rng(5), args.rate, args.duration, args.sites)
+    with ClockSampler(local) as clk:
+        st = srv.serve(reqs)
+    line = {
+        "metric": "serve p50/p99 request latency", "value": st["p50_s"], "unit": "s", "p99_s": st["p99_s"],
+        "n_gpus": 1, "steps": st["requests"], "warmup": 1, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "throughput": {"value": st["cell_steps_per_s"], "unit": "cell-steps/s", "cell_steps": st["cell_steps"]},
+        "config": {"workload": f"Poisson {args.rate}/s requests for {args.duration} s, 1-64 of {args.sites} sites, "
+                               "1-10 years, one 31-value vector each", "epoch_hours": st["epoch_hours"],
+                   "slots": st["slots"], "budget_gb": 150, "library_gb": lib.nbytes / 1e9,
+                   "library_generation_s": gen_s},
+        "epochs": st["epochs"], "gpu_launches": st["epochs"], "clocks": clk.summary(), "status": st["status"],
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="day", choices=["day", "ensemble", "serve"])
+    ap.add_argument("--sites", type=int, default=356)
+    ap.add_argument("--params-per-site", type=int, default=64)
+    ap.add_argument("--tune", action="store_true", help="ensemble: autotune the block size first")
+    ap.add_argument("--record-hours", type=int, default=None, help="ensemble: every record this long (profiling)")
+    ap.add_argument("--rate", type=float, default=50.0)
+    ap.add_argument("--duration", type=float, default=10.0)
+    ap.add_argument("--epoch-hours", type=int, default=168)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
@@ -319,6 +422,10 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "ensemble":
+        run_ensemble(args)
+    elif args.workload == "serve":
+        run_serve(args)
     else:
         run_ours(args)
 
