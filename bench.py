@@ -53,7 +53,7 @@ def _algorithmic_bytes(nhours):
     # static planes the step reads: 10 soil fields x 6 layers, albedos/z0, canopy structure (8),
     # fu/fl, frac, exist/sapfrac/CH4 inputs, cbiow (10 used), cbior, root weights
     stat_planes = (10 * 6) + 3 + 8 + 2 + 12 + 3 + 10 + 12 + 3
-    acc_planes = 23 + 1                                          # ACC + CH4 value planes
+    acc_planes = 24 + 1                                          # FLAG_ACC planes + CH4 value plane
     acc = 2 * 2 * acc_planes * 4
     return prog + stat_planes * 4 + acc + nhours * L.N_FORC * 4
 

@@ -206,21 +206,11 @@ constexpr int kEnsHourBlock = 128;
 
 inline size_t ens_smem(int block) { return (size_t)block * (sizeof(Col<float>) + sizeof(RunQ<float>)); }
 
-// Both ensemble kernels keep state and parameters in shared memory: ask for the
-// largest shared-memory carveout so the driver never picks a split with fewer
-// resident blocks (the choice is otherwise left to the driver per launch).
-template <typename K>
-cudaError_t ens_attributes(K k, size_t smem) {
-    cudaError_t err = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (err != cudaSuccess) return err;
-    return cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-}
-
 template <int NT, bool SU, bool SL>
 cudaError_t launch_ensemble(const EnsArgs& e, const DevParams<float>& P, int block, int grid, cudaStream_t s) {
     auto k = ensemble_kernel<NT, SU, SL>;
     const size_t smem = ens_smem(block);
-    cudaError_t err = ens_attributes(k, ens_smem(256));
+    cudaError_t err = fit_smem(k, block, smem, ens_smem(256));
     if (err != cudaSuccess) return err;
     k<<<grid, block, smem, s>>>(e, P);
     return cudaGetLastError();
@@ -231,7 +221,8 @@ cudaError_t launch_ensemble_hours(const EnsArgs& e, const DevParams<float>& P, i
                                   cudaStream_t s) {
     auto k = ensemble_hour_kernel<NT, SU, SL>;
     const size_t smem = ens_smem(kEnsHourBlock);
-    cudaError_t err = ens_attributes(k, smem);
+    static unsigned long long fitted = 0;
+    cudaError_t err = fit_smem_once(fitted, k, kEnsHourBlock, smem, smem);
     if (err != cudaSuccess) return err;
     const int grid = (e.nrun + kEnsHourBlock - 1) / kEnsHourBlock;
     for (int h = 0; h < nhour; ++h) k<<<grid, kEnsHourBlock, smem, s>>>(e, P, hour0, h);
@@ -244,7 +235,7 @@ template <int NT, bool SU, bool SL>
 int ensemble_occupancy(int block) {
     int n = 0;
     auto k = ensemble_kernel<NT, SU, SL>;
-    if (ens_attributes(k, ens_smem(256)) != cudaSuccess) return 0;
+    if (fit_smem(k, block, ens_smem(block), ens_smem(256)) != cudaSuccess) return 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, block, ens_smem(block)) != cudaSuccess) return 0;
     return n;
 }

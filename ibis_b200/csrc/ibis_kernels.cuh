@@ -262,13 +262,52 @@ static DevParams<R> make_dev_params(const IbisParams& h) {
     return d;
 }
 
+// The SM's 256 KB unified array is split between shared memory and L1, and L1
+// caches the register spills of these kernels.  Ask for the smallest
+// shared-memory carveout that holds `smem` bytes for every block the register
+// budget lets reside (228 KB of shared memory per SM on sm_100, 1 KB reserved
+// per block), so the rest stays L1, and allow `smem_max` dynamic bytes.
+template <typename K>
+cudaError_t fit_smem(K k, int block, size_t smem, size_t smem_max) {
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, k);
+    if (e != cudaSuccess) return e;
+    const int regs = (fa.numRegs + 7) / 8 * 8;
+    int blocks = regs > 0 ? 65536 / (block * regs) : 32;
+    blocks = blocks < 1 ? 1 : (blocks > 32 ? 32 : blocks);
+    const size_t per_sm = 228 * 1024;
+    const size_t need = (smem + fa.sharedSizeBytes + 1024) * (size_t)blocks;
+    int pct = (int)((need * 100 + per_sm - 1) / per_sm);
+    pct = pct > 100 ? 100 : pct;
+    if (smem_max > 48 * 1024) {
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+}
+
+// fit_smem once per kernel instantiation and device (`done` is the caller's
+// per-instantiation bit set; a repeated call is harmless).
+template <typename K>
+cudaError_t fit_smem_once(unsigned long long& done, K k, int block, size_t smem, size_t smem_max) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return fit_smem(k, block, smem, smem_max);
+    const unsigned long long bit = 1ull << dev;
+    if (done & bit) return cudaSuccess;
+    cudaError_t e = fit_smem(k, block, smem, smem_max);
+    if (e == cudaSuccess) done |= bit;
+    return e;
+}
+
 template <typename R, int NT, bool SU, bool SL, int BLOCK, int MINB>
 cudaError_t launch_fused(R* prog, const R* stat, const R* forc, R* diag, R* acc, int ncell, int ld, int nstep,
                          long long fstride, const DevParams<R>& P, int* status, cudaStream_t s) {
     const int grid = (ncell + BLOCK - 1) / BLOCK;
     const size_t smem = StateInSmem<R>::value ? BLOCK * sizeof(Col<R>) : 0;
     auto k = hourly_step_kernel<R, NT, SU, SL, BLOCK, MINB>;
-    if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    static unsigned long long fitted = 0;
+    cudaError_t e = fit_smem_once(fitted, k, BLOCK, smem, smem);
+    if (e != cudaSuccess) return e;
     k<<<grid, BLOCK, smem, s>>>(prog, stat, forc, diag, acc, ncell, ld, nstep, fstride, P, status);
     return cudaGetLastError();
 }
@@ -281,8 +320,10 @@ cudaError_t launch_split(R* prog, const R* stat, const R* forc, R* diag, R* acc,
     const size_t sm2 = StateInSmem<R>::value ? B2 * sizeof(Col<R>) : 0;
     auto k1 = surface_kernel<R, SU, SL, B1, M1>;
     auto k2 = ground_kernel<R, NT, B2, M2>;
-    if (sm1 > 48 * 1024) cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
-    if (sm2 > 48 * 1024) cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
+    static unsigned long long fitted1 = 0, fitted2 = 0;
+    cudaError_t e = fit_smem_once(fitted1, k1, B1, sm1, sm1);
+    if (e == cudaSuccess) e = fit_smem_once(fitted2, k2, B2, sm2, sm2);
+    if (e != cudaSuccess) return e;
     for (int h = 0; h < nstep; ++h) {
         const R* f = forc + (size_t)h * fstride;
         k1<<<g1, B1, sm1, s>>>(prog, stat, f, diag, mid, ncell, ld, P);

@@ -1,0 +1,218 @@
+"""Drop-in for the reference's step function over its own state pytrees.
+
+The reference's hot path is one pure function,
+
+    timestep_body(state, consts, params, dtime) -> state
+
+(python-port/ibis/timestepping/loops.py:234-284) over Equinox pytrees:
+``IBISState`` (state/model_state.py:28-63), ``PhysicalConstants``
+(constants.py:16-80) and ``SimParams`` (loops.py:72-134).  It has no operator,
+plugin or FFI layer.  :func:`timestep_body` here has the same signature and
+meaning: it reads the leaves the step needs from those objects (by attribute
+path, so any object with the same paths works), advances them one hour with
+the CUDA kernels, and returns a state of the same structure whose prognostic
+leaves are the new values and whose diagnostic leaves are the ones
+``timestep_body`` writes (loops.py:1158-1241).  Float64 leaves run the float64
+kernels; float32 leaves the production FP32 kernels.
+
+:func:`run_hours` is the multi-hour form with the day loop's accumulators
+(``_run_day_inner._step_body``, loops_gswp3.py:115-320): one launch for all
+hours, forcing given as arrays instead of the reference's weather generator.
+
+The leaves are copied to and from the device on every call (the reference's
+contract is a host-visible pytree); :class:`ibis_b200.columns.Columns` keeps
+state resident for callers that can.
+"""
+from __future__ import annotations
+
+import copy
+import dataclasses
+import os
+
+import numpy as np
+import torch
+
+from . import layout as L
+from .columns import Columns
+from .params import (FLAG_ACC, FLAG_BEDROCK, FLAG_CH4, FLAG_H2O_CONSISTENT, FLAG_SOIL_MEANS, FLAG_SUNSHADE_L,
+                     FLAG_SUNSHADE_U, StepParams)
+
+# Where each parameter of the flat record lives in the reference's objects.
+# Roots: consts (PhysicalConstants), params (SimParams), state (IBISState).
+PARAM_PATHS = {
+    **{k: f"consts.{k}" for k in ("stef", "vonk", "grav", "tmelt", "hvap", "hfus", "hsub", "ch2o", "cice", "cair",
+                                  "cvap", "rair", "rvap", "cappa", "rhow", "epsilon")},
+    "co2conc": "state.atm.co2conc",
+    **{k: f"state.snow.{k}" for k in ("z0sno", "rhos", "consno", "hsnotop", "hsnomin", "fimin", "fimax")},
+    **{k: f"params.veg_rad.{k}" for k in ("rhoveg", "tauveg", "oriev", "orieh")},
+    **{k: f"params.canopy.{k}" for k in ("cleaf", "cstem", "cgrass", "dleaf", "dstem", "alaiml", "alaimu", "chu",
+                                         "chs", "chl", "soil_beta_power")},
+    **{k: f"params.interception.{k}" for k in ("wliqumax", "wliqsmax", "wliqlmax", "wsnoumax", "wsnosmax",
+                                               "wsnolmax", "tdripu", "tdrips", "tdripl", "tblowu", "tblows",
+                                               "tblowl", "fmax")},
+    **{k: f"params.stomata_params.{k}" for k in ("tau15", "kc15", "ko15", "cimax", "o2conc", "alpha3", "theta3",
+                                                 "beta3", "alpha4", "theta4", "beta4", "gamma", "coefm", "coefb",
+                                                 "gsmin", "vmax_pft", "stressfac", "cap_kn")},
+    **{k: f"params.{k}" for k in ("wpudmax", "zwpmax", "bperm", "rhosoi_val", "csoi_mineral_val")},
+    "hsoi": "state.soil.hsoi",
+    "froot": "state.vegetation.froot",
+    "hsoi_bed": "params.bedrock.hsoi", "consoi_bed": "params.bedrock.consoi",
+    "rhosoi_bed": "params.bedrock.rhosoi", "csoi_bed": "params.bedrock.csoi",
+    **{k: f"params.fire.{k}" for k in ("d_crit", "vpd_ref", "d_crit_vpd")},
+    **{k: f"params.methane.{k}" for k in ("sat_crit", "z_max", "r_ch4", "q10p", "t_ref", "z_wt_max", "z_wt_ref",
+                                          "z_tau", "tau_oxid")},
+    **{k: f"params.bgc_params.{k}" for k in ("rwood", "rroot", "rgrowth")},
+}
+# Not parameters of the reference objects: omegasno is a module constant of the
+# radiation code (radiation.py:393, _OMEGASNO); flux_max and t_max_dev are read
+# from the environment when the step is traced (loops.py:665, 1143); dtime and
+# the year length are arguments.
+_ENV = {"flux_max": ("IBIS_FLUX_MAX", 2000.0), "t_max_dev": ("IBIS_T_MAX_DEV", 40.0)}
+
+
+def _get(roots: dict, path: str):
+    root, *rest = path.split(".")
+    obj = roots[root]
+    for part in rest:
+        if obj is None:
+            return None
+        obj = getattr(obj, part, None)
+    return obj
+
+
+def _replace(obj, name, value):
+    """A copy of ``obj`` with attribute ``name`` set (dataclass / eqx.Module,
+    NamedTuple, or plain object)."""
+    if dataclasses.is_dataclass(obj) and not isinstance(obj, type):
+        try:
+            return dataclasses.replace(obj, **{name: value})
+        except (TypeError, ValueError):
+            pass
+    if hasattr(obj, "_replace") and hasattr(obj, "_fields"):
+        return obj._replace(**{name: value})
+    new = copy.copy(obj)
+    object.__setattr__(new, name, value)
+    return new
+
+
+def tree_set(root, path: str, value):
+    """``root`` with the leaf at dotted ``path`` replaced (like ``eqx.tree_at``)."""
+    head, _, tail = path.partition(".")
+    if not tail:
+        return _replace(root, head, value)
+    return _replace(root, head, tree_set(getattr(root, head), tail, value))
+
+
+def step_params(state, consts, params, dtime: float, ndaypy: float = 365.0) -> StepParams:
+    """The flat parameter record (and variant flags) equivalent to the reference objects."""
+    roots = {"state": state, "consts": consts, "params": params}
+    P = StepParams()
+    for name, path in PARAM_PATHS.items():
+        v = _get(roots, path)
+        if v is None:
+            continue
+        n = np.size(getattr(P, name))
+        arr = np.asarray(v, dtype=np.float64).reshape(-1)
+        if name == "hsoi":
+            arr = arr[:L.NSOILAY]
+        if n > 1 and arr.size == 1:
+            arr = np.full(n, arr[0])
+        setattr(P, name, arr if n > 1 else float(arr[0]))
+    for name, (env, default) in _ENV.items():
+        setattr(P, name, float(os.environ.get(env, default)))
+    P.dtime = float(dtime)
+    P.ndaypy = float(ndaypy)
+    flags = 0
+    if getattr(state.soil, "tsoi_deep", None) is not None:
+        flags |= FLAG_BEDROCK
+    if bool(getattr(params, "h2o_consistent_weights", False)):
+        flags |= FLAG_H2O_CONSISTENT
+    sp = getattr(params, "stomata_params", None)
+    if bool(getattr(sp, "sunshade_u", False)):
+        flags |= FLAG_SUNSHADE_U
+    if bool(getattr(sp, "sunshade_l", False)):
+        flags |= FLAG_SUNSHADE_L
+    P.flags = flags
+    return P
+
+
+def _leaf_dict(state, group, ncell):
+    out = {}
+    for f in L.GROUPS[group]:
+        v = _get({"state": state}, "state." + f.leaf)
+        if v is None:
+            continue
+        a = np.asarray(v, dtype=np.float64)
+        if a.ndim == 0:
+            a = np.full(ncell, float(a))
+        out[f.name] = a
+    return out
+
+
+def _dtype_of(state):
+    return torch.float32 if np.asarray(state.soil.tg).dtype == np.float32 else torch.float64
+
+
+def _write_back(state, values: dict, group: str, dtype):
+    np_dtype = np.float32 if dtype == torch.float32 else np.float64
+    for f in L.GROUPS[group]:
+        if f.name not in values:
+            continue
+        old = _get({"state": state}, "state." + f.leaf)
+        if old is None:          # a leaf this state does not carry (no bedrock, extra diagnostics)
+            continue
+        v = np.asarray(values[f.name]).astype(np_dtype)
+        if old is not None and np.ndim(old) == 0:
+            v = np_dtype(v.reshape(-1)[0])
+        state = tree_set(state, f.leaf, v)
+    return state
+
+
+def timestep_body(state, consts, params, dtime: float, device="cuda"):
+    """One hourly step of ``state`` (same contract as the reference's ``timestep_body``)."""
+    P = step_params(state, consts, params, dtime)
+    ncell = int(np.asarray(state.soil.tg).shape[0])
+    dtype = _dtype_of(state)
+    prog = _leaf_dict(state, "PROG", ncell)
+    stat = _leaf_dict(state, "STAT", ncell)
+    forc = {k: v[None] for k, v in _leaf_dict(state, "FORC", ncell).items()}
+    cols = Columns.from_host(prog, stat, dtype=dtype, device=device, diag=True, acc=False)
+    cols.run(cols.forcing(forc), P)
+    torch.cuda.synchronize(cols.device)
+    status = cols.nonfinite()
+    state = _write_back(state, cols.prog_host(), "PROG", dtype)
+    state = _write_back(state, cols.diag_host(), "DIAG", dtype)
+    if status[0]:
+        import warnings
+        warnings.warn(f"non-finite state after the step (first cell {status[1]})", RuntimeWarning)
+    return state
+
+
+def run_hours(state, consts, params, forcing: dict, dtime: float, ch4_inund=None, soil_means: bool = False,
+              ndaypy: float = 365.0, acc=None, device="cuda"):
+    """``nhour`` hourly steps with the day loop's accumulators, in one launch.
+
+    ``forcing`` maps the ``atm`` leaf names of ``layout.FORC`` to (nhour, ncell[, k])
+    arrays.  ``ch4_inund`` (per-cell inundated fraction) turns on the hourly
+    wetland CH4 accumulator.  ``acc`` is a previous return value to continue
+    from.  Returns ``(state, acc)`` with ``acc`` a dict of the ``layout.ACC``
+    accumulators (value and Kahan planes kept for continuation)."""
+    P = step_params(state, consts, params, dtime, ndaypy)
+    P.flags = P.flags | FLAG_ACC | (FLAG_CH4 if ch4_inund is not None else 0) | (FLAG_SOIL_MEANS if soil_means else 0)
+    ncell = int(np.asarray(state.soil.tg).shape[0])
+    dtype = _dtype_of(state)
+    if dtype == torch.float64:
+        P.flags = P.flags & ~(1 << 8)        # plain sums in float64
+    prog = _leaf_dict(state, "PROG", ncell)
+    stat = _leaf_dict(state, "STAT", ncell)
+    if ch4_inund is not None:
+        stat["f_inund"] = np.asarray(ch4_inund, dtype=np.float64)
+    cols = Columns.from_host(prog, stat, dtype=dtype, device=device, acc=True)
+    if acc is not None:
+        cols.acc.copy_(torch.as_tensor(acc["_planes"], dtype=dtype))
+    cols.run(cols.forcing(forcing), P)
+    torch.cuda.synchronize(cols.device)
+    state = _write_back(state, cols.prog_host(), "PROG", dtype)
+    out = cols.acc_host(compensated=True)
+    out["_planes"] = cols.acc.cpu().numpy().copy()
+    return state, out
