@@ -19,7 +19,7 @@ __device__ __forceinline__ void sys9_zero(Sys9& s) {
 __device__ __forceinline__ void sys9_solve(Sys9& s, double (&x)[9]) {
     double f;
     double r0, r1, r2, r3, r4, r5, r6, r7, r8;
-    r0 = 1.0 / s.a00;
+    r0 = rcp(s.a00);
     f = s.a30 * r0;
     s.a33 = s.a33 - f * s.a03;
     s.a35 = s.a35 - f * s.a05;
@@ -28,7 +28,7 @@ __device__ __forceinline__ void sys9_solve(Sys9& s, double (&x)[9]) {
     s.a53 = s.a53 - f * s.a03;
     s.a55 = s.a55 - f * s.a05;
     s.b5 = s.b5 - f * s.b0;
-    r1 = 1.0 / s.a11;
+    r1 = rcp(s.a11);
     f = s.a31 * r1;
     s.a33 = s.a33 - f * s.a13;
     s.a35 = s.a35 - f * s.a15;
@@ -37,7 +37,7 @@ __device__ __forceinline__ void sys9_solve(Sys9& s, double (&x)[9]) {
     s.a53 = s.a53 - f * s.a13;
     s.a55 = s.a55 - f * s.a15;
     s.b5 = s.b5 - f * s.b1;
-    r2 = 1.0 / s.a22;
+    r2 = rcp(s.a22);
     f = s.a42 * r2;
     s.a44 = s.a44 - f * s.a24;
     s.a46 = s.a46 - f * s.a26;
@@ -46,7 +46,7 @@ __device__ __forceinline__ void sys9_solve(Sys9& s, double (&x)[9]) {
     s.a64 = s.a64 - f * s.a24;
     s.a66 = s.a66 - f * s.a26;
     s.b6 = s.b6 - f * s.b2;
-    r3 = 1.0 / s.a33;
+    r3 = rcp(s.a33);
     f = s.a43 * r3;
     s.a44 = s.a44 - f * s.a34;
     s.a45 = s.a45 - f * s.a35;
@@ -55,7 +55,7 @@ __device__ __forceinline__ void sys9_solve(Sys9& s, double (&x)[9]) {
     s.a54 = s.a54 - f * s.a34;
     s.a55 = s.a55 - f * s.a35;
     s.b5 = s.b5 - f * s.b3;
-    r4 = 1.0 / s.a44;
+    r4 = rcp(s.a44);
     f = s.a54 * r4;
     s.a55 = s.a55 - f * s.a45;
     s.a56 = s.a56 - f * s.a46;
@@ -80,7 +80,7 @@ __device__ __forceinline__ void sys9_solve(Sys9& s, double (&x)[9]) {
     s.a87 = s.a87 - f * s.a47;
     s.a88 = s.a88 - f * s.a48;
     s.b8 = s.b8 - f * s.b4;
-    r5 = 1.0 / s.a55;
+    r5 = rcp(s.a55);
     f = s.a65 * r5;
     s.a66 = s.a66 - f * s.a56;
     s.a67 = s.a67 - f * s.a57;
@@ -96,7 +96,7 @@ __device__ __forceinline__ void sys9_solve(Sys9& s, double (&x)[9]) {
     s.a87 = s.a87 - f * s.a57;
     s.a88 = s.a88 - f * s.a58;
     s.b8 = s.b8 - f * s.b5;
-    r6 = 1.0 / s.a66;
+    r6 = rcp(s.a66);
     f = s.a76 * r6;
     s.a77 = s.a77 - f * s.a67;
     s.a78 = s.a78 - f * s.a68;
@@ -105,11 +105,11 @@ __device__ __forceinline__ void sys9_solve(Sys9& s, double (&x)[9]) {
     s.a87 = s.a87 - f * s.a67;
     s.a88 = s.a88 - f * s.a68;
     s.b8 = s.b8 - f * s.b6;
-    r7 = 1.0 / s.a77;
+    r7 = rcp(s.a77);
     f = s.a87 * r7;
     s.a88 = s.a88 - f * s.a78;
     s.b8 = s.b8 - f * s.b7;
-    r8 = 1.0 / s.a88;
+    r8 = rcp(s.a88);
     x[8] = s.b8 * r8;
     x[7] = (s.b7 - s.a78 * x[8]) * r7;
     x[6] = (s.b6 - (s.a67 * x[7] + s.a68 * x[8])) * r6;

@@ -49,7 +49,7 @@ def main():
     done = set()
     for p, i, cols in ops:
         if p not in done:
-            out.append(f"    r{p} = 1.0 / s.a{p}{p};")
+            out.append(f"    r{p} = rcp(s.a{p}{p});")
             done.add(p)
         out.append(f"    f = s.a{i}{p} * r{p};")
         for j in cols:
@@ -61,7 +61,7 @@ def main():
         for j in terms:
             expr = f"s.a{i}{j} * x[{j}]" if expr is None else f"({expr} + s.a{i}{j} * x[{j}])"
         if i not in done:
-            out.append(f"    r{i} = 1.0 / s.a{i}{i};")
+            out.append(f"    r{i} = rcp(s.a{i}{i});")
             done.add(i)
         if expr is None:
             out.append(f"    x[{i}] = s.b{i} * r{i};")

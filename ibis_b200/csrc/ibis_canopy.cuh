@@ -326,15 +326,18 @@ __device__ __forceinline__ void turvap(double (&W)[9], TvOut<R>& o, const double
         const double psig = -(double)P.grav * (double)X.suction0 * pow((double)X.zwtot, -(double)X.bex0);
         hfac = exp(psig / ((double)P.rvap * tg));
     }
-    const double hfac2 = q34 / fmax(qg, eps);
-    double betaw = clip(((double)X.zwtot - (double)X.swilt0) / fmax(1.0 - (double)X.swilt0, eps), 0.0, 1.0);
-    if (beta_power != 1.0) betaw = pow(betaw, beta_power);
+    const double hfac2 = dv<R>(q34, fmax(qg, eps));
+    double betaw = clip(dv<R>((double)X.zwtot - (double)X.swilt0, fmax(1.0 - (double)X.swilt0, eps)), 0.0, 1.0);
+    if (beta_power != 1.0) {
+        if constexpr (sizeof(R) == 4) betaw = (double)powf((float)betaw, (float)beta_power);   // betaw in [0, 1]
+        else betaw = pow(betaw, beta_power);
+    }
     const double e34 = esat(t34);
     const double qs1 = qsat(e34, ps);
     const double dqs1 = dqsat(t34, qs1, e34);
-    const double xden = cp + ((double)P.zir * cube(t34)) / (double)T.sg;
-    const double bfac = hvap * dqs1 / xden;
-    const double betas = betaw / (1.0 + bfac * (1.0 - betaw));
+    const double xden = cp + dv<R>((double)P.zir * cube(t34), (double)T.sg);
+    const double bfac = dv<R>(hvap * dqs1, xden);
+    const double betas = dv<R>(betaw, 1.0 + bfac * (1.0 - betaw));
     double qgfac = (betas > 0.0) ? betas * hfac + (1.0 - betas) * hfac2 : hfac2;
     const double qeps = 1.0e-10;
     if (q34 > qg + qeps) qgfac = 1.0;
@@ -348,19 +351,19 @@ __device__ __forceinline__ void turvap(double (&W)[9], TvOut<R>& o, const double
     double fr[12];
 #pragma unroll
     for (int j = 0; j < 12; ++j) fr[j] = (double)S(IBIS_STAT_FRAC, j);
-    const double suw = fmin(fwux * su, 0.8 * (X.wliqu + X.wsnou) / fmax(dt * (qu - q12), eps));
+    const double suw = fmin(fwux * su, dv<R>(0.8 * (X.wliqu + X.wsnou), fmax(dt * (qu - q12), eps)));
     const double sut = fmax(0.0, (1.0 - fwux) * 0.5 * (tb * fr[0] + tb * fr[1] + tb * fr[2] + tc * fr[3]
                                                       + tb * fr[4] + tc * fr[5] + tb * fr[6] + tb * fr[7]));
     const double hvu = hvap + cvap * (ta - tmelt) - ch2o * (tu - tmelt);
     const double hsu = hsub + cvap * (ta - tmelt) - cice * (tu - tmelt);
     const double suh = suw * (X.rliqu * hvu + (1.0 - X.rliqu) * hsu) + sut * hvu;
-    const double ssw = fmin(fwsx * ss, 0.8 * (X.wliqs + X.wsnos) / fmax(dt * (qs - q12), eps));
+    const double ssw = fmin(fwsx * ss, dv<R>(0.8 * (X.wliqs + X.wsnos), fmax(dt * (qs - q12), eps)));
     const double ssh = ssw * (X.rliqs * (hvap + cvap * (ta - tmelt) - ch2o * (ts - tmelt))
                               + (1.0 - X.rliqs) * (hsub + cvap * (ta - tmelt) - cice * (ts - tmelt)));
-    const double slw = fmin(fwlx * sl, 0.8 * (X.wliql + X.wsnol) / fmax(dt * (ql - q34), eps));
+    const double slw = fmin(fwlx * sl, dv<R>(0.8 * (X.wliql + X.wsnol), fmax(dt * (ql - q34), eps)));
     const double tls = st.tcls, tl3 = st.tcl3, tl4 = st.tcl4;
     const double slt0 = fmax(0.0, (1.0 - fwlx) * 0.5 * (tls * fr[8] + tls * fr[9] + tl4 * fr[10] + tl3 * fr[11]));
-    const double slt = slt0 * (double)X.lai0 / fmax((double)X.lsl0, eps);
+    const double slt = dv<R>(slt0 * (double)X.lai0, fmax((double)X.lsl0, eps));
     const double hvl = hvap + cvap * (ta - tmelt) - ch2o * (tl - tmelt);
     const double slh = slw * (X.rliql * hvl + (1.0 - X.rliql) * (hsub + cvap * (ta - tmelt) - cice * (tl - tmelt)))
                      + slt * hvl;
@@ -368,7 +371,7 @@ __device__ __forceinline__ void turvap(double (&W)[9], TvOut<R>& o, const double
     // matrix and right-hand side (canopy_exchange.py:620-682)
     Sys9 M;
     sys9_zero(M);
-    const double rdt = 1.0 / dt;
+    const double rdt = P.rdt64;
     const double fi = X.fi;
     double r2 = su * cp;
     M.a00 = X.chux * rdt + wu * r2 + wu * suh * dqu;

@@ -11,12 +11,12 @@ template <typename T, int N>
 __device__ __forceinline__ void thomas(const T (&lo)[N], const T (&di)[N], const T (&up)[N], const T (&r)[N],
                                        T (&x)[N]) {
     T gam[N];
-    T alp = T(1.0) / di[0];
+    T alp = rcp(di[0]);
     gam[0] = up[0] * alp;
     x[0] = r[0] * alp;
 #pragma unroll
     for (int k = 1; k < N - 1; ++k) {
-        alp = T(1.0) / (di[k] - lo[k] * gam[k - 1]);
+        alp = rcp(di[k] - lo[k] * gam[k - 1]);
         gam[k] = up[k] * alp;
         x[k] = (r[k] - lo[k] * x[k - 1]) * alp;
     }
@@ -124,7 +124,7 @@ __device__ __forceinline__ void soil_water(double (&w)[NL], double& wpud, double
         const double hyd = (double)S(IBIS_STAT_HYDRAUL, k);
         const double suc = (double)S(IBIS_STAT_SUCTION, k);
         const double bex = (double)S(IBIS_STAT_BEX, k);
-        const double hm = P.sw_hm[k], wp = P.sw_wp[k], wm = P.sw_wm[k];
+        const double wp = P.sw_wp[k], wm = P.sw_wm[k];
         double a = wm * hyd_prev + wp * hyd;
         double b = wm * hyd_prev * suc_prev * bex_prev + wp * hyd * suc * bex;
         double zb = wm * bex_prev + wp * bex;
@@ -133,12 +133,19 @@ __device__ __forceinline__ void soil_water(double (&w)[NL], double& wpud, double
         int nn = nb + 2;
         double ws = consistent ? wp * w[k - 1] + wm * w[k] : wm * w[k - 1] + wp * w[k];
         double wa = fmin(ws, 1.0);
-        double bwn1 = b * ipow(wa, nn - 1);
+        const double pw1 = ipow(wa, nn - 1);
+        double bwn1 = b * pw1;
         double bwn = bwn1 * wa;
         if (bwn < dmin) bwn1 = 0.0;
         bwn = fmax(bwn, dmin);
-        double dw = (w[k] - w[k - 1]) / hm;
-        double wam1 = ipow(wa, m - 1);
+        double dw, wam1;
+        if constexpr (sizeof(R) == 4) {
+            dw = (w[k] - w[k - 1]) * P.sw_rhm[k];
+            wam1 = pw1 * pw1;                           // wa**(m-1) = (wa**(nn-1))**2
+        } else {
+            dw = (w[k] - w[k - 1]) / P.sw_hm[k];
+            wam1 = ipow(wa, m - 1);
+        }
         double ek = (-1.0 + (double)m) * a * (wam1 * wa) + ((0.0 * bwn) - (double)nn * bwn1 * wa) * dw;
         double fk = (double)(-m) * a * wam1 + (double)nn * bwn1 * dw;
         double zi = fmax(0.0, 1.0 - fmax(wisoi[k - 1], wisoi[k]));
@@ -158,25 +165,38 @@ __device__ __forceinline__ void soil_water(double (&w)[NL], double& wpud, double
 #pragma unroll
     for (int k = 0; k < NL; ++k) {
         const double h = (double)P.hsoi[k];
-        const double dt = dtime / fmax(pflo[k] * h, 1e-30);
-        const double hm = P.sw_hb[k];
-        const int km1 = k > 0 ? k - 1 : 0;
-        double d1 = dt * (f[k] * 0.5 * h / hm - g[k] / hm);
+        const double dt = dv<R>(dtime, fmax(pflo[k] * h, 1e-30));
+        double d1, d2, d3;
         double rk = w[k] + dt * (e[k + 1] - e[k]);
-        if (k == 0) {
-            rk = rk + dt * (fwtop + fwpud) / rhow;
-            d1 = 0.0;
-        }
-        double d2, d3;
-        if (k < NL - 1) {
-            const double hp = P.sw_hp[k];
-            d2 = 1.0 + dt * (-f[k + 1] * 0.5 * (double)P.hsoi[k + 1] / hp + f[k] * 0.5 * (double)P.hsoi[km1] / hm
-                             + g[k + 1] / hp + g[k] / hm);
-            d3 = dt * (-f[k + 1] * 0.5 * h / hp - g[k + 1] / hp);
+        if constexpr (sizeof(R) == 4) {
+            // the layer geometry as precomputed multipliers
+            const double rhb = P.sw_rhb[k];
+            d1 = dt * (f[k] * P.sw_c1[k] - g[k] * rhb);
+            if (k == 0) rk = rk + dt * (fwtop + fwpud) * P.rrhow64;
+            if (k < NL - 1) {
+                const double rhp = P.sw_rhp[k];
+                d2 = 1.0 + dt * (-f[k + 1] * P.sw_c3[k] + f[k] * P.sw_c5[k] + g[k + 1] * rhp + g[k] * rhb);
+                d3 = dt * (-f[k + 1] * P.sw_c6[k] - g[k + 1] * rhp);
+            } else {
+                d2 = 1.0 + dt * (-f[k + 1] + f[k] * P.sw_c5[k] + g[k] * rhb);
+                d3 = 0.0;
+            }
         } else {
-            d2 = 1.0 + dt * (-f[k + 1] + f[k] * 0.5 * (double)P.hsoi[km1] / hm + g[k] / hm);
-            d3 = 0.0;
+            const double hm = P.sw_hb[k];
+            const int km1 = k > 0 ? k - 1 : 0;
+            d1 = dt * (f[k] * 0.5 * h / hm - g[k] / hm);
+            if (k == 0) rk = rk + dt * (fwtop + fwpud) / rhow;
+            if (k < NL - 1) {
+                const double hp = P.sw_hp[k];
+                d2 = 1.0 + dt * (-f[k + 1] * 0.5 * (double)P.hsoi[k + 1] / hp + f[k] * 0.5 * (double)P.hsoi[km1] / hm
+                                 + g[k + 1] / hp + g[k] / hm);
+                d3 = dt * (-f[k + 1] * 0.5 * h / hp - g[k + 1] / hp);
+            } else {
+                d2 = 1.0 + dt * (-f[k + 1] + f[k] * 0.5 * (double)P.hsoi[km1] / hm + g[k] / hm);
+                d3 = 0.0;
+            }
         }
+        if (k == 0) d1 = 0.0;
         lo[k] = d1; di[k] = d2; up[k] = d3; r[k] = rk;
     }
     thomas(lo, di, up, r, wn);
@@ -185,10 +205,10 @@ __device__ __forceinline__ void soil_water(double (&w)[NL], double& wpud, double
 #pragma unroll
     for (int k = NL - 1; k >= 0; --k) {
         double zz = rhow * poros[k] * fmax(eps, 1.0 - wisoi[k]) * (double)P.hsoi[k];
-        double wk = wn[k] + dtime * fsq / zz;
-        double fsn = fmax(wk - 1.0, 0.0) * zz / dtime;
+        double wk = wn[k] + dv<R>(dtime * fsq, zz);
+        double fsn = dv<R>(fmax(wk - 1.0, 0.0) * zz, dtime);
         wk = fmin(wk, 1.0);
-        wflo[k] = wflo[k + 1] + (wk - w[k]) * zz / dtime;
+        wflo[k] = wflo[k + 1] + dv<R>((wk - w[k]) * zz, dtime);
         wn[k] = wk;
         fsq = fsn;
     }

@@ -237,7 +237,17 @@ static DevParams<R> make_dev_params(const IbisParams& h) {
         d.sw_hb[k] = hb > 1e-30 ? hb : 1e-30;
         double hp = k < NL - 1 ? 0.5 * (h.hsoi[k] + h.hsoi[k + 1]) : 1.0;
         d.sw_hp[k] = hp > 1e-30 ? hp : 1e-30;
+        const int km1 = k > 0 ? k - 1 : 0, kp1 = k < NL - 1 ? k + 1 : k;
+        d.sw_rhm[k] = k > 0 ? 1.0 / d.sw_hm[k] : 0.0;
+        d.sw_rhb[k] = 1.0 / d.sw_hb[k];
+        d.sw_rhp[k] = 1.0 / d.sw_hp[k];
+        d.sw_c1[k] = 0.5 * h.hsoi[k] / d.sw_hb[k];
+        d.sw_c3[k] = 0.5 * h.hsoi[kp1] / d.sw_hp[k];
+        d.sw_c5[k] = 0.5 * h.hsoi[km1] / d.sw_hb[k];
+        d.sw_c6[k] = 0.5 * h.hsoi[k] / d.sw_hp[k];
     }
+    d.rdt64 = 1.0 / h.dtime;
+    d.rrhow64 = 1.0 / h.rhow;
     // respiration tables formed in float32 as the reference does (loops_gswp3.py:185-190)
     const float per_s = (float)(h.ndaypy * 86400.0), mol = (float)(1000.0 / 12.0);
     for (int j = 0; j < 12; ++j) {

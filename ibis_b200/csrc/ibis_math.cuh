@@ -37,6 +37,23 @@ template <typename R>
 __device__ __forceinline__ R quart(R x) { R x2 = x * x; return x2 * x2; }
 
 // x**n for a small non-negative integer n (n <= 40), by repeated squaring.
+// Reciprocal: correctly rounded in double (the same bits as 1.0 / x, by the
+// reciprocal instruction sequence rather than the general division); the
+// build's single-precision division in float.
+__device__ __forceinline__ double rcp(double x) { return __drcp_rn(x); }
+__device__ __forceinline__ float rcp(float x) { return 1.0f / x; }
+
+// a / b inside the FP64 islands.  The FP32 kernels (R = float) multiply by the
+// reciprocal, which is shorter than a correctly rounded division and moves the
+// result by about one unit in the last place of a double -- far below their
+// FP32 error.  The FP64 kernels (R = double) keep the division, so they follow
+// the reference's float64 arithmetic operation for operation.
+template <typename R>
+__device__ __forceinline__ double dv(double a, double b) {
+    if constexpr (sizeof(R) == 4) return a * rcp(b);
+    else return a / b;
+}
+
 __device__ __forceinline__ double ipow(double x, int n) {
     double r = 1.0, b = x;
     bool any = false;

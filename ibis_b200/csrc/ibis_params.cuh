@@ -28,6 +28,12 @@ struct DevParams {
     double sw_wm[6];   // 1 - sw_wp[k]
     double sw_hb[6];   // row k: max(0.5 h[0] | 0.5 h[k-1] + 0.5 h[k], 1e-30)
     double sw_hp[6];   // row k < 5: max(0.5 * (h[k] + h[k+1]), 1e-30)
+    // the same geometry as multipliers, so the solve divides only by values
+    // that change per cell: 1/sw_hm, 1/sw_hb, 1/sw_hp, 0.5 h[k]/sw_hb,
+    // 0.5 h[k+1]/sw_hp, 0.5 h[k-1]/sw_hb, 0.5 h[k]/sw_hp
+    double sw_rhm[6], sw_rhb[6], sw_rhp[6], sw_c1[6], sw_c3[6], sw_c5[6], sw_c6[6];
+    double rdt64;      // 1 / dtime in double
+    double rrhow64;    // 1 / rhow in double
     R rwood_s[12], rroot_s[12], keep[12];  // float32-formed respiration rates (loops_gswp3.py:185-190)
     R ch4_w;           // float32(dtime / 86400)
     R rh_conv;         // float32(12e-3 * 86400)
