@@ -332,9 +332,18 @@ __device__ __forceinline__ void turvap(double (&W)[9], TvOut<R>& o, const double
         if constexpr (sizeof(R) == 4) betaw = (double)powf((float)betaw, (float)beta_power);   // betaw in [0, 1]
         else betaw = pow(betaw, beta_power);
     }
-    const double e34 = esat(t34);
-    const double qs1 = qsat(e34, ps);
-    const double dqs1 = dqsat(t34, qs1, e34);
+    double qs1, dqs1;
+    if constexpr (sizeof(R) == 4) {
+        // float kernels: the canopy-air saturation terms in float, like the
+        // five surface saturation terms above (they only weight betaw)
+        const float t34f = (float)t34, e34f = esat(t34f);
+        const float qs1f = qsat(e34f, (float)ps);
+        qs1 = qs1f; dqs1 = dqsat(t34f, qs1f, e34f);
+    } else {
+        const double e34 = esat(t34);
+        qs1 = qsat(e34, ps);
+        dqs1 = dqsat(t34, qs1, e34);
+    }
     const double xden = cp + dv<R>((double)P.zir * cube(t34), (double)T.sg);
     const double bfac = dv<R>(hvap * dqs1, xden);
     const double betas = dv<R>(betaw, 1.0 + bfac * (1.0 - betaw));

@@ -57,8 +57,8 @@ __device__ __forceinline__ double dv(double a, double b) {
 __device__ __forceinline__ double ipow(double x, int n) {
     double r = 1.0, b = x;
     bool any = false;
-#pragma unroll 1
-    for (int k = 0; k < 6 && n > 0; ++k) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {                 // predicated: no per-cell trip count
         if (n & 1) { r = any ? r * b : b; any = true; }
         n >>= 1;
         if (n) b = b * b;
