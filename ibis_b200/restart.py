@@ -1,0 +1,160 @@
+"""The reference's restart (checkpoint) files, read and written without JAX.
+
+The reference saves an ``IBISState`` as one ``.npz``: every leaf of
+``jax.tree.flatten(state)`` as ``leaf_{i}`` in flatten order (the Equinox
+field order of the state modules), ``num_leaves``, ``treedef_repr`` and
+``meta_*`` entries (python-port/ibis/io/restart.py:19-52), and loads it into a
+template state of the same structure (restart.py:63-193).  This module keeps
+that order as data (:data:`LEAVES`, the 258 leaves of the base state with
+bedrock, generated from the reference's own state classes) so a checkpoint can
+seed device columns, and device columns can be written back as a checkpoint,
+with no JAX present:
+
+* :func:`load` -> ``{leaf path: array}`` and the metadata;
+* :func:`columns_from_restart` -> :class:`~ibis_b200.columns.Columns` plus the
+  parameter record the state implies (soil layer thicknesses, root profile,
+  snow constants, CO2);
+* :func:`write_columns` / :func:`save` -> a checkpoint the reference's
+  ``load_state`` reads, with the prognostic (and, if kept, diagnostic) leaves
+  taken from the columns and every other leaf carried over.
+
+Only the base state is mapped.  A checkpoint that also carries optional
+trailing modules (permafrost, wetland, fire, accumulators of the calibration
+chain) keeps them untouched: they follow the base leaves and are copied
+through by position.
+"""
+from __future__ import annotations
+
+import re
+import types
+
+import numpy as np
+
+from . import layout as L
+from .restart_leaves import LEAVES
+
+BEDROCK_LEAF = "soil.tsoi_deep"
+
+
+def _soil_leaf_count(treedef_repr: str):
+    """Children of the SoilState node in a saved tree structure, or None."""
+    m = re.search(r"SoilState\[[^\]]*\], \[([^\]]*)\]", treedef_repr)
+    return None if m is None else m.group(1).count("*")
+
+
+def base_leaves(bedrock: bool):
+    """Leaf paths of the base state in checkpoint order."""
+    return [p for p in LEAVES if bedrock or p != BEDROCK_LEAF]
+
+
+def load(path: str):
+    """Read a checkpoint.  Returns ``(leaves, meta, extra)``: the base leaves by
+    path, the ``meta_*`` entries, and the trailing leaves of optional modules
+    (a list, by position)."""
+    z = np.load(path, allow_pickle=False)
+    n = int(z["num_leaves"])
+    arrays = [None if f"leaf_{i}_is_none" in z.files else z[f"leaf_{i}"] for i in range(n)]
+    nsoil_all = sum(1 for p in LEAVES if p.startswith("soil."))
+    if "treedef_repr" in z.files:
+        k = _soil_leaf_count(str(z["treedef_repr"]))
+        if k is None:
+            raise ValueError(f"{path}: no SoilState in the saved tree structure")
+        bedrock = k == nsoil_all
+    else:
+        bedrock = n in (len(LEAVES),) or n > len(LEAVES)
+    names = base_leaves(bedrock)
+    if n < len(names):
+        raise ValueError(f"{path}: {n} leaves, the base state has {len(names)}")
+    leaves = dict(zip(names, arrays[:len(names)]))
+    meta = {k[5:]: (z[k].item() if z[k].ndim == 0 else z[k]) for k in z.files if k.startswith("meta_")}
+    return leaves, meta, arrays[len(names):]
+
+
+def save(path: str, leaves: dict, meta: dict | None = None, extra=None, treedef_repr: str | None = None):
+    """Write ``leaves`` (base state by path, bedrock leaf optional) in the reference's checkpoint format."""
+    bedrock = leaves.get(BEDROCK_LEAF) is not None
+    names = base_leaves(bedrock)
+    missing = [p for p in names if p not in leaves]
+    if missing:
+        raise ValueError(f"leaves missing from the state: {missing[:5]}")
+    arrays = [leaves[p] for p in names] + list(extra or [])
+    out = {"num_leaves": np.asarray(len(arrays))}
+    if treedef_repr is not None:
+        out["treedef_repr"] = np.asarray(treedef_repr)
+    for i, a in enumerate(arrays):
+        if a is None:
+            out[f"leaf_{i}_is_none"] = np.asarray(True)
+        else:
+            out[f"leaf_{i}"] = np.asarray(a)
+    for k, v in (meta or {}).items():
+        out[f"meta_{k}"] = np.asarray(v)
+    np.savez_compressed(path, **out)
+
+
+def as_tree(leaves: dict):
+    """The flat leaves as nested attribute objects (``tree.soil.tsoi`` ...), the
+    shape :mod:`ibis_b200.dropin` reads."""
+    root = types.SimpleNamespace()
+    for path, v in leaves.items():
+        obj = root
+        *head, last = path.split(".")
+        for h in head:
+            if not hasattr(obj, h):
+                setattr(obj, h, types.SimpleNamespace())
+            obj = getattr(obj, h)
+        setattr(obj, last, v)
+    if not hasattr(root.soil, "tsoi_deep"):
+        root.soil.tsoi_deep = None
+    return root
+
+
+def columns_from_restart(path: str, dtype=None, device="cuda", params=None, diag=False, acc=True):
+    """Device columns holding a checkpoint's state, and the parameter record.
+
+    ``params`` supplies everything a checkpoint does not hold (a
+    :class:`~ibis_b200.params.StepParams`; defaults otherwise); the soil layer
+    thicknesses, root profile, snow constants and CO2 come from the state.
+    Returns ``(columns, params, leaves, meta, extra)``."""
+    import torch
+
+    from . import dropin
+    from .columns import Columns
+    from .params import FLAG_BEDROCK, StepParams
+
+    leaves, meta, extra = load(path)
+    tree = as_tree(leaves)
+    ncell = int(np.asarray(tree.soil.tg).shape[0])
+    prog = dropin._leaf_dict(tree, "PROG", ncell)
+    stat = dropin._leaf_dict(tree, "STAT", ncell)
+    P = (params or StepParams()).copy()
+    for name, leaf in (("hsoi", "soil.hsoi"), ("froot", "vegetation.froot"), ("co2conc", "atm.co2conc")):
+        v = leaves.get(leaf)
+        if v is not None:
+            v = np.asarray(v, dtype=np.float64).reshape(-1)
+            setattr(P, name, v[:L.NSOILAY] if name == "hsoi" else (v if name == "froot" else float(v[0])))
+    for name in ("z0sno", "rhos", "consno", "hsnotop", "hsnomin", "fimin", "fimax"):
+        v = leaves.get("snow." + name)
+        if v is not None:
+            setattr(P, name, float(np.asarray(v).reshape(-1)[0]))
+    P.flags = (P.flags | FLAG_BEDROCK) if leaves.get(BEDROCK_LEAF) is not None else (P.flags & ~FLAG_BEDROCK)
+    if dtype is None:
+        dtype = torch.float32 if np.asarray(tree.soil.tg).dtype == np.float32 else torch.float64
+    cols = Columns.from_host(prog, stat, dtype=dtype, device=device, diag=diag, acc=acc)
+    return cols, P, leaves, meta, extra
+
+
+def write_columns(path: str, cols, leaves: dict, meta=None, extra=None):
+    """Save ``cols``' prognostic state (and diagnostics, if the columns keep them)
+    into the checkpoint ``leaves`` came from, in the leaves' own dtypes."""
+    out = dict(leaves)
+    groups = [("PROG", cols.prog_host())]
+    if cols.diag is not None:
+        groups.append(("DIAG", cols.diag_host()))
+    for group, values in groups:
+        for f in L.GROUPS[group]:
+            old = out.get(f.leaf)
+            if old is None or f.name not in values:
+                continue
+            v = np.asarray(values[f.name]).astype(np.asarray(old).dtype)
+            out[f.leaf] = v.reshape(-1)[0] if np.ndim(old) == 0 else v.reshape(np.shape(old))
+    save(path, out, meta, extra)

@@ -96,7 +96,7 @@ lax = _types.SimpleNamespace(scan=_scan, fori_loop=_fori_loop, cond=_cond, selec
                              stop_gradient=lambda x: x)
 
 tree = _types.SimpleNamespace(map=_tree.tree_map, leaves=_tree.tree_leaves,
-                              flatten=_tree.tree_flatten)
+                              flatten=_tree.tree_flatten, unflatten=_tree.tree_unflatten)
 tree_util = _types.SimpleNamespace(tree_map=_tree.tree_map, tree_leaves=_tree.tree_leaves,
                                    tree_flatten=_tree.tree_flatten)
 

@@ -17,7 +17,12 @@ on seeded synthetic columns from ``ibis_b200.synth``, and writes the inputs
 and outputs to ``tests/golden/<case>.npz``.  The fixtures travel with the
 repository; this script only runs where ``/root/reference`` exists.
 
-Usage:  python tests/golden/make_golden.py [--check]
+It also writes ``ibis_b200/restart_leaves.py`` (the leaf order of the
+reference's checkpoint files, from its state classes) and the
+``restart_1996`` case: the reference's own checkpoint of a 171-cell transient
+run, stepped by its own ``timestep_body``.
+
+Usage:  python tests/golden/make_golden.py [--only CASE|restart_leaves]
 """
 from __future__ import annotations
 
@@ -132,7 +137,9 @@ def snapshot(st):
         v = get(st, f.leaf)
         out["prog." + f.name] = np.broadcast_to(v, (st.soil.tg.shape[0],) + v.shape[1:]) if f.name == "nytimes" else v
     for f in L.DIAG:
-        out["diag." + f.name] = get(st, f.leaf)
+        mod, leaf = f.leaf.split(".")
+        if hasattr(getattr(st, mod), leaf):      # diagnostics this build adds have no reference leaf
+            out["diag." + f.name] = get(st, f.leaf)
     return out
 
 
@@ -242,10 +249,108 @@ def build_case(name, spec):
     return wl
 
 
+RESTART = "/root/reference/verify_out_stage1/site_transient_1996.npz"
+LEAVES_PY = os.path.join(REPO, "ibis_b200", "restart_leaves.py")
+
+
+def leaf_paths(x, pre=""):
+    """Leaf paths of a state in jax.tree.flatten order (the stand-in's flatten)."""
+    from jax import _tree
+    c = _tree._children(x)
+    if c is None:
+        return [pre]
+    kind, ch, _ = c
+    if kind == "none":
+        return []
+    if kind == "dc":
+        names = [f.name for f in dataclasses.fields(x) if not f.metadata.get("static", False)]
+        return [p for n, v in zip(names, ch) for p in leaf_paths(v, f"{pre}.{n}" if pre else n)]
+    return [p for i, v in enumerate(ch) for p in leaf_paths(v, f"{pre}[{i}]")]
+
+
+def write_restart_leaves():
+    """ibis_b200/restart_leaves.py: the checkpoint leaf order of the reference's base IBISState."""
+    import jax
+    t = create_ibis_state(GridConfig(nlon=1, nlat=1, npoi=2, nbedrock=3))
+    paths = leaf_paths(t)
+    assert len(paths) == len(jax.tree.flatten(t)[0])
+    lines = ['"""Leaf order of the reference\'s base ``IBISState`` with bedrock: the order',
+             "``jax.tree.flatten`` gives and the restart files store (``leaf_{i}``).",
+             "",
+             "Generated by tests/golden/make_golden.py from the reference's own state",
+             "classes (python-port/ibis/state/*.py, model_state.py:35-63); do not edit.",
+             '"""', "", "LEAVES = ("]
+    lines += [f'    "{p}",' for p in paths] + [")", ""]
+    with open(LEAVES_PY, "w") as f:
+        f.write("\n".join(lines))
+    print(f"wrote {LEAVES_PY}: {len(paths)} leaves")
+
+
+def build_restart_case(nhour=6, record=(1, 2, 6), seed=15):
+    """A realistic state: the reference's checkpoint of a 171-cell transient run
+    (1996), loaded by the reference's own load_state, stepped by its own
+    timestep_body under default SimParams and synthetic forcing.  The inputs the
+    fixture stores come from ibis_b200.restart (this repository's loader), so the
+    case also checks that the loader and the leaf mapping carry every leaf the
+    step reads."""
+    from ibis.io.restart import load_state
+    from ibis_b200 import dropin, restart
+    leaves, meta, extra = restart.load(RESTART)
+    n = int(np.asarray(leaves["soil.tg"]).shape[0])
+    st, _ = load_state(RESTART, create_ibis_state(GridConfig(nlon=1, nlat=1, npoi=n, nbedrock=3)))
+    consts = get_constants()
+    rng = np.random.Generator(np.random.PCG64(seed))
+    lat = rng.uniform(-40.0, 70.0, size=n)
+    forc = synth.make_forcing(rng, lat, nhour, start_doy=172)
+    sp = dataclasses.replace(loops.default_sim_params(n), latitude=_a(np.deg2rad(lat)), bedrock=BedrockParams())
+    P = dropin.step_params(st, consts, sp, 3600.0)
+    tree = restart.as_tree(leaves)
+    prog = dropin._leaf_dict(tree, "PROG", n)
+    stat = dropin._leaf_dict(tree, "STAT", n)
+    stat["f_inund"] = np.zeros(n)
+    wl = synth.Workload(ncell=n, nhour=nhour, prog=prog, stat=stat, forc=forc, params=P, latitude=lat,
+                        start_doy=172, meta=dict(source="site_transient_1996"))
+    out = pack_inputs(wl)
+    for h in range(nhour):
+        st = set_forcing(st, wl.forcing_at(h))
+        st = loops.timestep_body(st, consts, sp, 3600.0)
+        if h + 1 in record:
+            for k, v in snapshot(st).items():
+                out[f"out.{h + 1}.{k}"] = v
+    out["meta.record"] = np.asarray(record)
+    path = os.path.join(HERE, "restart_1996.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path}: {len(out)} arrays, {os.path.getsize(path)} bytes")
+
+
+def write_restart_subset(ncell=16):
+    """tests/golden/restart_16cells.npz: the reference's checkpoint cut to its
+    first cells (every per-cell leaf sliced, the rest as stored), for tests that
+    load a checkpoint where the reference tree is absent."""
+    z = np.load(RESTART, allow_pickle=False)
+    n = int(np.asarray(z["leaf_3"]).shape[0])            # soil.tg
+    out = {}
+    for k in z.files:
+        v = z[k]
+        if k.startswith("leaf_") and not k.endswith("_is_none") and v.ndim >= 1 and v.shape[0] == n:
+            v = v[:ncell]
+        out[k] = v
+    path = os.path.join(HERE, f"restart_{ncell}cells.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path}: {os.path.getsize(path)} bytes")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--only", default=None)
     args = ap.parse_args()
+    if args.only in (None, "restart_leaves"):
+        write_restart_leaves()
+    if args.only in (None, "restart_1996"):
+        build_restart_case()
+        write_restart_subset()
+    if args.only in ("restart_leaves", "restart_1996"):
+        return
     for name, spec in CASES.items():
         if args.only and name != args.only:
             continue

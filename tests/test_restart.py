@@ -1,0 +1,108 @@
+"""Reading and writing the reference's checkpoint files (ibis_b200/restart.py).
+
+CPU: the leaf order, a save/load round trip, and -- where the reference tree is
+present -- every leaf this loader reads from the reference's own checkpoint
+against the reference's own ``load_state``.  GPU: a checkpoint seeds device
+columns whose steps match the reference's steps of the same checkpoint
+(tests/golden/restart_1996.npz, float64, 1e-9), and the columns write back a
+checkpoint that reads back exactly.
+"""
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+from ibis_b200 import layout as L
+from ibis_b200 import restart
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+FIXTURE = os.path.join(HERE, "golden", "restart_16cells.npz")
+REF_CKPT = "/root/reference/verify_out_stage1/site_transient_1996.npz"
+
+
+def test_leaf_order_covers_the_layout():
+    assert len(restart.LEAVES) == 258 and len(set(restart.LEAVES)) == 258
+    assert restart.LEAVES[:4] == ("soil.tsoi", "soil.wsoi", "soil.wisoi", "soil.tg")
+    for f in L.PROG + L.STAT:
+        if not f.leaf.startswith("methane."):
+            assert f.leaf in restart.LEAVES, f.leaf
+    assert len(restart.base_leaves(False)) == 257
+
+
+def test_fixture_loads():
+    leaves, meta, extra = restart.load(FIXTURE)
+    assert meta == {"year": 1996} and extra == []
+    assert leaves["soil.tsoi"].shape == (16, 6) and leaves["soil.tsoi_deep"].shape == (16, 3)
+    assert leaves["soil.hsoi"].shape == (7,)
+    assert np.all(leaves["soil.tsoi"] > 200.0) and np.all(leaves["soil.poros"] > 0.0)
+
+
+def test_save_load_round_trip(tmp_path):
+    leaves, meta, extra = restart.load(FIXTURE)
+    leaves["soil.tg"] = leaves["soil.tg"] + 1.0
+    p = tmp_path / "ck.npz"
+    restart.save(str(p), leaves, meta, extra=[np.arange(3.0)])
+    back, meta2, extra2 = restart.load(str(p))
+    assert meta2 == meta and len(extra2) == 1 and np.array_equal(extra2[0], np.arange(3.0))
+    for k in restart.LEAVES:
+        assert np.array_equal(np.asarray(back[k]), np.asarray(leaves[k])), k
+    nobed = {k: v for k, v in leaves.items() if k != restart.BEDROCK_LEAF}
+    restart.save(str(p), nobed, meta)
+    back, _, _ = restart.load(str(p))
+    assert restart.BEDROCK_LEAF not in back and len(back) == 257
+
+
+_REF_CHECK = r"""
+import sys, numpy as np
+sys.path.insert(0, "{golden}/jaxshim"); sys.path.insert(0, "{ref}"); sys.path.insert(0, "{repo}")
+from ibis.dimensions import GridConfig
+from ibis.state.model_state import create_ibis_state
+from ibis.io.restart import load_state
+from ibis_b200 import restart
+leaves, meta, extra = restart.load("{ckpt}")
+n = leaves["soil.tg"].shape[0]
+st, m = load_state("{ckpt}", create_ibis_state(GridConfig(nlon=1, nlat=1, npoi=n, nbedrock=3)))
+static = ("z0sno", "rhos", "consno", "hsnotop", "hsnomin", "fimin", "fimax")
+for path, v in leaves.items():
+    mod, leaf = path.split(".")
+    if mod == "snow" and leaf in static:
+        continue                                   # the reference takes these from its template
+    r = np.asarray(getattr(getattr(st, mod), leaf))
+    assert np.array_equal(r.astype(np.float64), np.asarray(v).astype(np.float64)), path
+print("leaves ok", len(leaves))
+"""
+
+
+@pytest.mark.skipif(not os.path.exists(REF_CKPT), reason="reference checkpoint not present")
+def test_loader_agrees_with_the_reference_loader():
+    code = _REF_CHECK.format(golden=os.path.join(HERE, "golden"), ref="/root/reference/python-port",
+                             repo=os.path.dirname(HERE), ckpt=REF_CKPT)
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0 and "leaves ok 258" in r.stdout, r.stderr[-3000:]
+
+
+@pytest.mark.gpu
+def test_checkpoint_columns_step_like_the_reference(cuda_lib, tmp_path):
+    import torch
+    from goldens import Case, compare
+    c = Case("restart_1996")
+    cols, P, leaves, meta, extra = restart.columns_from_restart(FIXTURE, dtype=torch.float64, diag=True, acc=False)
+    n = cols.ncell
+    forc = {k: v[:, :n] for k, v in c.forc.items()}
+    cols.run(cols.forcing(forc, 0, 6), c.params)
+    torch.cuda.synchronize()
+    want = {k: v[:n] for k, v in c.out(6, "prog").items()}
+    got = cols.prog_host()
+    bad = compare(got, want, 1e-9)
+    assert not bad, bad[:5]
+    p = tmp_path / "after.npz"
+    restart.write_columns(str(p), cols, leaves, meta, extra)
+    back, meta2, _ = restart.load(str(p))
+    prog = cols.prog_host()
+    for f in L.PROG:
+        v = np.asarray(back[f.leaf], dtype=np.float64)
+        ref = prog[f.name][0] if v.ndim == 0 else prog[f.name]
+        assert np.array_equal(v, np.asarray(ref).astype(np.float32).astype(np.float64).reshape(v.shape)), f.name
+    assert meta2 == meta
