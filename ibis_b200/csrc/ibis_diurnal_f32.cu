@@ -1,0 +1,57 @@
+// Device forcing generator: daily weather planes -> hourly forcing planes.
+#include <errno.h>
+#include <stdio.h>
+
+#include "../../include/ibis_b200.h"
+#include "ibis_diurnal.cuh"
+
+namespace ibis {
+
+// One thread per cell walks its days and hours; the writes of a warp to one
+// forcing plane are 32 consecutive floats.
+__global__ void __launch_bounds__(128) diurnal_kernel(const float* __restrict__ daily, const float* __restrict__ lat,
+                                                      float* __restrict__ forc, int ncell, int ld, int nday, int nh,
+                                                      int jday0, int day0, float dtime, uint32_t seed, bool obs) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ncell) return;
+    const double xlat = (double)__ldg(lat + i) * (3.14159265358979323846 / 180.0);
+    const float sinlat = (float)sin(xlat), coslat = (float)cos(xlat);
+#pragma unroll 1
+    for (int d = 0; d < nday; ++d) {
+        const int jday = (jday0 - 1 + d) % 365 + 1;
+        const DayGeom g = day_geometry(jday);
+        const DailyRec rec = load_daily(daily + (size_t)d * IBIS_DAILY_COUNT * ld + i, ld);
+        const uint32_t day = (uint32_t)(day0 + d);
+        const Event ev = precip_timing(draw24(seed, i, day, 0), draw24(seed, i, day, 1), rec.precip, dtime);
+#pragma unroll 1
+        for (int h = 0; h < nh; ++h) {
+            const Forc<float> F = diurnal_hour(rec, g, sinlat, coslat, (float)h * dtime, ev,
+                                               draw24(seed, i, day, 2 + h), dtime, obs);
+            store_forc(F, forc + (size_t)(d * nh + h) * IBIS_FORC_COUNT * ld + i, ld);
+        }
+    }
+}
+
+}  // namespace ibis
+
+extern "C" int ibis_diurnal_f32(const float* daily, const float* lat, float* forc, int ncell, int ld, int nday,
+                                int jday0, int day0, float dtime, unsigned int seed, unsigned int flags,
+                                void* stream) {
+    if (!daily || !lat || !forc) return -EINVAL;
+    if (ncell < 0 || nday < 0 || ld < ncell || ld % 32 || day0 < 0 || jday0 < 1 || jday0 > 366) return -EINVAL;
+    if (!(dtime > 0.0f)) return -EINVAL;
+    const int nh = (int)(86400.0f / dtime);
+    if (nh < 1 || nh > 254 || (float)nh * dtime != 86400.0f) return -EINVAL;
+    if (flags & ~IBIS_DIURNAL_OBSERVED_FIRA) return -EINVAL;
+    if (ncell == 0 || nday == 0) return 0;
+    const int block = 128, grid = (ncell + block - 1) / block;
+    ibis::diurnal_kernel<<<grid, block, 0, (cudaStream_t)stream>>>(daily, lat, forc, ncell, ld, nday, nh, jday0,
+                                                                   day0, dtime, (uint32_t)seed,
+                                                                   (flags & IBIS_DIURNAL_OBSERVED_FIRA) != 0);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        fprintf(stderr, "ibis_diurnal_f32: launch failed: %s\n", cudaGetErrorString(e));
+        return -(int)e - 1000;
+    }
+    return 0;
+}

@@ -18,6 +18,7 @@ The planes are grouped into buffers by how the step uses them:
            its running compensation)
 ``RUN``    per-run calibration vector of the ensemble kernels
 ``YEARLY`` accumulator totals an ensemble run reports at each year end
+``DAILY``  daily weather the device forcing generator turns into hours
 
 Each field names the leaf of the reference ``IBISState`` it mirrors
 (``python-port/ibis/state/*.py``), so host code can move data between the
@@ -258,7 +259,22 @@ YEARLY = (
     Field("ch4", "acc.ch4_day"),
 )
 
-GROUPS = {"PROG": PROG, "STAT": STAT, "FORC": FORC, "DIAG": DIAG, "ACC": ACC, "RUN": RUN, "YEARLY": YEARLY}
+# Daily weather the device forcing generator disaggregates to hours
+# (DailyWeather, python-port/ibis/physics/weather.py:79-90; fira is the
+# observed daily longwave the day loop may use instead of the generator's).
+DAILY = (
+    Field("tmax", "daily_weather.tmax"),
+    Field("tmin", "daily_weather.tmin"),
+    Field("cloud", "daily_weather.cloud"),
+    Field("precip", "daily_weather.precip"),
+    Field("psurf", "daily_weather.psurf"),
+    Field("qd", "daily_weather.qd"),
+    Field("ud", "daily_weather.ud"),
+    Field("fira", "gswp3.rlds"),
+)
+
+GROUPS = {"PROG": PROG, "STAT": STAT, "FORC": FORC, "DIAG": DIAG, "ACC": ACC, "RUN": RUN, "YEARLY": YEARLY,
+          "DAILY": DAILY}
 
 
 def offsets(group):
@@ -281,6 +297,7 @@ N_DIAG = nplanes(DIAG)
 N_ACC = nplanes(ACC)
 N_RUN = nplanes(RUN)
 N_YEARLY = nplanes(YEARLY)
+N_DAILY = nplanes(DAILY)
 
 OFF = {g: offsets(v) for g, v in GROUPS.items()}
 

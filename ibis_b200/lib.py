@@ -50,6 +50,8 @@ SIGNATURES = {
     "ibis_ensemble_f32": (ctypes.c_int, [_E, _P, ctypes.c_int, ctypes.c_void_p]),
     "ibis_ensemble_hours_f32": (ctypes.c_int, [_E, _P, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
     "ibis_ensemble_occupancy": (ctypes.c_int, [_P, ctypes.c_int]),
+    "ibis_diurnal_f32": (ctypes.c_int, [ctypes.c_void_p] * 3 + [ctypes.c_int] * 5
+                         + [ctypes.c_float, ctypes.c_uint, ctypes.c_uint, ctypes.c_void_p]),
 }
 
 

@@ -143,6 +143,22 @@ int ibis_ensemble_hours_f32(const IbisEnsemble* ens, const IbisParams* params, i
  * for the variant params->flags selects (0 when it cannot run). */
 int ibis_ensemble_occupancy(const IbisParams* params, int block);
 
+/* Hourly forcing from daily weather on the device: for each of nday days and
+ * each hour of the day (86400 / dtime hours), the FORC planes of that hour.
+ *   daily  [nday][IBIS_DAILY_COUNT][ld]   in: daily weather (IBIS_DAILY_* planes)
+ *   lat    [ld]                           in: latitude (degrees)
+ *   forc   [nday * 86400/dtime][IBIS_FORC_COUNT][ld]  out: hourly forcing, the
+ *          layout ibis_step_f32 reads
+ * Day d is day of year ((jday0 - 1 + d) mod 365) + 1 and draws its variates
+ * (event length and start, hourly wind) from a counter-based generator keyed by
+ * (seed, day0 + d, cell), so any day of any cell regenerates independently.
+ * flags: IBIS_DIURNAL_OBSERVED_FIRA takes the longwave from the fira plane.
+ * Replaces: compute_precip_timing + diurnal (python-port/ibis/physics/weather.py:395-601),
+ * called once per day and hour by _run_day_inner (loops_gswp3.py:115-124). */
+#define IBIS_DIURNAL_OBSERVED_FIRA 1u
+int ibis_diurnal_f32(const float* daily, const float* lat, float* forc, int ncell, int ld, int nday, int jday0,
+                     int day0, float dtime, unsigned int seed, unsigned int flags, void* stream);
+
 /* Same contract in float64 throughout (the float64 run of the reference's step). */
 int ibis_step_f64(double* prog, const double* stat, const double* forc, double* diag, double* acc, int ncell,
                   int ld, int nstep, const IbisParams* params, int* status, void* stream);

@@ -231,6 +231,19 @@ enum {
     IBIS_YEARLY_COUNT = 7
 };
 
+/* DAILY */
+enum {
+    IBIS_DAILY_TMAX = 0,  /* daily_weather.tmax */
+    IBIS_DAILY_TMIN = 1,  /* daily_weather.tmin */
+    IBIS_DAILY_CLOUD = 2,  /* daily_weather.cloud */
+    IBIS_DAILY_PRECIP = 3,  /* daily_weather.precip */
+    IBIS_DAILY_PSURF = 4,  /* daily_weather.psurf */
+    IBIS_DAILY_QD = 5,  /* daily_weather.qd */
+    IBIS_DAILY_UD = 6,  /* daily_weather.ud */
+    IBIS_DAILY_FIRA = 7,  /* gswp3.rlds */
+    IBIS_DAILY_COUNT = 8
+};
+
 /* Parameter record of the hourly step (all double; passed by value). */
 typedef struct IbisParams {
     double stef;

@@ -340,6 +340,73 @@ def write_restart_subset(ncell=16):
     print(f"wrote {path}: {os.path.getsize(path)} bytes")
 
 
+def daily_inputs(ncell=12, seed=16):
+    """Seeded daily weather for the diurnal fixture: warm and cold days, dry,
+    wet and very wet days (an event longer than the random length), humidity
+    above saturation at tmin, and latitudes from the polar night to the
+    midnight sun."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    tmin = rng.uniform(250.0, 295.0, ncell)
+    tmax = tmin + rng.uniform(2.0, 15.0, ncell)
+    d = dict(tmax=tmax, tmin=tmin, cloud=rng.uniform(0.0, 1.0, ncell),
+             precip=np.where(rng.uniform(size=ncell) < 0.4, 0.0, rng.gamma(0.8, 8.0, ncell)),
+             psurf=rng.uniform(70000.0, 103000.0, ncell), qd=rng.uniform(0.001, 0.02, ncell),
+             ud=rng.uniform(0.5, 8.0, ncell), fira=rng.uniform(200.0, 420.0, ncell))
+    d["precip"][0] = 400.0
+    d["precip"][1] = 0.0
+    lat = rng.uniform(-60.0, 70.0, ncell)
+    lat[2], lat[3] = 80.0, -80.0
+    return d, lat
+
+
+def write_diurnal_case(days=(15, 172), seed=7, dtime=3600.0):
+    """tests/golden/diurnal.npz: the reference's compute_precip_timing and
+    diurnal (weather.py:395-601) for 24 hours of two days, with their uniform
+    variates supplied from the counter-based generator the device uses."""
+    import jax
+    from ibis.physics import weather
+    from oracle.weather import uniform24
+    daily, lat = daily_inputs()
+    n = lat.size
+    queue = []
+
+    def uniform(key, shape, *a, **k):
+        return jnp.asarray(queue.pop(0).reshape(shape))
+
+    saved = getattr(jax.random, "uniform", None)
+    jax.random.uniform = uniform
+    out = {f"in.daily.{k}": v for k, v in daily.items()}
+    out["in.lat"] = lat
+    out["in.days"] = np.asarray(days)
+    out["in.seed"] = np.asarray(seed)
+    out["in.dtime"] = np.asarray(dtime)
+    key = jnp.asarray(np.array([0, 1], dtype=np.uint32))
+    try:
+        for di, jday in enumerate(days):
+            cells = np.arange(n)
+            queue[:] = [uniform24(seed, cells, di, 0), uniform24(seed, cells, di, 1)]
+            _, plens, startp, endp = weather.compute_precip_timing(key, _a(daily["precip"]), dtime)
+            for k, v in (("plens", plens), ("startp", startp), ("endp", endp)):
+                out[f"out.{di}.{k}"] = np.asarray(v, dtype=np.float64)
+            dw = weather.DailyWeather(td=_a(0.5 * (daily["tmax"] + daily["tmin"])), tmax=_a(daily["tmax"]),
+                                      tmin=_a(daily["tmin"]), cloud=_a(daily["cloud"]), precip=_a(daily["precip"]),
+                                      psurf=_a(daily["psurf"]), qd=_a(daily["qd"]), ud=_a(daily["ud"]),
+                                      iwet=_a(np.zeros(n)), xstore=_a(np.zeros((n, 3))))
+            for h in range(int(86400.0 / dtime)):
+                queue[:] = [uniform24(seed, cells, di, 2 + h)]
+                _, hw = weather.diurnal(h * dtime, jday, dw, _a(lat), plens, startp, endp, key, dtime)
+                for k in ("coszen", "ta", "qa", "ua", "fira", "raina", "snowa", "solad", "solai"):
+                    out[f"out.{di}.{h}.{k}"] = np.asarray(getattr(hw, k), dtype=np.float64)
+    finally:
+        if saved is None:
+            del jax.random.uniform
+        else:
+            jax.random.uniform = saved
+    path = os.path.join(HERE, "diurnal.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path}: {len(out)} arrays, {os.path.getsize(path)} bytes")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--only", default=None)
@@ -349,7 +416,9 @@ def main():
     if args.only in (None, "restart_1996"):
         build_restart_case()
         write_restart_subset()
-    if args.only in ("restart_leaves", "restart_1996"):
+    if args.only in (None, "diurnal"):
+        write_diurnal_case()
+    if args.only in ("restart_leaves", "restart_1996", "diurnal"):
         return
     for name, spec in CASES.items():
         if args.only and name != args.only:
