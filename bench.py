@@ -180,24 +180,21 @@ def run_ours(args):
     from ibis_b200 import synth
     from ibis_b200.columns import Columns
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from ibis_b200 import replicas
+    W = replicas.world_from_env()
+    world, rank, local = W.size, W.rank, W.local
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    replicas.init(W, "nccl", device=dev)
 
     def barrier():
-        if world > 1:
-            dist.barrier()
+        replicas.barrier(W)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample()
 
-    wl = synth.make_workload(args.ncell, HOURS, seed=1000 + rank)
+    wl = synth.make_workload(args.ncell, HOURS, seed=replicas.replica_seed(1000, rank))
     P = wl.params
     cols = Columns.from_host(wl.prog, wl.stat, dtype=torch.float32, device=dev, acc=True)
     forc = cols.forcing(wl.forc)
@@ -288,9 +285,8 @@ def run_ours(args):
 
     nonfinite = cols.nonfinite()
     if world > 1:
-        t = torch.tensor([ms_step, ms_plain, ms_e2e, ms_e2e_daily], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_step, ms_plain, ms_e2e, ms_e2e_daily = (float(x) for x in t.cpu())
+        ms_step, ms_plain, ms_e2e, ms_e2e_daily = replicas.max_over_ranks(W, [ms_step, ms_plain, ms_e2e,
+                                                                              ms_e2e_daily], device=dev)
     cell_steps = world * args.ncell * HOURS
     value = cell_steps / (ms_step / 1e3)
     peak, peak_kind = _peaks()
@@ -337,8 +333,7 @@ def run_ours(args):
         if cpu is not None:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.destroy_process_group()
+    replicas.finish(W)
 
 
 def run_ensemble(args):
