@@ -163,3 +163,38 @@ class Columns:
                           self.ld, nstep, ctypes.byref(p), _ptr(self.status), ctypes.c_void_p(stream.cuda_stream))
         _lib.check(rc, "ibis_step")
         return self
+
+    def run_from_host(self, host_forc: torch.Tensor, params: StepParams, chunk: int = 6, stream=None):
+        """Advance the columns through ``host_forc`` (a pinned host tensor
+        ``(nstep, IBIS_FORC_COUNT, ld)``), copying the forcing in chunks of
+        ``chunk`` hours on a second stream so the copy of chunk k+1 overlaps
+        the computation of chunk k.  Asynchronous on ``stream``: work queued on
+        it afterwards (a read-back of the state) runs after the last hour."""
+        if host_forc.device.type != "cpu" or host_forc.dtype != self.dtype or not host_forc.is_pinned():
+            raise ValueError("host forcing must be a pinned CPU tensor of the Columns' dtype")
+        if host_forc.dim() != 3 or host_forc.shape[1] != L.N_FORC or host_forc.shape[2] != self.ld:
+            raise ValueError(f"host forcing must be (nstep, {L.N_FORC}, {self.ld})")
+        nstep = host_forc.shape[0]
+        chunk = max(1, min(int(chunk), nstep))
+        stream = stream or torch.cuda.current_stream(self.device)
+        key = (chunk, host_forc.dtype)
+        if getattr(self, "_staging", None) is None or self._staging[0] != key:
+            bufs = [torch.empty((chunk, L.N_FORC, self.ld), dtype=self.dtype, device=self.device) for _ in range(2)]
+            self._staging = (key, bufs, torch.cuda.Stream(self.device),
+                             [torch.cuda.Event() for _ in range(2)], [torch.cuda.Event() for _ in range(2)])
+        _, bufs, copy_stream, copied, used = self._staging
+        start = torch.cuda.Event()
+        start.record(stream)
+        copy_stream.wait_event(start)
+        for k, h0 in enumerate(range(0, nstep, chunk)):
+            n = min(chunk, nstep - h0)
+            slot = k % 2
+            with torch.cuda.stream(copy_stream):
+                if k >= 2:
+                    copy_stream.wait_event(used[slot])        # the computation of chunk k-2 has read this buffer
+                bufs[slot][:n].copy_(host_forc[h0:h0 + n], non_blocking=True)
+                copied[slot].record(copy_stream)
+            stream.wait_event(copied[slot])
+            self.run(bufs[slot][:n], params, stream=stream)
+            used[slot].record(stream)
+        return self
