@@ -336,6 +336,68 @@ def run_ours(args):
     replicas.finish(W)
 
 
+def _plain_per_vector(spec, args, stream, hours=48):
+    """The ensemble through the single-parameter step API as a caller without
+    the ensemble kernels would drive it: per parameter vector one set of
+    columns (the 356 sites), one ``ibis_step`` launch per hour per vector.
+    Timed over the first ``hours`` hours of every record, beside the persistent
+    launch on the same truncated records (the full records would take minutes
+    in this form)."""
+    import torch
+    from ibis_b200 import ensemble as E
+    from ibis_b200 import layout as L
+    from ibis_b200 import synth
+    from ibis_b200.columns import Columns
+
+    nsite, nvec = spec.nsite, spec.nparam
+    short = E.EnsembleSpec(nsite=nsite, nparam=nvec, site_hours=np.minimum(spec.site_hours, hours), stat=spec.stat,
+                           prog=spec.prog, forc=spec.forc, site_first=spec.site_first, vectors=spec.vectors,
+                           params=spec.params, latitude=spec.latitude)
+    ens = E.Ensemble(short)
+    cols = [Columns.from_host(spec.prog, spec.stat, dtype=torch.float32, acc=True) for _ in range(nvec)]
+    for c in cols:
+        c.set_mode(0)
+    params = [E.apply_vector(spec.params, v) for v in spec.vectors]
+    ld = cols[0].ld
+    fp = np.zeros((hours, L.N_FORC, ld), dtype=np.float32)
+    for s_ in range(nsite):
+        fp[:, :, s_] = spec.forc[spec.site_first[s_]:spec.site_first[s_] + hours]
+    forc = torch.from_numpy(fp).cuda()
+
+    def plain_run():
+        for h in range(hours):
+            for c, P in zip(cols, params):
+                c.run(forc[h:h + 1], P, stream=stream)
+
+    def timed(fn, reset):
+        reset()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        b.synchronize()
+        return a.elapsed_time(b)
+
+    state0 = [c.prog.clone() for c in cols]
+
+    def reset_plain():
+        for c, p0 in zip(cols, state0):
+            c.prog.copy_(p0)
+            c.acc.zero_()
+
+    timed(plain_run, reset_plain)
+    ms_plain = min(timed(plain_run, reset_plain) for _ in range(2))
+    timed(ens.run, ens.reset)
+    ms_pers = min(timed(ens.run, ens.reset) for _ in range(2))
+    cs = nsite * nvec * hours
+    return {"hours": hours, "launches": hours * nvec, "ms": ms_plain, "value": cs / (ms_plain / 1e3),
+            "persistent_ms_same_records": ms_pers, "persistent_value_same_records": cs / (ms_pers / 1e3),
+            "persistent_vs_plain": ms_plain / ms_pers,
+            "note": "one single-parameter step launch per hour per parameter vector (ibis_step_config_f32, "
+                    "config 0), first 48 hours of every record"}
+
+
 def run_ensemble(args):
     """The calibration ensemble: 356 sites x 64 parameter vectors (22,784 runs),
     records of U{1..15} years, one step = every run over its whole record.  The
@@ -375,6 +437,7 @@ def run_ensemble(args):
     ms_eager = timed(lambda: ens.run_hourly(chunk=24, graph=False), args.steps)
     cs = ens.cell_steps()
     m = float(np.mean(ms))
+    plain = _plain_per_vector(spec, args, stream)
     line = {
         "metric": "cell-steps/s, calibration ensemble (persistent launch)", "value": cs / (m / 1e3),
         "unit": "cell-steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": m,
@@ -392,6 +455,7 @@ def run_ensemble(args):
                          "note": "one launch per hour, 24-hour CUDA graph replayed"},
         "hourly_eager": {"value": cs / (float(np.mean(ms_eager)) / 1e3), "ms_per_step": float(np.mean(ms_eager))},
         "persistent_vs_hourly_graph": float(np.mean(ms_graph)) / m,
+        "plain_per_vector": plain,
         "gpu_launches": args.steps,
         "clocks": clk.summary(), "nonfinite_runs": nonfinite[0], "bad_descriptors": nonfinite[1],
     }
