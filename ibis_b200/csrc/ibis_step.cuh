@@ -604,6 +604,8 @@ __device__ __forceinline__ void ground_phase(Col<R>& c, const Forc<R>& F, const 
             Ac.add(IBIS_ACC_AYTRUNOF, grunof * dt);
             Ac.add(IBIS_ACC_AYTDRAIN, wflo[NL] * dt);
             Ac.add(IBIS_ACC_AFSENA, M.fsena * dt);
+            Ac.base[(size_t)IBIS_ACC_STRESSTU_LAST * Ac.ld] = stresstu;
+            Ac.base[(size_t)IBIS_ACC_STRESSTL_LAST * Ac.ld] = stresstl;
         }
         if (P.flags & IBIS_FLAG_CH4) {
             R rh = S(IBIS_STAT_TCO2MIC) * P.rh_conv;

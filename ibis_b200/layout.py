@@ -19,6 +19,7 @@ The planes are grouped into buffers by how the step uses them:
 ``RUN``    per-run calibration vector of the ensemble kernels
 ``YEARLY`` accumulator totals an ensemble run reports at each year end
 ``DAILY``  daily weather the device forcing generator turns into hours
+``DAYST``  state of the daily cadence (phenology, 10-day means, soil carbon)
 
 Each field names the leaf of the reference ``IBISState`` it mirrors
 (``python-port/ibis/state/*.py``), so host code can move data between the
@@ -220,6 +221,10 @@ ACC = (
     Field("wisoi_mean", "acc.wisoi_day", NSOILAY),
     Field("tg_mean", "acc.tg_day"),
     Field("afsena", "acc.fsena"),
+    # last values, not sums: the soil-water stress of the day's last hour, which
+    # the next day's phenology reads (loops_gswp3.py:441-442)
+    Field("stresstu_last", "soil.stresstu"),
+    Field("stresstl_last", "soil.stresstl"),
 )
 
 # Per-run calibration vector of the ensemble kernels: the step-relevant
@@ -263,6 +268,7 @@ YEARLY = (
 # (DailyWeather, python-port/ibis/physics/weather.py:79-90; fira is the
 # observed daily longwave the day loop may use instead of the generator's).
 DAILY = (
+    Field("td", "daily_weather.td"),
     Field("tmax", "daily_weather.tmax"),
     Field("tmin", "daily_weather.tmin"),
     Field("cloud", "daily_weather.cloud"),
@@ -273,8 +279,63 @@ DAILY = (
     Field("fira", "gswp3.rlds"),
 )
 
+# State of the daily cadence (phenology, 10-day means, annual sums, soil
+# carbon), advanced once a day around the day's hourly steps
+# (loops_gswp3.py:382-608).  The 10-day means share their reference leaves
+# with the daily sums of ACC: before and after a day the reference holds the
+# means there, during the day the sums.
+DAYST = (
+    Field("plai", "vegetation.plai", NPFT),
+    Field("tc", "vegetation.tc"),
+    Field("tempu", "vegetation.tempu"),
+    Field("templ", "vegetation.templ"),
+    Field("agddu", "vegetation.agddu"),
+    Field("agddl", "vegetation.agddl"),
+    Field("dropu", "vegetation.dropu"),
+    Field("dropls", "vegetation.dropls"),
+    Field("dropl3", "vegetation.dropl3"),
+    Field("dropl4", "vegetation.dropl4"),
+    Field("tco2root", "vegetation.tco2root"),
+    Field("tnmin", "vegetation.tnmin"),
+    Field("a10td", "summary.a10td"),
+    Field("a10ancub", "summary.a10ancub"),
+    Field("a10ancls", "summary.a10ancls"),
+    Field("a10ancl3", "summary.a10ancl3"),
+    Field("a10ancl4", "summary.a10ancl4"),
+    Field("ayprcp", "summary.ayprcp"),
+    Field("ayaet", "summary.ayaet"),
+    Field("ayco2mic", "summary.ayco2mic"),
+    Field("ayco2root", "summary.ayco2root"),
+    Field("storedn", "summary.storedn"),
+    Field("yrleach", "summary.yrleach"),
+    Field("ynleach", "summary.ynleach"),
+    Field("clitlm", "carbon.clitlm"),
+    Field("clitls", "carbon.clitls"),
+    Field("clitll", "carbon.clitll"),
+    Field("clitrm", "carbon.clitrm"),
+    Field("clitrs", "carbon.clitrs"),
+    Field("clitrl", "carbon.clitrl"),
+    Field("clitwm", "carbon.clitwm"),
+    Field("clitws", "carbon.clitws"),
+    Field("clitwl", "carbon.clitwl"),
+    Field("csoislop", "carbon.csoislop"),
+    Field("csoislon", "carbon.csoislon"),
+    Field("csoipas", "carbon.csoipas"),
+    Field("totcmic", "carbon.totcmic"),
+    Field("decompl", "carbon.decompl"),
+    Field("decomps", "carbon.decomps"),
+    Field("totlit", "carbon.totlit"),
+    Field("totalit", "carbon.totalit"),
+    Field("totrlit", "carbon.totrlit"),
+    Field("totcsoi", "carbon.totcsoi"),
+    Field("totfall", "carbon.totfall"),
+    Field("falll", "carbon.falll"),
+    Field("fallr", "carbon.fallr"),
+    Field("fallw", "carbon.fallw"),
+)
+
 GROUPS = {"PROG": PROG, "STAT": STAT, "FORC": FORC, "DIAG": DIAG, "ACC": ACC, "RUN": RUN, "YEARLY": YEARLY,
-          "DAILY": DAILY}
+          "DAILY": DAILY, "DAYST": DAYST}
 
 
 def offsets(group):
@@ -298,6 +359,7 @@ N_ACC = nplanes(ACC)
 N_RUN = nplanes(RUN)
 N_YEARLY = nplanes(YEARLY)
 N_DAILY = nplanes(DAILY)
+N_DAYST = nplanes(DAYST)
 
 OFF = {g: offsets(v) for g, v in GROUPS.items()}
 

@@ -180,6 +180,66 @@ class StepParams:
         return s
 
 
+# Parameters of the daily cadence (phenology and soil biogeochemistry), all
+# double: PhenoParams (python-port/ibis/physics/phenology.py:30-86, read by
+# pheno, phenology.py:89-287) and BGCParams (io/parameters.py, read by soilbgc,
+# physics/biogeochem.py:23-243, and the decomposition factors of the day loop,
+# timestepping/loops_gswp3.py:494-555).  Defaults are the reference's.
+DAY_PARAM_FIELDS: list[tuple[str, int, object]] = [
+    ("ddays", 1, 15.0), ("tthresh_u_offset", 1, 5.0), ("tthresh_u_abs", 1, -100.0), ("gthresh_u_c", 1, 0.0),
+    ("gdd_thresh_u", 1, 100.0), ("gdd_ramp_u", 1, 50.0), ("tthresh_l_c", 1, 0.0), ("gthresh_l_c", 1, -5.0),
+    ("gdd_thresh_l", 1, 150.0), ("gdd_ramp_l", 1, 50.0), ("drop_thresh", 1, 0.0), ("drop_stress_thresh", 1, -1.0),
+    ("drop_floor", 1, 0.1),
+    ("lig_frac", 1, 0.5), ("fbsom", 1, 0.017), ("effac", 1, 0.4), ("bgc_fmax", 1, 0.45), ("rconst", 1, 1200.0),
+    ("cnleaf", 1, 40.0), ("cnroot", 1, 60.0), ("cnwood", 1, 200.0),
+    ("cnr", 8, (8.0, 15.0, 10.0, 15.0, 100.0, 150.0, 6.0, 250.0)),
+    ("klm", 1, 0.15), ("kls", 1, 0.01), ("kll", 1, 0.01), ("krm", 1, 0.1), ("krs", 1, 0.005), ("krl", 1, 0.005),
+    ("kwm", 1, 0.001), ("kws", 1, 0.001), ("kwl", 1, 0.001), ("kbn", 1, 0.045), ("kbp", 1, 0.005),
+    ("knb", 1, 0.001), ("kns", 1, 1e-06), ("kpb", 1, 0.0001), ("kps", 1, 1e-06), ("ksb", 1, 8e-07),
+    ("ylm", 1, 0.4), ("yls", 1, 0.3), ("yll", 1, 1.0), ("yrm", 1, 0.4), ("yrs", 1, 0.3), ("yrl", 1, 1.0),
+    ("ywm", 1, 0.4), ("yws", 1, 0.3), ("ywl", 1, 1.0), ("ybn", 1, 1.0), ("ybp", 1, 1.0), ("yps", 1, 1.0),
+    ("yns", 1, 1.0), ("ysb", 1, 0.2), ("ypb", 1, 0.2), ("ynb", 1, 0.25),
+    ("lt_e0", 1, 344.0), ("wfps_opt", 1, 60.0), ("k_scale", 1, 1.0),
+]
+
+
+class DayParams:
+    """Mutable record of :data:`DAY_PARAM_FIELDS` (reference defaults)."""
+
+    def __init__(self, **overrides):
+        for name, n, default in DAY_PARAM_FIELDS:
+            object.__setattr__(self, name, np.array(default, dtype=np.float64) if n > 1 else float(default))
+        for k, v in overrides.items():
+            setattr(self, k, v)
+
+    def __setattr__(self, key, value):
+        spec = {n: c for n, c, _ in DAY_PARAM_FIELDS}
+        if key not in spec:
+            raise AttributeError(f"no daily parameter named {key!r}")
+        if spec[key] > 1:
+            value = np.array(value, dtype=np.float64).reshape(-1)
+            if value.size != spec[key]:
+                raise ValueError(f"{key} needs {spec[key]} values")
+        else:
+            value = float(value)
+        object.__setattr__(self, key, value)
+
+    def to_c(self):
+        s = IbisDayParamsC()
+        for name, n, _ in DAY_PARAM_FIELDS:
+            v = getattr(self, name)
+            if n > 1:
+                getattr(s, name)[:] = [float(x) for x in v]
+            else:
+                setattr(s, name, float(v))
+        return s
+
+
+IbisDayParamsC = type("IbisDayParams", (ctypes.Structure,),
+                      {"_fields_": [(n, ctypes.c_double * c if c > 1 else ctypes.c_double)
+                                    for n, c, _ in DAY_PARAM_FIELDS]})
+
+
 def header_struct_text() -> str:
     lines = ["/* Parameter record of the hourly step (all double; passed by value). */",
              "typedef struct IbisParams {"]
@@ -200,4 +260,10 @@ def header_struct_text() -> str:
                     ("ACC", FLAG_ACC), ("CH4", FLAG_CH4), ("SOIL_MEANS", FLAG_SOIL_MEANS),
                     ("DIAG", FLAG_DIAG), ("KAHAN", FLAG_KAHAN)]:
         lines.append(f"#define IBIS_FLAG_{nm} {val}u")
+    lines.append("")
+    lines.append("/* Parameters of the daily cadence (phenology, soil biogeochemistry), all double. */")
+    lines.append("typedef struct IbisDayParams {")
+    for name, n, _ in DAY_PARAM_FIELDS:
+        lines.append(f"    double {name}[{n}];" if n > 1 else f"    double {name};")
+    lines.append("} IbisDayParams;")
     return "\n".join(lines) + "\n"

@@ -13,7 +13,7 @@ with no JAX present:
 * :func:`load` -> ``{leaf path: array}`` and the metadata;
 * :func:`columns_from_restart` -> :class:`~ibis_b200.columns.Columns` plus the
   parameter record the state implies (soil layer thicknesses, root profile,
-  snow constants, CO2);
+  CO2);
 * :func:`write_columns` / :func:`save` -> a checkpoint the reference's
   ``load_state`` reads, with the prognostic (and, if kept, diagnostic) leaves
   taken from the columns and every other leaf carried over.
@@ -108,35 +108,55 @@ def as_tree(leaves: dict):
     return root
 
 
-def columns_from_restart(path: str, dtype=None, device="cuda", params=None, diag=False, acc=True):
-    """Device columns holding a checkpoint's state, and the parameter record.
-
-    ``params`` supplies everything a checkpoint does not hold (a
-    :class:`~ibis_b200.params.StepParams`; defaults otherwise); the soil layer
-    thicknesses, root profile, snow constants and CO2 come from the state.
-    Returns ``(columns, params, leaves, meta, extra)``."""
-    import torch
-
-    from . import dropin
-    from .columns import Columns
+def params_from_leaves(leaves: dict, params=None):
+    """The parameter record a checkpoint implies: ``params`` (defaults otherwise)
+    with the soil layer thicknesses, root profile and CO2 of the state, and the
+    bedrock flag set when the state carries bedrock."""
     from .params import FLAG_BEDROCK, StepParams
-
-    leaves, meta, extra = load(path)
-    tree = as_tree(leaves)
-    ncell = int(np.asarray(tree.soil.tg).shape[0])
-    prog = dropin._leaf_dict(tree, "PROG", ncell)
-    stat = dropin._leaf_dict(tree, "STAT", ncell)
     P = (params or StepParams()).copy()
     for name, leaf in (("hsoi", "soil.hsoi"), ("froot", "vegetation.froot"), ("co2conc", "atm.co2conc")):
         v = leaves.get(leaf)
         if v is not None:
             v = np.asarray(v, dtype=np.float64).reshape(-1)
             setattr(P, name, v[:L.NSOILAY] if name == "hsoi" else (v if name == "froot" else float(v[0])))
-    for name in ("z0sno", "rhos", "consno", "hsnotop", "hsnomin", "fimin", "fimax"):
-        v = leaves.get("snow." + name)
-        if v is not None:
-            setattr(P, name, float(np.asarray(v).reshape(-1)[0]))
+    # the snow constants stay the record's: the reference's load_state takes them
+    # from its template, not from the file (older files carry outdated values,
+    # io/restart.py:174-183)
     P.flags = (P.flags | FLAG_BEDROCK) if leaves.get(BEDROCK_LEAF) is not None else (P.flags & ~FLAG_BEDROCK)
+    return P
+
+
+def group_from_leaves(leaves: dict, group: str, ncell: int) -> dict:
+    """The fields of a plane group (``layout.GROUPS``) the checkpoint holds, as
+    per-cell float64 arrays (scalars broadcast)."""
+    out = {}
+    for f in L.GROUPS[group]:
+        v = leaves.get(f.leaf)
+        if v is None:
+            continue
+        a = np.asarray(v, dtype=np.float64)
+        out[f.name] = np.full(ncell, float(a)) if a.ndim == 0 else a
+    return out
+
+
+def columns_from_restart(path: str, dtype=None, device="cuda", params=None, diag=False, acc=True):
+    """Device columns holding a checkpoint's state, and the parameter record.
+
+    ``params`` supplies everything a checkpoint does not hold (a
+    :class:`~ibis_b200.params.StepParams`; defaults otherwise); the soil layer
+    thicknesses, root profile and CO2 come from the state.
+    Returns ``(columns, params, leaves, meta, extra)``."""
+    import torch
+
+    from . import dropin
+    from .columns import Columns
+
+    leaves, meta, extra = load(path)
+    tree = as_tree(leaves)
+    ncell = int(np.asarray(tree.soil.tg).shape[0])
+    prog = dropin._leaf_dict(tree, "PROG", ncell)
+    stat = dropin._leaf_dict(tree, "STAT", ncell)
+    P = params_from_leaves(leaves, params)
     if dtype is None:
         dtype = torch.float32 if np.asarray(tree.soil.tg).dtype == np.float32 else torch.float64
     cols = Columns.from_host(prog, stat, dtype=dtype, device=device, diag=diag, acc=acc)

@@ -195,7 +195,9 @@ enum {
     IBIS_ACC_WISOI_MEAN = 36,  /* acc.wisoi_day, 6 planes */
     IBIS_ACC_TG_MEAN = 42,  /* acc.tg_day */
     IBIS_ACC_AFSENA = 43,  /* acc.fsena */
-    IBIS_ACC_COUNT = 44
+    IBIS_ACC_STRESSTU_LAST = 44,  /* soil.stresstu */
+    IBIS_ACC_STRESSTL_LAST = 45,  /* soil.stresstl */
+    IBIS_ACC_COUNT = 46
 };
 
 /* RUN */
@@ -233,15 +235,68 @@ enum {
 
 /* DAILY */
 enum {
-    IBIS_DAILY_TMAX = 0,  /* daily_weather.tmax */
-    IBIS_DAILY_TMIN = 1,  /* daily_weather.tmin */
-    IBIS_DAILY_CLOUD = 2,  /* daily_weather.cloud */
-    IBIS_DAILY_PRECIP = 3,  /* daily_weather.precip */
-    IBIS_DAILY_PSURF = 4,  /* daily_weather.psurf */
-    IBIS_DAILY_QD = 5,  /* daily_weather.qd */
-    IBIS_DAILY_UD = 6,  /* daily_weather.ud */
-    IBIS_DAILY_FIRA = 7,  /* gswp3.rlds */
-    IBIS_DAILY_COUNT = 8
+    IBIS_DAILY_TD = 0,  /* daily_weather.td */
+    IBIS_DAILY_TMAX = 1,  /* daily_weather.tmax */
+    IBIS_DAILY_TMIN = 2,  /* daily_weather.tmin */
+    IBIS_DAILY_CLOUD = 3,  /* daily_weather.cloud */
+    IBIS_DAILY_PRECIP = 4,  /* daily_weather.precip */
+    IBIS_DAILY_PSURF = 5,  /* daily_weather.psurf */
+    IBIS_DAILY_QD = 6,  /* daily_weather.qd */
+    IBIS_DAILY_UD = 7,  /* daily_weather.ud */
+    IBIS_DAILY_FIRA = 8,  /* gswp3.rlds */
+    IBIS_DAILY_COUNT = 9
+};
+
+/* DAYST */
+enum {
+    IBIS_DAYST_PLAI = 0,  /* vegetation.plai, 12 planes */
+    IBIS_DAYST_TC = 12,  /* vegetation.tc */
+    IBIS_DAYST_TEMPU = 13,  /* vegetation.tempu */
+    IBIS_DAYST_TEMPL = 14,  /* vegetation.templ */
+    IBIS_DAYST_AGDDU = 15,  /* vegetation.agddu */
+    IBIS_DAYST_AGDDL = 16,  /* vegetation.agddl */
+    IBIS_DAYST_DROPU = 17,  /* vegetation.dropu */
+    IBIS_DAYST_DROPLS = 18,  /* vegetation.dropls */
+    IBIS_DAYST_DROPL3 = 19,  /* vegetation.dropl3 */
+    IBIS_DAYST_DROPL4 = 20,  /* vegetation.dropl4 */
+    IBIS_DAYST_TCO2ROOT = 21,  /* vegetation.tco2root */
+    IBIS_DAYST_TNMIN = 22,  /* vegetation.tnmin */
+    IBIS_DAYST_A10TD = 23,  /* summary.a10td */
+    IBIS_DAYST_A10ANCUB = 24,  /* summary.a10ancub */
+    IBIS_DAYST_A10ANCLS = 25,  /* summary.a10ancls */
+    IBIS_DAYST_A10ANCL3 = 26,  /* summary.a10ancl3 */
+    IBIS_DAYST_A10ANCL4 = 27,  /* summary.a10ancl4 */
+    IBIS_DAYST_AYPRCP = 28,  /* summary.ayprcp */
+    IBIS_DAYST_AYAET = 29,  /* summary.ayaet */
+    IBIS_DAYST_AYCO2MIC = 30,  /* summary.ayco2mic */
+    IBIS_DAYST_AYCO2ROOT = 31,  /* summary.ayco2root */
+    IBIS_DAYST_STOREDN = 32,  /* summary.storedn */
+    IBIS_DAYST_YRLEACH = 33,  /* summary.yrleach */
+    IBIS_DAYST_YNLEACH = 34,  /* summary.ynleach */
+    IBIS_DAYST_CLITLM = 35,  /* carbon.clitlm */
+    IBIS_DAYST_CLITLS = 36,  /* carbon.clitls */
+    IBIS_DAYST_CLITLL = 37,  /* carbon.clitll */
+    IBIS_DAYST_CLITRM = 38,  /* carbon.clitrm */
+    IBIS_DAYST_CLITRS = 39,  /* carbon.clitrs */
+    IBIS_DAYST_CLITRL = 40,  /* carbon.clitrl */
+    IBIS_DAYST_CLITWM = 41,  /* carbon.clitwm */
+    IBIS_DAYST_CLITWS = 42,  /* carbon.clitws */
+    IBIS_DAYST_CLITWL = 43,  /* carbon.clitwl */
+    IBIS_DAYST_CSOISLOP = 44,  /* carbon.csoislop */
+    IBIS_DAYST_CSOISLON = 45,  /* carbon.csoislon */
+    IBIS_DAYST_CSOIPAS = 46,  /* carbon.csoipas */
+    IBIS_DAYST_TOTCMIC = 47,  /* carbon.totcmic */
+    IBIS_DAYST_DECOMPL = 48,  /* carbon.decompl */
+    IBIS_DAYST_DECOMPS = 49,  /* carbon.decomps */
+    IBIS_DAYST_TOTLIT = 50,  /* carbon.totlit */
+    IBIS_DAYST_TOTALIT = 51,  /* carbon.totalit */
+    IBIS_DAYST_TOTRLIT = 52,  /* carbon.totrlit */
+    IBIS_DAYST_TOTCSOI = 53,  /* carbon.totcsoi */
+    IBIS_DAYST_TOTFALL = 54,  /* carbon.totfall */
+    IBIS_DAYST_FALLL = 55,  /* carbon.falll */
+    IBIS_DAYST_FALLR = 56,  /* carbon.fallr */
+    IBIS_DAYST_FALLW = 57,  /* carbon.fallw */
+    IBIS_DAYST_COUNT = 58
 };
 
 /* Parameter record of the hourly step (all double; passed by value). */
@@ -465,5 +520,66 @@ typedef struct IbisParams {
 #define IBIS_FLAG_SOIL_MEANS 64u
 #define IBIS_FLAG_DIAG 128u
 #define IBIS_FLAG_KAHAN 256u
+
+/* Parameters of the daily cadence (phenology, soil biogeochemistry), all double. */
+typedef struct IbisDayParams {
+    double ddays;
+    double tthresh_u_offset;
+    double tthresh_u_abs;
+    double gthresh_u_c;
+    double gdd_thresh_u;
+    double gdd_ramp_u;
+    double tthresh_l_c;
+    double gthresh_l_c;
+    double gdd_thresh_l;
+    double gdd_ramp_l;
+    double drop_thresh;
+    double drop_stress_thresh;
+    double drop_floor;
+    double lig_frac;
+    double fbsom;
+    double effac;
+    double bgc_fmax;
+    double rconst;
+    double cnleaf;
+    double cnroot;
+    double cnwood;
+    double cnr[8];
+    double klm;
+    double kls;
+    double kll;
+    double krm;
+    double krs;
+    double krl;
+    double kwm;
+    double kws;
+    double kwl;
+    double kbn;
+    double kbp;
+    double knb;
+    double kns;
+    double kpb;
+    double kps;
+    double ksb;
+    double ylm;
+    double yls;
+    double yll;
+    double yrm;
+    double yrs;
+    double yrl;
+    double ywm;
+    double yws;
+    double ywl;
+    double ybn;
+    double ybp;
+    double yps;
+    double yns;
+    double ysb;
+    double ypb;
+    double ynb;
+    double lt_e0;
+    double wfps_opt;
+    double k_scale;
+} IbisDayParams;
 
 #endif /* IBIS_LAYOUT_H */

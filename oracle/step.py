@@ -27,7 +27,8 @@ FLAG_SOIL_MEANS = 1 << 6
 
 ACC_FIELDS = {"adrain": 1, "adsnow": 1, "adaet": 1, "a10ancub": 1, "a10ancls": 1, "a10ancl3": 1,
               "a10ancl4": 1, "aynpp": 12, "aynpptot": 1, "aygpptot": 1, "aytrunof": 1, "aytdrain": 1,
-              "ch4": 1, "tsoi_mean": 6, "wsoi_mean": 6, "wisoi_mean": 6, "tg_mean": 1, "afsena": 1}
+              "ch4": 1, "tsoi_mean": 6, "wsoi_mean": 6, "wisoi_mean": 6, "tg_mean": 1, "afsena": 1,
+              "stresstu_last": 1, "stresstl_last": 1}
 
 
 def new_acc(n):
@@ -332,6 +333,8 @@ def accumulate(acc, new, D, S, F, P):
     # canopy-top sensible heat of turvap (canopy_exchange.py:759), summed like
     # the other fluxes; the reference's day loop does not keep this sum
     acc["afsena"] = acc["afsena"] + D["fsena"] * dt
+    acc["stresstu_last"] = D["stresstu"].copy()
+    acc["stresstl_last"] = D["stresstl"].copy()
 
 
 def run_steps(prog, S, forcings, P, acc=None):

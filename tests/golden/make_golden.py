@@ -407,6 +407,73 @@ def write_diurnal_case(days=(15, 172), seed=7, dtime=3600.0):
     print(f"wrote {path}: {len(out)} arrays, {os.path.getsize(path)} bytes")
 
 
+def write_days_case(ndays=3, jday0=172, seed=9):
+    """tests/golden/days_16cells.npz: the reference's own GSWP3 day loop
+    (_run_month_scan, loops_gswp3.py:334-612) for ``ndays`` days on the 16-cell
+    checkpoint: phenology, 24 hourly steps with accumulators, 10-day means,
+    decomposition factors and soil BGC, every leaf recorded after each day.
+    Its variates (event timing, hourly wind) come from the counter-based
+    generator of the device forcing code; the float32 cast of each day is the
+    identity (the float64 run)."""
+    import jax
+    from ibis.io.restart import load_state
+    from oracle.weather import uniform24
+    fix = os.path.join(HERE, "restart_16cells.npz")
+    n = 16
+    st, _ = load_state(fix, create_ibis_state(GridConfig(nlon=1, nlat=1, npoi=n, nbedrock=3)))
+    consts = get_constants()
+    rng = np.random.Generator(np.random.PCG64(seed))
+    lat = rng.uniform(-40.0, 70.0, size=n)
+    sp = dataclasses.replace(loops.default_sim_params(n), latitude=_a(np.deg2rad(lat)), bedrock=BedrockParams())
+    days = []
+    for d in range(ndays):
+        dd, _ = daily_inputs(n, seed=seed + 10 + d)
+        dd["td"] = 0.5 * (dd["tmax"] + dd["tmin"]) + rng.uniform(-1.0, 1.0, n)
+        days.append(dd)
+    queue = []
+
+    def uniform(key, shape, *a, **k):
+        return jnp.asarray(queue.pop(0).reshape(shape))
+
+    saved = (getattr(jax.random, "uniform", None), loops_gswp3._cast_tree_f32)
+    jax.random.uniform = uniform
+    loops_gswp3._cast_tree_f32 = lambda tree: tree
+    out = {"in.lat": lat, "in.jday0": np.asarray(jday0), "in.seed": np.asarray(seed), "in.ndays": np.asarray(ndays)}
+    from ibis_b200 import dropin
+    from ibis_b200.params import PARAM_FIELDS, DAY_PARAM_FIELDS
+    P = dropin.step_params(st, consts, sp, 3600.0)
+    for name, _, _ in PARAM_FIELDS:
+        out["in.param." + name] = np.asarray(getattr(P, name), dtype=np.float64)
+    out["in.param.flags"] = np.asarray(P.flags, dtype=np.int64)
+    for name, _, _ in DAY_PARAM_FIELDS:
+        src = sp.bgc_params if hasattr(sp.bgc_params, "fmax" if name == "bgc_fmax" else name) else sp.pheno
+        out["in.dparam." + name] = np.asarray(getattr(src, "fmax" if name == "bgc_fmax" else name), dtype=np.float64)
+    for d, dd in enumerate(days):
+        for k, v in dd.items():
+            out[f"in.daily.{d}.{k}"] = np.asarray(v)
+    key = jnp.asarray(np.array([0, 1], dtype=np.uint32))
+    try:
+        for d, dd in enumerate(days):
+            cells = np.arange(n)
+            queue[:] = [uniform24(seed, cells, d, s) for s in range(26)]
+            xs = tuple(_a(np.asarray(dd[k])[None]) for k in ("td", "tmax", "tmin", "cloud", "precip", "psurf", "qd",
+                                                             "ud")) + (_a(np.zeros((1, n))), _a(dd["fira"][None]),
+                                                                       jnp.asarray(np.array([jday0 + d], np.int32)))
+            st, key, _ = loops_gswp3._run_month_scan(st, key, consts, sp, xs, 1, 365, 3600.0, 2)
+            assert not queue
+            for pth, v in zip(leaf_paths(st), jax.tree.flatten(st)[0]):
+                out[f"out.{d}.{pth}"] = np.asarray(v, dtype=np.float64)
+    finally:
+        if saved[0] is None:
+            del jax.random.uniform
+        else:
+            jax.random.uniform = saved[0]
+        loops_gswp3._cast_tree_f32 = saved[1]
+    path = os.path.join(HERE, "days_16cells.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path}: {len(out)} arrays, {os.path.getsize(path)} bytes")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--only", default=None)
@@ -418,7 +485,9 @@ def main():
         write_restart_subset()
     if args.only in (None, "diurnal"):
         write_diurnal_case()
-    if args.only in ("restart_leaves", "restart_1996", "diurnal"):
+    if args.only in (None, "days"):
+        write_days_case()
+    if args.only in ("restart_leaves", "restart_1996", "diurnal", "days"):
         return
     for name, spec in CASES.items():
         if args.only and name != args.only:
