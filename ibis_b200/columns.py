@@ -119,6 +119,19 @@ class Columns:
             v = v - a[L.N_ACC:]
         return synth.from_planes("ACC", v, self.ncell)
 
+    def set_acc(self, values: dict):
+        """Set accumulator planes (per-cell arrays named as ``layout.ACC``);
+        their compensation planes are zeroed, the other planes kept."""
+        if self.acc is None:
+            raise ValueError("accumulators were not allocated")
+        for name, v in values.items():
+            p0, k = L.OFF["ACC"][name]
+            a = np.asarray(v, dtype=np.float64).reshape(self.ncell, -1) if k > 1 else \
+                np.asarray(v, dtype=np.float64).reshape(1, self.ncell)
+            t = torch.from_numpy(np.ascontiguousarray(a.T if k > 1 else a)).to(self.acc)
+            self.acc[p0:p0 + k, :self.ncell] = t
+            self.acc[L.N_ACC + p0:L.N_ACC + p0 + k].zero_()
+
     def reset_acc(self):
         if self.acc is not None:
             self.acc.zero_()

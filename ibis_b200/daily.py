@@ -1,0 +1,147 @@
+"""The day loop on the device: daily cadence around the hourly steps.
+
+The reference's GSWP3 driver advances the state one day at a time
+(``_run_month_scan._day_body``, python-port/ibis/timestepping/loops_gswp3.py:382-608):
+phenology and the zeroing of the daily sums, the day's 24 hourly steps with
+their accumulators, then the 10-day means, annual sums, decomposition factors
+and one day of soil C/N.  :class:`DayLoop` keeps that whole day on the GPU:
+
+    ibis_day_begin  ->  ibis_diurnal_f32 (24 hours of forcing from the day's
+    weather)  ->  ibis_step (24 hours, accumulators on)  ->  ibis_day_end
+
+four launches per day with no host round trip, the daily-cadence state
+(``layout.DAYST``: phenology, 10-day means, annual sums, litter and soil
+carbon) resident beside the columns.  Seasonal formulations, the stress
+accumulator, crop and slot types are off, as in the reference's defaults.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import layout as L
+from . import lib as _lib
+from . import restart as _restart
+from . import synth
+from .columns import Columns
+from .forcing import OBSERVED_FIRA, hourly_forcing
+from .params import FLAG_ACC, DayParams, StepParams
+
+_TD = L.OFF["DAILY"]["td"][0]
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class DayLoop:
+    """Days of the reference's day loop on ``cols``.
+
+    ``params`` is the hourly step's record (accumulators are switched on),
+    ``day_params`` the phenology and soil-biogeochemistry constants, ``dayst``
+    the daily-cadence state as a dict of per-cell arrays named as
+    ``layout.DAYST`` (a checkpoint supplies it; see :meth:`from_restart`).
+    ``lat`` (degrees), ``seed``, ``jday`` (day of year of the next day) and
+    ``day`` (its counter for the variates) drive the forcing generator."""
+
+    def __init__(self, cols: Columns, params: StepParams, day_params: DayParams, dayst: dict, lat=None,
+                 seed: int = 0, jday: int = 1, day: int = 0, dtime: float = 3600.0, observed_fira: bool = True):
+        if cols.acc is None:
+            raise ValueError("the day loop needs the columns' accumulators")
+        self.cols = cols
+        self.params = params.copy()
+        self.params.flags |= FLAG_ACC
+        self.day_params = day_params
+        n, ld = cols.ncell, cols.ld
+        self.dayst = torch.from_numpy(synth.to_planes("DAYST", dayst, ld, cols._np_dtype)).to(cols.device)
+        lat = np.zeros(n) if lat is None else np.asarray(lat, dtype=np.float64)
+        lat_planes = np.zeros(ld, dtype=np.float32)
+        lat_planes[:n] = lat
+        self.lat = torch.from_numpy(lat_planes).to(cols.device)
+        self.seed, self.jday, self.day, self.dtime = int(seed), int(jday), int(day), float(dtime)
+        self.observed_fira = bool(observed_fira)
+        self.nh = int(round(86400.0 / self.dtime))
+        self._forc = None
+        self._td = torch.zeros(ld, dtype=cols.dtype, device=cols.device)
+        lib = _lib.load()
+        f32 = cols.dtype == torch.float32
+        self._begin = lib.ibis_day_begin_f32 if f32 else lib.ibis_day_begin_f64
+        self._end = lib.ibis_day_end_f32 if f32 else lib.ibis_day_end_f64
+
+    @classmethod
+    def from_restart(cls, path: str, dtype=torch.float32, device="cuda", params: StepParams | None = None,
+                     day_params: DayParams | None = None, **kw):
+        """A day loop seeded from a reference checkpoint: the columns, the
+        daily-cadence state, and the last hour's soil-water stress the next
+        day's phenology reads."""
+        cols, P, leaves, _, _ = _restart.columns_from_restart(path, dtype=dtype, device=device, params=params,
+                                                              acc=True)
+        n = cols.ncell
+        acc0 = _restart.group_from_leaves(leaves, "ACC", n)
+        cols.set_acc({k: acc0[k] for k in ("stresstu_last", "stresstl_last") if k in acc0})
+        dayst = _restart.group_from_leaves(leaves, "DAYST", n)
+        return cls(cols, P, day_params or DayParams(), dayst, **kw)
+
+    # ------------------------------------------------------------------ state
+    def dayst_host(self) -> dict:
+        return synth.from_planes("DAYST", self.dayst.cpu().numpy(), self.cols.ncell)
+
+    def set_dayst(self, dayst: dict):
+        a = synth.to_planes("DAYST", dayst, self.cols.ld, self.cols._np_dtype)
+        self.dayst.copy_(torch.from_numpy(a))
+
+    # ------------------------------------------------------------------ steps
+    def begin(self, td: torch.Tensor, stream=None):
+        """Phenology and the zeroing of the daily sums (``td``: the day's mean air temperature plane)."""
+        c = self.cols
+        stream = stream or torch.cuda.current_stream(c.device)
+        rc = self._begin(_ptr(c.stat), _ptr(self.dayst), _ptr(c.acc), _ptr(td), c.ncell, c.ld,
+                         ctypes.byref(self.params.to_c()), ctypes.byref(self.day_params.to_c()),
+                         ctypes.c_void_p(stream.cuda_stream))
+        _lib.check(rc, "ibis_day_begin")
+
+    def end(self, td: torch.Tensor, stream=None):
+        """10-day means, annual sums, decomposition factors, soil C/N and respiration sums."""
+        c = self.cols
+        stream = stream or torch.cuda.current_stream(c.device)
+        rc = self._end(_ptr(c.prog), _ptr(c.stat), _ptr(self.dayst), _ptr(c.acc), _ptr(td), c.ncell, c.ld,
+                       ctypes.byref(self.params.to_c()), ctypes.byref(self.day_params.to_c()),
+                       ctypes.c_void_p(stream.cuda_stream))
+        _lib.check(rc, "ibis_day_end")
+
+    def run_day(self, daily: torch.Tensor, forc: torch.Tensor | None = None, td: torch.Tensor | None = None,
+                stream=None):
+        """One day: ``daily`` is the day's weather ``(N_DAILY, ld)`` float32 on
+        the device.  The hourly forcing is generated from it unless ``forc``
+        (``(24, N_FORC, ld)`` in the columns' dtype) is given; the day's mean
+        temperature is its ``td`` plane unless ``td`` (``(ld,)`` in the
+        columns' dtype) is given."""
+        c = self.cols
+        stream = stream or torch.cuda.current_stream(c.device)
+        if daily.shape != (L.N_DAILY, c.ld) or daily.dtype != torch.float32 or daily.device != c.device:
+            raise ValueError(f"daily weather must be a ({L.N_DAILY}, {c.ld}) float32 tensor on the columns' device")
+        with torch.cuda.stream(stream):
+            self._td.copy_(daily[_TD] if td is None else td)
+            self.begin(self._td, stream)
+            if forc is None:
+                if self._forc is None:
+                    self._forc = torch.empty((self.nh, L.N_FORC, c.ld), dtype=torch.float32, device=c.device)
+                hourly_forcing(daily[None], self.lat, c.ncell, jday0=self.jday, day0=self.day, seed=self.seed,
+                               dtime=self.dtime, observed_fira=self.observed_fira, out=self._forc, stream=stream)
+                forc = self._forc if c.dtype == torch.float32 else self._forc.to(c.dtype)
+            c.run(forc, self.params, stream=stream)
+            self.end(self._td, stream)
+        self.jday = self.jday % 365 + 1
+        self.day += 1
+        return self
+
+    def run(self, daily: torch.Tensor, stream=None):
+        """``daily``: ``(nday, N_DAILY, ld)`` float32 on the device, one day after another."""
+        for d in range(daily.shape[0]):
+            self.run_day(daily[d], stream=stream)
+        return self
+
+
+__all__ = ["DayLoop", "OBSERVED_FIRA"]

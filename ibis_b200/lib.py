@@ -10,7 +10,7 @@ import ctypes
 import os
 import re
 
-from .params import IbisParamsC
+from .params import IbisDayParamsC, IbisParamsC
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
@@ -33,6 +33,8 @@ class IbisEnsembleC(ctypes.Structure):
 _c_int_p = ctypes.POINTER(ctypes.c_int)
 _P = ctypes.POINTER(IbisParamsC)
 _E = ctypes.POINTER(IbisEnsembleC)
+_DP = ctypes.POINTER(IbisDayParamsC)
+_V = ctypes.c_void_p
 
 # name -> (restype, argtypes); every function declared in include/*.h
 SIGNATURES = {
@@ -52,6 +54,10 @@ SIGNATURES = {
     "ibis_ensemble_occupancy": (ctypes.c_int, [_P, ctypes.c_int]),
     "ibis_diurnal_f32": (ctypes.c_int, [ctypes.c_void_p] * 3 + [ctypes.c_int] * 5
                          + [ctypes.c_float, ctypes.c_uint, ctypes.c_uint, ctypes.c_void_p]),
+    "ibis_day_begin_f32": (ctypes.c_int, [_V] * 4 + [ctypes.c_int] * 2 + [_P, _DP, _V]),
+    "ibis_day_begin_f64": (ctypes.c_int, [_V] * 4 + [ctypes.c_int] * 2 + [_P, _DP, _V]),
+    "ibis_day_end_f32": (ctypes.c_int, [_V] * 5 + [ctypes.c_int] * 2 + [_P, _DP, _V]),
+    "ibis_day_end_f64": (ctypes.c_int, [_V] * 5 + [ctypes.c_int] * 2 + [_P, _DP, _V]),
 }
 
 

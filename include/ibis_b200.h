@@ -159,6 +159,35 @@ int ibis_ensemble_occupancy(const IbisParams* params, int block);
 int ibis_diurnal_f32(const float* daily, const float* lat, float* forc, int ncell, int ld, int nday, int jday0,
                      int day0, float dtime, unsigned int seed, unsigned int flags, void* stream);
 
+/* Daily cadence of the day loop, one thread per cell, around a day's hourly
+ * steps (ibis_step_* with accumulators, fed by ibis_diurnal_f32 or by the
+ * caller's forcing):
+ *   stat   [IBIS_STAT_COUNT][ld]      frac, lai, ztop, zbot (begin), tco2mic (end)
+ *   dayst  [IBIS_DAYST_COUNT][ld]     phenology, 10-day means, annual sums,
+ *                                     litter and soil carbon pools (IBIS_DAYST_*)
+ *   acc    [2 * IBIS_ACC_COUNT][ld]   the step's accumulators with their
+ *                                     compensation planes
+ *   td     [ld]                       the day's mean air temperature (K)
+ *   prog   [IBIS_PROG_COUNT][ld]      soil temperature, water and ice (end)
+ * ibis_day_begin: phenology from the standing 10-day means and the last hour's
+ * soil-water stress (IBIS_ACC_STRESSTU_LAST / _STRESSTL_LAST), then the daily
+ * sums (adrain, adsnow, adaet, a10anc*) zeroed.
+ * ibis_day_end: 10-day means and annual sums from the daily sums, the
+ * decomposition factors, one day of soil C/N and the respiration sums.
+ * params supplies hsoi, ndaypy and epsilon; dayparams the phenology and
+ * soil-biogeochemistry constants.  Arithmetic is double for both buffer types.
+ * Replaces: the per-day body of _run_month_scan._day_body
+ * (python-port/ibis/timestepping/loops_gswp3.py:382-415 and 466-584), with
+ * pheno (physics/phenology.py:89-287) and soilbgc (physics/biogeochem.py:23-243). */
+int ibis_day_begin_f32(float* stat, float* dayst, float* acc, const float* td, int ncell, int ld,
+                       const IbisParams* params, const IbisDayParams* dayparams, void* stream);
+int ibis_day_begin_f64(double* stat, double* dayst, double* acc, const double* td, int ncell, int ld,
+                       const IbisParams* params, const IbisDayParams* dayparams, void* stream);
+int ibis_day_end_f32(const float* prog, float* stat, float* dayst, const float* acc, const float* td, int ncell,
+                     int ld, const IbisParams* params, const IbisDayParams* dayparams, void* stream);
+int ibis_day_end_f64(const double* prog, double* stat, double* dayst, const double* acc, const double* td,
+                     int ncell, int ld, const IbisParams* params, const IbisDayParams* dayparams, void* stream);
+
 /* Same contract in float64 throughout (the float64 run of the reference's step). */
 int ibis_step_f64(double* prog, const double* stat, const double* forc, double* diag, double* acc, int ncell,
                   int ld, int nstep, const IbisParams* params, int* status, void* stream);

@@ -42,3 +42,13 @@ def test_struct_layouts_match_ctypes(tmp_path):
     assert got[0] == ctypes.sizeof(IbisParamsC)
     assert got[1] == ctypes.sizeof(E)
     assert got[2:] == [getattr(E, n).offset for n in names]
+
+
+def test_day_params_layout_matches_ctypes(tmp_path):
+    from ibis_b200.params import IbisDayParamsC
+    names = [f[0] for f in IbisDayParamsC._fields_]
+    body = 'printf("%zu ", sizeof(IbisDayParams));'
+    body += "".join(f'printf("%zu ", offsetof(IbisDayParams, {n}));' for n in names)
+    got = _c_layout(tmp_path, body)
+    assert got[0] == ctypes.sizeof(IbisDayParamsC)
+    assert got[1:] == [getattr(IbisDayParamsC, n).offset for n in names]

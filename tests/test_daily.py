@@ -15,7 +15,7 @@ import numpy as np
 import pytest
 
 import oracle
-from goldens import compare
+from goldens import compare, rel_err
 from ibis_b200 import layout as L
 from ibis_b200 import restart
 from ibis_b200.params import DAY_PARAM_FIELDS, FLAG_ACC, FLAG_CH4, FLAG_KAHAN, PARAM_FIELDS, DayParams, StepParams
@@ -75,26 +75,228 @@ def test_checkpoint_implies_the_reference_parameters():
         np.testing.assert_allclose(getattr(Q, name), getattr(P, name), rtol=1e-12, err_msg=name)
 
 
-def test_oracle_day_loop_matches_reference_days():
+def day_weather(z, d):
+    return {k[len(f"in.daily.{d}."):]: v for k, v in z.items() if k.startswith(f"in.daily.{d}.")}
+
+
+def hourly(z, d, n):
+    """The day's 24 hourly forcing dicts (oracle/weather.py, observed longwave)."""
+    seed, jday0, cells, dd = int(z["in.seed"]), int(z["in.jday0"]), np.arange(n), day_weather(z, d)
+    plens, startp, endp = OW.precip_timing(OW.uniform24(seed, cells, d, 0), OW.uniform24(seed, cells, d, 1),
+                                           dd["precip"], 3600.0)
+    with np.errstate(all="ignore"):
+        return [OW.diurnal(h * 3600.0, jday0 + d, dd, z["in.lat"], plens, startp, endp,
+                           OW.uniform24(seed, cells, d, 2 + h), 3600.0, fira_obs=dd["fira"]) for h in range(24)]
+
+
+def oracle_days(ndays=None, perturb=None):
+    """The oracle's day loop on the three-day case; yields (day, prog, dayst,
+    stat, acc) after each day.  ``perturb`` = (day, hour, eps) scales the
+    temperatures of the state by (1 + eps) before that hour."""
     z, n, prog, stat, day, acc0, P = load_case()
     DP = day_params(z)
     acc = oracle.new_acc(n)
     for k in ACC_CHECK + ("stresstu_last", "stresstl_last"):
         if k in acc0:
             acc[k] = acc0[k].copy()
-    seed, jday0, cells = int(z["in.seed"]), int(z["in.jday0"]), np.arange(n)
-    for d in range(int(z["in.ndays"])):
-        dd = {k[len(f"in.daily.{d}."):]: v for k, v in z.items() if k.startswith(f"in.daily.{d}.")}
+    temps = ("tsoi", "tg", "tl", "tu", "ti", "tsno")
+    for d in range(int(z["in.ndays"]) if ndays is None else ndays):
+        dd = day_weather(z, d)
         day, stat, acc = OD.day_begin(day, stat, acc, dd["td"], P, DP)
-        plens, startp, endp = OW.precip_timing(OW.uniform24(seed, cells, d, 0), OW.uniform24(seed, cells, d, 1),
-                                               dd["precip"], 3600.0)
         with np.errstate(all="ignore"):
-            for h in range(24):
-                F = OW.diurnal(h * 3600.0, jday0 + d, dd, z["in.lat"], plens, startp, endp,
-                               OW.uniform24(seed, cells, d, 2 + h), 3600.0, fira_obs=dd["fira"])
-                prog, D, acc = oracle.step(prog, stat, F, P, acc)
+            for h, F in enumerate(hourly(z, d, n)):
+                if perturb is not None and perturb[:2] == (d, h):
+                    prog = {k: v * (1.0 + perturb[2]) if k in temps else v for k, v in prog.items()}
+                prog, _, acc = oracle.step(prog, stat, F, P, acc)
         day, stat = OD.day_end(prog, day, stat, acc, dd["td"], P, DP)
+        yield d, prog, day, stat, acc
+
+
+def test_oracle_day_loop_matches_reference_days():
+    z = load_case()[0]
+    for d, prog, day, stat, acc in oracle_days():
         bad = compare(prog, want(z, d, "PROG"), 1e-9) + compare(day, want(z, d, "DAYST"), 1e-9)
         bad += compare({k: stat[k] for k in STAT_CHECK}, want(z, d, "STAT"), 1e-9)
         bad += compare({k: acc[k] for k in ACC_CHECK}, want(z, d, "ACC"), 1e-6)
         assert not bad, (d, bad[:6])
+
+
+# Cells of the three-day case whose first day crosses a phase-change
+# threshold: cell 0 takes 400 mm of snow onto 289 K soil, cell 2 has a frozen
+# top layer under a thin snow cover.  A 1e-15 relative change of their
+# temperatures before hour 0 moves their end-of-day state by up to 2e-4
+# relative (test_threshold_cells_of_the_day_case), so last-bit differences
+# between CUDA's and the host's exp/log/pow do the same.
+DAY_THRESHOLD_CELLS = (0, 2)
+
+
+def test_threshold_cells_of_the_day_case():
+    """The exempt cells are threshold cells: the oracle's own day moves them
+    beyond 1e-9 under a 1e-15 perturbation and leaves every other cell within it."""
+    n = 16
+    _, base, bday, _, _ = next(oracle_days(1))
+    _, pert, pday, _, _ = next(oracle_days(1, perturb=(0, 0, -1e-15)))
+    err = np.zeros(n)
+    for got, ref in ((pert, base), (pday, bday)):
+        for k, w in ref.items():
+            e = np.nan_to_num(rel_err(np.asarray(got[k], np.float64), np.asarray(w, np.float64), 1e-3))
+            err = np.maximum(err, e.reshape(n, -1).max(axis=1))
+    moved = set(np.nonzero(err > 1e-9)[0].tolist())
+    assert moved == set(DAY_THRESHOLD_CELLS), sorted(moved)
+
+
+def _device_loop(dtype):
+    import torch
+    from ibis_b200.columns import Columns
+    from ibis_b200.daily import DayLoop
+    z, n, prog, stat, day, acc0, P = load_case()
+    cols = Columns.from_host(prog, stat, dtype=dtype, acc=True)
+    cols.set_acc({k: acc0[k] for k in ACC_CHECK + ("stresstu_last", "stresstl_last") if k in acc0})
+    loop = DayLoop(cols, P, day_params(z), day, lat=z["in.lat"], seed=int(z["in.seed"]), jday=int(z["in.jday0"]),
+                   day=0, observed_fira=True)
+    return z, n, cols, loop, torch
+
+
+def _daily_tensor(z, d, ld, torch):
+    from ibis_b200.forcing import daily_planes
+    dd = {k[len(f"in.daily.{d}."):]: v for k, v in z.items() if k.startswith(f"in.daily.{d}.")}
+    return dd, torch.from_numpy(daily_planes({k: v[None] for k, v in dd.items()}, ld)[0]).cuda()
+
+
+def _device_state(cols, loop):
+    from ibis_b200 import synth
+    stat = synth.from_planes("STAT", cols.stat.cpu().numpy(), cols.ncell)
+    return cols.prog_host(), loop.dayst_host(), stat, cols.acc_host()
+
+
+@pytest.mark.gpu
+def test_device_day_kernels_match_oracle(cuda_lib):
+    """ibis_day_begin_f64 / ibis_day_end_f64 on the oracle's own inputs of
+    each day of the three-day case: 1e-12 relative on everything they write."""
+    import torch
+    from ibis_b200 import synth
+    z, n, cols, loop, torch = _device_loop(torch.float64)
+    _, _, prog, stat, day, acc0, P = load_case()
+    DP = day_params(z)
+    acc = oracle.new_acc(n)
+    for k in ACC_CHECK + ("stresstu_last", "stresstl_last"):
+        if k in acc0:
+            acc[k] = acc0[k].copy()
+    pad = lambda a: torch.from_numpy(np.pad(np.asarray(a, np.float64), (0, cols.ld - n))).cuda()
+
+    def load(prog_, stat_, day_, acc_):
+        cols.set_prog(prog_)
+        cols.set_stat(stat_)
+        cols.set_acc(acc_)
+        loop.set_dayst(day_)
+
+    def check(day_, stat_, acc_=None):
+        gs = synth.from_planes("STAT", cols.stat.cpu().numpy(), n)
+        bad = compare(loop.dayst_host(), day_, 1e-12) + compare({k: gs[k] for k in stat_}, stat_, 1e-12)
+        if acc_ is not None:
+            bad += compare(cols.acc_host(), acc_, 1e-12)
+        return bad
+
+    for d in range(int(z["in.ndays"])):
+        dd = day_weather(z, d)
+        load(prog, stat, day, acc)
+        day, stat, acc = OD.day_begin(day, stat, acc, dd["td"], P, DP)
+        loop.begin(pad(dd["td"]))
+        torch.cuda.synchronize()
+        bad = check(day, stat, acc)
+        assert not bad, ("begin", d, bad[:6])
+        with np.errstate(all="ignore"):
+            for F in hourly(z, d, n):
+                prog, _, acc = oracle.step(prog, stat, F, P, acc)
+        load(prog, stat, day, acc)
+        day, stat = OD.day_end(prog, day, stat, acc, dd["td"], P, DP)
+        loop.end(pad(dd["td"]))
+        torch.cuda.synchronize()
+        bad = check(day, stat)
+        assert not bad, ("end", d, bad[:6])
+
+
+@pytest.mark.gpu
+def test_device_day_loop_f64_matches_reference_days(cuda_lib):
+    """The device day loop (daily kernels + the float64 hourly step), fed each
+    day's hourly forcing in float64, against the reference's day loop after
+    each of the three days: 1e-9 relative on every cell but the threshold
+    cells (DAY_THRESHOLD_CELLS), which stay within 1e-2 (their puddle ice,
+    ~8e-5 kg m-2, moves by 0.3 %)."""
+    import torch
+    from ibis_b200 import synth
+    z, n, cols, loop, torch = _device_loop(torch.float64)
+    keep = np.setdiff1d(np.arange(n), DAY_THRESHOLD_CELLS)
+    for d in range(int(z["in.ndays"])):
+        dd, daily = _daily_tensor(z, d, cols.ld, torch)
+        hours = hourly(z, d, n)
+        forc = {k: np.stack([F[k] for F in hours]) for k in hours[0]}
+        td = torch.from_numpy(np.pad(dd["td"], (0, cols.ld - n))).cuda()
+        loop.run_day(daily, forc=torch.from_numpy(synth.forcing_planes(forc, cols.ld, dtype=np.float64)).cuda(), td=td)
+        torch.cuda.synchronize()
+        prog, dayst, stat, acc = _device_state(cols, loop)
+        pairs = [(prog, want(z, d, "PROG")), (dayst, want(z, d, "DAYST")),
+                 ({k: stat[k] for k in STAT_CHECK}, want(z, d, "STAT"))]
+        for got, ref in pairs:
+            sub = lambda x, c: {k: np.asarray(v)[c] for k, v in x.items() if k in ref}
+            bad = compare(sub(got, keep), sub(ref, keep), 1e-9)
+            bad += compare(sub(got, list(DAY_THRESHOLD_CELLS)), sub(ref, list(DAY_THRESHOLD_CELLS)), 1e-2)
+            assert not bad, (d, bad[:6])
+        bad = compare({k: acc[k][keep] for k in ACC_CHECK}, {k: v[keep] for k, v in want(z, d, "ACC").items()}, 1e-6)
+        assert not bad, (d, bad[:6])
+
+
+@pytest.mark.gpu
+def test_device_day_loop_f32_generated_forcing(cuda_lib):
+    """The whole day on the device in float32 -- forcing generated from the
+    daily weather, hourly step, daily kernels -- against the reference's
+    float64 day loop after three days.
+
+    Float32 moves the canopy-air and leaf temperatures of single cells by up to
+    ~2 K within a day (the reference's own float32 run departs from its float64
+    run by up to 1.6 K in hourly canopy temperature,
+    docs/technote/17_numerics_verification.md:367-383), and through them the
+    fast litter pools.  So: phenology, 10-day means, canopy structure, slow soil
+    pools and leaching within 1e-4 relative on every cell; litter, microbial
+    carbon and respiration within 5e-2 on every cell and 5e-3 on all but three;
+    temperatures within 3 K on every cell and 0.2 K on all but three; soil
+    water within 3e-2 and 2e-3 on all but three."""
+    import torch
+    z, n, cols, loop, torch = _device_loop(torch.float32)
+    for d in range(int(z["in.ndays"])):
+        _, daily = _daily_tensor(z, d, cols.ld, torch)
+        loop.run_day(daily)
+    torch.cuda.synchronize()
+    d = int(z["in.ndays"]) - 1
+    prog, dayst, stat, acc = _device_state(cols, loop)
+    for group in (prog, dayst, stat):
+        for k, v in group.items():
+            assert np.all(np.isfinite(v)), k
+
+    def per_cell(got, ref, absolute=False):
+        a = np.asarray(got, np.float64).reshape(ref.shape)
+        e = np.abs(a - ref) if absolute else np.nan_to_num(rel_err(a, ref, 1e-3))
+        return np.sort(e.reshape(n, -1).max(axis=1))
+
+    w = want(z, d, "DAYST")
+    tight = ("tempu", "templ", "agddu", "agddl", "dropu", "dropls", "dropl3", "dropl4", "a10td", "a10ancub",
+             "a10ancls", "a10ancl3", "a10ancl4", "ayprcp", "csoislop", "csoislon", "csoipas", "totcsoi", "storedn",
+             "tnmin", "yrleach", "ynleach")
+    for k in tight:
+        assert per_cell(dayst[k], w[k])[-1] < 1e-4, k
+    for k in ("clitlm", "clitls", "clitll", "clitrm", "clitrs", "clitrl", "clitwm", "clitws", "clitwl", "totcmic",
+              "totlit", "ayco2mic", "ayaet"):
+        e = per_cell(dayst[k], w[k])
+        assert e[-1] < 5e-2 and e[-4] < 5e-3, (k, e[-4:])
+    w = want(z, d, "STAT")
+    for k in ("frac", "lai", "ztop", "zbot"):
+        assert per_cell(stat[k], w[k])[-1] < 1e-4, k
+    e = per_cell(stat["tco2mic"], w["tco2mic"])
+    assert e[-1] < 5e-2 and e[-4] < 5e-3, ("tco2mic", e[-4:])
+    w = want(z, d, "PROG")
+    for k in ("tsoi", "tg", "tu", "tl", "ts", "ti", "tsno", "t12", "t34"):
+        e = per_cell(prog[k], w[k], absolute=True)
+        assert e[-1] < 3.0 and e[-4] < 0.2, (k, e[-4:])
+    for k in ("wsoi", "wisoi"):
+        e = per_cell(prog[k], w[k])
+        assert e[-1] < 3e-2 and e[-4] < 2e-3, (k, e[-4:])
