@@ -42,6 +42,7 @@ UNITS = {
     "ibis_diurnal_f32.cu": ["-use_fast_math"],
     "ibis_step_f64.cu": ["--fmad=false"],
     "ibis_daily.cu": ["--fmad=false"],
+    "ibis_month.cu": ["--fmad=false"],
 }
 
 

@@ -381,10 +381,12 @@ __device__ __forceinline__ void fire_counters(Col<R>& c, R swilt0, const Forc<R>
     c.sdry_vpd = c.sdry_vpd + fl * hit;
 }
 
-// methane_flux (methane.py:233-383), kgC m-2 d-1
-template <typename R, typename Q>
-__device__ __forceinline__ R methane(R f_inund, R rh, const R (&t)[NL], const R (&w)[NL], const R (&i)[NL],
-                                     const DevParams<R>& P, const Q& q) {
+// wetland_water_table (methane.py:233-276): the water table inside the
+// inundated fraction, m; a finite observed depth `zwt_obs` replaces it, clipped
+// to [0, z_max] (methane.py:366-367).
+template <typename R>
+__device__ __forceinline__ R wetland_water_table(const R (&w)[NL], const R (&i)[NL], R z_wt_max, R zwt_obs,
+                                                 const DevParams<R>& P) {
     R acc = R(0.0);
 #pragma unroll
     for (int k = 0; k < NL; ++k) {
@@ -393,7 +395,15 @@ __device__ __forceinline__ R methane(R f_inund, R rh, const R (&t)[NL], const R 
     }
     R ttop = acc / P.ch4_wtot;
     R wet = clip(ttop / mx(P.sat_crit, R(1e-6)), R(0.0), R(1.0));
-    R zwt = q.z_wt_max() * (R(1.0) - wet);
+    R zwt = z_wt_max * (R(1.0) - wet);
+    return isfinite(zwt_obs) ? clip(zwt_obs, R(0.0), P.z_max) : zwt;
+}
+
+// methane_flux (methane.py:233-383), kgC m-2 d-1; zwt_obs NaN: the model's water table
+template <typename R, typename Q>
+__device__ __forceinline__ R methane(R f_inund, R rh, const R (&t)[NL], const R (&w)[NL], const R (&i)[NL],
+                                     R zwt_obs, const DevParams<R>& P, const Q& q) {
+    R zwt = wetland_water_table(w, i, q.z_wt_max(), zwt_obs, P);
     R tt = R(0.0), tw = R(0.0);
 #pragma unroll
     for (int k = 0; k < NL; ++k) {

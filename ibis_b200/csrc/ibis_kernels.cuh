@@ -404,7 +404,8 @@ static int hourly_step(R* prog, const R* stat, const R* forc, R* diag, R* acc, i
     if (ncell < 0 || nstep < 0 || ld < ncell || (ld % 32) != 0) return -EINVAL;
     if (ncell == 0 || nstep == 0) return 0;
     const unsigned known = IBIS_FLAG_BEDROCK | IBIS_FLAG_H2O_CONSISTENT | IBIS_FLAG_SUNSHADE_U | IBIS_FLAG_SUNSHADE_L |
-                           IBIS_FLAG_ACC | IBIS_FLAG_CH4 | IBIS_FLAG_SOIL_MEANS | IBIS_FLAG_DIAG | IBIS_FLAG_KAHAN;
+                           IBIS_FLAG_ACC | IBIS_FLAG_CH4 | IBIS_FLAG_SOIL_MEANS | IBIS_FLAG_DIAG | IBIS_FLAG_KAHAN |
+                           IBIS_FLAG_ZWT_OBS;
     if (hp->flags & ~known) return -EINVAL;
     if ((hp->flags & (IBIS_FLAG_ACC | IBIS_FLAG_CH4 | IBIS_FLAG_SOIL_MEANS)) && !acc) return -EINVAL;
     if ((hp->flags & IBIS_FLAG_DIAG) && !diag) return -EINVAL;

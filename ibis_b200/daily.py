@@ -13,6 +13,12 @@ four launches per day with no host round trip, the daily-cadence state
 (``layout.DAYST``: phenology, 10-day means, annual sums, litter and soil
 carbon) resident beside the columns.  Seasonal formulations, the stress
 accumulator, crop and slot types are off, as in the reference's defaults.
+
+:meth:`DayLoop.run_month` adds the month's wetland methane
+(``ibis_month_begin`` / ``ibis_month_end``: ``methane_step`` or
+``methane_step_from_mean``, optionally ``scale_month`` and the carbon
+partition, python-port/ibis/bgc/methane.py:431-496) over the ``layout.WET``
+planes.
 """
 from __future__ import annotations
 
@@ -27,9 +33,10 @@ from . import restart as _restart
 from . import synth
 from .columns import Columns
 from .forcing import OBSERVED_FIRA, hourly_forcing
-from .params import FLAG_ACC, DayParams, StepParams
+from .params import FLAG_ACC, FLAG_CH4, DayParams, StepParams
 
 _TD = L.OFF["DAILY"]["td"][0]
+MONTH_NEW_YEAR, MONTH_FROM_MEAN, MONTH_PARTITION = 1, 2, 4
 
 
 def _ptr(t):
@@ -69,6 +76,9 @@ class DayLoop:
         f32 = cols.dtype == torch.float32
         self._begin = lib.ibis_day_begin_f32 if f32 else lib.ibis_day_begin_f64
         self._end = lib.ibis_day_end_f32 if f32 else lib.ibis_day_end_f64
+        self._mbegin = lib.ibis_month_begin_f32 if f32 else lib.ibis_month_begin_f64
+        self._mend = lib.ibis_month_end_f32 if f32 else lib.ibis_month_end_f64
+        self.wet = torch.zeros((L.N_WET, ld), dtype=cols.dtype, device=cols.device)
 
     @classmethod
     def from_restart(cls, path: str, dtype=torch.float32, device="cuda", params: StepParams | None = None,
@@ -91,6 +101,13 @@ class DayLoop:
     def set_dayst(self, dayst: dict):
         a = synth.to_planes("DAYST", dayst, self.cols.ld, self.cols._np_dtype)
         self.dayst.copy_(torch.from_numpy(a))
+
+    def wet_host(self) -> dict:
+        return synth.from_planes("WET", self.wet.cpu().numpy(), self.cols.ncell)
+
+    def set_wet(self, wet: dict):
+        a = synth.to_planes("WET", wet, self.cols.ld, self.cols._np_dtype)
+        self.wet.copy_(torch.from_numpy(a))
 
     # ------------------------------------------------------------------ steps
     def begin(self, td: torch.Tensor, stream=None):
@@ -135,6 +152,39 @@ class DayLoop:
             self.end(self._td, stream)
         self.jday = self.jday % 365 + 1
         self.day += 1
+        return self
+
+    def begin_month(self, new_year: bool = False, stream=None):
+        """Zero the CH4 accumulator and keep ayco2mic for the carbon partition;
+        ``new_year`` clears the annual sums first (reset_annual)."""
+        c = self.cols
+        stream = stream or torch.cuda.current_stream(c.device)
+        rc = self._mbegin(_ptr(c.acc), _ptr(self.wet), _ptr(self.dayst), c.ncell, c.ld,
+                          MONTH_NEW_YEAR if new_year else 0, ctypes.c_void_p(stream.cuda_stream))
+        _lib.check(rc, "ibis_month_begin")
+
+    def end_month(self, ndays: int, from_mean: bool = True, scale: torch.Tensor | None = None,
+                  partition: bool = False, stream=None):
+        """The month's methane step; ``scale`` is an optional ``(ld,)`` inundated
+        fraction in the columns' dtype (scale_month)."""
+        c = self.cols
+        stream = stream or torch.cuda.current_stream(c.device)
+        if from_mean and not self.params.flags & FLAG_CH4:
+            raise ValueError("the month's mean flux needs the hourly CH4 accumulator (FLAG_CH4)")
+        if scale is not None and (scale.shape != (c.ld,) or scale.dtype != c.dtype or scale.device != c.device):
+            raise ValueError(f"scale must be a ({c.ld},) tensor of the columns' dtype and device")
+        flags = (MONTH_FROM_MEAN if from_mean else 0) | (MONTH_PARTITION if partition else 0)
+        rc = self._mend(_ptr(c.prog), _ptr(c.stat), _ptr(c.acc), _ptr(self.wet), _ptr(self.dayst),
+                        ctypes.c_void_p(0) if scale is None else _ptr(scale), c.ncell, c.ld, int(ndays),
+                        ctypes.byref(self.params.to_c()), flags, ctypes.c_void_p(stream.cuda_stream))
+        _lib.check(rc, "ibis_month_end")
+
+    def run_month(self, daily: torch.Tensor, from_mean: bool = True, scale: torch.Tensor | None = None,
+                  partition: bool = False, new_year: bool = False, stream=None):
+        """A calendar month (``daily``: ``(ndays, N_DAILY, ld)``) and its wetland methane."""
+        self.begin_month(new_year, stream)
+        self.run(daily, stream)
+        self.end_month(daily.shape[0], from_mean, scale, partition, stream)
         return self
 
     def run(self, daily: torch.Tensor, stream=None):

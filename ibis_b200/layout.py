@@ -20,6 +20,7 @@ The planes are grouped into buffers by how the step uses them:
 ``YEARLY`` accumulator totals an ensemble run reports at each year end
 ``DAILY``  daily weather the device forcing generator turns into hours
 ``DAYST``  state of the daily cadence (phenology, 10-day means, soil carbon)
+``WET``    monthly wetland methane state
 
 Each field names the leaf of the reference ``IBISState`` it mirrors
 (``python-port/ibis/state/*.py``), so host code can move data between the
@@ -116,6 +117,7 @@ STAT = (
     Field("sapfrac", "vegetation.sapfrac"),
     Field("tco2mic", "vegetation.tco2mic"),
     Field("f_inund", "methane.f_inund"),
+    Field("zwt_obs", "methane.zwt_obs"),   # observed wetland water table, m (NaN: the model's); read under FLAG_ZWT_OBS
 )
 
 FORC = (
@@ -334,8 +336,20 @@ DAYST = (
     Field("fallw", "carbon.fallw"),
 )
 
+# Monthly wetland methane (MethaneState, python-port/ibis/bgc/methane.py:404-423)
+# and what the month's end needs from its start: the heterotrophic respiration
+# total then (for the carbon partition) and the year's CH4 carbon taken out of
+# Rh so far (scripts/run_global.py:786-839).
+WET = (
+    Field("flux", "wetland.flux"),
+    Field("annual", "wetland.annual"),
+    Field("zwt", "wetland.zwt"),
+    Field("rh0", "summary.ayco2mic"),      # ayco2mic at the month's start
+    Field("ch4c", "summary.ayrh_ch4c"),    # the year's CH4 carbon taken out of Rh
+)
+
 GROUPS = {"PROG": PROG, "STAT": STAT, "FORC": FORC, "DIAG": DIAG, "ACC": ACC, "RUN": RUN, "YEARLY": YEARLY,
-          "DAILY": DAILY, "DAYST": DAYST}
+          "DAILY": DAILY, "DAYST": DAYST, "WET": WET}
 
 
 def offsets(group):
@@ -360,6 +374,7 @@ N_RUN = nplanes(RUN)
 N_YEARLY = nplanes(YEARLY)
 N_DAILY = nplanes(DAILY)
 N_DAYST = nplanes(DAYST)
+N_WET = nplanes(WET)
 
 OFF = {g: offsets(v) for g, v in GROUPS.items()}
 

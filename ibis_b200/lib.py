@@ -58,6 +58,10 @@ SIGNATURES = {
     "ibis_day_begin_f64": (ctypes.c_int, [_V] * 4 + [ctypes.c_int] * 2 + [_P, _DP, _V]),
     "ibis_day_end_f32": (ctypes.c_int, [_V] * 5 + [ctypes.c_int] * 2 + [_P, _DP, _V]),
     "ibis_day_end_f64": (ctypes.c_int, [_V] * 5 + [ctypes.c_int] * 2 + [_P, _DP, _V]),
+    "ibis_month_begin_f32": (ctypes.c_int, [_V] * 3 + [ctypes.c_int] * 2 + [ctypes.c_uint, _V]),
+    "ibis_month_begin_f64": (ctypes.c_int, [_V] * 3 + [ctypes.c_int] * 2 + [ctypes.c_uint, _V]),
+    "ibis_month_end_f32": (ctypes.c_int, [_V] * 6 + [ctypes.c_int] * 3 + [_P, ctypes.c_uint, _V]),
+    "ibis_month_end_f64": (ctypes.c_int, [_V] * 6 + [ctypes.c_int] * 3 + [_P, ctypes.c_uint, _V]),
 }
 
 

@@ -188,6 +188,40 @@ int ibis_day_end_f32(const float* prog, float* stat, float* dayst, const float* 
 int ibis_day_end_f64(const double* prog, double* stat, double* dayst, const double* acc, const double* td,
                      int ncell, int ld, const IbisParams* params, const IbisDayParams* dayparams, void* stream);
 
+/* Monthly wetland methane around a month of days (one thread per cell):
+ *   wet    [IBIS_WET_COUNT][ld]     flux, annual, zwt (the MethaneState leaves),
+ *                                   rh0 (ayco2mic at the month's start), ch4c
+ *                                   (the year's CH4 carbon taken out of Rh)
+ *   acc    [2 * IBIS_ACC_COUNT][ld] the step's accumulators (IBIS_ACC_CH4: the
+ *                                   sum of the day means of the hourly flux)
+ *   dayst  [IBIS_DAYST_COUNT][ld]   ayco2mic (may be NULL unless partitioning)
+ * ibis_month_begin: zero the CH4 accumulator, keep ayco2mic in rh0; with
+ * IBIS_MONTH_NEW_YEAR clear annual and ch4c first (reset_annual).
+ * ibis_month_end: the month's flux -- with IBIS_MONTH_FROM_MEAN the mean of
+ * the hourly fluxes (methane_step_from_mean), else methane_flux of the
+ * end-of-month state with Rh = tco2mic * 12e-3 * 86400 (methane_step) --, the
+ * water table (observed where params->flags has IBIS_FLAG_ZWT_OBS and the
+ * STAT zwt_obs plane is finite), annual += flux * ndays; then, if `scale`
+ * (per-cell inundated fraction, [ld]) is not NULL, scale_month; then with
+ * IBIS_MONTH_PARTITION the month's CH4 carbon (ch4_carbon_from_rh) is taken
+ * out of ayco2mic and added to ch4c.
+ * Replaces: methane_step / methane_step_from_mean / reset_annual / scale_month /
+ * ch4_carbon_from_rh (python-port/ibis/bgc/methane.py:431-496) as the GSWP3
+ * month driver calls them (timestepping/loops_gswp3.py:740-760). */
+#define IBIS_MONTH_NEW_YEAR 1u
+#define IBIS_MONTH_FROM_MEAN 2u
+#define IBIS_MONTH_PARTITION 4u
+int ibis_month_begin_f32(float* acc, float* wet, const float* dayst, int ncell, int ld, unsigned int flags,
+                         void* stream);
+int ibis_month_begin_f64(double* acc, double* wet, const double* dayst, int ncell, int ld, unsigned int flags,
+                         void* stream);
+int ibis_month_end_f32(const float* prog, const float* stat, const float* acc, float* wet, float* dayst,
+                       const float* scale, int ncell, int ld, int ndays, const IbisParams* params,
+                       unsigned int flags, void* stream);
+int ibis_month_end_f64(const double* prog, const double* stat, const double* acc, double* wet, double* dayst,
+                       const double* scale, int ncell, int ld, int ndays, const IbisParams* params,
+                       unsigned int flags, void* stream);
+
 /* Same contract in float64 throughout (the float64 run of the reference's step). */
 int ibis_step_f64(double* prog, const double* stat, const double* forc, double* diag, double* acc, int ncell,
                   int ld, int nstep, const IbisParams* params, int* status, void* stream);

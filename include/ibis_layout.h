@@ -84,7 +84,8 @@ enum {
     IBIS_STAT_SAPFRAC = 121,  /* vegetation.sapfrac */
     IBIS_STAT_TCO2MIC = 122,  /* vegetation.tco2mic */
     IBIS_STAT_F_INUND = 123,  /* methane.f_inund */
-    IBIS_STAT_COUNT = 124
+    IBIS_STAT_ZWT_OBS = 124,  /* methane.zwt_obs */
+    IBIS_STAT_COUNT = 125
 };
 
 /* FORC */
@@ -297,6 +298,16 @@ enum {
     IBIS_DAYST_FALLR = 56,  /* carbon.fallr */
     IBIS_DAYST_FALLW = 57,  /* carbon.fallw */
     IBIS_DAYST_COUNT = 58
+};
+
+/* WET */
+enum {
+    IBIS_WET_FLUX = 0,  /* wetland.flux */
+    IBIS_WET_ANNUAL = 1,  /* wetland.annual */
+    IBIS_WET_ZWT = 2,  /* wetland.zwt */
+    IBIS_WET_RH0 = 3,  /* summary.ayco2mic */
+    IBIS_WET_CH4C = 4,  /* summary.ayrh_ch4c */
+    IBIS_WET_COUNT = 5
 };
 
 /* Parameter record of the hourly step (all double; passed by value). */
@@ -520,6 +531,7 @@ typedef struct IbisParams {
 #define IBIS_FLAG_SOIL_MEANS 64u
 #define IBIS_FLAG_DIAG 128u
 #define IBIS_FLAG_KAHAN 256u
+#define IBIS_FLAG_ZWT_OBS 512u
 
 /* Parameters of the daily cadence (phenology, soil biogeochemistry), all double. */
 typedef struct IbisDayParams {

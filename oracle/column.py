@@ -365,7 +365,10 @@ def fire_counters(prog, wsoi0, wisoi0, swilt0, F, P):
 # ---------------------------------------------------------------------------
 
 
-def methane(f_inund, rh, tsoi, wsoi, wisoi, hsoi, P):
+def wetland_water_table(wsoi, wisoi, hsoi, P, zwt_obs=None):
+    """wetland_water_table (methane.py:233-276), with an observed depth (finite
+    entries of ``zwt_obs``, clipped to [0, z_max]) in its place where given
+    (methane.py:366-367)."""
     theta = clip(wsoi * (1.0 - wisoi) + wisoi, 0.0, 1.0)
     bot = np.cumsum(hsoi)
     top = np.concatenate([[0.0], bot[:-1]])
@@ -374,6 +377,17 @@ def methane(f_inund, rh, tsoi, wsoi, wisoi, hsoi, P):
     ttop = np.sum(theta * w[None, :], axis=1) / tot
     wet = clip(ttop / max(P.sat_crit, 1e-6), 0.0, 1.0)
     zwt = P.z_wt_max * (1.0 - wet)
+    if zwt_obs is not None:
+        zo = np.asarray(zwt_obs, dtype=np.float64)
+        with np.errstate(invalid="ignore"):
+            zwt = np.where(np.isfinite(zo), np.clip(zo, 0.0, P.z_max), zwt)
+    return zwt
+
+
+def methane(f_inund, rh, tsoi, wsoi, wisoi, hsoi, P, zwt_obs=None):
+    bot = np.cumsum(hsoi)
+    top = np.concatenate([[0.0], bot[:-1]])
+    zwt = wetland_water_table(wsoi, wisoi, hsoi, P, zwt_obs)
     below = bot[None, :] - np.maximum(zwt[:, None], top[None, :])
     an = clip(below / hsoi[None, :], 0.0, 1.0) * hsoi[None, :]
     th = an * (tsoi >= 273.15)

@@ -24,6 +24,7 @@ FLAG_SUNSHADE_L = 1 << 3
 FLAG_ACC = 1 << 4
 FLAG_CH4 = 1 << 5
 FLAG_SOIL_MEANS = 1 << 6
+FLAG_ZWT_OBS = 1 << 9
 
 ACC_FIELDS = {"adrain": 1, "adsnow": 1, "adaet": 1, "a10ancub": 1, "a10ancls": 1, "a10ancl3": 1,
               "a10ancl4": 1, "aynpp": 12, "aynpptot": 1, "aygpptot": 1, "aytrunof": 1, "aytdrain": 1,
@@ -256,7 +257,9 @@ def step(prog, S, F, P, acc=None):
         w = np.float64(np.float32(dt / 86400.0))
         if P.flags & FLAG_CH4:
             rh = S["tco2mic"] * np.float64(np.float32(12.0e-3 * 86400.0))
-            acc_new["ch4"] = acc_new["ch4"] + methane(S["f_inund"], rh, new["tsoi"], new["wsoi"], new["wisoi"], hsoi, P) * w
+            zo = S["zwt_obs"] if P.flags & FLAG_ZWT_OBS else None
+            acc_new["ch4"] = acc_new["ch4"] + methane(S["f_inund"], rh, new["tsoi"], new["wsoi"], new["wisoi"], hsoi, P,
+                                                      zo) * w
         if P.flags & FLAG_SOIL_MEANS:
             acc_new["tsoi_mean"] = acc_new["tsoi_mean"] + new["tsoi"] * w
             acc_new["wsoi_mean"] = acc_new["wsoi_mean"] + new["wsoi"] * w

@@ -474,6 +474,68 @@ def write_days_case(ndays=3, jday0=172, seed=9):
     print(f"wrote {path}: {len(out)} arrays, {os.path.getsize(path)} bytes")
 
 
+def write_methane_case(seed=21, ndays=31):
+    """tests/golden/methane_month.npz: the reference's monthly wetland methane
+    functions (bgc/methane.py:233-496) on the 16-cell checkpoint's soil state:
+    the water table with and without an observed depth (NaN, negative and
+    beyond-z_max entries included), the flux, ``methane_step``,
+    ``methane_step_from_mean``, ``scale_month``, ``ch4_carbon_from_rh`` and
+    ``reset_annual``, under the default and one non-default MethaneParams."""
+    from ibis.bgc import methane as M
+    from ibis.io.restart import load_state
+    n = 16
+    st, _ = load_state(os.path.join(HERE, "restart_16cells.npz"),
+                       create_ibis_state(GridConfig(nlon=1, nlat=1, npoi=n, nbedrock=3)))
+    so = st.soil
+    tsoi, wsoi, wisoi = (np.asarray(x, np.float64) for x in (so.tsoi, so.wsoi, so.wisoi))
+    hsoi = np.asarray(so.hsoi, np.float64)[:tsoi.shape[1]]
+    rng = np.random.Generator(np.random.PCG64(seed))
+    wisoi = wisoi.copy()
+    wisoi[:4] = rng.uniform(0.0, 0.9, (4, tsoi.shape[1]))        # frozen soil in a few cells
+    tsoi = tsoi.copy()
+    tsoi[4:7] = 270.0 + rng.uniform(0.0, 6.0, (3, tsoi.shape[1]))  # thawed/frozen layers around tmelt
+    f_inund = rng.uniform(-0.1, 1.1, n)
+    rh = rng.uniform(0.0, 5e-3, n)
+    rh[0] = -1e-4
+    zwt_obs = rng.uniform(-0.3, 5.0, n)
+    zwt_obs[rng.uniform(size=n) < 0.4] = np.nan
+    flux_month = rng.uniform(0.0, 1e-4, n)
+    annual0 = rng.uniform(0.0, 1e-2, n)
+    scale = rng.uniform(0.0, 1.2, n)
+    rh_now, rh_before = rng.uniform(0.2, 0.4, n), rng.uniform(0.0, 0.3, n)
+    out = {"in.tsoi": tsoi, "in.wsoi": wsoi, "in.wisoi": wisoi, "in.hsoi": hsoi, "in.f_inund": f_inund, "in.rh": rh,
+           "in.zwt_obs": zwt_obs, "in.flux_month": flux_month, "in.annual0": annual0, "in.scale": scale,
+           "in.rh_now": rh_now, "in.rh_before": rh_before, "in.ndays": np.asarray(ndays)}
+    variants = {"default": M.MethaneParams(),
+                "custom": M.MethaneParams(z_wt_max=0.45, sat_crit=0.85, q10p=2.1, r_ch4=0.31, z_tau=0.35,
+                                          tau_oxid=0.2, t_ref=290.0, z_max=3.0)}
+    a = lambda x: np.asarray(x, np.float64)
+    for tag, p in variants.items():
+        for f in ("sat_crit", "z_max", "r_ch4", "q10p", "t_ref", "z_wt_max", "z_wt_ref", "z_tau", "tau_oxid"):
+            out[f"param.{tag}.{f}"] = np.asarray(float(getattr(p, f)))
+        out[f"{tag}.zwt"] = a(M.wetland_water_table(_a(wsoi), _a(wisoi), _a(hsoi), p))
+        out[f"{tag}.flux"] = a(M.methane_flux(_a(f_inund), _a(rh), _a(tsoi), _a(wsoi), _a(wisoi), _a(hsoi), p))
+        out[f"{tag}.flux_obs"] = a(M.methane_flux(_a(f_inund), _a(rh), _a(tsoi), _a(wsoi), _a(wisoi), _a(hsoi), p,
+                                                  zwt_obs=_a(zwt_obs)))
+        m0 = M.MethaneState(flux=_a(np.zeros(n)), annual=_a(annual0), zwt=_a(np.zeros(n)))
+        for obs in (False, True):
+            zo = _a(zwt_obs) if obs else None
+            sfx = "_obs" if obs else ""
+            ms = M.methane_step(m0, _a(f_inund), _a(rh), _a(tsoi), _a(wsoi), _a(wisoi), _a(hsoi), ndays, p, zwt_obs=zo)
+            mm = M.methane_step_from_mean(m0, _a(flux_month), _a(wsoi), _a(wisoi), _a(hsoi), ndays, p, zwt_obs=zo)
+            for name, st_ in (("step", ms), ("mean", mm)):
+                for leaf in ("flux", "annual", "zwt"):
+                    out[f"{tag}.{name}{sfx}.{leaf}"] = a(getattr(st_, leaf))
+            sc = M.scale_month(mm, _a(annual0), _a(scale))
+            for leaf in ("flux", "annual", "zwt"):
+                out[f"{tag}.scaled{sfx}.{leaf}"] = a(getattr(sc, leaf))
+            out[f"{tag}.take{sfx}"] = a(M.ch4_carbon_from_rh(sc.annual, _a(annual0), _a(rh_now), _a(rh_before)))
+        out[f"{tag}.reset.annual"] = a(M.reset_annual(m0).annual)
+    path = os.path.join(HERE, "methane_month.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path}: {len(out)} arrays, {os.path.getsize(path)} bytes")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--only", default=None)
@@ -487,7 +549,9 @@ def main():
         write_diurnal_case()
     if args.only in (None, "days"):
         write_days_case()
-    if args.only in ("restart_leaves", "restart_1996", "diurnal", "days"):
+    if args.only in (None, "methane_month"):
+        write_methane_case()
+    if args.only in ("restart_leaves", "restart_1996", "diurnal", "days", "methane_month"):
         return
     for name, spec in CASES.items():
         if args.only and name != args.only:
