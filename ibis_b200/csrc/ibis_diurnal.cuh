@@ -6,7 +6,8 @@
 // direct/diffuse split (Friend transmissivity), the Campbell-Norman Fourier
 // temperature cycle, humidity capped at 99 % saturation, EPIC wind from one
 // variate, Idso longwave (or the observed daily value) and the rain/snow split
-// of the event.  The reference draws its variates from jax.random; these are
+// of the event; optionally an observed hourly shortwave in place of the
+// generator's (observed_shortwave, weather.py:458-481).  The reference draws its variates from jax.random; these are
 // counter-based (the SplitMix64 finalizer of Steele, Lea and Flood 2014 over
 // (seed, day, slot) and the cell), so any hour of any cell can be regenerated
 // without state.  FP32 arithmetic, with the day's orbital terms in double.
@@ -109,6 +110,27 @@ __device__ __forceinline__ Forc<float> diurnal_hour(const DailyRec& d, const Day
     F.rain = in_event && warm ? rate : 0.0f;
     F.snow = in_event && !warm ? rate : 0.0f;
     return F;
+}
+
+// observed_shortwave (weather.py:458-481): an observed hourly total `sw_obs`
+// split into direct and diffuse by the hourly clearness-index relation of
+// Spitters et al. (1986), all diffuse with the sun down, then into the two
+// bands; `s0` is the day's effective solar constant.
+__device__ __forceinline__ void observed_shortwave(float sw_obs, float s0, Forc<float>& F) {
+    const float cz = F.cosz;
+    const float kt = fminf(fmaxf(sw_obs / fmaxf(s0 * cz, 1.0f), 0.0f), 1.0f);
+    const float r = 0.847f - 1.61f * cz + 1.04f * cz * cz;
+    const float kk = (1.47f - r) / 1.66f;
+    float fd = kt <= 0.22f ? 1.0f
+             : kt <= 0.35f ? 1.0f - 6.4f * (kt - 0.22f) * (kt - 0.22f)
+             : kt <= kk    ? 1.47f - 1.66f * kt
+                           : r;
+    fd = cz <= 0.0f ? 1.0f : fminf(fmaxf(fd, 0.0f), 1.0f);
+    const float sw = fmaxf(sw_obs, 0.0f);
+    F.sd[0] = sw * 0.46f * (1.0f - fd);
+    F.sd[1] = sw * 0.54f * (1.0f - fd);
+    F.si[0] = sw * 0.46f * fd;
+    F.si[1] = sw * 0.54f * fd;
 }
 
 __device__ __forceinline__ void store_forc(const Forc<float>& F, float* __restrict__ f, int ld) {

@@ -129,12 +129,13 @@ class DayLoop:
         _lib.check(rc, "ibis_day_end")
 
     def run_day(self, daily: torch.Tensor, forc: torch.Tensor | None = None, td: torch.Tensor | None = None,
-                stream=None):
+                stream=None, sw_obs: torch.Tensor | None = None, use: torch.Tensor | None = None):
         """One day: ``daily`` is the day's weather ``(N_DAILY, ld)`` float32 on
         the device.  The hourly forcing is generated from it unless ``forc``
         (``(24, N_FORC, ld)`` in the columns' dtype) is given; the day's mean
         temperature is its ``td`` plane unless ``td`` (``(ld,)`` in the
-        columns' dtype) is given."""
+        columns' dtype) is given.  ``sw_obs`` ``(24, ld)`` and ``use``
+        ``(ld,)``: the day's observed hourly shortwave and the cells that use it."""
         c = self.cols
         stream = stream or torch.cuda.current_stream(c.device)
         if daily.shape != (L.N_DAILY, c.ld) or daily.dtype != torch.float32 or daily.device != c.device:
@@ -146,7 +147,9 @@ class DayLoop:
                 if self._forc is None:
                     self._forc = torch.empty((self.nh, L.N_FORC, c.ld), dtype=torch.float32, device=c.device)
                 hourly_forcing(daily[None], self.lat, c.ncell, jday0=self.jday, day0=self.day, seed=self.seed,
-                               dtime=self.dtime, observed_fira=self.observed_fira, out=self._forc, stream=stream)
+                               dtime=self.dtime, observed_fira=self.observed_fira, out=self._forc, stream=stream,
+                               sw_obs=None if sw_obs is None else sw_obs[None],
+                               use=None if use is None else use[None])
                 forc = self._forc if c.dtype == torch.float32 else self._forc.to(c.dtype)
             c.run(forc, self.params, stream=stream)
             self.end(self._td, stream)

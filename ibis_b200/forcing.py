@@ -35,9 +35,13 @@ def daily_planes(daily: dict, ld: int, dtype=np.float32):
 
 def hourly_forcing(daily: torch.Tensor, lat: torch.Tensor, ncell: int, jday0: int = 1, day0: int = 0,
                    seed: int = 0, dtime: float = 3600.0, observed_fira: bool = False, out: torch.Tensor | None = None,
-                   stream=None) -> torch.Tensor:
+                   stream=None, sw_obs: torch.Tensor | None = None, use: torch.Tensor | None = None) -> torch.Tensor:
     """Hourly FORC planes ``(nday * 86400/dtime, N_FORC, ld)`` for ``daily``
-    ``(nday, N_DAILY, ld)`` (float32, on the GPU) at latitudes ``lat`` (degrees)."""
+    ``(nday, N_DAILY, ld)`` (float32, on the GPU) at latitudes ``lat`` (degrees).
+
+    ``sw_obs`` ``(nday, 86400/dtime, ld)`` float32 and ``use`` ``(nday, ld)``
+    bool/uint8: an observed hourly shortwave total for the cell-days ``use``
+    marks (``observed_shortwave``, weather.py:458-481)."""
     if daily.dtype != torch.float32 or daily.device.type != "cuda" or daily.dim() != 3:
         raise ValueError("daily must be a (nday, N_DAILY, ld) float32 CUDA tensor")
     nday, npl, ld = daily.shape
@@ -49,6 +53,23 @@ def hourly_forcing(daily: torch.Tensor, lat: torch.Tensor, ncell: int, jday0: in
     if not (daily.is_contiguous() and out.is_contiguous() and lat.is_contiguous()):
         raise ValueError("buffers must be contiguous")
     stream = stream or torch.cuda.current_stream(daily.device)
+    if sw_obs is not None:
+        if use is None or sw_obs.shape != (nday, nh, ld) or sw_obs.dtype != torch.float32 or use.shape != (nday, ld):
+            raise ValueError(f"sw_obs must be ({nday}, {nh}, {ld}) float32 and use ({nday}, {ld})")
+        if sw_obs.device != daily.device or use.device != daily.device:
+            raise ValueError("sw_obs and use must be on the daily weather's device")
+        use8 = use.to(torch.uint8).contiguous()
+        sw_obs = sw_obs.contiguous()
+        for t in (use8, sw_obs):               # temporaries the kernel reads on `stream`
+            t.record_stream(stream)
+        rc = _lib.load().ibis_diurnal_sw_f32(ctypes.c_void_p(daily.data_ptr()), ctypes.c_void_p(lat.data_ptr()),
+                                             ctypes.c_void_p(sw_obs.data_ptr()), ctypes.c_void_p(use8.data_ptr()),
+                                             ctypes.c_void_p(out.data_ptr()), int(ncell), int(ld), int(nday),
+                                             int(jday0), int(day0), float(dtime), int(seed) & 0xFFFFFFFF,
+                                             OBSERVED_FIRA if observed_fira else 0,
+                                             ctypes.c_void_p(stream.cuda_stream))
+        _lib.check(rc, "ibis_diurnal_sw_f32")
+        return out
     rc = _lib.load().ibis_diurnal_f32(ctypes.c_void_p(daily.data_ptr()), ctypes.c_void_p(lat.data_ptr()),
                                       ctypes.c_void_p(out.data_ptr()), int(ncell), int(ld), int(nday), int(jday0),
                                       int(day0), float(dtime), int(seed) & 0xFFFFFFFF,

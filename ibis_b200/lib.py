@@ -54,6 +54,8 @@ SIGNATURES = {
     "ibis_ensemble_occupancy": (ctypes.c_int, [_P, ctypes.c_int]),
     "ibis_diurnal_f32": (ctypes.c_int, [ctypes.c_void_p] * 3 + [ctypes.c_int] * 5
                          + [ctypes.c_float, ctypes.c_uint, ctypes.c_uint, ctypes.c_void_p]),
+    "ibis_diurnal_sw_f32": (ctypes.c_int, [_V] * 5 + [ctypes.c_int] * 5
+                            + [ctypes.c_float, ctypes.c_uint, ctypes.c_uint, _V]),
     "ibis_day_begin_f32": (ctypes.c_int, [_V] * 4 + [ctypes.c_int] * 2 + [_P, _DP, _V]),
     "ibis_day_begin_f64": (ctypes.c_int, [_V] * 4 + [ctypes.c_int] * 2 + [_P, _DP, _V]),
     "ibis_day_end_f32": (ctypes.c_int, [_V] * 5 + [ctypes.c_int] * 2 + [_P, _DP, _V]),

@@ -159,6 +159,17 @@ int ibis_ensemble_occupancy(const IbisParams* params, int block);
 int ibis_diurnal_f32(const float* daily, const float* lat, float* forc, int ncell, int ld, int nday, int jday0,
                      int day0, float dtime, unsigned int seed, unsigned int flags, void* stream);
 
+/* ibis_diurnal_f32 with an observed hourly shortwave total where a cell-day
+ * has one: sw_obs [nday][86400/dtime][ld] (W m-2 at each hour), use [nday][ld]
+ * (nonzero: that cell-day uses it).  Where used, the total is split into direct
+ * and diffuse by the hourly clearness-index relation of Spitters et al. (1986)
+ * and into the two bands; elsewhere the generator's shortwave stands.
+ * Replaces: observed_shortwave (python-port/ibis/physics/weather.py:458-481), applied
+ * per hour by _run_day_inner (loops_gswp3.py:126-129). */
+int ibis_diurnal_sw_f32(const float* daily, const float* lat, const float* sw_obs, const unsigned char* use,
+                        float* forc, int ncell, int ld, int nday, int jday0, int day0, float dtime, unsigned int seed,
+                        unsigned int flags, void* stream);
+
 /* Daily cadence of the day loop, one thread per cell, around a day's hourly
  * steps (ibis_step_* with accumulators, fed by ibis_diurnal_f32 or by the
  * caller's forcing):

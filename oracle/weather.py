@@ -106,3 +106,22 @@ def diurnal(time, jday, daily, lat_deg, plens, startp, endp, u_wind, dtime, fira
     return dict(coszen=coszen, ta=ta, qa=qa, ua=ua, psurf=np.asarray(psurf, dtype=np.float64), fira=fira,
                 raina=np.where(in_event & warm, rate, 0.0), snowa=np.where(in_event & ~warm, rate, 0.0),
                 solad=solad, solai=solai)
+
+
+def observed_shortwave(sw_obs, use, coszen, jday, solad_gen, solai_gen):
+    """observed_shortwave (weather.py:458-481): where ``use`` is set, the observed
+    hourly total split into direct and diffuse by the hourly clearness-index
+    relation of Spitters et al. (1986), then into the two bands; elsewhere the
+    generator's values unchanged."""
+    coszen = np.asarray(coszen, dtype=np.float64)
+    kt = np.clip(sw_obs / np.maximum(effective_solar_constant(jday) * coszen, 1.0), 0.0, 1.0)
+    r = 0.847 - 1.61 * coszen + 1.04 * coszen ** 2
+    kk = (1.47 - r) / 1.66
+    fd = np.where(kt <= 0.22, 1.0, np.where(kt <= 0.35, 1.0 - 6.4 * (kt - 0.22) ** 2,
+                                            np.where(kt <= kk, 1.47 - 1.66 * kt, r)))
+    fd = np.where(coszen <= 0.0, 1.0, np.clip(fd, 0.0, 1.0))
+    sw = np.maximum(sw_obs, 0.0)
+    solad = sw[:, None] * BANDS[None, :] * (1.0 - fd)[:, None]
+    solai = sw[:, None] * BANDS[None, :] * fd[:, None]
+    use = np.asarray(use, dtype=bool)[:, None]
+    return np.where(use, solad, solad_gen), np.where(use, solai, solai_gen)

@@ -474,6 +474,30 @@ def write_days_case(ndays=3, jday0=172, seed=9):
     print(f"wrote {path}: {len(out)} arrays, {os.path.getsize(path)} bytes")
 
 
+def write_observed_sw_case(seed=23, n=64):
+    """tests/golden/observed_sw.npz: the reference's ``observed_shortwave``
+    (physics/weather.py:458-481) on random observed totals (negative, zero and
+    above-clear-sky included), sun heights (below the horizon included), masks
+    and generator values, on four days of the year."""
+    from ibis.physics.weather import observed_shortwave
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = {}
+    for d, jday in enumerate((1, 80, 172, 300)):
+        sw = rng.uniform(-50.0, 1300.0, n)
+        sw[:4] = (0.0, 1e-3, 1500.0, -1.0)
+        cz = rng.uniform(-0.3, 1.0, n)
+        cz[4:8] = (0.0, 1e-4, 1.0, -1e-4)
+        use = rng.uniform(size=n) < 0.7
+        sd, si = rng.uniform(0.0, 500.0, (n, 2)), rng.uniform(0.0, 200.0, (n, 2))
+        a, b = observed_shortwave(_a(sw), jnp.asarray(use), _a(cz), jday, _a(sd), _a(si))
+        out.update({f"{d}.sw": sw, f"{d}.coszen": cz, f"{d}.use": use, f"{d}.solad_gen": sd, f"{d}.solai_gen": si,
+                    f"{d}.jday": np.asarray(jday), f"{d}.solad": np.asarray(a, np.float64),
+                    f"{d}.solai": np.asarray(b, np.float64)})
+    path = os.path.join(HERE, "observed_sw.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path}: {len(out)} arrays, {os.path.getsize(path)} bytes")
+
+
 def write_methane_case(seed=21, ndays=31):
     """tests/golden/methane_month.npz: the reference's monthly wetland methane
     functions (bgc/methane.py:233-496) on the 16-cell checkpoint's soil state:
@@ -551,7 +575,9 @@ def main():
         write_days_case()
     if args.only in (None, "methane_month"):
         write_methane_case()
-    if args.only in ("restart_leaves", "restart_1996", "diurnal", "days", "methane_month"):
+    if args.only in (None, "observed_sw"):
+        write_observed_sw_case()
+    if args.only in ("restart_leaves", "restart_1996", "diurnal", "days", "methane_month", "observed_sw"):
         return
     for name, spec in CASES.items():
         if args.only and name != args.only:

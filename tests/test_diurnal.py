@@ -134,3 +134,55 @@ def test_generated_forcing_drives_the_step(cuda_lib):
     cols.run(f, wl.params)
     torch.cuda.synchronize()
     assert not cols.nonfinite()[0]
+
+
+def _sw_golden():
+    z = np.load(os.path.join(HERE, "golden", "observed_sw.npz"))
+    return {k: z[k] for k in z.files}
+
+
+def test_oracle_matches_reference_observed_shortwave():
+    z = _sw_golden()
+    for d in range(4):
+        a, b = W.observed_shortwave(z[f"{d}.sw"], z[f"{d}.use"], z[f"{d}.coszen"], int(z[f"{d}.jday"]),
+                                    z[f"{d}.solad_gen"], z[f"{d}.solai_gen"])
+        np.testing.assert_allclose(a, z[f"{d}.solad"], rtol=1e-12, atol=1e-300)
+        np.testing.assert_allclose(b, z[f"{d}.solai"], rtol=1e-12, atol=1e-300)
+    assert (z["0.coszen"] <= 0).any() and z["0.use"].any() and (~z["0.use"]).any()
+
+
+@pytest.mark.gpu
+def test_device_observed_shortwave_matches_oracle(cuda_lib):
+    """Generated forcing with an observed hourly shortwave on the cell-days
+    marked: shortwave = the oracle's observed_shortwave of the generator's hour
+    within 1e-4 relative / 1e-3 W m-2; every other field as without it."""
+    import torch
+    from ibis_b200 import forcing, layout as L, synth
+    z = _golden()
+    d, lat = _daily(z), z["in.lat"]
+    n = lat.size
+    ld = L.leading_dim(n)
+    rng = np.random.Generator(np.random.PCG64(5))
+    lat_t = torch.zeros(ld, dtype=torch.float32, device="cuda")
+    lat_t[:n] = torch.from_numpy(lat.astype(np.float32)).cuda()
+    for di, jday in enumerate(z["in.days"]):
+        planes = torch.from_numpy(forcing.daily_planes({k: v[None] for k, v in d.items()}, ld)).cuda()
+        sw = np.zeros((1, 24, ld), np.float32)
+        sw[0, :, :n] = rng.uniform(-20.0, 1100.0, (24, n))
+        use = np.zeros((1, ld), np.uint8)
+        use[0, :n] = rng.uniform(size=n) < 0.6
+        plain = forcing.hourly_forcing(planes, lat_t, n, jday0=int(jday), day0=di, seed=7)
+        got = forcing.hourly_forcing(planes, lat_t, n, jday0=int(jday), day0=di, seed=7,
+                                     sw_obs=torch.from_numpy(sw).cuda(), use=torch.from_numpy(use).cuda())
+        torch.cuda.synchronize()
+        got, plain = got.cpu().numpy(), plain.cpu().numpy()
+        for h in range(24):
+            g = synth.from_planes("FORC", got[h], n)
+            p = synth.from_planes("FORC", plain[h], n)
+            for k in g:
+                if k not in ("solad", "solai"):
+                    np.testing.assert_array_equal(g[k], p[k], err_msg=k)
+            sd, si = W.observed_shortwave(sw[0, h, :n].astype(np.float64), use[0, :n].astype(bool),
+                                          p["coszen"], int(jday), p["solad"], p["solai"])
+            np.testing.assert_allclose(g["solad"], sd, rtol=1e-4, atol=1e-3, err_msg=f"{di} {h} solad")
+            np.testing.assert_allclose(g["solai"], si, rtol=1e-4, atol=1e-3, err_msg=f"{di} {h} solai")
