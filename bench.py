@@ -493,9 +493,142 @@ def run_serve(args):
     print(json.dumps(line), flush=True)
 
 
+def run_month(args):
+    """The day loop over a month: 95,333 columns x 30 days, each day the
+    daily cadence (phenology, daily sums / 10-day means, decomposition, soil
+    C/N), 24 hours of forcing generated on the GPU from the day's weather and
+    24 hourly steps with accumulators and hourly CH4, then the month's wetland
+    methane (DayLoop.run_month).  One step = one month; the daily weather is
+    resident on the device.  e2e: the month's daily weather copied in from
+    pinned host memory and the prognostic, daily-cadence and wetland state read
+    back, inside the timed region."""
+    import torch
+    from ibis_b200 import forcing as _forcing
+    from ibis_b200 import synth
+    from ibis_b200.columns import Columns
+    from ibis_b200.daily import DayLoop
+    from ibis_b200.params import FLAG_CH4, DayParams
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    nday = args.days
+    wl = synth.make_workload(args.ncell, 1, seed=11)
+    rng = np.random.Generator(np.random.PCG64(12))
+    dayst = synth.make_dayst(rng, wl.stat, wl.latitude)
+    cols = Columns.from_host(wl.prog, wl.stat, dtype=torch.float32, device=dev, acc=True)
+    if args.config is not None:
+        cols.set_mode(args.config)
+    P = wl.params.copy()
+    P.flags |= FLAG_CH4
+    loop = DayLoop(cols, P, DayParams(), dayst, lat=wl.latitude, seed=5, jday=152, day=0)
+    h_daily = torch.from_numpy(_forcing.daily_planes(synth.make_daily_weather(rng, wl.latitude, nday),
+                                                     cols.ld)).pin_memory()
+    d_daily = h_daily.to(dev)
+    prog0, stat0, acc0, dayst0 = cols.prog.clone(), cols.stat.clone(), cols.acc.clone(), loop.dayst.clone()
+    tuned = None
+    if args.config is None:
+        from ibis_b200 import tune as _tune
+        f0 = _forcing.hourly_forcing(d_daily[:1].contiguous(), loop.lat, cols.ncell, jday0=152, seed=5,
+                                     observed_fira=True)
+        tuned = _tune.tune(cols, f0, P, reps=2)
+        del f0
+    stream = torch.cuda.current_stream(dev)
+    h_prog = torch.empty_like(cols.prog, device="cpu").pin_memory()
+    h_dayst = torch.empty_like(loop.dayst, device="cpu").pin_memory()
+    h_wet = torch.empty_like(loop.wet, device="cpu").pin_memory()
+
+    def reset():
+        cols.prog.copy_(prog0); cols.stat.copy_(stat0); cols.acc.copy_(acc0); loop.dayst.copy_(dayst0)
+        loop.wet.zero_()
+        loop.jday, loop.day = 152, 0
+
+    def month():
+        loop.run_month(d_daily, from_mean=True, new_year=False, stream=stream)
+
+    def month_e2e():
+        d_daily.copy_(h_daily, non_blocking=True)
+        loop.run_month(d_daily, from_mean=True, new_year=False, stream=stream)
+        h_prog.copy_(cols.prog, non_blocking=True)
+        h_dayst.copy_(loop.dayst, non_blocking=True)
+        h_wet.copy_(loop.wet, non_blocking=True)
+
+    def timed(fn, k):
+        out = []
+        for _ in range(k):
+            reset()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+            out.append(a.elapsed_time(b))
+        return out
+
+    with ClockSampler(local) as clk:
+        timed(month, args.warmup)
+        ms = timed(month, args.steps)
+    ms_e2e = timed(month_e2e, args.steps)
+    nonfinite = cols.nonfinite()
+
+    # where the month's time goes: each launch kind timed on its own over one month
+    reset()
+    parts = {"hourly_step": [], "forcing": [], "day_begin": [], "day_end": []}
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+    for d in range(nday):
+        daily = d_daily[d]
+        marks = [ev() for _ in range(5)]
+        marks[0].record(stream)
+        loop._td.copy_(daily[0])
+        loop.begin(loop._td, stream)
+        marks[1].record(stream)
+        _forcing.hourly_forcing(daily[None], loop.lat, cols.ncell, jday0=loop.jday, day0=loop.day, seed=loop.seed,
+                                observed_fira=True, out=loop._forc if loop._forc is not None else None,
+                                stream=stream)
+        marks[2].record(stream)
+        cols.run(loop._forc, loop.params, stream=stream)
+        marks[3].record(stream)
+        loop.end(loop._td, stream)
+        marks[4].record(stream)
+        marks[4].synchronize()
+        parts["day_begin"].append(marks[0].elapsed_time(marks[1]))
+        parts["forcing"].append(marks[1].elapsed_time(marks[2]))
+        parts["hourly_step"].append(marks[2].elapsed_time(marks[3]))
+        parts["day_end"].append(marks[3].elapsed_time(marks[4]))
+    part_ms = {k: float(np.sum(v)) for k, v in parts.items()}
+    m = float(np.mean(ms))
+    cs = args.ncell * 24 * nday
+    step_ms = part_ms["hourly_step"] / nday
+    bpl = _algorithmic_bytes(HOURS) * args.ncell
+    peak, peak_kind = _peaks()
+    line = {
+        "metric": "cell-steps/s, day loop over a month (daily cadence + hourly steps + monthly CH4)",
+        "value": cs / (m / 1e3), "unit": "cell-steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": m, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"{args.ncell} cells x {nday} days (one month) per step: per day the daily cadence, "
+                               "24 hours of forcing generated from the day's weather, 24 hourly steps with "
+                               "accumulators and hourly CH4; the month's wetland methane at its end",
+                   "ncell": args.ncell, "days": nday, "launch_config": cols.config,
+                   "tuned_ms": ({str(k): round(v, 4) for k, v in tuned["ms"].items()} if tuned else None),
+                   "l2": "state (27 MB) + statics (48 MB) + a day's forcing (110 MB) exceed L2 each day"},
+        "launch_ms_per_month": part_ms,
+        "roofline": {"bound": "hbm", "kernel": "hourly step (24 h per launch)",
+                     "achieved": bpl / (step_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": bpl / (step_ms / 1e3) / 1e9 / peak, "traffic": None, "peak_source": peak_kind},
+        "e2e": {"value": cs / (float(np.mean(ms_e2e)) / 1e3), "unit": "cell-steps/s",
+                "h2d_bytes_per_step": int(h_daily.numel() * 4),
+                "d2h_bytes_per_step": int((h_prog.numel() + h_dayst.numel() + h_wet.numel()) * 4)},
+        "gpu_launches": args.steps * (4 * nday + 2),
+        "clocks": clk.summary(), "nonfinite_columns": nonfinite[0],
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", default="day", choices=["day", "ensemble", "serve"])
+    ap.add_argument("--workload", default="day", choices=["day", "ensemble", "serve", "month"])
+    ap.add_argument("--days", type=int, default=30, help="month: days per step")
     ap.add_argument("--sites", type=int, default=356)
     ap.add_argument("--params-per-site", type=int, default=64)
     ap.add_argument("--tune", action="store_true", help="ensemble: autotune the block size first")
@@ -518,6 +651,8 @@ def main():
         run_reference(args)
     elif args.workload == "ensemble":
         run_ensemble(args)
+    elif args.workload == "month":
+        run_month(args)
     elif args.workload == "serve":
         run_serve(args)
     else:

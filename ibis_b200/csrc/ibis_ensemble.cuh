@@ -148,13 +148,14 @@ __global__ void __launch_bounds__(256, 1) ensemble_kernel(const EnsArgs e, const
             load_col(c, e.prog + r, e.ld_run);
             load_run_params(q, e.run_params + r, e.ld_run, P);
             const Stat<float> S{e.stat + site, e.ld_site};
-            const Acc<float> A{e.acc ? e.acc + r : nullptr, e.ld_run, kahan};
+            Acc<float> A{e.acc ? e.acc + r : nullptr, e.ld_run, kahan};
             // steps of this call until the run's next year end, and that year's index
             int next_year = e.year_steps - pos % e.year_steps;
             int year = pos / e.year_steps;
 #pragma unroll 1
             for (int s = 0; s < nstep; ++s) {
                 const Forc<float> F = load_forc_record(f + (size_t)s * IBIS_FORC_COUNT);
+                A.last = (s + 1 == nstep);
                 column_step<float, NT, SU, SL>(c, F, S, D, A, P, q);
                 if (s + 1 == next_year) {
                     if (e.yearly && year < e.nyear) yearly_snapshot(e, A, r, year);
@@ -190,7 +191,7 @@ __global__ void __launch_bounds__(128, 2) ensemble_hour_kernel(const EnsArgs e, 
     load_col(c, e.prog + r, e.ld_run);
     load_run_params(q, e.run_params + r, e.ld_run, P);
     const Stat<float> S{e.stat + site, e.ld_site};
-    const Acc<float> A{e.acc ? e.acc + r : nullptr, e.ld_run, (P.flags & IBIS_FLAG_KAHAN) != 0};
+    const Acc<float> A{e.acc ? e.acc + r : nullptr, e.ld_run, (P.flags & IBIS_FLAG_KAHAN) != 0, hour + 1 == nstep};
     const Forc<float> F = load_forc_record(e.forc + (size_t)(first + hour) * IBIS_FORC_COUNT);
     column_step<float, NT, SU, SL>(c, F, S, Diag<float>{nullptr, 0}, A, P, q);
     if (e.yearly && (pos + hour + 1) % e.year_steps == 0) {

@@ -140,6 +140,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) hourly_step_kernel(R* __restrict_
 #pragma unroll 1
     for (int s = 0; s < nstep; ++s) {
         Forc<R> F = load_forc(forc + (size_t)s * forc_stride + i, ld);
+        A.last = (s + 1 == nstep);
         column_step<R, NT, SU, SL>(c, F, S, D, A, P, UniformQ<R>{P});
     }
     R sum = store_col(c, prog + i, ld);

@@ -12,6 +12,7 @@ struct Acc {
     R* __restrict__ base;  // nullptr: no accumulators
     int ld;
     bool kahan;
+    bool last = true;      // the launch's last hour for this cell: keep the end-of-hour values
     __device__ __forceinline__ void add(int plane, R x) const {
         R* v = base + (size_t)plane * ld;
         if (kahan) {
@@ -604,8 +605,10 @@ __device__ __forceinline__ void ground_phase(Col<R>& c, const Forc<R>& F, const 
             Ac.add(IBIS_ACC_AYTRUNOF, grunof * dt);
             Ac.add(IBIS_ACC_AYTDRAIN, wflo[NL] * dt);
             Ac.add(IBIS_ACC_AFSENA, M.fsena * dt);
-            Ac.base[(size_t)IBIS_ACC_STRESSTU_LAST * Ac.ld] = stresstu;
-            Ac.base[(size_t)IBIS_ACC_STRESSTL_LAST * Ac.ld] = stresstl;
+            if (Ac.last) {
+                Ac.base[(size_t)IBIS_ACC_STRESSTU_LAST * Ac.ld] = stresstu;
+                Ac.base[(size_t)IBIS_ACC_STRESSTL_LAST * Ac.ld] = stresstl;
+            }
         }
         if (P.flags & IBIS_FLAG_CH4) {
             R rh = S(IBIS_STAT_TCO2MIC) * P.rh_conv;

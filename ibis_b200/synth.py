@@ -330,6 +330,48 @@ def make_workload(ncell, nhour, seed=0, lat_range=(-60.0, 80.0), lat=None, alpha
                     latitude=lat, start_doy=start_doy, meta=dict(seed=seed, edge_cases=cases, alpha=alpha))
 
 
+def make_dayst(rng, stat, lat):
+    """Seeded daily-cadence state (``layout.DAYST``) in the ranges of a spun-up
+    run: potential LAI from the columns' existence flags, 10-day means near the
+    climate of the latitude, annual sums part-way through a year, litter and
+    soil carbon pools of a few kgC m-2."""
+    n = lat.shape[0]
+    u = lambda lo, hi, shape=(n,): rng.uniform(lo, hi, shape)
+    tclim = 300.0 - 0.35 * np.abs(lat)
+    plai = stat["exist"] * u(0.5, 6.0, (n, L.NPFT))
+    d = dict(plai=plai, tc=tclim - 273.16 - u(5.0, 15.0), tempu=u(0.0, 1.0), templ=u(0.5, 1.0),
+             agddu=u(0.0, 3e6), agddl=u(0.0, 3e6), dropu=u(0.5, 1.0), dropls=u(0.5, 1.0), dropl3=u(0.5, 1.0),
+             dropl4=u(0.5, 1.0), tco2root=np.zeros(n), tnmin=u(0.0, 4e-8), a10td=tclim + u(-3.0, 3.0),
+             a10ancub=u(1e-7, 9e-7), a10ancls=u(1e-8, 5e-7), a10ancl3=u(1e-8, 5e-7), a10ancl4=u(1e-7, 9e-7),
+             ayprcp=u(100.0, 1800.0), ayaet=u(100.0, 1200.0), ayco2mic=u(0.05, 1.2), ayco2root=np.zeros(n),
+             storedn=u(0.01, 0.1), yrleach=u(2.0, 36.0), ynleach=u(0.2, 3.0))
+    pools = dict(clitlm=(2e-5, 2e-3), clitls=(4e-3, 0.1), clitll=(1.6e-3, 0.04), clitrm=(3e-5, 7e-4),
+                 clitrs=(8e-3, 0.15), clitrl=(5e-3, 0.08), clitwm=(0.0, 0.0), clitws=(4e-3, 1.0),
+                 clitwl=(3e-3, 0.8), csoislop=(1.0, 22.0), csoislon=(0.09, 2.3), csoipas=(1.3, 16.0),
+                 totcmic=(0.04, 0.55), falll=(0.03, 0.35), fallr=(0.04, 0.24), fallw=(0.005, 0.5))
+    for k, (lo, hi) in pools.items():
+        d[k] = u(lo, hi)
+    d["decompl"], d["decomps"] = u(0.1, 2.5), u(0.2, 2.3)
+    d["totfall"] = d["falll"] + d["fallr"] + d["fallw"]
+    return d
+
+
+def make_daily_weather(rng, lat, nday):
+    """Seeded daily weather (``layout.DAILY``, (nday, ncell) arrays) for the
+    device forcing generator: temperatures about the latitude's climate, cloud,
+    gamma-distributed precipitation on 40 % of days, humidity, wind and the
+    daily longwave."""
+    n = lat.shape[0]
+    tclim = 300.0 - 0.35 * np.abs(lat)
+    tmin = tclim[None, :] - rng.uniform(2.0, 10.0, (nday, n))
+    tmax = tmin + rng.uniform(3.0, 14.0, (nday, n))
+    wet = rng.uniform(size=(nday, n)) < 0.4
+    return dict(td=0.5 * (tmin + tmax), tmax=tmax, tmin=tmin, cloud=rng.uniform(0.0, 1.0, (nday, n)),
+                precip=np.where(wet, rng.gamma(0.8, 6.0, (nday, n)), 0.0), psurf=np.full((nday, n), 101300.0),
+                qd=rng.uniform(0.002, 0.015, (nday, n)), ud=rng.uniform(1.0, 6.0, (nday, n)),
+                fira=rng.uniform(250.0, 400.0, (nday, n)))
+
+
 # ----------------------------------------------------------------------------
 # plane packing
 # ----------------------------------------------------------------------------
