@@ -117,9 +117,46 @@ __device__ __forceinline__ Forc<R> load_forc(const R* __restrict__ f, int ld) {
     return F;
 }
 
+// Accumulators of the fused kernel kept in shared memory for the launch: plane p
+// of thread t at sacc[p * BLOCK + t] (consecutive threads, consecutive banks),
+// value planes then compensation planes as in the global buffer.  Only the
+// planes the flags write move: loaded before the first hour, stored after the
+// last, so the hourly read-modify-writes stay on chip.
+__device__ __forceinline__ bool acc_plane_used(int p, unsigned flags) {
+    const int q = p < IBIS_ACC_COUNT ? p : p - IBIS_ACC_COUNT;
+    if (p >= IBIS_ACC_COUNT && (!(flags & IBIS_FLAG_KAHAN) || q >= IBIS_ACC_STRESSTU_LAST)) return false;
+    if (q == IBIS_ACC_CH4) return (flags & IBIS_FLAG_CH4) != 0;
+    if (q >= IBIS_ACC_TSOI_MEAN && q < IBIS_ACC_AFSENA) return (flags & IBIS_FLAG_SOIL_MEANS) != 0;
+    return (flags & IBIS_FLAG_ACC) != 0;
+}
+
+template <typename R, bool TO_SMEM>
+__device__ __forceinline__ void acc_move(R* __restrict__ g, int ld, R* __restrict__ sacc, int sld, unsigned flags) {
+#pragma unroll 1
+    for (int p = 0; p < 2 * IBIS_ACC_COUNT; ++p) {
+        if (!acc_plane_used(p, flags)) continue;
+        if (TO_SMEM) sacc[p * sld] = g[(size_t)p * ld];
+        else g[(size_t)p * ld] = sacc[p * sld];
+    }
+}
+
+// Whether a fused configuration keeps its accumulators in shared memory: the
+// column state plus all accumulator planes of MINB resident blocks must fit
+// the SM's 228 KB (1 KB reserved per block).  Launches of fewer than
+// kAccSmemMinSteps hours keep them in global memory instead (ACCSM = false):
+// the on-chip copy only pays back over several hours, and the larger
+// shared-memory carveout leaves less L1 for the register spills.
+template <typename R, int BLOCK, int MINB, bool ACCSM = true>
+struct AccInSmem {
+    static constexpr bool value =
+        ACCSM && StateInSmem<R>::value &&
+        ((sizeof(Col<R>) + 2 * IBIS_ACC_COUNT * sizeof(R)) * BLOCK + 1024) * MINB <= 228 * 1024;
+};
+constexpr int kAccSmemMinSteps = 4;
+
 // Status word written by the kernels: [0] bit 0 = a column left the step with a
 // non-finite prognostic value; [1] = smallest such cell index (INT_MAX if none).
-template <typename R, int NT, bool SU, bool SL, int BLOCK, int MINB>
+template <typename R, int NT, bool SU, bool SL, int BLOCK, int MINB, bool ACCSM>
 __global__ void __launch_bounds__(BLOCK, MINB) hourly_step_kernel(R* __restrict__ prog, const R* __restrict__ stat,
                                                              const R* __restrict__ forc, R* __restrict__ diag,
                                                              R* __restrict__ acc, int ncell, int ld, int nstep,
@@ -136,13 +173,19 @@ __global__ void __launch_bounds__(BLOCK, MINB) hourly_step_kernel(R* __restrict_
     load_col(c, prog + i, ld);
     Stat<R> S{stat + i, ld};
     Diag<R> D{diag ? diag + i : nullptr, ld};
-    Acc<R> A{acc ? acc + i : nullptr, ld, (P.flags & IBIS_FLAG_KAHAN) != 0};
+    constexpr bool kAccSmem = AccInSmem<R, BLOCK, MINB, ACCSM>::value;
+    // with the accumulators on chip the view always points at shared memory
+    // (acc == nullptr comes with no accumulator flags, so nothing is added)
+    R* const sacc = kAccSmem ? reinterpret_cast<R*>(smem_raw + BLOCK * sizeof(Col<R>)) + threadIdx.x : nullptr;
+    Acc<R> A{kAccSmem ? sacc : (acc ? acc + i : nullptr), kAccSmem ? BLOCK : ld, (P.flags & IBIS_FLAG_KAHAN) != 0};
+    if (kAccSmem && acc) acc_move<R, true>(acc + i, ld, sacc, BLOCK, P.flags);
 #pragma unroll 1
     for (int s = 0; s < nstep; ++s) {
         Forc<R> F = load_forc(forc + (size_t)s * forc_stride + i, ld);
         A.last = (s + 1 == nstep);
         column_step<R, NT, SU, SL>(c, F, S, D, A, P, UniformQ<R>{P});
     }
+    if (kAccSmem && acc) acc_move<R, false>(acc + i, ld, sacc, BLOCK, P.flags);
     R sum = store_col(c, prog + i, ld);
     if (status && !finite(sum)) {
         atomicOr(status, 1);
@@ -310,14 +353,16 @@ cudaError_t fit_smem_once(unsigned long long& done, K k, int block, size_t smem,
     return e;
 }
 
-template <typename R, int NT, bool SU, bool SL, int BLOCK, int MINB>
+template <typename R, int NT, bool SU, bool SL, int BLOCK, int MINB, bool ACCSM>
 cudaError_t launch_fused(R* prog, const R* stat, const R* forc, R* diag, R* acc, int ncell, int ld, int nstep,
                          long long fstride, const DevParams<R>& P, int* status, cudaStream_t s) {
     const int grid = (ncell + BLOCK - 1) / BLOCK;
-    const size_t smem = StateInSmem<R>::value ? BLOCK * sizeof(Col<R>) : 0;
-    auto k = hourly_step_kernel<R, NT, SU, SL, BLOCK, MINB>;
+    const size_t col_smem = StateInSmem<R>::value ? BLOCK * sizeof(Col<R>) : 0;
+    const size_t acc_smem = AccInSmem<R, BLOCK, MINB, ACCSM>::value ? BLOCK * 2 * IBIS_ACC_COUNT * sizeof(R) : 0;
+    const size_t smem = col_smem + acc_smem;
+    auto k = hourly_step_kernel<R, NT, SU, SL, BLOCK, MINB, ACCSM>;
     static unsigned long long fitted = 0;
-    cudaError_t e = fit_smem_once(fitted, k, BLOCK, smem, smem);
+    cudaError_t e = fit_smem_once(fitted, k, BLOCK, col_smem + acc_smem, col_smem + acc_smem);
     if (e != cudaSuccess) return e;
     k<<<grid, BLOCK, smem, s>>>(prog, stat, forc, diag, acc, ncell, ld, nstep, fstride, P, status);
     return cudaGetLastError();
@@ -347,12 +392,20 @@ template <typename R, int NT, bool SU, bool SL, int CFG>
 cudaError_t run_config(R* prog, const R* stat, const R* forc, R* diag, R* acc, R* mid, int ncell, int ld, int nstep,
                        long long fs, const DevParams<R>& P, int* status, cudaStream_t s) {
     constexpr LaunchConfig C = kConfigs[CFG];
-    if constexpr (C.form == 0)
-        return launch_fused<R, NT, SU, SL, C.block, C.minb>(prog, stat, forc, diag, acc, ncell, ld, nstep, fs, P,
-                                                            status, s);
-    else
+    if constexpr (C.form == 0) {
+        // the default fused configuration (the plain entry points' and the
+        // per-hour callers') also has a global-accumulator twin for short launches
+        if constexpr (CFG == kDefaultFused && AccInSmem<R, C.block, C.minb>::value) {
+            if (nstep < kAccSmemMinSteps)
+                return launch_fused<R, NT, SU, SL, C.block, C.minb, false>(prog, stat, forc, diag, acc, ncell, ld,
+                                                                           nstep, fs, P, status, s);
+        }
+        return launch_fused<R, NT, SU, SL, C.block, C.minb, true>(prog, stat, forc, diag, acc, ncell, ld, nstep, fs,
+                                                                  P, status, s);
+    } else {
         return launch_split<R, NT, SU, SL, C.block, C.minb, C.block2, C.minb2>(prog, stat, forc, diag, acc, mid,
                                                                               ncell, ld, nstep, fs, P, status, s);
+    }
 }
 
 #define IBIS_RUN_ARGS(R) \
