@@ -249,7 +249,8 @@ def run_ours(args):
     def e2e_day():
         # the public host-buffer entry: forcing copied in chunks of hours on a
         # second stream, overlapping the computation of the previous chunk
-        cols.run_from_host(h_forc, P, chunk=args.e2e_chunk, stream=stream)
+        cols.run_from_host(h_forc, P, chunk=args.e2e_chunk if args.e2e_chunk == "auto" else int(args.e2e_chunk),
+                           stream=stream)
         h_prog.copy_(cols.prog, non_blocking=True)
 
     e2e_day()
@@ -318,7 +319,9 @@ def run_ours(args):
             "per_step_launch": {"value": cell_steps / (ms_plain / 1e3), "ms_per_step": ms_plain,
                                 "launches_per_step": HOURS, "launch_config": "fused, block 128, 2 blocks/SM",
                                 "achieved_gbs": _algorithmic_bytes(1) * args.ncell * HOURS / (ms_plain / 1e3) / 1e9},
-            "e2e": {"value": cell_steps / (ms_e2e / 1e3), "unit": "cell-steps/s", "chunk_hours": args.e2e_chunk,
+            "e2e": {"value": cell_steps / (ms_e2e / 1e3), "unit": "cell-steps/s",
+                    "chunk_hours": Columns.chunk_schedule(HOURS, args.e2e_chunk if args.e2e_chunk == "auto"
+                                                          else int(args.e2e_chunk)),
                     "h2d_bytes_per_step": int(h_forc.numel() * 4), "d2h_bytes_per_step": int(h_prog.numel() * 4)},
             "e2e_daily_forcing": {"value": cell_steps / (ms_e2e_daily / 1e3), "unit": "cell-steps/s",
                                   "h2d_bytes_per_step": int(h_daily.numel() * 4),
@@ -636,7 +639,8 @@ def main():
     ap.add_argument("--rate", type=float, default=50.0)
     ap.add_argument("--duration", type=float, default=10.0)
     ap.add_argument("--epoch-hours", type=int, default=168)
-    ap.add_argument("--e2e-chunk", type=int, default=6, help="hours per host-to-device forcing chunk in the e2e path")
+    ap.add_argument("--e2e-chunk", default="auto",
+                    help="hours per host-to-device forcing chunk in the e2e path ('auto': 2 hours, growing by half)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)

@@ -177,18 +177,35 @@ class Columns:
         _lib.check(rc, "ibis_step")
         return self
 
-    def run_from_host(self, host_forc: torch.Tensor, params: StepParams, chunk: int = 6, stream=None):
+    @staticmethod
+    def chunk_schedule(nstep: int, chunk="auto"):
+        """Hours per host-to-device chunk.  An integer gives equal chunks;
+        ``"auto"`` starts with 2 hours and grows each chunk by half, so the
+        copy of the next chunk (~0.09 ms per hour of forcing at 95,333 cells
+        over PCIe) stays shorter than the computation of the current one
+        (~0.14 ms per hour) and only the first, small copy is exposed."""
+        if chunk == "auto":
+            out, c = [], 2.0
+            while sum(out) < nstep:
+                out.append(min(int(c), nstep - sum(out)))
+                c *= 1.5
+            return out
+        c = max(1, min(int(chunk), nstep))
+        return [min(c, nstep - h0) for h0 in range(0, nstep, c)]
+
+    def run_from_host(self, host_forc: torch.Tensor, params: StepParams, chunk="auto", stream=None):
         """Advance the columns through ``host_forc`` (a pinned host tensor
-        ``(nstep, IBIS_FORC_COUNT, ld)``), copying the forcing in chunks of
-        ``chunk`` hours on a second stream so the copy of chunk k+1 overlaps
-        the computation of chunk k.  Asynchronous on ``stream``: work queued on
-        it afterwards (a read-back of the state) runs after the last hour."""
+        ``(nstep, IBIS_FORC_COUNT, ld)``), copying the forcing in chunks
+        (:meth:`chunk_schedule`) on a second stream so the copy of chunk k+1
+        overlaps the computation of chunk k.  Asynchronous on ``stream``: work
+        queued on it afterwards (a read-back of the state) runs after the last hour."""
         if host_forc.device.type != "cpu" or host_forc.dtype != self.dtype or not host_forc.is_pinned():
             raise ValueError("host forcing must be a pinned CPU tensor of the Columns' dtype")
         if host_forc.dim() != 3 or host_forc.shape[1] != L.N_FORC or host_forc.shape[2] != self.ld:
             raise ValueError(f"host forcing must be (nstep, {L.N_FORC}, {self.ld})")
         nstep = host_forc.shape[0]
-        chunk = max(1, min(int(chunk), nstep))
+        sched = self.chunk_schedule(nstep, chunk)
+        chunk = max(sched)
         stream = stream or torch.cuda.current_stream(self.device)
         key = (chunk, host_forc.dtype)
         if getattr(self, "_staging", None) is None or self._staging[0] != key:
@@ -199,8 +216,8 @@ class Columns:
         start = torch.cuda.Event()
         start.record(stream)
         copy_stream.wait_event(start)
-        for k, h0 in enumerate(range(0, nstep, chunk)):
-            n = min(chunk, nstep - h0)
+        h0 = 0
+        for k, n in enumerate(sched):
             slot = k % 2
             with torch.cuda.stream(copy_stream):
                 if k >= 2:
@@ -210,4 +227,5 @@ class Columns:
             stream.wait_event(copied[slot])
             self.run(bufs[slot][:n], params, stream=stream)
             used[slot].record(stream)
+            h0 += n
         return self

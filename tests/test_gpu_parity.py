@@ -118,7 +118,7 @@ def test_split_form_matches_fused_form(cuda_lib, name):
         np.testing.assert_allclose(out["split"][0][k], out["fused"][0][k], rtol=1e-3, atol=1e-4, err_msg=k)
 
 
-@pytest.mark.parametrize("chunk", [1, 5, 24])
+@pytest.mark.parametrize("chunk", [1, 5, 24, "auto"])
 def test_run_from_host_matches_device_run(cuda_lib, chunk):
     """Forcing streamed from pinned host memory in chunks gives the same bits as
     the same hours from device memory (the same kernel per hour; state and
