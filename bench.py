@@ -441,6 +441,33 @@ def run_ensemble(args):
     cs = ens.cell_steps()
     m = float(np.mean(ms))
     plain = _plain_per_vector(spec, args, stream)
+    # the daily-weather form: the same sites, vectors and record lengths over
+    # day records, each run generating its hours in the kernel
+    t0 = time.time()
+    spec_d = E.make_ensemble(args.sites, args.params_per_site, seed=7, site_hours=spec.site_hours, daily=True)
+    gen_d = time.time() - t0
+    ens_d = E.Ensemble(spec_d)
+
+    def timed_d(k):
+        out = []
+        for _ in range(k):
+            ens_d.reset()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            ens_d.run(block=block)
+            b.record(stream)
+            b.synchronize()
+            out.append(a.elapsed_time(b))
+        return out
+
+    timed_d(1)
+    ms_d = float(np.mean(timed_d(args.steps)))
+    daily_form = {"value": ens_d.cell_steps() / (ms_d / 1e3), "ms_per_step": ms_d,
+                  "forcing_gb": ens_d.day_records.numel() * 4 / 1e9, "generation_s": gen_d,
+                  "nonfinite_runs": ens_d.nonfinite()[0],
+                  "note": "same sites, vectors and record lengths over 48-byte day records; each run generates its "
+                          "hours in the kernel (ibis_ensemble_daily_f32)"}
+    del ens_d
     line = {
         "metric": "cell-steps/s, calibration ensemble (persistent launch)", "value": cs / (m / 1e3),
         "unit": "cell-steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": m,
@@ -459,6 +486,7 @@ def run_ensemble(args):
         "hourly_eager": {"value": cs / (float(np.mean(ms_eager)) / 1e3), "ms_per_step": float(np.mean(ms_eager))},
         "persistent_vs_hourly_graph": float(np.mean(ms_graph)) / m,
         "plain_per_vector": plain,
+        "daily_form": daily_form,
         "gpu_launches": args.steps,
         "clocks": clk.summary(), "nonfinite_runs": nonfinite[0], "bad_descriptors": nonfinite[1],
     }

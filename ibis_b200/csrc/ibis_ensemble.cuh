@@ -11,6 +11,7 @@
 // are shared by all runs at that site, and warps draw 32-run work items from a
 // device counter in the caller's order (longest records first).
 #pragma once
+#include "ibis_diurnal.cuh"
 #include "ibis_kernels.cuh"
 
 namespace ibis {
@@ -33,13 +34,28 @@ struct EnsArgs {
     int nwork;   // entries of order to run (nrun when order is NULL)
     int* queue;
     int* status;
+    // daily-weather form (IbisEnsembleDaily): run_forc indexes day records
+    const float* daily;     // [daily_len][kEnsDailyWords]; nullptr: hourly records in forc
+    const float* site_lat;  // [nsite] degrees
+    long long daily_len;
+    uint32_t seed;
+    bool obs_fira;
+    int nh;                 // steps per day
+    float dtime;
 };
+
+// A day record of the daily-weather form: the IBIS_DAILY_* words, the day of
+// year, two words of padding (48 bytes, three 16-byte loads).
+constexpr int kEnsDailyWords = 12;
+constexpr int kEnsDailyJday = IBIS_DAILY_COUNT;
 
 // A run whose descriptor points outside the buffers is flagged (status bit 1)
 // and skipped, so no access leaves the caller's arrays.
 __device__ __forceinline__ bool run_ok(const EnsArgs& e, int r, int site, int nstep, long long first, int pos) {
+    const long long len = e.daily ? e.daily_len : e.forc_len;
+    const long long need = e.daily ? ((long long)nstep + e.nh - 1) / e.nh : (long long)nstep;
     const bool ok = r >= 0 && r < e.nrun && site >= 0 && site < e.nsite && nstep >= 0 && first >= 0 &&
-                    first + nstep <= e.forc_len && pos >= 0;
+                    first + need <= len && pos >= 0;
     if (!ok && e.status) atomicOr(e.status, 2);
     return ok;
 }
@@ -68,6 +84,30 @@ __device__ __forceinline__ Forc<float> load_forc_record(const float* __restrict_
     F.si[0] = v[IBIS_FORC_SOLAI]; F.si[1] = v[IBIS_FORC_SOLAI + 1];
     F.fira = v[IBIS_FORC_FIRA]; F.rain = v[IBIS_FORC_RAINA]; F.snow = v[IBIS_FORC_SNOWA];
     return F;
+}
+
+// What a run of the daily-weather form keeps of its current day (in shared
+// memory): the day's weather, orbital terms and precipitation event, and the
+// site's latitude terms.
+struct DayCache {
+    DailyRec rec;
+    DayGeom g;
+    Event ev;
+    float sinlat, coslat;
+};
+
+// Day record `rec` of `site`: its weather and orbital terms, and the event the
+// counter-based variates (seed, record, site) place (ibis_diurnal.cuh).
+__device__ __forceinline__ void load_day(DayCache& dc, const EnsArgs& e, int site, long long rec) {
+    const float4* p = reinterpret_cast<const float4*>(e.daily + (size_t)rec * kEnsDailyWords);
+    const float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2);
+    const float v[kEnsDailyWords] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w};
+    dc.rec.tmax = v[IBIS_DAILY_TMAX]; dc.rec.tmin = v[IBIS_DAILY_TMIN]; dc.rec.cloud = v[IBIS_DAILY_CLOUD];
+    dc.rec.precip = v[IBIS_DAILY_PRECIP]; dc.rec.psurf = v[IBIS_DAILY_PSURF]; dc.rec.qd = v[IBIS_DAILY_QD];
+    dc.rec.ud = v[IBIS_DAILY_UD]; dc.rec.fira = v[IBIS_DAILY_FIRA];
+    dc.g = day_geometry((int)v[kEnsDailyJday]);
+    const uint32_t day = (uint32_t)rec;
+    dc.ev = precip_timing(draw24(e.seed, site, day, 0), draw24(e.seed, site, day, 1), dc.rec.precip, e.dtime);
 }
 
 // Fill one run's parameter source from its vector (planes [IBIS_RUN_PARAMS][ld]).
@@ -122,11 +162,19 @@ __device__ __forceinline__ void flag_nonfinite(const EnsArgs& e, float sum, int 
 // items run out, and runs each of its runs from its first hour to its last.
 // blockDim.x is a multiple of 32 (checked by the host), so every warp is whole
 // for the __shfl_sync that shares the item number.
-template <int NT, bool SU, bool SL>
+// With DAILY, each run's hours are generated from its site's day records as it
+// steps (the day's terms once a day, then one diurnal hour per step), so the
+// forcing read from memory is one 48-byte record per site-day instead of one
+// per site-hour; a run's hours start at midnight of record run_forc.
+template <int NT, bool SU, bool SL, bool DAILY>
 __global__ void __launch_bounds__(256, 1) ensemble_kernel(const EnsArgs e, const DevParams<float> P) {
     extern __shared__ unsigned char smem_raw[];
     Col<float>& c = reinterpret_cast<Col<float>*>(smem_raw)[threadIdx.x];
     RunQ<float>& q = reinterpret_cast<RunQ<float>*>(smem_raw + blockDim.x * sizeof(Col<float>))[threadIdx.x];
+    DayCache* const dc =
+        DAILY ? reinterpret_cast<DayCache*>(smem_raw + blockDim.x * (sizeof(Col<float>) + sizeof(RunQ<float>))) +
+                    threadIdx.x
+              : nullptr;
     const int lane = threadIdx.x & 31;
     const int nitem = (e.nwork + 31) >> 5;
     const bool kahan = (P.flags & IBIS_FLAG_KAHAN) != 0;
@@ -144,7 +192,12 @@ __global__ void __launch_bounds__(256, 1) ensemble_kernel(const EnsArgs e, const
         const long long first = in ? __ldg(e.run_forc + r) : -1;
         const int pos = in && e.run_pos ? __ldg(e.run_pos + r) : 0;
         if (idx < e.nwork && run_ok(e, r, site, nstep, first, pos)) {
-            const float* f = e.forc + (size_t)first * IBIS_FORC_COUNT;
+            const float* f = DAILY ? nullptr : e.forc + (size_t)first * IBIS_FORC_COUNT;
+            if constexpr (DAILY) {
+                const double xlat = (double)__ldg(e.site_lat + site) * (3.14159265358979323846 / 180.0);
+                dc->sinlat = (float)sin(xlat);
+                dc->coslat = (float)cos(xlat);
+            }
             load_col(c, e.prog + r, e.ld_run);
             load_run_params(q, e.run_params + r, e.ld_run, P);
             const Stat<float> S{e.stat + site, e.ld_site};
@@ -154,7 +207,15 @@ __global__ void __launch_bounds__(256, 1) ensemble_kernel(const EnsArgs e, const
             int year = pos / e.year_steps;
 #pragma unroll 1
             for (int s = 0; s < nstep; ++s) {
-                const Forc<float> F = load_forc_record(f + (size_t)s * IBIS_FORC_COUNT);
+                Forc<float> F;
+                if constexpr (DAILY) {
+                    const int d = s / e.nh, h = s - d * e.nh;
+                    if (h == 0) load_day(*dc, e, site, first + d);
+                    F = diurnal_hour(dc->rec, dc->g, dc->sinlat, dc->coslat, (float)h * e.dtime, dc->ev,
+                                     draw24(e.seed, site, (uint32_t)(first + d), 2 + h), e.dtime, e.obs_fira);
+                } else {
+                    F = load_forc_record(f + (size_t)s * IBIS_FORC_COUNT);
+                }
                 A.last = (s + 1 == nstep);
                 column_step<float, NT, SU, SL>(c, F, S, D, A, P, q);
                 if (s + 1 == next_year) {
@@ -205,13 +266,15 @@ static __global__ void advance_hour(int* hour0, int n) { *hour0 += n; }
 
 constexpr int kEnsHourBlock = 128;
 
-inline size_t ens_smem(int block) { return (size_t)block * (sizeof(Col<float>) + sizeof(RunQ<float>)); }
+inline size_t ens_smem(int block, bool daily = false) {
+    return (size_t)block * (sizeof(Col<float>) + sizeof(RunQ<float>) + (daily ? sizeof(DayCache) : 0));
+}
 
-template <int NT, bool SU, bool SL>
+template <int NT, bool SU, bool SL, bool DAILY = false>
 cudaError_t launch_ensemble(const EnsArgs& e, const DevParams<float>& P, int block, int grid, cudaStream_t s) {
-    auto k = ensemble_kernel<NT, SU, SL>;
-    const size_t smem = ens_smem(block);
-    cudaError_t err = fit_smem(k, block, smem, ens_smem(256));
+    auto k = ensemble_kernel<NT, SU, SL, DAILY>;
+    const size_t smem = ens_smem(block, DAILY);
+    cudaError_t err = fit_smem(k, block, smem, ens_smem(256, DAILY));
     if (err != cudaSuccess) return err;
     k<<<grid, block, smem, s>>>(e, P);
     return cudaGetLastError();
@@ -232,12 +295,12 @@ cudaError_t launch_ensemble_hours(const EnsArgs& e, const DevParams<float>& P, i
 }
 
 // Resident blocks of `block` threads per SM for the persistent kernel.
-template <int NT, bool SU, bool SL>
+template <int NT, bool SU, bool SL, bool DAILY = false>
 int ensemble_occupancy(int block) {
     int n = 0;
-    auto k = ensemble_kernel<NT, SU, SL>;
-    if (fit_smem(k, block, ens_smem(block), ens_smem(256)) != cudaSuccess) return 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, block, ens_smem(block)) != cudaSuccess) return 0;
+    auto k = ensemble_kernel<NT, SU, SL, DAILY>;
+    if (fit_smem(k, block, ens_smem(block, DAILY), ens_smem(256, DAILY)) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, block, ens_smem(block, DAILY)) != cudaSuccess) return 0;
     return n;
 }
 

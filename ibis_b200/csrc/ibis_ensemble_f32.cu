@@ -16,6 +16,13 @@ namespace ibis {
 IBIS_ENS_VARIANTS(IBIS_ENS_EXTERN, 9)
 IBIS_ENS_VARIANTS(IBIS_ENS_EXTERN, 6)
 #undef IBIS_ENS_EXTERN
+#define IBIS_ENS_DAILY_EXTERN(NT, SU, SL)                                                                    \
+    extern template cudaError_t launch_ensemble<NT, SU, SL, true>(const EnsArgs&, const DevParams<float>&, int, \
+                                                                  int, cudaStream_t);                          \
+    extern template int ensemble_occupancy<NT, SU, SL, true>(int);
+IBIS_ENS_VARIANTS(IBIS_ENS_DAILY_EXTERN, 9)
+IBIS_ENS_VARIANTS(IBIS_ENS_DAILY_EXTERN, 6)
+#undef IBIS_ENS_DAILY_EXTERN
 
 namespace {
 
@@ -92,10 +99,12 @@ extern "C" int ibis_ensemble_occupancy(const IbisParams* params, int block) {
 #undef IBIS_OCC
 }
 
-extern "C" int ibis_ensemble_f32(const IbisEnsemble* ens, const IbisParams* params, int block, void* stream) {
-    EnsArgs a{};
-    int rc = ens_args(ens, params, a);
-    if (rc || ens->nrun == 0) return rc;
+namespace {
+
+// The persistent launch of ibis_ensemble_f32 / ibis_ensemble_daily_f32 on a
+// validated description.
+template <bool DAILY>
+int ensemble_launch(const IbisEnsemble* ens, EnsArgs& a, const IbisParams* params, int block, void* stream) {
     if (!ens->queue) return -EINVAL;
     if (block != 0 && (block < 32 || block > 256 || block % 32)) return -EINVAL;
     int dev = 0, sms = 0;
@@ -108,7 +117,9 @@ extern "C" int ibis_ensemble_f32(const IbisEnsemble* ens, const IbisParams* para
         const int w = (nitem + sms - 1) / sms;          // warps per SM that cover every item in one pass
         block = 32 * (w < 1 ? 1 : (w > 8 ? 8 : w));
     }
-    const int occ = ibis_ensemble_occupancy(params, block);
+#define IBIS_OCC(NT, SU, SL) ensemble_occupancy<NT, SU, SL, DAILY>(block)
+    const int occ = IBIS_BY_VARIANT(params->flags, IBIS_OCC);
+#undef IBIS_OCC
     if (occ <= 0) return -EINVAL;
     const int per_block = block / 32;
     int grid = sms * occ;
@@ -116,12 +127,48 @@ extern "C" int ibis_ensemble_f32(const IbisEnsemble* ens, const IbisParams* para
     if (need < grid) grid = need;
     const DevParams<float> P = make_dev_params<float>(*params);
     cudaStream_t s = (cudaStream_t)stream;
-    rc = launch_error(cudaMemsetAsync(ens->queue, 0, sizeof(int), s), "ensemble queue reset");
+    const int rc = launch_error(cudaMemsetAsync(ens->queue, 0, sizeof(int), s), "ensemble queue reset");
     if (rc) return rc;
-#define IBIS_RUN(NT, SU, SL) launch_ensemble<NT, SU, SL>(a, P, block, grid, s)
+#define IBIS_RUN(NT, SU, SL) launch_ensemble<NT, SU, SL, DAILY>(a, P, block, grid, s)
     const cudaError_t err = IBIS_BY_VARIANT(params->flags, IBIS_RUN);
 #undef IBIS_RUN
     return launch_error(err, "ensemble launch");
+}
+
+}  // namespace
+
+extern "C" int ibis_ensemble_f32(const IbisEnsemble* ens, const IbisParams* params, int block, void* stream) {
+    EnsArgs a{};
+    int rc = ens_args(ens, params, a);
+    if (rc || ens->nrun == 0) return rc;
+    return ensemble_launch<false>(ens, a, params, block, stream);
+}
+
+extern "C" int ibis_ensemble_daily_f32(const IbisEnsemble* ens, const IbisEnsembleDaily* daily,
+                                       const IbisParams* params, int block, void* stream) {
+    if (!ens || !daily || !params) return -EINVAL;
+    if (!daily->records || !daily->site_lat || daily->len < 0 || ((uintptr_t)daily->records % 16) ||
+        (daily->flags & ~IBIS_DIURNAL_OBSERVED_FIRA))
+        return -EINVAL;
+    if (!(params->dtime > 0.0)) return -EINVAL;
+    const int nh = (int)(86400.0 / params->dtime);
+    if (nh < 1 || nh > 254 || (double)nh * params->dtime != 86400.0) return -EINVAL;
+    IbisEnsemble hourly = *ens;          // the hourly-record checks do not apply: no hourly records
+    alignas(16) static const float kNoRecords[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    hourly.forc = kNoRecords;
+    hourly.forc_len = 0;
+    EnsArgs a{};
+    int rc = ens_args(&hourly, params, a);
+    if (rc || ens->nrun == 0) return rc;
+    a.forc = nullptr;
+    a.daily = daily->records;
+    a.site_lat = daily->site_lat;
+    a.daily_len = daily->len;
+    a.seed = daily->seed;
+    a.obs_fira = (daily->flags & IBIS_DIURNAL_OBSERVED_FIRA) != 0;
+    a.nh = nh;
+    a.dtime = (float)params->dtime;
+    return ensemble_launch<true>(ens, a, params, block, stream);
 }
 
 extern "C" int ibis_ensemble_hours_f32(const IbisEnsemble* ens, const IbisParams* params, int* hour, int nhour,

@@ -15,7 +15,11 @@ candidate at every site in one launch instead:
   take 32 runs at a time from a device counter, longest records first;
 * :meth:`Ensemble.run_hourly` is the plain form: one launch per hour
   (``ibis_ensemble_hours_f32``), optionally captured in a CUDA graph of
-  ``chunk`` hours and replayed until the longest record ends.
+  ``chunk`` hours and replayed until the longest record ends;
+* with day records (``make_ensemble(..., daily=True)``) the persistent form
+  generates each run's hours from its site's daily weather as it steps
+  (``ibis_ensemble_daily_f32``: the reference's diurnal algorithm), so the
+  forcing held and read is 48 bytes per site-day instead of per site-hour.
 
 Runs are numbered site-major (run = site * nparam + p), so with 32 or 64
 parameter vectors every warp's runs share one site and one record length.
@@ -31,7 +35,7 @@ import torch
 from . import layout as L
 from . import lib as _lib
 from . import synth
-from .lib import IbisEnsembleC
+from .lib import IbisEnsembleC, IbisEnsembleDailyC
 from .params import FLAG_ACC, FLAG_CH4, StepParams
 
 YEAR_HOURS = 8760
@@ -91,12 +95,14 @@ class EnsembleSpec:
     site_hours: np.ndarray            # (nsite,) record length of each site (hours)
     stat: dict                        # per-site static fields (nsite, ...)
     prog: dict                        # per-site initial state (nsite, ...)
-    forc: np.ndarray                  # (total_hours, N_FORC) float32 records, site after site
+    forc: np.ndarray | None           # (total_hours, N_FORC) float32 records, site after site (None: day records)
     site_first: np.ndarray            # (nsite,) first record of each site in ``forc``
     vectors: np.ndarray               # (nparam, N_RUN) float32
     params: StepParams
     latitude: np.ndarray
     meta: dict = field(default_factory=dict)
+    daily: np.ndarray | None = None   # (total_days, DAILY_WORDS) day records; then site_first counts days
+    weather_seed: int = 0             # key of the daily form's counter-based variates
 
     @property
     def nrun(self) -> int:
@@ -114,13 +120,31 @@ def forcing_records(forc: dict) -> np.ndarray:
     return out
 
 
+DAILY_WORDS = 12      # IBIS_DAILY_* words, day of year, two padding words (48 bytes)
+
+
+def daily_records(daily: dict, jday0: int = 1) -> np.ndarray:
+    """(nday, DAILY_WORDS) float32 day records of one site from a dict of (nday,)
+    arrays named as ``layout.DAILY``; day d is day of year ((jday0 - 1 + d) mod 365) + 1."""
+    nday = np.shape(daily["tmax"])[0]
+    out = np.zeros((nday, DAILY_WORDS), dtype=np.float32)
+    for f in L.DAILY:
+        if f.name in daily:
+            out[:, L.OFF["DAILY"][f.name][0]] = np.asarray(daily[f.name]).reshape(nday)
+    out[:, L.N_DAILY] = (jday0 - 1 + np.arange(nday)) % 365 + 1
+    return out
+
+
 def make_ensemble(nsite: int, nparam: int, years=(1, 15), seed: int = 0, lat_range=(-40.0, 70.0),
                   year_hours: int = YEAR_HOURS, site_hours=None, alpha: float = 1.0,
-                  params: StepParams | None = None, include_default: bool = True) -> EnsembleSpec:
+                  params: StepParams | None = None, include_default: bool = True,
+                  daily: bool = False) -> EnsembleSpec:
     """Seeded synthetic ensemble: ``nsite`` towers with records of U{years} whole
     years (or the explicit ``site_hours``) of hourly forcing, ``nparam``
     calibration vectors drawn log-uniform within +-50% of the defaults (vector 0
-    is the default itself when ``include_default``)."""
+    is the default itself when ``include_default``).  With ``daily`` the
+    records are days of weather (``synth.make_daily_weather``) for the
+    daily form, and ``site_hours`` must be whole days."""
     rng = np.random.Generator(np.random.PCG64(seed))
     params = StepParams(co2conc=390.0e-6) if params is None else params
     lat = rng.uniform(lat_range[0], lat_range[1], size=nsite)
@@ -130,21 +154,33 @@ def make_ensemble(nsite: int, nparam: int, years=(1, 15), seed: int = 0, lat_ran
     stat = synth.make_columns(rng, nsite, alpha)
     recs, first, f0 = [], np.zeros(nsite, dtype=np.int64), []
     pos = 0
+    if daily and np.any(site_hours % 24):
+        raise ValueError("daily records need whole days")
     for s in range(nsite):
-        fs = synth.make_forcing(rng, lat[s:s + 1], int(site_hours[s]), start_doy=1)
-        recs.append(forcing_records(fs))
+        if daily:
+            nday = int(site_hours[s]) // 24
+            dw = synth.make_daily_weather(rng, lat[s:s + 1], nday)
+            recs.append(daily_records({k: v[:, 0] for k, v in dw.items()}, jday0=1))
+            fs = synth.make_forcing(rng, lat[s:s + 1], 1, start_doy=1)
+            pos_next = pos + nday
+        else:
+            fs = synth.make_forcing(rng, lat[s:s + 1], int(site_hours[s]), start_doy=1)
+            recs.append(forcing_records(fs))
+            pos_next = pos + int(site_hours[s])
         f0.append({k: v[0] for k, v in fs.items()})
         first[s] = pos
-        pos += int(site_hours[s])
+        pos = pos_next
     F0 = {k: np.concatenate([d[k] for d in f0], axis=0) for k in f0[0]}
     prog = synth.make_initial(rng, stat, F0)
     vec = draw_vectors(rng, nparam, params)
     if include_default and nparam > 0:
         vec[0] = default_vector(params)
-    forc = np.concatenate(recs, axis=0) if recs else np.zeros((0, L.N_FORC), np.float32)
-    return EnsembleSpec(nsite=nsite, nparam=nparam, site_hours=site_hours, stat=stat, prog=prog, forc=forc,
-                        site_first=first, vectors=vec, params=params, latitude=lat,
-                        meta=dict(seed=seed, years=years, year_hours=year_hours))
+    width = DAILY_WORDS if daily else L.N_FORC
+    table = np.concatenate(recs, axis=0) if recs else np.zeros((0, width), np.float32)
+    return EnsembleSpec(nsite=nsite, nparam=nparam, site_hours=site_hours, stat=stat, prog=prog,
+                        forc=None if daily else table, site_first=first, vectors=vec, params=params, latitude=lat,
+                        meta=dict(seed=seed, years=years, year_hours=year_hours),
+                        daily=table if daily else None, weather_seed=seed)
 
 
 class Ensemble:
@@ -174,7 +210,16 @@ class Ensemble:
         self.prog0 = torch.from_numpy(prog0).to(dev)
         self.prog = self.prog0.clone()
         self.stat = torch.from_numpy(synth.to_planes("STAT", spec.stat, self.ld_site)).to(dev)
-        self.forc = torch.from_numpy(np.ascontiguousarray(spec.forc, dtype=np.float32)).to(dev)
+        self.daily = spec.daily is not None
+        if self.daily:
+            self.forc = None
+            self.day_records = torch.from_numpy(np.ascontiguousarray(spec.daily, dtype=np.float32)).to(dev)
+            self.site_lat = torch.from_numpy(np.asarray(spec.latitude, dtype=np.float32)).to(dev)
+            self._dc = IbisEnsembleDailyC(records=self.day_records.data_ptr(), site_lat=self.site_lat.data_ptr(),
+                                          len=int(self.day_records.shape[0]), seed=int(spec.weather_seed) & 0xFFFFFFFF,
+                                          flags=1)
+        else:
+            self.forc = torch.from_numpy(np.ascontiguousarray(spec.forc, dtype=np.float32)).to(dev)
         self.run_params = torch.from_numpy(rp).to(dev)
         self.run_site = torch.from_numpy(site_of_run.astype(np.int32)).to(dev)
         self.run_forc = torch.from_numpy(spec.site_first[site_of_run].astype(np.int64)).to(dev)
@@ -200,7 +245,8 @@ class Ensemble:
         return IbisEnsembleC(prog=p(self.prog), acc=p(self.acc), stat=p(self.stat), forc=p(self.forc),
                              run_params=p(self.run_params), run_site=p(self.run_site), run_forc=p(self.run_forc),
                              run_nstep=p(self.run_nstep), run_pos=None, order=p(self.order),
-                             yearly=p(self.yearly), forc_len=int(self.forc.shape[0]), nrun=self.nrun,
+                             yearly=p(self.yearly), forc_len=0 if self.forc is None else int(self.forc.shape[0]),
+                             nrun=self.nrun,
                              ld_run=self.ld_run, nsite=self.nsite, ld_site=self.ld_site, nyear=self.nyear,
                              year_steps=self.year_steps, norder=self.nrun, queue=p(self.queue), status=p(self.status))
 
@@ -219,11 +265,19 @@ class Ensemble:
 
     def run(self, block: int = 0, stream=None):
         """Every run, whole record, in one persistent launch (``block`` 0 = automatic)."""
+        if self.daily:
+            _lib.check(self.lib.ibis_ensemble_daily_f32(ctypes.byref(self._c), ctypes.byref(self._dc),
+                                                        ctypes.byref(self._pc), int(block),
+                                                        ctypes.c_void_p(self._stream(stream))),
+                       "ibis_ensemble_daily_f32")
+            return
         _lib.check(self.lib.ibis_ensemble_f32(ctypes.byref(self._c), ctypes.byref(self._pc), int(block),
                                               ctypes.c_void_p(self._stream(stream))), "ibis_ensemble_f32")
 
     def run_hours(self, nhour: int, stream=None):
         """``nhour`` one-hour launches from the device hour counter (which they advance)."""
+        if self.daily:
+            raise ValueError("the one-launch-per-hour form reads hourly records; this ensemble has day records")
         _lib.check(self.lib.ibis_ensemble_hours_f32(ctypes.byref(self._c), ctypes.byref(self._pc),
                                                     ctypes.c_void_p(self.hour.data_ptr()), int(nhour),
                                                     ctypes.c_void_p(self._stream(stream))),

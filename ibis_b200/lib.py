@@ -30,6 +30,12 @@ class IbisEnsembleC(ctypes.Structure):
                 ("status", ctypes.c_void_p)]
 
 
+class IbisEnsembleDailyC(ctypes.Structure):
+    """ctypes mirror of ``IbisEnsembleDaily`` (include/ibis_b200.h)."""
+    _fields_ = [("records", ctypes.c_void_p), ("site_lat", ctypes.c_void_p), ("len", ctypes.c_longlong),
+                ("seed", ctypes.c_uint), ("flags", ctypes.c_uint)]
+
+
 _c_int_p = ctypes.POINTER(ctypes.c_int)
 _P = ctypes.POINTER(IbisParamsC)
 _E = ctypes.POINTER(IbisEnsembleC)
@@ -52,6 +58,8 @@ SIGNATURES = {
     "ibis_ensemble_f32": (ctypes.c_int, [_E, _P, ctypes.c_int, ctypes.c_void_p]),
     "ibis_ensemble_hours_f32": (ctypes.c_int, [_E, _P, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
     "ibis_ensemble_occupancy": (ctypes.c_int, [_P, ctypes.c_int]),
+    "ibis_ensemble_daily_f32": (ctypes.c_int, [_E, ctypes.POINTER(IbisEnsembleDailyC), _P, ctypes.c_int,
+                                               ctypes.c_void_p]),
     "ibis_diurnal_f32": (ctypes.c_int, [ctypes.c_void_p] * 3 + [ctypes.c_int] * 5
                          + [ctypes.c_float, ctypes.c_uint, ctypes.c_uint, ctypes.c_void_p]),
     "ibis_diurnal_sw_f32": (ctypes.c_int, [_V] * 5 + [ctypes.c_int] * 5

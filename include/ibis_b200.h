@@ -139,6 +139,33 @@ int ibis_ensemble_f32(const IbisEnsemble* ens, const IbisParams* params, int blo
 int ibis_ensemble_hours_f32(const IbisEnsemble* ens, const IbisParams* params, int* hour, int nhour,
                             void* stream);
 
+/* The daily-weather form of an ensemble: instead of hourly records, every
+ * site has day records and each run generates its hours as it steps, from the
+ * reference's diurnal algorithm (as ibis_diurnal_f32 does for columns), so a
+ * site-day costs 48 bytes of forcing instead of 24 x 48.
+ *   records   [len][12]: the IBIS_DAILY_* words of the day, its day of year
+ *             (1..366, as a float) at word IBIS_DAILY_COUNT, two padding words;
+ *             16-byte aligned
+ *   site_lat  [nsite] latitude (degrees)
+ *   seed      key of the counter-based variates, drawn per (seed, record, site)
+ *   flags     IBIS_DIURNAL_OBSERVED_FIRA: longwave from the fira word
+ * With this form ens->run_forc[r] is the run's first day record, ens->forc and
+ * ens->forc_len are not used, and a run's hours start at midnight of that day. */
+typedef struct IbisEnsembleDaily {
+    const float* records;
+    const float* site_lat;
+    long long len;
+    unsigned int seed;
+    unsigned int flags;
+} IbisEnsembleDaily;
+
+/* ibis_ensemble_f32 over day records (IbisEnsembleDaily) instead of hourly ones.
+ * Replaces: the calibration harness's per-site runs of the day loop, which
+ * disaggregate each day with compute_precip_timing + diurnal
+ * (python-port/ibis/physics/weather.py:395-601; loops_gswp3.py:115-124). */
+int ibis_ensemble_daily_f32(const IbisEnsemble* ens, const IbisEnsembleDaily* daily, const IbisParams* params,
+                            int block, void* stream);
+
 /* Resident blocks per SM of the persistent ensemble kernel at `block` threads,
  * for the variant params->flags selects (0 when it cannot run). */
 int ibis_ensemble_occupancy(const IbisParams* params, int block);

@@ -52,3 +52,13 @@ def test_day_params_layout_matches_ctypes(tmp_path):
     got = _c_layout(tmp_path, body)
     assert got[0] == ctypes.sizeof(IbisDayParamsC)
     assert got[1:] == [getattr(IbisDayParamsC, n).offset for n in names]
+
+
+def test_ensemble_daily_layout_matches_ctypes(tmp_path):
+    E = lib.IbisEnsembleDailyC
+    names = [f[0] for f in E._fields_]
+    body = 'printf("%zu ", sizeof(IbisEnsembleDaily));'
+    body += "".join(f'printf("%zu ", offsetof(IbisEnsembleDaily, {n}));' for n in names)
+    got = _c_layout(tmp_path, body)
+    assert got[0] == ctypes.sizeof(E)
+    assert got[1:] == [getattr(E, n).offset for n in names]

@@ -87,11 +87,11 @@ def _close_state(x, y, frac_min=0.97):
     assert np.all(frac >= frac_min), (int(np.argmin(frac)), float(frac.min()))
 
 
-def _close_acc(x, y):
-    """Accumulators within 1e-3 of the plane's largest magnitude in 97% of runs."""
+def _close_acc(x, y, frac_min=0.97):
+    """Accumulators within 1e-3 of the plane's largest magnitude in ``frac_min`` of the runs."""
     scale = np.maximum(np.abs(y).max(axis=1, keepdims=True), 1e-30)
     frac = (np.abs(x - y) <= 1e-3 * scale).mean(axis=1)
-    assert np.all(frac >= 0.97), (int(np.argmin(frac)), float(frac.min()))
+    assert np.all(frac >= frac_min), (int(np.argmin(frac)), float(frac.min()))
 
 
 def _run(ens, how, **kw):
@@ -174,3 +174,54 @@ def test_out_of_range_run_is_flagged_and_skipped(cuda_lib):
     assert bad_desc and not bad_nonfinite
     np.testing.assert_array_equal(ens.prog.cpu().numpy()[:, 5], before)
     assert not np.array_equal(ens.prog.cpu().numpy()[:, 6], before)
+
+
+def test_make_ensemble_day_records():
+    s = E.make_ensemble(3, 4, site_hours=np.array([48, 24, 72]), seed=4, daily=True)
+    assert s.forc is None and s.daily.shape == (6, E.DAILY_WORDS) and s.daily.dtype == np.float32
+    assert list(s.site_first) == [0, 2, 3]
+    assert list(s.daily[:, L.N_DAILY]) == [1, 2, 1, 1, 2, 3]          # day of year of each record
+    assert np.isfinite(s.daily).all() and np.all(s.daily[:, L.N_DAILY + 1:] == 0)
+    with pytest.raises(ValueError):
+        E.make_ensemble(2, 2, site_hours=np.array([30, 24]), daily=True)
+
+
+@pytest.mark.gpu
+def test_daily_form_matches_generated_hourly_records(cuda_lib):
+    """The persistent launch over day records (hours generated in the kernel)
+    against the same runs over hourly records that the column forcing generator
+    (ibis_diurnal_f32, same variates: seed, record, site) made from the same
+    days: the same forcing, so the states agree to the tolerances of the
+    hourly-vs-persistent comparison (the generator's and the step's arithmetic
+    are compiled in two places, so their last bits may differ; surface runoff,
+    a threshold quantity, then differs in a few of the 48 runs, so the
+    accumulators are held to 1e-3 in 85 % of them)."""
+    from ibis_b200 import forcing
+    nsite, nparam = 12, 4
+    hours = np.array([48, 72, 24, 96, 48, 72, 48, 24, 72, 96, 48, 72])
+    spec_d = E.make_ensemble(nsite, nparam, site_hours=hours, seed=9, daily=True)
+    ld = L.leading_dim(nsite)
+    lat = torch.zeros(ld, dtype=torch.float32, device="cuda")
+    lat[:nsite] = torch.from_numpy(spec_d.latitude.astype(np.float32)).cuda()
+    recs, first_h, pos = [], np.zeros(nsite, np.int64), 0
+    for s in range(nsite):
+        nday = int(hours[s]) // 24
+        d0 = int(spec_d.site_first[s])
+        days = spec_d.daily[d0:d0 + nday]
+        planes = np.zeros((nday, L.N_DAILY, ld), np.float32)
+        planes[:, :, s] = days[:, :L.N_DAILY]
+        f = forcing.hourly_forcing(torch.from_numpy(planes).cuda(), lat, nsite, jday0=int(days[0, L.N_DAILY]),
+                                   day0=d0, seed=spec_d.weather_seed, observed_fira=True)
+        recs.append(np.ascontiguousarray(f.cpu().numpy()[:, :, s]))
+        first_h[s] = pos
+        pos += int(hours[s])
+    spec_h = E.EnsembleSpec(nsite=nsite, nparam=nparam, site_hours=hours, stat=spec_d.stat, prog=spec_d.prog,
+                            forc=np.concatenate(recs, axis=0), site_first=first_h, vectors=spec_d.vectors,
+                            params=spec_d.params, latitude=spec_d.latitude)
+    a = _run(E.Ensemble(spec_d, year_steps=24), "persistent")
+    ens_h = E.Ensemble(spec_h, year_steps=24)
+    b = _run(ens_h, "persistent")
+    n = ens_h.nrun
+    assert np.isfinite(a[0][:, :n]).all() and a[3][0] == 0
+    _close_state(a[0][:, :n], b[0][:, :n], frac_min=0.9)
+    _close_acc(a[1][:L.N_ACC, :n] - a[1][L.N_ACC:, :n], b[1][:L.N_ACC, :n] - b[1][L.N_ACC:, :n], frac_min=0.85)
