@@ -115,7 +115,8 @@ def cpu_baseline_sample(ncell=16384, hours=HOURS, seed=123):
             prog, _, acc = oracle.step(prog, wl.stat, wl.forcing_at(h), wl.params, acc)
     dt = time.perf_counter() - t0
     return {"value": ncell * hours / dt, "unit": "cell-steps/s", "cores": 1, "kind": "port",
-            "sample": f"{ncell} cells x {hours} hourly steps of the configs[1] generator, float64 NumPy oracle, "
+            "sample": f"{ncell} cells x {hours} hourly steps of the bench's seeded column generator, float64 NumPy "
+                      f"oracle, "
                       f"{dt:.1f} s"}
 
 
