@@ -79,20 +79,51 @@ class DayLoop:
         self._mbegin = lib.ibis_month_begin_f32 if f32 else lib.ibis_month_begin_f64
         self._mend = lib.ibis_month_end_f32 if f32 else lib.ibis_month_end_f64
         self.wet = torch.zeros((L.N_WET, ld), dtype=cols.dtype, device=cols.device)
+        self.checkpoint = None          # (leaves, meta, extra) of the checkpoint the loop started from
 
     @classmethod
     def from_restart(cls, path: str, dtype=torch.float32, device="cuda", params: StepParams | None = None,
                      day_params: DayParams | None = None, **kw):
         """A day loop seeded from a reference checkpoint: the columns, the
-        daily-cadence state, and the last hour's soil-water stress the next
-        day's phenology reads."""
-        cols, P, leaves, _, _ = _restart.columns_from_restart(path, dtype=dtype, device=device, params=params,
-                                                              acc=True)
+        daily-cadence state, the running sums, and the last hour's soil-water
+        stress the next day's phenology reads (:meth:`save` writes them back)."""
+        cols, P, leaves, meta, extra = _restart.columns_from_restart(path, dtype=dtype, device=device,
+                                                                     params=params, acc=True)
         n = cols.ncell
+        # the annual sums and the last hour's stress carry on from the file; the
+        # a10anc* leaves hold 10-day means between days (DAYST), not sums
         acc0 = _restart.group_from_leaves(leaves, "ACC", n)
-        cols.set_acc({k: acc0[k] for k in ("stresstu_last", "stresstl_last") if k in acc0})
+        cols.set_acc({k: v for k, v in acc0.items() if not k.startswith("a10anc")})
         dayst = _restart.group_from_leaves(leaves, "DAYST", n)
-        return cls(cols, P, day_params or DayParams(), dayst, **kw)
+        loop = cls(cols, P, day_params or DayParams(), dayst, **kw)
+        loop.checkpoint = (leaves, meta, extra)
+        return loop
+
+    # the STAT fields the daily cadence rewrites
+    _STAT_WRITTEN = ("frac", "lai", "ztop", "zbot", "tco2mic")
+
+    def save(self, path: str, leaves: dict | None = None, meta=None, extra=None):
+        """Write the state after the last day as a reference checkpoint: the
+        prognostic state, the canopy structure and respiration the cadence
+        rewrites, the daily and annual sums and the last hour's stress, and the
+        daily-cadence state (phenology, 10-day means, carbon pools), into the
+        leaves of ``leaves`` (default: the checkpoint the loop started from);
+        every other leaf is carried over."""
+        if leaves is None:
+            if getattr(self, "checkpoint", None) is None:
+                raise ValueError("no checkpoint leaves to write into: pass leaves=")
+            leaves, meta0, extra0 = self.checkpoint
+            meta = meta0 if meta is None else meta
+            extra = extra0 if extra is None else extra
+        c = self.cols
+        stat = synth.from_planes("STAT", c.stat.cpu().numpy(), c.ncell)
+        acc = c.acc_host()
+        # between days the reference keeps the 10-day means in the leaves the
+        # step uses for daily sums: the DAYST values go last and win
+        acc = {k: v for k, v in acc.items() if not k.startswith("a10anc")}
+        groups = [("PROG", c.prog_host()), ("STAT", {k: stat[k] for k in self._STAT_WRITTEN}), ("ACC", acc),
+                  ("DAYST", self.dayst_host())]
+        _restart.write_state(path, leaves, groups, meta, extra)
 
     # ------------------------------------------------------------------ state
     def dayst_host(self) -> dict:

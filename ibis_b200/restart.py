@@ -163,13 +163,12 @@ def columns_from_restart(path: str, dtype=None, device="cuda", params=None, diag
     return cols, P, leaves, meta, extra
 
 
-def write_columns(path: str, cols, leaves: dict, meta=None, extra=None):
-    """Save ``cols``' prognostic state (and diagnostics, if the columns keep them)
-    into the checkpoint ``leaves`` came from, in the leaves' own dtypes."""
+def write_state(path: str, leaves: dict, groups, meta=None, extra=None):
+    """Save ``leaves`` with the values of ``groups`` -- a sequence of
+    (layout group, {field: per-cell array}) pairs, later pairs taking precedence
+    where two fields share a leaf -- written into the leaves they mirror, in the
+    leaves' own dtypes.  Leaves no group names are carried over unchanged."""
     out = dict(leaves)
-    groups = [("PROG", cols.prog_host())]
-    if cols.diag is not None:
-        groups.append(("DIAG", cols.diag_host()))
     for group, values in groups:
         for f in L.GROUPS[group]:
             old = out.get(f.leaf)
@@ -178,3 +177,12 @@ def write_columns(path: str, cols, leaves: dict, meta=None, extra=None):
             v = np.asarray(values[f.name]).astype(np.asarray(old).dtype)
             out[f.leaf] = v.reshape(-1)[0] if np.ndim(old) == 0 else v.reshape(np.shape(old))
     save(path, out, meta, extra)
+
+
+def write_columns(path: str, cols, leaves: dict, meta=None, extra=None):
+    """Save ``cols``' prognostic state (and diagnostics, if the columns keep them)
+    into the checkpoint ``leaves`` came from, in the leaves' own dtypes."""
+    groups = [("PROG", cols.prog_host())]
+    if cols.diag is not None:
+        groups.append(("DIAG", cols.diag_host()))
+    write_state(path, leaves, groups, meta, extra)

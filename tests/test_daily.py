@@ -300,3 +300,45 @@ def test_device_day_loop_f32_generated_forcing(cuda_lib):
     for k in ("wsoi", "wisoi"):
         e = per_cell(prog[k], w[k])
         assert e[-1] < 3e-2 and e[-4] < 2e-3, (k, e[-4:])
+
+
+@pytest.mark.gpu
+def test_day_loop_from_checkpoint_and_back(cuda_lib, tmp_path):
+    """DayLoop.from_restart seeds columns, daily-cadence state and running sums
+    from the 16-cell checkpoint; one float64 day (forcing as the reference
+    made it) and DayLoop.save give a checkpoint whose leaves are the loop's
+    state in the file's float32 and agree with the reference's own day loop to
+    float32 storage (1e-6 outside the threshold cells)."""
+    import torch
+    from ibis_b200 import synth
+    from ibis_b200.daily import DayLoop
+    z, n, prog, stat, day, acc0, P = load_case()
+    loop = DayLoop.from_restart(CKPT, dtype=torch.float64, params=P, day_params=day_params(z), lat=z["in.lat"],
+                                seed=int(z["in.seed"]), jday=int(z["in.jday0"]), day=0)
+    loop.params.flags = P.flags
+    cols = loop.cols
+    dd, daily = _daily_tensor(z, 0, cols.ld, torch)
+    hours = hourly(z, 0, n)
+    forc = {k: np.stack([F[k] for F in hours]) for k in hours[0]}
+    td = torch.from_numpy(np.pad(dd["td"], (0, cols.ld - n))).cuda()
+    loop.run_day(daily, forc=torch.from_numpy(synth.forcing_planes(forc, cols.ld, dtype=np.float64)).cuda(), td=td)
+    torch.cuda.synchronize()
+    path = tmp_path / "after_day.npz"
+    loop.save(str(path))
+    back, meta, _ = restart.load(str(path))
+    orig, meta0, _ = restart.load(CKPT)
+    assert meta == meta0
+    keep = np.setdiff1d(np.arange(n), DAY_THRESHOLD_CELLS)
+    acc = {k: v for k, v in cols.acc_host().items() if k in ACC_CHECK}
+    for group, values in (("PROG", cols.prog_host()), ("DAYST", loop.dayst_host()), ("ACC", acc)):
+        ref = want(z, 0, group)
+        for f in L.GROUPS[group]:
+            if f.leaf not in back or f.name not in ref or f.name not in values:
+                continue
+            mine = np.asarray(values[f.name]).astype(np.asarray(orig[f.leaf]).dtype).astype(np.float64)
+            if np.size(back[f.leaf]) == 1:       # a scalar leaf holds the first cell's value
+                mine = np.full(np.shape(ref[f.name]), mine.reshape(-1)[0])
+            v = np.broadcast_to(np.asarray(back[f.leaf], np.float64), np.shape(ref[f.name]))
+            v = v.reshape(np.shape(ref[f.name]))
+            assert np.array_equal(v, mine.reshape(v.shape)), f.name
+            assert not compare({f.name: v[keep]}, {f.name: ref[f.name][keep]}, 1e-6), (group, f.name)
