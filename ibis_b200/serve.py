@@ -42,7 +42,7 @@ from . import ensemble as E
 from . import layout as L
 from . import lib as _lib
 from . import synth
-from .lib import IbisEnsembleC
+from .lib import IbisEnsembleC, IbisEnsembleDailyC
 from .params import StepParams
 
 INT_MAX = 2 ** 31 - 1
@@ -73,12 +73,16 @@ class Result:
 
 class SiteLibrary:
     """Static planes, initial state and forcing records of the sites requests may
-    name, resident on the device (``years`` whole years of records per site)."""
+    name, resident on the device (``years`` whole years of records per site).
+    With ``daily`` the records are days of weather (48 bytes per site-day
+    instead of 48 per site-hour) and the runs generate their hours in the
+    kernel (``ibis_ensemble_daily_f32``); epochs are then whole days."""
 
     def __init__(self, nsite: int, years: int, seed: int = 0, year_hours: int = E.YEAR_HOURS, device="cuda",
-                 lat_range=(-40.0, 70.0), params: StepParams | None = None):
+                 lat_range=(-40.0, 70.0), params: StepParams | None = None, daily: bool = False):
         spec = E.make_ensemble(nsite, 1, site_hours=np.full(nsite, years * year_hours), seed=seed,
-                               lat_range=lat_range, year_hours=year_hours, params=params)
+                               lat_range=lat_range, year_hours=year_hours, params=params, daily=daily)
+        self.daily = bool(daily)
         self.spec = spec
         self.nsite, self.years, self.year_hours = nsite, years, year_hours
         self.device = torch.device(device)
@@ -87,9 +91,14 @@ class SiteLibrary:
         self.ld_site = L.leading_dim(nsite)
         self.stat = torch.from_numpy(synth.to_planes("STAT", spec.stat, self.ld_site)).to(self.device)
         self.prog = torch.from_numpy(synth.to_planes("PROG", spec.prog, self.ld_site)).to(self.device)
-        self.forc = torch.from_numpy(spec.forc).to(self.device)
-        self.first = spec.site_first.astype(np.int64)
+        self.forc = torch.from_numpy(spec.daily if daily else spec.forc).to(self.device)
+        self.first = spec.site_first.astype(np.int64)       # first record: an hour, or with ``daily`` a day
         self.params = spec.params
+        if daily:
+            self.lat = torch.from_numpy(np.asarray(spec.latitude, dtype=np.float32)).to(self.device)
+            self.daily_desc = IbisEnsembleDailyC(records=self.forc.data_ptr(), site_lat=self.lat.data_ptr(),
+                                                 len=int(self.forc.shape[0]),
+                                                 seed=int(spec.weather_seed) & 0xFFFFFFFF, flags=1)
 
     @property
     def nbytes(self) -> int:
@@ -112,6 +121,8 @@ class Server:
         self.max_years = library.years
         self.epoch_hours = int(epoch_hours)
         self.lookahead = max(1, int(lookahead))
+        if library.daily and self.epoch_hours % 24:
+            raise ValueError("a library of day records needs epochs of whole days")
         self.block = int(block)
         free_bytes = budget_bytes - library.nbytes
         if free_bytes <= 0:
@@ -156,7 +167,8 @@ class Server:
         d, h = self._desc[buf]
         k = active.size
         hf, hn, hp, ho = (h[x].numpy() for x in ("forc", "nstep", "pos", "order"))
-        hf[active] = self.lib.first[self.slot_site[active]] + self.slot_pos[active]
+        pos = self.slot_pos[active] // 24 if self.lib.daily else self.slot_pos[active]
+        hf[active] = self.lib.first[self.slot_site[active]] + pos
         hn[active] = n
         hp[active] = self.slot_pos[active]
         ho[:k] = active[np.argsort(-n, kind="stable")]          # longest first
@@ -167,10 +179,17 @@ class Server:
                           forc=self.lib.forc.data_ptr(), run_params=self.run_params.data_ptr(),
                           run_site=self.run_site.data_ptr(), run_forc=d["forc"].data_ptr(),
                           run_nstep=d["nstep"].data_ptr(), run_pos=d["pos"].data_ptr(), order=d["order"].data_ptr(),
-                          yearly=self.yearly.data_ptr(), forc_len=int(self.lib.forc.shape[0]), nrun=self.nslot,
+                          yearly=self.yearly.data_ptr(), forc_len=0 if self.lib.daily else int(self.lib.forc.shape[0]),
+                          nrun=self.nslot,
                           ld_run=self.ld, nsite=self.lib.nsite, ld_site=self.lib.ld_site, nyear=self.max_years,
                           year_steps=self.lib.year_hours, norder=k, queue=self.queue.data_ptr(),
                           status=self.status.data_ptr())
+        if self.lib.daily:
+            _lib.check(self._so.ibis_ensemble_daily_f32(ctypes.byref(e), ctypes.byref(self.lib.daily_desc),
+                                                        ctypes.byref(self._pc), self.block,
+                                                        ctypes.c_void_p(self.stream.cuda_stream)),
+                       "ibis_ensemble_daily_f32")
+            return
         _lib.check(self._so.ibis_ensemble_f32(ctypes.byref(e), ctypes.byref(self._pc), self.block,
                                               ctypes.c_void_p(self.stream.cuda_stream)), "ibis_ensemble_f32")
 

@@ -113,3 +113,34 @@ def test_realtime_loop_reports_latency(cuda_lib):
     st = srv.serve(reqs)
     assert st["requests"] == len(reqs) and st["p99_s"] >= st["p50_s"] > 0.0
     assert all(r.done >= r.arrival for r in srv.results.values())
+
+
+@pytest.mark.gpu
+def test_daily_library_request_alone_equals_in_mix_and_ensemble(cuda_lib):
+    """A library of day records (hours generated in the kernel): a request's
+    result is the same bits alone, in a mix admitted mid-flight, and as one
+    persistent daily-form ensemble launch of the same runs."""
+    lib = S.SiteLibrary(nsite=6, years=3, seed=1, year_hours=48, daily=True)
+    assert lib.forc.shape == (6 * 3 * 2, E.DAILY_WORDS)
+    rng = np.random.default_rng(6)
+    r0 = S.Request(rid=0, sites=np.array([0, 2, 5]), years=3, vector=E.draw_vectors(rng, 1)[0], arrival=0.0)
+    alone = S.Server(lib, budget_bytes=lib.nbytes + 64 * S.slot_bytes(3), epoch_hours=24)
+    alone.serve([r0], realtime=False, epoch_seconds=1.0)
+    a = alone.results[0]
+    others = _requests(rng, 10)
+    mix = S.Server(lib, budget_bytes=lib.nbytes + 64 * S.slot_bytes(3), epoch_hours=72)
+    st = mix.serve(others + [S.Request(rid=0, sites=r0.sites, years=3, vector=r0.vector, arrival=2.0)],
+                   realtime=False, epoch_seconds=1.0)
+    assert st["requests"] == 11 and st["status"][0] == 0 and mix.results[0].admitted > 0.0
+    np.testing.assert_array_equal(a.yearly, mix.results[0].yearly)
+    assert np.isfinite(a.yearly).all() and not a.nonfinite
+    spec = lib.spec
+    sub = E.EnsembleSpec(nsite=spec.nsite, nparam=1, site_hours=spec.site_hours, stat=spec.stat, prog=spec.prog,
+                         forc=None, site_first=spec.site_first, vectors=r0.vector[None].copy(), params=spec.params,
+                         latitude=spec.latitude, daily=spec.daily, weather_seed=spec.weather_seed)
+    ens = E.Ensemble(sub, year_steps=48)
+    ens.run()
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(a.yearly, ens.yearly_sums()[r0.sites])
+    with pytest.raises(ValueError):
+        S.Server(lib, budget_bytes=lib.nbytes + 64 * S.slot_bytes(3), epoch_hours=30)
