@@ -89,11 +89,15 @@ def hourly(z, d, n):
                            OW.uniform24(seed, cells, d, 2 + h), 3600.0, fira_obs=dd["fira"]) for h in range(24)]
 
 
-def oracle_days(ndays=None, perturb=None):
+def oracle_days(ndays=None, perturb=None, f_inund=None):
     """The oracle's day loop on the three-day case; yields (day, prog, dayst,
     stat, acc) after each day.  ``perturb`` = (day, hour, eps) scales the
-    temperatures of the state by (1 + eps) before that hour."""
+    temperatures of the state by (1 + eps) before that hour; ``f_inund`` turns
+    on the hourly wetland CH4 with that inundated fraction."""
     z, n, prog, stat, day, acc0, P = load_case()
+    if f_inund is not None:
+        P.flags |= FLAG_CH4
+        stat["f_inund"] = np.asarray(f_inund, np.float64)
     DP = day_params(z)
     acc = oracle.new_acc(n)
     for k in ACC_CHECK + ("stresstu_last", "stresstl_last"):
@@ -342,3 +346,43 @@ def test_day_loop_from_checkpoint_and_back(cuda_lib, tmp_path):
             v = v.reshape(np.shape(ref[f.name]))
             assert np.array_equal(v, mine.reshape(v.shape)), f.name
             assert not compare({f.name: v[keep]}, {f.name: ref[f.name][keep]}, 1e-6), (group, f.name)
+
+
+@pytest.mark.gpu
+def test_device_month_matches_oracle_month(cuda_lib):
+    """Three days as a month with hourly wetland CH4: ibis_month_begin, the
+    device day loop in float64, ibis_month_end (mean of the hourly fluxes, the
+    carbon partition) against the oracle's day loop and oracle.month on the
+    same inputs: 1e-9 outside the threshold cells."""
+    import torch
+    from ibis_b200 import synth
+    from oracle import month as OM
+    f_inund = np.random.default_rng(2).uniform(0.0, 1.0, 16)
+    z, n, _, _, day0, _, P = load_case()
+    *_, (d, prog, day, stat, acc) = list(oracle_days(f_inund=f_inund))
+    P.flags |= FLAG_CH4
+    nd = int(z["in.ndays"])
+    wet0 = dict(flux=np.zeros(n), annual=np.zeros(n), zwt=np.zeros(n))
+    ref, ay, take = OM.month_end(wet0, prog, stat, acc["ch4"], day["ayco2mic"], day0["ayco2mic"], nd,
+                                 np.asarray(P.hsoi, np.float64), P, from_mean=True, partition=True)
+    z, n, cols, loop, torch = _device_loop(torch.float64)
+    loop.params.flags |= FLAG_CH4
+    cols.stat[L.OFF["STAT"]["f_inund"][0], :n] = torch.from_numpy(f_inund).to(cols.stat)
+    loop.begin_month(new_year=True)
+    for d in range(nd):
+        dd, daily = _daily_tensor(z, d, cols.ld, torch)
+        hours = hourly(z, d, n)
+        forc = {k: np.stack([F[k] for F in hours]) for k in hours[0]}
+        td = torch.from_numpy(np.pad(dd["td"], (0, cols.ld - n))).cuda()
+        loop.run_day(daily, forc=torch.from_numpy(synth.forcing_planes(forc, cols.ld, dtype=np.float64)).cuda(),
+                     td=td)
+    loop.end_month(nd, from_mean=True, partition=True)
+    torch.cuda.synchronize()
+    keep = np.setdiff1d(np.arange(n), DAY_THRESHOLD_CELLS)
+    wet = loop.wet_host()
+    got = {"flux": wet["flux"], "annual": wet["annual"], "zwt": wet["zwt"], "ch4c": wet["ch4c"],
+           "ayco2mic": loop.dayst_host()["ayco2mic"]}
+    want_ = {"flux": ref["flux"], "annual": ref["annual"], "zwt": ref["zwt"], "ch4c": take, "ayco2mic": ay}
+    assert np.any(want_["flux"][keep] > 0.0) and np.any(take[keep] > 0.0)
+    bad = compare({k: v[keep] for k, v in got.items()}, {k: v[keep] for k, v in want_.items()}, 1e-9)
+    assert not bad, bad[:5]
