@@ -4,7 +4,7 @@ A :class:`Columns` owns the structure-of-arrays buffers of ``ncell`` columns on
 one GPU (torch tensors are used only as device allocations) and advances them
 through the C ABI of ``include/ibis_b200.h``.  Forcing for ``nstep`` hours is a
 ``(nstep, IBIS_FORC_COUNT, ld)`` device tensor; the whole run executes in one
-launch, so prognostic state stays in registers across the hours.
+launch, so prognostic state and accumulators stay on chip across the hours.
 """
 from __future__ import annotations
 
@@ -19,6 +19,8 @@ from . import synth
 from .params import StepParams, FLAG_DIAG, FLAG_ACC, FLAG_CH4, FLAG_SOIL_MEANS
 
 INT_MAX = 2 ** 31 - 1
+AUTO_FUSED = 6          # fused, block 224, accumulators on chip
+AUTO_MIN_HOURS = 4      # shorter launches keep the accumulators in global memory (configuration 0)
 _ACC_FLAGS = FLAG_ACC | FLAG_CH4 | FLAG_SOIL_MEANS
 
 
@@ -58,7 +60,15 @@ class Columns:
 
     def set_mode(self, mode: str):
         """``fused`` (one kernel per launch), ``split`` (surface + ground kernels per hour),
-        or an integer launch configuration (see ``lib.configs()``)."""
+        or an integer launch configuration (see ``lib.configs()``).
+
+        ``fused`` picks the configuration per call in FP32: block 224 with the
+        accumulators on chip (configuration 6, the fastest at 95,333 cells)
+        for launches of ``AUTO_MIN_HOURS`` hours or more, the default
+        configuration 0 (global accumulators) for shorter ones; ``tune.tune``
+        times every configuration on the caller's own batch instead."""
+        if mode is None:
+            mode = "fused"
         if isinstance(mode, (int, np.integer)) and not isinstance(mode, bool):
             cfgs = _lib.configs()
             if not 0 <= int(mode) < len(cfgs):
@@ -67,10 +77,10 @@ class Columns:
             form = cfgs[cfg]["form"]
         elif mode in ("fused", "split"):
             form = mode
-            cfg = 0 if mode == "fused" else 8
+            cfg = (None if self.dtype == torch.float32 else 0) if mode == "fused" else 8
         else:
             raise ValueError("mode must be 'fused', 'split' or a configuration index")
-        if self.dtype != torch.float32 and (form == "split" or cfg != 0):
+        if self.dtype != torch.float32 and (form == "split" or cfg not in (0, None)):
             raise ValueError("only the default fused form exists in float64")
         if form == "split" and self.scratch is None:
             self.scratch = torch.zeros((_lib.load().ibis_mid_planes(), self.ld), dtype=self.dtype,
@@ -145,6 +155,12 @@ class Columns:
         return bool(s[0] & 1), int(s[1])
 
     # -------------------------------------------------------------- compute
+    def launch_config(self, nstep: int) -> int:
+        """The launch configuration a call of ``nstep`` hours uses."""
+        if self.config is not None:
+            return self.config
+        return AUTO_FUSED if nstep >= AUTO_MIN_HOURS else 0
+
     def run(self, forc: torch.Tensor, params: StepParams, nstep: int | None = None, stream=None):
         """Advance the columns ``nstep`` hours with forcing ``forc`` (asynchronous)."""
         if forc.dtype != self.dtype or forc.device != self.device:
@@ -170,7 +186,7 @@ class Columns:
         if self.dtype == torch.float32:
             rc = self._cfg_fn(_ptr(self.prog), _ptr(self.stat), _ptr(forc), _ptr(self.diag), _ptr(self.acc),
                               _ptr(self.scratch), self.ncell, self.ld, nstep, ctypes.byref(p), _ptr(self.status),
-                              ctypes.c_void_p(stream.cuda_stream), self.config)
+                              ctypes.c_void_p(stream.cuda_stream), self.launch_config(nstep))
         else:
             rc = self._fn(_ptr(self.prog), _ptr(self.stat), _ptr(forc), _ptr(self.diag), _ptr(self.acc), self.ncell,
                           self.ld, nstep, ctypes.byref(p), _ptr(self.status), ctypes.c_void_p(stream.cuda_stream))

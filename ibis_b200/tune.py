@@ -73,5 +73,5 @@ def tune(cols, forc: torch.Tensor, params, nstep: int | None = None, reps: int =
     res = {"best": best, "ms": ms, "configs": [c for c in all_cfgs if c["id"] in ids]}
     if configs is None:
         _CACHE[key] = res
-    cols.set_mode(best if apply else mode0)
+    cols.set_mode(best if apply else ("fused" if mode0 is None else mode0))
     return res
