@@ -27,6 +27,7 @@ constexpr LaunchConfig kConfigs[] = {
     {1, 128, 2, 128, 3}, {1, 256, 1, 256, 2}, {1, 128, 3, 128, 4}};
 constexpr int kNumConfigs = sizeof(kConfigs) / sizeof(kConfigs[0]);
 constexpr int kDefaultFused = 0;
+constexpr int kLongFused = 6;      // ibis_step_f32's choice for launches of kAccSmemMinSteps hours or more
 constexpr int kDefaultSplit = 8;
 
 // FP32 kernels keep each column's prognostic state in shared memory (array of

@@ -16,8 +16,11 @@ IBIS_SUN_CONFIGS(IBIS_EXTERN, 9)
 
 extern "C" int ibis_step_f32(float* prog, const float* stat, const float* forc, float* diag, float* acc, int ncell,
                              int ld, int nstep, const IbisParams* params, int* status, void* stream) {
+    // launches of several hours take the fastest fused configuration at full
+    // size (block 224, accumulators on chip); shorter ones the default
+    const int cfg = nstep >= ibis::kAccSmemMinSteps ? ibis::kLongFused : ibis::kDefaultFused;
     return ibis::hourly_step<float>(prog, stat, forc, diag, acc, ncell, ld, nstep, params, status, stream, nullptr,
-                                    ibis::kDefaultFused);
+                                    cfg);
 }
 
 extern "C" int ibis_step_split_f32(float* prog, const float* stat, const float* forc, float* diag, float* acc,

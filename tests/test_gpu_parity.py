@@ -131,3 +131,33 @@ def test_run_from_host_matches_device_run(cuda_lib, chunk):
     b.run_from_host(forc.cpu().pin_memory(), c.params, chunk=chunk)
     torch.cuda.synchronize()
     assert torch.equal(a.prog, b.prog) and torch.equal(a.acc, b.acc)
+
+
+@pytest.mark.parametrize("nstep", [1, 24])
+def test_plain_entry_matches_its_configuration(cuda_lib, nstep):
+    """ibis_step_f32 (no configuration argument) gives the same bits as
+    ibis_step_config_f32 with the configuration it takes for that launch
+    length: block 224 with on-chip accumulators for a day, the default
+    configuration for one hour."""
+    import ctypes
+    from ibis_b200 import lib
+    c = Case("day_mixed")
+    so = lib.load()
+    out = []
+    for how in ("plain", "config"):
+        cols = Columns.from_host(c.prog, c.stat, dtype=torch.float32, acc=True)
+        forc = cols.forcing(c.forc, 0, nstep)
+        p = ctypes.byref(c.params.to_c())
+        ptr = lambda t: ctypes.c_void_p(t.data_ptr())
+        s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        if how == "plain":
+            rc = so.ibis_step_f32(ptr(cols.prog), ptr(cols.stat), ptr(forc), ctypes.c_void_p(0), ptr(cols.acc),
+                                  cols.ncell, cols.ld, nstep, p, ptr(cols.status), s)
+        else:
+            rc = so.ibis_step_config_f32(ptr(cols.prog), ptr(cols.stat), ptr(forc), ctypes.c_void_p(0),
+                                         ptr(cols.acc), ctypes.c_void_p(0), cols.ncell, cols.ld, nstep, p,
+                                         ptr(cols.status), s, 6 if nstep >= 4 else 0)
+        assert rc == 0
+        torch.cuda.synchronize()
+        out.append((cols.prog.clone(), cols.acc.clone()))
+    assert torch.equal(out[0][0], out[1][0]) and torch.equal(out[0][1], out[1][1])
