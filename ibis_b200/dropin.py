@@ -1,4 +1,4 @@
-"""Drop-in for the reference's step function over its own state pytrees.
+"""Drop-in for the reference's step function (and its day loop) over its own state pytrees.
 
 The reference's hot path is one pure function,
 
@@ -18,6 +18,8 @@ kernels; float32 leaves the production FP32 kernels.
 :func:`run_hours` is the multi-hour form with the day loop's accumulators
 (``_run_day_inner._step_body``, loops_gswp3.py:115-320): one launch for all
 hours, forcing given as arrays instead of the reference's weather generator.
+:func:`run_month_scan` runs whole days of the GSWP3 day loop
+(``_run_month_scan``, loops_gswp3.py:346-612) from the days' weather.
 
 The leaves are copied to and from the device on every call (the reference's
 contract is a host-visible pytree); :class:`ibis_b200.columns.Columns` keeps
@@ -216,3 +218,114 @@ def run_hours(state, consts, params, forcing: dict, dtime: float, ch4_inund=None
     out = cols.acc_host(compensated=True)
     out["_planes"] = cols.acc.cpu().numpy().copy()
     return state, out
+
+
+# Where each daily-cadence parameter lives in the reference's SimParams:
+# phenology (physics/phenology.py:20, PhenoParams) and soil biogeochemistry
+# (io/parameters.py:176, BGCParams; ``bgc_fmax`` is its ``fmax``).
+def _day_param_paths():
+    from .params import DAY_PARAM_FIELDS
+    names = [n for n, _, _ in DAY_PARAM_FIELDS]
+    pheno = names[:names.index("lig_frac")]
+    return {n: (f"params.pheno.{n}" if n in pheno else f"params.bgc_params.{'fmax' if n == 'bgc_fmax' else n}")
+            for n in names}
+
+
+DAY_PARAM_PATHS = _day_param_paths()
+_METHANE_FIELDS = ("sat_crit", "z_max", "r_ch4", "q10p", "t_ref", "z_wt_max", "z_wt_ref", "z_tau", "tau_oxid")
+
+
+def day_params(params):
+    """The daily-cadence parameter record equivalent to a reference ``SimParams``."""
+    from .params import DayParams
+    DP = DayParams()
+    for name, path in DAY_PARAM_PATHS.items():
+        v = _get({"params": params}, path)
+        if v is not None:
+            setattr(DP, name, np.asarray(v, dtype=np.float64) if np.size(v) > 1 else float(np.asarray(v)))
+    return DP
+
+
+def run_month_scan(state, consts, params, xs, nsoilcall: int, ndaypy: int, dtime: float, nband: int = 2,
+                   obs_sw: bool = False, ch4_hourly: bool = False, ch4_args=None, soil_means: bool = False,
+                   seed: int = 0, day0: int = 0, device="cuda"):
+    """Days of the reference's GSWP3 day loop on the GPU, with the arguments of
+    its ``_run_month_scan`` (python-port/ibis/timestepping/loops_gswp3.py:346-612):
+    ``xs`` = (td, tmax, tmin, cloud, precip, psurf, qd, ud, iwet, rlds, jdays[,
+    sw_h, use_h]) as (ndays, npoi) arrays (sw_h (ndays, 24, npoi)).  Returns
+    ``(state, (daily_gpp, daily_aet, daily_rh))`` -- the reference also returns
+    its PRNG key, which has no counterpart here: the day's variates (event
+    timing, hourly wind) come from the counter-based generator keyed by
+    (``seed``, ``day0`` + day, cell) instead of ``jax.random``.
+
+    Supported as the reference's defaults run it: one soil-BGC call per day
+    (``nsoilcall`` 1), two radiation bands, the seasonal formulations, stress
+    accumulator, crop and slot types off; ``iwet`` is not used (the reference's
+    day loop does not read it either)."""
+    from . import forcing as _forcing
+    from .daily import DayLoop
+    if int(nsoilcall) != 1 or int(nband) != 2:
+        raise NotImplementedError("one soil-BGC call per day and two radiation bands only")
+    xs = [np.asarray(x) for x in xs]
+    td, tmax, tmin, cloud, precip, psurf, qd, ud, _iwet, rlds, jdays = xs[:11]
+    sw_h = use_h = None
+    if obs_sw:
+        sw_h, use_h = xs[11], xs[12]
+    nday, ncell = td.shape
+    P = step_params(state, consts, params, dtime, ndaypy)
+    P.flags |= FLAG_ACC | (FLAG_SOIL_MEANS if soil_means else 0)
+    dtype = _dtype_of(state)
+    prog = _leaf_dict(state, "PROG", ncell)
+    stat = _leaf_dict(state, "STAT", ncell)
+    if ch4_hourly and ch4_args is not None:
+        from .params import FLAG_ZWT_OBS
+        f_inund, mp, zwt_obs = ch4_args
+        P.flags |= FLAG_CH4
+        stat["f_inund"] = np.asarray(f_inund, dtype=np.float64)
+        for k in _METHANE_FIELDS:
+            if getattr(mp, k, None) is not None:
+                setattr(P, k, float(getattr(mp, k)))
+        if zwt_obs is not None:
+            P.flags |= FLAG_ZWT_OBS
+            stat["zwt_obs"] = np.asarray(zwt_obs, dtype=np.float64)
+    cols = Columns.from_host(prog, stat, dtype=dtype, device=device, acc=True)
+    acc0 = _leaf_dict(state, "ACC", ncell)
+    cols.set_acc({k: v for k, v in acc0.items() if not k.startswith("a10anc")})
+    lat = np.rad2deg(np.asarray(_get({"params": params}, "params.latitude"), dtype=np.float64)).reshape(ncell)
+    loop = DayLoop(cols, P, day_params(params), _leaf_dict(state, "DAYST", ncell), lat=lat, seed=seed,
+                   jday=int(jdays[0]), day=day0, dtime=dtime, observed_fira=True)
+    daily = {"td": td, "tmax": tmax, "tmin": tmin, "cloud": cloud, "precip": precip, "psurf": psurf, "qd": qd,
+             "ud": ud, "fira": rlds}
+    d_daily = torch.from_numpy(_forcing.daily_planes(daily, cols.ld)).to(cols.device)
+    ld = cols.ld
+    sums = torch.zeros((nday + 1, 3, ld), dtype=dtype, device=cols.device)
+    planes = (L.OFF["ACC"]["aygpptot"][0], L.OFF["DAYST"]["ayaet"][0], L.OFF["DAYST"]["ayco2mic"][0])
+
+    def snap(i):
+        sums[i, 0] = cols.acc[planes[0]] - cols.acc[L.N_ACC + planes[0]]
+        sums[i, 1] = loop.dayst[planes[1]]
+        sums[i, 2] = loop.dayst[planes[2]]
+
+    snap(0)
+    for d in range(nday):
+        kw = {}
+        if sw_h is not None:
+            sw = np.zeros((sw_h.shape[1], ld), np.float32)
+            sw[:, :ncell] = sw_h[d]
+            use = np.zeros(ld, np.uint8)
+            use[:ncell] = np.asarray(use_h[d], dtype=bool)
+            kw = dict(sw_obs=torch.from_numpy(sw).to(cols.device), use=torch.from_numpy(use).to(cols.device))
+        loop.run_day(d_daily[d], **kw)
+        snap(d + 1)
+    torch.cuda.synchronize(cols.device)
+    s = sums.cpu().numpy().astype(np.float64)[:, :, :ncell]
+    diag = tuple(np.diff(s[:, j], axis=0) for j in range(3))
+    from . import synth
+    st = synth.from_planes("STAT", cols.stat.cpu().numpy(), ncell)
+    stat_now = {k: st[k] for k in DayLoop._STAT_WRITTEN}
+    acc = {k: v for k, v in cols.acc_host().items() if not k.startswith("a10anc")}
+    state = _write_back(state, cols.prog_host(), "PROG", dtype)
+    state = _write_back(state, stat_now, "STAT", dtype)
+    state = _write_back(state, acc, "ACC", dtype)
+    state = _write_back(state, loop.dayst_host(), "DAYST", dtype)
+    return state, diag

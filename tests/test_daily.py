@@ -386,3 +386,113 @@ def test_device_month_matches_oracle_month(cuda_lib):
     assert np.any(want_["flux"][keep] > 0.0) and np.any(take[keep] > 0.0)
     bad = compare({k: v[keep] for k, v in got.items()}, {k: v[keep] for k, v in want_.items()}, 1e-9)
     assert not bad, bad[:5]
+
+
+_DAY_MAP_CHECK = r"""
+import sys, numpy as np
+sys.path.insert(0, "{golden}/jaxshim"); sys.path.insert(0, "{ref}"); sys.path.insert(0, "{golden}"); sys.path.insert(0, "{repo}")
+import make_golden as mg
+from ibis_b200 import dropin
+from ibis_b200.params import DAY_PARAM_FIELDS
+z = np.load("{gold}")
+dp = dropin.day_params(mg.loops.default_sim_params(16))
+for name, n, _ in DAY_PARAM_FIELDS:
+    assert np.allclose(np.asarray(getattr(dp, name), float), z["in.dparam." + name], rtol=0, atol=0), name
+print("day mapping ok")
+"""
+
+
+@pytest.mark.skipif(not os.path.isdir("/root/reference/python-port"), reason="reference sources not present")
+def test_day_param_paths_against_reference_objects():
+    """dropin.DAY_PARAM_PATHS reads the reference's own SimParams to the values
+    the three-day fixture was run with."""
+    import subprocess
+    import sys
+    code = _DAY_MAP_CHECK.format(golden=os.path.join(HERE, "golden"), ref="/root/reference/python-port",
+                                 repo=os.path.dirname(HERE), gold=GOLD)
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0 and "day mapping ok" in r.stdout, r.stderr[-3000:]
+
+
+def _param_tree(z, lat_deg):
+    """consts/params attribute trees with the reference's paths, from the fixture's records."""
+    import types
+    from ibis_b200 import dropin
+
+    def put(root, path, v):
+        obj = root
+        *head, last = path.split(".")
+        for h in head:
+            if not hasattr(obj, h):
+                setattr(obj, h, types.SimpleNamespace())
+            obj = getattr(obj, h)
+        setattr(obj, last, v)
+
+    root = types.SimpleNamespace()
+    for name, path in dropin.PARAM_PATHS.items():
+        if path.startswith(("params.", "consts.")):
+            v = z["in.param." + name]
+            put(root, path, v if np.size(v) > 1 else float(v))
+    for name, path in dropin.DAY_PARAM_PATHS.items():
+        v = z["in.dparam." + name]
+        put(root, path, v if np.size(v) > 1 else float(v))
+    put(root, "params.latitude", np.deg2rad(lat_deg))
+    put(root, "params.h2o_consistent_weights", bool(int(z["in.param.flags"]) & 2))
+    return root.consts, root.params
+
+
+@pytest.mark.gpu
+def test_run_month_scan_dropin_equals_day_loop(cuda_lib):
+    """dropin.run_month_scan over the checkpoint's own state tree (float32, as
+    the reference's day loop runs) and the fixture's three days of weather:
+    the same bits as DayLoop on the same inputs, daily outputs equal to the
+    differences of the annual sums, and the state within the float32 day
+    loop's bounds of the reference's float64 run."""
+    import torch
+    from ibis_b200 import dropin
+    from ibis_b200.daily import DayLoop
+    z = load_case()[0]
+    n, nd = 16, int(z["in.ndays"])
+    leaves, _, _ = restart.load(CKPT)
+    state = restart.as_tree({k: (np.asarray(v).copy() if v is not None else None) for k, v in leaves.items()})
+    for k in ("z0sno", "rhos", "consno", "hsnotop", "hsnomin", "fimin", "fimax"):
+        setattr(state.snow, k, np.float32(z["in.param." + k]))      # the reference takes these from its template
+    consts, params = _param_tree(z, z["in.lat"])
+    days = [day_weather(z, d) for d in range(nd)]
+    xs = tuple(np.stack([dd[k] for dd in days]) for k in ("td", "tmax", "tmin", "cloud", "precip", "psurf", "qd",
+                                                         "ud")) + (np.zeros((nd, n)),
+                                                                   np.stack([dd["fira"] for dd in days]),
+                                                                   int(z["in.jday0"]) + np.arange(nd))
+    seed = int(z["in.seed"])
+    new, (gpp, aet, rh) = dropin.run_month_scan(state, consts, params, xs, 1, 365, 3600.0, seed=seed)
+    # the same days through DayLoop directly
+    P = dropin.step_params(state, consts, params, 3600.0, 365)
+    loop = DayLoop.from_restart(CKPT, dtype=torch.float32, params=P, day_params=dropin.day_params(params),
+                                lat=z["in.lat"], seed=seed, jday=int(z["in.jday0"]), day=0)
+    loop.params.flags = P.flags | FLAG_ACC
+    from ibis_b200 import forcing
+    daily = torch.from_numpy(forcing.daily_planes({k: np.stack([dd[k] for dd in days]) for k in days[0]},
+                                                  loop.cols.ld)).cuda()
+    loop.run(daily)
+    torch.cuda.synchronize()
+    prog = loop.cols.prog_host()
+    for f in L.PROG:
+        v = dropin._get({"s": new}, "s." + f.leaf)
+        if v is None or f.name not in prog:
+            continue
+        mine = np.asarray(prog[f.name]).astype(np.float32)
+        if np.ndim(v) == 0:
+            mine = mine.reshape(-1)[0]
+        assert np.array_equal(np.asarray(v), mine.reshape(np.shape(v))), f.name
+    dayst = loop.dayst_host()
+    for f in L.DAYST:
+        v = np.asarray(dropin._get({"s": new}, "s." + f.leaf), np.float64)
+        assert np.array_equal(v.reshape(-1), np.asarray(dayst[f.name], np.float32).astype(np.float64).reshape(-1)), \
+            f.name
+    ay0 = np.asarray(leaves["summary.ayaet"], np.float64)
+    np.testing.assert_allclose(np.cumsum(aet, axis=0)[-1], dayst["ayaet"] - ay0, rtol=1e-5, atol=1e-6)
+    assert gpp.shape == (nd, n) and rh.shape == (nd, n) and np.isfinite(gpp).all() and np.isfinite(rh).all()
+    w = want(z, nd - 1, "DAYST")
+    for k in ("tempu", "templ", "agddu", "agddl", "a10td", "ayprcp", "csoipas", "totcsoi"):
+        e = np.abs(np.asarray(dayst[k]) - w[k]) / np.maximum(np.abs(w[k]), 1e-3)
+        assert e.max() < 1e-4, (k, float(e.max()))
