@@ -409,6 +409,7 @@ def run_ensemble(args):
     replayed from a CUDA graph) are timed beside it."""
     import torch
     from ibis_b200 import ensemble as E
+    from ibis_b200 import synth
 
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
@@ -469,6 +470,27 @@ def run_ensemble(args):
                   "note": "same sites, vectors and record lengths over 48-byte day records; each run generates its "
                           "hours in the kernel (ibis_ensemble_daily_f32)"}
     del ens_d
+    # calibration runs with the daily cadence: 30 days of every run, one
+    # persistent launch per day between the day kernels (EnsembleDayLoop)
+    from ibis_b200.ensemble_daily import EnsembleDayLoop
+    rng_d = np.random.Generator(np.random.PCG64(8))
+    ndl = 30
+    edl_args = (spec.stat, spec.prog, synth.make_dayst(rng_d, spec.stat, spec.latitude),
+                synth.make_daily_weather(rng_d, spec.latitude, ndl), spec.latitude, spec.vectors, spec.params)
+    EnsembleDayLoop(*edl_args, seed=5, jday=150).run(3)
+    torch.cuda.synchronize()
+    edl = EnsembleDayLoop(*edl_args, seed=5, jday=150)
+    a_ev, b_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a_ev.record(stream)
+    edl.run()
+    b_ev.record(stream)
+    b_ev.synchronize()
+    ms_dl = a_ev.elapsed_time(b_ev)
+    day_loop = {"value": edl.cell_steps() / (ms_dl / 1e3), "ms": ms_dl, "days": ndl, "runs": edl.nrun,
+                "ms_per_day": ms_dl / ndl, "nonfinite_runs": edl.nonfinite()[0],
+                "note": "every run with the daily cadence (per-run canopy structure and carbon pools): per day the "
+                        "sites' forcing generated, day_begin, one persistent launch of 24 hours, day_end"}
+    del edl
     line = {
         "metric": "cell-steps/s, calibration ensemble (persistent launch)", "value": cs / (m / 1e3),
         "unit": "cell-steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": m,
@@ -488,6 +510,7 @@ def run_ensemble(args):
         "persistent_vs_hourly_graph": float(np.mean(ms_graph)) / m,
         "plain_per_vector": plain,
         "daily_form": daily_form,
+        "day_loop": day_loop,
         "gpu_launches": args.steps,
         "clocks": clk.summary(), "nonfinite_runs": nonfinite[0], "bad_descriptors": nonfinite[1],
     }

@@ -225,3 +225,44 @@ def test_daily_form_matches_generated_hourly_records(cuda_lib):
     assert np.isfinite(a[0][:, :n]).all() and a[3][0] == 0
     _close_state(a[0][:, :n], b[0][:, :n], frac_min=0.9)
     _close_acc(a[1][:L.N_ACC, :n] - a[1][L.N_ACC:, :n], b[1][:L.N_ACC, :n] - b[1][L.N_ACC:, :n], frac_min=0.85)
+
+
+@pytest.mark.gpu
+def test_ensemble_day_loop_matches_day_loop_on_columns(cuda_lib):
+    """Calibration runs with the daily cadence (EnsembleDayLoop: per-run static
+    and daily-cadence planes, one persistent launch per day between the day
+    kernels) against DayLoop on the same sites as columns, the default vector,
+    three days: the same forcing and day kernels, the step's last bits apart
+    (ensemble vs column kernel), so the states agree to the ensemble-vs-column
+    tolerances and the daily-cadence state to 1e-3 relative on 90 % of the runs;
+    a second vector gives finite, different runs."""
+    from ibis_b200.daily import DayLoop
+    from ibis_b200.ensemble_daily import EnsembleDayLoop
+    from ibis_b200.forcing import daily_planes
+    from ibis_b200.params import DayParams
+    rng = np.random.Generator(np.random.PCG64(21))
+    nsite, nday = 12, 3
+    lat = rng.uniform(-40.0, 70.0, nsite)
+    stat = synth.make_columns(rng, nsite, 1.0)
+    F0 = {k: v[0] for k, v in synth.make_forcing(rng, lat, 1, start_doy=150).items()}
+    prog = synth.make_initial(rng, stat, F0)
+    dayst = synth.make_dayst(rng, stat, lat)
+    daily = synth.make_daily_weather(rng, lat, nday)
+    P = StepParams(co2conc=390.0e-6)
+    vecs = np.stack([E.default_vector(P), E.draw_vectors(rng, 1, P)[0]])
+    edl = EnsembleDayLoop(stat, prog, dayst, daily, lat, vecs, P, seed=5, jday=150).run()
+    cols = Columns.from_host(prog, stat, dtype=torch.float32, acc=True)
+    loop = DayLoop(cols, P, DayParams(), dayst, lat=lat, seed=5, jday=150)
+    loop.run(torch.from_numpy(daily_planes(daily, cols.ld)).cuda())
+    torch.cuda.synchronize()
+    assert edl.day == nday and not edl.nonfinite()[0] and not edl.nonfinite()[1]
+    runs0 = np.arange(nsite) * 2                                  # the default vector's runs
+    x = edl.prog.cpu().numpy()[:, runs0]
+    y = cols.prog.cpu().numpy()[:, :nsite]
+    _close_state(x, y, frac_min=0.9)
+    a, b = edl.dayst_host(), loop.dayst_host()
+    for k in ("tempu", "templ", "agddu", "agddl", "a10td", "clitls", "clitrs", "csoislop", "csoipas", "totcmic"):
+        e = np.abs(a[k][runs0] - b[k]) / np.maximum(np.abs(b[k]), 1e-6)
+        assert np.mean(e <= 1e-3) >= 0.9, (k, float(e.max()))
+    p1 = edl.prog.cpu().numpy()[:, runs0 + 1]
+    assert np.isfinite(p1).all() and not np.array_equal(p1, x)
