@@ -253,10 +253,12 @@ def run_month_scan(state, consts, params, xs, nsoilcall: int, ndaypy: int, dtime
     its ``_run_month_scan`` (python-port/ibis/timestepping/loops_gswp3.py:346-612):
     ``xs`` = (td, tmax, tmin, cloud, precip, psurf, qd, ud, iwet, rlds, jdays[,
     sw_h, use_h]) as (ndays, npoi) arrays (sw_h (ndays, 24, npoi)).  Returns
-    ``(state, (daily_gpp, daily_aet, daily_rh))`` -- the reference also returns
-    its PRNG key, which has no counterpart here: the day's variates (event
-    timing, hourly wind) come from the counter-based generator keyed by
-    (``seed``, ``day0`` + day, cell) instead of ``jax.random``.
+    ``(state, daily)``: ``daily`` is the reference's per-day output -- GPP, AET
+    and Rh, then with ``ch4_hourly`` the CH4 day mean and with ``soil_means``
+    the day means of tsoi, wsoi, wisoi (ndays, npoi, 6) and tg.  The reference
+    also returns its PRNG key, which has no counterpart here: the day's
+    variates (event timing, hourly wind) come from the counter-based generator
+    keyed by (``seed``, ``day0`` + day, cell) instead of ``jax.random``.
 
     Supported as the reference's defaults run it: one soil-BGC call per day
     (``nsoilcall`` 1), two radiation bands, the seasonal formulations, stress
@@ -298,13 +300,20 @@ def run_month_scan(state, consts, params, xs, nsoilcall: int, ndaypy: int, dtime
              "ud": ud, "fira": rlds}
     d_daily = torch.from_numpy(_forcing.daily_planes(daily, cols.ld)).to(cols.device)
     ld = cols.ld
-    sums = torch.zeros((nday + 1, 3, ld), dtype=dtype, device=cols.device)
-    planes = (L.OFF["ACC"]["aygpptot"][0], L.OFF["DAYST"]["ayaet"][0], L.OFF["DAYST"]["ayco2mic"][0])
+    # running totals read at every day's end; the day's value is the difference
+    # (annual GPP, AET and Rh; with the options the CH4 day mean and the soil
+    # means, which the step sums across days here and per day in the reference)
+    acc_fields = ["aygpptot"] + (["ch4"] if P.flags & FLAG_CH4 else []) + \
+        (["tsoi_mean", "wsoi_mean", "wisoi_mean", "tg_mean"] if soil_means else [])
+    acc_planes = [p for f in acc_fields for p in range(L.OFF["ACC"][f][0], L.OFF["ACC"][f][0] + L.OFF["ACC"][f][1])]
+    day_planes = [L.OFF["DAYST"]["ayaet"][0], L.OFF["DAYST"]["ayco2mic"][0]]
+    sums = torch.zeros((nday + 1, len(acc_planes) + 2, ld), dtype=dtype, device=cols.device)
+    acc_idx = torch.tensor(acc_planes, device=cols.device)
+    day_idx = torch.tensor(day_planes, device=cols.device)
 
     def snap(i):
-        sums[i, 0] = cols.acc[planes[0]] - cols.acc[L.N_ACC + planes[0]]
-        sums[i, 1] = loop.dayst[planes[1]]
-        sums[i, 2] = loop.dayst[planes[2]]
+        sums[i, :len(acc_planes)] = cols.acc[acc_idx] - cols.acc[acc_idx + L.N_ACC]
+        sums[i, len(acc_planes):] = loop.dayst[day_idx]
 
     snap(0)
     for d in range(nday):
@@ -318,8 +327,15 @@ def run_month_scan(state, consts, params, xs, nsoilcall: int, ndaypy: int, dtime
         loop.run_day(d_daily[d], **kw)
         snap(d + 1)
     torch.cuda.synchronize(cols.device)
-    s = sums.cpu().numpy().astype(np.float64)[:, :, :ncell]
-    diag = tuple(np.diff(s[:, j], axis=0) for j in range(3))
+    s = np.diff(sums.cpu().numpy().astype(np.float64)[:, :, :ncell], axis=0)      # (nday, planes, ncell)
+    na = len(acc_planes)
+    diag = (s[:, 0], s[:, na], s[:, na + 1])
+    j = 1
+    for f in acc_fields[1:]:
+        k = L.OFF["ACC"][f][1]
+        v = s[:, j:j + k]
+        diag += (v[:, 0] if k == 1 else np.transpose(v, (0, 2, 1)),)
+        j += k
     from . import synth
     st = synth.from_planes("STAT", cols.stat.cpu().numpy(), ncell)
     stat_now = {k: st[k] for k in DayLoop._STAT_WRITTEN}

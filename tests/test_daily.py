@@ -9,6 +9,7 @@ sums, soil carbon), float64 throughout; 1e-6 for the accumulators the
 reference sums in float32 steps.
 """
 import os
+import types
 import warnings
 
 import numpy as np
@@ -416,7 +417,6 @@ def test_day_param_paths_against_reference_objects():
 
 def _param_tree(z, lat_deg):
     """consts/params attribute trees with the reference's paths, from the fixture's records."""
-    import types
     from ibis_b200 import dropin
 
     def put(root, path, v):
@@ -465,6 +465,13 @@ def test_run_month_scan_dropin_equals_day_loop(cuda_lib):
                                                                    int(z["in.jday0"]) + np.arange(nd))
     seed = int(z["in.seed"])
     new, (gpp, aet, rh) = dropin.run_month_scan(state, consts, params, xs, 1, 365, 3600.0, seed=seed)
+    # with the hourly CH4 and the soil means the day outputs gain them, per day
+    _, extra = dropin.run_month_scan(state, consts, params, xs, 1, 365, 3600.0, seed=seed, ch4_hourly=True,
+                                     ch4_args=(np.full(n, 0.3), types.SimpleNamespace(), None), soil_means=True)
+    assert len(extra) == 8 and extra[3].shape == (nd, n) and extra[4].shape == (nd, n, 6)
+    assert extra[7].shape == (nd, n) and np.all(extra[3] >= 0) and np.any(extra[3] > 0)
+    np.testing.assert_allclose(extra[7], np.broadcast_to(extra[7].mean(axis=0), extra[7].shape), rtol=0.05)
+    assert np.all((extra[7] > 200.0) & (extra[7] < 340.0))           # day-mean ground temperature, K
     # the same days through DayLoop directly
     P = dropin.step_params(state, consts, params, 3600.0, 365)
     loop = DayLoop.from_restart(CKPT, dtype=torch.float32, params=P, day_params=dropin.day_params(params),
