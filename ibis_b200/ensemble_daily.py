@@ -29,7 +29,7 @@ import torch
 from . import layout as L
 from . import lib as _lib
 from . import synth
-from .forcing import hourly_forcing
+from .forcing import daily_planes, hourly_forcing
 from .lib import IbisEnsembleC
 from .params import FLAG_ACC, DayParams, StepParams
 
@@ -85,7 +85,8 @@ class EnsembleDayLoop:
         self.day_params = day_params or DayParams()
         self._pc = self.params.to_c()
         self._dpc = self.day_params.to_c()
-        self.daily = torch.from_numpy(synth_daily_planes(daily, self.ld_site)).to(dev)
+        self.daily = torch.from_numpy(daily_planes(daily, self.ld_site)).to(dev)
+        self.hourly = torch.empty((24, L.N_FORC, self.ld_site), **f32)
         lat_planes = np.zeros(self.ld_site, dtype=np.float32)
         lat_planes[:self.nsite] = lat
         self.lat = torch.from_numpy(lat_planes).to(dev)
@@ -112,9 +113,9 @@ class EnsembleDayLoop:
         stream = stream or torch.cuda.current_stream(self.device)
         s = ctypes.c_void_p(stream.cuda_stream)
         with torch.cuda.stream(stream):
-            hourly = hourly_forcing(self.daily[d:d + 1], self.lat, self.nsite, jday0=self.jday, day0=d,
-                                    seed=self.seed, observed_fira=True, stream=stream)      # (24, N_FORC, ld_site)
-            self.records.view(self.nsite, 24, L.N_FORC).copy_(hourly[:, :, :self.nsite].permute(2, 0, 1))
+            hourly_forcing(self.daily[d:d + 1], self.lat, self.nsite, jday0=self.jday, day0=d, seed=self.seed,
+                           observed_fira=True, out=self.hourly, stream=stream)           # (24, N_FORC, ld_site)
+            self.records.view(self.nsite, 24, L.N_FORC).copy_(self.hourly[:, :, :self.nsite].permute(2, 0, 1))
             self.td[:self.nrun] = self.daily[d, _TD][self.site_index]
         n, ld = self.nrun, self.ld_run
         _lib.check(self.lib.ibis_day_begin_f32(_p(self.stat), _p(self.dayst), _p(self.acc), _p(self.td), n, ld,
@@ -153,8 +154,3 @@ class EnsembleDayLoop:
     def cell_steps(self) -> int:
         return self.nrun * 24 * self.day
 
-
-def synth_daily_planes(daily: dict, ld: int) -> np.ndarray:
-    """(nday, N_DAILY, ld) float32 planes of the sites' daily weather."""
-    from .forcing import daily_planes
-    return daily_planes(daily, ld)
