@@ -534,6 +534,15 @@ def run_serve(args):
     reqs = S.poisson_requests(np.random.default_rng(5), args.rate, args.duration, args.sites)
     with ClockSampler(local) as clk:
         st = srv.serve(reqs)
+    # the plain per-request form on the first 0.3 s of a Poisson stream, beside
+    # the continuous-batching server on the same requests
+    few = S.poisson_requests(np.random.default_rng(7), args.rate, 0.3, args.sites)
+    st_few = srv.serve(few)
+    pl = S.serve_plain(lib, few)
+    plain = {"requests": pl["requests"], "p50_s": pl["p50_s"], "p99_s": pl["p99_s"],
+             "batched_p50_s": st_few["p50_s"], "batched_p99_s": st_few["p99_s"],
+             "note": "the first 0.3 s of a Poisson stream: one persistent launch per request, one request at a "
+                     "time (plain) vs the continuous-batching server"}
     # the same requests over a library of day records (hours generated in the kernel)
     t0 = time.time()
     lib_d = S.SiteLibrary(args.sites, 10, seed=3, daily=True)
@@ -555,7 +564,9 @@ def run_serve(args):
                    "slots": st["slots"], "budget_gb": 150, "library_gb": lib.nbytes / 1e9,
                    "library_generation_s": gen_s},
         "epochs": st["epochs"], "gpu_launches": st["epochs"], "clocks": clk.summary(), "status": st["status"],
-        "daily_library": daily_library,
+        "daily_library": daily_library, "plain_per_request": plain,
+        "queue_depth": {"max": st["queue_depth_max"], "mean": st["queue_depth_mean"]},
+        "hbm_gb": st["hbm_gb"],
     }
     print(json.dumps(line), flush=True)
 

@@ -277,6 +277,7 @@ class Server:
         clock = (lambda: time.perf_counter() - t0) if realtime else (lambda: vclock)
         i, epochs, cell_steps, buf = 0, 0, 0, 0
         busy = 0.0
+        depths = []
         while i < len(requests) or pending or self._active or self._gathering:
             now = clock()
             while i < len(requests) and requests[i].arrival <= now:
@@ -297,6 +298,7 @@ class Server:
             while len(inflight) >= self.lookahead:
                 inflight.popleft().synchronize()
             n = np.minimum(self.epoch_hours, self.slot_len[occ] - self.slot_pos[occ])
+            depths.append(len(pending))
             self._launch(buf, occ, n)
             ev = torch.cuda.Event()
             ev.record(self.stream)
@@ -325,7 +327,17 @@ class Server:
                 "p99_s": float(np.percentile(lat, 99)) if lat.size else None,
                 "mean_s": float(lat.mean()) if lat.size else None,
                 "slots": self.nslot, "epoch_hours": self.epoch_hours,
+                "queue_depth_max": int(max(depths, default=0)),
+                "queue_depth_mean": float(np.mean(depths)) if depths else 0.0,
+                "hbm_gb": self.nbytes / 1e9,
                 "status": self.status.cpu().numpy().tolist()}
+
+    @property
+    def nbytes(self) -> int:
+        """Device bytes of the site library and the run slots."""
+        ts = [self.prog, self.acc, self.run_params, self.yearly, self.run_site]
+        ts += [t for d, _ in self._desc for t in d.values()]
+        return self.lib.nbytes + sum(t.numel() * t.element_size() for t in ts)
 
 
 def poisson_requests(rng, rate: float, duration: float, nsite_lib: int, max_sites: int = 64, max_years: int = 10,
@@ -345,3 +357,59 @@ def poisson_requests(rng, rate: float, duration: float, nsite_lib: int, max_site
         out.append(Request(rid=rid, sites=np.sort(sites), years=years, vector=vec, arrival=t))
         rid += 1
     return out
+
+
+def serve_plain(library: SiteLibrary, requests, block: int = 0) -> dict:
+    """The plain form of the request loop, for comparison: requests answered one
+    at a time in arrival order, each as its own persistent ensemble launch over
+    its runs' whole records (buffers allocated per request, no batching with
+    other requests).  Latency from arrival to the GPU-clock end of its launch."""
+    if library.daily:
+        raise ValueError("the plain form reads hourly records")
+    dev = library.device
+    so = _lib.load()
+    pc = library.params.to_c()
+    requests = sorted(requests, key=lambda r: r.arrival)
+    stream = torch.cuda.Stream(dev)
+    t0_ev = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    t0_ev.record(stream)
+    t0 = time.perf_counter()
+    lat = []
+    cell_steps = 0
+    for r in requests:
+        wait = r.arrival - (time.perf_counter() - t0)
+        if wait > 0:
+            time.sleep(wait)
+        nrun, ld = len(r.sites), L.leading_dim(len(r.sites))
+        sites = torch.from_numpy(np.asarray(r.sites, dtype=np.int64)).to(dev)
+        f32 = dict(dtype=torch.float32, device=dev)
+        with torch.cuda.stream(stream):
+            prog = torch.zeros((L.N_PROG, ld), **f32)
+            prog[:, :nrun] = library.prog[:, sites]
+            acc = torch.zeros((2 * L.N_ACC, ld), **f32)
+            rp = torch.zeros((L.N_RUN, ld), **f32)
+            rp[:, :nrun] = torch.from_numpy(np.asarray(r.vector, dtype=np.float32)).to(dev)[:, None]
+            yearly = torch.zeros((r.years, L.N_YEARLY, ld), **f32)
+            run_site = sites.to(torch.int32)
+            run_forc = torch.from_numpy(library.first[np.asarray(r.sites)]).to(dev)
+            run_nstep = torch.full((nrun,), r.years * library.year_hours, dtype=torch.int32, device=dev)
+            queue = torch.zeros(1, dtype=torch.int32, device=dev)
+            status = torch.tensor([0, INT_MAX], dtype=torch.int32, device=dev)
+        e = IbisEnsembleC(prog=prog.data_ptr(), acc=acc.data_ptr(), stat=library.stat.data_ptr(),
+                          forc=library.forc.data_ptr(), run_params=rp.data_ptr(), run_site=run_site.data_ptr(),
+                          run_forc=run_forc.data_ptr(), run_nstep=run_nstep.data_ptr(), run_pos=None, order=None,
+                          yearly=yearly.data_ptr(), forc_len=int(library.forc.shape[0]), nrun=nrun, ld_run=ld,
+                          nsite=library.nsite, ld_site=library.ld_site, nyear=r.years,
+                          year_steps=library.year_hours, norder=nrun, queue=queue.data_ptr(),
+                          status=status.data_ptr())
+        _lib.check(so.ibis_ensemble_f32(ctypes.byref(e), ctypes.byref(pc), int(block),
+                                        ctypes.c_void_p(stream.cuda_stream)), "ibis_ensemble_f32")
+        done = torch.cuda.Event(enable_timing=True)
+        done.record(stream)
+        done.synchronize()
+        lat.append(t0_ev.elapsed_time(done) / 1e3 - r.arrival)
+        cell_steps += nrun * r.years * library.year_hours
+    lat = np.asarray(lat)
+    return {"requests": len(lat), "p50_s": float(np.percentile(lat, 50)) if lat.size else None,
+            "p99_s": float(np.percentile(lat, 99)) if lat.size else None, "cell_steps": cell_steps}
