@@ -149,7 +149,7 @@ def test_daily_library_request_alone_equals_in_mix_and_ensemble(cuda_lib):
 @pytest.mark.gpu
 def test_plain_per_request_form_runs(cuda_lib):
     """serve_plain (one launch per request, one at a time) answers every request
-    with a finite latency no shorter than the batched server's on the same ones."""
+    with a finite latency and runs every hour of every run."""
     lib = _library()
     reqs = _requests(np.random.default_rng(11), 4)
     pl = S.serve_plain(lib, reqs)
