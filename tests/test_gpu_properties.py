@@ -5,7 +5,8 @@ python-port/tests/test_water_balance.py:34-49): the change of soil water plus
 puddle equals (rain reaching the soil - soil evaporation - transpiration -
 runoff - drainage) x dt within 2 % of the fluxes + 0.05 kg m-2, for a moist, a
 near-saturated and a saturated column under rain.  And a day of the workload
-stays finite and inside physical bounds.
+stays finite and inside physical bounds, as does a year of the day loop (daily
+cadence and monthly methane) on 4,096 cells.
 """
 import numpy as np
 import pytest
