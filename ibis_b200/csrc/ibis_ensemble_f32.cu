@@ -28,7 +28,7 @@ namespace {
 
 constexpr unsigned kEnsFlags = IBIS_FLAG_BEDROCK | IBIS_FLAG_H2O_CONSISTENT | IBIS_FLAG_SUNSHADE_U |
                                IBIS_FLAG_SUNSHADE_L | IBIS_FLAG_ACC | IBIS_FLAG_CH4 | IBIS_FLAG_SOIL_MEANS |
-                               IBIS_FLAG_KAHAN | IBIS_FLAG_ZWT_OBS;
+                               IBIS_FLAG_KAHAN | IBIS_FLAG_ZWT_OBS | IBIS_FLAG_ETPARTS | IBIS_FLAG_NEEPARTS;
 
 // Validate an ensemble description; fills `a`.  Returns 0, or -EINVAL.
 int ens_args(const IbisEnsemble* e, const IbisParams* hp, EnsArgs& a) {

@@ -119,30 +119,37 @@ __device__ __forceinline__ Forc<R> load_forc(const R* __restrict__ f, int ld) {
 }
 
 // Accumulators of the fused kernel kept in shared memory for the launch: plane p
-// of thread t at sacc[p * BLOCK + t] (consecutive threads, consecutive banks),
-// value planes then compensation planes as in the global buffer.  Only the
-// planes the flags write move: loaded before the first hour, stored after the
-// last, so the hourly read-modify-writes stay on chip.
+// of thread t at sacc[p * BLOCK + t] (consecutive threads, consecutive banks)
+// for the kAccOnChip planes every day loop keeps, then their compensation
+// planes; the optional planes from kAccOnChip on stay in global memory.  Only
+// the planes the flags write move: loaded before the first hour, stored after
+// the last, so the hourly read-modify-writes stay on chip.
 __device__ __forceinline__ bool acc_plane_used(int p, unsigned flags) {
     const int q = p < IBIS_ACC_COUNT ? p : p - IBIS_ACC_COUNT;
-    if (p >= IBIS_ACC_COUNT && (!(flags & IBIS_FLAG_KAHAN) || q >= IBIS_ACC_STRESSTU_LAST)) return false;
+    const bool last_value = q == IBIS_ACC_STRESSTU_LAST || q == IBIS_ACC_STRESSTL_LAST;    // no Kahan terms
+    if (p >= IBIS_ACC_COUNT && (!(flags & IBIS_FLAG_KAHAN) || last_value)) return false;
     if (q == IBIS_ACC_CH4) return (flags & IBIS_FLAG_CH4) != 0;
     if (q >= IBIS_ACC_TSOI_MEAN && q < IBIS_ACC_AFSENA) return (flags & IBIS_FLAG_SOIL_MEANS) != 0;
+    if (q >= IBIS_ACC_ET_TRANS && q <= IBIS_ACC_ET_SNOWSUB)
+        return (flags & IBIS_FLAG_ACC) && (flags & IBIS_FLAG_ETPARTS);
+    if (q == IBIS_ACC_NEE_NIGHT || q == IBIS_ACC_NEE_DAY)
+        return (flags & IBIS_FLAG_ACC) && (flags & IBIS_FLAG_NEEPARTS);
     return (flags & IBIS_FLAG_ACC) != 0;
 }
 
 template <typename R, bool TO_SMEM>
 __device__ __forceinline__ void acc_move(R* __restrict__ g, int ld, R* __restrict__ sacc, int sld, unsigned flags) {
 #pragma unroll 1
-    for (int p = 0; p < 2 * IBIS_ACC_COUNT; ++p) {
-        if (!acc_plane_used(p, flags)) continue;
-        if (TO_SMEM) sacc[p * sld] = g[(size_t)p * ld];
-        else g[(size_t)p * ld] = sacc[p * sld];
+    for (int p = 0; p < 2 * kAccOnChip; ++p) {
+        const int gp = p < kAccOnChip ? p : p - kAccOnChip + IBIS_ACC_COUNT;     // the plane in the global buffer
+        if (!acc_plane_used(gp, flags)) continue;
+        if (TO_SMEM) sacc[p * sld] = g[(size_t)gp * ld];
+        else g[(size_t)gp * ld] = sacc[p * sld];
     }
 }
 
 // Whether a fused configuration keeps its accumulators in shared memory: the
-// column state plus all accumulator planes of MINB resident blocks must fit
+// column state plus the on-chip accumulator planes of MINB resident blocks must fit
 // the SM's 228 KB (1 KB reserved per block).  Launches of fewer than
 // kAccSmemMinSteps hours keep them in global memory instead (ACCSM = false):
 // the on-chip copy only pays back over several hours, and the larger
@@ -151,7 +158,7 @@ template <typename R, int BLOCK, int MINB, bool ACCSM = true>
 struct AccInSmem {
     static constexpr bool value =
         ACCSM && StateInSmem<R>::value &&
-        ((sizeof(Col<R>) + 2 * IBIS_ACC_COUNT * sizeof(R)) * BLOCK + 1024) * MINB <= 228 * 1024;
+        ((sizeof(Col<R>) + 2 * kAccOnChip * sizeof(R)) * BLOCK + 1024) * MINB <= 228 * 1024;
 };
 constexpr int kAccSmemMinSteps = 4;
 
@@ -178,7 +185,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) hourly_step_kernel(R* __restrict_
     // with the accumulators on chip the view always points at shared memory
     // (acc == nullptr comes with no accumulator flags, so nothing is added)
     R* const sacc = kAccSmem ? reinterpret_cast<R*>(smem_raw + BLOCK * sizeof(Col<R>)) + threadIdx.x : nullptr;
-    Acc<R> A{kAccSmem ? sacc : (acc ? acc + i : nullptr), kAccSmem ? BLOCK : ld, (P.flags & IBIS_FLAG_KAHAN) != 0};
+    const bool kahan = (P.flags & IBIS_FLAG_KAHAN) != 0;
+    using AccT = Acc<R, kAccSmem ? BLOCK : 0>;
+    AccT A = kAccSmem ? AccT{sacc, ld, kahan, true, acc ? acc + i : nullptr} : AccT{acc ? acc + i : nullptr, ld, kahan};
     if (kAccSmem && acc) acc_move<R, true>(acc + i, ld, sacc, BLOCK, P.flags);
 #pragma unroll 1
     for (int s = 0; s < nstep; ++s) {
@@ -359,7 +368,7 @@ cudaError_t launch_fused(R* prog, const R* stat, const R* forc, R* diag, R* acc,
                          long long fstride, const DevParams<R>& P, int* status, cudaStream_t s) {
     const int grid = (ncell + BLOCK - 1) / BLOCK;
     const size_t col_smem = StateInSmem<R>::value ? BLOCK * sizeof(Col<R>) : 0;
-    const size_t acc_smem = AccInSmem<R, BLOCK, MINB, ACCSM>::value ? BLOCK * 2 * IBIS_ACC_COUNT * sizeof(R) : 0;
+    const size_t acc_smem = AccInSmem<R, BLOCK, MINB, ACCSM>::value ? BLOCK * 2 * kAccOnChip * sizeof(R) : 0;
     const size_t smem = col_smem + acc_smem;
     auto k = hourly_step_kernel<R, NT, SU, SL, BLOCK, MINB, ACCSM>;
     static unsigned long long fitted = 0;
@@ -460,7 +469,7 @@ static int hourly_step(R* prog, const R* stat, const R* forc, R* diag, R* acc, i
     if (ncell == 0 || nstep == 0) return 0;
     const unsigned known = IBIS_FLAG_BEDROCK | IBIS_FLAG_H2O_CONSISTENT | IBIS_FLAG_SUNSHADE_U | IBIS_FLAG_SUNSHADE_L |
                            IBIS_FLAG_ACC | IBIS_FLAG_CH4 | IBIS_FLAG_SOIL_MEANS | IBIS_FLAG_DIAG | IBIS_FLAG_KAHAN |
-                           IBIS_FLAG_ZWT_OBS;
+                           IBIS_FLAG_ZWT_OBS | IBIS_FLAG_ETPARTS | IBIS_FLAG_NEEPARTS;
     if (hp->flags & ~known) return -EINVAL;
     if ((hp->flags & (IBIS_FLAG_ACC | IBIS_FLAG_CH4 | IBIS_FLAG_SOIL_MEANS)) && !acc) return -EINVAL;
     if ((hp->flags & IBIS_FLAG_DIAG) && !diag) return -EINVAL;

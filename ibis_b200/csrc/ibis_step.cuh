@@ -6,27 +6,58 @@
 
 namespace ibis {
 
-// Accumulator view of one cell: value planes then compensation planes.
-template <typename R>
+// Planes below kAccOnChip are the accumulators every day loop keeps; the
+// planes from kAccOnChip on (the optional ET and NEE components) are summed
+// only under their own flags.  A kernel that holds the accumulators on chip
+// holds the first kind and leaves the second in the global buffer.
+constexpr int kAccOnChip = IBIS_ACC_ET_TRANS;
+static_assert(IBIS_ACC_NEE_DAY + 1 == IBIS_ACC_COUNT && IBIS_ACC_STRESSTL_LAST < kAccOnChip,
+              "the optional accumulator planes close the accumulator block");
+
+// Accumulator view of one cell: value planes then compensation planes.  In
+// the global form (SLD = 0) ``base`` addresses every plane with leading
+// dimension ``ld`` and the compensation term of plane p is plane
+// p + IBIS_ACC_COUNT.  In the on-chip form (SLD = the block size) ``base``
+// holds planes [0, kAccOnChip) with stride SLD and their compensation terms at
+// p + kAccOnChip; the optional planes stay in the global buffer ``far``
+// (leading dimension ``ld``).
+template <typename R, int SLD = 0>
 struct Acc {
     R* __restrict__ base;  // nullptr: no accumulators
     int ld;
     bool kahan;
     bool last = true;      // the launch's last hour for this cell: keep the end-of-hour values
-    __device__ __forceinline__ void add(int plane, R x) const {
-        R* v = base + (size_t)plane * ld;
-        if (kahan) {
-            R* cmp = base + (size_t)(plane + IBIS_ACC_COUNT) * ld;
-            R s = *v, cc = *cmp;
-            R y = x - cc;
-            R t = s + y;
-            *cmp = (t - s) - y;
-            *v = t;
+    R* __restrict__ far = nullptr;
+    __device__ __forceinline__ R& at(int plane) const {
+        if constexpr (SLD > 0) {
+            if (plane >= kAccOnChip) return far[(size_t)plane * ld];
+            return base[plane * SLD];
         } else {
-            *v = *v + x;
+            return base[(size_t)plane * ld];
         }
     }
-    __device__ __forceinline__ R get(int plane) const { return base[(size_t)plane * ld]; }
+    __device__ __forceinline__ R& comp(int plane) const {
+        if constexpr (SLD > 0) {
+            if (plane >= kAccOnChip) return far[(size_t)(plane + IBIS_ACC_COUNT) * ld];
+            return base[(plane + kAccOnChip) * SLD];
+        } else {
+            return base[(size_t)(plane + IBIS_ACC_COUNT) * ld];
+        }
+    }
+    __device__ __forceinline__ void add(int plane, R x) const {
+        R& v = at(plane);
+        if (kahan) {
+            R& cmp = comp(plane);
+            R s = v, cc = cmp;
+            R y = x - cc;
+            R t = s + y;
+            cmp = (t - s) - y;
+            v = t;
+        } else {
+            v = v + x;
+        }
+    }
+    __device__ __forceinline__ R get(int plane) const { return at(plane); }
 };
 
 // Values the surface phase (steps 1-9 of timestep_body) hands to the ground
@@ -308,9 +339,9 @@ __device__ __forceinline__ void surface_phase(Col<R>& c, const Forc<R>& F, const
 // Steps 10-12 of timestep_body -- snow, soil water and heat (+ bedrock),
 // freeze/thaw, the surface-temperature bound -- then the fire counters and the
 // day-loop accumulators (loops.py:676-1275; loops_gswp3.py:161-318).
-template <typename R, int NT, typename Q>
+template <typename R, int NT, typename Q, int SLD>
 __device__ __forceinline__ void ground_phase(Col<R>& c, const Forc<R>& F, const Stat<R>& S, const Diag<R>& D,
-                                             const Acc<R>& Ac, const DevParams<R>& P, const Q& q, const Mid<R>& M) {
+                                             const Acc<R, SLD>& Ac, const DevParams<R>& P, const Q& q, const Mid<R>& M) {
     const R eps = P.epsilon, dt = P.dtime;
     const R fi = c.fi;
     const R lai0 = S(IBIS_STAT_LAI, 0), lai1 = S(IBIS_STAT_LAI, 1);
@@ -583,7 +614,7 @@ __device__ __forceinline__ void ground_phase(Col<R>& c, const Forc<R>& F, const 
                 } else {
                     R old_ = Ac.get(IBIS_ACC_AYNPP + j);
                     R nw = old_ + inc;
-                    Ac.base[(size_t)(IBIS_ACC_AYNPP + j) * Ac.ld] = nw;
+                    Ac.at(IBIS_ACC_AYNPP + j) = nw;
                     npp = npp + (nw - old_);
                 }
             }
@@ -605,9 +636,26 @@ __device__ __forceinline__ void ground_phase(Col<R>& c, const Forc<R>& F, const 
             Ac.add(IBIS_ACC_AYTRUNOF, grunof * dt);
             Ac.add(IBIS_ACC_AYTDRAIN, wflo[NL] * dt);
             Ac.add(IBIS_ACC_AFSENA, M.fsena * dt);
+            // the optional ET components (loops_gswp3.py:263-272): the fluxes
+            // summed into adaet, kept apart, sublimation from the snow cover
+            // taken out of soil evaporation
+            if (P.flags & IBIS_FLAG_ETPARTS) {
+                const R snowsub = M.fvapi * c.fi * dt;
+                Ac.add(IBIS_ACC_ET_TRANS, M.gtrans * dt);
+                Ac.add(IBIS_ACC_ET_INTERC, M.ginvap * dt);
+                Ac.add(IBIS_ACC_ET_SOILEV, M.gsuvap * dt - snowsub);
+                Ac.add(IBIS_ACC_ET_SNOWSUB, snowsub);
+            }
+            // the optional day/night NEE (loops_gswp3.py:274-281): the day's Rh
+            // rate spread evenly over the steps less this step's NPP, booked to
+            // the night when the sun is below the horizon
+            if (P.flags & IBIS_FLAG_NEEPARTS) {
+                const R nee = S(IBIS_STAT_TCO2MIC) * cf - npp;
+                Ac.add(F.cosz <= R(0.0) ? IBIS_ACC_NEE_NIGHT : IBIS_ACC_NEE_DAY, nee);
+            }
             if (Ac.last) {
-                Ac.base[(size_t)IBIS_ACC_STRESSTU_LAST * Ac.ld] = stresstu;
-                Ac.base[(size_t)IBIS_ACC_STRESSTL_LAST * Ac.ld] = stresstl;
+                Ac.at(IBIS_ACC_STRESSTU_LAST) = stresstu;
+                Ac.at(IBIS_ACC_STRESSTL_LAST) = stresstl;
             }
         }
         if (P.flags & IBIS_FLAG_CH4) {
@@ -629,9 +677,9 @@ __device__ __forceinline__ void ground_phase(Col<R>& c, const Forc<R>& F, const 
 }
 
 // One full hourly step of a column in one kernel.
-template <typename R, int NT, bool SUN_U, bool SUN_L, typename Q>
+template <typename R, int NT, bool SUN_U, bool SUN_L, typename Q, int SLD>
 __device__ __forceinline__ void column_step(Col<R>& c, const Forc<R>& F, const Stat<R>& S, const Diag<R>& D,
-                                            const Acc<R>& Ac, const DevParams<R>& P, const Q& q) {
+                                            const Acc<R, SLD>& Ac, const DevParams<R>& P, const Q& q) {
     Mid<R> M;
     surface_phase<R, SUN_U, SUN_L>(c, F, S, D, P, q, M);
     ground_phase<R, NT>(c, F, S, D, Ac, P, q, M);

@@ -227,6 +227,14 @@ ACC = (
     # the next day's phenology reads (loops_gswp3.py:441-442)
     Field("stresstu_last", "soil.stresstu"),
     Field("stresstl_last", "soil.stresstl"),
+    # the optional ET and NEE components of the step's sums (state/et_parts.py,
+    # state/nee_parts.py; loops_gswp3.py:263-281): under FLAG_ETPARTS / FLAG_NEEPARTS
+    Field("et_trans", "etparts.trans"),
+    Field("et_interc", "etparts.interc"),
+    Field("et_soilev", "etparts.soilev"),
+    Field("et_snowsub", "etparts.snowsub"),
+    Field("nee_night", "neeparts.night"),
+    Field("nee_day", "neeparts.day"),
 )
 
 # Per-run calibration vector of the ensemble kernels: the step-relevant

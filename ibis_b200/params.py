@@ -95,9 +95,11 @@ FLAG_SOIL_MEANS = 1 << 6       # per-step day means of tsoi/wsoi/wisoi/tg (loops
 FLAG_DIAG = 1 << 7             # write the DIAG buffer
 FLAG_KAHAN = 1 << 8            # compensated accumulation (FP32 kernels)
 FLAG_ZWT_OBS = 1 << 9          # observed wetland water table (STAT zwt_obs, NaN = the model's; methane.py:366-367)
+FLAG_ETPARTS = 1 << 10         # ET components accumulated apart, with FLAG_ACC (loops_gswp3.py:263-272)
+FLAG_NEEPARTS = 1 << 11        # day- and night-time NEE accumulated apart, with FLAG_ACC (loops_gswp3.py:274-281)
 
 KNOWN_FLAGS = (FLAG_BEDROCK | FLAG_H2O_CONSISTENT | FLAG_SUNSHADE_U | FLAG_SUNSHADE_L | FLAG_ACC
-               | FLAG_CH4 | FLAG_SOIL_MEANS | FLAG_DIAG | FLAG_KAHAN | FLAG_ZWT_OBS)
+               | FLAG_CH4 | FLAG_SOIL_MEANS | FLAG_DIAG | FLAG_KAHAN | FLAG_ZWT_OBS | FLAG_ETPARTS | FLAG_NEEPARTS)
 
 # Default root profile (lower, upper) used by the synthetic columns; the reference keeps froot as a
 # state leaf vegetation.froot of shape (nsoilay, 2) shared by every cell.
@@ -259,7 +261,8 @@ def header_struct_text() -> str:
     for nm, val in [("BEDROCK", FLAG_BEDROCK), ("H2O_CONSISTENT", FLAG_H2O_CONSISTENT),
                     ("SUNSHADE_U", FLAG_SUNSHADE_U), ("SUNSHADE_L", FLAG_SUNSHADE_L),
                     ("ACC", FLAG_ACC), ("CH4", FLAG_CH4), ("SOIL_MEANS", FLAG_SOIL_MEANS),
-                    ("DIAG", FLAG_DIAG), ("KAHAN", FLAG_KAHAN), ("ZWT_OBS", FLAG_ZWT_OBS)]:
+                    ("DIAG", FLAG_DIAG), ("KAHAN", FLAG_KAHAN), ("ZWT_OBS", FLAG_ZWT_OBS),
+                    ("ETPARTS", FLAG_ETPARTS), ("NEEPARTS", FLAG_NEEPARTS)]:
         lines.append(f"#define IBIS_FLAG_{nm} {val}u")
     lines.append("")
     lines.append("/* Parameters of the daily cadence (phenology, soil biogeochemistry), all double. */")

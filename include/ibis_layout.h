@@ -198,7 +198,13 @@ enum {
     IBIS_ACC_AFSENA = 43,  /* acc.fsena */
     IBIS_ACC_STRESSTU_LAST = 44,  /* soil.stresstu */
     IBIS_ACC_STRESSTL_LAST = 45,  /* soil.stresstl */
-    IBIS_ACC_COUNT = 46
+    IBIS_ACC_ET_TRANS = 46,  /* etparts.trans */
+    IBIS_ACC_ET_INTERC = 47,  /* etparts.interc */
+    IBIS_ACC_ET_SOILEV = 48,  /* etparts.soilev */
+    IBIS_ACC_ET_SNOWSUB = 49,  /* etparts.snowsub */
+    IBIS_ACC_NEE_NIGHT = 50,  /* neeparts.night */
+    IBIS_ACC_NEE_DAY = 51,  /* neeparts.day */
+    IBIS_ACC_COUNT = 52
 };
 
 /* RUN */
@@ -532,6 +538,8 @@ typedef struct IbisParams {
 #define IBIS_FLAG_DIAG 128u
 #define IBIS_FLAG_KAHAN 256u
 #define IBIS_FLAG_ZWT_OBS 512u
+#define IBIS_FLAG_ETPARTS 1024u
+#define IBIS_FLAG_NEEPARTS 2048u
 
 /* Parameters of the daily cadence (phenology, soil biogeochemistry), all double. */
 typedef struct IbisDayParams {

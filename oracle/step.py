@@ -25,11 +25,14 @@ FLAG_ACC = 1 << 4
 FLAG_CH4 = 1 << 5
 FLAG_SOIL_MEANS = 1 << 6
 FLAG_ZWT_OBS = 1 << 9
+FLAG_ETPARTS = 1 << 10
+FLAG_NEEPARTS = 1 << 11
 
 ACC_FIELDS = {"adrain": 1, "adsnow": 1, "adaet": 1, "a10ancub": 1, "a10ancls": 1, "a10ancl3": 1,
               "a10ancl4": 1, "aynpp": 12, "aynpptot": 1, "aygpptot": 1, "aytrunof": 1, "aytdrain": 1,
               "ch4": 1, "tsoi_mean": 6, "wsoi_mean": 6, "wisoi_mean": 6, "tg_mean": 1, "afsena": 1,
-              "stresstu_last": 1, "stresstl_last": 1}
+              "stresstu_last": 1, "stresstl_last": 1, "et_trans": 1, "et_interc": 1, "et_soilev": 1,
+              "et_snowsub": 1, "nee_night": 1, "nee_day": 1}
 
 
 def new_acc(n):
@@ -338,6 +341,17 @@ def accumulate(acc, new, D, S, F, P):
     acc["afsena"] = acc["afsena"] + D["fsena"] * dt
     acc["stresstu_last"] = D["stresstu"].copy()
     acc["stresstl_last"] = D["stresstl"].copy()
+    if P.flags & FLAG_ETPARTS:                      # loops_gswp3.py:263-272
+        snowsub = D["fvapi"] * new["fi"] * dt
+        acc["et_trans"] = acc["et_trans"] + D["gtrans"] * dt
+        acc["et_interc"] = acc["et_interc"] + D["ginvap"] * dt
+        acc["et_soilev"] = acc["et_soilev"] + D["gsuvap"] * dt - snowsub
+        acc["et_snowsub"] = acc["et_snowsub"] + snowsub
+    if P.flags & FLAG_NEEPARTS:                     # loops_gswp3.py:274-281
+        nee = S["tco2mic"] * cf - npp
+        night = F["coszen"] <= 0.0
+        acc["nee_night"] = acc["nee_night"] + np.where(night, nee, 0.0)
+        acc["nee_day"] = acc["nee_day"] + np.where(night, 0.0, nee)
 
 
 def run_steps(prog, S, forcings, P, acc=None):

@@ -63,11 +63,12 @@ def _a(x):
     return jnp.asarray(np.asarray(x, dtype=np.float64))
 
 
-def reference_state(wl):
-    """IBISState (float64) holding the workload's prognostic and static fields."""
+def reference_state(wl, parts=False):
+    """IBISState (float64) holding the workload's prognostic and static fields
+    (with ``parts`` also the optional ET/NEE component modules)."""
     n = wl.ncell
     bed = bool(wl.params.flags & FLAG_BEDROCK)
-    st = create_ibis_state(GridConfig(nlon=2, nlat=1, npoi=n, nbedrock=3 if bed else 0))
+    st = create_ibis_state(GridConfig(nlon=2, nlat=1, npoi=n, nbedrock=3 if bed else 0), with_neeparts=parts)
     P, S = wl.prog, wl.stat
     hsoi = np.zeros(L.NSOILAY + 1)
     hsoi[:L.NSOILAY] = wl.params.hsoi
@@ -156,12 +157,13 @@ def run_steps(wl, record):
     return snaps
 
 
-def run_day_accumulators(wl):
-    """_run_day_inner over 24 hourly steps with CH4 and soil means on."""
+def run_day_accumulators(wl, parts=False):
+    """_run_day_inner over 24 hourly steps with CH4 and soil means on (and with
+    ``parts`` the ET/NEE component modules attached)."""
     assert wl.nhour == 24
     consts = get_constants()
     params = reference_params(wl)
-    st = reference_state(wl)
+    st = reference_state(wl, parts)
     F = wl.forc
 
     def fake_diurnal(time, jday, dw, lat, plens, startp, endp, key, dtime, nband=2):
@@ -193,7 +195,22 @@ def run_day_accumulators(wl):
     out["acc.wsoi_mean"] = np.asarray(acc[2], dtype=np.float64)
     out["acc.wisoi_mean"] = np.asarray(acc[3], dtype=np.float64)
     out["acc.tg_mean"] = np.asarray(acc[4], dtype=np.float64)
+    if parts:
+        for f in L.ACC:
+            if f.leaf.startswith(("etparts.", "neeparts.")):
+                out["acc." + f.name] = get(st_out, f.leaf)
     return out
+
+
+def write_parts_case():
+    """tests/golden/day_parts.npz: the day_mixed day of _run_day_inner again,
+    with the optional ET and NEE component modules attached
+    (state/et_parts.py, state/nee_parts.py; summed in loops_gswp3.py:263-281)."""
+    wl = build_case("day_mixed", CASES["day_mixed"])
+    out = {f"day.{k}": v for k, v in run_day_accumulators(wl, parts=True).items()}
+    path = os.path.join(HERE, "day_parts.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path}: {len(out)} arrays, {os.path.getsize(path)} bytes")
 
 
 def pack_inputs(wl):
@@ -577,7 +594,10 @@ def main():
         write_methane_case()
     if args.only in (None, "observed_sw"):
         write_observed_sw_case()
-    if args.only in ("restart_leaves", "restart_1996", "diurnal", "days", "methane_month", "observed_sw"):
+    if args.only in (None, "day_parts"):
+        write_parts_case()
+    if args.only in ("restart_leaves", "restart_1996", "diurnal", "days", "methane_month", "observed_sw",
+                     "day_parts"):
         return
     for name, spec in CASES.items():
         if args.only and name != args.only:

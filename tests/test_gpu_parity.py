@@ -181,3 +181,34 @@ def test_f32_day_accumulators_close_to_reference(cuda_lib):
     for k in ("tsoi_mean", "wsoi_mean", "tg_mean"):
         w = want[k]
         np.testing.assert_allclose(np.asarray(got[k]).reshape(w.shape), w, rtol=1e-4, atol=1e-5, err_msg=k)
+
+
+def test_et_and_nee_parts_match_reference(cuda_lib):
+    """The optional ET and NEE components summed by the step (FLAG_ETPARTS,
+    FLAG_NEEPARTS) against the reference's day with those modules attached:
+    float64 kernel within 1e-6 (as the other accumulators); the FP32 fused day
+    (on-chip accumulators) within 1e-3 of each plane's largest magnitude on 90 %
+    of the cells, its four ET parts summing to its AET."""
+    import os
+    from ibis_b200.params import FLAG_ETPARTS, FLAG_NEEPARTS
+    c = Case("day_mixed")
+    z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "day_parts.npz"))
+    parts = ("et_trans", "et_interc", "et_soilev", "et_snowsub", "nee_night", "nee_day")
+    want = {k: z["day.acc." + k] for k in parts}
+    for dtype in (torch.float64, torch.float32):
+        P = c.params.copy()
+        P.flags |= FLAG_ETPARTS | FLAG_NEEPARTS
+        if dtype == torch.float64:
+            P.flags &= ~(1 << 8)
+        cols = Columns.from_host(c.prog, c.stat, dtype=dtype, acc=True)
+        cols.run(cols.forcing(c.forc), P)
+        torch.cuda.synchronize()
+        got = cols.acc_host()
+        if dtype == torch.float64:
+            assert not compare({k: got[k] for k in parts}, want, 1e-6)
+            continue
+        for k in parts:
+            scale = max(float(np.abs(want[k]).max()), 1e-30)
+            assert np.mean(np.abs(got[k] - want[k]) <= 1e-3 * scale) >= 0.9, k
+        et = got["et_trans"] + got["et_interc"] + got["et_soilev"] + got["et_snowsub"]
+        np.testing.assert_allclose(et, got["adaet"], rtol=1e-5, atol=1e-5)

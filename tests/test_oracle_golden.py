@@ -51,3 +51,26 @@ def test_golden_cases_cover_the_edge_regimes():
     assert c.stat["fu"][0] == 0.0            # bare cell present
     assert np.any(c.prog["wisoi"] > 0.5)     # frozen cell present
     assert c.prog["wpud"][3] > 0.0           # flooded cell present
+
+
+def test_oracle_matches_reference_et_and_nee_parts():
+    """The optional ET and NEE components (loops_gswp3.py:263-281) against the
+    reference's day with those modules attached (tests/golden/day_parts.npz)."""
+    import os
+    from ibis_b200.params import FLAG_ETPARTS, FLAG_NEEPARTS
+    c = Case("day_mixed")
+    z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "day_parts.npz"))
+    want = {k[8:]: z[k] for k in z.files if k.startswith("day.acc.")}
+    P = c.params.copy()
+    P.flags |= FLAG_ETPARTS | FLAG_NEEPARTS
+    prog = {k: v.copy() for k, v in c.prog.items()}
+    acc = oracle.new_acc(c.ncell)
+    with np.errstate(all="ignore"):
+        for h in range(c.nhour):
+            prog, D, acc = oracle.step(prog, c.stat, c.forcing_at(h), P, acc)
+    parts = ("et_trans", "et_interc", "et_soilev", "et_snowsub", "nee_night", "nee_day")
+    assert not compare({k: acc[k] for k in parts}, {k: want[k] for k in parts}, 1e-9)
+    assert not compare(acc, {k: v for k, v in want.items() if k not in parts}, 1e-6)   # the rest unchanged
+    np.testing.assert_allclose(acc["et_trans"] + acc["et_interc"] + acc["et_soilev"] + acc["et_snowsub"],
+                               acc["adaet"], rtol=1e-12, atol=1e-12)
+    assert np.any(acc["nee_night"] != 0) and np.any(acc["nee_day"] != 0) and np.any(acc["et_snowsub"] != 0)

@@ -32,7 +32,7 @@ def test_poisson_requests_shape():
 
 
 def test_slot_bytes():
-    assert S.slot_bytes(10) == 4 * (71 + 92 + 31 + 70) + 28
+    assert S.slot_bytes(10) == 4 * (71 + 104 + 31 + 70) + 28
 
 
 # ---------------------------------------------------------------- GPU
