@@ -33,7 +33,7 @@ from . import restart as _restart
 from . import synth
 from .columns import Columns
 from .forcing import OBSERVED_FIRA, hourly_forcing
-from .params import FLAG_ACC, FLAG_CH4, DayParams, StepParams
+from .params import FLAG_ACC, FLAG_CH4, FLAG_ETPARTS, FLAG_NEEPARTS, DayParams, StepParams
 
 _TD = L.OFF["DAILY"]["td"][0]
 MONTH_NEW_YEAR, MONTH_FROM_MEAN, MONTH_PARTITION = 1, 2, 4
@@ -94,6 +94,11 @@ class DayLoop:
         # a10anc* leaves hold 10-day means between days (DAYST), not sums
         acc0 = _restart.group_from_leaves(leaves, "ACC", n)
         cols.set_acc({k: v for k, v in acc0.items() if not k.startswith("a10anc")})
+        # a checkpoint with the optional etparts / neeparts modules keeps summing them
+        if "et_trans" in acc0:
+            P.flags |= FLAG_ETPARTS
+        if "nee_night" in acc0:
+            P.flags |= FLAG_NEEPARTS
         dayst = _restart.group_from_leaves(leaves, "DAYST", n)
         loop = cls(cols, P, day_params or DayParams(), dayst, **kw)
         loop.checkpoint = (leaves, meta, extra)

@@ -36,7 +36,8 @@ import torch
 
 from . import layout as L
 from .columns import Columns
-from .params import (FLAG_ACC, FLAG_BEDROCK, FLAG_CH4, FLAG_H2O_CONSISTENT, FLAG_SOIL_MEANS, FLAG_SUNSHADE_L,
+from .params import (FLAG_ACC, FLAG_BEDROCK, FLAG_CH4, FLAG_ETPARTS, FLAG_H2O_CONSISTENT, FLAG_NEEPARTS,
+                     FLAG_SOIL_MEANS, FLAG_SUNSHADE_L,
                      FLAG_SUNSHADE_U, StepParams)
 
 # Where each parameter of the flat record lives in the reference's objects.
@@ -105,8 +106,22 @@ def tree_set(root, path: str, value):
     return _replace(root, head, tree_set(getattr(root, head), tail, value))
 
 
+# StomataParams switches whose formulations the step does not carry (all off by
+# default, stomata.py:98-159; acclim_pfts / acclim_per_pft only act with
+# acclim_on).  A parameter set that turns one on is refused, not silently run
+# without it.
+UNSUPPORTED_SWITCHES = ("vmax_mix", "scale_leaf_only", "acclim_on", "cap_scale_u", "cap_scale_l", "coefm_mix",
+                        "acclim_light", "frost_on", "gpp_split_by_capacity")
+
+
 def step_params(state, consts, params, dtime: float, ndaypy: float = 365.0) -> StepParams:
-    """The flat parameter record (and variant flags) equivalent to the reference objects."""
+    """The flat parameter record (and variant flags) equivalent to the reference
+    objects.  Raises NotImplementedError for a stomata switch of
+    ``UNSUPPORTED_SWITCHES`` that is on."""
+    sp = getattr(params, "stomata_params", None)
+    on = [k for k in UNSUPPORTED_SWITCHES if bool(getattr(sp, k, False))]
+    if on:
+        raise NotImplementedError(f"stomata_params switches not implemented by the B200 step: {', '.join(on)}")
     roots = {"state": state, "consts": consts, "params": params}
     P = StepParams()
     for name, path in PARAM_PATHS.items():
@@ -129,7 +144,6 @@ def step_params(state, consts, params, dtime: float, ndaypy: float = 365.0) -> S
         flags |= FLAG_BEDROCK
     if bool(getattr(params, "h2o_consistent_weights", False)):
         flags |= FLAG_H2O_CONSISTENT
-    sp = getattr(params, "stomata_params", None)
     if bool(getattr(sp, "sunshade_u", False)):
         flags |= FLAG_SUNSHADE_U
     if bool(getattr(sp, "sunshade_l", False)):
@@ -190,6 +204,17 @@ def timestep_body(state, consts, params, dtime: float, device="cuda"):
     return state
 
 
+_PARTS = ("et_trans", "et_interc", "et_soilev", "et_snowsub", "nee_night", "nee_day")
+
+
+def parts_flags(state) -> int:
+    """FLAG_ETPARTS / FLAG_NEEPARTS for the optional modules ``state`` carries:
+    the reference sums the ET components and the day/night NEE only when
+    ``state.etparts`` / ``state.neeparts`` is attached (loops_gswp3.py:265, 276)."""
+    return (FLAG_ETPARTS if getattr(state, "etparts", None) is not None else 0) | \
+        (FLAG_NEEPARTS if getattr(state, "neeparts", None) is not None else 0)
+
+
 def run_hours(state, consts, params, forcing: dict, dtime: float, ch4_inund=None, soil_means: bool = False,
               ndaypy: float = 365.0, acc=None, device="cuda"):
     """``nhour`` hourly steps with the day loop's accumulators, in one launch.
@@ -198,9 +223,13 @@ def run_hours(state, consts, params, forcing: dict, dtime: float, ch4_inund=None
     arrays.  ``ch4_inund`` (per-cell inundated fraction) turns on the hourly
     wetland CH4 accumulator.  ``acc`` is a previous return value to continue
     from.  Returns ``(state, acc)`` with ``acc`` a dict of the ``layout.ACC``
-    accumulators (value and Kahan planes kept for continuation)."""
+    accumulators (value and Kahan planes kept for continuation).  The ET and
+    NEE components of a state that carries ``etparts`` / ``neeparts`` are
+    summed on top of the state's values and written back into it, as the
+    reference's step body does."""
     P = step_params(state, consts, params, dtime, ndaypy)
     P.flags = P.flags | FLAG_ACC | (FLAG_CH4 if ch4_inund is not None else 0) | (FLAG_SOIL_MEANS if soil_means else 0)
+    P.flags |= parts_flags(state)
     ncell = int(np.asarray(state.soil.tg).shape[0])
     dtype = _dtype_of(state)
     if dtype == torch.float64:
@@ -210,12 +239,16 @@ def run_hours(state, consts, params, forcing: dict, dtime: float, ch4_inund=None
     if ch4_inund is not None:
         stat["f_inund"] = np.asarray(ch4_inund, dtype=np.float64)
     cols = Columns.from_host(prog, stat, dtype=dtype, device=device, acc=True)
+    parts = {k: v for k, v in _leaf_dict(state, "ACC", ncell).items() if k in _PARTS}
     if acc is not None:
         cols.acc.copy_(torch.as_tensor(acc["_planes"], dtype=dtype))
+    elif parts:
+        cols.set_acc(parts)
     cols.run(cols.forcing(forcing), P)
     torch.cuda.synchronize(cols.device)
     state = _write_back(state, cols.prog_host(), "PROG", dtype)
     out = cols.acc_host(compensated=True)
+    state = _write_back(state, {k: out[k] for k in parts}, "ACC", dtype)
     out["_planes"] = cols.acc.cpu().numpy().copy()
     return state, out
 
@@ -275,7 +308,7 @@ def run_month_scan(state, consts, params, xs, nsoilcall: int, ndaypy: int, dtime
         sw_h, use_h = xs[11], xs[12]
     nday, ncell = td.shape
     P = step_params(state, consts, params, dtime, ndaypy)
-    P.flags |= FLAG_ACC | (FLAG_SOIL_MEANS if soil_means else 0)
+    P.flags |= FLAG_ACC | (FLAG_SOIL_MEANS if soil_means else 0) | parts_flags(state)
     dtype = _dtype_of(state)
     prog = _leaf_dict(state, "PROG", ncell)
     stat = _leaf_dict(state, "STAT", ncell)

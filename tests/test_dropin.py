@@ -40,6 +40,19 @@ def test_tree_set_on_dataclass_namedtuple_namespace():
     assert new2.a == 5.0 and new2.b is new.b
 
 
+@pytest.mark.parametrize("switch", dropin.UNSUPPORTED_SWITCHES)
+def test_unimplemented_stomata_switch_is_refused(switch):
+    """A stomata formulation the step does not carry raises instead of running
+    the default formulation in its place; the implemented switches pass."""
+    state = types.SimpleNamespace(soil=types.SimpleNamespace(tsoi_deep=None))
+    sp = types.SimpleNamespace(sunshade_u=True, sunshade_l=False, **{switch: True})
+    with pytest.raises(NotImplementedError, match=switch):
+        dropin.step_params(state, types.SimpleNamespace(), types.SimpleNamespace(stomata_params=sp), 3600.0)
+    setattr(sp, switch, False)
+    P = dropin.step_params(state, types.SimpleNamespace(), types.SimpleNamespace(stomata_params=sp), 3600.0)
+    assert P.flags & FLAG_SUNSHADE_U and not P.flags & FLAG_BEDROCK
+
+
 _MAP_CHECK = r"""
 import sys, numpy as np
 sys.path.insert(0, "{golden}/jaxshim"); sys.path.insert(0, "{ref}"); sys.path.insert(0, "{golden}"); sys.path.insert(0, "{repo}")
@@ -139,3 +152,26 @@ def test_dropin_step_matches_reference_golden(cuda_lib, name):
             dg = {f.name: np.asarray(dropin._get({"s": state}, "s." + f.leaf)) for f in L.DIAG}
             bad += compare(dg, c.out(h + 1, "diag"), 1e-9)
             assert not bad, (h + 1, bad[:5])
+
+
+@pytest.mark.gpu
+def test_run_hours_sums_attached_et_and_nee_parts(cuda_lib):
+    """A state carrying the reference's optional ``etparts`` / ``neeparts``
+    modules gets them summed over the hours and written back (float64 state:
+    the reference's day with both modules within 1e-6, as the other
+    accumulators); a state without them is left without them."""
+    from goldens import Case, compare
+    c = Case("day_mixed")
+    z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "day_parts.npz"))
+    state, consts, params = _mock(c)
+    zero = np.zeros(c.ncell)
+    state.etparts = types.SimpleNamespace(trans=zero, interc=zero, soilev=zero, snowsub=zero)
+    state.neeparts = types.SimpleNamespace(night=zero, day=zero)
+    assert dropin.parts_flags(state) != 0
+    out, acc = dropin.run_hours(state, consts, params, c.forc, c.params.dtime)
+    got = {f.name: np.asarray(dropin._get({"s": out}, "s." + f.leaf)) for f in L.ACC
+           if f.leaf.startswith(("etparts.", "neeparts."))}
+    assert len(got) == 6
+    assert not compare(got, {k: z["day.acc." + k] for k in got}, 1e-6)
+    plain, _ = dropin.run_hours(_mock(c)[0], consts, params, c.forc, c.params.dtime)
+    assert getattr(plain, "etparts", None) is None and dropin.parts_flags(plain) == 0
