@@ -12,6 +12,10 @@ bool valid(const void* a, const void* b, const void* c, const void* d, int ncell
     if (!a || !b || !c || !d || !P || !dp) return false;
     if (ncell < 0 || ld < ncell || ld % 32) return false;
     if (!(P->ndaypy > 0.0) || !(dp->ddays > 0.0) || !(dp->gdd_ramp_u > 0.0) || !(dp->gdd_ramp_l > 0.0)) return false;
+    // the module switches are 0 or 1; the seasonal states need a time constant and a day of year
+    for (const double sw : {dp->seasonal_on, dp->stress_on, dp->sen_photoperiod_u, dp->sen_photoperiod_l})
+        if (sw != 0.0 && sw != 1.0) return false;
+    if (dp->seasonal_on != 0.0 && (!(dp->acclim_tau > 0.0) || !(dp->jday >= 1.0 && dp->jday <= 366.0))) return false;
     double h4 = 0.0;
     for (int k = 0; k < 4; ++k) {
         if (!(P->hsoi[k] > 0.0)) return false;

@@ -6,8 +6,10 @@
 //   day_end:   10-day means and annual sums, the Lloyd-Taylor x WFPS
 //              decomposition factors, one day of soil C/N
 //              (physics/biogeochem.py:23-243) and the respiration sums.
-// Seasonal formulations, the stress accumulator, crop and slot types are off
-// (the reference's defaults).  Buffers are the step's planes in R (float or
+// With the day parameters' module switches on, day_begin also advances the
+// seasonal states (loops_gswp3.py:418-437) and day_end the growing-season
+// stress sums (loops_gswp3.py:585-596).  Crop and slot types are off (the
+// reference's defaults).  Buffers are the step's planes in R (float or
 // double); every operation runs in double.  Constants the reference forms in
 // float32 are rounded to float32 here too.
 #pragma once
@@ -36,22 +38,54 @@ __device__ __forceinline__ void acc_zero(const Planes<R>& A, int p) {
     A.set(p + IBIS_ACC_COUNT, 0.0);
 }
 
-// pheno (phenology.py:89-287)
+// Astronomical day length in hours (state/seasonal.py:56-61): solar
+// declination 23.44 deg x sin(2 pi (doy - 81) / 365), the sunrise hour angle,
+// clipped for polar day and night.
+__device__ __forceinline__ double daylength_hours(double lat, double doy) {
+    const double pi = 3.141592653589793;
+    const double decl = 0.40910518 * sin(2.0 * pi * (doy - 81.0) / 365.0);
+    const double x = fmin(fmax(-tan(lat) * tan(decl), -1.0), 1.0);
+    return 24.0 / pi * acos(x);
+}
+
+// The seasonal states, once a day before phenology (loops_gswp3.py:418-437):
+// acclimation S += (T - S) / tau; the senescence sums of cold degree-days below
+// Tb while the day length is decreasing and below Pstart, reset otherwise.
+// Returns through sen_u / sen_l whether photoperiod-gated senescence starts.
+template <typename R>
+__device__ __forceinline__ void seasonal_states(const Planes<R>& D, double td, const IbisDayParams& dp, bool& sen_u,
+                                                bool& sen_l) {
+    const double tc = td - 273.16, lat = D.get(IBIS_DAYST_LATITUDE);
+    const double dl = daylength_hours(lat, dp.jday);
+    const bool dec = dl < daylength_hours(lat, dp.jday - 1.0);
+    const double x = D.get(IBIS_DAYST_ACCLIM_X);
+    const double su = (dec && dl < dp.sen_pstart_u) ? D.get(IBIS_DAYST_SSEN_U) + fmax(dp.sen_tb_u - tc, 0.0) : 0.0;
+    const double sl = (dec && dl < dp.sen_pstart_l) ? D.get(IBIS_DAYST_SSEN_L) + fmax(dp.sen_tb_l - tc, 0.0) : 0.0;
+    D.set(IBIS_DAYST_ACCLIM_X, x + (tc - x) / dp.acclim_tau);
+    D.set(IBIS_DAYST_SSEN_U, su);
+    D.set(IBIS_DAYST_SSEN_L, sl);
+    sen_u = dp.sen_photoperiod_u != 0.0 && su >= dp.sen_ycrit_u;
+    sen_l = dp.sen_photoperiod_l != 0.0 && sl >= dp.sen_ycrit_l;
+}
+
+// pheno (phenology.py:89-287); sen_u / sen_l: photoperiod-gated senescence
+// (phenology.py:148-150, 170-172)
 template <typename R>
 __device__ __forceinline__ void phenology(const Planes<R>& S, const Planes<R>& D, double td, double stresstu,
-                                          double stresstl, const IbisDayParams& dp, double epsilon) {
+                                          double stresstl, const IbisDayParams& dp, double epsilon, bool sen_u,
+                                          bool sen_l) {
     const double tmelt = 273.16, ddfac = 1.0 / dp.ddays;
     const double a10td = D.get(IBIS_DAYST_A10TD);
     const double tthr_u = fmax(fmax(0.0 + tmelt, D.get(IBIS_DAYST_TC) + dp.tthresh_u_offset + tmelt),
                                dp.tthresh_u_abs + tmelt);
     const double gthr_u = dp.gthresh_u_c + tmelt;
-    const double agddu = a10td < gthr_u ? 0.0 : D.get(IBIS_DAYST_AGDDU) + td - gthr_u;
-    const double tempu = a10td < tthr_u ? fmax(0.0, D.get(IBIS_DAYST_TEMPU) - ddfac)
-                                        : fmin(1.0, fmax(0.0, agddu - dp.gdd_thresh_u) / dp.gdd_ramp_u);
+    const double agddu = (a10td < gthr_u || sen_u) ? 0.0 : D.get(IBIS_DAYST_AGDDU) + td - gthr_u;
+    const double tempu = (a10td < tthr_u || sen_u) ? fmax(0.0, D.get(IBIS_DAYST_TEMPU) - ddfac)
+                                                   : fmin(1.0, fmax(0.0, agddu - dp.gdd_thresh_u) / dp.gdd_ramp_u);
     const double tthr_l = dp.tthresh_l_c + tmelt, gthr_l = dp.gthresh_l_c + tmelt;
-    const double agddl = a10td < gthr_l ? 0.0 : D.get(IBIS_DAYST_AGDDL) + td - gthr_l;
-    const double templ = a10td < tthr_l ? fmax(0.0, D.get(IBIS_DAYST_TEMPL) - ddfac)
-                                        : fmin(1.0, fmax(0.0, agddl - dp.gdd_thresh_l) / dp.gdd_ramp_l);
+    const double agddl = (a10td < gthr_l || sen_l) ? 0.0 : D.get(IBIS_DAYST_AGDDL) + td - gthr_l;
+    const double templ = (a10td < tthr_l || sen_l) ? fmax(0.0, D.get(IBIS_DAYST_TEMPL) - ddfac)
+                                                   : fmin(1.0, fmax(0.0, agddl - dp.gdd_thresh_l) / dp.gdd_ramp_l);
     auto drop = [&](int plane, int anc, double s) {
         const double old = D.get(plane);
         const bool dry = D.get(anc) < dp.drop_thresh || s < dp.drop_stress_thresh;
@@ -239,7 +273,10 @@ __global__ void __launch_bounds__(128) day_begin_kernel(R* stat, R* dayst, R* ac
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ncell) return;
     const Planes<R> S{stat + i, ld}, D{dayst + i, ld}, A{acc + i, ld};
-    phenology(S, D, (double)td[i], A.get(IBIS_ACC_STRESSTU_LAST), A.get(IBIS_ACC_STRESSTL_LAST), dp, c.epsilon);
+    bool sen_u = false, sen_l = false;
+    if (dp.seasonal_on != 0.0) seasonal_states(D, (double)td[i], dp, sen_u, sen_l);
+    phenology(S, D, (double)td[i], A.get(IBIS_ACC_STRESSTU_LAST), A.get(IBIS_ACC_STRESSTL_LAST), dp, c.epsilon, sen_u,
+              sen_l);
     const int sums[7] = {IBIS_ACC_ADRAIN, IBIS_ACC_ADSNOW, IBIS_ACC_ADAET, IBIS_ACC_A10ANCUB, IBIS_ACC_A10ANCLS,
                          IBIS_ACC_A10ANCL3, IBIS_ACC_A10ANCL4};
 #pragma unroll
@@ -283,6 +320,14 @@ __global__ void __launch_bounds__(128) day_end_kernel(const R* prog, R* stat, R*
     const double conv = (double)(float)(12.0e-3 * 86400.0);
     D.set(IBIS_DAYST_AYCO2MIC, D.get(IBIS_DAYST_AYCO2MIC) + tco2mic * conv);
     D.set(IBIS_DAYST_AYCO2ROOT, D.get(IBIS_DAYST_AYCO2ROOT) + D.get(IBIS_DAYST_TCO2ROOT) * conv);
+    // growing-season soil-water stress sums from the day's last hour
+    // (loops_gswp3.py:585-596): days warmer than tmelt + stress_accum_tmin
+    if (dp.stress_on != 0.0) {
+        const double grow = (double)td[i] > 273.16 + dp.stress_accum_tmin ? 1.0 : 0.0;
+        D.set(IBIS_DAYST_AYSTRESSU, D.get(IBIS_DAYST_AYSTRESSU) + A.get(IBIS_ACC_STRESSTU_LAST) * grow);
+        D.set(IBIS_DAYST_AYSTRESSL, D.get(IBIS_DAYST_AYSTRESSL) + A.get(IBIS_ACC_STRESSTL_LAST) * grow);
+        D.set(IBIS_DAYST_STRESS_NDAY, D.get(IBIS_DAYST_STRESS_NDAY) + grow);
+    }
 }
 
 }  // namespace ibis

@@ -22,6 +22,7 @@ planes.
 """
 from __future__ import annotations
 
+import copy
 import ctypes
 
 import numpy as np
@@ -33,7 +34,7 @@ from . import restart as _restart
 from . import synth
 from .columns import Columns
 from .forcing import OBSERVED_FIRA, hourly_forcing
-from .params import FLAG_ACC, FLAG_CH4, FLAG_ETPARTS, FLAG_NEEPARTS, DayParams, StepParams
+from .params import FLAG_ACC, FLAG_CH4, DayParams, StepParams
 
 _TD = L.OFF["DAILY"]["td"][0]
 MONTH_NEW_YEAR, MONTH_FROM_MEAN, MONTH_PARTITION = 1, 2, 4
@@ -51,7 +52,10 @@ class DayLoop:
     the daily-cadence state as a dict of per-cell arrays named as
     ``layout.DAYST`` (a checkpoint supplies it; see :meth:`from_restart`).
     ``lat`` (degrees), ``seed``, ``jday`` (day of year of the next day) and
-    ``day`` (its counter for the variates) drive the forcing generator."""
+    ``day`` (its counter for the variates) drive the forcing generator; ``lat``
+    and ``jday`` also give the day length of the seasonal states, which advance
+    with ``day_params.seasonal_on`` (the growing-season stress sums with
+    ``day_params.stress_on``)."""
 
     def __init__(self, cols: Columns, params: StepParams, day_params: DayParams, dayst: dict, lat=None,
                  seed: int = 0, jday: int = 1, day: int = 0, dtime: float = 3600.0, observed_fira: bool = True):
@@ -60,10 +64,13 @@ class DayLoop:
         self.cols = cols
         self.params = params.copy()
         self.params.flags |= FLAG_ACC
-        self.day_params = day_params
+        self.day_params = copy.deepcopy(day_params)
         n, ld = cols.ncell, cols.ld
-        self.dayst = torch.from_numpy(synth.to_planes("DAYST", dayst, ld, cols._np_dtype)).to(cols.device)
+        if self.day_params.seasonal_on and lat is None:
+            raise ValueError("the seasonal states need the cells' latitudes (lat=)")
         lat = np.zeros(n) if lat is None else np.asarray(lat, dtype=np.float64)
+        dayst = dict(dayst, latitude=np.deg2rad(lat))
+        self.dayst = torch.from_numpy(synth.to_planes("DAYST", dayst, ld, cols._np_dtype)).to(cols.device)
         lat_planes = np.zeros(ld, dtype=np.float32)
         lat_planes[:n] = lat
         self.lat = torch.from_numpy(lat_planes).to(cols.device)
@@ -94,11 +101,6 @@ class DayLoop:
         # a10anc* leaves hold 10-day means between days (DAYST), not sums
         acc0 = _restart.group_from_leaves(leaves, "ACC", n)
         cols.set_acc({k: v for k, v in acc0.items() if not k.startswith("a10anc")})
-        # a checkpoint with the optional etparts / neeparts modules keeps summing them
-        if "et_trans" in acc0:
-            P.flags |= FLAG_ETPARTS
-        if "nee_night" in acc0:
-            P.flags |= FLAG_NEEPARTS
         dayst = _restart.group_from_leaves(leaves, "DAYST", n)
         loop = cls(cols, P, day_params or DayParams(), dayst, **kw)
         loop.checkpoint = (leaves, meta, extra)
@@ -135,7 +137,9 @@ class DayLoop:
         return synth.from_planes("DAYST", self.dayst.cpu().numpy(), self.cols.ncell)
 
     def set_dayst(self, dayst: dict):
-        a = synth.to_planes("DAYST", dayst, self.cols.ld, self.cols._np_dtype)
+        """Replace the daily-cadence state; the latitude plane is kept unless given."""
+        a = synth.to_planes("DAYST", {"latitude": self.dayst_host()["latitude"], **dayst}, self.cols.ld,
+                            self.cols._np_dtype)
         self.dayst.copy_(torch.from_numpy(a))
 
     def wet_host(self) -> dict:
@@ -150,6 +154,7 @@ class DayLoop:
         """Phenology and the zeroing of the daily sums (``td``: the day's mean air temperature plane)."""
         c = self.cols
         stream = stream or torch.cuda.current_stream(c.device)
+        self.day_params.jday = float(self.jday)
         rc = self._begin(_ptr(c.stat), _ptr(self.dayst), _ptr(c.acc), _ptr(td), c.ncell, c.ld,
                          ctypes.byref(self.params.to_c()), ctypes.byref(self.day_params.to_c()),
                          ctypes.c_void_p(stream.cuda_stream))

@@ -257,11 +257,13 @@ def run_hours(state, consts, params, forcing: dict, dtime: float, ch4_inund=None
 # phenology (physics/phenology.py:20, PhenoParams) and soil biogeochemistry
 # (io/parameters.py:176, BGCParams; ``bgc_fmax`` is its ``fmax``).
 def _day_param_paths():
-    from .params import DAY_PARAM_FIELDS
-    names = [n for n, _, _ in DAY_PARAM_FIELDS]
+    from .params import DAY_LOOP_FIELDS, DAY_PARAM_FIELDS
+    names = [n for n, _, _ in DAY_PARAM_FIELDS if n not in DAY_LOOP_FIELDS]
     pheno = names[:names.index("lig_frac")]
-    return {n: (f"params.pheno.{n}" if n in pheno else f"params.bgc_params.{'fmax' if n == 'bgc_fmax' else n}")
-            for n in names}
+    out = {n: (f"params.pheno.{n}" if n in pheno else f"params.bgc_params.{'fmax' if n == 'bgc_fmax' else n}")
+           for n in names}
+    out["acclim_tau"] = "params.stomata_params.acclim_tau"
+    return out
 
 
 DAY_PARAM_PATHS = _day_param_paths()
@@ -293,14 +295,18 @@ def run_month_scan(state, consts, params, xs, nsoilcall: int, ndaypy: int, dtime
     variates (event timing, hourly wind) come from the counter-based generator
     keyed by (``seed``, ``day0`` + day, cell) instead of ``jax.random``.
 
-    Supported as the reference's defaults run it: one soil-BGC call per day
-    (``nsoilcall`` 1), two radiation bands, the seasonal formulations, stress
-    accumulator, crop and slot types off; ``iwet`` is not used (the reference's
-    day loop does not read it either)."""
+    Supported: one soil-BGC call per day (``nsoilcall`` 1), two radiation
+    bands, no per-cell growth habits (``slot_habit``); the optional state
+    modules the state carries (stress, ET parts, seasonal states with
+    photoperiod-gated senescence, NEE parts) advance as in the reference, with
+    the stomata switches of ``UNSUPPORTED_SWITCHES`` off.  ``iwet`` is not used
+    (the reference's day loop does not read it either)."""
     from . import forcing as _forcing
     from .daily import DayLoop
     if int(nsoilcall) != 1 or int(nband) != 2:
         raise NotImplementedError("one soil-BGC call per day and two radiation bands only")
+    if getattr(params, "slot_habit", None) is not None:
+        raise NotImplementedError("per-cell growth habits (params.slot_habit) are not implemented")
     xs = [np.asarray(x) for x in xs]
     td, tmax, tmin, cloud, precip, psurf, qd, ud, _iwet, rlds, jdays = xs[:11]
     sw_h = use_h = None
@@ -327,7 +333,12 @@ def run_month_scan(state, consts, params, xs, nsoilcall: int, ndaypy: int, dtime
     acc0 = _leaf_dict(state, "ACC", ncell)
     cols.set_acc({k: v for k, v in acc0.items() if not k.startswith("a10anc")})
     lat = np.rad2deg(np.asarray(_get({"params": params}, "params.latitude"), dtype=np.float64)).reshape(ncell)
-    loop = DayLoop(cols, P, day_params(params), _leaf_dict(state, "DAYST", ncell), lat=lat, seed=seed,
+    DP = day_params(params)
+    # the optional modules of the daily cadence advance when the state carries
+    # them (loops_gswp3.py:423, 589)
+    DP.seasonal_on = float(getattr(state, "seasonal", None) is not None)
+    DP.stress_on = float(getattr(state, "stress", None) is not None)
+    loop = DayLoop(cols, P, DP, _leaf_dict(state, "DAYST", ncell), lat=lat, seed=seed,
                    jday=int(jdays[0]), day=day0, dtime=dtime, observed_fira=True)
     daily = {"td": td, "tmax": tmax, "tmin": tmin, "cloud": cloud, "precip": precip, "psurf": psurf, "qd": qd,
              "ud": ud, "fira": rlds}

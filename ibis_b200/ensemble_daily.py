@@ -66,6 +66,7 @@ class EnsembleDayLoop:
                                                   ((0, 0), (0, self.ld_run - self.nrun)))
         self.prog = torch.from_numpy(run_planes("PROG", prog)).to(dev)
         self.stat = torch.from_numpy(run_planes("STAT", stat)).to(dev)
+        dayst = dict(dayst, latitude=np.deg2rad(np.asarray(lat, np.float64)))    # the seasonal states' day length
         self.dayst = torch.from_numpy(run_planes("DAYST", dayst)).to(dev)
         self.acc = torch.zeros((2 * L.N_ACC, self.ld_run), **f32)
         rp = np.zeros((L.N_RUN, self.ld_run), dtype=np.float32)
@@ -118,6 +119,7 @@ class EnsembleDayLoop:
             self.records.view(self.nsite, 24, L.N_FORC).copy_(self.hourly[:, :, :self.nsite].permute(2, 0, 1))
             self.td[:self.nrun] = self.daily[d, _TD][self.site_index]
         n, ld = self.nrun, self.ld_run
+        self._dpc.jday = float(self.jday)                   # the day length of the seasonal states
         _lib.check(self.lib.ibis_day_begin_f32(_p(self.stat), _p(self.dayst), _p(self.acc), _p(self.td), n, ld,
                                                ctypes.byref(self._pc), ctypes.byref(self._dpc), s), "ibis_day_begin")
         _lib.check(self.lib.ibis_ensemble_f32(ctypes.byref(self._c), ctypes.byref(self._pc), 0, s),

@@ -342,6 +342,18 @@ DAYST = (
     Field("falll", "carbon.falll"),
     Field("fallr", "carbon.fallr"),
     Field("fallw", "carbon.fallw"),
+    # the optional modules of the daily cadence (loops_gswp3.py:418-437,
+    # 585-596): the seasonal states (temperature acclimation, Delpierre
+    # senescence) and the growing-season soil-water stress sums, advanced only
+    # when the day parameters switch them on; the latitude (radians) gives the
+    # day length the senescence states read
+    Field("acclim_x", "seasonal.acclim_x"),
+    Field("ssen_u", "seasonal.ssen_u"),
+    Field("ssen_l", "seasonal.ssen_l"),
+    Field("aystressu", "stress.aystressu"),
+    Field("aystressl", "stress.aystressl"),
+    Field("stress_nday", "stress.nday"),
+    Field("latitude", "params.latitude"),
 )
 
 # Monthly wetland methane (MethaneState, python-port/ibis/bgc/methane.py:404-423)

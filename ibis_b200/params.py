@@ -187,12 +187,16 @@ class StepParams:
 # double: PhenoParams (python-port/ibis/physics/phenology.py:30-86, read by
 # pheno, phenology.py:89-287) and BGCParams (io/parameters.py, read by soilbgc,
 # physics/biogeochem.py:23-243, and the decomposition factors of the day loop,
-# timestepping/loops_gswp3.py:494-555).  Defaults are the reference's.
+# timestepping/loops_gswp3.py:494-555), and the acclimation time constant of
+# StomataParams (physics/stomata.py:116) the seasonal module advances with.
+# The photoperiod switches are 0 or 1.  Defaults are the reference's.
 DAY_PARAM_FIELDS: list[tuple[str, int, object]] = [
     ("ddays", 1, 15.0), ("tthresh_u_offset", 1, 5.0), ("tthresh_u_abs", 1, -100.0), ("gthresh_u_c", 1, 0.0),
     ("gdd_thresh_u", 1, 100.0), ("gdd_ramp_u", 1, 50.0), ("tthresh_l_c", 1, 0.0), ("gthresh_l_c", 1, -5.0),
     ("gdd_thresh_l", 1, 150.0), ("gdd_ramp_l", 1, 50.0), ("drop_thresh", 1, 0.0), ("drop_stress_thresh", 1, -1.0),
-    ("drop_floor", 1, 0.1),
+    ("drop_floor", 1, 0.1), ("stress_accum_tmin", 1, -100.0),
+    ("sen_photoperiod_u", 1, 0.0), ("sen_pstart_u", 1, 14.0), ("sen_tb_u", 1, 20.0), ("sen_ycrit_u", 1, 300.0),
+    ("sen_photoperiod_l", 1, 0.0), ("sen_pstart_l", 1, 14.0), ("sen_tb_l", 1, 20.0), ("sen_ycrit_l", 1, 300.0),
     ("lig_frac", 1, 0.5), ("fbsom", 1, 0.017), ("effac", 1, 0.4), ("bgc_fmax", 1, 0.45), ("rconst", 1, 1200.0),
     ("cnleaf", 1, 40.0), ("cnroot", 1, 60.0), ("cnwood", 1, 200.0),
     ("cnr", 8, (8.0, 15.0, 10.0, 15.0, 100.0, 150.0, 6.0, 250.0)),
@@ -203,7 +207,13 @@ DAY_PARAM_FIELDS: list[tuple[str, int, object]] = [
     ("ywm", 1, 0.4), ("yws", 1, 0.3), ("ywl", 1, 1.0), ("ybn", 1, 1.0), ("ybp", 1, 1.0), ("yps", 1, 1.0),
     ("yns", 1, 1.0), ("ysb", 1, 0.2), ("ypb", 1, 0.2), ("ynb", 1, 0.25),
     ("lt_e0", 1, 344.0), ("wfps_opt", 1, 60.0), ("k_scale", 1, 1.0),
+    ("acclim_tau", 1, 10.93),
+    # set by the day loop, not parameters of the reference: the day of year of
+    # the day, and whether the state carries the seasonal / stress modules (0 or 1)
+    ("jday", 1, 1.0), ("seasonal_on", 1, 0.0), ("stress_on", 1, 0.0),
 ]
+# the day parameters the day loop sets itself
+DAY_LOOP_FIELDS = ("jday", "seasonal_on", "stress_on")
 
 
 class DayParams:

@@ -214,8 +214,14 @@ int ibis_diurnal_sw_f32(const float* daily, const float* lat, const float* sw_ob
  * decomposition factors, one day of soil C/N and the respiration sums.
  * params supplies hsoi, ndaypy and epsilon; dayparams the phenology and
  * soil-biogeochemistry constants.  Arithmetic is double for both buffer types.
+ * With dayparams->seasonal_on = 1, ibis_day_begin first advances the seasonal
+ * states (acclim_x, ssen_u, ssen_l; day length from the latitude plane and
+ * dayparams->jday) and gates phenology by photoperiod where sen_photoperiod_*
+ * is 1; with stress_on = 1, ibis_day_end adds the last hour's stress to the
+ * growing-season sums (aystressu, aystressl, stress_nday).  Switches other
+ * than 0 or 1 return -EINVAL.
  * Replaces: the per-day body of _run_month_scan._day_body
- * (python-port/ibis/timestepping/loops_gswp3.py:382-415 and 466-584), with
+ * (python-port/ibis/timestepping/loops_gswp3.py:382-437, 466-596), with
  * pheno (physics/phenology.py:89-287) and soilbgc (physics/biogeochem.py:23-243). */
 int ibis_day_begin_f32(float* stat, float* dayst, float* acc, const float* td, int ncell, int ld,
                        const IbisParams* params, const IbisDayParams* dayparams, void* stream);

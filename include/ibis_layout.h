@@ -303,7 +303,14 @@ enum {
     IBIS_DAYST_FALLL = 55,  /* carbon.falll */
     IBIS_DAYST_FALLR = 56,  /* carbon.fallr */
     IBIS_DAYST_FALLW = 57,  /* carbon.fallw */
-    IBIS_DAYST_COUNT = 58
+    IBIS_DAYST_ACCLIM_X = 58,  /* seasonal.acclim_x */
+    IBIS_DAYST_SSEN_U = 59,  /* seasonal.ssen_u */
+    IBIS_DAYST_SSEN_L = 60,  /* seasonal.ssen_l */
+    IBIS_DAYST_AYSTRESSU = 61,  /* stress.aystressu */
+    IBIS_DAYST_AYSTRESSL = 62,  /* stress.aystressl */
+    IBIS_DAYST_STRESS_NDAY = 63,  /* stress.nday */
+    IBIS_DAYST_LATITUDE = 64,  /* params.latitude */
+    IBIS_DAYST_COUNT = 65
 };
 
 /* WET */
@@ -556,6 +563,15 @@ typedef struct IbisDayParams {
     double drop_thresh;
     double drop_stress_thresh;
     double drop_floor;
+    double stress_accum_tmin;
+    double sen_photoperiod_u;
+    double sen_pstart_u;
+    double sen_tb_u;
+    double sen_ycrit_u;
+    double sen_photoperiod_l;
+    double sen_pstart_l;
+    double sen_tb_l;
+    double sen_ycrit_l;
     double lig_frac;
     double fbsom;
     double effac;
@@ -600,6 +616,10 @@ typedef struct IbisDayParams {
     double lt_e0;
     double wfps_opt;
     double k_scale;
+    double acclim_tau;
+    double jday;
+    double seasonal_on;
+    double stress_on;
 } IbisDayParams;
 
 #endif /* IBIS_LAYOUT_H */

@@ -3,15 +3,18 @@
 The checker of the device daily kernels (ibis_b200/csrc/ibis_daily.cuh).  One
 day of the reference's GSWP3 day loop (``_run_month_scan._day_body``,
 python-port/ibis/timestepping/loops_gswp3.py:382-608) around its 24 hourly
-steps, with the seasonal formulations, the stress accumulator, crop and
-IBIS 3.0 slot types off (their defaults) and one soil-BGC call per day:
+steps, with crop and IBIS 3.0 slot types off (their defaults) and one soil-BGC
+call per day:
 
 * :func:`day_begin` -- capture the 10-day means, zero the daily sums
-  (loops_gswp3.py:402-415), and ``pheno`` (physics/phenology.py:89-287);
+  (loops_gswp3.py:402-415), advance the seasonal states when the state
+  carries them (loops_gswp3.py:418-437), and ``pheno``
+  (physics/phenology.py:89-287);
 * :func:`day_end` -- 10-day means and annual sums (loops_gswp3.py:466-492),
   the decomposition factors (loops_gswp3.py:494-562), ``soilbgc``
-  (physics/biogeochem.py:23-243) and the heterotrophic-respiration sums
-  (loops_gswp3.py:575-584).
+  (physics/biogeochem.py:23-243), the heterotrophic-respiration sums
+  (loops_gswp3.py:575-584) and, when the state carries them, the
+  growing-season stress sums (loops_gswp3.py:585-596).
 
 State travels in dicts named as ``ibis_b200.layout`` (STAT, ACC, DAYST
 fields).  Float32 constants of the reference's decomposition code are kept as
@@ -25,20 +28,46 @@ f32 = np.float32
 DAILY_SUMS = ("adrain", "adsnow", "adaet", "a10ancub", "a10ancls", "a10ancl3", "a10ancl4")
 
 
-def pheno(day: dict, stat: dict, means: dict, td, stresstu, stresstl, DP, epsilon):
-    """Phenology of one day (phenology.py:89-287, habit and photoperiod gating off)."""
+def daylength_hours(lat, doy):
+    """state/seasonal.py:56-61 (latitude in radians, 1-based day of year)."""
+    decl = 0.40910518 * np.sin(2.0 * np.pi * (doy - 81.0) / 365.0)
+    return 24.0 / np.pi * np.arccos(np.clip(-np.tan(lat) * np.tan(decl), -1.0, 1.0))
+
+
+def seasonal_states(day: dict, td, DP):
+    """The seasonal states advanced from the day's mean temperature
+    (loops_gswp3.py:418-437); returns (day, sen_u, sen_l), the photoperiod
+    senescence triggers None where the switch is off."""
+    tc = td - 273.16
+    dl = daylength_hours(day["latitude"], DP.jday)
+    dec = dl < daylength_hours(day["latitude"], DP.jday - 1)
+    x = day["acclim_x"] + (tc - day["acclim_x"]) / DP.acclim_tau
+    su = np.where(dec & (dl < DP.sen_pstart_u), day["ssen_u"] + np.maximum(DP.sen_tb_u - tc, 0.0), 0.0)
+    sl = np.where(dec & (dl < DP.sen_pstart_l), day["ssen_l"] + np.maximum(DP.sen_tb_l - tc, 0.0), 0.0)
+    sen_u = su >= DP.sen_ycrit_u if DP.sen_photoperiod_u else None
+    sen_l = sl >= DP.sen_ycrit_l if DP.sen_photoperiod_l else None
+    return dict(day, acclim_x=x, ssen_u=su, ssen_l=sl), sen_u, sen_l
+
+
+def pheno(day: dict, stat: dict, means: dict, td, stresstu, stresstl, DP, epsilon, sen_u=None, sen_l=None):
+    """Phenology of one day (phenology.py:89-287, habit off); ``sen_u`` /
+    ``sen_l`` gate it by photoperiod (phenology.py:148-150, 170-172)."""
     tmelt = 273.16
     ddfac = 1.0 / DP.ddays
     a10td = means["a10td"]
     tthr_u = np.maximum(np.maximum(0.0 + tmelt, day["tc"] + DP.tthresh_u_offset + tmelt), DP.tthresh_u_abs + tmelt)
     gthr_u = DP.gthresh_u_c + tmelt
     cold_u, greset_u = a10td < tthr_u, a10td < gthr_u
+    if sen_u is not None:
+        cold_u, greset_u = cold_u | sen_u, greset_u | sen_u
     agddu = np.where(greset_u, 0.0, day["agddu"] + td - gthr_u)
     tempu = np.where(cold_u, np.maximum(0.0, day["tempu"] - ddfac),
                      np.minimum(1.0, np.maximum(0.0, agddu - DP.gdd_thresh_u) / DP.gdd_ramp_u))
     tthr_l = DP.tthresh_l_c + tmelt
     gthr_l = DP.gthresh_l_c + tmelt
     cold_l, greset_l = a10td < tthr_l, a10td < gthr_l
+    if sen_l is not None:
+        cold_l, greset_l = cold_l | sen_l, greset_l | sen_l
     agddl = np.where(greset_l, 0.0, day["agddl"] + td - gthr_l)
     templ = np.where(cold_l, np.maximum(0.0, day["templ"] - ddfac),
                      np.minimum(1.0, np.maximum(0.0, agddl - DP.gdd_thresh_l) / DP.gdd_ramp_l))
@@ -81,7 +110,10 @@ def pheno(day: dict, stat: dict, means: dict, td, stresstu, stresstl, DP, epsilo
 def day_begin(day: dict, stat: dict, acc: dict, td, P, DP):
     """Start of a day: phenology from the standing 10-day means, then the daily sums zeroed."""
     means = {k: day[k] for k in ("a10td", "a10ancub", "a10ancls", "a10ancl3", "a10ancl4")}
-    day, stat = pheno(day, stat, means, td, acc["stresstu_last"], acc["stresstl_last"], DP, P.epsilon)
+    sen_u = sen_l = None
+    if DP.seasonal_on:
+        day, sen_u, sen_l = seasonal_states(day, td, DP)
+    day, stat = pheno(day, stat, means, td, acc["stresstu_last"], acc["stresstl_last"], DP, P.epsilon, sen_u, sen_l)
     acc = dict(acc)
     for k in DAILY_SUMS:
         acc[k] = np.zeros_like(acc[k])
@@ -239,4 +271,9 @@ def day_end(prog: dict, day: dict, stat: dict, acc: dict, td, P, DP, ndaypy=365,
     stat = dict(stat, tco2mic=tco2mic)
     day["ayco2mic"] = day["ayco2mic"] + tco2mic * f32(12.0e-3 * 86400.0)
     day["ayco2root"] = day["ayco2root"] + day["tco2root"] * f32(12.0e-3 * 86400.0)
+    if DP.stress_on:
+        grow = (td > 273.16 + DP.stress_accum_tmin).astype(np.float64)
+        day["aystressu"] = day["aystressu"] + acc["stresstu_last"] * grow
+        day["aystressl"] = day["aystressl"] + acc["stresstl_last"] * grow
+        day["stress_nday"] = day["stress_nday"] + grow
     return day, stat

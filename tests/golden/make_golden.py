@@ -424,24 +424,43 @@ def write_diurnal_case(days=(15, 172), seed=7, dtime=3600.0):
     print(f"wrote {path}: {len(out)} arrays, {os.path.getsize(path)} bytes")
 
 
-def write_days_case(ndays=3, jday0=172, seed=9):
+def write_days_case(ndays=3, jday0=172, seed=9, modules=False):
     """tests/golden/days_16cells.npz: the reference's own GSWP3 day loop
     (_run_month_scan, loops_gswp3.py:334-612) for ``ndays`` days on the 16-cell
     checkpoint: phenology, 24 hourly steps with accumulators, 10-day means,
     decomposition factors and soil BGC, every leaf recorded after each day.
     Its variates (event timing, hourly wind) come from the counter-based
     generator of the device forcing code; the float32 cast of each day is the
-    identity (the float64 run)."""
+    identity (the float64 run).
+
+    With ``modules`` (tests/golden/days_modules_16cells.npz) the state carries
+    the optional stress, ET-parts, seasonal and NEE-parts modules, seeded with
+    random seasonal and stress states, under photoperiod-gated senescence of
+    both canopies with low critical sums and a growing-season threshold of
+    12 C, so the senescence triggers and the growing-season mask both split
+    the cells."""
     import jax
     from ibis.io.restart import load_state
     from oracle.weather import uniform24
     fix = os.path.join(HERE, "restart_16cells.npz")
     n = 16
-    st, _ = load_state(fix, create_ibis_state(GridConfig(nlon=1, nlat=1, npoi=n, nbedrock=3)))
+    grid = GridConfig(nlon=1, nlat=1, npoi=n, nbedrock=3)
+    st, _ = load_state(fix, create_ibis_state(grid, with_neeparts=modules))
     consts = get_constants()
     rng = np.random.Generator(np.random.PCG64(seed))
     lat = rng.uniform(-40.0, 70.0, size=n)
     sp = dataclasses.replace(loops.default_sim_params(n), latitude=_a(np.deg2rad(lat)), bedrock=BedrockParams())
+    if modules:
+        mrng = np.random.Generator(np.random.PCG64(seed + 1))
+        st = eqx.tree_at(lambda s: (s.seasonal.acclim_x, s.seasonal.ssen_u, s.seasonal.ssen_l), st,
+                         (_a(mrng.uniform(-5.0, 25.0, n)), _a(mrng.uniform(0.0, 40.0, n)),
+                          _a(mrng.uniform(0.0, 40.0, n))))
+        st = eqx.tree_at(lambda s: (s.stress.aystressu, s.stress.aystressl, s.stress.nday), st,
+                         (_a(mrng.uniform(0.0, 50.0, n)), _a(mrng.uniform(0.0, 50.0, n)),
+                          _a(np.floor(mrng.uniform(0.0, 60.0, n)))))
+        sp = dataclasses.replace(sp, pheno=dataclasses.replace(
+            sp.pheno, sen_photoperiod_u=True, sen_photoperiod_l=True, sen_ycrit_u=25.0, sen_ycrit_l=40.0,
+            stress_accum_tmin=12.0))
     days = []
     for d in range(ndays):
         dd, _ = daily_inputs(n, seed=seed + 10 + d)
@@ -455,16 +474,23 @@ def write_days_case(ndays=3, jday0=172, seed=9):
     saved = (getattr(jax.random, "uniform", None), loops_gswp3._cast_tree_f32)
     jax.random.uniform = uniform
     loops_gswp3._cast_tree_f32 = lambda tree: tree
-    out = {"in.lat": lat, "in.jday0": np.asarray(jday0), "in.seed": np.asarray(seed), "in.ndays": np.asarray(ndays)}
+    out = {"in.lat": lat, "in.jday0": np.asarray(jday0), "in.seed": np.asarray(seed), "in.ndays": np.asarray(ndays),
+           "in.modules": np.asarray(int(modules))}
+    if modules:
+        for leaf in ("seasonal.acclim_x", "seasonal.ssen_u", "seasonal.ssen_l", "stress.aystressu",
+                     "stress.aystressl", "stress.nday"):
+            mod, name = leaf.split(".")
+            out["in." + leaf] = np.asarray(getattr(getattr(st, mod), name), dtype=np.float64)
     from ibis_b200 import dropin
-    from ibis_b200.params import PARAM_FIELDS, DAY_PARAM_FIELDS
+    from ibis_b200.params import PARAM_FIELDS
     P = dropin.step_params(st, consts, sp, 3600.0)
+    P.flags |= dropin.parts_flags(st)
     for name, _, _ in PARAM_FIELDS:
         out["in.param." + name] = np.asarray(getattr(P, name), dtype=np.float64)
     out["in.param.flags"] = np.asarray(P.flags, dtype=np.int64)
-    for name, _, _ in DAY_PARAM_FIELDS:
-        src = sp.bgc_params if hasattr(sp.bgc_params, "fmax" if name == "bgc_fmax" else name) else sp.pheno
-        out["in.dparam." + name] = np.asarray(getattr(src, "fmax" if name == "bgc_fmax" else name), dtype=np.float64)
+    DP = dropin.day_params(sp)
+    for name in dropin.DAY_PARAM_PATHS:
+        out["in.dparam." + name] = np.asarray(getattr(DP, name), dtype=np.float64)
     for d, dd in enumerate(days):
         for k, v in dd.items():
             out[f"in.daily.{d}.{k}"] = np.asarray(v)
@@ -486,7 +512,7 @@ def write_days_case(ndays=3, jday0=172, seed=9):
         else:
             jax.random.uniform = saved[0]
         loops_gswp3._cast_tree_f32 = saved[1]
-    path = os.path.join(HERE, "days_16cells.npz")
+    path = os.path.join(HERE, "days_modules_16cells.npz" if modules else "days_16cells.npz")
     np.savez_compressed(path, **out)
     print(f"wrote {path}: {len(out)} arrays, {os.path.getsize(path)} bytes")
 
@@ -596,8 +622,10 @@ def main():
         write_observed_sw_case()
     if args.only in (None, "day_parts"):
         write_parts_case()
+    if args.only in (None, "days_modules"):
+        write_days_case(jday0=250, modules=True)
     if args.only in ("restart_leaves", "restart_1996", "diurnal", "days", "methane_month", "observed_sw",
-                     "day_parts"):
+                     "day_parts", "days_modules"):
         return
     for name, spec in CASES.items():
         if args.only and name != args.only:

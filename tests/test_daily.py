@@ -26,13 +26,17 @@ from oracle import weather as OW
 warnings.filterwarnings("ignore", category=RuntimeWarning)
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLD = os.path.join(HERE, "golden", "days_16cells.npz")
+GOLD_MODULES = os.path.join(HERE, "golden", "days_modules_16cells.npz")
+MODULE_LEAVES = {"acclim_x": "seasonal.acclim_x", "ssen_u": "seasonal.ssen_u", "ssen_l": "seasonal.ssen_l",
+                 "aystressu": "stress.aystressu", "aystressl": "stress.aystressl", "stress_nday": "stress.nday"}
+PARTS = ("et_trans", "et_interc", "et_soilev", "et_snowsub", "nee_night", "nee_day")
 CKPT = os.path.join(HERE, "golden", "restart_16cells.npz")
 ACC_CHECK = ("adrain", "adsnow", "adaet", "aynpp", "aynpptot", "aygpptot", "aytrunof", "aytdrain")
 STAT_CHECK = ("frac", "lai", "ztop", "zbot", "tco2mic")
 
 
-def load_case():
-    z = np.load(GOLD)
+def load_case(gold=GOLD):
+    z = np.load(gold)
     z = {k: z[k] for k in z.files}
     leaves, _, _ = restart.load(CKPT)
     n = int(np.asarray(leaves["soil.tg"]).shape[0])
@@ -42,6 +46,9 @@ def load_case():
     stat = dropin._leaf_dict(tree, "STAT", n)
     stat["f_inund"] = np.zeros(n)
     day = restart.group_from_leaves(leaves, "DAYST", n)
+    day["latitude"] = np.deg2rad(z["in.lat"])
+    for name, leaf in MODULE_LEAVES.items():
+        day[name] = z.get("in." + leaf, np.zeros(n))
     acc0 = restart.group_from_leaves(leaves, "ACC", n)
     P = StepParams()
     for name, _, _ in PARAM_FIELDS:
@@ -51,9 +58,12 @@ def load_case():
 
 
 def day_params(z):
+    """The case's day parameters; with the optional modules both switched on."""
     DP = DayParams()
     for name, _, _ in DAY_PARAM_FIELDS:
-        setattr(DP, name, z["in.dparam." + name])
+        if "in.dparam." + name in z:
+            setattr(DP, name, z["in.dparam." + name])
+    DP.seasonal_on = DP.stress_on = float(z.get("in.modules", 0))
     return DP
 
 
@@ -90,12 +100,13 @@ def hourly(z, d, n):
                            OW.uniform24(seed, cells, d, 2 + h), 3600.0, fira_obs=dd["fira"]) for h in range(24)]
 
 
-def oracle_days(ndays=None, perturb=None, f_inund=None):
-    """The oracle's day loop on the three-day case; yields (day, prog, dayst,
-    stat, acc) after each day.  ``perturb`` = (day, hour, eps) scales the
-    temperatures of the state by (1 + eps) before that hour; ``f_inund`` turns
-    on the hourly wetland CH4 with that inundated fraction."""
-    z, n, prog, stat, day, acc0, P = load_case()
+def oracle_days(ndays=None, perturb=None, f_inund=None, gold=GOLD):
+    """The oracle's day loop on a three-day case; yields (day, prog, dayst,
+    stat, acc) after each day.  ``perturb`` = (day, hour, eps[, fields])
+    scales the temperatures (or ``fields``) of the state by (1 + eps) before
+    that hour; ``f_inund`` turns on the hourly wetland CH4 with that
+    inundated fraction."""
+    z, n, prog, stat, day, acc0, P = load_case(gold)
     if f_inund is not None:
         P.flags |= FLAG_CH4
         stat["f_inund"] = np.asarray(f_inund, np.float64)
@@ -107,23 +118,83 @@ def oracle_days(ndays=None, perturb=None, f_inund=None):
     temps = ("tsoi", "tg", "tl", "tu", "ti", "tsno")
     for d in range(int(z["in.ndays"]) if ndays is None else ndays):
         dd = day_weather(z, d)
+        DP.jday = float(int(z["in.jday0"]) + d)
         day, stat, acc = OD.day_begin(day, stat, acc, dd["td"], P, DP)
         with np.errstate(all="ignore"):
             for h, F in enumerate(hourly(z, d, n)):
                 if perturb is not None and perturb[:2] == (d, h):
-                    prog = {k: v * (1.0 + perturb[2]) if k in temps else v for k, v in prog.items()}
+                    fields = perturb[3] if len(perturb) > 3 else temps
+                    prog = {k: v * (1.0 + perturb[2]) if k in fields else v for k, v in prog.items()}
                 prog, _, acc = oracle.step(prog, stat, F, P, acc)
         day, stat = OD.day_end(prog, day, stat, acc, dd["td"], P, DP)
         yield d, prog, day, stat, acc
 
 
-def test_oracle_day_loop_matches_reference_days():
-    z = load_case()[0]
-    for d, prog, day, stat, acc in oracle_days():
-        bad = compare(prog, want(z, d, "PROG"), 1e-9) + compare(day, want(z, d, "DAYST"), 1e-9)
-        bad += compare({k: stat[k] for k in STAT_CHECK}, want(z, d, "STAT"), 1e-9)
-        bad += compare({k: acc[k] for k in ACC_CHECK}, want(z, d, "ACC"), 1e-6)
+# Threshold cells of the modules case (three days from day 250): 1e-15
+# relative changes of the temperatures or of the water, ice and snow state before
+# hour 0 or hour 12 of the first day move cells 0, 3, 4 and 11 beyond 1e-9
+# within the three days (test_threshold_cells_of_the_modules_case); cell 0 by
+# 8e-7 on the third day.
+MODULE_THRESHOLD_CELLS = (0, 3, 4, 11)
+
+
+def _cells(x, cells, ref):
+    return {k: np.asarray(v)[list(cells)] for k, v in x.items() if k in ref}
+
+
+def _compare_day(z, d, prog, day, stat, acc, exempt=()):
+    """Every state field of day ``d`` against the case: 1e-9 (1e-6 for the
+    float32-summed accumulators) outside ``exempt``, 1e-2 on it."""
+    n = len(z["in.lat"])
+    keep = np.setdiff1d(np.arange(n), exempt)
+    wa = want(z, d, "ACC")
+    pairs = [(prog, want(z, d, "PROG"), 1e-9), (day, want(z, d, "DAYST"), 1e-9),
+             ({k: stat[k] for k in STAT_CHECK}, want(z, d, "STAT"), 1e-9),
+             ({k: acc[k] for k in ACC_CHECK + PARTS if k in wa}, wa, 1e-6)]
+    bad = []
+    for got, ref, tol in pairs:
+        bad += compare(_cells(got, keep, ref), _cells(ref, keep, ref), tol)
+        if len(exempt):
+            bad += compare(_cells(got, exempt, ref), _cells(ref, exempt, ref), 1e-2)
+    return bad
+
+
+@pytest.mark.parametrize("gold", [GOLD, GOLD_MODULES], ids=["base", "modules"])
+def test_oracle_day_loop_matches_reference_days(gold):
+    """The base case on every cell, and the case whose state carries the
+    optional modules (seasonal states with photoperiod-gated senescence,
+    growing-season stress sums, ET and NEE parts) outside its threshold cells:
+    every state field after each day."""
+    z = load_case(gold)[0]
+    exempt = MODULE_THRESHOLD_CELLS if gold == GOLD_MODULES else ()
+    checked = set()
+    for d, prog, day, stat, acc in oracle_days(gold=gold):
+        checked |= set(want(z, d, "DAYST"))
+        bad = _compare_day(z, d, prog, day, stat, acc, exempt)
         assert not bad, (d, bad[:6])
+    assert (set(MODULE_LEAVES) <= checked) == (gold == GOLD_MODULES)
+
+
+def test_threshold_cells_of_the_modules_case():
+    """The exempt cells of the modules case are threshold cells: over the three
+    days, 1e-15 perturbations (either sign) of the oracle's own temperatures or
+    of its water, ice and snow state, before hour 0 or hour 12 of the first day,
+    move exactly them beyond 1e-9."""
+    n = 16
+    base = list(oracle_days(gold=GOLD_MODULES))
+    moved = set()
+    cases = [(h, eps, f) for h in (0, 12) for eps in (-1e-15, 1e-15)
+             for f in (("tsoi", "tg", "tl", "tu", "ti", "tsno"), ("wsoi", "wisoi", "hsno", "wpud", "wipud", "fi"))]
+    for h, eps, fields in cases:
+        for (_, bp, bd, _, _), (_, pp, pd, _, _) in zip(base, oracle_days(gold=GOLD_MODULES,
+                                                                          perturb=(0, h, eps, fields))):
+            err = np.zeros(n)
+            for got, ref in ((pp, bp), (pd, bd)):
+                for k, w in ref.items():
+                    e = np.nan_to_num(rel_err(np.asarray(got[k], np.float64), np.asarray(w, np.float64), 1e-3))
+                    err = np.maximum(err, e.reshape(n, -1).max(axis=1))
+            moved |= set(np.nonzero(err > 1e-9)[0].tolist())
+    assert moved == set(MODULE_THRESHOLD_CELLS), sorted(moved)
 
 
 # Cells of the three-day case whose first day crosses a phase-change
@@ -150,11 +221,11 @@ def test_threshold_cells_of_the_day_case():
     assert moved == set(DAY_THRESHOLD_CELLS), sorted(moved)
 
 
-def _device_loop(dtype):
+def _device_loop(dtype, gold=GOLD):
     import torch
     from ibis_b200.columns import Columns
     from ibis_b200.daily import DayLoop
-    z, n, prog, stat, day, acc0, P = load_case()
+    z, n, prog, stat, day, acc0, P = load_case(gold)
     cols = Columns.from_host(prog, stat, dtype=dtype, acc=True)
     cols.set_acc({k: acc0[k] for k in ACC_CHECK + ("stresstu_last", "stresstl_last") if k in acc0})
     loop = DayLoop(cols, P, day_params(z), day, lat=z["in.lat"], seed=int(z["in.seed"]), jday=int(z["in.jday0"]),
@@ -175,13 +246,16 @@ def _device_state(cols, loop):
 
 
 @pytest.mark.gpu
-def test_device_day_kernels_match_oracle(cuda_lib):
+@pytest.mark.parametrize("gold", [GOLD, GOLD_MODULES], ids=["base", "modules"])
+def test_device_day_kernels_match_oracle(cuda_lib, gold):
     """ibis_day_begin_f64 / ibis_day_end_f64 on the oracle's own inputs of
-    each day of the three-day case: 1e-12 relative on everything they write."""
+    each day of a three-day case (with the optional modules: seasonal states,
+    photoperiod-gated phenology, stress sums): 1e-12 relative on everything
+    they write."""
     import torch
     from ibis_b200 import synth
-    z, n, cols, loop, torch = _device_loop(torch.float64)
-    _, _, prog, stat, day, acc0, P = load_case()
+    z, n, cols, loop, torch = _device_loop(torch.float64, gold)
+    _, _, prog, stat, day, acc0, P = load_case(gold)
     DP = day_params(z)
     acc = oracle.new_acc(n)
     for k in ACC_CHECK + ("stresstu_last", "stresstl_last"):
@@ -205,6 +279,7 @@ def test_device_day_kernels_match_oracle(cuda_lib):
     for d in range(int(z["in.ndays"])):
         dd = day_weather(z, d)
         load(prog, stat, day, acc)
+        DP.jday = loop.jday = int(z["in.jday0"]) + d
         day, stat, acc = OD.day_begin(day, stat, acc, dd["td"], P, DP)
         loop.begin(pad(dd["td"]))
         torch.cuda.synchronize()
@@ -219,6 +294,30 @@ def test_device_day_kernels_match_oracle(cuda_lib):
         torch.cuda.synchronize()
         bad = check(day, stat)
         assert not bad, ("end", d, bad[:6])
+
+
+@pytest.mark.gpu
+def test_device_day_loop_with_modules_matches_reference_days(cuda_lib):
+    """The device day loop in float64 on the case whose state carries the
+    optional modules (seasonal states with photoperiod-gated senescence of both
+    canopies, growing-season stress sums, ET and NEE parts) against the
+    reference's day loop after each of the three days: every state field
+    within 1e-9 (1e-6 for the float32-summed accumulators) outside the case's
+    threshold cells, which stay within 1e-2."""
+    import torch
+    from ibis_b200 import synth
+    z, n, cols, loop, torch = _device_loop(torch.float64, GOLD_MODULES)
+    assert loop.day_params.seasonal_on == 1.0 and loop.params.flags & (3 << 10)
+    for d in range(int(z["in.ndays"])):
+        dd, daily = _daily_tensor(z, d, cols.ld, torch)
+        hours = hourly(z, d, n)
+        forc = {k: np.stack([F[k] for F in hours]) for k in hours[0]}
+        td = torch.from_numpy(np.pad(dd["td"], (0, cols.ld - n))).cuda()
+        loop.run_day(daily, forc=torch.from_numpy(synth.forcing_planes(forc, cols.ld, dtype=np.float64)).cuda(), td=td)
+        torch.cuda.synchronize()
+        prog, dayst, stat, acc = _device_state(cols, loop)
+        bad = _compare_day(z, d, prog, dayst, stat, acc, MODULE_THRESHOLD_CELLS)
+        assert not bad, (d, bad[:6])
 
 
 @pytest.mark.gpu
@@ -395,18 +494,24 @@ sys.path.insert(0, "{golden}/jaxshim"); sys.path.insert(0, "{ref}"); sys.path.in
 import make_golden as mg
 from ibis_b200 import dropin
 from ibis_b200.params import DAY_PARAM_FIELDS
+from ibis_b200.params import DayParams
 z = np.load("{gold}")
-dp = dropin.day_params(mg.loops.default_sim_params(16))
-for name, n, _ in DAY_PARAM_FIELDS:
-    assert np.allclose(np.asarray(getattr(dp, name), float), z["in.dparam." + name], rtol=0, atol=0), name
+sp = mg.loops.default_sim_params(16)
+dp, defaults = dropin.day_params(sp), DayParams()
+for name, path in dropin.DAY_PARAM_PATHS.items():
+    assert dropin._get(dict(params=sp), path) is not None, path
+    v = np.asarray(getattr(dp, name), float)
+    ref = z["in.dparam." + name] if "in.dparam." + name in z.files else np.asarray(getattr(defaults, name), float)
+    assert np.array_equal(v, ref), name
 print("day mapping ok")
 """
 
 
 @pytest.mark.skipif(not os.path.isdir("/root/reference/python-port"), reason="reference sources not present")
 def test_day_param_paths_against_reference_objects():
-    """dropin.DAY_PARAM_PATHS reads the reference's own SimParams to the values
-    the three-day fixture was run with."""
+    """dropin.DAY_PARAM_PATHS resolves every path on the reference's own
+    SimParams, to the values the three-day fixture was run with and, for the
+    module parameters, to the defaults DayParams restates."""
     import subprocess
     import sys
     code = _DAY_MAP_CHECK.format(golden=os.path.join(HERE, "golden"), ref="/root/reference/python-port",
@@ -434,6 +539,8 @@ def _param_tree(z, lat_deg):
             v = z["in.param." + name]
             put(root, path, v if np.size(v) > 1 else float(v))
     for name, path in dropin.DAY_PARAM_PATHS.items():
+        if "in.dparam." + name not in z:
+            continue
         v = z["in.dparam." + name]
         put(root, path, v if np.size(v) > 1 else float(v))
     put(root, "params.latitude", np.deg2rad(lat_deg))
@@ -493,7 +600,10 @@ def test_run_month_scan_dropin_equals_day_loop(cuda_lib):
         assert np.array_equal(np.asarray(v), mine.reshape(np.shape(v))), f.name
     dayst = loop.dayst_host()
     for f in L.DAYST:
-        v = np.asarray(dropin._get({"s": new}, "s." + f.leaf), np.float64)
+        v = dropin._get({"s": new}, "s." + f.leaf)
+        if v is None:                   # the optional modules, and the latitude (a parameter)
+            continue
+        v = np.asarray(v, np.float64)
         assert np.array_equal(v.reshape(-1), np.asarray(dayst[f.name], np.float32).astype(np.float64).reshape(-1)), \
             f.name
     ay0 = np.asarray(leaves["summary.ayaet"], np.float64)
@@ -503,3 +613,65 @@ def test_run_month_scan_dropin_equals_day_loop(cuda_lib):
     for k in ("tempu", "templ", "agddu", "agddl", "a10td", "ayprcp", "csoipas", "totcsoi"):
         e = np.abs(np.asarray(dayst[k]) - w[k]) / np.maximum(np.abs(w[k]), 1e-3)
         assert e.max() < 1e-4, (k, float(e.max()))
+
+
+@pytest.mark.gpu
+def test_run_month_scan_dropin_with_state_modules(cuda_lib):
+    """dropin.run_month_scan over a float32 state tree that carries the
+    reference's optional modules (seasonal, stress, ET parts, NEE parts) and
+    parameters with photoperiod-gated senescence: the modules advance and are
+    written back.  Against the reference's float64 run of the same three days:
+    the seasonal states (functions of the daily mean temperature and the day
+    length) within 1e-5, the day counts exact, the stress sums within 1e-3
+    (the stress of the float32 step), transpiration and interception loss
+    within 1e-3 of their largest magnitude on 90 % of the cells, the net NEE
+    within 2e-2 of its largest magnitude, and the four ET parts summing to the
+    AET booked over the days.  The float64
+    day loop checks every part against the reference to 1e-9
+    (test_device_day_loop_with_modules_matches_reference_days)."""
+    from ibis_b200 import dropin
+    z = load_case(GOLD_MODULES)[0]
+    n, nd = 16, int(z["in.ndays"])
+    leaves, _, _ = restart.load(CKPT)
+    state = restart.as_tree({k: (np.asarray(v).copy() if v is not None else None) for k, v in leaves.items()})
+    for k in ("z0sno", "rhos", "consno", "hsnotop", "hsnomin", "fimin", "fimax"):
+        setattr(state.snow, k, np.float32(z["in.param." + k]))
+    f = lambda leaf: np.asarray(z["in." + leaf], np.float32)
+    state.seasonal = types.SimpleNamespace(acclim_x=f("seasonal.acclim_x"), ssen_u=f("seasonal.ssen_u"),
+                                           ssen_l=f("seasonal.ssen_l"))
+    state.stress = types.SimpleNamespace(aystressu=f("stress.aystressu"), aystressl=f("stress.aystressl"),
+                                         nday=f("stress.nday"), u_smooth=np.zeros(n, np.float32))
+    zero = np.zeros(n, np.float32)
+    state.etparts = types.SimpleNamespace(trans=zero, interc=zero, soilev=zero, snowsub=zero)
+    state.neeparts = types.SimpleNamespace(night=zero, day=zero)
+    consts, params = _param_tree(z, z["in.lat"])
+    assert params.pheno.sen_photoperiod_u == 1.0
+    days = [day_weather(z, d) for d in range(nd)]
+    xs = tuple(np.stack([dd[k] for dd in days]) for k in ("td", "tmax", "tmin", "cloud", "precip", "psurf", "qd",
+                                                         "ud")) + (np.zeros((nd, n)),
+                                                                   np.stack([dd["fira"] for dd in days]),
+                                                                   int(z["in.jday0"]) + np.arange(nd))
+    new, _ = dropin.run_month_scan(state, consts, params, xs, 1, 365, 3600.0, seed=int(z["in.seed"]))
+    w = lambda leaf: z[f"out.{nd - 1}.{leaf}"]
+    for leaf in ("seasonal.acclim_x", "seasonal.ssen_u", "seasonal.ssen_l"):
+        np.testing.assert_allclose(dropin._get({"s": new}, "s." + leaf), w(leaf), rtol=1e-5, atol=1e-4, err_msg=leaf)
+    np.testing.assert_array_equal(new.stress.nday, w("stress.nday"))
+    for leaf in ("stress.aystressu", "stress.aystressl"):
+        np.testing.assert_allclose(dropin._get({"s": new}, "s." + leaf), w(leaf), rtol=0, atol=1e-3, err_msg=leaf)
+    assert np.any(new.seasonal.ssen_u >= 25.0) and np.any(new.seasonal.ssen_u == 0.0)
+    close = lambda g, ref: np.mean(np.abs(g - ref) <= 1e-3 * max(float(np.abs(ref).max()), 1e-30)) >= 0.9
+    for leaf in ("etparts.trans", "etparts.interc"):
+        assert close(np.asarray(dropin._get({"s": new}, "s." + leaf), np.float64), w(leaf)), leaf
+    # an hour whose float32 sun height sits at the horizon books its NEE to the
+    # other side of the night/day split, and the net is a small difference of
+    # GPP-sized terms: the sum is compared, within 2e-2 of its largest magnitude
+    net = np.asarray(new.neeparts.night, np.float64) + new.neeparts.day
+    net_ref = w("neeparts.night") + w("neeparts.day")
+    assert np.all(np.abs(net - net_ref) <= 2e-2 * np.abs(net_ref).max()), np.abs(net - net_ref).max()
+    # soil evaporation and snow sublimation split on the snow cover, which the
+    # float32 day with generated forcing moves in single cells; their sum with
+    # the other two parts is the AET the state booked over the days
+    et = sum(np.asarray(getattr(new.etparts, k), np.float64) for k in ("trans", "interc", "soilev", "snowsub"))
+    np.testing.assert_allclose(et, np.asarray(new.summary.ayaet, np.float64) - leaves["summary.ayaet"],
+                               rtol=1e-4, atol=1e-4)
+    assert state.seasonal.acclim_x is not new.seasonal.acclim_x
