@@ -34,7 +34,7 @@ from . import restart as _restart
 from . import synth
 from .columns import Columns
 from .forcing import OBSERVED_FIRA, hourly_forcing
-from .params import FLAG_ACC, FLAG_CH4, DayParams, StepParams
+from .params import FLAG_ACC, FLAG_CH4, FLAG_ETPARTS, FLAG_NEEPARTS, DayParams, StepParams
 
 _TD = L.OFF["DAILY"]["td"][0]
 MONTH_NEW_YEAR, MONTH_FROM_MEAN, MONTH_PARTITION = 1, 2, 4
@@ -93,7 +93,10 @@ class DayLoop:
                      day_params: DayParams | None = None, **kw):
         """A day loop seeded from a reference checkpoint: the columns, the
         daily-cadence state, the running sums, and the last hour's soil-water
-        stress the next day's phenology reads (:meth:`save` writes them back)."""
+        stress the next day's phenology reads, and the optional modules the
+        checkpoint carries -- wetland CH4 state, stress sums, ET and NEE parts,
+        seasonal states -- which then keep advancing (:meth:`save` writes them
+        all back)."""
         cols, P, leaves, meta, extra = _restart.columns_from_restart(path, dtype=dtype, device=device,
                                                                      params=params, acc=True)
         n = cols.ncell
@@ -102,7 +105,15 @@ class DayLoop:
         acc0 = _restart.group_from_leaves(leaves, "ACC", n)
         cols.set_acc({k: v for k, v in acc0.items() if not k.startswith("a10anc")})
         dayst = _restart.group_from_leaves(leaves, "DAYST", n)
-        loop = cls(cols, P, day_params or DayParams(), dayst, **kw)
+        # the optional modules the checkpoint carries keep advancing
+        DP = copy.deepcopy(day_params or DayParams())
+        DP.seasonal_on = float("seasonal.acclim_x" in leaves)
+        DP.stress_on = float("stress.nday" in leaves)
+        P.flags |= (FLAG_ETPARTS if "etparts.trans" in leaves else 0) | \
+            (FLAG_NEEPARTS if "neeparts.night" in leaves else 0)
+        loop = cls(cols, P, DP, dayst, **kw)
+        if "wetland.flux" in leaves:
+            loop.set_wet(_restart.group_from_leaves(leaves, "WET", n))
         loop.checkpoint = (leaves, meta, extra)
         return loop
 
@@ -128,7 +139,9 @@ class DayLoop:
         # between days the reference keeps the 10-day means in the leaves the
         # step uses for daily sums: the DAYST values go last and win
         acc = {k: v for k, v in acc.items() if not k.startswith("a10anc")}
+        wet = self.wet_host() if "wetland.flux" in leaves else {}
         groups = [("PROG", c.prog_host()), ("STAT", {k: stat[k] for k in self._STAT_WRITTEN}), ("ACC", acc),
+                  ("WET", {k: v for k, v in wet.items() if k != "rh0"}),
                   ("DAYST", self.dayst_host())]
         _restart.write_state(path, leaves, groups, meta, extra)
 

@@ -18,10 +18,16 @@ with no JAX present:
   ``load_state`` reads, with the prognostic (and, if kept, diagnostic) leaves
   taken from the columns and every other leaf carried over.
 
-Only the base state is mapped.  A checkpoint that also carries optional
-trailing modules (permafrost, wetland, fire, accumulators of the calibration
-chain) keeps them untouched: they follow the base leaves and are copied
-through by position.
+After the base leaves a checkpoint can carry optional modules, in the
+state's field order (state/model_state.py:40-63).  Those the day loop uses are
+named by their count, as the reference's loader identifies them
+(io/restart.py:60-62, 94-133): the wetland CH4 state (3 leaves; a saved tree
+structure naming ``MethaneState`` settles it, else the count), then the chain
+of calibration modules, each implying the ones before it -- StressAccum (4
+leaves; 3 in files written before its smoothed-stress leaf), ETParts,
+SeasonalState, NEEParts (0, 4, 8, 11 or 13 leaves; 3, 7, 10 or 12 in the old
+form).  Trailing leaves that no such count explains (permafrost, fire, BVOC
+modules) are kept untouched and copied through by position.
 """
 from __future__ import annotations
 
@@ -36,6 +42,39 @@ from .restart_leaves import LEAVES
 BEDROCK_LEAF = "soil.tsoi_deep"
 
 
+WETLAND_LEAVES = ("wetland.flux", "wetland.annual", "wetland.zwt")
+CHAIN = (("stress.aystressu", "stress.aystressl", "stress.nday", "stress.u_smooth"),
+         ("etparts.trans", "etparts.interc", "etparts.soilev", "etparts.snowsub"),
+         ("seasonal.acclim_x", "seasonal.ssen_u", "seasonal.ssen_l"),
+         ("neeparts.night", "neeparts.day"))
+TRAILING = WETLAND_LEAVES + tuple(p for mod in CHAIN for p in mod)
+OLD_STRESS_LEAVES = 3
+
+
+def _chain_names(n: int, old: bool):
+    """Leaf names of a chain of ``n`` leaves (``old``: the 3-leaf StressAccum), or None."""
+    names = []
+    for k, mod in enumerate(CHAIN):
+        if len(names) >= n:
+            break
+        names += list(mod[:OLD_STRESS_LEAVES] if old and k == 0 else mod)
+    return names if len(names) == n else None
+
+
+def trailing_names(n: int, treedef_repr: str | None = None):
+    """Names of the ``n`` leaves after the base state, or None when the count
+    (and the saved tree structure) does not identify them."""
+    chain = lambda m: m >= 0 and (_chain_names(m, False) is not None or _chain_names(m, True) is not None)
+    wet = ("MethaneState" in treedef_repr) if treedef_repr is not None else (not chain(n) and chain(n - 3))
+    rest = n - (len(WETLAND_LEAVES) if wet else 0)
+    if rest < 0:
+        return None
+    names = _chain_names(rest, False) or _chain_names(rest, True)
+    if names is None:
+        return None
+    return (list(WETLAND_LEAVES) if wet else []) + names
+
+
 def _soil_leaf_count(treedef_repr: str):
     """Children of the SoilState node in a saved tree structure, or None."""
     m = re.search(r"SoilState\[[^\]]*\], \[([^\]]*)\]", treedef_repr)
@@ -48,9 +87,9 @@ def base_leaves(bedrock: bool):
 
 
 def load(path: str):
-    """Read a checkpoint.  Returns ``(leaves, meta, extra)``: the base leaves by
-    path, the ``meta_*`` entries, and the trailing leaves of optional modules
-    (a list, by position)."""
+    """Read a checkpoint.  Returns ``(leaves, meta, extra)``: the base leaves and
+    the named optional modules (:func:`trailing_names`) by path, the ``meta_*``
+    entries, and trailing leaves no count identifies (a list, by position)."""
     z = np.load(path, allow_pickle=False)
     n = int(z["num_leaves"])
     arrays = [None if f"leaf_{i}_is_none" in z.files else z[f"leaf_{i}"] for i in range(n)]
@@ -67,16 +106,24 @@ def load(path: str):
         raise ValueError(f"{path}: {n} leaves, the base state has {len(names)}")
     leaves = dict(zip(names, arrays[:len(names)]))
     meta = {k[5:]: (z[k].item() if z[k].ndim == 0 else z[k]) for k in z.files if k.startswith("meta_")}
-    return leaves, meta, arrays[len(names):]
+    trail = arrays[len(names):]
+    tnames = trailing_names(len(trail), str(z["treedef_repr"]) if "treedef_repr" in z.files else None)
+    if tnames is None:
+        return leaves, meta, trail
+    leaves.update(zip(tnames, trail))
+    return leaves, meta, []
 
 
 def save(path: str, leaves: dict, meta: dict | None = None, extra=None, treedef_repr: str | None = None):
-    """Write ``leaves`` (base state by path, bedrock leaf optional) in the reference's checkpoint format."""
+    """Write ``leaves`` (base state by path, bedrock leaf optional, then the
+    named optional modules present, in the state's order) and ``extra`` in the
+    reference's checkpoint format."""
     bedrock = leaves.get(BEDROCK_LEAF) is not None
     names = base_leaves(bedrock)
     missing = [p for p in names if p not in leaves]
     if missing:
         raise ValueError(f"leaves missing from the state: {missing[:5]}")
+    names = names + [p for p in TRAILING if p in leaves]
     arrays = [leaves[p] for p in names] + list(extra or [])
     out = {"num_leaves": np.asarray(len(arrays))}
     if treedef_repr is not None:

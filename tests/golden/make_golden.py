@@ -357,6 +357,42 @@ def write_restart_subset(ncell=16):
     print(f"wrote {path}: {os.path.getsize(path)} bytes")
 
 
+def write_restart_modules_case(seed=31):
+    """tests/golden/restart_modules_16cells.npz: the reference's own
+    ``save_state`` (io/restart.py:19-52) of the 16-cell checkpoint's state with
+    the wetland CH4 state and the four calibration modules (stress, ET parts,
+    seasonal, NEE parts) attached, every module leaf filled with distinct
+    seeded values, recorded by leaf path in restart_modules_values.npz.  The
+    NumPy stand-in for ``jax`` has no JAX tree-structure text, so that entry
+    is dropped: readers identify the modules by their leaf count, as the
+    reference's ``load_state`` does for files without it (io/restart.py:109-115)."""
+    from ibis.io.restart import load_state, save_state
+    from ibis.bgc.methane import create_methane_state
+    n = 16
+    st, _ = load_state(os.path.join(HERE, "restart_16cells.npz"),
+                       create_ibis_state(GridConfig(nlon=1, nlat=1, npoi=n, nbedrock=3), with_neeparts=True))
+    st = eqx.tree_at(lambda s: s.wetland, st, create_methane_state(n), is_leaf=lambda x: x is None)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    values = {}
+    modules = (("wetland", ("flux", "annual", "zwt")), ("stress", ("aystressu", "aystressl", "nday", "u_smooth")),
+               ("etparts", ("trans", "interc", "soilev", "snowsub")), ("seasonal", ("acclim_x", "ssen_u", "ssen_l")),
+               ("neeparts", ("night", "day")))
+    for mod, names in modules:
+        vals = tuple(rng.uniform(0.1, 10.0, n).astype(np.float32) for _ in names)
+        st = eqx.tree_at(lambda s, mod=mod, names=names: tuple(getattr(getattr(s, mod), k) for k in names), st,
+                         tuple(jnp.asarray(v) for v in vals))
+        values.update({f"value.{mod}.{k}": v for k, v in zip(names, vals)})
+    path = os.path.join(HERE, "restart_modules_16cells.npz")
+    tmp = path[:-4] + "_tmp.npz"
+    save_state(st, tmp, metadata={"year": 1996})
+    z = np.load(tmp, allow_pickle=False)
+    out = {k: z[k] for k in z.files if k != "treedef_repr"}
+    os.remove(tmp)
+    np.savez_compressed(path, **out)
+    np.savez_compressed(os.path.join(HERE, "restart_modules_values.npz"), **values)
+    print(f"wrote {path}: {int(out['num_leaves'])} leaves, {os.path.getsize(path)} bytes")
+
+
 def daily_inputs(ncell=12, seed=16):
     """Seeded daily weather for the diurnal fixture: warm and cold days, dry,
     wet and very wet days (an event longer than the random length), humidity
@@ -624,8 +660,10 @@ def main():
         write_parts_case()
     if args.only in (None, "days_modules"):
         write_days_case(jday0=250, modules=True)
+    if args.only in (None, "restart_modules"):
+        write_restart_modules_case()
     if args.only in ("restart_leaves", "restart_1996", "diurnal", "days", "methane_month", "observed_sw",
-                     "day_parts", "days_modules"):
+                     "day_parts", "days_modules", "restart_modules"):
         return
     for name, spec in CASES.items():
         if args.only and name != args.only:

@@ -449,6 +449,49 @@ def test_day_loop_from_checkpoint_and_back(cuda_lib, tmp_path):
 
 
 @pytest.mark.gpu
+def test_day_loop_from_checkpoint_with_modules(cuda_lib, tmp_path):
+    """A checkpoint that carries the wetland state and the four calibration
+    modules (the reference's own save_state): DayLoop.from_restart switches the
+    modules on and loads the wetland planes; after one float64 day DayLoop.save
+    writes the modules back advanced as the day loop advances them -- the
+    acclimation state relaxed toward the day's temperature, the stress sums and
+    day count grown by the last hour's stress and one day (the default
+    threshold counts every day), the ET parts grown by the day's AET -- and
+    the wetland state and smoothed stress as they were."""
+    import torch
+    from ibis_b200.daily import DayLoop
+    from ibis_b200.params import FLAG_ETPARTS, FLAG_NEEPARTS
+    z, n, prog, stat, day, acc0, P = load_case()
+    ckpt = os.path.join(HERE, "golden", "restart_modules_16cells.npz")
+    leaves0, _, _ = restart.load(ckpt)
+    loop = DayLoop.from_restart(ckpt, dtype=torch.float64, params=P, day_params=day_params(z), lat=z["in.lat"],
+                                seed=int(z["in.seed"]), jday=int(z["in.jday0"]), day=0)
+    assert loop.day_params.seasonal_on == 1.0 and loop.day_params.stress_on == 1.0
+    assert loop.params.flags & FLAG_ETPARTS and loop.params.flags & FLAG_NEEPARTS
+    np.testing.assert_array_equal(loop.wet_host()["zwt"], leaves0["wetland.zwt"])
+    dd, daily = _daily_tensor(z, 0, loop.cols.ld, torch)
+    ay0 = loop.dayst_host()["ayaet"].copy()
+    loop.run_day(daily)
+    torch.cuda.synchronize()
+    acc = loop.cols.acc_host()
+    loop.save(str(tmp_path / "ck.npz"))
+    back, _, extra = restart.load(str(tmp_path / "ck.npz"))
+    assert extra == []
+    f64 = lambda k: np.asarray(back[k], np.float64)
+    x0 = np.asarray(leaves0["seasonal.acclim_x"], np.float64)
+    np.testing.assert_allclose(f64("seasonal.acclim_x"), x0 + (dd["td"] - 273.16 - x0) / 10.93, rtol=1e-6)
+    np.testing.assert_array_equal(back["stress.nday"], (np.asarray(leaves0["stress.nday"], np.float64) + 1.0)
+                                  .astype(np.asarray(leaves0["stress.nday"]).dtype))
+    np.testing.assert_allclose(f64("stress.aystressu"), np.asarray(leaves0["stress.aystressu"], np.float64)
+                               + acc["stresstu_last"], rtol=1e-6)
+    et = sum(f64("etparts." + k) - np.asarray(leaves0["etparts." + k], np.float64)
+             for k in ("trans", "interc", "soilev", "snowsub"))
+    np.testing.assert_allclose(et, loop.dayst_host()["ayaet"] - ay0, rtol=1e-5, atol=1e-5)
+    for k in ("wetland.flux", "wetland.annual", "wetland.zwt", "stress.u_smooth"):
+        np.testing.assert_array_equal(back[k], leaves0[k], err_msg=k)
+
+
+@pytest.mark.gpu
 def test_device_month_matches_oracle_month(cuda_lib):
     """Three days as a month with hourly wetland CH4: ibis_month_begin, the
     device day loop in float64, ibis_month_end (mean of the hourly fluxes, the

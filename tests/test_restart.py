@@ -43,7 +43,7 @@ def test_save_load_round_trip(tmp_path):
     leaves, meta, extra = restart.load(FIXTURE)
     leaves["soil.tg"] = leaves["soil.tg"] + 1.0
     p = tmp_path / "ck.npz"
-    restart.save(str(p), leaves, meta, extra=[np.arange(3.0)])
+    restart.save(str(p), leaves, meta, extra=[np.arange(3.0)])      # one trailing leaf: no module count
     back, meta2, extra2 = restart.load(str(p))
     assert meta2 == meta and len(extra2) == 1 and np.array_equal(extra2[0], np.arange(3.0))
     for k in restart.LEAVES:
@@ -52,6 +52,85 @@ def test_save_load_round_trip(tmp_path):
     restart.save(str(p), nobed, meta)
     back, _, _ = restart.load(str(p))
     assert restart.BEDROCK_LEAF not in back and len(back) == 257
+
+
+MODULES = os.path.join(HERE, "golden", "restart_modules_16cells.npz")
+MODULE_VALUES = os.path.join(HERE, "golden", "restart_modules_values.npz")
+
+
+def test_trailing_names_follow_the_module_chain():
+    """The optional modules after the base leaves are named by their count as
+    the reference's loader identifies them: the calibration chain (stress, ET
+    parts, seasonal, NEE parts; the old 3-leaf stress form), with the wetland
+    state before it where the saved tree structure names it or the count
+    leaves no other reading."""
+    chain = [p for mod in restart.CHAIN for p in mod]
+    old = chain[:3] + chain[4:]
+    for n in (0, 4, 8, 11, 13):
+        assert restart.trailing_names(n) == chain[:n]
+    for n in (3, 7, 10, 12):
+        assert restart.trailing_names(n) == old[:n]
+    wet = list(restart.WETLAND_LEAVES)
+    assert restart.trailing_names(16) == wet + chain and restart.trailing_names(11 + 3) == wet + chain[:11]
+    assert restart.trailing_names(7, "CustomNode(MethaneState[()], [*, *, *])") == wet + chain[:4]
+    assert restart.trailing_names(7) == old[:7]            # without the structure: the old chain, as the reference
+    assert restart.trailing_names(6) == wet + old[:3]
+    for n in (1, 2, 5, 9, 20):
+        assert restart.trailing_names(n) is None, n
+
+
+def test_modules_checkpoint_round_trip(tmp_path):
+    """The reference's own checkpoint with the wetland state and the four
+    calibration modules attached: every module leaf read by name with the
+    values the reference saved, and written back in the same order."""
+    leaves, meta, extra = restart.load(MODULES)
+    want = np.load(MODULE_VALUES)
+    assert extra == [] and len(leaves) == 258 + 16
+    for k in want.files:
+        assert np.array_equal(np.asarray(leaves[k[len("value."):]]), want[k]), k
+    leaves["seasonal.ssen_u"] = leaves["seasonal.ssen_u"] + 1.0
+    p = tmp_path / "ck.npz"
+    restart.save(str(p), leaves, meta)
+    z = np.load(str(p))
+    ref = np.load(MODULES)
+    assert int(z["num_leaves"]) == int(ref["num_leaves"])
+    i = restart.LEAVES.index("soil.tg")
+    assert np.array_equal(z[f"leaf_{i}"], ref[f"leaf_{i}"])
+    back, _, _ = restart.load(str(p))
+    assert np.array_equal(back["seasonal.ssen_u"], want["value.seasonal.ssen_u"] + 1.0)
+
+
+_MODULES_REF_CHECK = r"""
+import sys, numpy as np
+sys.path.insert(0, "{golden}/jaxshim"); sys.path.insert(0, "{ref}"); sys.path.insert(0, "{repo}")
+from ibis.dimensions import GridConfig
+from ibis.state.model_state import create_ibis_state
+from ibis.io.restart import load_state
+from ibis_b200 import restart
+leaves, meta, extra = restart.load("{src}")
+for k in [k for k in leaves if k.split(".")[0] in ("wetland", "stress", "etparts", "seasonal", "neeparts")]:
+    leaves[k] = (np.asarray(leaves[k]) * 2.0 + 1.0).astype(np.float32)
+restart.save("{dst}", leaves, meta)
+st, m = load_state("{dst}", create_ibis_state(GridConfig(nlon=1, nlat=1, npoi=16, nbedrock=3), with_neeparts=True))
+n = 0
+for k, v in leaves.items():
+    mod, leaf = k.split(".")
+    if mod in ("wetland", "stress", "etparts", "seasonal", "neeparts"):
+        assert np.array_equal(np.asarray(getattr(getattr(st, mod), leaf)), v), k
+        n += 1
+print("modules ok", n)
+"""
+
+
+@pytest.mark.skipif(not os.path.isdir("/root/reference/python-port"), reason="reference sources not present")
+def test_saved_modules_load_in_the_reference(tmp_path):
+    """A checkpoint with the modules written here loads in the reference's own
+    ``load_state`` (wetland state attached by it from the count) with every
+    module leaf as written."""
+    code = _MODULES_REF_CHECK.format(golden=os.path.join(HERE, "golden"), ref="/root/reference/python-port",
+                                     repo=os.path.dirname(HERE), src=MODULES, dst=str(tmp_path / "ck.npz"))
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0 and "modules ok 16" in r.stdout, r.stderr[-3000:]
 
 
 _REF_CHECK = r"""
