@@ -715,7 +715,7 @@ def main():
     ap.add_argument("--duration", type=float, default=10.0)
     ap.add_argument("--epoch-hours", type=int, default=168)
     ap.add_argument("--e2e-chunk", default="auto",
-                    help="hours per host-to-device forcing chunk in the e2e path ('auto': 2 hours, growing by half)")
+                    help="hours per host-to-device forcing chunk in the e2e path ('auto': 4 hours, growing by 1.75)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)

@@ -137,14 +137,33 @@ __device__ __forceinline__ bool acc_plane_used(int p, unsigned flags) {
     return (flags & IBIS_FLAG_ACC) != 0;
 }
 
+// The planes move in batches of kAccMoveBatch: all loads of a batch are issued
+// before its stores, so a thread has that many global loads in flight instead
+// of waiting out one load latency per plane at the start of every launch.
+constexpr int kAccMoveBatch = 16;
+
 template <typename R, bool TO_SMEM>
 __device__ __forceinline__ void acc_move(R* __restrict__ g, int ld, R* __restrict__ sacc, int sld, unsigned flags) {
+    constexpr int kPlanes = 2 * kAccOnChip;
+    auto global_plane = [](int p) { return p < kAccOnChip ? p : p - kAccOnChip + IBIS_ACC_COUNT; };
 #pragma unroll 1
-    for (int p = 0; p < 2 * kAccOnChip; ++p) {
-        const int gp = p < kAccOnChip ? p : p - kAccOnChip + IBIS_ACC_COUNT;     // the plane in the global buffer
-        if (!acc_plane_used(gp, flags)) continue;
-        if (TO_SMEM) sacc[p * sld] = g[(size_t)gp * ld];
-        else g[(size_t)gp * ld] = sacc[p * sld];
+    for (int p0 = 0; p0 < kPlanes; p0 += kAccMoveBatch) {
+        R v[kAccMoveBatch];
+        bool use[kAccMoveBatch];
+#pragma unroll
+        for (int j = 0; j < kAccMoveBatch; ++j) {
+            const int p = p0 + j;
+            use[j] = p < kPlanes && acc_plane_used(global_plane(p), flags);
+            if (TO_SMEM) v[j] = use[j] ? g[(size_t)global_plane(p) * ld] : R(0.0);
+            else v[j] = use[j] ? sacc[p * sld] : R(0.0);
+        }
+#pragma unroll
+        for (int j = 0; j < kAccMoveBatch; ++j) {
+            const int p = p0 + j;
+            if (!use[j]) continue;
+            if (TO_SMEM) sacc[p * sld] = v[j];
+            else g[(size_t)global_plane(p) * ld] = v[j];
+        }
     }
 }
 
