@@ -59,16 +59,45 @@ def _algorithmic_bytes(nhours):
 
 
 class ClockSampler:
-    """nvidia-smi sampling of SM clocks and throttle reasons during a timed region."""
+    """SM clocks and clock-event (throttle) reasons sampled during a timed
+    region: NVML read every 2 ms from a thread (reads only), with the
+    nvidia-smi query as the fallback where NVML cannot be loaded."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.proc = None
+        self.rows = []
+        self.thread = None
+
+    def _poll(self, nv, h, bits):
+        while not self.stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.rows.append((float(sm), float(mx), [n for n, bit in zip(self.NAMES, bits) if r & bit]))
+            except Exception:
+                return
+            self.stop.wait(0.002)
 
     def __enter__(self):
+        import threading
+        self.stop = threading.Event()
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            h = nv.nvmlDeviceGetHandleByIndex(int(self.gpu))
+            bits = (nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap)
+            self.thread = threading.Thread(target=self._poll, args=(nv, h, bits), daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.thread = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
                                           "--format=csv,noheader,nounits", "-lms", "100"],
@@ -79,6 +108,9 @@ class ClockSampler:
 
     def __exit__(self, *a):
         self.out = ""
+        if self.thread is not None:
+            self.stop.set()
+            self.thread.join(timeout=5)
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -87,19 +119,17 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        rows = []
+        rows = list(self.rows)
         for line in (self.out or "").strip().splitlines():
             p = [x.strip() for x in line.split(",")]
-            if len(p) >= 9:
-                rows.append(p)
+            if len(p) >= 9 and p[1].replace(".", "").isdigit() and p[2].replace(".", "").isdigit():
+                rows.append((float(p[1]), float(p[2]),
+                             [n for i, n in enumerate(self.NAMES) if p[5 + i].lower().startswith("active")]))
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mxs = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mxs) if mxs else None,
-                "reasons": reasons, "samples": len(rows)}
+        return {"sm_mhz": float(np.median([r[0] for r in rows])), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": sorted({n for r in rows for n in r[2]}), "samples": len(rows),
+                "source": "nvml" if self.rows else "nvidia-smi"}
 
 
 def cpu_baseline_sample(ncell=16384, hours=HOURS, seed=123):
