@@ -266,3 +266,42 @@ def test_ensemble_day_loop_matches_day_loop_on_columns(cuda_lib):
         assert np.mean(e <= 1e-3) >= 0.9, (k, float(e.max()))
     p1 = edl.prog.cpu().numpy()[:, runs0 + 1]
     assert np.isfinite(p1).all() and not np.array_equal(p1, x)
+
+
+@pytest.mark.gpu
+def test_ensemble_day_loop_advances_state_modules(cuda_lib):
+    """EnsembleDayLoop with the daily cadence's optional modules on (seasonal
+    states with photoperiod-gated senescence of the upper canopy, growing-season
+    stress sums): per run, the same module states as DayLoop on the same sites
+    as columns -- the seasonal states (functions of the day's temperature, the
+    latitude and the day of year) within 1e-6, the day counts exact, the
+    stress sums within 1e-3 on 90 % of the runs."""
+    from ibis_b200.daily import DayLoop
+    from ibis_b200.ensemble_daily import EnsembleDayLoop
+    from ibis_b200.forcing import daily_planes
+    from ibis_b200.params import DayParams
+    rng = np.random.Generator(np.random.PCG64(22))
+    nsite, nday = 12, 3
+    lat = rng.uniform(-40.0, 70.0, nsite)
+    stat = synth.make_columns(rng, nsite, 1.0)
+    F0 = {k: v[0] for k, v in synth.make_forcing(rng, lat, 1, start_doy=250).items()}
+    prog = synth.make_initial(rng, stat, F0)
+    dayst = synth.make_dayst(rng, stat, lat)
+    dayst.update(acclim_x=rng.uniform(0.0, 20.0, nsite), ssen_u=rng.uniform(0.0, 30.0, nsite),
+                 ssen_l=rng.uniform(0.0, 30.0, nsite), stress_nday=np.floor(rng.uniform(0.0, 50.0, nsite)))
+    daily = synth.make_daily_weather(rng, lat, nday)
+    P = StepParams(co2conc=390.0e-6)
+    DP = DayParams(seasonal_on=1.0, stress_on=1.0, sen_photoperiod_u=1.0, sen_ycrit_u=20.0, stress_accum_tmin=10.0)
+    vecs = E.default_vector(P)[None]
+    edl = EnsembleDayLoop(stat, prog, dayst, daily, lat, vecs, P, day_params=DP, seed=5, jday=250).run()
+    cols = Columns.from_host(prog, stat, dtype=torch.float32, acc=True)
+    loop = DayLoop(cols, P, DP, dayst, lat=lat, seed=5, jday=250)
+    loop.run(torch.from_numpy(daily_planes(daily, cols.ld)).cuda())
+    torch.cuda.synchronize()
+    a, b = edl.dayst_host(), loop.dayst_host()
+    for k in ("acclim_x", "ssen_u", "ssen_l"):
+        np.testing.assert_allclose(a[k], b[k], rtol=1e-6, atol=1e-5, err_msg=k)
+    np.testing.assert_array_equal(a["stress_nday"], b["stress_nday"])
+    assert np.any(a["stress_nday"] > dayst["stress_nday"]) and np.any(a["ssen_u"] != dayst["ssen_u"])
+    for k in ("aystressu", "aystressl"):
+        assert np.mean(np.abs(a[k] - b[k]) <= 1e-3) >= 0.9, k
