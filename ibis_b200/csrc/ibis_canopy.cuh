@@ -41,6 +41,173 @@ __device__ __forceinline__ void c4_rate(R& ag, R& an, R par, R ci, R vmax, R rda
     an = ag - rdark;
 }
 
+// farquhar_c3 / farquhar_c4 with the IBIS 3.0 factors (stomata.py:228-318): the
+// big leaf's light-rate factor `jf` (acclim_light; 1 when off), and with `cap`
+// the canopy-level co-limitation: the light limit times `fl`, the capacity
+// limits and dark respiration times `fc` (cap_scale).
+template <typename R>
+__device__ __forceinline__ void c3_rate_x(R& ag, R& an, R par, R ci, R vmax, R gst, R kc, R ko, R rdark, R jf,
+                                          bool jon, bool cap, R fl, R fc, const DevParams<R>& P) {
+    R je = par * R(4.59e-06) * P.alpha3 * (ci - gst) / (ci + R(2.0) * gst);
+    if (jon) je = je * jf;
+    R jc = vmax * (ci - gst) / (ci + kc * (R(1.0) + P.o2conc / ko));
+    R js = vmax / R(2.2);
+    if (cap) { je = je * fl; jc = jc * fc; js = js * fc; rdark = rdark * fc; }
+    ag = colimit(colimit(je, jc, P.theta3), js, P.beta3);
+    an = ag - rdark;
+}
+
+template <typename R>
+__device__ __forceinline__ void c4_rate_x(R& ag, R& an, R par, R ci, R vmax, R rdark, R jf, bool jon, bool cap, R fl,
+                                          R fc, const DevParams<R>& P) {
+    R je = par * R(4.59e-06) * P.alpha4;
+    if (jon) je = je * jf;
+    R jc = vmax;
+    R ji = R(18.0e3) * vmax * ci;
+    if (cap) { je = je * fl; jc = jc * fc; ji = ji * fc; rdark = rdark * fc; }
+    ag = colimit(colimit(je, jc, P.theta4), ji, P.beta4);
+    an = ag - rdark;
+}
+
+// ---------------------------------------------------------------------------
+// IBIS 3.0 big-leaf parameters (stomata.py:566-660; loops.py:218-231, 291-309)
+// ---------------------------------------------------------------------------
+
+// The per-PFT factor on vmax: acclimation f_S(acclim_x) of the PFTs in the mask,
+// times the frost ramp on the day's mean air temperature, times the cropland
+// share's grass capacity.  `vf` says whether the reference forms a factor at all.
+template <typename R>
+struct PftFactor {
+    bool acclim, frost, crop;
+    R ax, ff, cf;
+    __device__ __forceinline__ bool vf() const { return acclim || crop; }
+    __device__ __forceinline__ R at(int p, const DevParams<R>& P) const {
+        R f = R(1.0);
+        if (acclim) {
+            const R m = P.acclim_mask[p];
+            const R fs = clip((ax - P.acclim_s0_pft[p]) / P.acclim_smax_pft[p], R(0.0), R(1.0));
+            f = R(1.0) - m + m * fs;
+            if (frost) f = f * (R(1.0) - m + m * ff);
+        }
+        if (crop) {
+            const R g = R(1.0) + cf * P.crop_inc[p];
+            f = acclim ? f * g : g;
+        }
+        return f;
+    }
+};
+
+template <typename R>
+__device__ __forceinline__ PftFactor<R> pft_factor(const Stat<R>& S, const DevParams<R>& P) {
+    PftFactor<R> f;
+    f.acclim = (P.flags & IBIS_FLAG_ACCLIM) != 0;
+    f.frost = f.acclim && (P.flags & IBIS_FLAG_FROST) != 0;
+    f.crop = (P.flags & IBIS_FLAG_CROP) != 0;
+    f.ax = f.acclim ? S(IBIS_STAT_ACCLIM_X) : R(0.0);
+    f.ff = f.frost ? clip((S(IBIS_STAT_TD) - R(273.16) - P.frost_t0) / (P.frost_t1 - P.frost_t0), R(0.0), R(1.0))
+                   : R(1.0);
+    f.cf = f.crop ? S(IBIS_STAT_CROPFRAC) : R(0.0);
+    return f;
+}
+
+// _mix_vmax (stomata.py:580-590): the displayed-LAI-weighted mean of a per-PFT
+// value over the PFTs idx[0..N), `fallback` where they have no leaves
+template <typename R, int N, typename V>
+__device__ __forceinline__ R mix_pft(const int (&idx)[N], const Stat<R>& S, const V& val, R fallback) {
+    R tot = R(0.0), sw = R(0.0);
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        const R w = S(IBIS_STAT_FRAC, idx[i]);
+        tot = tot + w;
+        sw = sw + w * val(idx[i]);
+    }
+    return tot > R(1.0e-6) ? sw / mx(tot, R(1.0e-6)) : fallback;
+}
+
+__device__ constexpr int kBroadleafPfts[5] = {0, 1, 2, 4, 6};
+__device__ constexpr int kConiferPfts[3] = {3, 5, 7};
+__device__ constexpr int kShrubPfts[2] = {8, 9};
+
+// Per-PFT values read by the big-leaf selection: the source's vmax, times the
+// PFT factor when EFF; or the source's per-PFT Ball-Berry slopes.
+template <typename R, typename Q, int KIND>
+struct PftValue {
+    const Q& q;
+    const PftFactor<R>& pf;
+    const DevParams<R>& P;
+    __device__ __forceinline__ R operator()(int p) const {
+        if constexpr (KIND == 0) return q.vmax(p);
+        else if constexpr (KIND == 1) return pf.vf() ? q.vmax(p) * pf.at(p, P) : q.vmax(p);
+        else return q.coefm_pft(p);
+    }
+};
+
+// _select_vmax_upper / _select_vmax_shrub (stomata.py:592-631) over the values v:
+// the priority pick, or with vmax_mix the displayed-LAI-weighted mean
+template <typename R, bool LOWER, typename V>
+__device__ __forceinline__ void select_big_leaves(R (&out)[LOWER ? 3 : 2], const V& v, const Stat<R>& S, bool mix) {
+    if constexpr (!LOWER) {
+        R ub = S(IBIS_STAT_EXIST, 0) > R(0.5) ? v(0) : (S(IBIS_STAT_EXIST, 2) > R(0.5) ? v(2) : v(4));
+        R uc = S(IBIS_STAT_EXIST, 3) > R(0.5) ? v(3) : v(5);
+        if (mix) {
+            ub = mix_pft(kBroadleafPfts, S, v, ub);
+            uc = mix_pft(kConiferPfts, S, v, uc);
+        }
+        out[0] = ub;
+        out[1] = uc;
+    } else {
+        R ls = v(8);
+        if (mix) ls = mix_pft(kShrubPfts, S, v, ls);
+        out[0] = ls;
+        out[1] = v(11);
+        out[2] = v(10);
+    }
+}
+
+// Nominal vmax (vn), light-rate factor (jf; jon = whether it applies) and
+// Ball-Berry slope (cm) of the upper big leaves [broadleaf, conifer] or, with
+// LOWER, of the lower ones [shrub, C3 grass, C4 grass] (stomata.py:592-660, 800-835).
+template <typename R, bool LOWER, typename Q>
+__device__ __forceinline__ void big_leaves(R (&vn)[LOWER ? 3 : 2], R (&jf)[LOWER ? 3 : 2], R (&cm)[LOWER ? 3 : 2],
+                                           bool& jon, const Stat<R>& S, const DevParams<R>& P, const Q& q) {
+    constexpr int NLF = LOWER ? 3 : 2;
+    const PftFactor<R> pf = pft_factor(S, P);
+    const bool mix = (P.flags & IBIS_FLAG_VMAX_MIX) != 0;
+    select_big_leaves<R, LOWER>(vn, PftValue<R, Q, 1>{q, pf, P}, S, mix);
+    jon = pf.vf() && (P.flags & IBIS_FLAG_ACCLIM_LIGHT) != 0;
+    if (jon) {
+        R rv[NLF];
+        select_big_leaves<R, LOWER>(rv, PftValue<R, Q, 0>{q, pf, P}, S, mix);
+#pragma unroll
+        for (int j = 0; j < NLF; ++j) jf[j] = vn[j] / mx(rv[j], P.epsilon);
+    } else {
+#pragma unroll
+        for (int j = 0; j < NLF; ++j) jf[j] = R(1.0);
+    }
+    if (P.flags & IBIS_FLAG_COEFM_MIX) {
+        const PftValue<R, Q, 2> cp{q, pf, P};
+        if constexpr (!LOWER) {
+            cm[0] = mix_pft(kBroadleafPfts, S, cp, q.coefm(0));
+            cm[1] = mix_pft(kConiferPfts, S, cp, q.coefm(1));
+        } else {
+            cm[0] = mix_pft(kShrubPfts, S, cp, q.coefm(2));
+            cm[1] = q.coefm_pft(11);
+            cm[2] = q.coefm_pft(10);
+        }
+    } else {
+        if constexpr (!LOWER) { cm[0] = q.coefm(0); cm[1] = q.coefm(1); }
+        else { cm[0] = q.coefm(2); cm[1] = q.coefm(4); cm[2] = q.coefm(3); }
+    }
+}
+
+// _capacity_integral (stomata.py:370-375): (1 - e^-Kn L)/(Kn L), 0 without leaves
+template <typename R>
+__device__ __forceinline__ R capacity_integral(R lai, R kn) {
+    const R x = kn * lai;
+    const R f = x > R(1.0e-4) ? -em1(-x) / mx(x, R(1.0e-4)) : R(1.0) - R(0.5) * x;
+    return lai > R(0.0) ? f : R(0.0);
+}
+
 template <typename R>
 struct Kin { R kc, ko, gst, vm3, vm4; };
 
@@ -71,17 +238,18 @@ __device__ __forceinline__ void ball_berry(R& cs, R& gs, R& ci, R an, R gb, R rh
     gs = gsn;
 }
 
-// canopy_scaling, F77 denominator k*LAI (stomata.py:442-512)
+// canopy_scaling (stomata.py:442-512): denominator k*LAI (F77) or, with
+// LEAF_ONLY (scale_leaf_only), k*(LAI+SAI)
 template <typename R>
 __device__ __forceinline__ R light_scaling(R toppar, R k, R h, const R (&sc)[4], R lai, R sai, R& a10s, R& a10d,
-                                           const DevParams<R>& P) {
+                                           const DevParams<R>& P, bool leaf_only = false) {
     R ext = (k * sc[0] + h * sc[1] - h * sc[2]) / mx(sc[3], P.epsilon);
     ext = clip(ext, R(0.1), R(10.0));
     R pxai = ext * (lai + sai);
     R plai = ext * lai;
     bool has = plai > R(0.0);
     bool day = toppar > R(10.0);
-    R sday = (R(1.0) - ex(-pxai)) / mx(plai, P.epsilon);
+    R sday = (R(1.0) - ex(-pxai)) / mx(leaf_only ? pxai : plai, P.epsilon);
     R snight = a10s / mx(a10d, P.epsilon);
     if (has && day) {
         a10s = P.zweight * a10s + (R(1.0) - P.zweight) * sday * toppar;
@@ -131,55 +299,83 @@ struct Stom {
 };
 
 // One pass of stomata over the five big leaves.  Updates the carried ci/gs/cs
-// and a10 running means in `c`.  SUN_U/SUN_L select the sunlit/shaded canopy.
+// and a10 running means in `c`.  SUN_U/SUN_L select the sunlit/shaded canopy;
+// a parameter source with Q::x3 adds the IBIS 3.0 switches (vmax and slope
+// mixing, acclimation with its light-rate factor and frost ramp, cropland
+// capacity, canopy-level capacity scaling, leaf-only light scaling).
 template <typename R, bool SUN_U, bool SUN_L, typename Q>
 __device__ __forceinline__ void stomata(Stom<R>& o, Col<R>& c, R tu, R tl, R t12, R t34, R q12, R q34, R su,
                                         R sl, R ps, const Rad<R>& Rd, R fwetu, R fwetl, const Stat<R>& S,
                                         R stresstu, R stresstl, const DevParams<R>& P, const Q& q) {
+    constexpr bool X3 = Q::x3;
     const R eps = P.epsilon;
     const R lai0 = S(IBIS_STAT_LAI, 0), lai1 = S(IBIS_STAT_LAI, 1);
     const R sai0 = S(IBIS_STAT_SAI, 0), sai1 = S(IBIS_STAT_SAI, 1);
+    const bool leaf_only = X3 && (P.flags & IBIS_FLAG_LEAF_ONLY) != 0;
     // ---------------- upper canopy: broadleaf (group 0) and conifer (group 1)
     {
         Kin<R> K = kinetics(tu, P);
         R gmn = R(1.05) * K.gst;
         R gb = clip(su * R(25.5), R(0.1), R(10.0));
         R rh = mx(R(0.30), q12 / mx(qsat(esat(t12), ps), eps));
-        R vn[2];
-        vn[0] = S(IBIS_STAT_EXIST, 0) > R(0.5) ? q.vmax(0)
-              : (S(IBIS_STAT_EXIST, 2) > R(0.5) ? q.vmax(2) : q.vmax(4));
-        vn[1] = S(IBIS_STAT_EXIST, 3) > R(0.5) ? q.vmax(3) : q.vmax(5);
+        R vn[2], jf[2], cm[2];
+        bool jon = false;
+        if constexpr (X3) {
+            big_leaves<R, false>(vn, jf, cm, jon, S, P, q);
+        } else {
+            vn[0] = S(IBIS_STAT_EXIST, 0) > R(0.5) ? q.vmax(0)
+                  : (S(IBIS_STAT_EXIST, 2) > R(0.5) ? q.vmax(2) : q.vmax(4));
+            vn[1] = S(IBIS_STAT_EXIST, 3) > R(0.5) ? q.vmax(3) : q.vmax(5);
+            cm[0] = q.coefm(0);
+            cm[1] = q.coefm(1);
+        }
+        const bool cap = X3 && !SUN_U && (P.flags & IBIS_FLAG_CAP_SCALE_U) != 0;
         SunShade<R> ss;
         if (SUN_U) ss = sunshade(Rd.scu, Rd.dbeamu, Rd.termu6, Rd.termu7, lai1, sai1, P);
-        R ag[2], an[2];
+        R ag[2], an[2], ci0[2], vmx[2], rdk[2];
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
             R ci = clip(c.ci_u[j], gmn, P.cimax);
             R vmax = vn[j] * K.vm3 * stresstu;
             R rd = P.gamma[j] * vn[j] * K.vm3;
-            c3_rate(ag[j], an[j], Rd.topparu, ci, vmax, K.gst, K.kc, K.ko, rd, P);
+            if constexpr (X3) c3_rate_x(ag[j], an[j], Rd.topparu, ci, vmax, K.gst, K.kc, K.ko, rd, jf[j], jon, false,
+                                        R(0.0), R(0.0), P);
+            else c3_rate(ag[j], an[j], Rd.topparu, ci, vmax, K.gst, K.kc, K.ko, rd, P);
             R bb = an[j];
             if (SUN_U) {
                 R ags, ans, agh, anh;
-                c3_rate(ags, ans, ss.psun, ci, vmax * ss.vsun, K.gst, K.kc, K.ko, rd * ss.vsun, P);
-                c3_rate(agh, anh, ss.psha, ci, vmax * ss.vsha, K.gst, K.kc, K.ko, rd * ss.vsha, P);
+                if constexpr (X3) {
+                    c3_rate_x(ags, ans, ss.psun, ci, vmax * ss.vsun, K.gst, K.kc, K.ko, rd * ss.vsun, jf[j], jon,
+                              false, R(0.0), R(0.0), P);
+                    c3_rate_x(agh, anh, ss.psha, ci, vmax * ss.vsha, K.gst, K.kc, K.ko, rd * ss.vsha, jf[j], jon,
+                              false, R(0.0), R(0.0), P);
+                } else {
+                    c3_rate(ags, ans, ss.psun, ci, vmax * ss.vsun, K.gst, K.kc, K.ko, rd * ss.vsun, P);
+                    c3_rate(agh, anh, ss.psha, ci, vmax * ss.vsha, K.gst, K.kc, K.ko, rd * ss.vsha, P);
+                }
                 R inv = lai1 > R(0.0) ? R(1.0) / mx(lai1, R(1.0e-6)) : R(0.0);
                 ag[j] = (ags + agh) * inv;
                 an[j] = (ans + anh) * inv;
                 bb = an[j];
             }
+            ci0[j] = ci;
+            vmx[j] = vmax;
+            rdk[j] = rd;
             c.ci_u[j] = ci;
-            ball_berry(c.cs_u[j], c.gs_u[j], c.ci_u[j], bb, gb, rh, q.coefm(j), P.coefb[j], stresstu, P.gsmin[j],
+            ball_berry(c.cs_u[j], c.gs_u[j], c.ci_u[j], bb, gb, rh, cm[j], P.coefb[j], stresstu, P.gsmin[j],
                        gmn, gmn, P);
         }
-        R scale = light_scaling(Rd.topparu, Rd.termu6, Rd.termu7, Rd.scu, lai1, sai1, c.a10su, c.a10du, P);
+        R scale = light_scaling(Rd.topparu, Rd.termu6, Rd.termu7, Rd.scu, lai1, sai1, c.a10su, c.a10du, P, leaf_only);
+        const R fcap = cap ? capacity_integral(lai1, P.cap_kn) : R(0.0);
         R tcs[2];
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
             R agc = ag[j], anc = an[j];
-            if (!SUN_U) { agc = ag[j] * scale; anc = an[j] * scale; }
+            if (cap) c3_rate_x(agc, anc, Rd.topparu, ci0[j], vmx[j], K.gst, K.kc, K.ko, rdk[j], jf[j], jon, true,
+                               scale, fcap, P);
+            else if (!SUN_U) { agc = ag[j] * scale; anc = an[j] * scale; }
             R csc = mx(gmn, P.co2conc - anc / gb);
-            R gsc = mx(mx(P.gsmin[j], P.coefb[j] * stresstu), q.coefm(j) * anc * rh / csc + P.coefb[j] * stresstu);
+            R gsc = mx(mx(P.gsmin[j], P.coefb[j] * stresstu), cm[j] * anc * rh / csc + P.coefb[j] * stresstu);
             tcs[j] = total_conductance(su, gsc);
             o.ag_u[j] = agc * (R(1.0) - fwetu);
             o.an_u[j] = anc * (R(1.0) - fwetu);
@@ -193,25 +389,54 @@ __device__ __forceinline__ void stomata(Stom<R>& o, Col<R>& c, R tu, R tl, R t12
         R gmn = R(1.05) * K.gst;
         R gb = clip(sl * R(25.5), R(0.1), R(10.0));
         R rh = mx(R(0.30), q34 / mx(qsat(esat(t34), ps), eps));
+        const int grp[3] = {2, 4, 3};
+        R vn[3], jf[3], cm[3];
+        bool jon = false;
+        if constexpr (X3) {
+            big_leaves<R, true>(vn, jf, cm, jon, S, P, q);
+        } else {
+            vn[0] = q.vmax(8);
+            vn[1] = q.vmax(11);
+            vn[2] = q.vmax(10);
+#pragma unroll
+            for (int j = 0; j < 3; ++j) cm[j] = q.coefm(grp[j]);
+        }
+        const bool cap = X3 && !SUN_L && (P.flags & IBIS_FLAG_CAP_SCALE_L) != 0;
         SunShade<R> ss;
         if (SUN_L) ss = sunshade(Rd.scl, Rd.dbeaml, Rd.terml6, Rd.terml7, lai0, sai0, P);
-        const int grp[3] = {2, 4, 3};
-        R ag[3], an[3];
+        R ag[3], an[3], ci0[3], vmx[3], rdk[3];
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
             const bool c4 = (j == 2);
             const int g = grp[j];
-            R vn = j == 0 ? q.vmax(8) : (j == 1 ? q.vmax(11) : q.vmax(10));
             R ci = clip(c.ci_l[j], c4 ? R(0.0) : gmn, P.cimax);
             R vm = c4 ? K.vm4 : K.vm3;
-            R vmax = vn * vm * stresstl;
-            R rd = P.gamma[g] * vn * vm;
-            if (c4) c4_rate(ag[j], an[j], Rd.topparl, ci, vmax, rd, P);
-            else c3_rate(ag[j], an[j], Rd.topparl, ci, vmax, K.gst, K.kc, K.ko, rd, P);
+            R vmax = vn[j] * vm * stresstl;
+            R rd = P.gamma[g] * vn[j] * vm;
+            if constexpr (X3) {
+                if (c4) c4_rate_x(ag[j], an[j], Rd.topparl, ci, vmax, rd, jf[j], jon, false, R(0.0), R(0.0), P);
+                else c3_rate_x(ag[j], an[j], Rd.topparl, ci, vmax, K.gst, K.kc, K.ko, rd, jf[j], jon, false, R(0.0),
+                               R(0.0), P);
+            } else {
+                if (c4) c4_rate(ag[j], an[j], Rd.topparl, ci, vmax, rd, P);
+                else c3_rate(ag[j], an[j], Rd.topparl, ci, vmax, K.gst, K.kc, K.ko, rd, P);
+            }
             R bb = an[j];
             if (SUN_L) {
                 R ags, ans, agh, anh;
-                if (c4) {
+                if constexpr (X3) {
+                    if (c4) {
+                        c4_rate_x(ags, ans, ss.psun, ci, vmax * ss.vsun, rd * ss.vsun, jf[j], jon, false, R(0.0),
+                                  R(0.0), P);
+                        c4_rate_x(agh, anh, ss.psha, ci, vmax * ss.vsha, rd * ss.vsha, jf[j], jon, false, R(0.0),
+                                  R(0.0), P);
+                    } else {
+                        c3_rate_x(ags, ans, ss.psun, ci, vmax * ss.vsun, K.gst, K.kc, K.ko, rd * ss.vsun, jf[j], jon,
+                                  false, R(0.0), R(0.0), P);
+                        c3_rate_x(agh, anh, ss.psha, ci, vmax * ss.vsha, K.gst, K.kc, K.ko, rd * ss.vsha, jf[j], jon,
+                                  false, R(0.0), R(0.0), P);
+                    }
+                } else if (c4) {
                     c4_rate(ags, ans, ss.psun, ci, vmax * ss.vsun, rd * ss.vsun, P);
                     c4_rate(agh, anh, ss.psha, ci, vmax * ss.vsha, rd * ss.vsha, P);
                 } else {
@@ -223,20 +448,31 @@ __device__ __forceinline__ void stomata(Stom<R>& o, Col<R>& c, R tu, R tl, R t12
                 an[j] = (ans + anh) * inv;
                 bb = an[j];
             }
+            ci0[j] = ci;
+            vmx[j] = vmax;
+            rdk[j] = rd;
             c.ci_l[j] = ci;
-            ball_berry(c.cs_l[j], c.gs_l[j], c.ci_l[j], bb, gb, rh, q.coefm(g), P.coefb[g], stresstl, P.gsmin[g],
+            ball_berry(c.cs_l[j], c.gs_l[j], c.ci_l[j], bb, gb, rh, cm[j], P.coefb[g], stresstl, P.gsmin[g],
                        c4 ? R(1.0e-8) : gmn, c4 ? R(0.0) : gmn, P);
         }
-        R scale = light_scaling(Rd.topparl, Rd.terml6, Rd.terml7, Rd.scl, lai0, sai0, c.a10sl, c.a10dl, P);
+        R scale = light_scaling(Rd.topparl, Rd.terml6, Rd.terml7, Rd.scl, lai0, sai0, c.a10sl, c.a10dl, P, leaf_only);
+        const R fcap = cap ? capacity_integral(lai0, P.cap_kn) : R(0.0);
         R tcs[3];
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
             const bool c4 = (j == 2);
             const int g = grp[j];
             R agc = ag[j], anc = an[j];
-            if (!SUN_L) { agc = ag[j] * scale; anc = an[j] * scale; }
+            if (cap) {
+                if (c4) c4_rate_x(agc, anc, Rd.topparl, ci0[j], vmx[j], rdk[j], jf[j], jon, true, scale, fcap, P);
+                else c3_rate_x(agc, anc, Rd.topparl, ci0[j], vmx[j], K.gst, K.kc, K.ko, rdk[j], jf[j], jon, true, scale,
+                               fcap, P);
+            } else if (!SUN_L) {
+                agc = ag[j] * scale;
+                anc = an[j] * scale;
+            }
             R csc = mx(c4 ? R(1.0e-8) : gmn, P.co2conc - anc / gb);
-            R gsc = mx(mx(P.gsmin[g], P.coefb[g] * stresstl), q.coefm(g) * anc * rh / csc + P.coefb[g] * stresstl);
+            R gsc = mx(mx(P.gsmin[g], P.coefb[g] * stresstl), cm[j] * anc * rh / csc + P.coefb[g] * stresstl);
             tcs[j] = total_conductance(sl, gsc);
             o.ag_l[j] = agc * (R(1.0) - fwetl);
             o.an_l[j] = anc * (R(1.0) - fwetl);

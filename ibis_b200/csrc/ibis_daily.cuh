@@ -274,7 +274,12 @@ __global__ void __launch_bounds__(128) day_begin_kernel(R* stat, R* dayst, R* ac
     if (i >= ncell) return;
     const Planes<R> S{stat + i, ld}, D{dayst + i, ld}, A{acc + i, ld};
     bool sen_u = false, sen_l = false;
-    if (dp.seasonal_on != 0.0) seasonal_states(D, (double)td[i], dp, sen_u, sen_l);
+    if (dp.seasonal_on != 0.0) {
+        seasonal_states(D, (double)td[i], dp, sen_u, sen_l);
+        // the day's hourly steps read the acclimation state from their STAT plane
+        // (IBIS_FLAG_ACCLIM), as the reference's steps read state.seasonal.acclim_x
+        S.set(IBIS_STAT_ACCLIM_X, D.get(IBIS_DAYST_ACCLIM_X));
+    }
     phenology(S, D, (double)td[i], A.get(IBIS_ACC_STRESSTU_LAST), A.get(IBIS_ACC_STRESSTL_LAST), dp, c.epsilon, sen_u,
               sen_l);
     const int sums[7] = {IBIS_ACC_ADRAIN, IBIS_ACC_ADSNOW, IBIS_ACC_ADAET, IBIS_ACC_A10ANCUB, IBIS_ACC_A10ANCLS,

@@ -181,9 +181,17 @@ struct AccInSmem {
 };
 constexpr int kAccSmemMinSteps = 4;
 
+// The uniform parameter source of a kernel: with X3 the one that compiles in the
+// IBIS 3.0 extensions of the step (any IBIS_FLAGS_X3 flag selects those kernels).
+template <typename R, bool X3>
+__device__ __forceinline__ auto uniform_source(const DevParams<R>& P) {
+    if constexpr (X3) return UniformQ3<R>{{P}};
+    else return UniformQ<R>{P};
+}
+
 // Status word written by the kernels: [0] bit 0 = a column left the step with a
 // non-finite prognostic value; [1] = smallest such cell index (INT_MAX if none).
-template <typename R, int NT, bool SU, bool SL, int BLOCK, int MINB, bool ACCSM>
+template <typename R, int NT, bool SU, bool SL, int BLOCK, int MINB, bool ACCSM, bool X3>
 __global__ void __launch_bounds__(BLOCK, MINB) hourly_step_kernel(R* __restrict__ prog, const R* __restrict__ stat,
                                                              const R* __restrict__ forc, R* __restrict__ diag,
                                                              R* __restrict__ acc, int ncell, int ld, int nstep,
@@ -212,7 +220,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) hourly_step_kernel(R* __restrict_
     for (int s = 0; s < nstep; ++s) {
         Forc<R> F = load_forc(forc + (size_t)s * forc_stride + i, ld);
         A.last = (s + 1 == nstep);
-        column_step<R, NT, SU, SL>(c, F, S, D, A, P, UniformQ<R>{P});
+        column_step<R, NT, SU, SL>(c, F, S, D, A, P, uniform_source<R, X3>(P));
     }
     if (kAccSmem && acc) acc_move<R, false>(acc + i, ld, sacc, BLOCK, P.flags);
     R sum = store_col(c, prog + i, ld);
@@ -225,7 +233,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) hourly_step_kernel(R* __restrict_
 // Two-kernel form of one hour: the surface phase writes the hand-off values to
 // `mid` (kMidCount planes), the ground phase reads them.  Both phases load the
 // column from `prog` and write back what they change.
-template <typename R, bool SU, bool SL, int BLOCK, int MINB>
+template <typename R, bool SU, bool SL, int BLOCK, int MINB, bool X3>
 __global__ void __launch_bounds__(BLOCK, MINB) surface_kernel(R* __restrict__ prog, const R* __restrict__ stat,
                                                                     const R* __restrict__ forc, R* __restrict__ diag,
                                                                     R* __restrict__ mid, int ncell, int ld,
@@ -243,12 +251,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) surface_kernel(R* __restrict__ pr
     Diag<R> D{diag ? diag + i : nullptr, ld};
     Forc<R> F = load_forc(forc + i, ld);
     Mid<R> M;
-    surface_phase<R, SU, SL>(c, F, S, D, P, UniformQ<R>{P}, M);
+    surface_phase<R, SU, SL>(c, F, S, D, P, uniform_source<R, X3>(P), M);
     mid_store(M, mid + i, ld);
     store_col(c, prog + i, ld);
 }
 
-template <typename R, int NT, int BLOCK, int MINB>
+template <typename R, int NT, int BLOCK, int MINB, bool X3>
 __global__ void __launch_bounds__(BLOCK, MINB) ground_kernel(R* __restrict__ prog, const R* __restrict__ stat,
                                                                    const R* __restrict__ forc, R* __restrict__ diag,
                                                                    R* __restrict__ acc, const R* __restrict__ mid,
@@ -269,7 +277,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) ground_kernel(R* __restrict__ pro
     Forc<R> F = load_forc(forc + i, ld);
     Mid<R> M;
     mid_load(M, mid + i, ld);
-    ground_phase<R, NT>(c, F, S, D, A, P, UniformQ<R>{P}, M);
+    ground_phase<R, NT>(c, F, S, D, A, P, uniform_source<R, X3>(P), M);
     R sum = store_col(c, prog + i, ld);
     if (status && !finite(sum)) {
         atomicOr(status, 1);
@@ -328,6 +336,16 @@ static DevParams<R> make_dev_params(const IbisParams& h) {
         d.rroot_s[j] = (R)(((float)h.rroot[j] / per_s) * mol);
         d.keep[j] = (R)(1.0f - (float)h.rgrowth[j]);
     }
+    // crop_vfac's increments (loops.py:218-231), float32 values as the reference forms them
+    for (int j = 0; j < 12; ++j) d.crop_inc[j] = (R)0.0;
+    if (h.crop_c4_share < 0.0) {
+        d.crop_inc[10] = (R)(float)(h.crop_vmax_scale_c4 - 1.0);
+        d.crop_inc[11] = (R)(float)(h.crop_vmax_scale_c3 - 1.0);
+    } else {
+        const double qc = h.crop_c4_share > 1.0 ? 1.0 : h.crop_c4_share;
+        const double s_mix = (1.0 - qc) * h.crop_vmax_scale_c3 + qc * h.crop_vmax_scale_c4;
+        d.crop_inc[10] = d.crop_inc[11] = (R)(float)(s_mix - 1.0);
+    }
     d.ch4_w = (R)(float)(h.dtime / 86400.0);
     d.rh_conv = (R)(float)(12.0e-3 * 86400.0);
     double top = 0.0, tot = 0.0;
@@ -382,14 +400,14 @@ cudaError_t fit_smem_once(unsigned long long& done, K k, int block, size_t smem,
     return e;
 }
 
-template <typename R, int NT, bool SU, bool SL, int BLOCK, int MINB, bool ACCSM>
+template <typename R, int NT, bool SU, bool SL, int BLOCK, int MINB, bool ACCSM, bool X3>
 cudaError_t launch_fused(R* prog, const R* stat, const R* forc, R* diag, R* acc, int ncell, int ld, int nstep,
                          long long fstride, const DevParams<R>& P, int* status, cudaStream_t s) {
     const int grid = (ncell + BLOCK - 1) / BLOCK;
     const size_t col_smem = StateInSmem<R>::value ? BLOCK * sizeof(Col<R>) : 0;
     const size_t acc_smem = AccInSmem<R, BLOCK, MINB, ACCSM>::value ? BLOCK * 2 * kAccOnChip * sizeof(R) : 0;
     const size_t smem = col_smem + acc_smem;
-    auto k = hourly_step_kernel<R, NT, SU, SL, BLOCK, MINB, ACCSM>;
+    auto k = hourly_step_kernel<R, NT, SU, SL, BLOCK, MINB, ACCSM, X3>;
     static unsigned long long fitted = 0;
     cudaError_t e = fit_smem_once(fitted, k, BLOCK, col_smem + acc_smem, col_smem + acc_smem);
     if (e != cudaSuccess) return e;
@@ -397,14 +415,14 @@ cudaError_t launch_fused(R* prog, const R* stat, const R* forc, R* diag, R* acc,
     return cudaGetLastError();
 }
 
-template <typename R, int NT, bool SU, bool SL, int B1, int M1, int B2, int M2>
+template <typename R, int NT, bool SU, bool SL, int B1, int M1, int B2, int M2, bool X3>
 cudaError_t launch_split(R* prog, const R* stat, const R* forc, R* diag, R* acc, R* mid, int ncell, int ld,
                          int nstep, long long fstride, const DevParams<R>& P, int* status, cudaStream_t s) {
     const int g1 = (ncell + B1 - 1) / B1, g2 = (ncell + B2 - 1) / B2;
     const size_t sm1 = StateInSmem<R>::value ? B1 * sizeof(Col<R>) : 0;
     const size_t sm2 = StateInSmem<R>::value ? B2 * sizeof(Col<R>) : 0;
-    auto k1 = surface_kernel<R, SU, SL, B1, M1>;
-    auto k2 = ground_kernel<R, NT, B2, M2>;
+    auto k1 = surface_kernel<R, SU, SL, B1, M1, X3>;
+    auto k2 = ground_kernel<R, NT, B2, M2, X3>;
     static unsigned long long fitted1 = 0, fitted2 = 0;
     cudaError_t e = fit_smem_once(fitted1, k1, B1, sm1, sm1);
     if (e == cudaSuccess) e = fit_smem_once(fitted2, k2, B2, sm2, sm2);
@@ -417,7 +435,7 @@ cudaError_t launch_split(R* prog, const R* stat, const R* forc, R* diag, R* acc,
     return cudaGetLastError();
 }
 
-template <typename R, int NT, bool SU, bool SL, int CFG>
+template <typename R, int NT, bool SU, bool SL, int CFG, bool X3 = false>
 cudaError_t run_config(R* prog, const R* stat, const R* forc, R* diag, R* acc, R* mid, int ncell, int ld, int nstep,
                        long long fs, const DevParams<R>& P, int* status, cudaStream_t s) {
     constexpr LaunchConfig C = kConfigs[CFG];
@@ -426,14 +444,14 @@ cudaError_t run_config(R* prog, const R* stat, const R* forc, R* diag, R* acc, R
         // per-hour callers') also has a global-accumulator twin for short launches
         if constexpr (CFG == kDefaultFused && AccInSmem<R, C.block, C.minb>::value) {
             if (nstep < kAccSmemMinSteps)
-                return launch_fused<R, NT, SU, SL, C.block, C.minb, false>(prog, stat, forc, diag, acc, ncell, ld,
-                                                                           nstep, fs, P, status, s);
+                return launch_fused<R, NT, SU, SL, C.block, C.minb, false, X3>(prog, stat, forc, diag, acc, ncell,
+                                                                               ld, nstep, fs, P, status, s);
         }
-        return launch_fused<R, NT, SU, SL, C.block, C.minb, true>(prog, stat, forc, diag, acc, ncell, ld, nstep, fs,
-                                                                  P, status, s);
+        return launch_fused<R, NT, SU, SL, C.block, C.minb, true, X3>(prog, stat, forc, diag, acc, ncell, ld, nstep,
+                                                                      fs, P, status, s);
     } else {
-        return launch_split<R, NT, SU, SL, C.block, C.minb, C.block2, C.minb2>(prog, stat, forc, diag, acc, mid,
-                                                                              ncell, ld, nstep, fs, P, status, s);
+        return launch_split<R, NT, SU, SL, C.block, C.minb, C.block2, C.minb2, X3>(prog, stat, forc, diag, acc, mid,
+                                                                                  ncell, ld, nstep, fs, P, status, s);
     }
 }
 
@@ -450,13 +468,26 @@ cudaError_t run_config(R* prog, const R* stat, const R* forc, R* diag, R* acc, R
 #define IBIS_SUN_CONFIGS(X, NT)                                                                                \
     X(NT, true, false, 0) X(NT, false, true, 0) X(NT, true, true, 0)                                           \
     X(NT, true, false, 8) X(NT, false, true, 8) X(NT, true, true, 8)
+// The IBIS 3.0 kernels (X3): every canopy variant in the two default
+// configurations, and the long fused configuration for both canopies F77 or
+// both sunlit/shaded.  X(NT, SU, SL, CFG).
+#define IBIS_X3_CONFIGS(X, NT)                                                                                 \
+    X(NT, false, false, 0) X(NT, false, false, 6) X(NT, false, false, 8)                                       \
+    X(NT, true, true, 0) X(NT, true, true, 6) X(NT, true, true, 8)                                             \
+    X(NT, true, false, 0) X(NT, true, false, 8) X(NT, false, true, 0) X(NT, false, true, 8)
 
-template <typename R, int NT, bool SU, bool SL>
+template <typename R, int NT, bool SU, bool SL, bool X3>
 cudaError_t dispatch_config(int cfg, R* prog, const R* stat, const R* forc, R* diag, R* acc, R* mid, int ncell,
                             int ld, int nstep, long long fs, const DevParams<R>& P, int* status, cudaStream_t s) {
 #define IBIS_ARGS prog, stat, forc, diag, acc, mid, ncell, ld, nstep, fs, P, status, s
     if constexpr (sizeof(R) == 8) {
-        return run_config<R, NT, SU, SL, kDefaultFused>(IBIS_ARGS);
+        // the float64 kernels always carry the IBIS 3.0 extensions: with their
+        // switches off they perform the F77 step's operations
+        return run_config<R, NT, SU, SL, kDefaultFused, true>(IBIS_ARGS);
+    } else if constexpr (X3) {
+        if (cfg == kLongFused && SU == SL) return run_config<R, NT, SU, SL, kLongFused, true>(IBIS_ARGS);
+        if (kConfigs[cfg].form == 0) return run_config<R, NT, SU, SL, kDefaultFused, true>(IBIS_ARGS);
+        return run_config<R, NT, SU, SL, kDefaultSplit, true>(IBIS_ARGS);
     } else if constexpr (SU || SL) {
         if (kConfigs[cfg].form == 0) return run_config<R, NT, SU, SL, kDefaultFused>(IBIS_ARGS);
         return run_config<R, NT, SU, SL, kDefaultSplit>(IBIS_ARGS);
@@ -488,7 +519,7 @@ static int hourly_step(R* prog, const R* stat, const R* forc, R* diag, R* acc, i
     if (ncell == 0 || nstep == 0) return 0;
     const unsigned known = IBIS_FLAG_BEDROCK | IBIS_FLAG_H2O_CONSISTENT | IBIS_FLAG_SUNSHADE_U | IBIS_FLAG_SUNSHADE_L |
                            IBIS_FLAG_ACC | IBIS_FLAG_CH4 | IBIS_FLAG_SOIL_MEANS | IBIS_FLAG_DIAG | IBIS_FLAG_KAHAN |
-                           IBIS_FLAG_ZWT_OBS | IBIS_FLAG_ETPARTS | IBIS_FLAG_NEEPARTS;
+                           IBIS_FLAG_ZWT_OBS | IBIS_FLAG_ETPARTS | IBIS_FLAG_NEEPARTS | IBIS_FLAGS_X3;
     if (hp->flags & ~known) return -EINVAL;
     if ((hp->flags & (IBIS_FLAG_ACC | IBIS_FLAG_CH4 | IBIS_FLAG_SOIL_MEANS)) && !acc) return -EINVAL;
     if ((hp->flags & IBIS_FLAG_DIAG) && !diag) return -EINVAL;
@@ -501,9 +532,13 @@ static int hourly_step(R* prog, const R* stat, const R* forc, R* diag, R* acc, i
     const bool bed = hp->flags & IBIS_FLAG_BEDROCK;
     const bool su = hp->flags & IBIS_FLAG_SUNSHADE_U;
     const bool sl = hp->flags & IBIS_FLAG_SUNSHADE_L;
+    const bool x3 = (hp->flags & IBIS_FLAGS_X3) != 0;
     cudaError_t e;
-#define IBIS_CASE(NT_, SU_, SL_) \
-    e = dispatch_config<R, NT_, SU_, SL_>(cfg, prog, stat, forc, diag, acc, mid, ncell, ld, nstep, fstride, P, status, s)
+#define IBIS_CASE(NT_, SU_, SL_)                                                                                     \
+    e = x3 ? dispatch_config<R, NT_, SU_, SL_, true>(cfg, prog, stat, forc, diag, acc, mid, ncell, ld, nstep, fstride, \
+                                                     P, status, s)                                                   \
+           : dispatch_config<R, NT_, SU_, SL_, false>(cfg, prog, stat, forc, diag, acc, mid, ncell, ld, nstep,       \
+                                                      fstride, P, status, s)
     if (bed) {
         if (su) { if (sl) IBIS_CASE(9, true, true); else IBIS_CASE(9, true, false); }
         else { if (sl) IBIS_CASE(9, false, true); else IBIS_CASE(9, false, false); }

@@ -40,6 +40,10 @@ struct DevParams {
     R ch4_wtop[6];     // thickness weights of the wetland water-table average (methane.py:266-270)
     R ch4_wtot;        // their sum, floored at 1e-12
     R hsoi_top[6], hsoi_bot[6];  // layer tops/bottoms (cumsum of hsoi)
+    // per-PFT capacity increment per unit cropland share (loops.py:218-231): the C4
+    // (PFT 10) and C3 (PFT 11) vmax scales less one, formed in float32 as the
+    // reference forms them on float32 masks; zero for the other PFTs
+    R crop_inc[12];
 };
 
 // The parameters a calibration ensemble varies per run (the 31-parameter
@@ -50,9 +54,14 @@ struct DevParams {
 // UniformQ (one parameter record for every cell) or RunQ (one run's values,
 // 33 words: an odd stride, so a warp reading one field of its 32 runs' records
 // in shared memory touches 32 different banks).
+//
+// ``x3`` marks the sources of the kernels compiled with the IBIS 3.0 extensions
+// of the step (IBIS_FLAGS_X3): the F77 kernels carry none of their code.
 template <typename R>
 struct UniformQ {
+    static constexpr bool x3 = false;
     const DevParams<R>& P;
+    __device__ __forceinline__ R coefm_pft(int p) const { return P.coefm_pft[p]; }
     __device__ __forceinline__ R vmax(int j) const { return P.vmax_pft[j]; }
     __device__ __forceinline__ R coefm(int g) const { return P.coefm[g]; }
     __device__ __forceinline__ R stressfac() const { return P.stressfac; }
@@ -73,8 +82,16 @@ struct UniformQ {
     __device__ __forceinline__ R keep(int j) const { return P.keep[j]; }
 };
 
+// One parameter record for every cell, in the kernels that carry the IBIS 3.0
+// extensions.
+template <typename R>
+struct UniformQ3 : UniformQ<R> {
+    static constexpr bool x3 = true;
+};
+
 template <typename R>
 struct RunQ {
+    static constexpr bool x3 = false;
     R vmax_[12], coefm_[5], stressfac_, znorm_, beta_, wliqumax_, wliqsmax_, wliqlmax_, fmax_, wliqmin_;
     R r_ch4_, q10p_, z_tau_, tau_oxid_, z_wt_max_, rwood_, rroot_, keep_;
     __device__ __forceinline__ R vmax(int j) const { return vmax_[j]; }

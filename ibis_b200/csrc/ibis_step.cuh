@@ -98,9 +98,11 @@ __device__ __forceinline__ void mid_load(Mid<R>& m, const R* __restrict__ p, int
     m.fsena = v[27];
 }
 
-// setsoi (soil_physics.py:37-140): conductivity of layer k
-template <typename R>
-__device__ __forceinline__ R layer_conductivity(const Col<R>& c, const Stat<R>& S, int k) {
+// setsoi (soil_physics.py:37-140): conductivity of layer k; with X3 and
+// IBIS_FLAG_FORGANIC the dry conductivity of organic solids blended in
+// (soil_physics.py:74-77)
+template <bool X3, typename R>
+__device__ __forceinline__ R layer_conductivity(const Col<R>& c, const Stat<R>& S, const DevParams<R>& P, int k) {
     R fs = R(0.01) * S(IBIS_STAT_SAND, k);
     R fc = R(0.01) * S(IBIS_STAT_CLAY, k);
     R fsilt = R(1.0) - fs - fc;
@@ -108,6 +110,12 @@ __device__ __forceinline__ R layer_conductivity(const Col<R>& c, const Stat<R>& 
     R pliq = por * c.wsoi[k] * (R(1.0) - c.wisoi[k]);
     R pice = por * c.wisoi[k];
     R dry = fs * R(0.300) + fsilt * R(0.265) + fc * R(0.250);
+    if constexpr (X3) {
+        if (P.flags & IBIS_FLAG_FORGANIC) {
+            const R fo = S(IBIS_STAT_FORGANIC, k);
+            dry = (R(1.0) - fo) * dry + fo * R(0.05);
+        }
+    }
     return dry * pw(R(56.0), pliq) * pw(R(224.0), pice);
 }
 
@@ -134,6 +142,23 @@ __device__ __forceinline__ void evap_sources(const Col<R>& c, const Forc<R>& F, 
         hvasug = (q1 + q3) * zvap + (q2 + q4) * zsub;
         hvasui = P.hsub + P.cvap * (F.ta - P.tmelt) - P.cice * (c.tsno[0] - P.tmelt);
     }
+}
+
+// capacity_shares (stomata.py:566-577) of one big leaf: the capacity-weighted
+// leaf area (floored at 1e-12), the leaf area, and whether the capacity shares apply
+template <typename R, int N, typename Q>
+__device__ __forceinline__ void capacity_group(const int (&idx)[N], const Stat<R>& S, const Q& q, R& twm, R& tf,
+                                               bool& on) {
+    R tw = R(0.0);
+    tf = R(0.0);
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        const R f = S(IBIS_STAT_FRAC, idx[i]);
+        tw = tw + f * q.vmax(idx[i]);
+        tf = tf + f;
+    }
+    on = tw > R(1.0e-12);
+    twm = mx(tw, R(1.0e-12));
 }
 
 // drystress (stomata.py:515-562)
@@ -168,7 +193,7 @@ __device__ __forceinline__ void surface_phase(Col<R>& c, const Forc<R>& F, const
     const R fu = S(IBIS_STAT_FU), fl = S(IBIS_STAT_FL);
     R q1, q2, q3, q4, hvasug, hvasui;
     evap_sources(c, F, P, q1, q2, q3, q4, hvasug, hvasui);
-    const R consoi0 = layer_conductivity(c, S, 0);
+    const R consoi0 = layer_conductivity<Q::x3>(c, S, P, 0);
 
     // ---- 2-3. wet fractions and radiation (loops.py:331-354)
     Rad<R> Rd;
@@ -351,7 +376,7 @@ __device__ __forceinline__ void ground_phase(Col<R>& c, const Forc<R>& F, const 
     R wliql = c.wliql, wsnol = c.wsnol;
     R consoi[NL];
 #pragma unroll
-    for (int k = 0; k < NL; ++k) consoi[k] = layer_conductivity(c, S, k);
+    for (int k = 0; k < NL; ++k) consoi[k] = layer_conductivity<Q::x3>(c, S, P, k);
     R q1, q2, q3, q4, hvasug_, hvasui_;
     evap_sources(c, F, P, q1, q2, q3, q4, hvasug_, hvasui_);
     R stressu[NL], stressl[NL], stresstu, stresstl;
@@ -587,6 +612,18 @@ __device__ __forceinline__ void ground_phase(Col<R>& c, const Forc<R>& F, const 
             const R funcb = ex(R(3500.0) * (R(1.0 / 288.16) - R(1.0) / mx(root_t, R(200.0))));
             const R cf = R(12.0e-3) * dt;
             const R sap = S(IBIS_STAT_SAPFRAC);
+            // with gpp_split_by_capacity (X3), each big leaf's GPP is divided among
+            // its PFTs by leaf area x vmax, re-normalised to the leaf-area sum
+            // (capacity_shares, stomata.py:566-577; loops_gswp3.py:197-205)
+            R twm[3] = {R(1.0), R(1.0), R(1.0)}, tfs[3] = {R(0.0), R(0.0), R(0.0)};
+            bool by_cap[3] = {false, false, false};
+            if constexpr (Q::x3) {
+                if (P.flags & IBIS_FLAG_GPP_CAPACITY) {
+                    capacity_group(kBroadleafPfts, S, q, twm[0], tfs[0], by_cap[0]);
+                    capacity_group(kConiferPfts, S, q, twm[1], tfs[1], by_cap[1]);
+                    capacity_group(kShrubPfts, S, q, twm[2], tfs[2], by_cap[2]);
+                }
+            }
             R npp = R(0.0);
 #pragma unroll
             for (int j = 0; j < 12; ++j) {
@@ -601,9 +638,14 @@ __device__ __forceinline__ void ground_phase(Col<R>& c, const Forc<R>& F, const 
                     lai_ = lai0; cov = fl * smask; sp = R(1.0);
                     wood = j < 10;
                 }
+                R share = S(IBIS_STAT_FRAC, j);
+                if constexpr (Q::x3) {
+                    const int gi = j < 8 ? ((j == 3 || j == 5 || j == 7) ? 1 : 0) : (j < 10 ? 2 : -1);
+                    if (gi >= 0 && by_cap[gi]) share = share * q.vmax(j) / twm[gi] * tfs[gi];
+                }
                 R g;
-                if (j < 8) g = an * S(IBIS_STAT_FRAC, j) * lai_ * cov;
-                else g = an * S(IBIS_STAT_FRAC, j) * lai_ * fl * smask;
+                if (j < 8) g = an * share * lai_ * cov;
+                else g = an * share * lai_ * fl * smask;
                 R r = q.rroot(j) * S(IBIS_STAT_CBIOR, j) * funcb;
                 if (wood) r = (j < 8 ? q.rwood(j) * S(IBIS_STAT_CBIOW, j) * sp * funca
                                      : q.rwood(j) * S(IBIS_STAT_CBIOW, j) * funca) + r;

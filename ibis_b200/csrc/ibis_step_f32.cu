@@ -12,6 +12,11 @@ IBIS_F77_CONFIGS(IBIS_EXTERN, 9)
 IBIS_SUN_CONFIGS(IBIS_EXTERN, 6)
 IBIS_SUN_CONFIGS(IBIS_EXTERN, 9)
 #undef IBIS_EXTERN
+#define IBIS_EXTERN_X3(NT, SU, SL, CFG) \
+    extern template cudaError_t run_config<float, NT, SU, SL, CFG, true>(IBIS_RUN_ARGS(float));
+IBIS_X3_CONFIGS(IBIS_EXTERN_X3, 6)
+IBIS_X3_CONFIGS(IBIS_EXTERN_X3, 9)
+#undef IBIS_EXTERN_X3
 }  // namespace ibis
 
 extern "C" int ibis_step_f32(float* prog, const float* stat, const float* forc, float* diag, float* acc, int ncell,

@@ -71,6 +71,11 @@ class DayLoop:
         lat = np.zeros(n) if lat is None else np.asarray(lat, dtype=np.float64)
         dayst = dict(dayst, latitude=np.deg2rad(lat))
         self.dayst = torch.from_numpy(synth.to_planes("DAYST", dayst, ld, cols._np_dtype)).to(cols.device)
+        # the hourly steps read the acclimation state from their own STAT plane
+        # (IBIS_FLAG_ACCLIM); ibis_day_begin refreshes it each day it advances
+        if "acclim_x" in dayst:
+            p_ax = L.OFF["STAT"]["acclim_x"][0]
+            cols.stat[p_ax] = self.dayst[L.OFF["DAYST"]["acclim_x"][0]]
         lat_planes = np.zeros(ld, dtype=np.float32)
         lat_planes[:n] = lat
         self.lat = torch.from_numpy(lat_planes).to(cols.device)

@@ -36,9 +36,10 @@ import torch
 
 from . import layout as L
 from .columns import Columns
-from .params import (FLAG_ACC, FLAG_BEDROCK, FLAG_CH4, FLAG_ETPARTS, FLAG_H2O_CONSISTENT, FLAG_NEEPARTS,
-                     FLAG_SOIL_MEANS, FLAG_SUNSHADE_L,
-                     FLAG_SUNSHADE_U, StepParams)
+from .params import (FLAG_ACC, FLAG_ACCLIM, FLAG_ACCLIM_LIGHT, FLAG_BEDROCK, FLAG_CAP_SCALE_L, FLAG_CAP_SCALE_U,
+                     FLAG_CH4, FLAG_COEFM_MIX, FLAG_CROP, FLAG_ETPARTS, FLAG_FORGANIC, FLAG_FROST,
+                     FLAG_GPP_CAPACITY, FLAG_H2O_CONSISTENT, FLAG_LEAF_ONLY, FLAG_NEEPARTS, FLAG_SOIL_MEANS,
+                     FLAG_SUNSHADE_L, FLAG_SUNSHADE_U, FLAG_VMAX_MIX, StepParams)
 
 # Where each parameter of the flat record lives in the reference's objects.
 # Roots: consts (PhysicalConstants), params (SimParams), state (IBISState).
@@ -55,7 +56,9 @@ PARAM_PATHS = {
                                                "tblowl", "fmax")},
     **{k: f"params.stomata_params.{k}" for k in ("tau15", "kc15", "ko15", "cimax", "o2conc", "alpha3", "theta3",
                                                  "beta3", "alpha4", "theta4", "beta4", "gamma", "coefm", "coefb",
-                                                 "gsmin", "vmax_pft", "stressfac", "cap_kn")},
+                                                 "gsmin", "vmax_pft", "stressfac", "cap_kn", "coefm_pft",
+                                                 "frost_t0", "frost_t1")},
+    **{f"crop_{k}": f"params.crop.{k}" for k in ("vmax_scale_c3", "vmax_scale_c4", "c4_share")},
     **{k: f"params.{k}" for k in ("wpudmax", "zwpmax", "bperm", "rhosoi_val", "csoi_mineral_val")},
     "hsoi": "state.soil.hsoi",
     "froot": "state.vegetation.froot",
@@ -106,23 +109,48 @@ def tree_set(root, path: str, value):
     return _replace(root, head, tree_set(getattr(root, head), tail, value))
 
 
-# StomataParams switches whose formulations the step does not carry (all off by
-# default, stomata.py:98-159; acclim_pfts / acclim_per_pft only act with
-# acclim_on).  A parameter set that turns one on is refused, not silently run
-# without it.
-UNSUPPORTED_SWITCHES = ("vmax_mix", "scale_leaf_only", "acclim_on", "cap_scale_u", "cap_scale_l", "coefm_mix",
-                        "acclim_light", "frost_on", "gpp_split_by_capacity")
+# StomataParams switches (stomata.py:98-159) -> the step's variant flags.  Every
+# switch of the reference's stomata formulation has one; acclim_on acts only on a
+# state that carries the seasonal module (loops.py:294) and frost_on only with it
+# (loops.py:305).
+SWITCH_FLAGS = {"vmax_mix": FLAG_VMAX_MIX, "coefm_mix": FLAG_COEFM_MIX, "gpp_split_by_capacity": FLAG_GPP_CAPACITY,
+                "acclim_light": FLAG_ACCLIM_LIGHT, "cap_scale_u": FLAG_CAP_SCALE_U, "cap_scale_l": FLAG_CAP_SCALE_L,
+                "scale_leaf_only": FLAG_LEAF_ONLY, "sunshade_u": FLAG_SUNSHADE_U, "sunshade_l": FLAG_SUNSHADE_L}
+# Switches the step does not carry: none.  Per-cell PFT tables (the IBIS 3.0
+# zone types, io/pft_types.py) are refused by step_params instead.
+UNSUPPORTED_SWITCHES: tuple = ()
+# Per-PFT tables that IBIS 3.0 zone types make per-cell (npoi, 12)
+_PFT_TABLES = ("params.stomata_params.vmax_pft", "params.stomata_params.coefm_pft",
+               "params.stomata_params.acclim_s0_pft", "params.stomata_params.acclim_smax_pft",
+               "params.bgc_params.rwood", "params.bgc_params.rroot", "params.bgc_params.rgrowth")
+
+
+def _stomata_flags(state, params, sp) -> int:
+    flags = 0
+    for name, flag in SWITCH_FLAGS.items():
+        if bool(getattr(sp, name, False)):
+            flags |= flag
+    if bool(getattr(sp, "acclim_on", False)) and getattr(state, "seasonal", None) is not None:
+        flags |= FLAG_ACCLIM
+        if bool(getattr(sp, "frost_on", False)):
+            flags |= FLAG_FROST
+    if getattr(params, "cropfrac", None) is not None:
+        flags |= FLAG_CROP
+    if getattr(params, "forganic", None) is not None:
+        flags |= FLAG_FORGANIC
+    return flags
 
 
 def step_params(state, consts, params, dtime: float, ndaypy: float = 365.0) -> StepParams:
     """The flat parameter record (and variant flags) equivalent to the reference
-    objects.  Raises NotImplementedError for a stomata switch of
-    ``UNSUPPORTED_SWITCHES`` that is on."""
+    objects.  Raises NotImplementedError for per-cell PFT tables (IBIS 3.0
+    zone types), which the step does not carry."""
     sp = getattr(params, "stomata_params", None)
-    on = [k for k in UNSUPPORTED_SWITCHES if bool(getattr(sp, k, False))]
-    if on:
-        raise NotImplementedError(f"stomata_params switches not implemented by the B200 step: {', '.join(on)}")
     roots = {"state": state, "consts": consts, "params": params}
+    for path in _PFT_TABLES:
+        v = _get(roots, path)
+        if v is not None and np.ndim(v) == 2:
+            raise NotImplementedError(f"per-cell PFT table {path} (IBIS 3.0 zone types) is not implemented")
     P = StepParams()
     for name, path in PARAM_PATHS.items():
         v = _get(roots, path)
@@ -139,17 +167,38 @@ def step_params(state, consts, params, dtime: float, ndaypy: float = 365.0) -> S
         setattr(P, name, float(os.environ.get(env, default)))
     P.dtime = float(dtime)
     P.ndaypy = float(ndaypy)
-    flags = 0
+    # the acclimated PFTs as a mask, and the acclimation constants per PFT (the
+    # scalars repeated when acclim_per_pft is off: the same arithmetic, loops.py:295-303)
+    if sp is not None:
+        mask = np.zeros(12)
+        for k in tuple(getattr(sp, "acclim_pfts", (3, 5, 8))):
+            mask[int(k)] = 1.0
+        P.acclim_mask = mask
+        if bool(getattr(sp, "acclim_per_pft", False)):
+            P.acclim_s0_pft = np.asarray(sp.acclim_s0_pft, dtype=np.float64).reshape(12)
+            P.acclim_smax_pft = np.asarray(sp.acclim_smax_pft, dtype=np.float64).reshape(12)
+        else:
+            P.acclim_s0_pft = np.full(12, float(getattr(sp, "acclim_s0", -3.063)))
+            P.acclim_smax_pft = np.full(12, float(getattr(sp, "acclim_smax", 17.72)))
+    flags = _stomata_flags(state, params, sp)
     if getattr(state.soil, "tsoi_deep", None) is not None:
         flags |= FLAG_BEDROCK
     if bool(getattr(params, "h2o_consistent_weights", False)):
         flags |= FLAG_H2O_CONSISTENT
-    if bool(getattr(sp, "sunshade_u", False)):
-        flags |= FLAG_SUNSHADE_U
-    if bool(getattr(sp, "sunshade_l", False)):
-        flags |= FLAG_SUNSHADE_L
     P.flags = flags
     return P
+
+
+def _stat_dict(state, params, ncell):
+    """STAT planes of ``state`` plus the per-cell SimParams arrays the step reads
+    (``cropfrac``, ``forganic``: the layout's ``sim.`` leaves)."""
+    stat = _leaf_dict(state, "STAT", ncell)
+    for f in L.STAT:
+        if f.leaf.startswith("sim."):
+            v = getattr(params, f.leaf[4:], None)
+            if v is not None:
+                stat[f.name] = np.asarray(v, dtype=np.float64).reshape((ncell,) + ((f.k,) if f.k > 1 else ()))
+    return stat
 
 
 def _leaf_dict(state, group, ncell):
@@ -190,7 +239,7 @@ def timestep_body(state, consts, params, dtime: float, device="cuda"):
     ncell = int(np.asarray(state.soil.tg).shape[0])
     dtype = _dtype_of(state)
     prog = _leaf_dict(state, "PROG", ncell)
-    stat = _leaf_dict(state, "STAT", ncell)
+    stat = _stat_dict(state, params, ncell)
     forc = {k: v[None] for k, v in _leaf_dict(state, "FORC", ncell).items()}
     cols = Columns.from_host(prog, stat, dtype=dtype, device=device, diag=True, acc=False)
     cols.run(cols.forcing(forc), P)
@@ -235,7 +284,7 @@ def run_hours(state, consts, params, forcing: dict, dtime: float, ch4_inund=None
     if dtype == torch.float64:
         P.flags = P.flags & ~(1 << 8)        # plain sums in float64
     prog = _leaf_dict(state, "PROG", ncell)
-    stat = _leaf_dict(state, "STAT", ncell)
+    stat = _stat_dict(state, params, ncell)
     if ch4_inund is not None:
         stat["f_inund"] = np.asarray(ch4_inund, dtype=np.float64)
     cols = Columns.from_host(prog, stat, dtype=dtype, device=device, acc=True)
@@ -298,9 +347,9 @@ def run_month_scan(state, consts, params, xs, nsoilcall: int, ndaypy: int, dtime
     Supported: one soil-BGC call per day (``nsoilcall`` 1), two radiation
     bands, no per-cell growth habits (``slot_habit``); the optional state
     modules the state carries (stress, ET parts, seasonal states with
-    photoperiod-gated senescence, NEE parts) advance as in the reference, with
-    the stomata switches of ``UNSUPPORTED_SWITCHES`` off.  ``iwet`` is not used
-    (the reference's day loop does not read it either)."""
+    photoperiod-gated senescence, NEE parts) advance as in the reference, and
+    the step's acclimation reads the seasonal state each day's start leaves.
+    ``iwet`` is not used (the reference's day loop does not read it either)."""
     from . import forcing as _forcing
     from .daily import DayLoop
     if int(nsoilcall) != 1 or int(nband) != 2:
@@ -317,7 +366,7 @@ def run_month_scan(state, consts, params, xs, nsoilcall: int, ndaypy: int, dtime
     P.flags |= FLAG_ACC | (FLAG_SOIL_MEANS if soil_means else 0) | parts_flags(state)
     dtype = _dtype_of(state)
     prog = _leaf_dict(state, "PROG", ncell)
-    stat = _leaf_dict(state, "STAT", ncell)
+    stat = _stat_dict(state, params, ncell)
     if ch4_hourly and ch4_args is not None:
         from .params import FLAG_ZWT_OBS
         f_inund, mp, zwt_obs = ch4_args

@@ -118,7 +118,20 @@ STAT = (
     Field("tco2mic", "vegetation.tco2mic"),
     Field("f_inund", "methane.f_inund"),
     Field("zwt_obs", "methane.zwt_obs"),   # observed wetland water table, m (NaN: the model's); read under FLAG_ZWT_OBS
+    # inputs of the IBIS 3.0 extensions, read only under their flags: the state of
+    # temperature acclimation (FLAG_ACCLIM; the day loop refreshes it each day), the
+    # day's mean air temperature of the state (FLAG_FROST), and the per-cell arrays
+    # of SimParams ("sim." leaves): the cropland share (FLAG_CROP) and the organic
+    # fraction of the soil solids per layer (FLAG_FORGANIC)
+    Field("acclim_x", "seasonal.acclim_x"),
+    Field("td", "atm.td"),
+    Field("cropfrac", "sim.cropfrac"),
+    Field("forganic", "sim.forganic", NSOILAY),
 )
+
+#: Leaf prefixes of fields that are not leaves of the base reference state: the
+#: wetland inputs, the optional seasonal module and per-cell SimParams arrays.
+OPTIONAL_LEAF_PREFIXES = ("methane.", "seasonal.", "sim.")
 
 FORC = (
     Field("ta", "atm.ta"),

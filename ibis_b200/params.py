@@ -62,6 +62,16 @@ PARAM_FIELDS: list[tuple[str, int, object]] = [
     ("vmax_pft", 12, (65e-6, 65e-6, 40e-6, 30e-6, 30e-6, 25e-6,
                       30e-6, 30e-6, 27.5e-6, 27.5e-6, 15e-6, 25e-6)),
     ("stressfac", 1, -5.0), ("cap_kn", 1, 0.15),
+    # IBIS 3.0 stomata extensions (stomata.py:98-159; all act only under their IBIS_FLAG_* switches):
+    # the per-PFT Ball-Berry slopes of coefm_mix; the acclimated PFTs (acclim_pfts as a 0/1 mask) and the
+    # per-PFT acclimation constants (the scalars acclim_s0/acclim_smax repeated when acclim_per_pft is off);
+    # the frost ramp on the day's mean air temperature, C
+    ("coefm_pft", 12, (10.0, 10.0, 10.0, 6.0, 10.0, 6.0, 10.0, 6.0, 9.0, 9.0, 4.0, 9.0)),
+    ("acclim_mask", 12, (0.0, 0.0, 0.0, 1.0, 0.0, 1.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0)),
+    ("acclim_s0_pft", 12, (-3.063,) * 12), ("acclim_smax_pft", 12, (17.72,) * 12),
+    ("frost_t0", 1, -5.0), ("frost_t1", 1, 5.0),
+    # --- CropParams of the cropland share's grass capacity (io/parameters.py:262-278; loops.py:218-231)
+    ("crop_vmax_scale_c3", 1, 1.0), ("crop_vmax_scale_c4", 1, 1.0), ("crop_c4_share", 1, -1.0),
     # --- soil constants of SimParams (loops.py:92-111)
     ("wpudmax", 1, 10.0), ("zwpmax", 1, 0.5), ("bperm", 1, 0.04),
     ("rhosoi_val", 1, 2650.0 * 0.99 + 1300.0 * 0.01), ("csoi_mineral_val", 1, 870.0 * 0.99 + 1920.0 * 0.01),
@@ -97,9 +107,25 @@ FLAG_KAHAN = 1 << 8            # compensated accumulation (FP32 kernels)
 FLAG_ZWT_OBS = 1 << 9          # observed wetland water table (STAT zwt_obs, NaN = the model's; methane.py:366-367)
 FLAG_ETPARTS = 1 << 10         # ET components accumulated apart, with FLAG_ACC (loops_gswp3.py:263-272)
 FLAG_NEEPARTS = 1 << 11        # day- and night-time NEE accumulated apart, with FLAG_ACC (loops_gswp3.py:274-281)
+# IBIS 3.0 extensions of the step (off: the F77 step).  Any of them selects the
+# extended kernel instantiations; the F77 kernels never carry their code.
+FLAG_VMAX_MIX = 1 << 12        # StomataParams.vmax_mix: big-leaf vmax = displayed-LAI-weighted mean (stomata.py:598-631)
+FLAG_COEFM_MIX = 1 << 13       # StomataParams.coefm_mix: big-leaf slope from coefm_pft (stomata.py:646-657)
+FLAG_GPP_CAPACITY = 1 << 14    # StomataParams.gpp_split_by_capacity: NPP shares by leaf area x vmax (loops_gswp3.py:197-205)
+FLAG_ACCLIM = 1 << 15          # StomataParams.acclim_on with a seasonal state: vmax x f_S(acclim_x) (loops.py:291-303)
+FLAG_ACCLIM_LIGHT = 1 << 16    # StomataParams.acclim_light: the big leaf's capacity factor also on the light limit
+FLAG_FROST = 1 << 17           # StomataParams.frost_on: frost ramp on atm.td, with FLAG_ACCLIM (loops.py:305-309)
+FLAG_CAP_SCALE_U = 1 << 18     # StomataParams.cap_scale_u: canopy-level co-limitation (stomata.py:889-896)
+FLAG_CAP_SCALE_L = 1 << 19     # StomataParams.cap_scale_l
+FLAG_LEAF_ONLY = 1 << 20       # StomataParams.scale_leaf_only: light scaling over leaves and stems (stomata.py:442-512)
+FLAG_CROP = 1 << 21            # SimParams.cropfrac present: grass capacity on the cropland share (loops.py:218-231)
+FLAG_FORGANIC = 1 << 22        # SimParams.forganic present: organic dry conductivity (soil_physics.py:74-77)
+X3_FLAGS = (FLAG_VMAX_MIX | FLAG_COEFM_MIX | FLAG_GPP_CAPACITY | FLAG_ACCLIM | FLAG_ACCLIM_LIGHT | FLAG_FROST
+            | FLAG_CAP_SCALE_U | FLAG_CAP_SCALE_L | FLAG_LEAF_ONLY | FLAG_CROP | FLAG_FORGANIC)
 
 KNOWN_FLAGS = (FLAG_BEDROCK | FLAG_H2O_CONSISTENT | FLAG_SUNSHADE_U | FLAG_SUNSHADE_L | FLAG_ACC
-               | FLAG_CH4 | FLAG_SOIL_MEANS | FLAG_DIAG | FLAG_KAHAN | FLAG_ZWT_OBS | FLAG_ETPARTS | FLAG_NEEPARTS)
+               | FLAG_CH4 | FLAG_SOIL_MEANS | FLAG_DIAG | FLAG_KAHAN | FLAG_ZWT_OBS | FLAG_ETPARTS | FLAG_NEEPARTS
+               | X3_FLAGS)
 
 # Default root profile (lower, upper) used by the synthetic columns; the reference keeps froot as a
 # state leaf vegetation.froot of shape (nsoilay, 2) shared by every cell.
@@ -272,8 +298,13 @@ def header_struct_text() -> str:
                     ("SUNSHADE_U", FLAG_SUNSHADE_U), ("SUNSHADE_L", FLAG_SUNSHADE_L),
                     ("ACC", FLAG_ACC), ("CH4", FLAG_CH4), ("SOIL_MEANS", FLAG_SOIL_MEANS),
                     ("DIAG", FLAG_DIAG), ("KAHAN", FLAG_KAHAN), ("ZWT_OBS", FLAG_ZWT_OBS),
-                    ("ETPARTS", FLAG_ETPARTS), ("NEEPARTS", FLAG_NEEPARTS)]:
+                    ("ETPARTS", FLAG_ETPARTS), ("NEEPARTS", FLAG_NEEPARTS),
+                    ("VMAX_MIX", FLAG_VMAX_MIX), ("COEFM_MIX", FLAG_COEFM_MIX), ("GPP_CAPACITY", FLAG_GPP_CAPACITY),
+                    ("ACCLIM", FLAG_ACCLIM), ("ACCLIM_LIGHT", FLAG_ACCLIM_LIGHT), ("FROST", FLAG_FROST),
+                    ("CAP_SCALE_U", FLAG_CAP_SCALE_U), ("CAP_SCALE_L", FLAG_CAP_SCALE_L),
+                    ("LEAF_ONLY", FLAG_LEAF_ONLY), ("CROP", FLAG_CROP), ("FORGANIC", FLAG_FORGANIC)]:
         lines.append(f"#define IBIS_FLAG_{nm} {val}u")
+    lines.append(f"#define IBIS_FLAGS_X3 {X3_FLAGS}u   /* any of these selects the IBIS 3.0 kernels */")
     lines.append("")
     lines.append("/* Parameters of the daily cadence (phenology, soil biogeochemistry), all double. */")
     lines.append("typedef struct IbisDayParams {")

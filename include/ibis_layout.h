@@ -85,7 +85,11 @@ enum {
     IBIS_STAT_TCO2MIC = 122,  /* vegetation.tco2mic */
     IBIS_STAT_F_INUND = 123,  /* methane.f_inund */
     IBIS_STAT_ZWT_OBS = 124,  /* methane.zwt_obs */
-    IBIS_STAT_COUNT = 125
+    IBIS_STAT_ACCLIM_X = 125,  /* seasonal.acclim_x */
+    IBIS_STAT_TD = 126,  /* atm.td */
+    IBIS_STAT_CROPFRAC = 127,  /* sim.cropfrac */
+    IBIS_STAT_FORGANIC = 128,  /* sim.forganic, 6 planes */
+    IBIS_STAT_COUNT = 134
 };
 
 /* FORC */
@@ -397,6 +401,15 @@ typedef struct IbisParams {
     double vmax_pft[12];
     double stressfac;
     double cap_kn;
+    double coefm_pft[12];
+    double acclim_mask[12];
+    double acclim_s0_pft[12];
+    double acclim_smax_pft[12];
+    double frost_t0;
+    double frost_t1;
+    double crop_vmax_scale_c3;
+    double crop_vmax_scale_c4;
+    double crop_c4_share;
     double wpudmax;
     double zwpmax;
     double bperm;
@@ -504,6 +517,15 @@ typedef struct IbisParams {
     A(vmax_pft, 12) \
     S(stressfac) \
     S(cap_kn) \
+    A(coefm_pft, 12) \
+    A(acclim_mask, 12) \
+    A(acclim_s0_pft, 12) \
+    A(acclim_smax_pft, 12) \
+    S(frost_t0) \
+    S(frost_t1) \
+    S(crop_vmax_scale_c3) \
+    S(crop_vmax_scale_c4) \
+    S(crop_c4_share) \
     S(wpudmax) \
     S(zwpmax) \
     S(bperm) \
@@ -547,6 +569,18 @@ typedef struct IbisParams {
 #define IBIS_FLAG_ZWT_OBS 512u
 #define IBIS_FLAG_ETPARTS 1024u
 #define IBIS_FLAG_NEEPARTS 2048u
+#define IBIS_FLAG_VMAX_MIX 4096u
+#define IBIS_FLAG_COEFM_MIX 8192u
+#define IBIS_FLAG_GPP_CAPACITY 16384u
+#define IBIS_FLAG_ACCLIM 32768u
+#define IBIS_FLAG_ACCLIM_LIGHT 65536u
+#define IBIS_FLAG_FROST 131072u
+#define IBIS_FLAG_CAP_SCALE_U 262144u
+#define IBIS_FLAG_CAP_SCALE_L 524288u
+#define IBIS_FLAG_LEAF_ONLY 1048576u
+#define IBIS_FLAG_CROP 2097152u
+#define IBIS_FLAG_FORGANIC 4194304u
+#define IBIS_FLAGS_X3 8384512u   /* any of these selects the IBIS 3.0 kernels */
 
 /* Parameters of the daily cadence (phenology, soil biogeochemistry), all double. */
 typedef struct IbisDayParams {

@@ -8,7 +8,8 @@ from __future__ import annotations
 
 import numpy as np
 
-from .physics import clip, cube, esat, qsat, dqsat, hvapf, hsubf
+from .physics import (clip, cube, esat, qsat, dqsat, hvapf, hsubf, FLAG_VMAX_MIX, FLAG_COEFM_MIX, FLAG_ACCLIM,
+                      FLAG_ACCLIM_LIGHT, FLAG_FROST, FLAG_CAP_SCALE_U, FLAG_CAP_SCALE_L, FLAG_LEAF_ONLY, FLAG_CROP)
 
 
 # ---------------------------------------------------------------------------
@@ -199,19 +200,128 @@ def colimit(j1, j2, theta):
     return np.minimum(q / theta, c / q)
 
 
-def c3_rate(par, ci, vmax, gstar, kc, ko, rdark, P):
+def c3_rate(par, ci, vmax, gstar, kc, ko, rdark, P, je_fac=None, f_light=None, f_cap=None):
+    """farquhar_c3 (stomata.py:228-276): je_fac scales the light-limited rate
+    (acclim_light); f_light / f_cap the canopy-level co-limitation (cap_scale)."""
     je = par * 4.59e-06 * P.alpha3 * (ci - gstar) / (ci + 2.0 * gstar)
+    if je_fac is not None:
+        je = je * je_fac
     jc = vmax * (ci - gstar) / (ci + kc * (1.0 + P.o2conc / ko))
     js = vmax / 2.2
+    if f_cap is not None:
+        je, jc, js, rdark = je * f_light, jc * f_cap, js * f_cap, rdark * f_cap
     ag = colimit(colimit(je, jc, P.theta3), js, P.beta3)
     return ag, ag - rdark
 
 
-def c4_rate(par, ci, vmax, rdark, P):
+def c4_rate(par, ci, vmax, rdark, P, je_fac=None, f_light=None, f_cap=None):
+    """farquhar_c4 (stomata.py:279-318), with the same optional factors as c3_rate."""
     je = par * 4.59e-06 * P.alpha4
+    if je_fac is not None:
+        je = je * je_fac
+    jc = vmax
     ji = 18.0e3 * vmax * ci
-    ag = colimit(colimit(je, vmax, P.theta4), ji, P.beta4)
+    if f_cap is not None:
+        je, jc, ji, rdark = je * f_light, jc * f_cap, ji * f_cap, rdark * f_cap
+    ag = colimit(colimit(je, jc, P.theta4), ji, P.beta4)
     return ag, ag - rdark
+
+
+BROADLEAF_PFTS = (0, 1, 2, 4, 6)
+CONIFER_PFTS = (3, 5, 7)
+SHRUB_PFTS = (8, 9)
+
+
+def mix_pft(frac, vp, idx, fallback, eps=1e-6):
+    """_mix_vmax (stomata.py:580-590): the displayed-LAI-weighted mean of a per-PFT
+    table over one big leaf's PFTs; ``fallback`` where they have no leaves."""
+    ix = list(idx)
+    w = frac[:, ix]
+    tot = np.sum(w, axis=1)
+    vpi = vp[:, ix] if vp.ndim == 2 else vp[ix][None, :]
+    mixed = np.sum(w * vpi, axis=1) / np.maximum(tot, eps)
+    return np.where(tot > eps, mixed, fallback)
+
+
+def crop_increments(P):
+    """Per-PFT ``g - 1`` per unit cropland share of crop_vfac (loops.py:218-231): the C4
+    (PFT 10) and C3 (PFT 11) scales less one, or the share-mixed scale less one; the
+    reference forms them on float32 masks, so they are float32 values."""
+    f32 = np.float32
+    q = P.crop_c4_share
+    inc = np.zeros(12)
+    if q < 0.0:
+        inc[10] = float(f32(P.crop_vmax_scale_c4 - 1.0))
+        inc[11] = float(f32(P.crop_vmax_scale_c3 - 1.0))
+    else:
+        qc = min(max(q, 0.0), 1.0)
+        s_mix = (1.0 - qc) * P.crop_vmax_scale_c3 + qc * P.crop_vmax_scale_c4
+        inc[10] = inc[11] = float(f32(s_mix - 1.0))
+    return inc
+
+
+def capacity_factor(S, P):
+    """The per-PFT factor on vmax (None: the F77 step): temperature acclimation of the
+    PFTs in acclim_pfts with the frost ramp (loops.py:291-309), then the cropland
+    share's grass capacity (crop_vfac, loops.py:218-231)."""
+    vfac = None
+    if P.flags & FLAG_ACCLIM:
+        m = np.asarray(P.acclim_mask, dtype=np.float64)[None, :]
+        fs = clip((S["acclim_x"][:, None] - np.asarray(P.acclim_s0_pft)[None, :])
+                  / np.asarray(P.acclim_smax_pft)[None, :], 0.0, 1.0)
+        vfac = 1.0 - m + m * fs
+        if P.flags & FLAG_FROST:
+            ff = clip((S["td"] - 273.16 - P.frost_t0) / (P.frost_t1 - P.frost_t0), 0.0, 1.0)
+            vfac = vfac * (1.0 - m + m * ff[:, None])
+    if P.flags & FLAG_CROP:
+        g = 1.0 + S["cropfrac"][:, None] * crop_increments(P)[None, :]
+        vfac = g if vfac is None else vfac * g
+    return vfac
+
+
+def big_leaves(S, P):
+    """Nominal vmax, light-rate factor (None: none) and Ball-Berry slope of the five big
+    leaves (ub, uc, ls, l3, l4): _select_vmax_upper / _select_vmax_shrub with vmax_mix,
+    acclim_light and _slopes with coefm_mix (stomata.py:592-660, 800-835)."""
+    exist, frac = S["exist"], S["frac"]
+    eps = P.epsilon
+    vp = np.asarray(P.vmax_pft, dtype=np.float64)
+    vfac = capacity_factor(S, P)
+    mix = bool(P.flags & FLAG_VMAX_MIX)
+
+    def select(v):
+        col = (lambda k: v[:, k]) if v.ndim == 2 else (lambda k: v[k])
+        ub = np.where(exist[:, 0] > 0.5, col(0), np.where(exist[:, 2] > 0.5, col(2), col(4)))
+        uc = np.where(exist[:, 3] > 0.5, col(3), col(5))
+        ls = np.broadcast_to(col(8), frac.shape[:1])
+        if mix:
+            ub = mix_pft(frac, v, BROADLEAF_PFTS, ub)
+            uc = mix_pft(frac, v, CONIFER_PFTS, uc)
+            ls = mix_pft(frac, v, SHRUB_PFTS, ls)
+        return ub, uc, ls, np.broadcast_to(col(11), frac.shape[:1]), np.broadcast_to(col(10), frac.shape[:1])
+
+    veff = vp if vfac is None else vp[None, :] * vfac
+    vn = select(veff)
+    je = (None,) * 5
+    if (P.flags & FLAG_ACCLIM_LIGHT) and vfac is not None:
+        raw = select(vp[None, :])
+        je = tuple(a / np.maximum(b, eps) for a, b in zip(vn, raw))
+    cm = np.asarray(P.coefm, dtype=np.float64)
+    if P.flags & FLAG_COEFM_MIX:
+        cp = np.asarray(P.coefm_pft, dtype=np.float64)
+        n = frac.shape[0]
+        slopes = (mix_pft(frac, cp, BROADLEAF_PFTS, cm[0]), mix_pft(frac, cp, CONIFER_PFTS, cm[1]),
+                  mix_pft(frac, cp, SHRUB_PFTS, cm[2]), np.full(n, cp[11]), np.full(n, cp[10]))
+    else:
+        slopes = (cm[0], cm[1], cm[2], cm[4], cm[3])
+    return vn, je, slopes
+
+
+def capacity_integral(lai, kn):
+    """_capacity_integral (stomata.py:370-375): (1 - e^-Kn L)/(Kn L), 0 without leaves."""
+    x = kn * lai
+    f = np.where(x > 1.0e-4, -np.expm1(-x) / np.maximum(x, 1.0e-4), 1.0 - 0.5 * x)
+    return np.where(lai > 0.0, f, 0.0)
 
 
 def kinetics(tleaf, P):
@@ -237,7 +347,8 @@ def ball_berry(an, cs0, gs0, ci0, gb, rh, m, b0, stress, gmin, cmin, imin, P):
 
 
 def light_scaling(toppar, k, h, sc, lai, sai, a10s, a10d, P):
-    """canopy_scaling (stomata.py:442-512), F77 denominator k*LAI."""
+    """canopy_scaling (stomata.py:442-512): denominator k*LAI (F77) or, with
+    scale_leaf_only, k*(LAI+SAI)."""
     ext = (k * sc[:, 0] + h * sc[:, 1] - h * sc[:, 2]) / np.maximum(sc[:, 3], P.epsilon)
     ext = clip(ext, 0.1, 10.0)
     pxai = ext * (lai + sai)
@@ -245,7 +356,8 @@ def light_scaling(toppar, k, h, sc, lai, sai, a10s, a10d, P):
     zw = np.exp(-1.0 / (10.0 * 86400.0 / P.dtime))
     has = plai > 0.0
     day = toppar > 10.0
-    sday = (1.0 - np.exp(-pxai)) / np.maximum(plai, P.epsilon)
+    denom = pxai if P.flags & FLAG_LEAF_ONLY else plai
+    sday = (1.0 - np.exp(-pxai)) / np.maximum(denom, P.epsilon)
     upd = has & day
     a10s_n = np.where(upd, zw * a10s + (1.0 - zw) * sday * toppar, a10s)
     a10d_n = np.where(upd, zw * a10d + (1.0 - zw) * toppar, a10d)
@@ -291,44 +403,48 @@ def stomata(tu, tl, t12, t34, q12, q34, su, sl, ps, R, st, fwetu, fwetl, S, stre
             sun_u=False, sun_l=False):
     """One stomata pass (stomata.py:732-1080). ``st`` holds the carried ci/gs/cs and a10 values."""
     eps = P.epsilon
-    lai, sai, exist = S["lai"], S["sai"], S["exist"]
-    vp = np.asarray(P.vmax_pft)
-    gam, cm, cb, gmin = (np.asarray(P.gamma), np.asarray(P.coefm), np.asarray(P.coefb), np.asarray(P.gsmin))
+    lai, sai = S["lai"], S["sai"]
+    gam, cb, gmin = (np.asarray(P.gamma), np.asarray(P.coefb), np.asarray(P.gsmin))
+    (vub, vuc, vls, vl3, vl4), (jub, juc, jls, jl3, jl4), (mub, muc, mls, ml3, ml4) = big_leaves(S, P)
+    cap_u = bool(P.flags & FLAG_CAP_SCALE_U) and not sun_u
+    cap_l = bool(P.flags & FLAG_CAP_SCALE_L) and not sun_l
     out = {}
-    # ---- upper canopy
+    # ---- upper canopy: broadleaf (group 0) and conifer (group 1)
     kc, ko, gst, vm3, _ = kinetics(tu, P)
     gmn = 1.05 * gst
     gb = clip(su * 25.5, 0.1, 10.0)
     rh = np.maximum(0.30, q12 / np.maximum(qsat(esat(t12), ps), eps))
-    vub = np.where(exist[:, 0] > 0.5, vp[0], np.where(exist[:, 2] > 0.5, vp[2], vp[4]))
-    vuc = np.where(exist[:, 3] > 0.5, vp[3], vp[5])
     if sun_u:
         ssu = sunshade(R["scalcoefu"], R["dbeamu"], R["termu6"], R["termu7"], lai[:, 1], sai[:, 1], P)
     leaves = {}
-    for j, (vn, g) in enumerate(((vub, 0), (vuc, 1))):
+    for j, (vn, g, jf, m) in enumerate(((vub, 0, jub, mub), (vuc, 1, juc, muc))):
         ci = clip(st["ci_upper"][:, j], gmn, P.cimax)
         vmax = vn * vm3 * stresstu
         rd = gam[g] * vn * vm3
-        ag, an = c3_rate(R["topparu"], ci, vmax, gst, kc, ko, rd, P)
+        ag, an = c3_rate(R["topparu"], ci, vmax, gst, kc, ko, rd, P, je_fac=jf)
         if sun_u:
-            agc, anc = _sunshade_rate(ssu, lai[:, 1], lambda par, v: c3_rate(par, ci, vmax * v, gst, kc, ko, rd * v, P))
+            agc, anc = _sunshade_rate(ssu, lai[:, 1],
+                                      lambda par, v: c3_rate(par, ci, vmax * v, gst, kc, ko, rd * v, P, je_fac=jf))
             bb_an = anc
         else:
             agc = anc = None
             bb_an = an
-        cs, gs, ci_n = ball_berry(bb_an, st["cs_upper"][:, j], st["gs_upper"][:, j], ci, gb, rh, cm[g], cb[g],
+        cs, gs, ci_n = ball_berry(bb_an, st["cs_upper"][:, j], st["gs_upper"][:, j], ci, gb, rh, m, cb[g],
                                   stresstu, gmin[g], gmn, gmn, P)
-        leaves[j] = (ag, an, agc, anc, cs, gs, ci_n)
+        leaves[j] = (ag, an, agc, anc, cs, gs, ci_n, ci, vmax, rd, jf, m)
     scale_u, out["a10scalparamu"], out["a10daylightu"] = light_scaling(
         R["topparu"], R["termu6"], R["termu7"], R["scalcoefu"], lai[:, 1], sai[:, 1],
         st["a10scalparamu"], st["a10daylightu"], P)
+    fcap_u = capacity_integral(lai[:, 1], P.cap_kn) if cap_u else None
     ag_u, an_u, tc_u = [], [], []
     for j, g in ((0, 0), (1, 1)):
-        ag, an, agc, anc, cs, gs, ci_n = leaves[j]
-        if not sun_u:
+        ag, an, agc, anc, cs, gs, ci_n, ci0, vmax, rd, jf, m = leaves[j]
+        if cap_u:
+            agc, anc = c3_rate(R["topparu"], ci0, vmax, gst, kc, ko, rd, P, je_fac=jf, f_light=scale_u, f_cap=fcap_u)
+        elif not sun_u:
             agc, anc = ag * scale_u, an * scale_u
         csc = np.maximum(gmn, P.co2conc - anc / gb)
-        gsc = np.maximum(np.maximum(gmin[g], cb[g] * stresstu), cm[g] * anc * rh / csc + cb[g] * stresstu)
+        gsc = np.maximum(np.maximum(gmin[g], cb[g] * stresstu), m * anc * rh / csc + cb[g] * stresstu)
         tc_u.append(total_conductance(su, gsc))
         ag_u.append(agc * (1.0 - fwetu))
         an_u.append(anc * (1.0 - fwetu))
@@ -346,37 +462,45 @@ def stomata(tu, tl, t12, t34, q12, q34, su, sl, ps, R, st, fwetu, fwetl, S, stre
     rh = np.maximum(0.30, q34 / np.maximum(qsat(esat(t34), ps), eps))
     if sun_l:
         ssl = sunshade(R["scalcoefl"], R["dbeaml"], R["terml6"], R["terml7"], lai[:, 0], sai[:, 0], P)
-    spec = ((0, vp[8], 2, False), (1, vp[11], 4, False), (2, vp[10], 3, True))
+    spec = ((0, vls, 2, False, jls, mls), (1, vl3, 4, False, jl3, ml3), (2, vl4, 3, True, jl4, ml4))
     leaves = {}
-    for j, vn, g, c4 in spec:
+    for j, vn, g, c4, jf, m in spec:
         ci = clip(st["ci_lower"][:, j], 0.0 if c4 else gmn, P.cimax)
         vmax = vn * (vm4 if c4 else vm3) * stresstl
         rd = gam[g] * vn * (vm4 if c4 else vm3)
         if c4:
-            ag, an = c4_rate(R["topparl"], ci, vmax, rd, P)
-            fn = (lambda par, v, ci=ci, vmax=vmax, rd=rd: c4_rate(par, ci, vmax * v, rd * v, P))
+            ag, an = c4_rate(R["topparl"], ci, vmax, rd, P, je_fac=jf)
+            fn = (lambda par, v, ci=ci, vmax=vmax, rd=rd, jf=jf: c4_rate(par, ci, vmax * v, rd * v, P, je_fac=jf))
         else:
-            ag, an = c3_rate(R["topparl"], ci, vmax, gst, kc, ko, rd, P)
-            fn = (lambda par, v, ci=ci, vmax=vmax, rd=rd: c3_rate(par, ci, vmax * v, gst, kc, ko, rd * v, P))
+            ag, an = c3_rate(R["topparl"], ci, vmax, gst, kc, ko, rd, P, je_fac=jf)
+            fn = (lambda par, v, ci=ci, vmax=vmax, rd=rd, jf=jf:
+                  c3_rate(par, ci, vmax * v, gst, kc, ko, rd * v, P, je_fac=jf))
         if sun_l:
             agc, anc = _sunshade_rate(ssl, lai[:, 0], fn)
             bb_an = anc
         else:
             agc = anc = None
             bb_an = an
-        cs, gs, ci_n = ball_berry(bb_an, st["cs_lower"][:, j], st["gs_lower"][:, j], ci, gb, rh, cm[g], cb[g],
+        cs, gs, ci_n = ball_berry(bb_an, st["cs_lower"][:, j], st["gs_lower"][:, j], ci, gb, rh, m, cb[g],
                                   stresstl, gmin[g], 1.0e-8 if c4 else gmn, 0.0 if c4 else gmn, P)
-        leaves[j] = (ag, an, agc, anc, cs, gs, ci_n, g, c4)
+        leaves[j] = (ag, an, agc, anc, cs, gs, ci_n, g, c4, ci, vmax, rd, jf, m)
     scale_l, out["a10scalparaml"], out["a10daylightl"] = light_scaling(
         R["topparl"], R["terml6"], R["terml7"], R["scalcoefl"], lai[:, 0], sai[:, 0],
         st["a10scalparaml"], st["a10daylightl"], P)
+    fcap_l = capacity_integral(lai[:, 0], P.cap_kn) if cap_l else None
     ag_l, an_l, tc_l = [], [], []
     for j in range(3):
-        ag, an, agc, anc, cs, gs, ci_n, g, c4 = leaves[j]
-        if not sun_l:
+        ag, an, agc, anc, cs, gs, ci_n, g, c4, ci0, vmax, rd, jf, m = leaves[j]
+        if cap_l:
+            if c4:
+                agc, anc = c4_rate(R["topparl"], ci0, vmax, rd, P, je_fac=jf, f_light=scale_l, f_cap=fcap_l)
+            else:
+                agc, anc = c3_rate(R["topparl"], ci0, vmax, gst, kc, ko, rd, P, je_fac=jf, f_light=scale_l,
+                                   f_cap=fcap_l)
+        elif not sun_l:
             agc, anc = ag * scale_l, an * scale_l
         csc = np.maximum(1.0e-8 if c4 else gmn, P.co2conc - anc / gb)
-        gsc = np.maximum(np.maximum(gmin[g], cb[g] * stresstl), cm[g] * anc * rh / csc + cb[g] * stresstl)
+        gsc = np.maximum(np.maximum(gmin[g], cb[g] * stresstl), m * anc * rh / csc + cb[g] * stresstl)
         tc_l.append(total_conductance(sl, gsc))
         ag_l.append(agc * (1.0 - fwetl))
         an_l.append(anc * (1.0 - fwetl))

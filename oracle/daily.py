@@ -113,6 +113,8 @@ def day_begin(day: dict, stat: dict, acc: dict, td, P, DP):
     sen_u = sen_l = None
     if DP.seasonal_on:
         day, sen_u, sen_l = seasonal_states(day, td, DP)
+        # the day's steps read the advanced acclimation state (loops.py:294-303)
+        stat = dict(stat, acclim_x=day["acclim_x"])
     day, stat = pheno(day, stat, means, td, acc["stresstu_last"], acc["stresstl_last"], DP, P.epsilon, sen_u, sen_l)
     acc = dict(acc)
     for k in DAILY_SUMS:

@@ -9,6 +9,20 @@ from __future__ import annotations
 
 import numpy as np
 
+# IBIS 3.0 extensions of the step, as carried in ``P.flags`` (the values of
+# ibis_b200.params.FLAG_*; off = the F77 step)
+FLAG_VMAX_MIX = 1 << 12
+FLAG_COEFM_MIX = 1 << 13
+FLAG_GPP_CAPACITY = 1 << 14
+FLAG_ACCLIM = 1 << 15
+FLAG_ACCLIM_LIGHT = 1 << 16
+FLAG_FROST = 1 << 17
+FLAG_CAP_SCALE_U = 1 << 18
+FLAG_CAP_SCALE_L = 1 << 19
+FLAG_LEAF_ONLY = 1 << 20
+FLAG_CROP = 1 << 21
+FLAG_FORGANIC = 1 << 22
+
 # ---------------------------------------------------------------------------
 # small helpers
 # ---------------------------------------------------------------------------
@@ -115,6 +129,9 @@ def setsoi(S, prog, tsno0, ta, P):
     pliq = poros * wsoi * (1.0 - wisoi)
     pice = poros * wisoi
     dry = fs * 0.300 + fsilt * 0.265 + fc * 0.250
+    if P.flags & FLAG_FORGANIC:                 # organic solids (soil_physics.py:74-77)
+        fo = S["forganic"]
+        dry = (1.0 - fo) * dry + fo * 0.05
     consoi = dry * (56.0 ** pliq) * (224.0 ** pice)
 
     wpud, wipud = prog["wpud"], prog["wipud"]

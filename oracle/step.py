@@ -13,7 +13,7 @@ from __future__ import annotations
 
 import numpy as np
 
-from .physics import clip, cube, setsoi, fwetcal, cascade, radiation, evap_intercepted
+from .physics import clip, cube, setsoi, fwetcal, cascade, radiation, evap_intercepted, FLAG_GPP_CAPACITY
 from .canopy import aero_geometry, transfer, weight_veg, weight_snow, stomata, turvap
 from .column import (snow_block, water_bounds, soil_water, soil_heat, phase_change, puddle_phase,
                      fire_counters, methane)
@@ -284,8 +284,31 @@ def respiration_rates(P):
     return rwood, rroot, keep
 
 
+def capacity_shares(frac, vp, idx, eps=1e-12):
+    """capacity_shares (stomata.py:566-577): a big leaf's GPP shares by leaf area x vmax,
+    re-normalised to the leaf-area sum; the leaf-area shares where there is no capacity."""
+    ix = list(idx)
+    f = frac[:, ix]
+    w = f * np.asarray(vp)[ix][None, :]
+    tw = np.sum(w, axis=1, keepdims=True)
+    tf = np.sum(f, axis=1, keepdims=True)
+    return np.where(tw > eps, w / np.maximum(tw, eps) * tf, f)
+
+
+def gpp_shares(frac, P):
+    """Per-PFT shares of the big leaves' GPP in the NPP sums: the leaf-area fractions
+    (F77), or with gpp_split_by_capacity the capacity shares (loops_gswp3.py:197-205)."""
+    if not P.flags & FLAG_GPP_CAPACITY:
+        return frac
+    share = frac.copy()
+    for idx in ((0, 1, 2, 4, 6), (3, 5, 7), (8, 9)):
+        share[:, list(idx)] = capacity_shares(frac, P.vmax_pft, idx)
+    return share
+
+
 def accumulate(acc, new, D, S, F, P):
-    """Day/annual accumulators of _step_body (loops_gswp3.py:161-302), F77 GPP split."""
+    """Day/annual accumulators of _step_body (loops_gswp3.py:161-302), with the F77 or
+    the capacity split of each big leaf's GPP among its PFTs."""
     dt = P.dtime
     froot = np.asarray(P.froot).reshape(6, 2)
     an_ub, an_uc = D["an_upper"][:, 0], D["an_upper"][:, 1]
@@ -303,16 +326,17 @@ def accumulate(acc, new, D, S, F, P):
     yn_old = acc["aynpp"]
     yn = yn_old.copy()
     cbw, cbr, sap = S["cbiow"], S["cbior"], S["sapfrac"]
+    share = gpp_shares(frac, P)
     for j in (0, 1, 2, 4, 6):
-        g = an_ub * frac[:, j] * lai_u * fu
+        g = an_ub * share[:, j] * lai_u * fu
         r = rwood[j] * cbw[:, j] * sap * funca + rroot[j] * cbr[:, j] * funcb
         yn[:, j] = yn[:, j] + keep[j] * (g - r) * cf
     for j in (3, 5, 7):
-        g = an_uc * frac[:, j] * lai_u * fu
+        g = an_uc * share[:, j] * lai_u * fu
         r = rwood[j] * cbw[:, j] * sap * funca + rroot[j] * cbr[:, j] * funcb
         yn[:, j] = yn[:, j] + keep[j] * (g - r) * cf
     for j in (8, 9):
-        g = an_ls * frac[:, j] * lai_l * fl * smask
+        g = an_ls * share[:, j] * lai_l * fl * smask
         r = rwood[j] * cbw[:, j] * funca + rroot[j] * cbr[:, j] * funcb
         yn[:, j] = yn[:, j] + keep[j] * (g - r) * cf
     g = an_l4 * frac[:, 10] * lai_l * fl * smask

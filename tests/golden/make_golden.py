@@ -63,12 +63,19 @@ def _a(x):
     return jnp.asarray(np.asarray(x, dtype=np.float64))
 
 
-def reference_state(wl, parts=False):
+def reference_state(wl, parts=False, seasonal=False):
     """IBISState (float64) holding the workload's prognostic and static fields
-    (with ``parts`` also the optional ET/NEE component modules)."""
+    (with ``parts`` also the optional ET/NEE component modules, with ``seasonal``
+    the seasonal module -- and the stress and ET-part modules it brings -- holding
+    the workload's acclimation state, and the day's mean air temperature)."""
     n = wl.ncell
     bed = bool(wl.params.flags & FLAG_BEDROCK)
-    st = create_ibis_state(GridConfig(nlon=2, nlat=1, npoi=n, nbedrock=3 if bed else 0), with_neeparts=parts)
+    st = create_ibis_state(GridConfig(nlon=2, nlat=1, npoi=n, nbedrock=3 if bed else 0), with_neeparts=parts,
+                           with_seasonal=seasonal)
+    if seasonal:
+        st = dataclasses.replace(st, seasonal=dataclasses.replace(st.seasonal, acclim_x=_a(wl.stat["acclim_x"])))
+    if "td" in wl.stat:
+        st = dataclasses.replace(st, atm=dataclasses.replace(st.atm, td=_a(wl.stat["td"])))
     P, S = wl.prog, wl.stat
     hsoi = np.zeros(L.NSOILAY + 1)
     hsoi[:L.NSOILAY] = wl.params.hsoi
@@ -144,10 +151,10 @@ def snapshot(st):
     return out
 
 
-def run_steps(wl, record):
+def run_steps(wl, record, ref=None):
+    """timestep_body hour by hour; ``ref`` = (params, state) built by the caller."""
     consts = get_constants()
-    params = reference_params(wl)
-    st = reference_state(wl)
+    params, st = ref if ref is not None else (reference_params(wl), reference_state(wl))
     snaps = {}
     for h in range(wl.nhour):
         st = set_forcing(st, wl.forcing_at(h))
@@ -157,13 +164,18 @@ def run_steps(wl, record):
     return snaps
 
 
-def run_day_accumulators(wl, parts=False):
+def run_day_accumulators(wl, parts=False, ref=None):
     """_run_day_inner over 24 hourly steps with CH4 and soil means on (and with
-    ``parts`` the ET/NEE component modules attached)."""
+    ``parts`` the ET/NEE component modules attached; ``ref`` = (params, state)
+    built by the caller, whose ET/NEE modules are recorded when present)."""
     assert wl.nhour == 24
     consts = get_constants()
-    params = reference_params(wl)
-    st = reference_state(wl, parts)
+    if ref is not None:
+        params, st = ref
+        parts = st.etparts is not None
+    else:
+        params = reference_params(wl)
+        st = reference_state(wl, parts)
     F = wl.forc
 
     def fake_diurnal(time, jday, dw, lat, plens, startp, endp, key, dtime, nband=2):
@@ -197,7 +209,7 @@ def run_day_accumulators(wl, parts=False):
     out["acc.tg_mean"] = np.asarray(acc[4], dtype=np.float64)
     if parts:
         for f in L.ACC:
-            if f.leaf.startswith(("etparts.", "neeparts.")):
+            if f.leaf.startswith(("etparts.", "neeparts.")) and getattr(st_out, f.leaf.split(".")[0]) is not None:
                 out["acc." + f.name] = get(st_out, f.leaf)
     return out
 
@@ -264,6 +276,80 @@ def build_case(name, spec):
         p.rwood, p.rroot, p.rgrowth = (np.full(12, f(p.rwood[0])), np.full(12, f(p.rroot[0])),
                                         np.full(12, f(p.rgrowth[0])))
     return wl
+
+
+# The IBIS 3.0 extensions of the step, run by the reference with its own switches:
+# "release" takes the stomata, soil-BGC respiration and methane sections of the
+# release parameter file (loaded by the reference's own loaders) on 16 columns for
+# a day with the accumulators and a seasonal state; "switches" turns on the
+# switches that file leaves off (canopy-level capacity scaling on both stories,
+# leaf-only light scaling, acclimation of four PFTs with the light-rate factor and
+# the frost ramp, the cropland share's grass capacity, organic soil solids).
+X3_CASES = {
+    "release": dict(ncell=16, nhour=24, seed=41, record=(1, 6, 24), day=True,
+                    yaml="configs/params/params_31s_ch4h.yaml"),
+    "switches": dict(ncell=12, nhour=6, seed=42, record=(1, 6),
+                     stomata=dict(cap_scale_u=True, cap_scale_l=True, scale_leaf_only=True, acclim_on=True,
+                                  acclim_pfts=(3, 5, 8, 10), acclim_light=True, frost_on=True, frost_t0=-8.0,
+                                  frost_t1=8.0, cap_kn=0.2),
+                     crop=dict(vmax_scale_c3=0.33, vmax_scale_c4=1.16, c4_share=-1.0), forganic=True),
+}
+
+
+def build_x3_case(name, spec):
+    """Workload, reference parameters and reference state of an IBIS 3.0 case; the
+    workload's flat parameters come from the drop-in's mapping of the reference
+    objects (so the case also pins that mapping)."""
+    from ibis.io.physics_params import (load_physics_params, build_stomata_params, build_bgc_params,
+                                        build_methane_params)
+    from ibis.io.parameters import CropParams
+    from ibis_b200 import dropin
+    from ibis_b200.params import FLAG_KAHAN, FLAG_ETPARTS
+    wl = synth.make_workload(spec["ncell"], spec["nhour"], seed=spec["seed"], edge_cases=True, bedrock=True)
+    n = wl.ncell
+    rng = np.random.Generator(np.random.PCG64(spec["seed"] + 2000))
+    wl.stat["acclim_x"] = rng.uniform(-12.0, 28.0, n)
+    wl.stat["td"] = rng.uniform(262.0, 290.0, n)
+    run_flags = FLAG_KAHAN
+    if spec.get("day"):
+        run_flags |= FLAG_ACC | FLAG_CH4 | FLAG_SOIL_MEANS
+        wl.forc["fira"][:] = wl.forc["fira"][0][None, :]
+    params = reference_params(wl)
+    if "yaml" in spec:
+        d = load_physics_params(os.path.join(REF, spec["yaml"]))
+        params = dataclasses.replace(params, stomata_params=build_stomata_params(d), bgc_params=build_bgc_params(d),
+                                     methane=build_methane_params(d),
+                                     h2o_consistent_weights=bool(d.get("soil", {}).get("h2o_consistent_weights")))
+    else:
+        params = dataclasses.replace(params, stomata_params=dataclasses.replace(params.stomata_params,
+                                                                              **spec["stomata"]))
+    if "crop" in spec:
+        wl.stat["cropfrac"] = rng.uniform(0.0, 1.0, n)
+        params = dataclasses.replace(params, crop=CropParams(**spec["crop"]), cropfrac=_a(wl.stat["cropfrac"]))
+    if spec.get("forganic"):
+        wl.stat["forganic"] = rng.uniform(0.0, 0.6, (n, L.NSOILAY))
+        params = dataclasses.replace(params, forganic=_a(wl.stat["forganic"]))
+    st = reference_state(wl, seasonal=True)
+    P = dropin.step_params(st, get_constants(), params, float(wl.params.dtime))
+    P.flags |= run_flags | (FLAG_ETPARTS if spec.get("day") else 0)
+    wl.params = P
+    return wl, params, st
+
+
+def write_x3_case(name):
+    spec = X3_CASES[name]
+    wl, params, st = build_x3_case(name, spec)
+    out = pack_inputs(wl)
+    for h, snap in run_steps(wl, set(spec["record"]), ref=(params, st)).items():
+        for k, v in snap.items():
+            out[f"out.{h}.{k}"] = v
+    if spec.get("day"):
+        for k, v in run_day_accumulators(wl, ref=(params, st)).items():
+            out[f"day.{k}"] = v
+    out["meta.record"] = np.asarray(spec["record"])
+    path = os.path.join(HERE, f"{name}.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path}: {len(out)} arrays, {os.path.getsize(path)} bytes")
 
 
 RESTART = "/root/reference/verify_out_stage1/site_transient_1996.npz"
@@ -662,8 +748,11 @@ def main():
         write_days_case(jday0=250, modules=True)
     if args.only in (None, "restart_modules"):
         write_restart_modules_case()
+    for name in X3_CASES:
+        if args.only in (None, name):
+            write_x3_case(name)
     if args.only in ("restart_leaves", "restart_1996", "diurnal", "days", "methane_month", "observed_sw",
-                     "day_parts", "days_modules", "restart_modules"):
+                     "day_parts", "days_modules", "restart_modules") + tuple(X3_CASES):
         return
     for name, spec in CASES.items():
         if args.only and name != args.only:

@@ -22,7 +22,8 @@ class Case:
         self.forc = {k[8:]: v for k, v in self.z.items() if k.startswith("in.forc.")}
         P = StepParams()
         for name_, n, _ in PARAM_FIELDS:
-            setattr(P, name_, self.z["in.param." + name_])
+            if "in.param." + name_ in self.z:      # fixtures written before a parameter existed hold its default
+                setattr(P, name_, self.z["in.param." + name_])
         P.flags = int(self.z["in.param.flags"])
         self.params = P
         self.ncell = self.prog["tg"].shape[0]

@@ -32,7 +32,7 @@ def test_step_rejects_bad_shapes(so):
         assert so.ibis_step_f32(DEV, DEV, DEV, NUL, DEV, ncell, ld, nstep, p, NUL, NUL) == EINVAL
     assert so.ibis_step_f32(NUL, DEV, DEV, NUL, DEV, 30, 32, 1, p, NUL, NUL) == EINVAL
     bad = StepParams().to_c()
-    bad.flags = 1 << 20
+    bad.flags = 1 << 30                      # no such variant
     assert so.ibis_step_f32(DEV, DEV, DEV, NUL, DEV, 30, 32, 1, ctypes.byref(bad), NUL, NUL) == EINVAL
 
 

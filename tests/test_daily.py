@@ -52,7 +52,8 @@ def load_case(gold=GOLD):
     acc0 = restart.group_from_leaves(leaves, "ACC", n)
     P = StepParams()
     for name, _, _ in PARAM_FIELDS:
-        setattr(P, name, z["in.param." + name])
+        if "in.param." + name in z:
+            setattr(P, name, z["in.param." + name])
     P.flags = (int(z["in.param.flags"]) | FLAG_ACC) & ~(FLAG_CH4 | FLAG_KAHAN)
     return z, n, prog, stat, day, acc0, P
 
@@ -578,7 +579,7 @@ def _param_tree(z, lat_deg):
 
     root = types.SimpleNamespace()
     for name, path in dropin.PARAM_PATHS.items():
-        if path.startswith(("params.", "consts.")):
+        if path.startswith(("params.", "consts.")) and "in.param." + name in z:
             v = z["in.param." + name]
             put(root, path, v if np.size(v) > 1 else float(v))
     for name, path in dropin.DAY_PARAM_PATHS.items():

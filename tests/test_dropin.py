@@ -103,7 +103,7 @@ def _mock(case, h=0):
     bed = bool(P.flags & FLAG_BEDROCK)
     leaves = {}
     for f in L.PROG + L.STAT:
-        if f.leaf.startswith("methane.") or (f.name == "tsoi_deep" and not bed):
+        if f.leaf.startswith(L.OPTIONAL_LEAF_PREFIXES) or (f.name == "tsoi_deep" and not bed):
             continue
         src = case.prog if f in L.PROG else case.stat
         leaves["state." + f.leaf] = np.asarray(src[f.name], dtype=np.float64).copy()

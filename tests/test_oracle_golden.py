@@ -74,3 +74,65 @@ def test_oracle_matches_reference_et_and_nee_parts():
     np.testing.assert_allclose(acc["et_trans"] + acc["et_interc"] + acc["et_soilev"] + acc["et_snowsub"],
                                acc["adaet"], rtol=1e-12, atol=1e-12)
     assert np.any(acc["nee_night"] != 0) and np.any(acc["nee_day"] != 0) and np.any(acc["et_snowsub"] != 0)
+
+
+X3_CASES = ("release", "switches")
+
+
+@pytest.mark.parametrize("name", X3_CASES)
+def test_oracle_matches_reference_ibis3_steps(name):
+    """The IBIS 3.0 extensions of the step (vmax and slope mixing, capacity split,
+    acclimation with per-PFT constants, light-rate factor, frost ramp, canopy-level
+    capacity scaling, leaf-only light scaling, cropland grass capacity, organic
+    soil solids) against the reference run with its own switches on: the release
+    parameter file's stomata, respiration and methane sections, and the switches
+    that file leaves off (make_golden.py build_x3_case)."""
+    c = Case(name)
+    prog = {k: v.copy() for k, v in c.prog.items()}
+    acc = oracle.new_acc(c.ncell)
+    checked = 0
+    with np.errstate(all="ignore"):
+        for h in range(c.nhour):
+            prog, D, acc = oracle.step(prog, c.stat, c.forcing_at(h), c.params, acc)
+            if (h + 1) in c.record:
+                bad = compare(prog, c.out(h + 1, "prog"), 1e-12) + compare(D, c.out(h + 1, "diag"), 1e-12)
+                assert not bad, (h + 1, bad[:5])
+                checked += 1
+    assert checked == len(c.record)
+
+
+def test_oracle_matches_reference_release_day_accumulators():
+    """_run_day_inner's sums under the release switches: the NPP split by capacity,
+    the ET components of the modules the seasonal state brings, CH4 and soil means."""
+    c = Case("release")
+    prog = {k: v.copy() for k, v in c.prog.items()}
+    acc = oracle.new_acc(c.ncell)
+    with np.errstate(all="ignore"):
+        for h in range(c.nhour):
+            prog, D, acc = oracle.step(prog, c.stat, c.forcing_at(h), c.params, acc)
+    want = c.day("acc")
+    assert "et_trans" in want and "aynpp" in want
+    assert not compare(acc, want, 1e-6)                       # CH4 cast to float32 per step by the reference
+    assert not compare({k: acc[k] for k in ("aynpp", "aynpptot", "aygpptot", "et_trans")},
+                       {k: want[k] for k in ("aynpp", "aynpptot", "aygpptot", "et_trans")}, 1e-12)
+    assert not compare(prog, c.day("prog"), 1e-12)
+
+
+def test_release_case_exercises_the_switches():
+    """The fixtures reach the switched branches: acclimation factors strictly
+    between 0 and 1 and at both clips, mixed big leaves, capacity shares that
+    differ from the leaf-area shares, crop and organic inputs present."""
+    from oracle.canopy import capacity_factor, big_leaves
+    from oracle.step import gpp_shares
+    c = Case("release")
+    vf = capacity_factor(c.stat, c.params)
+    acc_pfts = vf[:, [3, 5, 8]]
+    assert np.any(acc_pfts == 0.0) and np.any(acc_pfts == 1.0) and np.any((acc_pfts > 0) & (acc_pfts < 1))
+    sh = gpp_shares(c.stat["frac"], c.params)
+    assert np.max(np.abs(sh - c.stat["frac"])) > 1e-3
+    (vub, *_), _, (mub, *_) = big_leaves(c.stat, c.params)
+    assert np.unique(np.round(mub, 9)).size > 3
+    s = Case("switches")
+    assert s.stat["cropfrac"].max() > 0.5 and s.stat["forganic"].max() > 0.3
+    _, je, _ = big_leaves(s.stat, s.params)
+    assert all(j is not None for j in je) and np.any(je[4] != 1.0)

@@ -26,7 +26,7 @@ def test_leaf_order_covers_the_layout():
     assert len(restart.LEAVES) == 258 and len(set(restart.LEAVES)) == 258
     assert restart.LEAVES[:4] == ("soil.tsoi", "soil.wsoi", "soil.wisoi", "soil.tg")
     for f in L.PROG + L.STAT:
-        if not f.leaf.startswith("methane."):
+        if not f.leaf.startswith(L.OPTIONAL_LEAF_PREFIXES):
             assert f.leaf in restart.LEAVES, f.leaf
     assert len(restart.base_leaves(False)) == 257
 
