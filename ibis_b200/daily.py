@@ -136,7 +136,10 @@ class DayLoop:
             if getattr(self, "checkpoint", None) is None:
                 raise ValueError("no checkpoint leaves to write into: pass leaves=")
             leaves, meta0, extra0 = self.checkpoint
-            meta = meta0 if meta is None else meta
+            if meta is None:
+                meta = meta0
+            elif _restart.TREEDEF_KEY in meta0:      # keep the checkpoint's tree structure with the caller's meta
+                meta = {**meta, _restart.TREEDEF_KEY: meta0[_restart.TREEDEF_KEY]}
             extra = extra0 if extra is None else extra
         c = self.cols
         stat = synth.from_planes("STAT", c.stat.cpu().numpy(), c.ncell)

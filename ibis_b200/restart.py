@@ -86,38 +86,96 @@ def base_leaves(bedrock: bool):
     return [p for p in LEAVES if bedrock or p != BEDROCK_LEAF]
 
 
-def load(path: str):
-    """Read a checkpoint.  Returns ``(leaves, meta, extra)``: the base leaves and
-    the named optional modules (:func:`trailing_names`) by path, the ``meta_*``
-    entries, and trailing leaves no count identifies (a list, by position)."""
+def _bedrock_from_shapes(arrays):
+    """Whether a checkpoint without a saved tree structure carries the bedrock
+    leaf: its position holds ``soil.tsoi_deep`` (npoi, nbedrock) with bedrock
+    and ``snow.fi`` (npoi,) without."""
+    i = LEAVES.index(BEDROCK_LEAF)
+    a = arrays[i] if i < len(arrays) else None
+    return a is not None and np.ndim(a) == 2
+
+
+def load_full(path: str):
+    """Read a checkpoint.  Returns ``(leaves, meta, extra, treedef_repr)``: the
+    base leaves and the named optional modules (:func:`trailing_names`) by path,
+    the ``meta_*`` entries, trailing leaves no count identifies (a list, by
+    position), and the saved tree structure (None when the file has none)."""
     z = np.load(path, allow_pickle=False)
     n = int(z["num_leaves"])
     arrays = [None if f"leaf_{i}_is_none" in z.files else z[f"leaf_{i}"] for i in range(n)]
     nsoil_all = sum(1 for p in LEAVES if p.startswith("soil."))
-    if "treedef_repr" in z.files:
-        k = _soil_leaf_count(str(z["treedef_repr"]))
+    tree = str(z["treedef_repr"]) if "treedef_repr" in z.files else None
+    if tree is not None:
+        k = _soil_leaf_count(tree)
         if k is None:
             raise ValueError(f"{path}: no SoilState in the saved tree structure")
         bedrock = k == nsoil_all
     else:
-        bedrock = n in (len(LEAVES),) or n > len(LEAVES)
+        bedrock = _bedrock_from_shapes(arrays)
     names = base_leaves(bedrock)
     if n < len(names):
         raise ValueError(f"{path}: {n} leaves, the base state has {len(names)}")
     leaves = dict(zip(names, arrays[:len(names)]))
     meta = {k[5:]: (z[k].item() if z[k].ndim == 0 else z[k]) for k in z.files if k.startswith("meta_")}
     trail = arrays[len(names):]
-    tnames = trailing_names(len(trail), str(z["treedef_repr"]) if "treedef_repr" in z.files else None)
+    tnames = trailing_names(len(trail), tree)
     if tnames is None:
-        return leaves, meta, trail
+        return leaves, meta, trail, tree
     leaves.update(zip(tnames, trail))
-    return leaves, meta, []
+    return leaves, meta, [], tree
+
+
+def load(path: str):
+    """Read a checkpoint: ``(leaves, meta, extra)`` of :func:`load_full`."""
+    leaves, meta, extra, _ = load_full(path)
+    return leaves, meta, extra
+
+
+# Class names of the state modules in the reference's saved tree structures
+# (state/model_state.py:28-63 and the module classes), by leaf-path prefix.
+_MODULE_CLASS = {"soil": "SoilState", "snow": "SnowState", "canopy": "CanopyState", "atm": "AtmState",
+                 "vegetation": "VegetationState", "carbon": "CarbonState", "hydrology": "HydrologyDiag",
+                 "summary": "SummaryState", "wetland": "MethaneState", "stress": "StressAccum",
+                 "etparts": "ETParts", "seasonal": "SeasonalState", "neeparts": "NEEParts"}
+
+
+def treedef_for(names, n_extra: int = 0) -> str:
+    """A tree structure in the form of the reference's ``repr(treedef)`` for a
+    state with the leaves ``names`` (checkpoint order) and ``n_extra``
+    unnamed trailing leaves: one node per module, named by its class, with one
+    ``*`` per leaf.  It carries what loaders read from it -- the soil module's
+    leaf count (bedrock) and whether ``MethaneState`` is present."""
+    nodes, counts = [], {}
+    for p in names:
+        mod = p.split(".")[0]
+        if mod not in counts:
+            nodes.append(mod)
+            counts[mod] = 0
+        counts[mod] += 1
+    parts = [f"CustomNode({_MODULE_CLASS.get(m, m)}[(Missing,)], [{', '.join(['*'] * counts[m])}])" for m in nodes]
+    if n_extra:
+        parts.append(f"[{', '.join(['*'] * n_extra)}]")
+    return f"PyTreeDef(CustomNode(IBISState[(Missing,)], [{', '.join(parts)}]))"
+
+
+def _treedef_agrees(tree: str, names) -> bool:
+    """Whether a saved tree structure still describes a state with the leaves
+    ``names``: the same soil leaf count and the same optional modules."""
+    k = _soil_leaf_count(tree)
+    if k is None or k != sum(1 for p in names if p.startswith("soil.")):
+        return False
+    mods = {p.split(".")[0] for p in names}
+    return all((_MODULE_CLASS[m] in tree) == (m in mods) for m in ("wetland", "stress", "etparts", "seasonal",
+                                                                   "neeparts"))
 
 
 def save(path: str, leaves: dict, meta: dict | None = None, extra=None, treedef_repr: str | None = None):
     """Write ``leaves`` (base state by path, bedrock leaf optional, then the
     named optional modules present, in the state's order) and ``extra`` in the
-    reference's checkpoint format."""
+    reference's checkpoint format.  The file always carries a tree structure:
+    ``treedef_repr`` (the structure of the file the leaves came from) while it
+    still describes the leaves written, else one made by :func:`treedef_for`,
+    so a loader never has to tell the optional modules apart by leaf count."""
     bedrock = leaves.get(BEDROCK_LEAF) is not None
     names = base_leaves(bedrock)
     missing = [p for p in names if p not in leaves]
@@ -126,8 +184,9 @@ def save(path: str, leaves: dict, meta: dict | None = None, extra=None, treedef_
     names = names + [p for p in TRAILING if p in leaves]
     arrays = [leaves[p] for p in names] + list(extra or [])
     out = {"num_leaves": np.asarray(len(arrays))}
-    if treedef_repr is not None:
-        out["treedef_repr"] = np.asarray(treedef_repr)
+    if treedef_repr is None or not _treedef_agrees(treedef_repr, names):
+        treedef_repr = treedef_for(names, len(extra or []))
+    out["treedef_repr"] = np.asarray(treedef_repr)
     for i, a in enumerate(arrays):
         if a is None:
             out[f"leaf_{i}_is_none"] = np.asarray(True)
@@ -198,7 +257,7 @@ def columns_from_restart(path: str, dtype=None, device="cuda", params=None, diag
     from . import dropin
     from .columns import Columns
 
-    leaves, meta, extra = load(path)
+    leaves, meta, extra, treedef = load_full(path)
     tree = as_tree(leaves)
     ncell = int(np.asarray(tree.soil.tg).shape[0])
     prog = dropin._leaf_dict(tree, "PROG", ncell)
@@ -207,14 +266,25 @@ def columns_from_restart(path: str, dtype=None, device="cuda", params=None, diag
     if dtype is None:
         dtype = torch.float32 if np.asarray(tree.soil.tg).dtype == np.float32 else torch.float64
     cols = Columns.from_host(prog, stat, dtype=dtype, device=device, diag=diag, acc=acc)
+    meta = dict(meta)
+    if treedef is not None:
+        meta[TREEDEF_KEY] = treedef
     return cols, P, leaves, meta, extra
+
+
+# A checkpoint's saved tree structure rides with its metadata dict between
+# columns_from_restart and write_state under this key; it is never written as
+# a meta_ entry.
+TREEDEF_KEY = "__treedef_repr__"
 
 
 def write_state(path: str, leaves: dict, groups, meta=None, extra=None):
     """Save ``leaves`` with the values of ``groups`` -- a sequence of
     (layout group, {field: per-cell array}) pairs, later pairs taking precedence
     where two fields share a leaf -- written into the leaves they mirror, in the
-    leaves' own dtypes.  Leaves no group names are carried over unchanged."""
+    leaves' own dtypes.  Leaves no group names are carried over unchanged; the
+    tree structure of the file they came from (in ``meta`` from
+    :func:`columns_from_restart`) is written back while it still fits."""
     out = dict(leaves)
     for group, values in groups:
         for f in L.GROUPS[group]:
@@ -223,7 +293,9 @@ def write_state(path: str, leaves: dict, groups, meta=None, extra=None):
                 continue
             v = np.asarray(values[f.name]).astype(np.asarray(old).dtype)
             out[f.leaf] = v.reshape(-1)[0] if np.ndim(old) == 0 else v.reshape(np.shape(old))
-    save(path, out, meta, extra)
+    meta = dict(meta or {})
+    treedef = meta.pop(TREEDEF_KEY, None)
+    save(path, out, meta, extra, treedef)
 
 
 def write_columns(path: str, cols, leaves: dict, meta=None, extra=None):

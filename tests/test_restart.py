@@ -185,3 +185,68 @@ def test_checkpoint_columns_step_like_the_reference(cuda_lib, tmp_path):
         ref = prog[f.name][0] if v.ndim == 0 else prog[f.name]
         assert np.array_equal(v, np.asarray(ref).astype(np.float32).astype(np.float64).reshape(v.shape)), f.name
     assert meta2 == meta
+
+
+def _with_modules(leaves, mods, n):
+    out = dict(leaves)
+    rng = np.random.default_rng(3)
+    for m in mods:
+        for p in (restart.WETLAND_LEAVES if m == "wetland" else next(c for c in restart.CHAIN if c[0].startswith(m))):
+            out[p] = rng.random(n)
+    return out
+
+
+def test_written_modules_read_back_by_name(tmp_path):
+    """Every file this module writes carries a tree structure, so the optional
+    modules come back by name where their leaf counts alone are ambiguous: the
+    wetland state plus a 4-leaf StressAccum (7 trailing leaves, also the old
+    3-leaf StressAccum plus ETParts) and wetland + StressAccum + ETParts (11, also
+    StressAccum + ETParts + SeasonalState); with and without bedrock."""
+    leaves, meta, _ = restart.load(FIXTURE)
+    n = leaves["soil.tg"].shape[0]
+    for bed in (True, False):
+        base = leaves if bed else {k: v for k, v in leaves.items() if k != restart.BEDROCK_LEAF}
+        for mods in (("wetland", "stress"), ("wetland", "stress", "etparts"), ("stress",),
+                     ("stress", "etparts", "seasonal")):
+            state = _with_modules(base, mods, n)
+            p = str(tmp_path / "m.npz")
+            restart.write_state(p, state, [], meta)
+            back, _, extra = restart.load(p)
+            assert extra == [] and set(back) == set(state), (bed, mods)
+            for k, v in state.items():
+                assert np.array_equal(np.asarray(back[k]), np.asarray(v)), (bed, mods, k)
+
+
+def test_bedrock_without_tree_structure_from_shapes(tmp_path):
+    """A file without a saved tree structure: bedrock is read from the array at
+    the bedrock leaf's position (soil.tsoi_deep is (npoi, 3), snow.fi (npoi,)),
+    so a no-bedrock state carrying a module is not taken for a bedrock state."""
+    leaves, meta, _ = restart.load(FIXTURE)
+    n = leaves["soil.tg"].shape[0]
+    nobed = _with_modules({k: v for k, v in leaves.items() if k != restart.BEDROCK_LEAF}, ("stress",), n)
+    p = str(tmp_path / "nt.npz")
+    restart.save(p, nobed, meta)
+    z = dict(np.load(p))
+    z.pop("treedef_repr")
+    np.savez(p, **z)
+    back, _, extra = restart.load(p)
+    assert restart.BEDROCK_LEAF not in back and extra == []
+    assert all(np.array_equal(np.asarray(back[k]), np.asarray(v)) for k, v in nobed.items())
+
+
+def test_loaded_tree_structure_is_written_back(tmp_path):
+    """A checkpoint's own tree structure is written back when the module set is
+    unchanged, and replaced by one naming the modules when it is not."""
+    leaves, meta, extra = restart.load(MODULES)
+    p = str(tmp_path / "w.npz")
+    restart.save(p, leaves, meta, extra)
+    leaves, meta, extra, tree = restart.load_full(p)
+    assert tree is not None and "MethaneState" in tree
+    restart.save(p, leaves, meta, extra, tree)
+    assert str(np.load(p)["treedef_repr"]) == tree
+    fewer = {k: v for k, v in leaves.items() if not k.startswith("wetland.")}
+    restart.save(p, fewer, meta, extra, tree)
+    t2 = str(np.load(p)["treedef_repr"])
+    assert "MethaneState" not in t2 and "SoilState" in t2
+    back, _, _ = restart.load(p)
+    assert set(back) == set(fewer)
