@@ -1,1 +1,1 @@
-"""B200-native hourly land-surface step of IBIS 3.0 (see README.md)."""
+"""B200-native hourly land-surface step of IBIS 3.0: CUDA kernels for sm_100a behind a C ABI, and the Python host side."""

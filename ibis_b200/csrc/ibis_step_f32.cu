@@ -1,6 +1,8 @@
 // FP32 production kernels of the hourly step (FP64 islands in the canopy and
 // soil-water solves) and their C-ABI entry points.  The kernel instantiations
 // live in ibis_f32_inst_*.cu so they compile in parallel.
+#include <atomic>
+
 #include "../../include/ibis_b200.h"
 #include "ibis_kernels.cuh"
 
@@ -62,18 +64,20 @@ extern "C" int ibis_config_info(int config, int* form, int* block, int* min_bloc
 // Two-kernel step without any allocation by the caller or the library.
 //
 // Some callers cannot call cudaMalloc at the point where they run the step: an
-// XLA custom-call handler must not allocate behind XLA's allocator, code that
-// runs while a stream is being captured into a CUDA graph cannot allocate, and
-// serving loops that reserve all device memory up front have nothing left to
-// hand out.  For them the hand-off planes of the two-kernel form live in a
-// fixed device array owned by this library, sized for kNoAllocMaxLd cells.
+// XLA custom-call handler must not allocate behind XLA's allocator, and serving
+// loops that reserve all device memory up front have nothing left to hand out.
+// For them the hand-off planes of the two-kernel form live in a fixed device
+// array owned by this library, sized for kNoAllocMaxLd cells.
 // ---------------------------------------------------------------------------
 namespace {
 constexpr int kNoAllocMaxLd = 32768;   // largest leading dimension (cells, padded to 32) accepted
 constexpr int kMaxDevices = 64;
 // kMidCount planes x kNoAllocMaxLd floats = 3.5 MiB, resident on every GPU that loads the library.
 static __device__ __align__(256) float g_noalloc_mid[ibis::kMidCount * kNoAllocMaxLd];
-float* g_noalloc_ptr[kMaxDevices] = {nullptr};
+// The array's device address per device, looked up on the first call there.
+// Host threads may race on a slot; every writer stores the same address, and
+// the atomics make the race well defined.  Not refreshed after cudaDeviceReset.
+std::atomic<float*> g_noalloc_ptr[kMaxDevices];
 }  // namespace
 
 extern "C" int ibis_step_split_noalloc_f32(float* prog, const float* stat, const float* forc, float* diag,
@@ -86,7 +90,8 @@ extern "C" int ibis_step_split_noalloc_f32(float* prog, const float* stat, const
     }
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return -ENODEV;
-    if (!g_noalloc_ptr[dev]) {
+    float* mid = g_noalloc_ptr[dev].load(std::memory_order_relaxed);
+    if (!mid) {
         // once per device, with that device current: the device address of the array
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_mid);
@@ -94,8 +99,9 @@ extern "C" int ibis_step_split_noalloc_f32(float* prog, const float* stat, const
             fprintf(stderr, "ibis_step_split_noalloc_f32: cudaGetSymbolAddress failed: %s\n", cudaGetErrorString(e));
             return -(int)e - 1000;
         }
-        g_noalloc_ptr[dev] = static_cast<float*>(p);
+        mid = static_cast<float*>(p);
+        g_noalloc_ptr[dev].store(mid, std::memory_order_relaxed);
     }
-    return ibis::hourly_step<float>(prog, stat, forc, diag, acc, ncell, ld, nstep, params, status, stream,
-                                    g_noalloc_ptr[dev], ibis::kDefaultSplit);
+    return ibis::hourly_step<float>(prog, stat, forc, diag, acc, ncell, ld, nstep, params, status, stream, mid,
+                                    ibis::kDefaultSplit);
 }

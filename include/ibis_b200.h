@@ -67,15 +67,16 @@ int ibis_num_configs(void);
 int ibis_config_info(int config, int* form, int* block, int* min_blocks, int* block2, int* min_blocks2);
 
 /* ibis_step_split_f32 for callers that cannot allocate device memory (an XLA
- * custom-call handler that must not allocate behind XLA's allocator, code that
- * runs while a stream is being captured into a CUDA graph, a serving loop that
- * reserved all memory up front).  No counterpart in the reference: the
+ * custom-call handler, which must not allocate behind XLA's own allocator; a
+ * serving loop that reserved all device memory up front and has none left to
+ * hand out).  No counterpart in the reference: the
  * hand-off planes live in a fixed array inside this library, sized for at most
  * 32768 cells (ld <= 32768, 3.5 MiB held on every GPU that loads the library
  * until the process exits); larger ld returns -EINVAL with a message on stderr.
  * No cudaMalloc, cudaFree or other allocating call is made.  The first call on
  * each device looks up the array's device address (cudaGetSymbolAddress), so
- * make that first call before any stream capture.  Every call on a device
+ * make that first call before any stream capture; the cached address is not
+ * refreshed after cudaDeviceReset.  Every call on a device
  * shares the one array and it keeps the last call's contents; the surface
  * kernel writes every value the ground kernel reads, so nothing needs
  * clearing, but calls that overlap on the GPU (different streams, or

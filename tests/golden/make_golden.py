@@ -4,7 +4,7 @@ The reference (UW-GCRL/ibis, ``python-port/``) is JAX + Equinox code and
 neither is installed here, so this script puts a small NumPy-backed stand-in
 for ``jax``/``jax.numpy``/``equinox`` (``tests/golden/jaxshim``) first on
 ``sys.path`` and imports the reference package unmodified from
-``/root/reference/python-port``.  It then runs, in float64:
+``$IBIS_REFERENCE/python-port`` (default ``/root/reference``).  It then runs, in float64:
 
 * ``ibis.timestepping.loops.timestep_body`` hour by hour, recording the state
   it returns (prognostic and diagnostic leaves), and
@@ -15,7 +15,7 @@ for ``jax``/``jax.numpy``/``equinox`` (``tests/golden/jaxshim``) first on
 
 on seeded synthetic columns from ``ibis_b200.synth``, and writes the inputs
 and outputs to ``tests/golden/<case>.npz``.  The fixtures travel with the
-repository; this script only runs where ``/root/reference`` exists.
+repository; this script only runs where the reference tree exists.
 
 It also writes ``ibis_b200/restart_leaves.py`` (the leaf order of the
 reference's checkpoint files, from its state classes) and the
@@ -36,7 +36,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REF = "/root/reference/python-port"
+# the reference project's root (holding python-port/); this script reads it there
+REF_ROOT = os.environ.get("IBIS_REFERENCE", "/root/reference")
+REF = os.path.join(REF_ROOT, "python-port")
 
 os.environ.pop("IBIS_FLUX_MAX", None)
 os.environ.pop("IBIS_T_MAX_DEV", None)
@@ -352,7 +354,7 @@ def write_x3_case(name):
     print(f"wrote {path}: {len(out)} arrays, {os.path.getsize(path)} bytes")
 
 
-RESTART = "/root/reference/verify_out_stage1/site_transient_1996.npz"
+RESTART = os.path.join(REF_ROOT, "verify_out_stage1", "site_transient_1996.npz")
 LEAVES_PY = os.path.join(REPO, "ibis_b200", "restart_leaves.py")
 
 

@@ -9,6 +9,13 @@ from ibis_b200 import layout as L
 from ibis_b200.params import PARAM_FIELDS, StepParams
 
 GOLDEN_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+# The reference project's root (the directory holding python-port/), for the
+# tests that import or read the reference itself; they skip when it is unset
+# or absent.
+REF_ROOT = os.environ.get("IBIS_REFERENCE", "")
+REF_PORT = os.path.join(REF_ROOT, "python-port") if REF_ROOT else ""
+HAVE_REF = bool(REF_ROOT) and os.path.isdir(REF_PORT)
 CASES = ("day_mixed", "nobedrock", "sunshade", "perturbed", "restart_1996")
 
 

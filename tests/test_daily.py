@@ -16,7 +16,7 @@ import numpy as np
 import pytest
 
 import oracle
-from goldens import compare, rel_err
+from goldens import HAVE_REF, REF_PORT, compare, rel_err
 from ibis_b200 import layout as L
 from ibis_b200 import restart
 from ibis_b200.params import DAY_PARAM_FIELDS, FLAG_ACC, FLAG_CH4, FLAG_KAHAN, PARAM_FIELDS, DayParams, StepParams
@@ -551,14 +551,14 @@ print("day mapping ok")
 """
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference/python-port"), reason="reference sources not present")
+@pytest.mark.skipif(not HAVE_REF, reason="reference sources not present (IBIS_REFERENCE)")
 def test_day_param_paths_against_reference_objects():
     """dropin.DAY_PARAM_PATHS resolves every path on the reference's own
     SimParams, to the values the three-day fixture was run with and, for the
     module parameters, to the defaults DayParams restates."""
     import subprocess
     import sys
-    code = _DAY_MAP_CHECK.format(golden=os.path.join(HERE, "golden"), ref="/root/reference/python-port",
+    code = _DAY_MAP_CHECK.format(golden=os.path.join(HERE, "golden"), ref=REF_PORT,
                                  repo=os.path.dirname(HERE), gold=GOLD)
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0 and "day mapping ok" in r.stdout, r.stderr[-3000:]

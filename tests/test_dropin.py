@@ -17,7 +17,7 @@ from ibis_b200 import layout as L
 from ibis_b200.params import PARAM_FIELDS, FLAG_BEDROCK, FLAG_H2O_CONSISTENT, FLAG_SUNSHADE_L, FLAG_SUNSHADE_U
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = "/root/reference/python-port"
+from goldens import REF_PORT as REF  # noqa: E402
 
 
 @dataclasses.dataclass(frozen=True)
@@ -74,7 +74,7 @@ print("mapping ok")
 """
 
 
-@pytest.mark.skipif(not os.path.isdir(REF), reason="reference sources not present")
+@pytest.mark.skipif(not REF or not os.path.isdir(REF), reason="reference sources not present (IBIS_REFERENCE)")
 def test_param_mapping_against_reference_objects():
     code = _MAP_CHECK.format(golden=os.path.join(HERE, "golden"), ref=REF, repo=os.path.dirname(HERE))
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600)

@@ -19,7 +19,8 @@ from ibis_b200 import restart
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 FIXTURE = os.path.join(HERE, "golden", "restart_16cells.npz")
-REF_CKPT = "/root/reference/verify_out_stage1/site_transient_1996.npz"
+from goldens import HAVE_REF, REF_PORT, REF_ROOT  # noqa: E402
+REF_CKPT = os.path.join(REF_ROOT, "verify_out_stage1", "site_transient_1996.npz") if REF_ROOT else ""
 
 
 def test_leaf_order_covers_the_layout():
@@ -122,12 +123,12 @@ print("modules ok", n)
 """
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference/python-port"), reason="reference sources not present")
+@pytest.mark.skipif(not HAVE_REF, reason="reference sources not present (IBIS_REFERENCE)")
 def test_saved_modules_load_in_the_reference(tmp_path):
     """A checkpoint with the modules written here loads in the reference's own
     ``load_state`` (wetland state attached by it from the count) with every
     module leaf as written."""
-    code = _MODULES_REF_CHECK.format(golden=os.path.join(HERE, "golden"), ref="/root/reference/python-port",
+    code = _MODULES_REF_CHECK.format(golden=os.path.join(HERE, "golden"), ref=REF_PORT,
                                      repo=os.path.dirname(HERE), src=MODULES, dst=str(tmp_path / "ck.npz"))
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0 and "modules ok 16" in r.stdout, r.stderr[-3000:]
@@ -154,9 +155,9 @@ print("leaves ok", len(leaves))
 """
 
 
-@pytest.mark.skipif(not os.path.exists(REF_CKPT), reason="reference checkpoint not present")
+@pytest.mark.skipif(not REF_CKPT or not os.path.exists(REF_CKPT), reason="reference checkpoint not present (IBIS_REFERENCE)")
 def test_loader_agrees_with_the_reference_loader():
-    code = _REF_CHECK.format(golden=os.path.join(HERE, "golden"), ref="/root/reference/python-port",
+    code = _REF_CHECK.format(golden=os.path.join(HERE, "golden"), ref=REF_PORT,
                              repo=os.path.dirname(HERE), ckpt=REF_CKPT)
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0 and "leaves ok 258" in r.stdout, r.stderr[-3000:]
