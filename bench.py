@@ -204,6 +204,158 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+
+# ---------------------------------------------------------------------------- sub-workloads of the default line
+def _release_params():
+    """The step's parameter record under the reference's release parameter file
+    (python-port/configs/params/params_31s_ch4h.yaml: sunlit/shaded canopies,
+    vmax and slope mixing, the NPP split by capacity, temperature acclimation
+    with per-PFT constants, consistent soil-water weights, its respiration and
+    methane values), as the release fixture holds it (tests/golden/release.npz,
+    made by the reference's own loaders)."""
+    from ibis_b200.params import PARAM_FIELDS, StepParams
+    z = np.load(os.path.join(REPO, "tests", "golden", "release.npz"))
+    P = StepParams()
+    for name, _, _ in PARAM_FIELDS:
+        if "in.param." + name in z.files:
+            setattr(P, name, z["in.param." + name])
+    P.flags = int(z["in.param.flags"])
+    return P
+
+
+def release_day(wl, dev, stream, flush, steps):
+    """The day workload (95,333 columns x 24 h, accumulators + hourly CH4) under
+    the release parameter file's switches: the IBIS 3.0 kernels, long fused
+    configuration."""
+    import torch
+    from ibis_b200.columns import Columns
+    P = _release_params()
+    rng = np.random.Generator(np.random.PCG64(41))
+    stat = dict(wl.stat, acclim_x=rng.uniform(-12.0, 28.0, wl.ncell))
+    cols = Columns.from_host(wl.prog, stat, dtype=torch.float32, device=dev, acc=True)
+    cols.set_mode(6)
+    forc = cols.forcing(wl.forc)
+    prog0, acc0 = cols.prog.clone(), cols.acc.clone()
+    for _ in range(3):
+        cols.run(forc, P, stream=stream)
+    out = []
+    for _ in range(steps):
+        cols.prog.copy_(prog0)
+        cols.acc.copy_(acc0)
+        flush.fill_(1.0)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        cols.run(forc, P, stream=stream)
+        b.record(stream)
+        out.append((a, b))
+    torch.cuda.synchronize(dev)
+    ms = float(np.mean([a.elapsed_time(b) for a, b in out]))
+    from ibis_b200.params import X3_FLAGS
+    names = {1 << 2: "sunshade_u", 1 << 3: "sunshade_l", 1 << 1: "h2o_consistent_weights", 1 << 12: "vmax_mix",
+             1 << 13: "coefm_mix", 1 << 14: "gpp_split_by_capacity", 1 << 15: "acclim_on (per-PFT constants)",
+             1 << 10: "ET parts"}
+    return {"value": wl.ncell * HOURS / (ms / 1e3), "unit": "cell-steps/s", "ms_per_step": ms,
+            "switches": [v for k, v in names.items() if P.flags & k], "x3_kernels": bool(P.flags & X3_FLAGS),
+            "nonfinite_columns": cols.nonfinite()[0],
+            "note": "the same day under the reference's release parameter file "
+                    "(configs/params/params_31s_ch4h.yaml, as captured by tests/golden/release.npz); per-cell "
+                    "acclimation states seeded U(-12, 28) C"}
+
+
+def ensemble_bounded(stream, hours=48):
+    """The 356-site x 64-vector calibration ensemble (22,784 runs) over the first
+    ``hours`` hours of every record: the persistent launch, the batched hourly
+    form (one launch per hour for all runs, replayed from a CUDA graph) and the
+    per-vector plain form (one single-parameter launch per hour per vector); and
+    the full records' makespan estimated from the persistent hour."""
+    import torch
+    from ibis_b200 import ensemble as E
+    spec = E.make_ensemble(356, 64, years=(1, 15), seed=7, site_hours=np.full(356, hours))
+    ens = E.Ensemble(spec)
+
+    def timed(fn, k):
+        out = []
+        for _ in range(k):
+            ens.reset()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+            out.append(a.elapsed_time(b))
+        return out
+
+    timed(ens.run, 2)
+    ms_p = float(np.median(timed(ens.run, 3)))
+    timed(lambda: ens.run_hourly(chunk=24, graph=True), 1)
+    ms_g = float(np.median(timed(lambda: ens.run_hourly(chunk=24, graph=True), 3)))
+    plain = _plain_per_vector(spec, None, stream, hours=hours)
+    cs = ens.cell_steps()
+    longest = 15 * 8760
+    return {"hours": hours, "runs": ens.nrun, "cell_steps": cs,
+            "persistent": {"value": cs / (ms_p / 1e3), "ms": ms_p, "launches": 1},
+            "hourly_graph": {"value": cs / (ms_g / 1e3), "ms": ms_g, "launches": hours},
+            "plain_per_vector": {"value": plain["value"], "ms": plain["ms"], "launches": plain["launches"]},
+            "persistent_vs_hourly_graph": ms_g / ms_p, "persistent_vs_plain_per_vector": plain["ms"] / ms_p,
+            "full_record_makespan_estimate_s": ms_p / hours * longest / 1e3,
+            "note": f"first {hours} h of every run; the full records (1-15 years) take about the persistent "
+                    "hour's time x the longest record (131,400 h): one thread's per-hour latency bounds the "
+                    "makespan"}
+
+
+def serve_bounded(rate=50.0, duration=2.0):
+    """The request loop over a library of day records (356 sites, 10 years):
+    Poisson arrivals at ``rate``/s for ``duration`` s, 1-64 sites, 1-10 years,
+    continuously batched; p50/p99 request latency and throughput."""
+    from ibis_b200 import serve as S
+    lib = S.SiteLibrary(356, 10, seed=3, daily=True)
+    srv = S.Server(lib, budget_bytes=150e9, epoch_hours=168)
+    srv.serve(S.poisson_requests(np.random.default_rng(1), rate, 0.2, 356, max_years=1))
+    st = srv.serve(S.poisson_requests(np.random.default_rng(5), rate, duration, 356))
+    return {"requests": st["requests"], "p50_s": st["p50_s"], "p99_s": st["p99_s"],
+            "cell_steps_per_s": st["cell_steps_per_s"], "epochs": st["epochs"], "slots": st["slots"],
+            "queue_depth_max": st["queue_depth_max"], "hbm_gb": st["hbm_gb"], "status": st["status"],
+            "note": f"Poisson {rate}/s for {duration} s, day-record library (hours generated in the kernel); "
+                    "latency from arrival to the result in host memory, GPU clock"}
+
+
+def single_cell(dev, stream, cpu_hours=480):
+    """configs[0]'s shape: one column x 8,760 hourly steps, the whole year in one
+    fused launch on the GPU (FP32 and FP64), beside the float64 oracle on one
+    host core over a bounded sample of the same year."""
+    import torch
+    import oracle
+    from ibis_b200 import synth
+    from ibis_b200.columns import Columns
+    wl = synth.make_workload(1, 8760, seed=17)
+    out = {}
+    for name, dt in (("f32", torch.float32), ("f64", torch.float64)):
+        cols = Columns.from_host(wl.prog, wl.stat, dtype=dt, device=dev, acc=True)
+        forc = cols.forcing(wl.forc)
+        P = wl.params.copy()
+        if dt == torch.float64:
+            P.flags &= ~(1 << 8)
+        cols.run(forc[:24], P, stream=stream)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        cols.run(forc, P, stream=stream)
+        b.record(stream)
+        b.synchronize()
+        ms = a.elapsed_time(b)
+        out["gpu_" + name] = {"ms_per_year": ms, "value": 8760 / (ms / 1e3), "unit": "cell-steps/s"}
+    prog, acc = wl.prog, oracle.new_acc(1)
+    t0 = time.perf_counter()
+    with np.errstate(all="ignore"):
+        for h in range(cpu_hours):
+            prog, _, acc = oracle.step(prog, wl.stat, wl.forcing_at(h), wl.params, acc)
+    dt = time.perf_counter() - t0
+    out["cpu_f64_oracle"] = {"value": cpu_hours / dt, "unit": "cell-steps/s", "cores": 1,
+                             "year_estimate_s": dt / cpu_hours * 8760,
+                             "sample": f"first {cpu_hours} hours of the year, float64 NumPy oracle"}
+    out["note"] = ("1 column x 8,760 h: the GPU runs one thread through the year (latency bound); the reference's "
+                   "JAX CPU path is not installable here, so the CPU leg is the float64 NumPy port on one core")
+    return out
+
 # ---------------------------------------------------------------------------- our arm
 def run_ours(args):
     import torch
@@ -316,6 +468,13 @@ def run_ours(args):
                                                                    stream=stream), 5)))
 
     nonfinite = cols.nonfinite()
+    # the sub-workloads of the default line (one GPU only: the scaling runs time the day alone)
+    extras = {}
+    if world == 1 and not args.no_extras:
+        extras["release_params"] = release_day(wl, dev, stream, flush, args.steps)
+        extras["ensemble"] = ensemble_bounded(stream)
+        extras["serve"] = serve_bounded()
+        extras["single_cell"] = single_cell(dev, stream)
     if world > 1:
         ms_step, ms_plain, ms_e2e, ms_e2e_daily = replicas.max_over_ranks(W, [ms_step, ms_plain, ms_e2e,
                                                                               ms_e2e_daily], device=dev)
@@ -325,13 +484,27 @@ def run_ours(args):
     bpl = _algorithmic_bytes(HOURS) * args.ncell
     achieved = bpl / (ms_step / 1e3) / 1e9
     traffic = None
+    issue = None
     tpath = os.path.join(REPO, "profiles", "hourly_step_traffic.json")
+    clocks = clk.summary()
     if os.path.exists(tpath):
         with open(tpath) as f:
             tj = json.load(f)
         per_cell = tj.get("fused_day_bytes_per_cell")
         if per_cell:
             traffic = float(per_cell) * args.ncell
+        ipc = tj.get("fused_day_warp_instructions_per_cell_hour")
+        if ipc and clocks.get("sm_mhz"):
+            # the bound that applies: warp-instruction issue, 4 schedulers per SM each
+            # issuing one warp instruction per cycle at the sampled SM clock
+            n_sm = torch.cuda.get_device_properties(dev).multi_processor_count
+            winst = float(ipc) * args.ncell * HOURS
+            ach = winst / (ms_step / 1e3) / 1e9
+            pk = n_sm * 4 * clocks["sm_mhz"] * 1e6 / 1e9
+            issue = {"bound": "issue", "achieved": ach, "peak": pk, "unit": "G warp-instructions/s",
+                     "frac": ach / pk, "warp_instructions_per_launch": winst,
+                     "source": "instructions per cell-hour from profiles/hourly_step_kernel_f32_day_32768cells.md; "
+                               f"peak = {n_sm} SMs x 4 schedulers x median sampled SM clock"}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps,
@@ -347,6 +520,7 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": peak_kind, "algorithmic_bytes_per_launch": bpl},
+            "issue_roofline": issue,
             "per_step_launch": {"value": cell_steps / (ms_plain / 1e3), "ms_per_step": ms_plain,
                                 "launches_per_step": HOURS, "launch_config": "fused, block 128, 2 blocks/SM",
                                 "achieved_gbs": _algorithmic_bytes(1) * args.ncell * HOURS / (ms_plain / 1e3) / 1e9},
@@ -361,9 +535,10 @@ def run_ours(args):
                                   "note": "daily weather in, hourly forcing generated on the GPU by the reference's "
                                           "diurnal algorithm (not the hourly generator of the workload above)"},
             "gpu_launches": args.steps * (1 if cfg_desc["form"] == "fused" else 2 * HOURS),
-            "clocks": clk.summary(),
+            "clocks": clocks,
             "nonfinite_columns": nonfinite[0],
         }
+        line.update(extras)
         if cpu is not None:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
@@ -752,6 +927,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--ncell", type=int, default=NCELL)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="day only: skip the release-parameter, ensemble, serve and single-column sub-workloads")
     ap.add_argument("--config", type=int, default=None, help="launch configuration (default: autotuned)")
     args = ap.parse_args()
     if args.warmup < 3:

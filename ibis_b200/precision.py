@@ -1,18 +1,33 @@
-"""Precision report: the FP32 kernels against the FP64 kernels over a year.
+"""Precision report: the FP32 kernels against float64 over a year.
 
 The production kernels run the step in FP32 with two FP64 islands (the 9x9
 canopy energy/vapour system of ``turvap`` and the soil-water tridiagonal solve)
 and Kahan-compensated accumulators; the FP64 kernels run every operation in
 double and match the float64 CPU restatement of the reference to ~1e-13 per
-step.  :func:`report` runs both on the same seeded cells for a year of hourly
-forcing and states, per annual flux, the maximum and mean relative error of
-the FP32 result over the cells and the relative error of the all-cell total,
-and whether the integer-valued counters of the state agree exactly.
+step.  :func:`report` runs, on the first ``ncell`` columns of the 95,333-cell
+population (the columns of the day workload's generator, latitude
+U(-60, 80), Dirichlet(0.5) plant types) for a year of seeded hourly forcing:
+
+* ``f32``   -- the production FP32 kernels;
+* ``f64``   -- the FP64 kernels (the float64 GPU oracle);
+* ``f64_f32state`` -- the FP64 kernels with the prognostic state rounded to
+  float32 after every hour, as the reference's own FP32 production run stores
+  its state (``_cast_tree_f32`` after each step, loops_gswp3.py:304): the
+  drift any float32-state implementation has, whatever its arithmetic;
+* optionally the float64 CPU oracle (the restatement of the reference pinned
+  to its outputs) on the first ``oracle_cells`` columns;
+
+and states, per annual flux, the maximum and mean relative error over the
+cells and the relative error of the all-cell total, against ``f64``, and
+whether the integer-valued counters agree exactly.  :func:`full_size_year`
+runs the FP32 kernels on all 95,333 columns for a year with the hourly forcing
+generated on the device from daily weather.
 
 The reference documents its own float32 run against its float64 run the same
 way (docs/technote/17_numerics_verification.md:367-383).
 
-Run ``python -m ibis_b200.precision [ncell] [nhour]`` for a JSON report.
+Run ``python -m ibis_b200.precision [ncell] [nhour] [oracle_cells]`` for a JSON
+report, ``python -m ibis_b200.precision --full`` for the full-size year.
 """
 from __future__ import annotations
 
@@ -35,6 +50,7 @@ FLUXES = {
     "runoff": "aytrunof", "drainage": "aytdrain", "ch4": "ch4",
 }
 COUNTERS = ("nytimes", "nfirestep", "nfirestep_vpd")
+POPULATION = 95333
 
 
 def _rel(a32, a64, floor):
@@ -55,65 +71,194 @@ def _stats(a32, a64, floor_frac=1e-3):
             "floor": floor, "fp64_total": tot64}
 
 
-def report(ncell: int = 1000, nhour: int = 8760, seed: int = 2024, chunk: int = 720, device="cuda",
-           lat_range=(-60.0, 80.0), alpha: float = 0.5) -> dict:
-    """Run ``ncell`` cells for ``nhour`` hours in FP32 and FP64; return the report."""
+def population(ncell: int, seed: int = 2024, lat_range=(-60.0, 80.0), alpha: float = 0.5):
+    """The first ``ncell`` columns of the 95,333-cell population: static planes,
+    latitudes and a generator for their forcing (the columns are drawn for the
+    whole population, so the first 1,000 are the same whatever ``ncell``)."""
     rng = np.random.Generator(np.random.PCG64(seed))
-    lat = rng.uniform(lat_range[0], lat_range[1], size=ncell)
-    stat = synth.make_columns(rng, ncell, alpha)
+    lat = rng.uniform(lat_range[0], lat_range[1], size=POPULATION)[:ncell]
+    stat = {k: v[:ncell] for k, v in synth.make_columns(rng, POPULATION, alpha).items()}
+    return stat, lat, np.random.Generator(np.random.PCG64(seed + 1))
+
+
+def _annual(cols, nhour):
+    acc, prog = cols.acc_host(), cols.prog_host()
+    out = {name: np.asarray(acc[a], np.float64) for name, a in FLUXES.items()}
+    days = nhour / 24.0
+    out["tsoi_mean"] = np.asarray(acc["tsoi_mean"], np.float64) / days
+    out["prog"] = prog
+    return out
+
+
+def _compare(x, ref):
+    res = {"fluxes": {}, "soil_t": {}, "counters": {}}
+    for name in FLUXES:
+        res["fluxes"][name] = _stats(x[name], ref[name])
+    for k in range(L.NSOILAY):
+        res["soil_t"][f"layer{k}"] = _stats(x["tsoi_mean"][:, k], ref["tsoi_mean"][:, k])
+    for name in COUNTERS:
+        d = np.abs(np.asarray(x["prog"][name]) - np.asarray(ref["prog"][name]))
+        res["counters"][name] = {"equal_frac": float(np.mean(d == 0.0)), "max_abs_diff": float(np.max(d)),
+                                 "integer_valued": bool(np.all(x["prog"][name] == np.round(x["prog"][name])))}
+    return res
+
+
+def _oracle_chunk(task):
+    import oracle
+    prog, stat, forcs, P = task
+    n = prog["tg"].shape[0]
+    acc = oracle.new_acc(n)
+    with np.errstate(all="ignore"):
+        for F in forcs:
+            for h in range(F["ta"].shape[0]):
+                prog, _, acc = oracle.step(prog, stat, {k: v[h] for k, v in F.items()}, P, acc)
+    return prog, acc
+
+
+def report(ncell: int = 1000, nhour: int = 8760, seed: int = 2024, chunk: int = 720, device="cuda",
+           oracle_cells: int = 0, legs=("f32", "f64", "f64_f32state")) -> dict:
+    """Run the legs on the first ``ncell`` columns for ``nhour`` hours; return the
+    report (every leg against ``f64``; with ``oracle_cells`` also ``f64`` and
+    ``f32`` against the float64 oracle on the first ``oracle_cells`` columns)."""
+    stat, lat, rng = population(ncell, seed)
     f0 = synth.make_forcing(rng, lat, min(chunk, nhour), start_doy=1)
     prog = synth.make_initial(rng, stat, {k: v[0] for k, v in f0.items()})
     P = StepParams(co2conc=390.0e-6)
     P.flags = P.flags | FLAG_SOIL_MEANS
     P64 = P.copy()
     P64.flags = P64.flags & ~FLAG_KAHAN
-    c32 = Columns.from_host(prog, stat, dtype=torch.float32, acc=True, device=device)
-    c64 = Columns.from_host(prog, stat, dtype=torch.float64, acc=True, device=device)
+    cols = {}
+    if "f32" in legs:
+        cols["f32"] = Columns.from_host(prog, stat, dtype=torch.float32, acc=True, device=device)
+    for leg in ("f64", "f64_f32state"):
+        if leg in legs or leg == "f64":
+            cols[leg] = Columns.from_host(prog, stat, dtype=torch.float64, acc=True, device=device)
+    oracle_forc = []
     t0 = time.time()
     h = 0
     fc = f0
-    gpu_ms = {"f32": 0.0, "f64": 0.0}
+    gpu_ms = {k: 0.0 for k in cols}
     while h < nhour:
         n = min(chunk, nhour - h)
         if h > 0:
             fc = synth.make_forcing(rng, lat, n, start_doy=1, start_hour=h)
-        for cols, par, key in ((c32, P, "f32"), (c64, P64, "f64")):
-            planes = synth.forcing_planes(fc, cols.ld, 0, n,
-                                          dtype=np.float32 if cols.dtype == torch.float32 else np.float64)
-            f = torch.from_numpy(planes).to(cols.device)
+        if oracle_cells:
+            oracle_forc.append({k: v[:n, :oracle_cells].copy() for k, v in fc.items()})
+        for leg, c in cols.items():
+            planes = synth.forcing_planes(fc, c.ld, 0, n,
+                                          dtype=np.float32 if c.dtype == torch.float32 else np.float64)
+            f = torch.from_numpy(planes).to(c.device)
+            par = P if leg == "f32" else P64
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record()
-            for d in range(0, n, 24):          # one launch per day, as the day loop runs
-                cols.run(f[d:d + 24], par)
+            if leg == "f64_f32state":
+                for d in range(n):             # one hour per launch, the state stored as float32 between hours
+                    c.run(f[d:d + 1], par)
+                    c.prog.copy_(c.prog.float())
+            else:
+                for d in range(0, n, 24):      # one launch per day, as the day loop runs
+                    c.run(f[d:d + 24], par)
             b.record()
             b.synchronize()
-            gpu_ms[key] += a.elapsed_time(b)
+            gpu_ms[leg] += a.elapsed_time(b)
         h += n
     torch.cuda.synchronize()
-    a32, a64 = c32.acc_host(), c64.acc_host()
-    p32, p64 = c32.prog_host(), c64.prog_host()
-    out = {"ncell": ncell, "nhour": nhour, "seed": seed, "wall_s": time.time() - t0, "gpu_ms": gpu_ms,
-           "nonfinite": {"f32": c32.nonfinite()[0], "f64": c64.nonfinite()[0]}, "fluxes": {}, "soil_t": {},
-           "state": {}, "counters": {}}
-    for name, acc in FLUXES.items():
-        out["fluxes"][name] = _stats(a32[acc], a64[acc])
-    days = nhour / 24.0
-    for k in range(L.NSOILAY):
-        out["soil_t"][f"layer{k}"] = _stats(a32["tsoi_mean"][:, k] / days, a64["tsoi_mean"][:, k] / days)
-    for name in ("tsoi", "wsoi", "tg", "tu", "tl", "fi", "hsno"):
-        out["state"][name] = _stats(p32[name], p64[name])
-    for name in COUNTERS:
-        d = np.abs(p32[name] - p64[name])
-        out["counters"][name] = {"equal_frac": float(np.mean(d == 0.0)), "max_abs_diff": float(np.max(d)),
-                                 "integer_valued": bool(np.all(p32[name] == np.round(p32[name])))}
+    res = {k: _annual(c, nhour) for k, c in cols.items()}
+    out = {"ncell": ncell, "nhour": nhour, "seed": seed, "population": f"first {ncell} of {POPULATION} columns",
+           "wall_s": time.time() - t0, "gpu_ms": gpu_ms,
+           "nonfinite": {k: c.nonfinite()[0] for k, c in cols.items()}, "legs": {}}
+    for leg in cols:
+        if leg != "f64":
+            out["legs"][leg] = _compare(res[leg], res["f64"])
+    # the final state of the FP32 leg against the FP64 leg
+    if "f32" in res:
+        out["state"] = {name: _stats(res["f32"]["prog"][name], res["f64"]["prog"][name])
+                        for name in ("tsoi", "wsoi", "tg", "tu", "tl", "fi", "hsno")}
+        out["fluxes"] = out["legs"]["f32"]["fluxes"]
+        out["soil_t"] = out["legs"]["f32"]["soil_t"]
+        out["counters"] = out["legs"]["f32"]["counters"]
+    if oracle_cells:
+        import multiprocessing as mp
+        import os
+        nproc = max(1, min(oracle_cells, (os.cpu_count() or 1)))
+        idx = np.array_split(np.arange(oracle_cells), nproc)
+        sl = lambda d, ix: {k: np.asarray(v)[ix] for k, v in d.items()}
+        tasks = [(sl(prog, ix), sl(stat, ix), [{k: v[:, ix] for k, v in F.items()} for F in oracle_forc], P64)
+                 for ix in idx if ix.size]
+        t1 = time.time()
+        with mp.get_context("spawn").Pool(len(tasks)) as pool:
+            parts = pool.map(_oracle_chunk, tasks)
+        oprog = {k: np.concatenate([p[0][k] for p in parts]) for k in parts[0][0]}
+        oacc = {k: np.concatenate([p[1][k] for p in parts]) for k in parts[0][1]}
+        ores = {name: np.asarray(oacc[a], np.float64) for name, a in FLUXES.items()}
+        ores["tsoi_mean"] = oacc["tsoi_mean"] / (nhour / 24.0)
+        ores["prog"] = oprog
+        sub = lambda r: {**{k: v[:oracle_cells] for k, v in r.items() if k != "prog"},
+                         "prog": {k: np.asarray(v)[:oracle_cells] for k, v in r["prog"].items()}}
+        out["oracle"] = {"cells": oracle_cells, "processes": len(tasks), "wall_s": time.time() - t1,
+                         "f64_vs_oracle": _compare(sub(res["f64"]), ores)}
+        if "f32" in res:
+            out["oracle"]["f32_vs_oracle"] = _compare(sub(res["f32"]), ores)
     return out
+
+
+def full_size_year(ncell: int = POPULATION, ndays: int = 365, seed: int = 2024, check_cells: int = 1000,
+                   device="cuda") -> dict:
+    """All ``ncell`` columns of the population in FP32 for ``ndays`` days, the
+    hourly forcing generated on the device from seeded daily weather (the
+    reference's diurnal algorithm, ``ibis_diurnal_f32``): time, finiteness,
+    physical bounds, and whether the first ``check_cells`` columns equal a run of
+    those columns alone (columns are independent, so they must, bit for bit)."""
+    from . import forcing as _forcing
+    stat, lat, rng = population(ncell, seed)
+    daily = synth.make_daily_weather(rng, lat, ndays)
+    f0 = synth.make_forcing(np.random.Generator(np.random.PCG64(seed + 3)), lat, 1, start_doy=1)
+    prog = synth.make_initial(rng, stat, {k: v[0] for k, v in f0.items()})
+    P = StepParams(co2conc=390.0e-6)
+    P.flags = P.flags | FLAG_SOIL_MEANS
+    big = Columns.from_host(prog, stat, dtype=torch.float32, acc=True, device=device)
+    small = Columns.from_host({k: v[:check_cells] for k, v in prog.items()},
+                              {k: v[:check_cells] for k, v in stat.items()}, dtype=torch.float32, acc=True,
+                              device=device)
+    big.set_mode(6)
+    small.set_mode(6)
+    d_daily = torch.from_numpy(_forcing.daily_planes(daily, big.ld)).to(big.device)
+    lat_d = torch.zeros(big.ld, dtype=torch.float32, device=big.device)
+    lat_d[:ncell] = torch.from_numpy(lat.astype(np.float32)).to(big.device)
+    step_ms = 0.0
+    t0 = time.time()
+    for d in range(ndays):
+        f = _forcing.hourly_forcing(d_daily[d:d + 1], lat_d, ncell, jday0=1 + d, day0=d, seed=seed)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        big.run(f, P)
+        b.record()
+        small.run(f[:, :, :small.ld].contiguous(), P)
+        b.synchronize()
+        step_ms += a.elapsed_time(b)
+    torch.cuda.synchronize()
+    pb, ps = big.prog_host(), small.prog_host()
+    ab, as_ = big.acc_host(), small.acc_host()
+    same = all(np.array_equal(np.asarray(pb[k])[:check_cells], np.asarray(ps[k])) for k in pb) and \
+        all(np.array_equal(np.asarray(ab[k])[:check_cells], np.asarray(as_[k])) for k in ab)
+    bounds = {"tsoi_K": [float(pb["tsoi"].min()), float(pb["tsoi"].max())],
+              "wsoi": [float(pb["wsoi"].min()), float(pb["wsoi"].max())],
+              "tu_K": [float(pb["tu"].min()), float(pb["tu"].max())]}
+    return {"ncell": ncell, "days": ndays, "step_ms": step_ms, "wall_s": time.time() - t0,
+            "cell_steps_per_s": ncell * 24 * ndays / (step_ms / 1e3), "nonfinite": big.nonfinite()[0],
+            "first_cells_equal_alone": bool(same), "check_cells": check_cells, "bounds": bounds,
+            "annual_gpp_total": float(np.sum(ab["aygpptot"])), "annual_runoff_total": float(np.sum(ab["aytrunof"]))}
 
 
 def main(argv=None):
     argv = sys.argv[1:] if argv is None else argv
+    if argv and argv[0] == "--full":
+        print(json.dumps(full_size_year(), indent=1))
+        return
     ncell = int(argv[0]) if argv else 1000
     nhour = int(argv[1]) if len(argv) > 1 else 8760
-    print(json.dumps(report(ncell, nhour), indent=1))
+    ocells = int(argv[2]) if len(argv) > 2 else 0
+    print(json.dumps(report(ncell, nhour, oracle_cells=ocells), indent=1))
 
 
 if __name__ == "__main__":

@@ -106,6 +106,8 @@ def _mock(case, h=0):
         if f.leaf.startswith(L.OPTIONAL_LEAF_PREFIXES) or (f.name == "tsoi_deep" and not bed):
             continue
         src = case.prog if f in L.PROG else case.stat
+        if f.name not in src:          # inputs of switched-off extensions the fixture does not carry
+            continue
         leaves["state." + f.leaf] = np.asarray(src[f.name], dtype=np.float64).copy()
     leaves["state.vegetation.nytimes"] = np.float64(case.prog["nytimes"][0])
     for f in L.FORC:
