@@ -458,6 +458,7 @@ template <typename R>
 struct Aero {
     R rhoa, cp, za, z1, z2, z3, z4, z12, z34, bdl, bdu, dil, diu, exphl, expl, exphu, expu;
     R alogav, alog1, alog2, alog3, alog4, aloga;
+    R hl, hu;   // the exponents of expl and expu (the FP32 wind profile works from them)
 };
 
 // canini (canopy_exchange.py:192-280); u2/alogu/alogl are returned separately (they are carried)
@@ -487,6 +488,7 @@ __device__ __forceinline__ void aero_geometry(Aero<R>& A, R& u2, R& alogu, R& al
     R z3 = x1 * ztop0 + rw;
     R z4 = x1 * zbot0 + rw;
     A.z3 = z3; A.z4 = z4; A.z34 = R(0.5) * (z3 + z4);
+    A.hl = bveg * (z3 - z4);
     A.exphl = ex(R(0.5) * bveg * (z3 - z4));
     A.expl = A.exphl * A.exphl;
     R displ = x1 * R(0.7) * z3;
@@ -504,6 +506,7 @@ __device__ __forceinline__ void aero_geometry(Aero<R>& A, R& u2, R& alogu, R& al
     R z1 = x1 * ztop1 + rw;
     R z2 = x1 * zbot1 + rw;
     A.z1 = z1; A.z2 = z2; A.z12 = R(0.5) * (z1 + z2);
+    A.hu = bveg * (z1 - z2);
     A.exphu = ex(R(0.5) * bveg * (z1 - z2));
     A.expu = A.exphu * A.exphu;
     R dispu = x1 * R(0.7) * z1 + (R(1.0) - x1) * displ;
@@ -549,6 +552,40 @@ __device__ __forceinline__ void stability(R& sm, R& sh, R tb, R tt, R ttfac, R q
 template <typename R>
 struct Trans { R cu, cl, su, ss, sl, sg, si; };
 
+// The exponential wind profile inside one canopy story (canopy_exchange.py:
+// 365-392) in closed form, for the FP32 kernels.  With E = exp(h) the
+// reference forms y = ((x+1)E + (x-1)/E) / ((x+1)E - (x-1)/E) and then the
+// profile coefficients from y + 1 and y - 1.  In float32, y rounds to 1 once E
+// passes ~3e3 (a dense canopy), so (y - 1) keeps no correct digit and the wind
+// at the story's bottom, proportional to (y - 1) E, comes out wrong by O(1).
+// With D = 2x sinh h + 2 cosh h (= the reference's denominator) the same
+// quantities are
+//   y = (x cosh h + sinh h) / (x sinh h + cosh h),
+//   a = k (x+1) E,  b = k (x-1)/E,  k = tau / (D bd),
+//   a + b = 2k (x cosh h + sinh h),  a/E^.5 + b E^.5 = 2k (x cosh h/2 + sinh h/2),
+//   a/E + b E = 2k x,  bd (a/E - b E) = 2 tau / D,
+// with sinh and cosh from expm1, which stay accurate for every h.
+template <typename R>
+struct Profile {
+    R y;       // the reference's y
+    R d;       // D / 2
+    R top2;    // (a + b) / k
+    R mid2;    // (a / E^.5 + b E^.5) / k
+};
+
+template <typename R>
+__device__ __forceinline__ Profile<R> profile(R x, R h) {
+    const R ep = em1(h), em = em1(-h), ep2 = em1(R(0.5) * h), em2 = em1(R(-0.5) * h);
+    const R sh = R(0.5) * (ep - em), ch = R(1.0) + R(0.5) * (ep + em);
+    const R sh2 = R(0.5) * (ep2 - em2), ch2 = R(1.0) + R(0.5) * (ep2 + em2);
+    Profile<R> p;
+    p.d = x * sh + ch;
+    p.y = (x * ch + sh) / p.d;
+    p.top2 = R(2.0) * (x * ch + sh);
+    p.mid2 = R(2.0) * (x * ch2 + sh2);
+    return p;
+}
+
 // turcof (canopy_exchange.py:333-426); strat = (sml, shl, smu, shu) carried across passes
 template <typename R>
 __device__ __forceinline__ void transfer(Trans<R>& T, R (&strat)[4], R& u2, R& alogu, R& alogl, const Aero<R>& A,
@@ -558,28 +595,52 @@ __device__ __forceinline__ void transfer(Trans<R>& T, R (&strat)[4], R& u2, R& a
     stability(strat[0], strat[1], t34, t12, R(1.0), q34, q12, A.z3, A.z2, alogl, A.alog2, u2, first, P);
     stability(strat[2], strat[3], t12, F.ta, P.tfac, q12, F.qa, A.z1, A.za, alogu, A.aloga, F.ua, first, P);
     R v = (A.alog4 - A.alogav) / vonk;
-    R x = (v * v) * A.bdl;
-    R rw = R(1.0) / A.expl;
-    R yl = ((x + R(1)) * A.expl + (x - R(1)) * rw) / ((x + R(1)) * A.expl - (x - R(1)) * rw);
-    R nalogl = A.alog3 - vonk * sq(yl / A.bdl);
-    v = (A.alog2 - nalogl) / vonk;
-    x = (v * v) * A.bdu / strat[0];
-    rw = R(1.0) / A.expu;
-    R yu = ((x + R(1)) * A.expu + (x - R(1)) * rw) / ((x + R(1)) * A.expu - (x - R(1)) * rw);
-    R nalogu = A.alog1 - vonk * sq(yu / A.bdu);
-    v = F.ua * vonk / (A.aloga - nalogu);
-    R tauu = (v * v) * strat[2];
-    R a = R(0.5) * tauu * (yu + R(1)) / A.bdu;
-    R b = R(0.5) * tauu * (yu - R(1)) / A.bdu;
-    R taul = A.bdu * (a / A.expu - b * A.expu);
-    R cc = R(0.5) * taul * (yl + R(1)) / A.bdl;
-    R d = R(0.5) * taul * (yl - R(1)) / A.bdl;
-    R u1 = mx(R(0.01), sq(mx(R(0.0), a + b)));
-    R u12 = mx(R(0.01), sq(mx(R(0.0), a / A.exphu + b * A.exphu)));
-    R nu2 = mx(R(0.01), sq(mx(R(0.0), a / A.expu + b * A.expu)));
-    R u3 = mx(R(0.01), sq(mx(R(0.0), cc + d)));
-    R u34 = mx(R(0.01), sq(mx(R(0.0), cc / A.exphl + d * A.exphl)));
-    R u4 = mx(R(0.01), sq(mx(R(0.0), cc / A.expl + d * A.expl)));
+    R u1, u12, nu2, u3, u34, u4, nalogl, nalogu;
+    if constexpr (sizeof(R) == 4) {
+        // FP32: the closed forms of Profile (no cancellation in y - 1)
+        const R xl = (v * v) * A.bdl;
+        const Profile<R> pl = profile(xl, A.hl);
+        nalogl = A.alog3 - vonk * sq(pl.y / A.bdl);
+        v = (A.alog2 - nalogl) / vonk;
+        const R xu = (v * v) * A.bdu / strat[0];
+        const Profile<R> pu = profile(xu, A.hu);
+        nalogu = A.alog1 - vonk * sq(pu.y / A.bdu);
+        v = F.ua * vonk / (A.aloga - nalogu);
+        const R tauu = (v * v) * strat[2];
+        const R ku = R(0.5) * tauu / (pu.d * A.bdu);
+        const R taul = tauu / pu.d;
+        const R kl = R(0.5) * taul / (pl.d * A.bdl);
+        u1 = mx(R(0.01), sq(mx(R(0.0), ku * pu.top2)));
+        u12 = mx(R(0.01), sq(mx(R(0.0), ku * pu.mid2)));
+        nu2 = mx(R(0.01), sq(mx(R(0.0), R(2.0) * ku * xu)));
+        u3 = mx(R(0.01), sq(mx(R(0.0), kl * pl.top2)));
+        u34 = mx(R(0.01), sq(mx(R(0.0), kl * pl.mid2)));
+        u4 = mx(R(0.01), sq(mx(R(0.0), R(2.0) * kl * xl)));
+    } else {
+        // FP64: the reference's operations
+        R x = (v * v) * A.bdl;
+        R rw = R(1.0) / A.expl;
+        R yl = ((x + R(1)) * A.expl + (x - R(1)) * rw) / ((x + R(1)) * A.expl - (x - R(1)) * rw);
+        nalogl = A.alog3 - vonk * sq(yl / A.bdl);
+        v = (A.alog2 - nalogl) / vonk;
+        x = (v * v) * A.bdu / strat[0];
+        rw = R(1.0) / A.expu;
+        R yu = ((x + R(1)) * A.expu + (x - R(1)) * rw) / ((x + R(1)) * A.expu - (x - R(1)) * rw);
+        nalogu = A.alog1 - vonk * sq(yu / A.bdu);
+        v = F.ua * vonk / (A.aloga - nalogu);
+        R tauu = (v * v) * strat[2];
+        R a = R(0.5) * tauu * (yu + R(1)) / A.bdu;
+        R b = R(0.5) * tauu * (yu - R(1)) / A.bdu;
+        R taul = A.bdu * (a / A.expu - b * A.expu);
+        R cc = R(0.5) * taul * (yl + R(1)) / A.bdl;
+        R d = R(0.5) * taul * (yl - R(1)) / A.bdl;
+        u1 = mx(R(0.01), sq(mx(R(0.0), a + b)));
+        u12 = mx(R(0.01), sq(mx(R(0.0), a / A.exphu + b * A.exphu)));
+        nu2 = mx(R(0.01), sq(mx(R(0.0), a / A.expu + b * A.expu)));
+        u3 = mx(R(0.01), sq(mx(R(0.0), cc + d)));
+        u34 = mx(R(0.01), sq(mx(R(0.0), cc / A.exphl + d * A.exphl)));
+        u4 = mx(R(0.01), sq(mx(R(0.0), cc / A.expl + d * A.expl)));
+    }
     R ca = F.ua * strat[3] * P.vonk2 / ((A.aloga - nalogu) * (A.aloga - A.alog1));
     ca = mn(P.cdmax, ca / (R(1.0) + ca * R(1e-20)));
     const R rhoa = A.rhoa;
