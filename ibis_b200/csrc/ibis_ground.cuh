@@ -222,67 +222,88 @@ __device__ __forceinline__ void soil_water(double (&w)[NL], double& wpud, double
 // soilheat / soilheat_with_bedrock (soil_physics.py:385-490, bedrock.py:88-153)
 // NT = 6 (no bedrock) or 9; the first NL layers carry water.
 // ---------------------------------------------------------------------------
+// soilheat (soil_physics.py:385-490) or soilheat_with_bedrock (bedrock.py:88-153):
+// always double.  In float32 the solve works on absolute temperatures (~280 K,
+// one ulp 3e-5 K) while the deep layers change by ~1e-4 K an hour, so each
+// hour's rounding is a sizeable part of their change, and a consistent residue
+// (the same rounding repeated while a layer changes slowly) integrates over a
+// year into a drift of the deep column (-0.03 to -0.09 K a year, every cell
+// colder, measured against the float64 kernels).  The FP32 kernels therefore
+// widen the inputs, solve and form the fluxes in double, and round only the new
+// temperatures; the FP64 kernels perform the same operations as before.
+//
+// The layers' starting temperatures are t[k] + dtp[k] (dtp: the heat of the
+// transpired water, loops.py:1008-1025), summed here in double: in float32 an
+// hourly increment below half an ulp of the temperature would be dropped every
+// hour.
 template <typename R, int NT>
-__device__ __forceinline__ void soil_heat(R (&t)[NT], R (&hflo)[NL + 1], const R (&owsoi)[NL], const R (&wsoi)[NL],
-                                          const R (&wisoi)[NL], const R (&poros)[NL], const R (&consoi)[NL],
-                                          const R (&csoi)[NL], const R (&rhosoi)[NL], R c0pud0, R c1pud0, R fhtop,
-                                          const R (&wflo)[NL + 1], const DevParams<R>& P) {
-    R h[NT], con[NT + 1], whf[NT + 1], c0[NT], c1[NT];
+__device__ __forceinline__ void soil_heat(R (&t)[NT], R (&hflo)[NL + 1], const R (&dtp)[NL], const R (&owsoi)[NL],
+                                          const R (&wsoi)[NL], const R (&wisoi)[NL], const R (&poros)[NL],
+                                          const R (&consoi)[NL], const R (&csoi)[NL], const R (&rhosoi)[NL],
+                                          R c0pud0, R c1pud0, R fhtop, const R (&wflo)[NL + 1],
+                                          const DevParams<R>& P) {
+    using D = double;
+    D h[NT], con[NT + 1], whf[NT + 1], c0[NT], c1[NT], td[NT];
 #pragma unroll
-    for (int k = 0; k < NT; ++k) h[k] = k < NL ? P.hsoi[k] : P.hsoi_bed[k - NL];
-    auto cons = [&](int k) -> R { return k < NL ? consoi[k] : P.consoi_bed; };
-    con[0] = R(0.0);
-    con[NT] = R(0.0);
-    whf[0] = wflo[0] * P.ch2o * t[0];
+    for (int k = 0; k < NT; ++k) {
+        h[k] = k < NL ? (D)P.hsoi[k] : (D)P.hsoi_bed[k - NL];
+        td[k] = k < NL ? (D)t[k] + (D)dtp[k] : (D)t[k];
+    }
+    const D ch2o = (D)P.ch2o, dtime = (D)P.dtime;
+    auto cons = [&](int k) -> D { return k < NL ? (D)consoi[k] : (D)P.consoi_bed; };
+    con[0] = 0.0;
+    con[NT] = 0.0;
+    whf[0] = (D)wflo[0] * ch2o * td[0];
 #pragma unroll
     for (int k = 1; k < NT; ++k) {
-        con[k] = R(1.0) / (R(0.5) * (h[k - 1] / mx(cons(k - 1), R(1e-12)) + h[k] / mx(cons(k), R(1e-12))));
+        con[k] = dv<R>(1.0, 0.5 * (dv<R>(h[k - 1], fmax(cons(k - 1), 1e-12)) + dv<R>(h[k], fmax(cons(k), 1e-12))));
         if (k < NL) {
-            R tav = (h[k] * t[k - 1] + h[k - 1] * t[k]) / (h[k - 1] + h[k]);
-            whf[k] = wflo[k] * P.ch2o * tav;
+            D tav = dv<R>(h[k] * td[k - 1] + h[k - 1] * td[k], h[k - 1] + h[k]);
+            whf[k] = (D)wflo[k] * ch2o * tav;
         }
     }
-    R drain = wflo[NL] * P.ch2o * t[NL - 1];
+    D drain = (D)wflo[NL] * ch2o * td[NL - 1];
 #pragma unroll
     for (int k = NL; k <= NT; ++k) whf[k] = drain;
 #pragma unroll
     for (int k = 0; k < NT; ++k) {
         if (k < NL) {
-            R r1 = (R(1.0) - poros[k]) * csoi[k] * rhosoi[k];
-            R r2 = poros[k] * (R(1.0) - wisoi[k]) * P.ch2o * P.rhow;
-            R r3 = poros[k] * wisoi[k] * P.cice * P.rhow;
-            R pud0 = k == 0 ? c0pud0 : R(0.0);
-            R pud1 = k == 0 ? c1pud0 : R(0.0);
-            c0[k] = pud0 + (r1 + r2 * owsoi[k] + r3) * h[k];
-            c1[k] = pud1 + (r1 + r2 * wsoi[k] + r3) * h[k];
+            const D por = (D)poros[k];
+            D r1 = (1.0 - por) * (D)csoi[k] * (D)rhosoi[k];
+            D r2 = por * (1.0 - (D)wisoi[k]) * ch2o * (D)P.rhow;
+            D r3 = por * (D)wisoi[k] * (D)P.cice * (D)P.rhow;
+            D pud0 = k == 0 ? (D)c0pud0 : 0.0;
+            D pud1 = k == 0 ? (D)c1pud0 : 0.0;
+            c0[k] = pud0 + (r1 + r2 * (D)owsoi[k] + r3) * h[k];
+            c1[k] = pud1 + (r1 + r2 * (D)wsoi[k] + r3) * h[k];
         } else {
             // bedrock: zero porosity and water, so (1-0) csoi rho plus 0 * 0 terms (bedrock.py:132-150)
-            R r1 = (R(1.0) - R(0.0)) * P.csoi_bed * P.rhosoi_bed;
-            R v = R(0.0) + (r1 + R(0.0) * R(0.0) + R(0.0)) * h[k];
+            D r1 = (1.0 - 0.0) * (D)P.csoi_bed * (D)P.rhosoi_bed;
+            D v = 0.0 + (r1 + 0.0 * 0.0 + 0.0) * h[k];
             c0[k] = v;
             c1[k] = v;
         }
     }
-    R lo[NT], di[NT], up[NT], r[NT], tn[NT];
+    D lo[NT], di[NT], up[NT], r[NT], tn[NT];
 #pragma unroll
     for (int k = 0; k < NT; ++k) {
-        R rw = P.dtime / c1[k];
+        D rw = dv<R>(dtime, c1[k]);
         lo[k] = -rw * con[k];
-        di[k] = R(1.0) + rw * (con[k] + con[k + 1]);
+        di[k] = 1.0 + rw * (con[k] + con[k + 1]);
         up[k] = -rw * con[k + 1];
-        r[k] = (c0[k] / c1[k]) * t[k] + rw * (whf[k] - whf[k + 1]);
-        if (k == 0) r[k] = r[k] + (P.dtime / c1[k]) * fhtop;
+        r[k] = dv<R>(c0[k], c1[k]) * td[k] + rw * (whf[k] - whf[k + 1]);
+        if (k == 0) r[k] = r[k] + dv<R>(dtime, c1[k]) * (D)fhtop;
     }
     thomas(lo, di, up, r, tn);
-    R s = fhtop;
-    hflo[0] = s;
+    D s = (D)fhtop;
+    hflo[0] = (R)s;
 #pragma unroll
     for (int k = 0; k < NT; ++k) {
-        s = s - (c1[k] * tn[k] - c0[k] * t[k]) / P.dtime;
-        if (k < NL) hflo[k + 1] = s;
+        s = s - dv<R>(c1[k] * tn[k] - c0[k] * td[k], dtime);
+        if (k < NL) hflo[k + 1] = (R)s;
     }
 #pragma unroll
-    for (int k = 0; k < NT; ++k) t[k] = tn[k];
+    for (int k = 0; k < NT; ++k) t[k] = (R)tn[k];
 }
 
 // wadjust (soil_physics.py:147-189); returns the mass adjustment rate

@@ -522,7 +522,7 @@ __device__ __forceinline__ void ground_phase(Col<R>& c, const Forc<R>& F, const 
     const R gtransu = M.fvaput * R(2.0) * lai1 * fu;
     const R gtransl = M.fvaplt * R(2.0) * lai0 * fl * (R(1.0) - fi);
     const R sstu = mx(stresstu, eps), sstl = mx(stresstl, eps);
-    R tpt[NT];
+    R tpt[NT], dtp[NL];
 #pragma unroll
     for (int k = 0; k < NL; ++k) {
         R wu_ = stresstu >= R(1.0) ? P.froot[2 * k + 1] : stressu[k] / sstu;
@@ -534,7 +534,8 @@ __device__ __forceinline__ void ground_phase(Col<R>& c, const Forc<R>& F, const 
         R c0 = k == 0 ? c0pud0 : R(0.0);
         R cx = c0 + ((R(1.0) - poros[k]) * csoi[k] * rhosoi[k] + poros[k] * (R(1.0) - wisw[k]) * wsw[k] * P.ch2o * P.rhow
                      + poros[k] * wisw[k] * P.cice * P.rhow) * P.hsoi[k];
-        tpt[k] = c.tsoi[k] + (-dt * P.ch2o * (uu * (tu - c.tsoi[k]) + ul * (tl - c.tsoi[k])) / mx(cx, eps));
+        dtp[k] = -dt * P.ch2o * (uu * (tu - c.tsoi[k]) + ul * (tl - c.tsoi[k])) / mx(cx, eps);
+        tpt[k] = c.tsoi[k] + dtp[k];
     }
     const R fhtop_soil = heatg_avg + raing_avg * P.ch2o * (traing_avg - tpt[0])
                        - grunof * P.ch2o * mx(P.tmelt - tpt[0], R(0.0));
@@ -554,9 +555,13 @@ __device__ __forceinline__ void ground_phase(Col<R>& c, const Forc<R>& F, const 
     }
     const R c1pud0 = P.ch2o * wpud_h + P.cice * wiw;
     R hflo[NL + 1];
+    // the solve starts from tsoi + dtp, summed in double (soil_heat)
+#pragma unroll
+    for (int k = 0; k < NL; ++k) tpt[k] = c.tsoi[k];
 #pragma unroll
     for (int k = NL; k < NT; ++k) tpt[k] = c.tsoi_deep[k - NL];
-    soil_heat<R, NT>(tpt, hflo, wsw, wnew, wisw, poros, consoi, csoi, rhosoi, c0pud0, c1pud0, fhtop_soil, wflo, P);
+    soil_heat<R, NT>(tpt, hflo, dtp, wsw, wnew, wisw, poros, consoi, csoi, rhosoi, c0pud0, c1pud0, fhtop_soil, wflo,
+                     P);
     R gadj = water_bounds(wnew, wisw, poros, P);
     R pflo_ft[NL];
     R tft[NL];

