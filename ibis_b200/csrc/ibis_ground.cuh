@@ -222,26 +222,100 @@ __device__ __forceinline__ void soil_water(double (&w)[NL], double& wpud, double
 // soilheat / soilheat_with_bedrock (soil_physics.py:385-490, bedrock.py:88-153)
 // NT = 6 (no bedrock) or 9; the first NL layers carry water.
 // ---------------------------------------------------------------------------
-// soilheat (soil_physics.py:385-490) or soilheat_with_bedrock (bedrock.py:88-153):
-// always double.  In float32 the solve works on absolute temperatures (~280 K,
-// one ulp 3e-5 K) while the deep layers change by ~1e-4 K an hour, so each
-// hour's rounding is a sizeable part of their change, and a consistent residue
-// (the same rounding repeated while a layer changes slowly) integrates over a
-// year into a drift of the deep column (-0.03 to -0.09 K a year, every cell
-// colder, measured against the float64 kernels).  The FP32 kernels therefore
-// widen the inputs, solve and form the fluxes in double, and round only the new
-// temperatures; the FP64 kernels perform the same operations as before.
+// The soil heat solve of the FP32 kernels in increment form: the same system
+// for delta = T_new - t, whose right-hand side holds only small terms -- the
+// heat-capacity change times t, the transpired water's heat, the flux
+// divergence, and the conduction of the current temperature differences -- so
+// float32 rounds relative to the hour's change, not to the temperature.
+template <int NT>
+__device__ __forceinline__ void soil_heat_increments(float (&t)[NT], float (&hflo)[NL + 1], const float (&dtp)[NL],
+                                                     const float (&owsoi)[NL], const float (&wsoi)[NL],
+                                                     const float (&wisoi)[NL], const float (&poros)[NL],
+                                                     const float (&consoi)[NL], const float (&csoi)[NL],
+                                                     const float (&rhosoi)[NL], float c0pud0, float c1pud0,
+                                                     float fhtop, const float (&wflo)[NL + 1],
+                                                     const DevParams<float>& P) {
+    float h[NT], con[NT + 1], whf[NT + 1], c0[NT], c1[NT], dc[NT], ts[NT];
+#pragma unroll
+    for (int k = 0; k < NT; ++k) {
+        h[k] = k < NL ? P.hsoi[k] : P.hsoi_bed[k - NL];
+        ts[k] = k < NL ? t[k] + dtp[k] : t[k];      // the starting temperatures, for the advected heat
+    }
+    auto cons = [&](int k) -> float { return k < NL ? consoi[k] : P.consoi_bed; };
+    con[0] = 0.0f;
+    con[NT] = 0.0f;
+    whf[0] = wflo[0] * P.ch2o * ts[0];
+#pragma unroll
+    for (int k = 1; k < NT; ++k) {
+        con[k] = 1.0f / (0.5f * (h[k - 1] / fmaxf(cons(k - 1), 1e-12f) + h[k] / fmaxf(cons(k), 1e-12f)));
+        if (k < NL) whf[k] = wflo[k] * P.ch2o * ((h[k] * ts[k - 1] + h[k - 1] * ts[k]) / (h[k - 1] + h[k]));
+    }
+    const float drain = wflo[NL] * P.ch2o * ts[NL - 1];
+#pragma unroll
+    for (int k = NL; k <= NT; ++k) whf[k] = drain;
+#pragma unroll
+    for (int k = 0; k < NT; ++k) {
+        if (k < NL) {
+            const float r1 = (1.0f - poros[k]) * csoi[k] * rhosoi[k];
+            const float r2 = poros[k] * (1.0f - wisoi[k]) * P.ch2o * P.rhow;
+            const float r3 = poros[k] * wisoi[k] * P.cice * P.rhow;
+            c0[k] = (k == 0 ? c0pud0 : 0.0f) + (r1 + r2 * owsoi[k] + r3) * h[k];
+            c1[k] = (k == 0 ? c1pud0 : 0.0f) + (r1 + r2 * wsoi[k] + r3) * h[k];
+            dc[k] = (k == 0 ? c0pud0 - c1pud0 : 0.0f) + r2 * (owsoi[k] - wsoi[k]) * h[k];   // c0 - c1
+        } else {
+            c0[k] = c1[k] = P.csoi_bed * P.rhosoi_bed * h[k];
+            dc[k] = 0.0f;
+        }
+    }
+    float lo[NT], di[NT], up[NT], r[NT], dl[NT];
+#pragma unroll
+    for (int k = 0; k < NT; ++k) {
+        const float rw = P.dtime / c1[k];
+        lo[k] = -rw * con[k];
+        di[k] = 1.0f + rw * (con[k] + con[k + 1]);
+        up[k] = -rw * con[k + 1];
+        // (c0/c1) ts + rw (F - conduction of t) - t, term by term
+        float cond = con[k] * (t[k] - (k > 0 ? t[k - 1] : t[k]));
+        if (k + 1 < NT) cond = cond + con[k + 1] * (t[k] - t[k + 1]);
+        float flux = whf[k] - whf[k + 1] + (k == 0 ? fhtop : 0.0f);
+        r[k] = (dc[k] / c1[k]) * t[k] + (c0[k] / c1[k]) * (k < NL ? dtp[k] : 0.0f) + rw * (flux - cond);
+    }
+    thomas(lo, di, up, r, dl);
+    float s = fhtop;
+    hflo[0] = s;
+#pragma unroll
+    for (int k = 0; k < NT; ++k) {
+        // (c1 T_new - c0 ts) / dt with T_new = t + delta and ts = t + dtp
+        s = s - (c1[k] * dl[k] - dc[k] * t[k] - c0[k] * (k < NL ? dtp[k] : 0.0f)) / P.dtime;
+        if (k < NL) hflo[k + 1] = s;
+    }
+#pragma unroll
+    for (int k = 0; k < NT; ++k) t[k] = t[k] + dl[k];
+}
+
+// soilheat (soil_physics.py:385-490) or soilheat_with_bedrock (bedrock.py:88-153).
+// The FP64 kernels perform the reference's operations on absolute temperatures.
+// The FP32 kernels solve for the increments (soil_heat_increments above): on
+// absolute temperatures (~280 K, one ulp 3e-5 K) float32 rounds each hour by a
+// sizeable part of a deep layer's change (~1e-4 K), and the residue repeats
+// while a layer changes slowly -- over a year it cooled the deep column of every
+// cell by 0.03-0.09 K against the float64 kernels, and with it the runoff, ET
+// and CH4 sums drifted by up to 4e-4.
 //
 // The layers' starting temperatures are t[k] + dtp[k] (dtp: the heat of the
-// transpired water, loops.py:1008-1025), summed here in double: in float32 an
-// hourly increment below half an ulp of the temperature would be dropped every
-// hour.
+// transpired water, loops.py:1008-1025), kept apart because in float32 an
+// hourly increment below half an ulp of the temperature would be dropped.
 template <typename R, int NT>
 __device__ __forceinline__ void soil_heat(R (&t)[NT], R (&hflo)[NL + 1], const R (&dtp)[NL], const R (&owsoi)[NL],
                                           const R (&wsoi)[NL], const R (&wisoi)[NL], const R (&poros)[NL],
                                           const R (&consoi)[NL], const R (&csoi)[NL], const R (&rhosoi)[NL],
                                           R c0pud0, R c1pud0, R fhtop, const R (&wflo)[NL + 1],
                                           const DevParams<R>& P) {
+    if constexpr (sizeof(R) == 4) {
+        soil_heat_increments<NT>(t, hflo, dtp, owsoi, wsoi, wisoi, poros, consoi, csoi, rhosoi, c0pud0, c1pud0, fhtop,
+                                 wflo, P);
+        return;
+    }
     using D = double;
     D h[NT], con[NT + 1], whf[NT + 1], c0[NT], c1[NT], td[NT];
 #pragma unroll

@@ -555,7 +555,7 @@ __device__ __forceinline__ void ground_phase(Col<R>& c, const Forc<R>& F, const 
     }
     const R c1pud0 = P.ch2o * wpud_h + P.cice * wiw;
     R hflo[NL + 1];
-    // the solve starts from tsoi + dtp, summed in double (soil_heat)
+    // the solve starts from tsoi + dtp, the increment kept apart (soil_heat)
 #pragma unroll
     for (int k = 0; k < NL; ++k) tpt[k] = c.tsoi[k];
 #pragma unroll

@@ -16,7 +16,8 @@ Tolerances (as for the F77 step in test_gpu_parity.py):
   near-zero fields, tests/goldens.py:FLOORS); day accumulators 1e-6 (the
   reference casts each step's CH4 flux to float32).
 * FP32 kernels vs the float64 oracle after one hour: the bounds of the F77
-  step's FP32 test.
+  step's FP32 test (test_gpu_parity.FP32_ONE_HOUR); conductances and
+  intercellular CO2 within 1e-4.
 """
 import types
 import warnings
@@ -94,13 +95,13 @@ def test_f32_kernel_close_to_oracle(cuda_lib, name):
     cols = _run(c, torch.float32, 1)
     prog, _, _ = _oracle(c, 1)
     got = cols.prog_host()
-    for k in ("tsoi", "tg", "tu", "ts", "tl", "t12", "t34", "tsno", "ti", "tsoi_deep"):
-        g, w = np.asarray(got[k], np.float64).reshape(prog[k].shape), prog[k]
-        out = np.abs(g - w) > 0.5 + 2e-3 * np.abs(w)
-        assert out.reshape(out.shape[0], -1).any(axis=1).sum() <= 1 and np.max(np.abs(g - w)) <= 2.0, k
+    from test_gpu_parity import FP32_ONE_HOUR
+    for k, bound in FP32_ONE_HOUR.items():
+        g = np.asarray(got[k], np.float64).reshape(prog[k].shape)
+        assert float(np.max(np.abs(g - prog[k]))) <= bound, k
     for k in ("gs_upper", "gs_lower", "ci_upper", "ci_lower"):
         g, w = np.asarray(got[k], np.float64).reshape(prog[k].shape), prog[k]
-        np.testing.assert_allclose(g, w, rtol=1e-2, atol=1e-6, err_msg=k)
+        np.testing.assert_allclose(g, w, rtol=1e-4, atol=1e-8, err_msg=k)
 
 
 def test_f32_release_day_close_to_reference(cuda_lib):

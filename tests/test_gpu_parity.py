@@ -5,11 +5,13 @@ Tolerances:
   6 steps on every golden case, with absolute floors for near-zero fields
   (tests/goldens.py:FLOORS).  Cells may differ only where a threshold branch of
   the reference flips on last-bit differences; none does on these cases.
-* FP32 kernels (FP64 canopy and soil-water solves) vs the float64 oracle:
-  relative 2e-3 on temperatures/states after one step in all but 1% of the
-  cells, those within 2 K (the reference's own float32 run differs from its
-  float64 run by up to 1.6 K hourly in canopy temperature,
-  docs/technote/17_numerics_verification.md:367-383).
+* FP32 kernels (FP64 canopy and soil-water solves) vs the float64 oracle
+  after one step, every cell: temperatures within 5 mK, soil water and ice
+  within 1e-5, snow and puddle stores within their own small bounds -- a small
+  multiple of the measured departure (at most 1.1 mK on the realistic
+  restart_1996 state, 0.2 mK on the synthetic cases; the reference's own
+  float32 run departs from its float64 run by up to 1.6 K hourly in canopy
+  temperature over a year, docs/technote/17_numerics_verification.md:367-383).
 * After several hours, cells sitting on a phase-change threshold in the
   realistic restart_1996 state are exempt (tests/goldens.py:THRESHOLD_CELLS).
 """
@@ -84,22 +86,19 @@ def test_f32_kernel_close_to_oracle(cuda_lib, name):
     cols = _run_gpu(c, torch.float32, 1)
     prog, D, acc = _run_oracle(c, 1)
     got = cols.prog_host()
-    for k in ("tsoi", "tg", "tu", "ts", "tl", "t12", "t34", "tsno", "ti", "tsoi_deep"):
-        _close_most(got[k], prog[k], k, rtol=2e-3, atol=0.5, worst=2.0)
-    for k in ("wsoi", "wisoi", "fi"):
-        _close_most(got[k], prog[k], k, rtol=2e-3, atol=2e-3, worst=2e-2)
+    for k, bound in FP32_ONE_HOUR.items():
+        g = np.asarray(got[k], np.float64).reshape(prog[k].shape)
+        err = float(np.max(np.abs(g - prog[k])))
+        assert err <= bound, (k, err, bound)
 
 
-def _close_most(g, w, k, rtol, atol, worst):
-    """FP32 vs float64 after one hour: every cell within rtol/atol except at most
-    1% of the cells (at least one), which must stay within ``worst`` (absolute):
-    the reference's own float32 run departs from its float64 run by up to 1.6 K
-    in hourly canopy temperature (docs/technote/17_numerics_verification.md:367-383)."""
-    g = np.asarray(g, np.float64).reshape(np.shape(w))
-    out = np.abs(g - w) > atol + rtol * np.abs(w)
-    cells = np.any(out.reshape(out.shape[0], -1), axis=1)
-    assert cells.sum() <= max(1, int(0.01 * cells.size)), (k, int(cells.sum()))
-    assert np.max(np.abs(g - w)) <= worst, (k, float(np.max(np.abs(g - w))))
+# FP32 vs float64 after one hour, absolute, every cell: about 5x the largest
+# departure measured over the golden cases (temperatures K, stores kg m-2 or
+# fractions)
+FP32_ONE_HOUR = {
+    **{k: 5e-3 for k in ("tsoi", "tg", "tu", "ts", "tl", "t12", "t34", "tsno", "ti", "tsoi_deep")},
+    "wsoi": 1e-5, "wisoi": 1e-5, "fi": 2e-6, "hsno": 3e-5, "wpud": 5e-4, "wipud": 2e-5, "q12": 2e-6, "q34": 2e-6,
+}
 
 
 @pytest.mark.parametrize("name", ["day_mixed", "sunshade"])

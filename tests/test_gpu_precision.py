@@ -1,16 +1,17 @@
-"""FP32 production kernels against the FP64 kernels over a year, and the FP64
-kernels against the oracle over a week (last-bit differences between CUDA's
-and the host's arithmetic grow slowly through the snow and soil-water
-coupling; after 6 steps they are below 1e-9, tests/test_gpu_parity.py).
+"""FP32 production kernels against the FP64 kernels and the float64 oracle over
+a year, and the FP64 kernels against the oracle over a week and a year.
 
-Bounds (relative error of the all-cell annual total, 1,000 cells x 8,760 h):
-GPP, NPP, ET, canopy sensible heat and the annual-mean soil temperature of
-every layer within 1e-4; runoff and drainage within 1e-3 and wetland CH4
-within 2e-3, which follow soil moisture, whose FP32 trajectory departs further
-from the FP64 one.  Integer-valued counters stay integers; the fire-season
-counters are threshold counts of FP state and agree in at least 98% of cells.
-The reference's own float32 run differs from its float64 run by more than this
-(docs/technote/17_numerics_verification.md:367-383).
+Bounds (relative error of the all-cell annual total, the first 1,000 columns of
+the 95,333-cell population x 8,760 h): every annual flux -- GPP, NPP, ET,
+canopy sensible heat, runoff, drainage, wetland CH4 -- and the annual-mean soil
+temperature of every layer within 1e-4 of the FP64 kernels (measured: at most
+6.7e-6, soil temperature 1.6e-8), and within 1e-4 of the float64 oracle on
+the first 16 columns; the FP64 kernels within 1e-5 of the oracle over the year
+(measured 5.6e-7 on 100 columns).  Integer-valued counters stay integers,
+``nytimes`` is exact, and the fire-season counters -- threshold counts of
+floating-point state -- agree in at least 99 % of cells (measured 99.9 % and
+99.6 %).  Storing the soil water in float32 alone (the ``f64_w32`` leg) moves
+no annual total by more than 1e-5 (measured 3.4e-7).
 """
 import warnings
 
@@ -29,29 +30,33 @@ warnings.filterwarnings("ignore", category=RuntimeWarning)
 
 @pytest.fixture(scope="module")
 def year_report(cuda_lib):
-    return precision.report(1000, 8760)
+    return precision.report(1000, 8760, oracle_cells=16)
 
 
 def test_no_nonfinite(year_report):
-    assert not year_report["nonfinite"]["f32"] and not year_report["nonfinite"]["f64"]
+    assert not any(year_report["nonfinite"].values())
 
 
-@pytest.mark.parametrize("flux,bound", [("gpp", 1e-4), ("npp", 1e-4), ("et", 1e-4), ("sensible_heat", 1e-4),
-                                        ("runoff", 1e-3), ("drainage", 1e-3), ("ch4", 2e-3)])
-def test_annual_flux_totals(year_report, flux, bound):
-    assert year_report["fluxes"][flux]["total_rel"] < bound, year_report["fluxes"][flux]
+@pytest.mark.parametrize("flux", list(precision.FLUXES))
+def test_annual_flux_totals(year_report, flux):
+    assert year_report["fluxes"][flux]["total_rel"] < 1e-4, year_report["fluxes"][flux]
+    assert year_report["oracle"]["f32_vs_oracle"]["fluxes"][flux]["total_rel"] < 1e-4
+    assert year_report["oracle"]["f64_vs_oracle"]["fluxes"][flux]["total_rel"] < 1e-5
+    assert year_report["legs"]["f64_w32"]["fluxes"][flux]["total_rel"] < 1e-5
 
 
 def test_soil_temperature_by_layer(year_report):
     for k, v in year_report["soil_t"].items():
-        assert v["total_rel"] < 1e-4 and v["max_rel"] < 1e-3, (k, v)
+        assert v["total_rel"] < 1e-4 and v["max_rel"] < 1e-4, (k, v)
 
 
 def test_counters(year_report):
     c = year_report["counters"]
     assert all(v["integer_valued"] for v in c.values())
     assert c["nytimes"]["equal_frac"] == 1.0
-    assert c["nfirestep"]["equal_frac"] >= 0.98 and c["nfirestep_vpd"]["equal_frac"] >= 0.98
+    assert c["nfirestep"]["equal_frac"] >= 0.99 and c["nfirestep_vpd"]["equal_frac"] >= 0.99
+    o = year_report["oracle"]["f64_vs_oracle"]["counters"]
+    assert all(v["equal_frac"] == 1.0 for v in o.values())
 
 
 def test_f64_kernel_tracks_oracle_for_a_week(cuda_lib):
