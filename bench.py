@@ -30,6 +30,11 @@ REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
 METRIC = "cell-steps/s at 95,333 cells, ≤1e-4 rel err vs FP64; serve p50/p99 latency"
+# What every CPU number of this file is
+CPU_CAVEAT = ("the only CPU implementation of the step available here is the float64 NumPy restatement of the "
+              "reference (the oracle): the reference's own JAX CPU path cannot be installed on this image (no jax, "
+              "jaxlib or equinox), and no compiled CPU port was built, so GPU-to-CPU ratios against it overstate "
+              "the speed-up over a compiled (XLA or C++) CPU path")
 NCELL = 95333
 HOURS = 24
 
@@ -147,7 +152,8 @@ def cpu_baseline_sample(ncell=16384, hours=HOURS, seed=123):
     return {"value": ncell * hours / dt, "unit": "cell-steps/s", "cores": 1, "kind": "port",
             "sample": f"{ncell} cells x {hours} hourly steps of the bench's seeded column generator, float64 NumPy "
                       f"oracle, "
-                      f"{dt:.1f} s"}
+                      f"{dt:.1f} s",
+            "note": CPU_CAVEAT}
 
 
 # ---------------------------------------------------------------------------- reference arm
@@ -199,8 +205,7 @@ def run_reference(args):
             "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": len(tasks), "kind": "port",
                              "sample": f"{ncell} cells x {HOURS} h per step over {len(tasks)} spawned processes"},
             "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "note": "the reference's JAX step is not installable here (no jax/jaxlib/equinox wheels); this arm "
-                    "times the oracle port of its algorithm"}
+            "note": CPU_CAVEAT}
     print(json.dumps(line), flush=True)
 
 
@@ -351,7 +356,8 @@ def single_cell(dev, stream, cpu_hours=480):
     dt = time.perf_counter() - t0
     out["cpu_f64_oracle"] = {"value": cpu_hours / dt, "unit": "cell-steps/s", "cores": 1,
                              "year_estimate_s": dt / cpu_hours * 8760,
-                             "sample": f"first {cpu_hours} hours of the year, float64 NumPy oracle"}
+                             "sample": f"first {cpu_hours} hours of the year, float64 NumPy oracle",
+                             "note": CPU_CAVEAT}
     out["note"] = ("1 column x 8,760 h: the GPU runs one thread through the year (latency bound); the reference's "
                    "JAX CPU path is not installable here, so the CPU leg is the float64 NumPy port on one core")
     return out
