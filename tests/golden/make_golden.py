@@ -548,7 +548,7 @@ def write_diurnal_case(days=(15, 172), seed=7, dtime=3600.0):
     print(f"wrote {path}: {len(out)} arrays, {os.path.getsize(path)} bytes")
 
 
-def write_days_case(ndays=3, jday0=172, seed=9, modules=False):
+def write_days_case(ndays=3, jday0=172, seed=9, modules=False, release=False):
     """tests/golden/days_16cells.npz: the reference's own GSWP3 day loop
     (_run_month_scan, loops_gswp3.py:334-612) for ``ndays`` days on the 16-cell
     checkpoint: phenology, 24 hourly steps with accumulators, 10-day means,
@@ -562,7 +562,12 @@ def write_days_case(ndays=3, jday0=172, seed=9, modules=False):
     random seasonal and stress states, under photoperiod-gated senescence of
     both canopies with low critical sums and a growing-season threshold of
     12 C, so the senescence triggers and the growing-season mask both split
-    the cells."""
+    the cells.  With ``release`` as well (tests/golden/days_release_16cells.npz)
+    the stomata section of the release parameter file
+    (configs/params/params_31s_ch4h.yaml, by the reference's own loader: vmax and
+    slope mixing, the NPP split by capacity, acclimation with per-PFT constants,
+    sunlit/shaded canopies) and its consistent soil-water weights apply, so the
+    acclimation the seasonal state drives reaches the hourly steps."""
     import jax
     from ibis.io.restart import load_state
     from oracle.weather import uniform24
@@ -585,6 +590,10 @@ def write_days_case(ndays=3, jday0=172, seed=9, modules=False):
         sp = dataclasses.replace(sp, pheno=dataclasses.replace(
             sp.pheno, sen_photoperiod_u=True, sen_photoperiod_l=True, sen_ycrit_u=25.0, sen_ycrit_l=40.0,
             stress_accum_tmin=12.0))
+    if release:
+        from ibis.io.physics_params import load_physics_params, build_stomata_params
+        d = load_physics_params(os.path.join(REF, "configs/params/params_31s_ch4h.yaml"))
+        sp = dataclasses.replace(sp, stomata_params=build_stomata_params(d), h2o_consistent_weights=True)
     days = []
     for d in range(ndays):
         dd, _ = daily_inputs(n, seed=seed + 10 + d)
@@ -636,7 +645,8 @@ def write_days_case(ndays=3, jday0=172, seed=9, modules=False):
         else:
             jax.random.uniform = saved[0]
         loops_gswp3._cast_tree_f32 = saved[1]
-    path = os.path.join(HERE, "days_modules_16cells.npz" if modules else "days_16cells.npz")
+    path = os.path.join(HERE, "days_release_16cells.npz" if release else
+                        "days_modules_16cells.npz" if modules else "days_16cells.npz")
     np.savez_compressed(path, **out)
     print(f"wrote {path}: {len(out)} arrays, {os.path.getsize(path)} bytes")
 
@@ -748,13 +758,15 @@ def main():
         write_parts_case()
     if args.only in (None, "days_modules"):
         write_days_case(jday0=250, modules=True)
+    if args.only in (None, "days_release"):
+        write_days_case(jday0=250, modules=True, release=True)
     if args.only in (None, "restart_modules"):
         write_restart_modules_case()
     for name in X3_CASES:
         if args.only in (None, name):
             write_x3_case(name)
     if args.only in ("restart_leaves", "restart_1996", "diurnal", "days", "methane_month", "observed_sw",
-                     "day_parts", "days_modules", "restart_modules") + tuple(X3_CASES):
+                     "day_parts", "days_modules", "days_release", "restart_modules") + tuple(X3_CASES):
         return
     for name, spec in CASES.items():
         if args.only and name != args.only:

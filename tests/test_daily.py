@@ -27,6 +27,10 @@ warnings.filterwarnings("ignore", category=RuntimeWarning)
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLD = os.path.join(HERE, "golden", "days_16cells.npz")
 GOLD_MODULES = os.path.join(HERE, "golden", "days_modules_16cells.npz")
+# the modules case again under the release parameter file's stomata switches
+# (acclimation driven by the seasonal state, vmax and slope mixing, capacity split,
+# sunlit/shaded canopies)
+GOLD_RELEASE = os.path.join(HERE, "golden", "days_release_16cells.npz")
 MODULE_LEAVES = {"acclim_x": "seasonal.acclim_x", "ssen_u": "seasonal.ssen_u", "ssen_l": "seasonal.ssen_l",
                  "aystressu": "stress.aystressu", "aystressl": "stress.aystressl", "stress_nday": "stress.nday"}
 PARTS = ("et_trans", "et_interc", "et_soilev", "et_snowsub", "nee_night", "nee_day")
@@ -160,12 +164,13 @@ def _compare_day(z, d, prog, day, stat, acc, exempt=()):
     return bad
 
 
-@pytest.mark.parametrize("gold", [GOLD, GOLD_MODULES], ids=["base", "modules"])
+@pytest.mark.parametrize("gold", [GOLD, GOLD_MODULES, GOLD_RELEASE], ids=["base", "modules", "release"])
 def test_oracle_day_loop_matches_reference_days(gold):
-    """The base case on every cell, and the case whose state carries the
-    optional modules (seasonal states with photoperiod-gated senescence,
-    growing-season stress sums, ET and NEE parts) outside its threshold cells:
-    every state field after each day."""
+    """The base case on every cell, the case whose state carries the optional
+    modules (seasonal states with photoperiod-gated senescence, growing-season
+    stress sums, ET and NEE parts) outside its threshold cells, and that case
+    under the release parameter file's stomata switches on every cell: every
+    state field after each day."""
     z = load_case(gold)[0]
     exempt = MODULE_THRESHOLD_CELLS if gold == GOLD_MODULES else ()
     checked = set()
@@ -173,22 +178,23 @@ def test_oracle_day_loop_matches_reference_days(gold):
         checked |= set(want(z, d, "DAYST"))
         bad = _compare_day(z, d, prog, day, stat, acc, exempt)
         assert not bad, (d, bad[:6])
-    assert (set(MODULE_LEAVES) <= checked) == (gold == GOLD_MODULES)
+    assert (set(MODULE_LEAVES) <= checked) == (gold != GOLD)
 
 
-def test_threshold_cells_of_the_modules_case():
-    """The exempt cells of the modules case are threshold cells: over the three
+@pytest.mark.parametrize("gold", [GOLD_MODULES, GOLD_RELEASE], ids=["modules", "release"])
+def test_threshold_cells_of_the_modules_case(gold):
+    """The exempt cells of the modules case (and of the same case under the
+    release parameter file's switches) are threshold cells: over the three
     days, 1e-15 perturbations (either sign) of the oracle's own temperatures or
     of its water, ice and snow state, before hour 0 or hour 12 of the first day,
     move exactly them beyond 1e-9."""
     n = 16
-    base = list(oracle_days(gold=GOLD_MODULES))
+    base = list(oracle_days(gold=gold))
     moved = set()
     cases = [(h, eps, f) for h in (0, 12) for eps in (-1e-15, 1e-15)
              for f in (("tsoi", "tg", "tl", "tu", "ti", "tsno"), ("wsoi", "wisoi", "hsno", "wpud", "wipud", "fi"))]
     for h, eps, fields in cases:
-        for (_, bp, bd, _, _), (_, pp, pd, _, _) in zip(base, oracle_days(gold=GOLD_MODULES,
-                                                                          perturb=(0, h, eps, fields))):
+        for (_, bp, bd, _, _), (_, pp, pd, _, _) in zip(base, oracle_days(gold=gold, perturb=(0, h, eps, fields))):
             err = np.zeros(n)
             for got, ref in ((pp, bp), (pd, bd)):
                 for k, w in ref.items():
@@ -247,7 +253,7 @@ def _device_state(cols, loop):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("gold", [GOLD, GOLD_MODULES], ids=["base", "modules"])
+@pytest.mark.parametrize("gold", [GOLD, GOLD_MODULES, GOLD_RELEASE], ids=["base", "modules", "release"])
 def test_device_day_kernels_match_oracle(cuda_lib, gold):
     """ibis_day_begin_f64 / ibis_day_end_f64 on the oracle's own inputs of
     each day of a three-day case (with the optional modules: seasonal states,
@@ -309,6 +315,32 @@ def test_device_day_loop_with_modules_matches_reference_days(cuda_lib):
     from ibis_b200 import synth
     z, n, cols, loop, torch = _device_loop(torch.float64, GOLD_MODULES)
     assert loop.day_params.seasonal_on == 1.0 and loop.params.flags & (3 << 10)
+    for d in range(int(z["in.ndays"])):
+        dd, daily = _daily_tensor(z, d, cols.ld, torch)
+        hours = hourly(z, d, n)
+        forc = {k: np.stack([F[k] for F in hours]) for k in hours[0]}
+        td = torch.from_numpy(np.pad(dd["td"], (0, cols.ld - n))).cuda()
+        loop.run_day(daily, forc=torch.from_numpy(synth.forcing_planes(forc, cols.ld, dtype=np.float64)).cuda(), td=td)
+        torch.cuda.synchronize()
+        prog, dayst, stat, acc = _device_state(cols, loop)
+        bad = _compare_day(z, d, prog, dayst, stat, acc, MODULE_THRESHOLD_CELLS)
+        assert not bad, (d, bad[:6])
+
+
+@pytest.mark.gpu
+def test_device_day_loop_with_release_switches_matches_reference_days(cuda_lib):
+    """The device day loop in float64 under the release parameter file's
+    stomata switches, the acclimation state advanced each day by ibis_day_begin
+    and read by that day's hourly steps, against the reference's day loop after
+    each of the three days: every state field within 1e-9 (1e-6 for the
+    float32-summed accumulators) outside the case's threshold cells -- the same
+    four as the modules case, proven by the same perturbations
+    (test_threshold_cells_of_the_modules_case) -- which stay within 1e-2."""
+    import torch
+    from ibis_b200 import synth
+    from ibis_b200.params import FLAG_ACCLIM
+    z, n, cols, loop, torch = _device_loop(torch.float64, GOLD_RELEASE)
+    assert loop.day_params.seasonal_on == 1.0 and loop.params.flags & FLAG_ACCLIM
     for d in range(int(z["in.ndays"])):
         dd, daily = _daily_tensor(z, d, cols.ld, torch)
         hours = hourly(z, d, n)
