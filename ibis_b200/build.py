@@ -46,6 +46,12 @@ UNITS = {
     "ibis_ens_inst_d.cu": F32_FLAGS,
     "ibis_ens_inst_e.cu": F32_FLAGS,
     "ibis_ens_inst_f.cu": F32_FLAGS,
+    "ibis_ens_x3_inst_a.cu": F32_FLAGS,
+    "ibis_ens_x3_inst_b.cu": F32_FLAGS,
+    "ibis_ens_x3_inst_c.cu": F32_FLAGS,
+    "ibis_ens_x3_inst_d.cu": F32_FLAGS,
+    "ibis_ens_x3_inst_e.cu": F32_FLAGS,
+    "ibis_ens_x3_inst_f.cu": F32_FLAGS,
     "ibis_diurnal_f32.cu": ["-use_fast_math"],
     "ibis_step_f64.cu": ["--fmad=false"],
     "ibis_daily.cu": ["--fmad=false"],

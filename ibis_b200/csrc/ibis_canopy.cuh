@@ -129,7 +129,8 @@ __device__ constexpr int kConiferPfts[3] = {3, 5, 7};
 __device__ constexpr int kShrubPfts[2] = {8, 9};
 
 // Per-PFT values read by the big-leaf selection: the source's vmax, times the
-// PFT factor when EFF; or the source's per-PFT Ball-Berry slopes.
+// PFT factor when EFF; or the per-PFT Ball-Berry slopes of the parameter record
+// (coefm_pft is not one of the parameters a calibration run varies).
 template <typename R, typename Q, int KIND>
 struct PftValue {
     const Q& q;
@@ -138,7 +139,7 @@ struct PftValue {
     __device__ __forceinline__ R operator()(int p) const {
         if constexpr (KIND == 0) return q.vmax(p);
         else if constexpr (KIND == 1) return pf.vf() ? q.vmax(p) * pf.at(p, P) : q.vmax(p);
-        else return q.coefm_pft(p);
+        else return P.coefm_pft[p];
     }
 };
 
@@ -191,8 +192,8 @@ __device__ __forceinline__ void big_leaves(R (&vn)[LOWER ? 3 : 2], R (&jf)[LOWER
             cm[1] = mix_pft(kConiferPfts, S, cp, q.coefm(1));
         } else {
             cm[0] = mix_pft(kShrubPfts, S, cp, q.coefm(2));
-            cm[1] = q.coefm_pft(11);
-            cm[2] = q.coefm_pft(10);
+            cm[1] = P.coefm_pft[11];
+            cm[2] = P.coefm_pft[10];
         }
     } else {
         if constexpr (!LOWER) { cm[0] = q.coefm(0); cm[1] = q.coefm(1); }

@@ -12,6 +12,8 @@
 // device counter in the caller's order (longest records first).
 #pragma once
 #include "ibis_diurnal.cuh"
+#include <type_traits>
+
 #include "ibis_kernels.cuh"
 
 namespace ibis {
@@ -166,11 +168,16 @@ __device__ __forceinline__ void flag_nonfinite(const EnsArgs& e, float sum, int 
 // steps (the day's terms once a day, then one diurnal hour per step), so the
 // forcing read from memory is one 48-byte record per site-day instead of one
 // per site-hour; a run's hours start at midnight of record run_forc.
-template <int NT, bool SU, bool SL, bool DAILY>
+// With X3 the runs step with the IBIS 3.0 extensions (IBIS_FLAGS_X3).
+template <bool X3>
+using RunSource = std::conditional_t<X3, RunQ3<float>, RunQ<float>>;
+
+template <int NT, bool SU, bool SL, bool DAILY, bool X3>
 __global__ void __launch_bounds__(256, 1) ensemble_kernel(const EnsArgs e, const DevParams<float> P) {
     extern __shared__ unsigned char smem_raw[];
     Col<float>& c = reinterpret_cast<Col<float>*>(smem_raw)[threadIdx.x];
-    RunQ<float>& q = reinterpret_cast<RunQ<float>*>(smem_raw + blockDim.x * sizeof(Col<float>))[threadIdx.x];
+    RunSource<X3>& q =
+        reinterpret_cast<RunSource<X3>*>(smem_raw + blockDim.x * sizeof(Col<float>))[threadIdx.x];
     DayCache* const dc =
         DAILY ? reinterpret_cast<DayCache*>(smem_raw + blockDim.x * (sizeof(Col<float>) + sizeof(RunQ<float>))) +
                     threadIdx.x
@@ -233,7 +240,7 @@ __global__ void __launch_bounds__(256, 1) ensemble_kernel(const EnsArgs e, const
 // Plain form: one launch per hour over all runs; run r takes its step when the
 // hour (*hour0 + k) is inside its record.  The hour is read from device memory
 // so a captured sequence of launches can be replayed (advance_hour moves it).
-template <int NT, bool SU, bool SL>
+template <int NT, bool SU, bool SL, bool X3>
 __global__ void __launch_bounds__(128, 2) ensemble_hour_kernel(const EnsArgs e, const DevParams<float> P,
                                                                const int* __restrict__ hour0, int k) {
     // hour0 is written only by advance_hour, a later launch on the same stream
@@ -248,7 +255,8 @@ __global__ void __launch_bounds__(128, 2) ensemble_hour_kernel(const EnsArgs e, 
     if (!run_ok(e, r, site, nstep, first, pos)) return;
     extern __shared__ unsigned char smem_raw[];
     Col<float>& c = reinterpret_cast<Col<float>*>(smem_raw)[threadIdx.x];
-    RunQ<float>& q = reinterpret_cast<RunQ<float>*>(smem_raw + blockDim.x * sizeof(Col<float>))[threadIdx.x];
+    RunSource<X3>& q =
+        reinterpret_cast<RunSource<X3>*>(smem_raw + blockDim.x * sizeof(Col<float>))[threadIdx.x];
     load_col(c, e.prog + r, e.ld_run);
     load_run_params(q, e.run_params + r, e.ld_run, P);
     const Stat<float> S{e.stat + site, e.ld_site};
@@ -270,9 +278,9 @@ inline size_t ens_smem(int block, bool daily = false) {
     return (size_t)block * (sizeof(Col<float>) + sizeof(RunQ<float>) + (daily ? sizeof(DayCache) : 0));
 }
 
-template <int NT, bool SU, bool SL, bool DAILY = false>
+template <int NT, bool SU, bool SL, bool DAILY = false, bool X3 = false>
 cudaError_t launch_ensemble(const EnsArgs& e, const DevParams<float>& P, int block, int grid, cudaStream_t s) {
-    auto k = ensemble_kernel<NT, SU, SL, DAILY>;
+    auto k = ensemble_kernel<NT, SU, SL, DAILY, X3>;
     const size_t smem = ens_smem(block, DAILY);
     cudaError_t err = fit_smem(k, block, smem, ens_smem(256, DAILY));
     if (err != cudaSuccess) return err;
@@ -280,10 +288,10 @@ cudaError_t launch_ensemble(const EnsArgs& e, const DevParams<float>& P, int blo
     return cudaGetLastError();
 }
 
-template <int NT, bool SU, bool SL>
+template <int NT, bool SU, bool SL, bool X3 = false>
 cudaError_t launch_ensemble_hours(const EnsArgs& e, const DevParams<float>& P, int* hour0, int nhour,
                                   cudaStream_t s) {
-    auto k = ensemble_hour_kernel<NT, SU, SL>;
+    auto k = ensemble_hour_kernel<NT, SU, SL, X3>;
     const size_t smem = ens_smem(kEnsHourBlock);
     static unsigned long long fitted = 0;
     cudaError_t err = fit_smem_once(fitted, k, kEnsHourBlock, smem, smem);
@@ -295,10 +303,10 @@ cudaError_t launch_ensemble_hours(const EnsArgs& e, const DevParams<float>& P, i
 }
 
 // Resident blocks of `block` threads per SM for the persistent kernel.
-template <int NT, bool SU, bool SL, bool DAILY = false>
+template <int NT, bool SU, bool SL, bool DAILY = false, bool X3 = false>
 int ensemble_occupancy(int block) {
     int n = 0;
-    auto k = ensemble_kernel<NT, SU, SL, DAILY>;
+    auto k = ensemble_kernel<NT, SU, SL, DAILY, X3>;
     if (fit_smem(k, block, ens_smem(block, DAILY), ens_smem(256, DAILY)) != cudaSuccess) return 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, block, ens_smem(block, DAILY)) != cudaSuccess) return 0;
     return n;

@@ -23,12 +23,25 @@ IBIS_ENS_VARIANTS(IBIS_ENS_EXTERN, 6)
 IBIS_ENS_VARIANTS(IBIS_ENS_DAILY_EXTERN, 9)
 IBIS_ENS_VARIANTS(IBIS_ENS_DAILY_EXTERN, 6)
 #undef IBIS_ENS_DAILY_EXTERN
+#define IBIS_ENS_X3_EXTERN(NT, SU, SL)                                                                       \
+    extern template cudaError_t launch_ensemble<NT, SU, SL, false, true>(const EnsArgs&, const DevParams<float>&, \
+                                                                         int, int, cudaStream_t);               \
+    extern template int ensemble_occupancy<NT, SU, SL, false, true>(int);                                       \
+    extern template cudaError_t launch_ensemble<NT, SU, SL, true, true>(const EnsArgs&, const DevParams<float>&,  \
+                                                                        int, int, cudaStream_t);                \
+    extern template int ensemble_occupancy<NT, SU, SL, true, true>(int);                                        \
+    extern template cudaError_t launch_ensemble_hours<NT, SU, SL, true>(const EnsArgs&, const DevParams<float>&,  \
+                                                                        int*, int, cudaStream_t);
+IBIS_ENS_VARIANTS(IBIS_ENS_X3_EXTERN, 9)
+IBIS_ENS_VARIANTS(IBIS_ENS_X3_EXTERN, 6)
+#undef IBIS_ENS_X3_EXTERN
 
 namespace {
 
 constexpr unsigned kEnsFlags = IBIS_FLAG_BEDROCK | IBIS_FLAG_H2O_CONSISTENT | IBIS_FLAG_SUNSHADE_U |
                                IBIS_FLAG_SUNSHADE_L | IBIS_FLAG_ACC | IBIS_FLAG_CH4 | IBIS_FLAG_SOIL_MEANS |
-                               IBIS_FLAG_KAHAN | IBIS_FLAG_ZWT_OBS | IBIS_FLAG_ETPARTS | IBIS_FLAG_NEEPARTS;
+                               IBIS_FLAG_KAHAN | IBIS_FLAG_ZWT_OBS | IBIS_FLAG_ETPARTS | IBIS_FLAG_NEEPARTS |
+                               IBIS_FLAGS_X3;
 
 // Validate an ensemble description; fills `a`.  Returns 0, or -EINVAL.
 int ens_args(const IbisEnsemble* e, const IbisParams* hp, EnsArgs& a) {
@@ -77,15 +90,18 @@ int launch_error(cudaError_t err, const char* what) {
     return -(int)err - 1000;
 }
 
-// Expands CALL(NT, SU, SL) for the model variant the flags select.
-#define IBIS_BY_VARIANT(flags, CALL)                                                           \
-    (((flags) & IBIS_FLAG_BEDROCK)                                                            \
-         ? (((flags) & IBIS_FLAG_SUNSHADE_U)                                                  \
-                ? (((flags) & IBIS_FLAG_SUNSHADE_L) ? CALL(9, true, true) : CALL(9, true, false))  \
-                : (((flags) & IBIS_FLAG_SUNSHADE_L) ? CALL(9, false, true) : CALL(9, false, false))) \
-         : (((flags) & IBIS_FLAG_SUNSHADE_U)                                                  \
-                ? (((flags) & IBIS_FLAG_SUNSHADE_L) ? CALL(6, true, true) : CALL(6, true, false))  \
-                : (((flags) & IBIS_FLAG_SUNSHADE_L) ? CALL(6, false, true) : CALL(6, false, false))))
+// Expands CALL(NT, SU, SL, X3) for the model variant the flags select: any
+// IBIS_FLAGS_X3 flag selects the kernels with the IBIS 3.0 extensions.
+#define IBIS_BY_CANOPY(flags, CALL, X3)                                                              \
+    (((flags) & IBIS_FLAG_BEDROCK)                                                                  \
+         ? (((flags) & IBIS_FLAG_SUNSHADE_U)                                                        \
+                ? (((flags) & IBIS_FLAG_SUNSHADE_L) ? CALL(9, true, true, X3) : CALL(9, true, false, X3))  \
+                : (((flags) & IBIS_FLAG_SUNSHADE_L) ? CALL(9, false, true, X3) : CALL(9, false, false, X3))) \
+         : (((flags) & IBIS_FLAG_SUNSHADE_U)                                                        \
+                ? (((flags) & IBIS_FLAG_SUNSHADE_L) ? CALL(6, true, true, X3) : CALL(6, true, false, X3))  \
+                : (((flags) & IBIS_FLAG_SUNSHADE_L) ? CALL(6, false, true, X3) : CALL(6, false, false, X3))))
+#define IBIS_BY_VARIANT(flags, CALL) \
+    (((flags) & IBIS_FLAGS_X3) ? IBIS_BY_CANOPY(flags, CALL, true) : IBIS_BY_CANOPY(flags, CALL, false))
 
 }  // namespace
 }  // namespace ibis
@@ -94,7 +110,7 @@ using namespace ibis;
 
 extern "C" int ibis_ensemble_occupancy(const IbisParams* params, int block) {
     if (!params || block < 32 || block > 256 || block % 32) return 0;
-#define IBIS_OCC(NT, SU, SL) ensemble_occupancy<NT, SU, SL>(block)
+#define IBIS_OCC(NT, SU, SL, X3) ensemble_occupancy<NT, SU, SL, false, X3>(block)
     return IBIS_BY_VARIANT(params->flags, IBIS_OCC);
 #undef IBIS_OCC
 }
@@ -117,7 +133,7 @@ int ensemble_launch(const IbisEnsemble* ens, EnsArgs& a, const IbisParams* param
         const int w = (nitem + sms - 1) / sms;          // warps per SM that cover every item in one pass
         block = 32 * (w < 1 ? 1 : (w > 8 ? 8 : w));
     }
-#define IBIS_OCC(NT, SU, SL) ensemble_occupancy<NT, SU, SL, DAILY>(block)
+#define IBIS_OCC(NT, SU, SL, X3) ensemble_occupancy<NT, SU, SL, DAILY, X3>(block)
     const int occ = IBIS_BY_VARIANT(params->flags, IBIS_OCC);
 #undef IBIS_OCC
     if (occ <= 0) return -EINVAL;
@@ -129,7 +145,7 @@ int ensemble_launch(const IbisEnsemble* ens, EnsArgs& a, const IbisParams* param
     cudaStream_t s = (cudaStream_t)stream;
     const int rc = launch_error(cudaMemsetAsync(ens->queue, 0, sizeof(int), s), "ensemble queue reset");
     if (rc) return rc;
-#define IBIS_RUN(NT, SU, SL) launch_ensemble<NT, SU, SL, DAILY>(a, P, block, grid, s)
+#define IBIS_RUN(NT, SU, SL, X3) launch_ensemble<NT, SU, SL, DAILY, X3>(a, P, block, grid, s)
     const cudaError_t err = IBIS_BY_VARIANT(params->flags, IBIS_RUN);
 #undef IBIS_RUN
     return launch_error(err, "ensemble launch");
@@ -180,7 +196,7 @@ extern "C" int ibis_ensemble_hours_f32(const IbisEnsemble* ens, const IbisParams
     if (nhour == 0) return 0;
     const DevParams<float> P = make_dev_params<float>(*params);
     cudaStream_t s = (cudaStream_t)stream;
-#define IBIS_RUN(NT, SU, SL) launch_ensemble_hours<NT, SU, SL>(a, P, hour, nhour, s)
+#define IBIS_RUN(NT, SU, SL, X3) launch_ensemble_hours<NT, SU, SL, X3>(a, P, hour, nhour, s)
     const cudaError_t err = IBIS_BY_VARIANT(params->flags, IBIS_RUN);
 #undef IBIS_RUN
     return launch_error(err, "ensemble hourly launch");

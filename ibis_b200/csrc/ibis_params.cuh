@@ -61,7 +61,6 @@ template <typename R>
 struct UniformQ {
     static constexpr bool x3 = false;
     const DevParams<R>& P;
-    __device__ __forceinline__ R coefm_pft(int p) const { return P.coefm_pft[p]; }
     __device__ __forceinline__ R vmax(int j) const { return P.vmax_pft[j]; }
     __device__ __forceinline__ R coefm(int g) const { return P.coefm[g]; }
     __device__ __forceinline__ R stressfac() const { return P.stressfac; }
@@ -113,5 +112,13 @@ struct RunQ {
     __device__ __forceinline__ R rroot(int) const { return rroot_; }
     __device__ __forceinline__ R keep(int) const { return keep_; }
 };
+
+// One run's parameters in the kernels that carry the IBIS 3.0 extensions (the
+// same record; the extensions' own tables come from the parameter record).
+template <typename R>
+struct RunQ3 : RunQ<R> {
+    static constexpr bool x3 = true;
+};
+static_assert(sizeof(RunQ3<float>) == sizeof(RunQ<float>), "the run record's shared-memory size is one");
 
 }  // namespace ibis

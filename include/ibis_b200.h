@@ -129,7 +129,10 @@ typedef struct IbisEnsemble {
  * launch: grid = SMs x resident blocks of `block` threads (a multiple of 32,
  * <= 256; 0 picks one from the run count), each warp drawing 32 runs at a time
  * from the work counter.  params->flags selects the model variants and the
- * accumulators as for ibis_step_f32 (no diagnostics). */
+ * accumulators as for ibis_step_f32 (no diagnostics), the IBIS_FLAGS_X3
+ * switches included: a run's vector replaces the parameters it carries, and
+ * the switches' own tables (coefm_pft, the acclimation tables, crop scales)
+ * come from params. */
 int ibis_ensemble_f32(const IbisEnsemble* ens, const IbisParams* params, int block, void* stream);
 
 /* The same runs advanced `nhour` hours in nhour launches (one per hour), from

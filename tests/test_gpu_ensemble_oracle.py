@@ -10,7 +10,9 @@ paths are checked against it:
   kernel -- the oracle gets the hours ``ibis_diurnal_f32`` generates from the
   same days with the same variates;
 * one request answered by the serving loop (3 sites, 2 model years of 48
-  hours): its per-year sums against the oracle's sums over each year.
+  hours): its per-year sums against the oracle's sums over each year;
+* both ensemble forms under the release parameter file's switches (the kernels
+  with the IBIS 3.0 extensions), the oracle under the same switches.
 
 Tolerances (FP32 kernels against float64 after 48 hours): temperatures within
 ``T_ABS`` K, soil water within ``W_ABS``, and the day-loop sums within
@@ -84,9 +86,22 @@ def _errors(got_prog, got_acc, want_prog, want_acc):
     return e
 
 
-def _ensemble_vs_oracle(daily):
+def release_params():
+    """The release parameter file's step parameters (tests/golden/release.npz)
+    for an ensemble: its switches and tables, the run accumulators on."""
+    from goldens import Case
+    from ibis_b200 import params as prm
+    P = Case("release").params.copy()
+    P.flags |= prm.FLAG_ACC | prm.FLAG_CH4 | prm.FLAG_KAHAN
+    return P
+
+
+def _ensemble_vs_oracle(daily, params=None):
     nsite, nparam, hours = 8, 4, 48
-    spec = E.make_ensemble(nsite, nparam, site_hours=np.full(nsite, hours), seed=23, daily=daily)
+    spec = E.make_ensemble(nsite, nparam, site_hours=np.full(nsite, hours), seed=23, daily=daily, params=params)
+    if params is not None:
+        # per-site acclimation states for the release file's temperature acclimation
+        spec.stat["acclim_x"] = np.random.default_rng(5).uniform(-12.0, 28.0, nsite)
     ens = E.Ensemble(spec, year_steps=24)
     ens.run()
     torch.cuda.synchronize()
@@ -154,6 +169,34 @@ def test_ensemble_runs_match_oracle(cuda_lib):
 def test_daily_form_ensemble_runs_match_oracle(cuda_lib):
     e = _ensemble_vs_oracle(True)
     assert e["temp"] < T_ABS and e["water"] < W_ABS and e["acc"] < ACC_REL, e
+
+
+def test_release_ensemble_runs_match_oracle(cuda_lib):
+    """Runs under the release parameter file's switches (the ensemble kernels
+    with the IBIS 3.0 extensions) against the oracle under the same switches,
+    hourly records and the daily form."""
+    for daily in (False, True):
+        e = _ensemble_vs_oracle(daily, params=release_params())
+        assert e["temp"] < T_ABS and e["water"] < W_ABS and e["acc"] < ACC_REL, (daily, e)
+
+
+def test_release_switches_change_ensemble_runs(cuda_lib):
+    """The same runs without the switches give other conductances, so the
+    extended ensemble kernels are not running the F77 step."""
+    from ibis_b200.params import X3_FLAGS
+    out = []
+    for strip in (False, True):
+        P = release_params()
+        if strip:
+            P.flags &= ~X3_FLAGS
+        spec = E.make_ensemble(4, 2, site_hours=np.full(4, 24), seed=3, params=P)
+        spec.stat["acclim_x"] = np.full(4, 5.0)
+        ens = E.Ensemble(spec, year_steps=24)
+        ens.run()
+        torch.cuda.synchronize()
+        out.append(ens.prog_host())
+    d = np.abs(np.asarray(out[0]["gs_upper"]) - np.asarray(out[1]["gs_upper"]))
+    assert float(np.max(d)) > 1e-6
 
 
 def test_served_request_matches_oracle(cuda_lib):
