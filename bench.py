@@ -436,7 +436,13 @@ def run_ours(args):
     h_prog = torch.empty_like(cols.prog, device="cpu").pin_memory()
 
     def e2e_day():
-        # the public host-buffer entry: forcing copied in chunks of hours on a
+        # the public host-buffer entry (ibis_step_host_f32): the columns in
+        # groups, each group's forcing copied in, stepped and its state copied
+        # out on the library's streams, overlapping the other groups' hours
+        cols.run_host(h_forc, P, host_prog=h_prog, group=args.e2e_group, stream=stream)
+
+    def e2e_hour_chunks():
+        # the same through run_from_host: forcing copied in chunks of hours on a
         # second stream, overlapping the computation of the previous chunk
         cols.run_from_host(h_forc, P, chunk=args.e2e_chunk if args.e2e_chunk == "auto" else int(args.e2e_chunk),
                            stream=stream)
@@ -444,6 +450,8 @@ def run_ours(args):
 
     e2e_day()
     ms_e2e = float(np.sum(timed(e2e_day, args.steps))) / args.steps
+    e2e_hour_chunks()
+    ms_e2e_chunks = float(np.sum(timed(e2e_hour_chunks, args.steps))) / args.steps
 
     # end to end from daily weather: 32 B per cell-day in, the hourly forcing
     # generated on the GPU (ibis_diurnal_f32, the reference's diurnal algorithm)
@@ -482,8 +490,8 @@ def run_ours(args):
         extras["serve"] = serve_bounded()
         extras["single_cell"] = single_cell(dev, stream)
     if world > 1:
-        ms_step, ms_plain, ms_e2e, ms_e2e_daily = replicas.max_over_ranks(W, [ms_step, ms_plain, ms_e2e,
-                                                                              ms_e2e_daily], device=dev)
+        ms_step, ms_plain, ms_e2e, ms_e2e_daily, ms_e2e_chunks = replicas.max_over_ranks(
+            W, [ms_step, ms_plain, ms_e2e, ms_e2e_daily, ms_e2e_chunks], device=dev)
     cell_steps = world * args.ncell * HOURS
     value = cell_steps / (ms_step / 1e3)
     peak, peak_kind = _peaks()
@@ -530,10 +538,14 @@ def run_ours(args):
             "per_step_launch": {"value": cell_steps / (ms_plain / 1e3), "ms_per_step": ms_plain,
                                 "launches_per_step": HOURS, "launch_config": "fused, block 128, 2 blocks/SM",
                                 "achieved_gbs": _algorithmic_bytes(1) * args.ncell * HOURS / (ms_plain / 1e3) / 1e9},
-            "e2e": {"value": cell_steps / (ms_e2e / 1e3), "unit": "cell-steps/s",
-                    "chunk_hours": Columns.chunk_schedule(HOURS, args.e2e_chunk if args.e2e_chunk == "auto"
-                                                          else int(args.e2e_chunk)),
+            "e2e": {"value": cell_steps / (ms_e2e / 1e3), "unit": "cell-steps/s", "ms_per_step": ms_e2e,
+                    "entry": "Columns.run_host -> ibis_step_host_f32",
+                    "group_cells": args.e2e_group or "auto (a twentieth of the columns)",
                     "h2d_bytes_per_step": int(h_forc.numel() * 4), "d2h_bytes_per_step": int(h_prog.numel() * 4)},
+            "e2e_hour_chunks": {"value": cell_steps / (ms_e2e_chunks / 1e3), "unit": "cell-steps/s",
+                                "ms_per_step": ms_e2e_chunks, "entry": "Columns.run_from_host + a state read-back",
+                                "chunk_hours": Columns.chunk_schedule(HOURS, args.e2e_chunk if args.e2e_chunk == "auto"
+                                                                      else int(args.e2e_chunk))},
             "e2e_daily_forcing": {"value": cell_steps / (ms_e2e_daily / 1e3), "unit": "cell-steps/s",
                                   "h2d_bytes_per_step": int(h_daily.numel() * 4),
                                   "d2h_bytes_per_step": int(h_prog.numel() * 4),
@@ -925,6 +937,8 @@ def main():
     ap.add_argument("--rate", type=float, default=50.0)
     ap.add_argument("--duration", type=float, default=10.0)
     ap.add_argument("--epoch-hours", type=int, default=168)
+    ap.add_argument("--e2e-group", type=int, default=0,
+                    help="columns per group of the host-buffer entry (a multiple of 32; 0: a twentieth of the columns)")
     ap.add_argument("--e2e-chunk", default="auto",
                     help="hours per host-to-device forcing chunk in the e2e path ('auto': 4 hours, growing by 1.75)")
     ap.add_argument("--gpus", type=int, default=1)

@@ -193,6 +193,47 @@ class Columns:
         _lib.check(rc, "ibis_step")
         return self
 
+    def run_host(self, host_forc: torch.Tensor, params: StepParams, host_prog: torch.Tensor | None = None,
+                 group: int = 0, stream=None):
+        """Advance the columns through ``host_forc`` (a pinned host tensor
+        ``(nstep, IBIS_FORC_COUNT, ld)``) and, with ``host_prog`` (a pinned host
+        tensor shaped like ``prog``), copy the state after the last hour out:
+        ``ibis_step_host_f32``, which cuts the columns into groups of ``group``
+        cells (0: twenty groups) whose copies overlap the other groups' hours.
+        Asynchronous on ``stream``; read ``host_prog`` after synchronising it.
+        FP32 columns only; a two-kernel launch mode runs the library's fused choice."""
+        if self.dtype != torch.float32:
+            raise ValueError("run_host runs FP32 columns")
+        if host_forc.device.type != "cpu" or host_forc.dtype != self.dtype or not host_forc.is_pinned():
+            raise ValueError("host forcing must be a pinned CPU tensor of the Columns' dtype")
+        if host_forc.dim() != 3 or host_forc.shape[1] != L.N_FORC or host_forc.shape[2] != self.ld:
+            raise ValueError(f"host forcing must be (nstep, {L.N_FORC}, {self.ld})")
+        if not host_forc.is_contiguous():
+            raise ValueError("host forcing must be contiguous")
+        if host_prog is not None and (host_prog.device.type != "cpu" or not host_prog.is_pinned()
+                                      or host_prog.shape != self.prog.shape or host_prog.dtype != self.dtype
+                                      or not host_prog.is_contiguous()):
+            raise ValueError("host_prog must be a pinned contiguous CPU tensor shaped like prog")
+        nstep = host_forc.shape[0]
+        if getattr(self, "_host_forc", None) is None or self._host_forc.shape[0] < nstep:
+            self._host_forc = torch.empty((nstep, L.N_FORC, self.ld), dtype=self.dtype, device=self.device)
+        cfg = self.launch_config(nstep)
+        if _lib.configs()[cfg]["form"] != "fused":
+            cfg = -1                       # a two-kernel configuration needs scratch: the library's own choice
+        flags = params.flags & ~FLAG_DIAG if self.diag is None else params.flags | FLAG_DIAG
+        if self.acc is None:
+            flags &= ~_ACC_FLAGS
+        p = params.to_c()
+        p.flags = flags
+        if stream is None:
+            stream = torch.cuda.current_stream(self.device)
+        rc = _lib.load().ibis_step_host_f32(_ptr(self.prog), _ptr(self.stat), _ptr(host_forc),
+                                            _ptr(self._host_forc), _ptr(self.diag), _ptr(self.acc), _ptr(host_prog),
+                                            self.ncell, self.ld, nstep, ctypes.byref(p), _ptr(self.status),
+                                            int(group), int(cfg), ctypes.c_void_p(stream.cuda_stream))
+        _lib.check(rc, "ibis_step_host_f32")
+        return self
+
     @staticmethod
     def chunk_schedule(nstep: int, chunk="auto"):
         """Hours per host-to-device chunk.  An integer gives equal chunks;

@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) hourly_step_kernel(R* __restrict_
     R sum = store_col(c, prog + i, ld);
     if (status && !finite(sum)) {
         atomicOr(status, 1);
-        atomicMin(status + 1, i);
+        atomicMin(status + 1, i + P.cell0);
     }
 }
 
@@ -281,7 +281,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) ground_kernel(R* __restrict__ pro
     R sum = store_col(c, prog + i, ld);
     if (status && !finite(sum)) {
         atomicOr(status, 1);
-        atomicMin(status + 1, i);
+        atomicMin(status + 1, i + P.cell0);
     }
 }
 
@@ -511,7 +511,7 @@ cudaError_t dispatch_config(int cfg, R* prog, const R* stat, const R* forc, R* d
 
 template <typename R>
 static int hourly_step(R* prog, const R* stat, const R* forc, R* diag, R* acc, int ncell, int ld, int nstep,
-                       const IbisParams* hp, int* status, void* stream, R* mid, int cfg) {
+                       const IbisParams* hp, int* status, void* stream, R* mid, int cfg, int cell0 = 0) {
     if (!prog || !stat || !forc || !hp) return -EINVAL;
     if (cfg < 0 || cfg >= kNumConfigs) return -EINVAL;
     if (kConfigs[cfg].form == 1 && (!mid || sizeof(R) != 4)) return -EINVAL;
@@ -525,6 +525,7 @@ static int hourly_step(R* prog, const R* stat, const R* forc, R* diag, R* acc, i
     if ((hp->flags & IBIS_FLAG_DIAG) && !diag) return -EINVAL;
     if (!(hp->dtime > 0.0)) return -EINVAL;
     DevParams<R> P = make_dev_params<R>(*hp);
+    P.cell0 = cell0;
     if (!(hp->flags & IBIS_FLAG_DIAG)) diag = nullptr;
     if (!(hp->flags & (IBIS_FLAG_ACC | IBIS_FLAG_CH4 | IBIS_FLAG_SOIL_MEANS))) acc = nullptr;
     const long long fstride = (long long)IBIS_FORC_COUNT * ld;

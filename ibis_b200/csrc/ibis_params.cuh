@@ -44,6 +44,9 @@ struct DevParams {
     // (PFT 10) and C3 (PFT 11) vmax scales less one, formed in float32 as the
     // reference forms them on float32 masks; zero for the other PFTs
     R crop_inc[12];
+    // index of the launch's first column in the caller's numbering: a launch
+    // over a group of columns (ibis_step_host_f32) reports status[1] in it
+    int cell0;
 };
 
 // The parameters a calibration ensemble varies per run (the 31-parameter

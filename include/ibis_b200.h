@@ -84,6 +84,30 @@ int ibis_config_info(int config, int* form, int* block, int* min_blocks, int* bl
 int ibis_step_split_noalloc_f32(float* prog, const float* stat, const float* forc, float* diag, float* acc,
                                 int ncell, int ld, int nstep, const IbisParams* params, int* status, void* stream);
 
+/* ibis_step_f32 with the forcing in HOST memory and the prognostic state read
+ * back to HOST memory, for callers whose inputs start and end on the host (the
+ * reference's timestep_body called on NumPy state, a day loop fed from files).
+ * The columns are cut into groups of `group` cells (a multiple of 32; 0 = a
+ * twentieth of ncell, rounded up to 32; raised so there are at most 64 groups);
+ * each group's forcing is copied in, stepped and copied out on streams of the
+ * library's own, so the copies of one group overlap the steps of the others.
+ *   host_forc  [nstep][IBIS_FORC_COUNT][ld]  pinned HOST: hourly forcing
+ *   forc       [nstep][IBIS_FORC_COUNT][ld]  DEVICE: where the forcing lands
+ *   host_prog  [IBIS_PROG_COUNT][ld] pinned HOST, or NULL: the state after the
+ *              last hour (device prog is updated either way)
+ *   config     -1 (ibis_step_f32's choice) or a fused launch configuration
+ *   other arguments as for ibis_step_f32; status[1] counts cells from 0 over
+ *   all groups.
+ * Everything queued on `stream` before the call runs first, and work queued on
+ * it afterwards (a read of host_prog after a stream synchronise) runs after
+ * every group's hours and copies.  Calls from several host threads are
+ * serialised by the library (they share its streams).
+ * Replaces: timestep_body (loops.py:234) iterated by _step_body (loops_gswp3.py:115)
+ * on host arrays. */
+int ibis_step_host_f32(float* prog, const float* stat, const float* host_forc, float* forc, float* diag, float* acc,
+                       float* host_prog, int ncell, int ld, int nstep, const IbisParams* params, int* status,
+                       int group, int config, void* stream);
+
 /* A calibration ensemble: nrun runs, each one parameter vector at one site
  * over its own record of hourly forcing.  Per-run buffers use ld_run, per-site
  * buffers ld_site (both multiples of 32, >= the count).

@@ -36,6 +36,21 @@ def test_step_rejects_bad_shapes(so):
     assert so.ibis_step_f32(DEV, DEV, DEV, NUL, DEV, 30, 32, 1, ctypes.byref(bad), NUL, NUL) == EINVAL
 
 
+def test_host_step_rejects_bad_arguments(so):
+    p = _p()
+    args = (DEV, DEV, DEV, DEV, NUL, DEV, NUL)
+    assert so.ibis_step_host_f32(*args, 30, 33, 1, p, NUL, 0, -1, NUL) == EINVAL      # ld not a multiple of 32
+    assert so.ibis_step_host_f32(*args, 40, 32, 1, p, NUL, 0, -1, NUL) == EINVAL      # ncell > ld
+    assert so.ibis_step_host_f32(*args, 30, 32, 1, p, NUL, 48, -1, NUL) == EINVAL     # group not a multiple of 32
+    assert so.ibis_step_host_f32(*args, 30, 32, 1, p, NUL, -32, -1, NUL) == EINVAL
+    split = next(c["id"] for c in lib.configs() if c["form"] == "split")
+    assert so.ibis_step_host_f32(*args, 30, 32, 1, p, NUL, 0, split, NUL) == EINVAL   # needs scratch
+    assert so.ibis_step_host_f32(*args, 30, 32, 1, p, NUL, 0, 99, NUL) == EINVAL
+    assert so.ibis_step_host_f32(DEV, DEV, NUL, DEV, NUL, DEV, NUL, 30, 32, 1, p, NUL, 0, -1, NUL) == EINVAL
+    assert so.ibis_step_host_f32(DEV, DEV, DEV, NUL, NUL, DEV, NUL, 30, 32, 1, p, NUL, 0, -1, NUL) == EINVAL
+    assert so.ibis_step_host_f32(*args, 0, 32, 1, p, NUL, 0, -1, NUL) == 0             # nothing to do
+
+
 def test_day_kernels_reject_bad_arguments(so):
     p, dp = _p(), ctypes.byref(DayParams().to_c())
     for f in (so.ibis_day_begin_f32, so.ibis_day_begin_f64):

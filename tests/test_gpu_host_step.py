@@ -1,0 +1,68 @@
+"""The step from host buffers (``ibis_step_host_f32`` through
+``Columns.run_host``): the columns cut into groups, each group's forcing copied
+in, stepped and copied out on the library's streams.
+
+The groups run the same kernels on the same columns as one launch over every
+column, so the state, the accumulators and the state copied to the host equal
+that launch's bit for bit, whatever the group size (several groups per compute
+stream included).  A column made non-finite in a late group is reported in the
+caller's numbering of the columns.  Every loop of the step has a fixed trip
+count and its two float-to-int conversions read static soil inputs, so a NaN
+in the forcing stays data: it propagates into that column and is flagged.
+"""
+import numpy as np
+import pytest
+import torch
+
+from ibis_b200 import synth
+from ibis_b200.columns import Columns
+from ibis_b200.params import StepParams, FLAG_ACC, FLAG_CH4, FLAG_KAHAN
+
+pytestmark = pytest.mark.gpu
+
+NCELL, HOURS = 5000, 6
+
+
+def _workload(seed=3):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    stat = synth.make_columns(rng, NCELL)
+    forc = synth.make_forcing(rng, rng.uniform(-40.0, 70.0, NCELL), HOURS, start_doy=172)
+    prog = synth.make_initial(rng, stat, {k: v[0] for k, v in forc.items()})
+    P = StepParams(co2conc=390.0e-6)
+    P.flags |= FLAG_ACC | FLAG_CH4 | FLAG_KAHAN
+    return prog, stat, forc, P
+
+
+def _columns(prog, stat):
+    return Columns.from_host(prog, stat, dtype=torch.float32, acc=True)
+
+
+@pytest.mark.parametrize("group", [0, 256, 640, 4992])
+def test_host_groups_equal_one_launch(cuda_lib, group):
+    prog, stat, forc, P = _workload()
+    ref = _columns(prog, stat)
+    ref.run(ref.forcing(forc), P)
+    cols = _columns(prog, stat)
+    h_forc = torch.from_numpy(synth.forcing_planes(forc, cols.ld)).pin_memory()
+    h_prog = torch.zeros_like(cols.prog, device="cpu").pin_memory()
+    stream = torch.cuda.Stream()
+    cols.run_host(h_forc, P, host_prog=h_prog, group=group, stream=stream)
+    stream.synchronize()
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(cols.prog.cpu().numpy(), ref.prog.cpu().numpy())
+    np.testing.assert_array_equal(cols.acc.cpu().numpy(), ref.acc.cpu().numpy())
+    np.testing.assert_array_equal(h_prog.numpy()[:, :NCELL], ref.prog.cpu().numpy()[:, :NCELL])
+    assert not cols.nonfinite()[0]
+
+
+def test_host_step_reports_cells_in_caller_numbering(cuda_lib):
+    prog, stat, forc, P = _workload()
+    bad = 3301                                         # in the sixth group of 640 cells
+    forc = {k: v.copy() for k, v in forc.items()}
+    forc["ta"][2, bad] = np.nan
+    cols = _columns(prog, stat)
+    h_forc = torch.from_numpy(synth.forcing_planes(forc, cols.ld)).pin_memory()
+    cols.run_host(h_forc, P, group=640)
+    torch.cuda.synchronize()
+    flagged, first = cols.nonfinite()
+    assert flagged and first == bad
