@@ -175,36 +175,46 @@ extern "C" int ibis_step_host_f32(float* prog, const float* stat, const float* h
     cudaStream_t user = (cudaStream_t)stream;
     // everything queued on the caller's stream before this call comes first
     if ((e = cudaEventRecord(h.start, user)) != cudaSuccess) return host_error(e, "event record");
-    cudaStreamWaitEvent(h.h2d, h.start, 0);
-    cudaStreamWaitEvent(h.d2h, h.start, 0);
-    for (int k = 0; k < kHostStreams && k < ngroup; ++k) cudaStreamWaitEvent(h.comp[k], h.start, 0);
+    e = cudaStreamWaitEvent(h.h2d, h.start, 0);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(h.d2h, h.start, 0);
+    for (int k = 0; k < kHostStreams && k < ngroup && e == cudaSuccess; ++k)
+        e = cudaStreamWaitEvent(h.comp[k], h.start, 0);
+    if (e != cudaSuccess) return host_error(e, "stream wait");
     const size_t pitch = (size_t)ld * sizeof(float);
-    for (int g = 0; g < ngroup; ++g) {
+    int rc = 0, queued = 0;                         // groups whose work is on the library's streams
+    const char* what = nullptr;
+    for (int g = 0; g < ngroup && !rc; ++g) {
         const int c0 = g * group, n = ncell - c0 < group ? ncell - c0 : group;
         const size_t width = (size_t)n * sizeof(float);
-        if (nstep > 0) {
-            e = cudaMemcpy2DAsync(forc + c0, pitch, host_forc + c0, pitch, width, (size_t)nstep * IBIS_FORC_COUNT,
-                                  cudaMemcpyHostToDevice, h.h2d);
-            if (e != cudaSuccess) return host_error(e, "forcing copy");
-        }
-        if ((e = cudaEventRecord(h.landed[g], h.h2d)) != cudaSuccess) return host_error(e, "event record");
         cudaStream_t cs = h.comp[g % kHostStreams];
-        cudaStreamWaitEvent(cs, h.landed[g], 0);
-        const int rc = ibis::hourly_step<float>(prog + c0, stat + c0, forc + c0, diag ? diag + c0 : nullptr,
-                                                acc ? acc + c0 : nullptr, n, ld, nstep, params, status, cs, nullptr,
-                                                cfg, c0);
-        if (rc) return rc;
-        if ((e = cudaEventRecord(h.stepped[g], cs)) != cudaSuccess) return host_error(e, "event record");
-        if (host_prog) {
-            cudaStreamWaitEvent(h.d2h, h.stepped[g], 0);
-            e = cudaMemcpy2DAsync(host_prog + c0, pitch, prog + c0, pitch, width, IBIS_PROG_COUNT,
-                                  cudaMemcpyDeviceToHost, h.d2h);
-            if (e != cudaSuccess) return host_error(e, "state copy");
+        e = nstep > 0 ? cudaMemcpy2DAsync(forc + c0, pitch, host_forc + c0, pitch, width,
+                                          (size_t)nstep * IBIS_FORC_COUNT, cudaMemcpyHostToDevice, h.h2d)
+                      : cudaSuccess;
+        if (e == cudaSuccess) e = cudaEventRecord(h.landed[g], h.h2d);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(cs, h.landed[g], 0);
+        if (e != cudaSuccess) { what = "forcing copy"; break; }
+        rc = ibis::hourly_step<float>(prog + c0, stat + c0, forc + c0, diag ? diag + c0 : nullptr,
+                                      acc ? acc + c0 : nullptr, n, ld, nstep, params, status, cs, nullptr, cfg, c0);
+        e = cudaEventRecord(h.stepped[g], cs);
+        if (e != cudaSuccess) { what = "event record"; break; }
+        ++queued;
+        if (host_prog && !rc) {
+            e = cudaStreamWaitEvent(h.d2h, h.stepped[g], 0);
+            if (e == cudaSuccess)
+                e = cudaMemcpy2DAsync(host_prog + c0, pitch, prog + c0, pitch, width, IBIS_PROG_COUNT,
+                                      cudaMemcpyDeviceToHost, h.d2h);
+            if (e != cudaSuccess) { what = "state copy"; break; }
         }
     }
-    // the caller's stream continues after every group's hours and copies
-    for (int g = 0; g < ngroup; ++g) cudaStreamWaitEvent(user, h.stepped[g], 0);
-    if ((e = cudaEventRecord(h.out_done, h.d2h)) != cudaSuccess) return host_error(e, "event record");
-    if ((e = cudaStreamWaitEvent(user, h.out_done, 0)) != cudaSuccess) return host_error(e, "stream wait");
+    // the caller's stream continues after every queued group's hours and copies,
+    // on failure too, so that nothing of this call is still running when the
+    // caller's stream reaches its next work
+    cudaError_t j = cudaSuccess;
+    for (int g = 0; g < queued && j == cudaSuccess; ++g) j = cudaStreamWaitEvent(user, h.stepped[g], 0);
+    if (j == cudaSuccess) j = cudaEventRecord(h.out_done, h.d2h);
+    if (j == cudaSuccess) j = cudaStreamWaitEvent(user, h.out_done, 0);
+    if (what) return host_error(e, what);
+    if (rc) return rc;
+    if (j != cudaSuccess) return host_error(j, "stream join");
     return 0;
 }
