@@ -194,14 +194,16 @@ class Columns:
         return self
 
     def run_host(self, host_forc: torch.Tensor, params: StepParams, host_prog: torch.Tensor | None = None,
-                 group: int = 0, stream=None):
+                 group: int = 0, chunk: int = 0, stream=None):
         """Advance the columns through ``host_forc`` (a pinned host tensor
         ``(nstep, IBIS_FORC_COUNT, ld)``) and, with ``host_prog`` (a pinned host
         tensor shaped like ``prog``), copy the state after the last hour out:
-        ``ibis_step_host_f32``, which cuts the columns into groups of ``group``
-        cells (0: twenty groups) whose copies overlap the other groups' hours.
-        Asynchronous on ``stream``; read ``host_prog`` after synchronising it.
-        FP32 columns only; a two-kernel launch mode runs the library's fused choice."""
+        ``ibis_step_host_f32``, which overlaps the copies with the steps -- in
+        groups of ``group`` columns for batches of several waves (0: twenty
+        groups), or, for smaller ones, in chunks of ``chunk`` hours (0: 4 hours
+        growing by 1.75).  Asynchronous on ``stream``; read ``host_prog`` after
+        synchronising it.  FP32 columns only; a two-kernel launch mode runs the
+        library's fused choice."""
         if self.dtype != torch.float32:
             raise ValueError("run_host runs FP32 columns")
         if host_forc.device.type != "cpu" or host_forc.dtype != self.dtype or not host_forc.is_pinned():
@@ -230,7 +232,8 @@ class Columns:
         rc = _lib.load().ibis_step_host_f32(_ptr(self.prog), _ptr(self.stat), _ptr(host_forc),
                                             _ptr(self._host_forc), _ptr(self.diag), _ptr(self.acc), _ptr(host_prog),
                                             self.ncell, self.ld, nstep, ctypes.byref(p), _ptr(self.status),
-                                            int(group), int(cfg), ctypes.c_void_p(stream.cuda_stream))
+                                            int(group), int(chunk), int(cfg),
+                                            ctypes.c_void_p(stream.cuda_stream))
         _lib.check(rc, "ibis_step_host_f32")
         return self
 

@@ -108,25 +108,34 @@ extern "C" int ibis_step_split_noalloc_f32(float* prog, const float* stat, const
 }
 
 // ---------------------------------------------------------------------------
-// The step from host buffers.  The columns are cut into groups; each group's
-// forcing is copied in on one copy stream, its hours run on one of a few
-// compute streams, and its state is copied out on a second copy stream, so the
-// copies of one group overlap the steps of the others and the groups' kernels
-// fill the SMs together (no group waits for another group's slowest column).
+// The step from host buffers.  A batch of several waves is cut into groups of
+// columns: each group's forcing is copied in on one copy stream, its hours run
+// on one of a few compute streams, and its state is copied out on a second
+// copy stream, so the copies of one group overlap the steps of the others and
+// the groups' kernels fill the SMs together (no group waits for another
+// group's slowest column).  A batch of about a wave or less has no later
+// waves to hide copies behind: its hours are cut into chunks instead, the
+// copy of each chunk overlapping the steps of the chunk before.
 // ---------------------------------------------------------------------------
 namespace {
 constexpr int kHostStreams = 16;    // compute streams the groups take in turn
 constexpr int kHostMaxGroups = 64;
+constexpr int kHostMaxPieces = 256; // (group, chunk of hours) pairs of one call
 // groups when the caller leaves the size to the library: at 95,333 cells x 24
 // hours a day from host to host took 3.86 ms in 20 groups, 3.94 ms in 16 and
 // 4.2 ms in 8 (the same day with its forcing already on the device: 3.66 ms)
 constexpr int kHostAutoGroups = 20;
+// batches of more than this many waves of the launch configuration are cut
+// into groups, smaller ones into chunks of hours.  A day from host to host,
+// groups / chunks: 1 wave (33,152 cells) 2.30 / 1.71 ms; 1.25 waves 2.37 /
+// 2.68 ms; 1.5 waves 2.54 / 2.77 ms; 2 waves 2.88 / 3.00 ms.
+constexpr double kHostGroupWaves = 1.15;
 
 struct HostPipe {
     bool ready = false;
     cudaStream_t h2d = nullptr, d2h = nullptr, comp[kHostStreams] = {};
     cudaEvent_t start = nullptr, out_done = nullptr;
-    cudaEvent_t landed[kHostMaxGroups] = {}, stepped[kHostMaxGroups] = {};
+    cudaEvent_t landed[kHostMaxPieces] = {}, stepped[kHostMaxGroups] = {};
 };
 std::mutex g_host_mu;
 HostPipe g_host[kMaxDevices];
@@ -139,10 +148,10 @@ cudaError_t host_pipe_init(HostPipe& h) {
         e = cudaStreamCreateWithFlags(&h.comp[k], cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h.start, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h.out_done, cudaEventDisableTiming);
-    for (int g = 0; g < kHostMaxGroups && e == cudaSuccess; ++g) {
+    for (int g = 0; g < kHostMaxPieces && e == cudaSuccess; ++g)
         e = cudaEventCreateWithFlags(&h.landed[g], cudaEventDisableTiming);
-        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h.stepped[g], cudaEventDisableTiming);
-    }
+    for (int g = 0; g < kHostMaxGroups && e == cudaSuccess; ++g)
+        e = cudaEventCreateWithFlags(&h.stepped[g], cudaEventDisableTiming);
     h.ready = e == cudaSuccess;
     return e;
 }
@@ -151,23 +160,65 @@ int host_error(cudaError_t e, const char* what) {
     fprintf(stderr, "ibis_step_host_f32: %s failed: %s\n", what, cudaGetErrorString(e));
     return -(int)e - 1000;
 }
+
+// Hours of each chunk: `chunk` hours each; or, with chunk 0, one chunk of every
+// hour when `whole`, else 4 hours growing by 1.75 per chunk, the last taking a
+// remainder under half its size (a copy of each chunk then stays within the
+// steps of the chunk before, and few launches keep their tails few).
+int chunk_schedule(int nstep, int chunk, bool whole, int* out, int cap) {
+    int n = 0, h = 0;
+    double c = 4.0;
+    while (h < nstep) {
+        int m;
+        if (chunk > 0) m = chunk;
+        else if (whole) m = nstep;
+        else {
+            m = (int)c;
+            const int rem = nstep - h;
+            if (m > rem || rem - m < m / 2.0) m = rem;
+            c *= 1.75;
+        }
+        if (m > nstep - h) m = nstep - h;
+        if (n == cap) return -1;
+        out[n++] = m;
+        h += m;
+    }
+    return n;
+}
 }  // namespace
 
 extern "C" int ibis_step_host_f32(float* prog, const float* stat, const float* host_forc, float* forc, float* diag,
                                   float* acc, float* host_prog, int ncell, int ld, int nstep,
-                                  const IbisParams* params, int* status, int group, int config, void* stream) {
+                                  const IbisParams* params, int* status, int group, int chunk, int config,
+                                  void* stream) {
     if (!prog || !stat || !host_forc || !forc || !params) return -EINVAL;
-    if (ncell < 0 || nstep < 0 || ld < ncell || ld % 32 || group < 0 || group % 32) return -EINVAL;
+    if (ncell < 0 || nstep < 0 || ld < ncell || ld % 32 || group < 0 || group % 32 || chunk < 0) return -EINVAL;
     if (config < -1 || config >= ibis::kNumConfigs || (config >= 0 && ibis::kConfigs[config].form != 0))
         return -EINVAL;
     if (ncell == 0) return 0;
     const int cfg = config >= 0 ? config : (nstep >= ibis::kAccSmemMinSteps ? ibis::kLongFused : ibis::kDefaultFused);
-    if (group == 0) group = ((ncell + kHostAutoGroups - 1) / kHostAutoGroups + 31) / 32 * 32;
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return -ENODEV;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) return -ENODEV;
+    if (group == 0) {
+        // whole blocks per group: a partial block in every group would add
+        // blocks to the batch, and a batch of whole waves would spill into one more
+        const int block = ibis::kConfigs[cfg].block;
+        const double wave = (double)sms * block * ibis::kConfigs[cfg].minb;
+        group = ncell > kHostGroupWaves * wave
+                    ? ((ncell + kHostAutoGroups - 1) / kHostAutoGroups + block - 1) / block * block
+                    : (ncell + 31) / 32 * 32;
+    }
     const int min_group = ((ncell + kHostMaxGroups - 1) / kHostMaxGroups + 31) / 32 * 32;
     if (group < min_group) group = min_group;
     const int ngroup = (ncell + group - 1) / group;
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return -ENODEV;
+    int sched[kHostMaxPieces];
+    const int nchunk = chunk_schedule(nstep, chunk, ngroup > 1, sched, kHostMaxPieces);
+    if (nchunk < 0 || (long long)ngroup * nchunk > kHostMaxPieces) {
+        fprintf(stderr, "ibis_step_host_f32: %d groups x %d chunks exceed %d pieces\n", ngroup, nchunk,
+                kHostMaxPieces);
+        return -EINVAL;
+    }
     std::lock_guard<std::mutex> lock(g_host_mu);   // one caller at a time uses the device's streams and events
     HostPipe& h = g_host[dev];
     cudaError_t e = host_pipe_init(h);
@@ -181,24 +232,30 @@ extern "C" int ibis_step_host_f32(float* prog, const float* stat, const float* h
         e = cudaStreamWaitEvent(h.comp[k], h.start, 0);
     if (e != cudaSuccess) return host_error(e, "stream wait");
     const size_t pitch = (size_t)ld * sizeof(float);
+    const size_t fstride = (size_t)IBIS_FORC_COUNT * ld;
     int rc = 0, queued = 0;                         // groups whose work is on the library's streams
     const char* what = nullptr;
-    for (int g = 0; g < ngroup && !rc; ++g) {
+    for (int g = 0; g < ngroup && !rc && !what; ++g) {
         const int c0 = g * group, n = ncell - c0 < group ? ncell - c0 : group;
         const size_t width = (size_t)n * sizeof(float);
         cudaStream_t cs = h.comp[g % kHostStreams];
-        e = nstep > 0 ? cudaMemcpy2DAsync(forc + c0, pitch, host_forc + c0, pitch, width,
-                                          (size_t)nstep * IBIS_FORC_COUNT, cudaMemcpyHostToDevice, h.h2d)
-                      : cudaSuccess;
-        if (e == cudaSuccess) e = cudaEventRecord(h.landed[g], h.h2d);
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(cs, h.landed[g], 0);
-        if (e != cudaSuccess) { what = "forcing copy"; break; }
-        rc = ibis::hourly_step<float>(prog + c0, stat + c0, forc + c0, diag ? diag + c0 : nullptr,
-                                      acc ? acc + c0 : nullptr, n, ld, nstep, params, status, cs, nullptr, cfg, c0);
-        e = cudaEventRecord(h.stepped[g], cs);
-        if (e != cudaSuccess) { what = "event record"; break; }
-        ++queued;
-        if (host_prog && !rc) {
+        for (int k = 0, h0 = 0; k < nchunk && !rc; h0 += sched[k], ++k) {
+            const int m = sched[k];
+            cudaEvent_t landed = h.landed[g * nchunk + k];
+            e = cudaMemcpy2DAsync(forc + h0 * fstride + c0, pitch, host_forc + h0 * fstride + c0, pitch, width,
+                                  (size_t)m * IBIS_FORC_COUNT, cudaMemcpyHostToDevice, h.h2d);
+            if (e == cudaSuccess) e = cudaEventRecord(landed, h.h2d);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(cs, landed, 0);
+            if (e != cudaSuccess) { what = "forcing copy"; break; }
+            rc = ibis::hourly_step<float>(prog + c0, stat + c0, forc + h0 * fstride + c0, diag ? diag + c0 : nullptr,
+                                          acc ? acc + c0 : nullptr, n, ld, m, params, status, cs, nullptr, cfg, c0);
+        }
+        // the group's stream position, recorded on failure too so the join below covers it
+        const cudaError_t r = cudaEventRecord(h.stepped[g], cs);
+        if (r == cudaSuccess) ++queued;
+        else if (!what) { what = "event record"; e = r; }
+        if (what || rc) break;
+        if (host_prog) {
             e = cudaStreamWaitEvent(h.d2h, h.stepped[g], 0);
             if (e == cudaSuccess)
                 e = cudaMemcpy2DAsync(host_prog + c0, pitch, prog + c0, pitch, width, IBIS_PROG_COUNT,

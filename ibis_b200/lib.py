@@ -55,7 +55,7 @@ SIGNATURES = {
     "ibis_step_split_noalloc_f32": (ctypes.c_int, [ctypes.c_void_p] * 5 + [ctypes.c_int] * 3
                                     + [_P, ctypes.c_void_p, ctypes.c_void_p]),
     "ibis_config_info": (ctypes.c_int, [ctypes.c_int] + [_c_int_p] * 5),
-    "ibis_step_host_f32": (ctypes.c_int, [_V] * 7 + [ctypes.c_int] * 3 + [_P, _V, ctypes.c_int, ctypes.c_int, _V]),
+    "ibis_step_host_f32": (ctypes.c_int, [_V] * 7 + [ctypes.c_int] * 3 + [_P, _V] + [ctypes.c_int] * 3 + [_V]),
     "ibis_ensemble_f32": (ctypes.c_int, [_E, _P, ctypes.c_int, ctypes.c_void_p]),
     "ibis_ensemble_hours_f32": (ctypes.c_int, [_E, _P, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
     "ibis_ensemble_occupancy": (ctypes.c_int, [_P, ctypes.c_int]),

@@ -87,10 +87,17 @@ int ibis_step_split_noalloc_f32(float* prog, const float* stat, const float* for
 /* ibis_step_f32 with the forcing in HOST memory and the prognostic state read
  * back to HOST memory, for callers whose inputs start and end on the host (the
  * reference's timestep_body called on NumPy state, a day loop fed from files).
- * The columns are cut into groups of `group` cells (a multiple of 32; 0 = a
- * twentieth of ncell, rounded up to 32; raised so there are at most 64 groups);
- * each group's forcing is copied in, stepped and copied out on streams of the
- * library's own, so the copies of one group overlap the steps of the others.
+ * The copies overlap the steps on streams of the library's own:
+ *   - a batch of more than 1.15 waves of the launch configuration is cut into
+ *     groups of columns (`group` cells, a multiple of 32; 0 = a twentieth of
+ *     ncell, rounded up to whole blocks of the launch configuration; raised
+ *     so there are at most 64 groups), each
+ *     group's forcing copied in, stepped and its state copied out while other
+ *     groups step;
+ *   - a smaller batch (group 0) is one group whose hours are cut into chunks,
+ *     each chunk's copy overlapping the steps of the chunk before.
+ *   `chunk` sets the hours per chunk (0: all hours for several groups; 4 hours
+ *   growing by 1.75 per chunk for one group); groups x chunks <= 256.
  *   host_forc  [nstep][IBIS_FORC_COUNT][ld]  pinned HOST: hourly forcing
  *   forc       [nstep][IBIS_FORC_COUNT][ld]  DEVICE: where the forcing lands
  *   host_prog  [IBIS_PROG_COUNT][ld] pinned HOST, or NULL: the state after the
@@ -106,7 +113,7 @@ int ibis_step_split_noalloc_f32(float* prog, const float* stat, const float* for
  * on host arrays. */
 int ibis_step_host_f32(float* prog, const float* stat, const float* host_forc, float* forc, float* diag, float* acc,
                        float* host_prog, int ncell, int ld, int nstep, const IbisParams* params, int* status,
-                       int group, int config, void* stream);
+                       int group, int chunk, int config, void* stream);
 
 /* A calibration ensemble: nrun runs, each one parameter vector at one site
  * over its own record of hourly forcing.  Per-run buffers use ld_run, per-site

@@ -39,16 +39,18 @@ def test_step_rejects_bad_shapes(so):
 def test_host_step_rejects_bad_arguments(so):
     p = _p()
     args = (DEV, DEV, DEV, DEV, NUL, DEV, NUL)
-    assert so.ibis_step_host_f32(*args, 30, 33, 1, p, NUL, 0, -1, NUL) == EINVAL      # ld not a multiple of 32
-    assert so.ibis_step_host_f32(*args, 40, 32, 1, p, NUL, 0, -1, NUL) == EINVAL      # ncell > ld
-    assert so.ibis_step_host_f32(*args, 30, 32, 1, p, NUL, 48, -1, NUL) == EINVAL     # group not a multiple of 32
-    assert so.ibis_step_host_f32(*args, 30, 32, 1, p, NUL, -32, -1, NUL) == EINVAL
+    f = so.ibis_step_host_f32
+    assert f(*args, 30, 33, 1, p, NUL, 0, 0, -1, NUL) == EINVAL      # ld not a multiple of 32
+    assert f(*args, 40, 32, 1, p, NUL, 0, 0, -1, NUL) == EINVAL      # ncell > ld
+    assert f(*args, 30, 32, 1, p, NUL, 48, 0, -1, NUL) == EINVAL     # group not a multiple of 32
+    assert f(*args, 30, 32, 1, p, NUL, -32, 0, -1, NUL) == EINVAL
+    assert f(*args, 30, 32, 1, p, NUL, 0, -1, -1, NUL) == EINVAL     # negative chunk
     split = next(c["id"] for c in lib.configs() if c["form"] == "split")
-    assert so.ibis_step_host_f32(*args, 30, 32, 1, p, NUL, 0, split, NUL) == EINVAL   # needs scratch
-    assert so.ibis_step_host_f32(*args, 30, 32, 1, p, NUL, 0, 99, NUL) == EINVAL
-    assert so.ibis_step_host_f32(DEV, DEV, NUL, DEV, NUL, DEV, NUL, 30, 32, 1, p, NUL, 0, -1, NUL) == EINVAL
-    assert so.ibis_step_host_f32(DEV, DEV, DEV, NUL, NUL, DEV, NUL, 30, 32, 1, p, NUL, 0, -1, NUL) == EINVAL
-    assert so.ibis_step_host_f32(*args, 0, 32, 1, p, NUL, 0, -1, NUL) == 0             # nothing to do
+    assert f(*args, 30, 32, 1, p, NUL, 0, 0, split, NUL) == EINVAL   # needs scratch
+    assert f(*args, 30, 32, 1, p, NUL, 0, 0, 99, NUL) == EINVAL
+    assert f(DEV, DEV, NUL, DEV, NUL, DEV, NUL, 30, 32, 1, p, NUL, 0, 0, -1, NUL) == EINVAL
+    assert f(DEV, DEV, DEV, NUL, NUL, DEV, NUL, 30, 32, 1, p, NUL, 0, 0, -1, NUL) == EINVAL
+    assert f(*args, 0, 32, 1, p, NUL, 0, 0, -1, NUL) == 0             # nothing to do
 
 
 def test_day_kernels_reject_bad_arguments(so):

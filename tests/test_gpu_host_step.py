@@ -1,14 +1,16 @@
 """The step from host buffers (``ibis_step_host_f32`` through
-``Columns.run_host``): the columns cut into groups, each group's forcing copied
-in, stepped and copied out on the library's streams.
+``Columns.run_host``): the columns cut into groups and the hours into chunks,
+each piece's forcing copied in, stepped and copied out on the library's streams.
 
-The groups run the same kernels on the same columns as one launch over every
-column, so the state, the accumulators and the state copied to the host equal
-that launch's bit for bit, whatever the group size (several groups per compute
-stream included).  A column made non-finite in a late group is reported in the
-caller's numbering of the columns.  Every loop of the step has a fixed trip
-count and its two float-to-int conversions read static soil inputs, so a NaN
-in the forcing stays data: it propagates into that column and is flagged.
+The groups and chunks of hours run the same kernels on the same columns as
+one launch over every column and hour, so the state, the accumulators and the
+state copied to the host equal that launch's bit for bit, whatever the group
+size (several groups per compute stream included) and chunk length (the
+caller's Columns fix the launch configuration for all of them).  A column
+made non-finite in a late group is reported in the caller's numbering of the
+columns.  Every loop of the step has a fixed trip count and its two
+float-to-int conversions read static soil inputs, so a NaN in the forcing
+stays data: it propagates into that column and is flagged.
 """
 import numpy as np
 import pytest
@@ -37,8 +39,8 @@ def _columns(prog, stat):
     return Columns.from_host(prog, stat, dtype=torch.float32, acc=True)
 
 
-@pytest.mark.parametrize("group", [0, 256, 640, 4992])
-def test_host_groups_equal_one_launch(cuda_lib, group):
+@pytest.mark.parametrize("group,chunk", [(0, 0), (256, 0), (640, 0), (4992, 0), (5024, 2), (640, 3), (0, 1)])
+def test_host_groups_equal_one_launch(cuda_lib, group, chunk):
     prog, stat, forc, P = _workload()
     ref = _columns(prog, stat)
     ref.run(ref.forcing(forc), P)
@@ -46,7 +48,7 @@ def test_host_groups_equal_one_launch(cuda_lib, group):
     h_forc = torch.from_numpy(synth.forcing_planes(forc, cols.ld)).pin_memory()
     h_prog = torch.zeros_like(cols.prog, device="cpu").pin_memory()
     stream = torch.cuda.Stream()
-    cols.run_host(h_forc, P, host_prog=h_prog, group=group, stream=stream)
+    cols.run_host(h_forc, P, host_prog=h_prog, group=group, chunk=chunk, stream=stream)
     stream.synchronize()
     torch.cuda.synchronize()
     np.testing.assert_array_equal(cols.prog.cpu().numpy(), ref.prog.cpu().numpy())
