@@ -76,8 +76,15 @@ SIGNATURES = {
 }
 
 
+_configs = None
+
+
 def configs():
-    """List of dicts describing the launch configurations of the FP32 kernels."""
+    """List of dicts describing the launch configurations of the FP32 kernels
+    (read from the library once; the table is compiled in)."""
+    global _configs
+    if _configs is not None:
+        return [dict(c) for c in _configs]
     L = load()
     out = []
     for i in range(L.ibis_num_configs()):
@@ -86,7 +93,9 @@ def configs():
         f, b, m, b2, m2 = (x.value for x in v)
         out.append(dict(id=i, form="fused" if f == 0 else "split", block=b, min_blocks=m, block2=b2,
                         min_blocks2=m2))
-    return out
+    _configs = out
+    return [dict(c) for c in out]
+
 
 _lib = None
 
