@@ -11,7 +11,7 @@ paths are checked against it:
   same days with the same variates;
 * one request answered by the serving loop (3 sites, 2 model years of 48
   hours): its per-year sums against the oracle's sums over each year;
-* both ensemble forms under the release parameter file's switches (the kernels
+* every ensemble form under the release parameter file's switches (the kernels
   with the IBIS 3.0 extensions), the oracle under the same switches.
 
 Tolerances (FP32 kernels against float64 after 48 hours): temperatures within
@@ -96,14 +96,17 @@ def release_params():
     return P
 
 
-def _ensemble_vs_oracle(daily, params=None):
+def _ensemble_vs_oracle(daily, params=None, hourly=False):
     nsite, nparam, hours = 8, 4, 48
     spec = E.make_ensemble(nsite, nparam, site_hours=np.full(nsite, hours), seed=23, daily=daily, params=params)
     if params is not None:
         # per-site acclimation states for the release file's temperature acclimation
         spec.stat["acclim_x"] = np.random.default_rng(5).uniform(-12.0, 28.0, nsite)
     ens = E.Ensemble(spec, year_steps=24)
-    ens.run()
+    if hourly:
+        ens.run_hourly(chunk=24, graph=False)          # one launch per hour
+    else:
+        ens.run()
     torch.cuda.synchronize()
     assert not ens.nonfinite()[0]
     got_p, got_a = ens.prog_host(), ens.acc_host()
@@ -173,11 +176,12 @@ def test_daily_form_ensemble_runs_match_oracle(cuda_lib):
 
 def test_release_ensemble_runs_match_oracle(cuda_lib):
     """Runs under the release parameter file's switches (the ensemble kernels
-    with the IBIS 3.0 extensions) against the oracle under the same switches,
-    hourly records and the daily form."""
-    for daily in (False, True):
-        e = _ensemble_vs_oracle(daily, params=release_params())
-        assert e["temp"] < T_ABS and e["water"] < W_ABS and e["acc"] < ACC_REL, (daily, e)
+    with the IBIS 3.0 extensions) against the oracle under the same switches:
+    the persistent launch over hourly records and over day records, and one
+    launch per hour."""
+    for daily, hourly in ((False, False), (True, False), (False, True)):
+        e = _ensemble_vs_oracle(daily, params=release_params(), hourly=hourly)
+        assert e["temp"] < T_ABS and e["water"] < W_ABS and e["acc"] < ACC_REL, (daily, hourly, e)
 
 
 def test_release_switches_change_ensemble_runs(cuda_lib):
