@@ -675,6 +675,60 @@ def write_observed_sw_case(seed=23, n=64):
     print(f"wrote {path}: {len(out)} arrays, {os.path.getsize(path)} bytes")
 
 
+def write_wetland_case(seed=41, nlat=12, nlon=20, nmonth=9):
+    """tests/golden/wetland_area.npz: the reference's wetland-area functions on
+    seeded inputs -- the learned wetland's month-by-month feature builder
+    (bgc/wetland_learned.py:49-104) over ``nmonth`` months on a ``nlat`` x
+    ``nlon`` grid with about 60 % land (its lags, 3-month means and 5 x 5
+    neighbourhood means wrapping at every edge), ``hybrid_fraction`` (:107-110),
+    and the dynamic wetland area's ``root_zone_water`` / ``dynamic_fraction``
+    (bgc/wetland_area.py:22-39), frozen layers and zero spreads included."""
+    from ibis.bgc import wetland_learned as WL
+    from ibis.bgc import wetland_area as WA
+    rng = np.random.Generator(np.random.PCG64(seed))
+    I, J = np.where(rng.random((nlat, nlon)) < 0.6)
+    n, nl = len(I), 6
+    poros = rng.uniform(0.3, 0.6, (n, nl))
+    hsoi = np.array([0.10, 0.15, 0.25, 0.50, 1.0, 2.0])
+    ws = rng.uniform(0.0, 1.0, (nmonth, n, nl)).astype(np.float32)
+    wi = rng.uniform(0.0, 0.3, (nmonth, n, nl)).astype(np.float32)
+    ts = rng.uniform(250.0, 300.0, (nmonth, n, nl)).astype(np.float32)
+    tg = rng.uniform(250.0, 300.0, (nmonth, n)).astype(np.float32)
+    pr = rng.uniform(0.0, 200.0, (nmonth, n)).astype(np.float32)
+    et = rng.uniform(0.0, 100.0, (nmonth, n)).astype(np.float32)
+    ro = rng.uniform(0.0, 80.0, (nmonth, n)).astype(np.float32)
+    fb = WL.FeatureBuilder(I, J, poros, hsoi, nlat, nlon)
+    out = {"in.I": I, "in.J": J, "in.poros": poros, "in.hsoi": hsoi, "in.ws": ws, "in.wi": wi, "in.ts": ts,
+           "in.tg": tg, "in.prcp": pr, "in.aet": et, "in.runoff": ro, "in.nlat": np.asarray(nlat),
+           "in.nlon": np.asarray(nlon), "dyn_feats": np.array(WL.DYN_FEATS), "stat_feats": np.array(WL.STAT_FEATS)}
+    feats = np.zeros((nmonth, len(WL.DYN_FEATS), n))
+    for t in range(nmonth):
+        f = fb.step(ts[t], ws[t], wi[t], tg[t], pr[t], et[t], ro[t])
+        for k, name in enumerate(WL.DYN_FEATS):
+            feats[t, k] = f[name]
+    out["out.feats"] = feats
+    # hybrid fraction: anomalies of both signs, bounds hit from above and below
+    fclim = rng.uniform(0.0, 0.5, n); fmax = rng.uniform(0.05, 0.9, n); P = rng.uniform(0.0, 1.0, n)
+    pbar = rng.uniform(0.0, 1.0, n); lam = rng.uniform(0.0, 3.0, n)
+    fclim[:3] = (0.0, 0.9, 0.2)
+    out.update({"in.fclim": fclim, "in.fmax": fmax, "in.P": P, "in.pbar": pbar, "in.lam": lam,
+                "out.hybrid": np.asarray(WL.hybrid_fraction(fclim, P, pbar, lam, fmax), np.float64)})
+    # dynamic area: root-zone water (frozen layers count 0) and the bounded anomaly fraction
+    W = WA.root_zone_water(ws[0], poros, hsoi, ts[0])
+    mu = rng.uniform(0.05, 0.3, n); sd = rng.uniform(0.0, 0.1, n)
+    sd[:4] = (0.0, 1e-10, 1e-9, 2e-9)
+    beta = rng.uniform(0.0, 0.2, n); fmin = rng.uniform(0.0, 0.05, n)
+    frozen = np.asarray(ts[0][:, 0], np.float64) <= WA.T_FREEZE
+    out.update({"in.mu": mu, "in.sd": sd, "in.beta": beta, "in.fmin": fmin, "out.W": np.asarray(W, np.float64),
+                "out.dynamic": np.asarray(WA.dynamic_fraction(fclim, W, mu, sd, beta, fmin, fmax, frozen=frozen),
+                                          np.float64),
+                "meta.t_freeze": np.asarray(WA.T_FREEZE), "meta.root_layers": np.asarray(WA.ROOT_LAYERS),
+                "meta.nb": np.asarray(WL.NB)})
+    path = os.path.join(HERE, "wetland_area.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path}: {len(out)} arrays, {os.path.getsize(path)} bytes")
+
+
 def write_methane_case(seed=21, ndays=31):
     """tests/golden/methane_month.npz: the reference's monthly wetland methane
     functions (bgc/methane.py:233-496) on the 16-cell checkpoint's soil state:
@@ -754,6 +808,8 @@ def main():
         write_methane_case()
     if args.only in (None, "observed_sw"):
         write_observed_sw_case()
+    if args.only in (None, "wetland_area"):
+        write_wetland_case()
     if args.only in (None, "day_parts"):
         write_parts_case()
     if args.only in (None, "days_modules"):
@@ -765,7 +821,7 @@ def main():
     for name in X3_CASES:
         if args.only in (None, name):
             write_x3_case(name)
-    if args.only in ("restart_leaves", "restart_1996", "diurnal", "days", "methane_month", "observed_sw",
+    if args.only in ("restart_leaves", "restart_1996", "diurnal", "days", "methane_month", "observed_sw", "wetland_area",
                      "day_parts", "days_modules", "days_release", "restart_modules") + tuple(X3_CASES):
         return
     for name, spec in CASES.items():
