@@ -56,6 +56,7 @@ UNITS = {
     "ibis_step_f64.cu": ["--fmad=false"],
     "ibis_daily.cu": ["--fmad=false"],
     "ibis_month.cu": ["--fmad=false"],
+    "ibis_wetland.cu": ["--fmad=false"],
 }
 
 

@@ -36,6 +36,22 @@ class IbisEnsembleDailyC(ctypes.Structure):
                 ("seed", ctypes.c_uint), ("flags", ctypes.c_uint)]
 
 
+class IbisWetlandBuilderC(ctypes.Structure):
+    """ctypes mirror of ``IbisWetlandBuilder`` (include/ibis_b200.h)."""
+    _fields_ = [("npoi", ctypes.c_int), ("ld", ctypes.c_int), ("nlat", ctypes.c_int), ("nlon", ctypes.c_int),
+                ("cell_i", ctypes.c_void_p), ("cell_j", ctypes.c_void_p), ("poros", ctypes.c_void_p),
+                ("hsoi", ctypes.c_double * 4), ("lf", ctypes.c_void_p), ("buf", ctypes.c_void_p),
+                ("work", ctypes.c_void_p), ("nmonth", ctypes.c_int)]
+
+
+class IbisForestC(ctypes.Structure):
+    """ctypes mirror of ``IbisForest`` (include/ibis_b200.h)."""
+    _fields_ = [("nband", ctypes.c_int), ("nfeat", ctypes.c_int), ("tree_first", ctypes.c_void_p),
+                ("node_first", ctypes.c_void_p), ("left", ctypes.c_void_p), ("right", ctypes.c_void_p),
+                ("feature", ctypes.c_void_p), ("value", ctypes.c_void_p), ("default_left", ctypes.c_void_p),
+                ("base_margin", ctypes.c_void_p), ("transform", ctypes.c_void_p)]
+
+
 _c_int_p = ctypes.POINTER(ctypes.c_int)
 _P = ctypes.POINTER(IbisParamsC)
 _E = ctypes.POINTER(IbisEnsembleC)
@@ -55,6 +71,11 @@ SIGNATURES = {
     "ibis_step_split_noalloc_f32": (ctypes.c_int, [ctypes.c_void_p] * 5 + [ctypes.c_int] * 3
                                     + [_P, ctypes.c_void_p, ctypes.c_void_p]),
     "ibis_config_info": (ctypes.c_int, [ctypes.c_int] + [_c_int_p] * 5),
+    "ibis_wetland_dynamic_f32": (ctypes.c_int, [_V] * 4 + [ctypes.c_int] * 2 + [_P, _V]),
+    "ibis_wetland_grid": (ctypes.c_int, [ctypes.POINTER(IbisWetlandBuilderC), _V]),
+    "ibis_wetland_features": (ctypes.c_int, [ctypes.POINTER(IbisWetlandBuilderC)] + [_V] * 4),
+    "ibis_wetland_learned": (ctypes.c_int, [ctypes.POINTER(IbisForestC), _V] + [ctypes.c_int] * 2 + [_V] * 7
+                             + [ctypes.c_int] + [_V] * 3),
     "ibis_step_host_f32": (ctypes.c_int, [_V] * 7 + [ctypes.c_int] * 3 + [_P, _V] + [ctypes.c_int] * 3 + [_V]),
     "ibis_ensemble_f32": (ctypes.c_int, [_E, _P, ctypes.c_int, ctypes.c_void_p]),
     "ibis_ensemble_hours_f32": (ctypes.c_int, [_E, _P, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),

@@ -301,6 +301,95 @@ int ibis_month_end_f64(const double* prog, const double* stat, const double* acc
                        const double* scale, int ncell, int ld, int ndays, const IbisParams* params,
                        unsigned int flags, void* stream);
 
+/* ---------------------------------------------------------------------------
+ * Wetland (inundated) area of the monthly methane: the two optional sources of
+ * the month's fraction besides the WAD2M climatology.  Arithmetic in float64,
+ * as the reference's host-side numpy.
+ * ------------------------------------------------------------------------- */
+
+/* Dynamic wetland area: f = clip(clip(fclim (1 + beta A), fmin, fmax), 0, 1),
+ * A = (W - mu) / sd (0 where sd <= 1e-9 or the top layer is frozen), W the
+ * liquid water of the top four layers (wsoi * poros * hsoi, a layer at or
+ * below 273.16 K counting 0) of the state in `prog` / `stat`.
+ *   area   [6][ld] double: fclim, mu, sd, beta, fmin, fmax of the month
+ *   f_out  [ld] float: the month's fraction (e.g. the STAT f_inund plane)
+ * Replaces: root_zone_water / dynamic_fraction (python-port/ibis/bgc/wetland_area.py:22-39)
+ * as the global driver calls them (scripts/run_global.py:806-810). */
+int ibis_wetland_dynamic_f32(const float* prog, const float* stat, const double* area, float* f_out, int ncell,
+                             int ld, const IbisParams* params, void* stream);
+
+/* The learned wetland's feature builder, one month per call: the 33 monthly
+ * predictors in the model's order (DYN_FEATS) from the month's MEAN soil state
+ * and its water totals, with the months it keeps for lags, 3-month means and
+ * the 5 x 5 neighbourhood means (a box filter that wraps at every edge of the
+ * nlat x nlon grid, as scipy's uniform_filter(mode='wrap')). */
+#define IBIS_WETLAND_NFEAT 33
+enum {
+    IBIS_WFB_W = 0,        /* W of the last 4 months, oldest first */
+    IBIS_WFB_PRCP = 4,     /* precipitation, 3 months */
+    IBIS_WFB_RUNOFF = 7,   /* runoff + drainage, 3 months */
+    IBIS_WFB_W3 = 10,      /* 3-month means of W, 4 months */
+    IBIS_WFB_P3 = 14,      /* of precipitation, 4 months */
+    IBIS_WFB_R3 = 18,      /* of runoff, 4 months */
+    IBIS_WFB_NP3 = 22,     /* neighbourhood means of P3, 3 months */
+    IBIS_WFB_NR3 = 25,     /* of R3, 3 months */
+    IBIS_WFB_COUNT = 28
+};
+typedef struct IbisWetlandBuilder {
+    int npoi, ld, nlat, nlon;
+    const int* cell_i;     /* [npoi] device: grid row of each land point */
+    const int* cell_j;     /* [npoi] device: grid column */
+    const double* poros;   /* [4][ld] device: porosity of the top four layers */
+    double hsoi[4];        /* thickness of the top four layers, m */
+    double* lf;            /* [nlat*nlon] device: box filter of the land mask (ibis_wetland_grid) */
+    double* buf;           /* [IBIS_WFB_COUNT][ld] device: months kept (in/out) */
+    double* work;          /* [4][nlat*nlon] device: scratch */
+    int nmonth;            /* months stepped before this call */
+} IbisWetlandBuilder;
+
+/* Fill b->lf: the box filter of the land mask (1 at the land points). */
+int ibis_wetland_grid(const IbisWetlandBuilder* b, void* stream);
+
+/* One month: means [19][ld] float (tsoi 6, wsoi 6, wisoi 6, tg), totals [3][ld]
+ * float (precipitation, AET, runoff + drainage of the month); feats
+ * [IBIS_WETLAND_NFEAT][ld] double out.  The caller increments b->nmonth after.
+ * Replaces: FeatureBuilder.step (python-port/ibis/bgc/wetland_learned.py:75-104). */
+int ibis_wetland_features(const IbisWetlandBuilder* b, const float* means, const float* totals, double* feats,
+                          void* stream);
+
+/* The trained models, one gradient-boosted tree ensemble per wetland band, in
+ * flat node arrays (from XGBoost JSON boosters by ibis_b200/wetland.py): a
+ * row goes left where its predictor is below `value` (float32), or, where it
+ * is NaN, the way default_left says; a leaf's `value` is its output; a model's
+ * prediction is base_margin plus its trees' leaves summed in float32, tree
+ * after tree, then transform (0 identity, 1 logistic). */
+typedef struct IbisForest {
+    int nband, nfeat;
+    const int* tree_first;            /* [nband + 1] device */
+    const int* node_first;            /* [ntree + 1] device */
+    const int* left;                  /* [nnode] device, -1 at a leaf */
+    const int* right;                 /* [nnode] device */
+    const int* feature;               /* [nnode] device */
+    const float* value;               /* [nnode] device */
+    const unsigned char* default_left;/* [nnode] device */
+    const float* base_margin;         /* [nband] device */
+    const int* transform;             /* [nband] device */
+} IbisForest;
+
+/* The learned fraction of one month: every land point gets clip(f_base, 0, 1),
+ * then each cell p of the trained file (land point pts[p], band[p]) gets
+ * clip(clip(fclim[p] + lam[band] (P - pbar[p]), 0, fmax[p]), 0, 1), P its
+ * model's prediction (clipped to [0, 1]) on the 33 predictors of `feats` at
+ * the point and the file's 12 static predictors.  Device arrays:
+ *   pts, band [ncells] int;  fclim, pbar (the month's), fmax [ncells] double;
+ *   stat [ncells][12] double;  lam [nband] double;  f_base, f_out [ld] float
+ * Replaces: LearnedWetland.predict / fraction and hybrid_fraction
+ * (python-port/ibis/bgc/wetland_learned.py:107-160). */
+int ibis_wetland_learned(const IbisForest* forest, const double* feats, int npoi, int ld, const int* pts,
+                         const int* band, const double* fclim, const double* pbar, const double* fmax,
+                         const double* stat, const double* lam, int ncells, const float* f_base, float* f_out,
+                         void* stream);
+
 /* Same contract in float64 throughout (the float64 run of the reference's step). */
 int ibis_step_f64(double* prog, const double* stat, const double* forc, double* diag, double* acc, int ncell,
                   int ld, int nstep, const IbisParams* params, int* status, void* stream);

@@ -2,6 +2,8 @@
 import ctypes
 import os
 
+import pytest
+
 from ibis_b200 import build, lib
 
 
@@ -59,6 +61,17 @@ def test_ensemble_daily_layout_matches_ctypes(tmp_path):
     names = [f[0] for f in E._fields_]
     body = 'printf("%zu ", sizeof(IbisEnsembleDaily));'
     body += "".join(f'printf("%zu ", offsetof(IbisEnsembleDaily, {n}));' for n in names)
+    got = _c_layout(tmp_path, body)
+    assert got[0] == ctypes.sizeof(E)
+    assert got[1:] == [getattr(E, n).offset for n in names]
+
+
+@pytest.mark.parametrize("struct,cname", [("IbisWetlandBuilderC", "IbisWetlandBuilder"), ("IbisForestC", "IbisForest")])
+def test_wetland_layouts_match_ctypes(tmp_path, struct, cname):
+    E = getattr(lib, struct)
+    names = [f[0] for f in E._fields_]
+    body = f'printf("%zu ", sizeof({cname}));'
+    body += "".join(f'printf("%zu ", offsetof({cname}, {n}));' for n in names)
     got = _c_layout(tmp_path, body)
     assert got[0] == ctypes.sizeof(E)
     assert got[1:] == [getattr(E, n).offset for n in names]
