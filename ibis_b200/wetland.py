@@ -265,21 +265,17 @@ class LearnedWetland:
         _lib.check(rc, "ibis_wetland_learned")
         return out
 
-
-def _fraction_host(self, imonth: int, feats: dict, f_base) -> np.ndarray:
-    """:meth:`LearnedWetland.fraction` with the reference's arguments
-    (``LearnedWetland.fraction``): ``feats`` ``{name: (npoi,) array}``, ``f_base``
-    ``(npoi,)``; returns the ``(npoi,)`` float32 fraction."""
-    fd = np.zeros((NFEAT, self.ld))
-    for k, name in enumerate(DYN_FEATS):
-        fd[k, :self.npoi] = np.asarray(feats[name], np.float64)
-    fb = np.zeros(self.ld, np.float32)
-    fb[:self.npoi] = np.asarray(f_base, np.float32)
-    out = self.fraction(imonth, torch.from_numpy(fd).to(self.device), torch.from_numpy(fb).to(self.device))
-    return out.cpu().numpy()[:self.npoi]
-
-
-LearnedWetland.fraction_host = _fraction_host
+    def fraction_host(self, imonth: int, feats: dict, f_base) -> np.ndarray:
+        """:meth:`fraction` with the reference's arguments (``LearnedWetland.fraction``):
+        ``feats`` ``{name: (npoi,) array}``, ``f_base`` ``(npoi,)``; returns the
+        ``(npoi,)`` float32 fraction."""
+        fd = np.zeros((NFEAT, self.ld))
+        for k, name in enumerate(DYN_FEATS):
+            fd[k, :self.npoi] = np.asarray(feats[name], np.float64)
+        fb = np.zeros(self.ld, np.float32)
+        fb[:self.npoi] = np.asarray(f_base, np.float32)
+        out = self.fraction(imonth, torch.from_numpy(fd).to(self.device), torch.from_numpy(fb).to(self.device))
+        return out.cpu().numpy()[:self.npoi]
 
 
 def run_month_learned(loop, daily: torch.Tensor, fb: FeatureBuilder, lw: LearnedWetland, imonth: int,

@@ -128,10 +128,9 @@ def test_learned_fraction_equals_oracle(cuda_lib):
         got = lw.fraction(imonth, torch.from_numpy(fd).cuda(), torch.from_numpy(base).cuda()).cpu().numpy()[:n]
         want = lo.fraction(imonth, feats, base[:n].astype(np.float64))
         np.testing.assert_array_equal(got, want.astype(np.float32), err_msg=f"month {imonth}")
-    # the boosters' predictions themselves, per band
-    X = lo.features(feats)
-    P = lo.predict(feats)
-    assert np.isfinite(P).all() and X.shape[1] == 45
+    # the reference's call form: predictor dict and base fraction on the host
+    got = lw.fraction_host(3, feats, base[:n])
+    np.testing.assert_array_equal(got, lo.fraction(3, feats, base[:n].astype(np.float64)).astype(np.float32))
 
 
 def test_learned_month_on_the_day_loop(cuda_lib):
