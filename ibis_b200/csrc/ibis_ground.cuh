@@ -476,29 +476,76 @@ __device__ __forceinline__ void fire_counters(Col<R>& c, R swilt0, const Forc<R>
     c.sdry_vpd = c.sdry_vpd + fl * hit;
 }
 
+// Methane parameters of one cell: the parameter source's (one set per launch,
+// or per run), or under IBIS_FLAG_CH4_BANDS the set of the cell's band
+// (`band` = the STAT ch4_band value: 0 tropical, 1 temperate, 2 boreal), as
+// biome_methane_params gives every cell its band's values (methane.py:521-563).
+template <typename R>
+struct Ch4Par {
+    R sat_crit, z_max, r_ch4, q10p, t_ref, z_wt_max, z_tau, tau_oxid, wtot;
+    R wtop[NL];
+};
+
+// entry b (0, 1 or 2) of a 3-entry table by selects, so no index into the
+// parameter record depends on data
+template <typename R>
+__device__ __forceinline__ R pick3(const R (&a)[3], int b) { return b == 2 ? a[2] : (b == 1 ? a[1] : a[0]); }
+
+template <typename R, typename Q>
+__device__ __forceinline__ Ch4Par<R> ch4_params(R band, const DevParams<R>& P, const Q& q) {
+    Ch4Par<R> m;
+    if (P.flags & IBIS_FLAG_CH4_BANDS) {
+        const int b = band >= R(1.5) ? 2 : (band >= R(0.5) ? 1 : 0);   // NaN: the first band
+        m.sat_crit = pick3(P.ch4b_sat_crit, b);
+        m.z_max = pick3(P.ch4b_z_max, b);
+        m.r_ch4 = pick3(P.ch4b_r_ch4, b);
+        m.q10p = pick3(P.ch4b_q10p, b);
+        m.t_ref = pick3(P.ch4b_t_ref, b);
+        m.z_wt_max = pick3(P.ch4b_z_wt_max, b);
+        m.z_tau = pick3(P.ch4b_z_tau, b);
+        m.tau_oxid = pick3(P.ch4b_tau_oxid, b);
+        m.wtot = pick3(P.ch4b_wtot, b);
+#pragma unroll
+        for (int k = 0; k < NL; ++k)
+            m.wtop[k] = b == 2 ? P.ch4b_wtop[2][k] : (b == 1 ? P.ch4b_wtop[1][k] : P.ch4b_wtop[0][k]);
+    } else {
+        m.sat_crit = P.sat_crit;
+        m.z_max = P.z_max;
+        m.r_ch4 = q.r_ch4();
+        m.q10p = q.q10p();
+        m.t_ref = P.t_ref;
+        m.z_wt_max = q.z_wt_max();
+        m.z_tau = q.z_tau();
+        m.tau_oxid = q.tau_oxid();
+        m.wtot = P.ch4_wtot;
+#pragma unroll
+        for (int k = 0; k < NL; ++k) m.wtop[k] = P.ch4_wtop[k];
+    }
+    return m;
+}
+
 // wetland_water_table (methane.py:233-276): the water table inside the
 // inundated fraction, m; a finite observed depth `zwt_obs` replaces it, clipped
 // to [0, z_max] (methane.py:366-367).
 template <typename R>
-__device__ __forceinline__ R wetland_water_table(const R (&w)[NL], const R (&i)[NL], R z_wt_max, R zwt_obs,
-                                                 const DevParams<R>& P) {
+__device__ __forceinline__ R wetland_water_table(const R (&w)[NL], const R (&i)[NL], const Ch4Par<R>& m, R zwt_obs) {
     R acc = R(0.0);
 #pragma unroll
     for (int k = 0; k < NL; ++k) {
         R th = clip(w[k] * (R(1.0) - i[k]) + i[k], R(0.0), R(1.0));
-        acc = acc + th * P.ch4_wtop[k];
+        acc = acc + th * m.wtop[k];
     }
-    R ttop = acc / P.ch4_wtot;
-    R wet = clip(ttop / mx(P.sat_crit, R(1e-6)), R(0.0), R(1.0));
-    R zwt = z_wt_max * (R(1.0) - wet);
-    return isfinite(zwt_obs) ? clip(zwt_obs, R(0.0), P.z_max) : zwt;
+    R ttop = acc / m.wtot;
+    R wet = clip(ttop / mx(m.sat_crit, R(1e-6)), R(0.0), R(1.0));
+    R zwt = m.z_wt_max * (R(1.0) - wet);
+    return isfinite(zwt_obs) ? clip(zwt_obs, R(0.0), m.z_max) : zwt;
 }
 
 // methane_flux (methane.py:233-383), kgC m-2 d-1; zwt_obs NaN: the model's water table
-template <typename R, typename Q>
+template <typename R>
 __device__ __forceinline__ R methane(R f_inund, R rh, const R (&t)[NL], const R (&w)[NL], const R (&i)[NL],
-                                     R zwt_obs, const DevParams<R>& P, const Q& q) {
-    R zwt = wetland_water_table(w, i, q.z_wt_max(), zwt_obs, P);
+                                     R zwt_obs, const Ch4Par<R>& m, const DevParams<R>& P) {
+    R zwt = wetland_water_table(w, i, m, zwt_obs);
     R tt = R(0.0), tw = R(0.0);
 #pragma unroll
     for (int k = 0; k < NL; ++k) {
@@ -510,11 +557,11 @@ __device__ __forceinline__ R methane(R f_inund, R rh, const R (&t)[NL], const R 
     }
     R tth = tt > R(1e-12) ? tw / mx(tt, R(1e-12)) : t[0];
     R zp = mx(zwt, R(0.0));
-    R rha = mx(rh, R(0.0)) * ex(-zp / mx(q.z_tau(), R(1e-6)));
-    R q10 = pw(q.q10p(), (tth - P.t_ref) / R(10.0));
-    R prod = mx(rha, R(0.0)) * q.r_ch4() * q10 * (tth >= R(273.15) ? R(1.0) : R(0.0));
+    R rha = mx(rh, R(0.0)) * ex(-zp / mx(m.z_tau, R(1e-6)));
+    R q10 = pw(m.q10p, (tth - m.t_ref) / R(10.0));
+    R prod = mx(rha, R(0.0)) * m.r_ch4 * q10 * (tth >= R(273.15) ? R(1.0) : R(0.0));
     R area = clip(mx(f_inund, R(0.0)), R(0.0), R(1.0));
-    return area * prod * ex(-zp / mx(q.tau_oxid(), R(1e-6)));
+    return area * prod * ex(-zp / mx(m.tau_oxid, R(1e-6)));
 }
 
 }  // namespace ibis

@@ -360,6 +360,17 @@ static DevParams<R> make_dev_params(const IbisParams& h) {
         top = bot;
     }
     d.ch4_wtot = (R)(tot > 1e-12 ? tot : 1e-12);
+    for (int b = 0; b < 3; ++b) {
+        double btop = 0.0, btot = 0.0;
+        for (int k = 0; k < NL; ++k) {
+            double w = h.ch4b_z_wt_ref[b] - btop;
+            w = w < 0.0 ? 0.0 : (w > h.hsoi[k] ? h.hsoi[k] : w);
+            d.ch4b_wtop[b][k] = (R)w;
+            btot += w;
+            btop += h.hsoi[k];
+        }
+        d.ch4b_wtot[b] = (R)(btot > 1e-12 ? btot : 1e-12);
+    }
     return d;
 }
 
@@ -519,7 +530,8 @@ static int hourly_step(R* prog, const R* stat, const R* forc, R* diag, R* acc, i
     if (ncell == 0 || nstep == 0) return 0;
     const unsigned known = IBIS_FLAG_BEDROCK | IBIS_FLAG_H2O_CONSISTENT | IBIS_FLAG_SUNSHADE_U | IBIS_FLAG_SUNSHADE_L |
                            IBIS_FLAG_ACC | IBIS_FLAG_CH4 | IBIS_FLAG_SOIL_MEANS | IBIS_FLAG_DIAG | IBIS_FLAG_KAHAN |
-                           IBIS_FLAG_ZWT_OBS | IBIS_FLAG_ETPARTS | IBIS_FLAG_NEEPARTS | IBIS_FLAGS_X3;
+                           IBIS_FLAG_ZWT_OBS | IBIS_FLAG_ETPARTS | IBIS_FLAG_NEEPARTS | IBIS_FLAGS_X3 |
+                           IBIS_FLAG_CH4_BANDS;
     if (hp->flags & ~known) return -EINVAL;
     if ((hp->flags & (IBIS_FLAG_ACC | IBIS_FLAG_CH4 | IBIS_FLAG_SOIL_MEANS)) && !acc) return -EINVAL;
     if ((hp->flags & IBIS_FLAG_DIAG) && !diag) return -EINVAL;

@@ -49,6 +49,7 @@ __global__ void __launch_bounds__(128) month_end_kernel(const R* __restrict__ pr
         ic[k] = G(IBIS_PROG_WISOI + k);
     }
     const UniformQ<R> q{P};
+    const Ch4Par<R> m = ch4_params((P.flags & IBIS_FLAG_CH4_BANDS) ? S(IBIS_STAT_CH4_BAND) : R(0.0), P, q);
     const R zo = (P.flags & IBIS_FLAG_ZWT_OBS) ? S(IBIS_STAT_ZWT_OBS) : R(NAN);
     const R nd = R(ndays);
     const R a0 = W[(size_t)IBIS_WET_ANNUAL * ld];
@@ -57,9 +58,9 @@ __global__ void __launch_bounds__(128) month_end_kernel(const R* __restrict__ pr
         flux = (acc[(size_t)IBIS_ACC_CH4 * ld + i] - acc[(size_t)(IBIS_ACC_CH4 + IBIS_ACC_COUNT) * ld + i]) / nd;
     } else {
         const R rh = S(IBIS_STAT_TCO2MIC) * P.rh_conv;
-        flux = methane(S(IBIS_STAT_F_INUND), rh, t, w, ic, zo, P, q);
+        flux = methane(S(IBIS_STAT_F_INUND), rh, t, w, ic, zo, m, P);
     }
-    const R zwt = wetland_water_table(w, ic, q.z_wt_max(), zo, P);
+    const R zwt = wetland_water_table(w, ic, m, zo);
     R annual = a0 + flux * nd;
     if (scale) {
         const R f = R((float)scale[i]);

@@ -47,6 +47,10 @@ struct DevParams {
     // index of the launch's first column in the caller's numbering: a launch
     // over a group of columns (ibis_step_host_f32) reports status[1] in it
     int cell0;
+    // per-band thickness weights of the wetland water-table average and their
+    // sums (IBIS_FLAG_CH4_BANDS: from ch4b_z_wt_ref as ch4_wtop from z_wt_ref)
+    R ch4b_wtop[3][6];
+    R ch4b_wtot[3];
 };
 
 // The parameters a calibration ensemble varies per run (the 31-parameter

@@ -708,7 +708,8 @@ __device__ __forceinline__ void ground_phase(Col<R>& c, const Forc<R>& F, const 
         if (P.flags & IBIS_FLAG_CH4) {
             R rh = S(IBIS_STAT_TCO2MIC) * P.rh_conv;
             const R zo = (P.flags & IBIS_FLAG_ZWT_OBS) ? S(IBIS_STAT_ZWT_OBS) : R(NAN);
-            R flux = methane(S(IBIS_STAT_F_INUND), rh, c.tsoi, c.wsoi, c.wisoi, zo, P, q);
+            const Ch4Par<R> m = ch4_params((P.flags & IBIS_FLAG_CH4_BANDS) ? S(IBIS_STAT_CH4_BAND) : R(0.0), P, q);
+            R flux = methane(S(IBIS_STAT_F_INUND), rh, c.tsoi, c.wsoi, c.wisoi, zo, m, P);
             Ac.add(IBIS_ACC_CH4, flux * P.ch4_w);
         }
         if (P.flags & IBIS_FLAG_SOIL_MEANS) {

@@ -154,7 +154,7 @@ def step_params(state, consts, params, dtime: float, ndaypy: float = 365.0) -> S
     P = StepParams()
     for name, path in PARAM_PATHS.items():
         v = _get(roots, path)
-        if v is None:
+        if v is None or name in _METHANE_FIELDS:
             continue
         n = np.size(getattr(P, name))
         arr = np.asarray(v, dtype=np.float64).reshape(-1)
@@ -163,6 +163,10 @@ def step_params(state, consts, params, dtime: float, ndaypy: float = 365.0) -> S
         if n > 1 and arr.size == 1:
             arr = np.full(n, arr[0])
         setattr(P, name, arr if n > 1 else float(arr[0]))
+    mp = getattr(params, "methane", None)
+    if mp is not None:
+        ncell = int(np.size(np.asarray(state.soil.tg)))
+        apply_methane(P, {}, mp, ncell)
     for name, (env, default) in _ENV.items():
         setattr(P, name, float(os.environ.get(env, default)))
     P.dtime = float(dtime)
@@ -189,15 +193,60 @@ def step_params(state, consts, params, dtime: float, ndaypy: float = 365.0) -> S
     return P
 
 
+def methane_sets(mp, ncell):
+    """A reference ``MethaneParams`` as the step takes it: ``(values, None)``
+    when every field is one value, or ``(tables, band)`` when fields are
+    per-cell arrays (``biome_methane_params``, methane.py:521-563): the cells'
+    distinct parameter sets -- at most three, one per wetland band -- as the
+    ``ch4b_*`` tables and each cell's set as its ch4_band value."""
+    fields = [k for k in _METHANE_FIELDS if getattr(mp, k, None) is not None]
+    if not any(np.size(getattr(mp, k)) > 1 for k in fields):
+        return {k: float(np.asarray(getattr(mp, k)).reshape(-1)[0]) for k in fields}, None
+    rows = np.stack([np.broadcast_to(np.asarray(getattr(mp, k), np.float64).reshape(-1) if np.size(getattr(mp, k)) > 1
+                                     else np.asarray(getattr(mp, k), np.float64), (ncell,)) for k in fields], axis=1)
+    sets, band = np.unique(rows, axis=0, return_inverse=True)
+    if len(sets) > 3:
+        raise NotImplementedError(f"per-cell methane parameters in {len(sets)} distinct sets (the step takes up to "
+                                  "three bands, as biome_methane_params forms them)")
+    tables = {k: [float(sets[min(b, len(sets) - 1), j]) for b in range(3)] for j, k in enumerate(fields)}
+    if "z_wt_ref" in tables and len(set(tables["z_wt_ref"])) > 1:
+        raise NotImplementedError("per-cell z_wt_ref (the reference's water table takes one)")
+    return tables, np.asarray(band, np.float64).reshape(ncell)
+
+
+def apply_methane(P, stat, mp, ncell):
+    """Put ``methane_sets(mp)`` into the step's record ``P`` (scalars, or the
+    per-band tables with FLAG_CH4_BANDS and the first set as the scalars) and
+    the STAT dict ``stat`` (the ch4_band plane)."""
+    from .params import FLAG_CH4_BANDS
+    vals, band = methane_sets(mp, ncell)
+    if band is None:
+        for k, v in vals.items():
+            setattr(P, k, v)
+        P.flags &= ~FLAG_CH4_BANDS
+        return
+    for k, t in vals.items():
+        setattr(P, "ch4b_" + k, np.asarray(t, np.float64))
+        setattr(P, k, t[0])
+    P.flags |= FLAG_CH4_BANDS
+    stat["ch4_band"] = band
+
+
 def _stat_dict(state, params, ncell):
     """STAT planes of ``state`` plus the per-cell SimParams arrays the step reads
-    (``cropfrac``, ``forganic``: the layout's ``sim.`` leaves)."""
+    (``cropfrac``, ``forganic``: the layout's ``sim.`` leaves) and, where the
+    methane parameters are per cell, their band plane."""
     stat = _leaf_dict(state, "STAT", ncell)
     for f in L.STAT:
         if f.leaf.startswith("sim."):
             v = getattr(params, f.leaf[4:], None)
             if v is not None:
                 stat[f.name] = np.asarray(v, dtype=np.float64).reshape((ncell,) + ((f.k,) if f.k > 1 else ()))
+    mp = getattr(params, "methane", None)
+    if mp is not None:
+        _, band = methane_sets(mp, ncell)
+        if band is not None:
+            stat["ch4_band"] = band
     return stat
 
 
@@ -372,9 +421,8 @@ def run_month_scan(state, consts, params, xs, nsoilcall: int, ndaypy: int, dtime
         f_inund, mp, zwt_obs = ch4_args
         P.flags |= FLAG_CH4
         stat["f_inund"] = np.asarray(f_inund, dtype=np.float64)
-        for k in _METHANE_FIELDS:
-            if getattr(mp, k, None) is not None:
-                setattr(P, k, float(getattr(mp, k)))
+        stat.pop("ch4_band", None)
+        apply_methane(P, stat, mp, ncell)
         if zwt_obs is not None:
             P.flags |= FLAG_ZWT_OBS
             stat["zwt_obs"] = np.asarray(zwt_obs, dtype=np.float64)

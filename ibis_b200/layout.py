@@ -127,6 +127,9 @@ STAT = (
     Field("td", "atm.td"),
     Field("cropfrac", "sim.cropfrac"),
     Field("forganic", "sim.forganic", NSOILAY),
+    # the cell's wetland band for per-band methane parameters (FLAG_CH4_BANDS): 0 tropical, 1 temperate,
+    # 2 boreal -- the latitude rule or the Koeppen wetland type of biome_methane_params (methane.py:536-548)
+    Field("ch4_band", "sim.ch4_band"),
 )
 
 #: Leaf prefixes of fields that are not leaves of the base reference state: the

@@ -89,6 +89,11 @@ PARAM_FIELDS: list[tuple[str, int, object]] = [
     ("sat_crit", 1, 0.95), ("z_max", 1, 4.0), ("r_ch4", 1, 0.23), ("q10p", 1, 1.60),
     ("t_ref", 1, 295.15), ("z_wt_max", 1, 0.30), ("z_wt_ref", 1, 0.50), ("z_tau", 1, 0.50),
     ("tau_oxid", 1, 0.10),
+    # per-band MethaneParams [tropical, temperate, boreal] selected per cell by the STAT ch4_band plane under
+    # FLAG_CH4_BANDS: biome_methane_params (methane.py:521-563) with or without a parameter file's methane_bands
+    ("ch4b_sat_crit", 3, (0.95,) * 3), ("ch4b_z_max", 3, (4.0,) * 3), ("ch4b_r_ch4", 3, (0.23,) * 3),
+    ("ch4b_q10p", 3, (1.60,) * 3), ("ch4b_t_ref", 3, (295.15,) * 3), ("ch4b_z_wt_max", 3, (0.30,) * 3),
+    ("ch4b_z_wt_ref", 3, (0.50,) * 3), ("ch4b_z_tau", 3, (0.50,) * 3), ("ch4b_tau_oxid", 3, (0.10,) * 3),
     # --- BGCParams respiration used by the NPP accumulator (io/parameters.py:248-259)
     ("rwood", 12, (0.0125,) * 12), ("rroot", 12, (1.25,) * 12), ("rgrowth", 12, (0.30,) * 12),
     ("ndaypy", 1, 365.0),
@@ -120,12 +125,15 @@ FLAG_CAP_SCALE_L = 1 << 19     # StomataParams.cap_scale_l
 FLAG_LEAF_ONLY = 1 << 20       # StomataParams.scale_leaf_only: light scaling over leaves and stems (stomata.py:442-512)
 FLAG_CROP = 1 << 21            # SimParams.cropfrac present: grass capacity on the cropland share (loops.py:218-231)
 FLAG_FORGANIC = 1 << 22        # SimParams.forganic present: organic dry conductivity (soil_physics.py:74-77)
+# per-cell methane parameters by wetland band (biome_methane_params, methane.py:521-563): the ch4b_* tables
+# indexed by the STAT ch4_band plane (0 tropical, 1 temperate, 2 boreal) in every CH4 of the step and the month
+FLAG_CH4_BANDS = 1 << 23
 X3_FLAGS = (FLAG_VMAX_MIX | FLAG_COEFM_MIX | FLAG_GPP_CAPACITY | FLAG_ACCLIM | FLAG_ACCLIM_LIGHT | FLAG_FROST
             | FLAG_CAP_SCALE_U | FLAG_CAP_SCALE_L | FLAG_LEAF_ONLY | FLAG_CROP | FLAG_FORGANIC)
 
 KNOWN_FLAGS = (FLAG_BEDROCK | FLAG_H2O_CONSISTENT | FLAG_SUNSHADE_U | FLAG_SUNSHADE_L | FLAG_ACC
                | FLAG_CH4 | FLAG_SOIL_MEANS | FLAG_DIAG | FLAG_KAHAN | FLAG_ZWT_OBS | FLAG_ETPARTS | FLAG_NEEPARTS
-               | X3_FLAGS)
+               | X3_FLAGS | FLAG_CH4_BANDS)
 
 # Default root profile (lower, upper) used by the synthetic columns; the reference keeps froot as a
 # state leaf vegetation.froot of shape (nsoilay, 2) shared by every cell.
@@ -279,6 +287,55 @@ IbisDayParamsC = type("IbisDayParams", (ctypes.Structure,),
                                     for n, c, _ in DAY_PARAM_FIELDS]})
 
 
+#: biome_methane_params' per-biome constants [tropical, temperate, boreal] (methane.py:504, 519)
+R_CH4_BIOME = (0.15, 0.32, 0.18)
+T_REF_BIOME = (299.6, 283.0, 277.9)
+CH4_BAND_FIELDS = ("sat_crit", "z_max", "r_ch4", "q10p", "t_ref", "z_wt_max", "z_wt_ref", "z_tau", "tau_oxid")
+CH4_BANDS = ("tropical", "temperate", "boreal")
+
+
+def methane_band_index(lat_deg, band_index=None) -> np.ndarray:
+    """The STAT ch4_band plane (0 tropical, 1 temperate, 2 boreal) the way
+    biome_methane_params assigns biomes (methane.py:536-548): tropical for
+    -30 < lat < 30, boreal for lat >= 60, temperate otherwise; a Koeppen
+    wetland type ``band_index`` >= 0 (0, 1, 2) replaces the latitude rule."""
+    lat = np.asarray(lat_deg, np.float64)
+    trop = (lat > -30.0) & (lat < 30.0)
+    boreal = lat >= 60.0
+    if band_index is not None:
+        bi = np.asarray(band_index)
+        trop = np.where(bi >= 0, bi == 0, trop)
+        boreal = np.where(bi >= 0, bi == 2, boreal)
+    return np.where(trop, 0.0, np.where(boreal, 2.0, 1.0))
+
+
+def with_methane_bands(P: "StepParams", bands: dict | None = None) -> "StepParams":
+    """A copy of ``P`` with per-band methane parameters (FLAG_CH4_BANDS) as
+    biome_methane_params forms them (methane.py:521-563): without ``bands`` the
+    per-biome r_ch4 and t_ref constants and ``P``'s other values; with a
+    parameter file's ``methane_bands`` section ({tropical|temperate|boreal:
+    {field: value}}) each band's given fields, ``P``'s value elsewhere."""
+    out = P.copy()
+    tables = {f: [float(getattr(P, f))] * 3 for f in CH4_BAND_FIELDS}
+    if bands is None:
+        tables["r_ch4"] = list(R_CH4_BIOME)
+        tables["t_ref"] = list(T_REF_BIOME)
+    else:
+        given = sorted({k for v in bands.values() for k in v})
+        bad = [k for k in given if k not in CH4_BAND_FIELDS]
+        if bad:
+            raise KeyError(f"unknown methane fields in methane_bands: {bad}")
+        if "z_wt_ref" in given:
+            # the reference's water table takes one z_wt_ref (its layer weights do not broadcast per cell)
+            raise ValueError("methane_bands cannot vary z_wt_ref")
+        for f in given:
+            tables[f] = [float(bands.get(b, {}).get(f, getattr(P, f))) for b in CH4_BANDS]
+    for f, t in tables.items():
+        setattr(out, "ch4b_" + f, np.asarray(t, np.float64))
+    out.flags |= FLAG_CH4_BANDS
+    return out
+
+
 def header_struct_text() -> str:
     lines = ["/* Parameter record of the hourly step (all double; passed by value). */",
              "typedef struct IbisParams {"]
@@ -302,7 +359,8 @@ def header_struct_text() -> str:
                     ("VMAX_MIX", FLAG_VMAX_MIX), ("COEFM_MIX", FLAG_COEFM_MIX), ("GPP_CAPACITY", FLAG_GPP_CAPACITY),
                     ("ACCLIM", FLAG_ACCLIM), ("ACCLIM_LIGHT", FLAG_ACCLIM_LIGHT), ("FROST", FLAG_FROST),
                     ("CAP_SCALE_U", FLAG_CAP_SCALE_U), ("CAP_SCALE_L", FLAG_CAP_SCALE_L),
-                    ("LEAF_ONLY", FLAG_LEAF_ONLY), ("CROP", FLAG_CROP), ("FORGANIC", FLAG_FORGANIC)]:
+                    ("LEAF_ONLY", FLAG_LEAF_ONLY), ("CROP", FLAG_CROP), ("FORGANIC", FLAG_FORGANIC),
+                    ("CH4_BANDS", FLAG_CH4_BANDS)]:
         lines.append(f"#define IBIS_FLAG_{nm} {val}u")
     lines.append(f"#define IBIS_FLAGS_X3 {X3_FLAGS}u   /* any of these selects the IBIS 3.0 kernels */")
     lines.append("")

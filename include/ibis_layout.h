@@ -89,7 +89,8 @@ enum {
     IBIS_STAT_TD = 126,  /* atm.td */
     IBIS_STAT_CROPFRAC = 127,  /* sim.cropfrac */
     IBIS_STAT_FORGANIC = 128,  /* sim.forganic, 6 planes */
-    IBIS_STAT_COUNT = 134
+    IBIS_STAT_CH4_BAND = 134,  /* sim.ch4_band */
+    IBIS_STAT_COUNT = 135
 };
 
 /* FORC */
@@ -435,6 +436,15 @@ typedef struct IbisParams {
     double z_wt_ref;
     double z_tau;
     double tau_oxid;
+    double ch4b_sat_crit[3];
+    double ch4b_z_max[3];
+    double ch4b_r_ch4[3];
+    double ch4b_q10p[3];
+    double ch4b_t_ref[3];
+    double ch4b_z_wt_max[3];
+    double ch4b_z_wt_ref[3];
+    double ch4b_z_tau[3];
+    double ch4b_tau_oxid[3];
     double rwood[12];
     double rroot[12];
     double rgrowth[12];
@@ -551,6 +561,15 @@ typedef struct IbisParams {
     S(z_wt_ref) \
     S(z_tau) \
     S(tau_oxid) \
+    A(ch4b_sat_crit, 3) \
+    A(ch4b_z_max, 3) \
+    A(ch4b_r_ch4, 3) \
+    A(ch4b_q10p, 3) \
+    A(ch4b_t_ref, 3) \
+    A(ch4b_z_wt_max, 3) \
+    A(ch4b_z_wt_ref, 3) \
+    A(ch4b_z_tau, 3) \
+    A(ch4b_tau_oxid, 3) \
     A(rwood, 12) \
     A(rroot, 12) \
     A(rgrowth, 12) \
@@ -580,6 +599,7 @@ typedef struct IbisParams {
 #define IBIS_FLAG_LEAF_ONLY 1048576u
 #define IBIS_FLAG_CROP 2097152u
 #define IBIS_FLAG_FORGANIC 4194304u
+#define IBIS_FLAG_CH4_BANDS 8388608u
 #define IBIS_FLAGS_X3 8384512u   /* any of these selects the IBIS 3.0 kernels */
 
 /* Parameters of the daily cadence (phenology, soil biogeochemistry), all double. */

@@ -7,6 +7,8 @@ accumulators of ``timestepping/loops_gswp3.py`` in float64 NumPy.
 """
 from __future__ import annotations
 
+import types
+
 import numpy as np
 
 from .physics import clip, esat, thomas
@@ -365,17 +367,34 @@ def fire_counters(prog, wsoi0, wisoi0, swilt0, F, P):
 # ---------------------------------------------------------------------------
 
 
+CH4_FIELDS = ("sat_crit", "z_max", "r_ch4", "q10p", "t_ref", "z_wt_max", "z_wt_ref", "z_tau", "tau_oxid")
+FLAG_CH4_BANDS = 1 << 23
+
+
+def methane_params(P, S):
+    """The methane parameters each cell uses: ``P``'s, or under FLAG_CH4_BANDS
+    per-cell arrays of the ``ch4b_*`` tables at the cell's band (STAT ch4_band:
+    0 tropical, 1 temperate, 2 boreal), as biome_methane_params gives every
+    cell its band's values (methane.py:521-563)."""
+    if not P.flags & FLAG_CH4_BANDS:
+        return P
+    band = np.asarray(S["ch4_band"], np.float64)
+    b = np.where(band >= 1.5, 2, np.where(band >= 0.5, 1, 0))
+    return types.SimpleNamespace(**{f: np.asarray(getattr(P, "ch4b_" + f), np.float64)[b] for f in CH4_FIELDS})
+
+
 def wetland_water_table(wsoi, wisoi, hsoi, P, zwt_obs=None):
     """wetland_water_table (methane.py:233-276), with an observed depth (finite
     entries of ``zwt_obs``, clipped to [0, z_max]) in its place where given
-    (methane.py:366-367)."""
+    (methane.py:366-367).  ``P``'s methane fields are scalars or per-cell arrays."""
     theta = clip(wsoi * (1.0 - wisoi) + wisoi, 0.0, 1.0)
     bot = np.cumsum(hsoi)
     top = np.concatenate([[0.0], bot[:-1]])
-    w = np.minimum(np.maximum(P.z_wt_ref - top, 0.0), hsoi)
-    tot = max(np.sum(w), 1e-12)
-    ttop = np.sum(theta * w[None, :], axis=1) / tot
-    wet = clip(ttop / max(P.sat_crit, 1e-6), 0.0, 1.0)
+    zref = np.asarray(P.z_wt_ref, np.float64)
+    w = np.minimum(np.maximum(zref[..., None] - top, 0.0), hsoi)         # (nlayer,) or per cell (ncell, nlayer)
+    tot = np.maximum(np.sum(w, axis=-1), 1e-12)
+    ttop = np.sum(theta * w, axis=1) / tot
+    wet = clip(ttop / np.maximum(P.sat_crit, 1e-6), 0.0, 1.0)
     zwt = P.z_wt_max * (1.0 - wet)
     if zwt_obs is not None:
         zo = np.asarray(zwt_obs, dtype=np.float64)
@@ -394,8 +413,8 @@ def methane(f_inund, rh, tsoi, wsoi, wisoi, hsoi, P, zwt_obs=None):
     tt = np.sum(th, axis=1)
     tth = np.where(tt > 1e-12, np.sum(th * tsoi, axis=1) / np.maximum(tt, 1e-12), tsoi[:, 0])
     zp = np.maximum(zwt, 0.0)
-    rha = np.maximum(rh, 0.0) * np.exp(-zp / max(P.z_tau, 1e-6))
+    rha = np.maximum(rh, 0.0) * np.exp(-zp / np.maximum(P.z_tau, 1e-6))
     q10 = P.q10p ** ((tth - P.t_ref) / 10.0)
     prod = np.maximum(rha, 0.0) * P.r_ch4 * q10 * (tth >= 273.15)
     area = clip(np.maximum(f_inund, 0.0), 0.0, 1.0)
-    return area * prod * np.exp(-zp / max(P.tau_oxid, 1e-6))
+    return area * prod * np.exp(-zp / np.maximum(P.tau_oxid, 1e-6))

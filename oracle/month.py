@@ -21,7 +21,7 @@ from __future__ import annotations
 import numpy as np
 
 from .column import methane as methane_flux
-from .column import wetland_water_table
+from .column import methane_params, wetland_water_table
 
 RH_CONV = np.float64(np.float32(12.0e-3 * 86400.0))
 
@@ -66,6 +66,7 @@ def month_end(wet: dict, prog: dict, stat: dict, ch4_sum, ayco2mic, rh0, ndays, 
     inundated fraction ``scale``, optionally with the CH4 carbon taken out of
     Rh.  Returns (wet, ayco2mic, take)."""
     a0 = wet["annual"]
+    P = methane_params(P, stat)
     if from_mean:
         new = methane_step_from_mean(wet, ch4_sum / ndays, prog["wsoi"], prog["wisoi"], hsoi, ndays, P, zwt_obs)
     else:

@@ -16,7 +16,7 @@ import numpy as np
 from .physics import clip, cube, setsoi, fwetcal, cascade, radiation, evap_intercepted, FLAG_GPP_CAPACITY
 from .canopy import aero_geometry, transfer, weight_veg, weight_snow, stomata, turvap
 from .column import (snow_block, water_bounds, soil_water, soil_heat, phase_change, puddle_phase,
-                     fire_counters, methane)
+                     fire_counters, methane, methane_params)
 
 FLAG_BEDROCK = 1 << 0
 FLAG_SUNSHADE_U = 1 << 2
@@ -261,8 +261,8 @@ def step(prog, S, F, P, acc=None):
         if P.flags & FLAG_CH4:
             rh = S["tco2mic"] * np.float64(np.float32(12.0e-3 * 86400.0))
             zo = S["zwt_obs"] if P.flags & FLAG_ZWT_OBS else None
-            acc_new["ch4"] = acc_new["ch4"] + methane(S["f_inund"], rh, new["tsoi"], new["wsoi"], new["wisoi"], hsoi, P,
-                                                      zo) * w
+            acc_new["ch4"] = acc_new["ch4"] + methane(S["f_inund"], rh, new["tsoi"], new["wsoi"], new["wisoi"], hsoi,
+                                                      methane_params(P, S), zo) * w
         if P.flags & FLAG_SOIL_MEANS:
             acc_new["tsoi_mean"] = acc_new["tsoi_mean"] + new["tsoi"] * w
             acc_new["wsoi_mean"] = acc_new["wsoi_mean"] + new["wsoi"] * w

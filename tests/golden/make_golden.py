@@ -791,6 +791,68 @@ def write_methane_case(seed=21, ndays=31):
     print(f"wrote {path}: {len(out)} arrays, {os.path.getsize(path)} bytes")
 
 
+def write_methane_bands_case(seed=21, ndays=31):
+    """tests/golden/methane_bands.npz: the reference's wetland methane with
+    per-cell parameters by biome (``biome_methane_params``,
+    bgc/methane.py:521-563) on the 16-cell checkpoint's soil state: the
+    latitude rule alone (the validated production constants), with Koeppen
+    wetland types overriding it in some cells, and the release parameter
+    file's methane section and ``methane_bands`` (loaded by the reference's own
+    loader) -- the per-cell parameters, water table, flux (with and without an
+    observed depth) and ``methane_step``."""
+    import json
+    from ibis.bgc import methane as M
+    from ibis.io.physics_params import load_physics_params, build_methane_params
+    from ibis.io.restart import load_state
+    n = 16
+    st, _ = load_state(os.path.join(HERE, "restart_16cells.npz"),
+                       create_ibis_state(GridConfig(nlon=1, nlat=1, npoi=n, nbedrock=3)))
+    so = st.soil
+    tsoi, wsoi, wisoi = (np.asarray(x, np.float64) for x in (so.tsoi, so.wsoi, so.wisoi))
+    hsoi = np.asarray(so.hsoi, np.float64)[:tsoi.shape[1]]
+    rng = np.random.Generator(np.random.PCG64(seed))
+    tsoi = tsoi.copy()
+    tsoi[4:7] = 270.0 + rng.uniform(0.0, 6.0, (3, tsoi.shape[1]))
+    f_inund = rng.uniform(0.0, 1.0, n)
+    rh = rng.uniform(0.0, 5e-3, n)
+    zwt_obs = rng.uniform(-0.3, 5.0, n)
+    zwt_obs[rng.uniform(size=n) < 0.4] = np.nan
+    annual0 = rng.uniform(0.0, 1e-2, n)
+    # latitudes on and around the biome edges; Koeppen types (-1: the latitude rule)
+    lat = np.array([-60.0, -30.0, -29.999, -10.0, 0.0, 10.0, 29.999, 30.0, 45.0, 59.999, 60.0, 65.0, 70.0, 75.0,
+                    -45.0, 20.0])
+    band_index = np.array([-1, 0, 1, -1, 2, -1, -1, 0, 2, -1, 1, -1, 0, -1, 2, -1])
+    d = load_physics_params(os.path.join(REF, "configs/params/params_31s_ch4h.yaml"))
+    base, bands = build_methane_params(d), d["methane_bands"]
+    out = {"in.tsoi": tsoi, "in.wsoi": wsoi, "in.wisoi": wisoi, "in.hsoi": hsoi, "in.f_inund": f_inund, "in.rh": rh,
+           "in.zwt_obs": zwt_obs, "in.annual0": annual0, "in.ndays": np.asarray(ndays), "in.lat": lat,
+           "in.band_index": band_index, "in.bands": np.asarray(json.dumps(bands))}
+    fields = ("sat_crit", "z_max", "r_ch4", "q10p", "t_ref", "z_wt_max", "z_wt_ref", "z_tau", "tau_oxid")
+    for f in fields:
+        out[f"base.default.{f}"] = np.asarray(float(getattr(M.MethaneParams(), f)))
+        out[f"base.release.{f}"] = np.asarray(float(getattr(base, f)))
+    variants = {"biome": (M.biome_methane_params(_a(lat)), "default", False, False),
+                "biome_koppen": (M.biome_methane_params(_a(lat), band_index=band_index), "default", True, False),
+                "release": (M.biome_methane_params(_a(lat), base=base, bands=bands, band_index=band_index),
+                            "release", True, True)}
+    a = lambda x: np.asarray(x, np.float64)
+    for tag, (p, b, koppen, with_bands) in variants.items():
+        out[f"meta.{tag}"] = np.asarray([b, str(int(koppen)), str(int(with_bands))])
+        for f in fields:
+            out[f"param.{tag}.{f}"] = np.broadcast_to(a(getattr(p, f)), (n,)).copy()
+        out[f"{tag}.zwt"] = a(M.wetland_water_table(_a(wsoi), _a(wisoi), _a(hsoi), p))
+        out[f"{tag}.flux"] = a(M.methane_flux(_a(f_inund), _a(rh), _a(tsoi), _a(wsoi), _a(wisoi), _a(hsoi), p))
+        out[f"{tag}.flux_obs"] = a(M.methane_flux(_a(f_inund), _a(rh), _a(tsoi), _a(wsoi), _a(wisoi), _a(hsoi), p,
+                                                  zwt_obs=_a(zwt_obs)))
+        m0 = M.MethaneState(flux=_a(np.zeros(n)), annual=_a(annual0), zwt=_a(np.zeros(n)))
+        ms = M.methane_step(m0, _a(f_inund), _a(rh), _a(tsoi), _a(wsoi), _a(wisoi), _a(hsoi), ndays, p)
+        for leaf in ("flux", "annual", "zwt"):
+            out[f"{tag}.step.{leaf}"] = a(getattr(ms, leaf))
+    path = os.path.join(HERE, "methane_bands.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path}: {len(out)} arrays, {os.path.getsize(path)} bytes")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--only", default=None)
@@ -810,6 +872,8 @@ def main():
         write_observed_sw_case()
     if args.only in (None, "wetland_area"):
         write_wetland_case()
+    if args.only in (None, "methane_bands"):
+        write_methane_bands_case()
     if args.only in (None, "day_parts"):
         write_parts_case()
     if args.only in (None, "days_modules"):
@@ -821,7 +885,7 @@ def main():
     for name in X3_CASES:
         if args.only in (None, name):
             write_x3_case(name)
-    if args.only in ("restart_leaves", "restart_1996", "diurnal", "days", "methane_month", "observed_sw", "wetland_area",
+    if args.only in ("restart_leaves", "restart_1996", "diurnal", "days", "methane_month", "observed_sw", "wetland_area", "methane_bands",
                      "day_parts", "days_modules", "days_release", "restart_modules") + tuple(X3_CASES):
         return
     for name, spec in CASES.items():

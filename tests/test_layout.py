@@ -17,7 +17,7 @@ def test_layout_header_is_current():
 
 
 def test_plane_counts():
-    assert L.N_PROG == 71 and L.N_STAT == 134 and L.N_FORC == 12
+    assert L.N_PROG == 71 and L.N_STAT == 135 and L.N_FORC == 12
     assert L.N_DIAG == 111 and L.N_ACC == 52
     assert L.leading_dim(1) == 32 and L.leading_dim(95333) % 32 == 0
 

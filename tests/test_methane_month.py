@@ -184,3 +184,165 @@ def test_device_hourly_ch4_with_observed_water_table(cuda_lib):
         for h in range(nh):
             prog, _, acc2 = oracle.step(prog, stat, c.forcing_at(h), P2, acc2)
     assert np.any(np.abs(acc2["ch4"] - acc["ch4"]) > 1e-6 * np.abs(acc["ch4"]).max())
+
+
+# ---------------------------------------------------------------------------
+# per-cell methane parameters by biome (biome_methane_params, methane.py:521-563)
+# ---------------------------------------------------------------------------
+BANDS_GOLD = os.path.join(HERE, "golden", "methane_bands.npz")
+BAND_TAGS = ("biome", "biome_koppen", "release")
+
+
+def band_params(z, tag):
+    """StepParams with the tag's per-band tables (FLAG_CH4_BANDS) and the ch4_band plane,
+    built by ibis_b200.params from the tag's base values, Koeppen types and bands."""
+    import json
+    from ibis_b200.params import StepParams, methane_band_index, with_methane_bands
+    base, koppen, with_bands = (str(x) for x in z[f"meta.{tag}"])
+    P = StepParams()
+    for f in MP_FIELDS:
+        setattr(P, f, float(z[f"base.{base}.{f}"]))
+    bands = json.loads(str(z["in.bands"])) if with_bands == "1" else None
+    band = methane_band_index(z["in.lat"], z["in.band_index"] if koppen == "1" else None)
+    return with_methane_bands(P, bands), band
+
+
+@pytest.mark.parametrize("tag", BAND_TAGS)
+def test_band_tables_give_the_reference_per_cell_parameters(tag):
+    from oracle.column import methane_params
+    z = dict(np.load(BANDS_GOLD))
+    P, band = band_params(z, tag)
+    per_cell = methane_params(P, {"ch4_band": band})
+    for f in MP_FIELDS:
+        np.testing.assert_array_equal(np.broadcast_to(getattr(per_cell, f), band.shape), z[f"param.{tag}.{f}"],
+                                      err_msg=f)
+
+
+@pytest.mark.parametrize("tag", BAND_TAGS)
+def test_oracle_matches_reference_per_band_methane(tag):
+    from oracle.column import methane_params
+    z = dict(np.load(BANDS_GOLD))
+    P, band = band_params(z, tag)
+    m = methane_params(P, {"ch4_band": band})
+    t, w, i, h = z["in.tsoi"], z["in.wsoi"], z["in.wisoi"], z["in.hsoi"]
+    close(OM.wetland_water_table(w, i, h, m), z[f"{tag}.zwt"])
+    close(OM.methane_flux(z["in.f_inund"], z["in.rh"], t, w, i, h, m), z[f"{tag}.flux"])
+    close(OM.methane_flux(z["in.f_inund"], z["in.rh"], t, w, i, h, m, z["in.zwt_obs"]), z[f"{tag}.flux_obs"])
+    m0 = dict(flux=np.zeros_like(z["in.annual0"]), annual=z["in.annual0"], zwt=np.zeros_like(z["in.annual0"]))
+    ms = OM.methane_step(m0, z["in.f_inund"], z["in.rh"], t, w, i, h, int(z["in.ndays"]), m)
+    for leaf in ("flux", "annual", "zwt"):
+        close(ms[leaf], z[f"{tag}.step.{leaf}"])
+
+
+def test_band_tables_refuse_what_the_reference_cannot_run():
+    from ibis_b200.params import StepParams, with_methane_bands
+    with pytest.raises(KeyError):
+        with_methane_bands(StepParams(), {"boreal": {"r_ch5": 0.1}})
+    with pytest.raises(ValueError):
+        with_methane_bands(StepParams(), {"boreal": {"z_wt_ref": 0.3}})
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("tag", BAND_TAGS)
+def test_device_month_per_band_matches_reference(cuda_lib, tag):
+    """ibis_month_end_f64 from the end-of-month state with per-band parameters
+    (FLAG_CH4_BANDS, the STAT ch4_band plane) against the reference's own
+    methane_step under biome_methane_params: 1e-12."""
+    import torch
+    from ibis_b200 import dropin, restart
+    from ibis_b200.columns import Columns
+    from ibis_b200.daily import DayLoop
+    from ibis_b200.params import DayParams
+    z = dict(np.load(BANDS_GOLD))
+    n = 16
+    Pb, band = band_params(z, tag)
+    leaves, _, _ = restart.load(CKPT)
+    tree = restart.as_tree(leaves)
+    prog = dropin._leaf_dict(tree, "PROG", n)
+    stat = dropin._leaf_dict(tree, "STAT", n)
+    prog.update(tsoi=z["in.tsoi"], wsoi=z["in.wsoi"], wisoi=z["in.wisoi"])
+    stat.update(f_inund=z["in.f_inund"], tco2mic=z["in.rh"] / OM.RH_CONV, ch4_band=band)
+    P = restart.params_from_leaves(leaves)
+    np.testing.assert_array_equal(np.asarray(P.hsoi), z["in.hsoi"])
+    for f in MP_FIELDS:
+        setattr(P, f, getattr(Pb, f))
+        setattr(P, "ch4b_" + f, getattr(Pb, "ch4b_" + f))
+    P.flags |= Pb.flags
+    cols = Columns.from_host(prog, stat, dtype=torch.float64, acc=True)
+    loop = DayLoop(cols, P, DayParams(), {})
+    loop.set_wet(dict(flux=np.zeros(n), annual=z["in.annual0"].copy(), zwt=np.zeros(n)))
+    loop.begin_month()
+    loop.end_month(int(z["in.ndays"]), from_mean=False)
+    torch.cuda.synchronize()
+    got = loop.wet_host()
+    for leaf in ("flux", "annual", "zwt"):
+        close(got[leaf], z[f"{tag}.step.{leaf}"])
+
+
+@pytest.mark.gpu
+def test_device_hourly_ch4_per_band(cuda_lib):
+    """The hourly step's CH4 accumulator with per-band parameters (the release
+    file's methane_bands over Koeppen and latitude bands) equals the oracle
+    step's, float64 over six hours of the day_mixed case (1e-9) and float32
+    within 1e-5 of the largest sum; and the bands matter."""
+    import json
+    import torch
+    import oracle
+    from goldens import Case
+    from ibis_b200.columns import Columns
+    from ibis_b200.params import FLAG_ACC, FLAG_CH4, FLAG_CH4_BANDS, FLAG_KAHAN, methane_band_index, with_methane_bands
+    z = dict(np.load(BANDS_GOLD))
+    c = Case("day_mixed")
+    n = c.ncell
+    rng = np.random.Generator(np.random.PCG64(9))
+    stat = dict(c.stat)
+    stat["f_inund"] = rng.uniform(0.0, 1.0, n)
+    stat["ch4_band"] = methane_band_index(rng.uniform(-60.0, 80.0, n), rng.integers(-1, 3, n))
+    P = with_methane_bands(c.params, json.loads(str(z["in.bands"])))
+    P.flags = (P.flags | FLAG_ACC | FLAG_CH4) & ~FLAG_KAHAN
+    nh = min(6, c.nhour)
+    prog, acc = dict(c.prog), oracle.new_acc(n)
+    with np.errstate(all="ignore"):
+        for h in range(nh):
+            prog, _, acc = oracle.step(prog, stat, c.forcing_at(h), P, acc)
+    for dtype, rtol in ((torch.float64, 1e-9), (torch.float32, None)):
+        Pd = P.copy()
+        if dtype == torch.float32:
+            Pd.flags |= FLAG_KAHAN
+        cols = Columns.from_host(c.prog, stat, dtype=dtype, acc=True)
+        cols.run(cols.forcing(c.forc, 0, nh), Pd)
+        torch.cuda.synchronize()
+        got = cols.acc_host()["ch4"]
+        if rtol:
+            np.testing.assert_allclose(got, acc["ch4"], rtol=rtol, atol=1e-300)
+        else:
+            assert np.max(np.abs(got - acc["ch4"])) <= 1e-5 * np.abs(acc["ch4"]).max()
+    P2 = P.copy()
+    P2.flags &= ~FLAG_CH4_BANDS
+    prog, acc2 = dict(c.prog), oracle.new_acc(n)
+    with np.errstate(all="ignore"):
+        for h in range(nh):
+            prog, _, acc2 = oracle.step(prog, stat, c.forcing_at(h), P2, acc2)
+    assert np.any(np.abs(acc2["ch4"] - acc["ch4"]) > 1e-3 * np.abs(acc["ch4"]).max())
+
+
+@pytest.mark.parametrize("tag", BAND_TAGS)
+def test_dropin_maps_per_cell_methane_parameters(tag):
+    """The drop-in reads a reference MethaneParams with per-cell fields (as
+    biome_methane_params returns it) into band tables and a band plane that
+    give every cell its own values back."""
+    import types as _t
+    from ibis_b200 import dropin
+    from ibis_b200.params import StepParams, FLAG_CH4_BANDS
+    from oracle.column import methane_params
+    z = dict(np.load(BANDS_GOLD))
+    mp = _t.SimpleNamespace(**{f: z[f"param.{tag}.{f}"] for f in MP_FIELDS})
+    P, stat = StepParams(), {}
+    dropin.apply_methane(P, stat, mp, 16)
+    assert P.flags & FLAG_CH4_BANDS
+    got = methane_params(P, stat)
+    for f in MP_FIELDS:
+        np.testing.assert_array_equal(np.broadcast_to(getattr(got, f), (16,)), z[f"param.{tag}.{f}"], err_msg=f)
+    scalar = _t.SimpleNamespace(**{f: float(z[f"base.default.{f}"]) for f in MP_FIELDS})
+    dropin.apply_methane(P, stat, scalar, 16)
+    assert not P.flags & FLAG_CH4_BANDS and P.r_ch4 == float(z["base.default.r_ch4"])
