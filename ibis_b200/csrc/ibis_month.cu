@@ -39,7 +39,8 @@ int month_end(const R* prog, const R* stat, const R* acc, R* wet, R* dayst, cons
     if (hp->flags & ~(unsigned)IBIS_FLAG_ZWT_OBS & ~(IBIS_FLAG_BEDROCK | IBIS_FLAG_H2O_CONSISTENT |
                                                    IBIS_FLAG_SUNSHADE_U | IBIS_FLAG_SUNSHADE_L | IBIS_FLAG_ACC |
                                                    IBIS_FLAG_CH4 | IBIS_FLAG_SOIL_MEANS | IBIS_FLAG_DIAG |
-                                                   IBIS_FLAG_KAHAN | IBIS_FLAG_ETPARTS | IBIS_FLAG_NEEPARTS))
+                                                   IBIS_FLAG_KAHAN | IBIS_FLAG_ETPARTS | IBIS_FLAG_NEEPARTS |
+                                                   IBIS_FLAGS_X3 | IBIS_FLAG_CH4_BANDS))
         return -EINVAL;
     if (!(hp->dtime > 0.0)) return -EINVAL;
     if (ncell == 0) return 0;
