@@ -200,10 +200,11 @@ class Columns:
         tensor shaped like ``prog``), copy the state after the last hour out:
         ``ibis_step_host_f32``, which overlaps the copies with the steps -- in
         groups of ``group`` columns for batches of several waves (0: twenty
-        groups), or, for smaller ones, in chunks of ``chunk`` hours (0: 4 hours
-        growing by 1.75).  Asynchronous on ``stream``; read ``host_prog`` after
-        synchronising it.  FP32 columns only; a two-kernel launch mode runs the
-        library's fused choice."""
+        groups), each group's hours in chunks (``chunk`` hours each, ``-c``:
+        ``c`` hours then the rest; 0: a third of the hours then the rest, or for
+        a batch of about one wave 4 hours growing by 1.75).  Asynchronous on
+        ``stream``; read ``host_prog`` after synchronising it.  FP32 columns
+        only; a two-kernel launch mode runs the library's fused choice."""
         if self.dtype != torch.float32:
             raise ValueError("run_host runs FP32 columns")
         if host_forc.device.type != "cpu" or host_forc.dtype != self.dtype or not host_forc.is_pinned():

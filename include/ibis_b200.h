@@ -96,8 +96,10 @@ int ibis_step_split_noalloc_f32(float* prog, const float* stat, const float* for
  *     groups step;
  *   - a smaller batch (group 0) is one group whose hours are cut into chunks,
  *     each chunk's copy overlapping the steps of the chunk before.
- *   `chunk` sets the hours per chunk (0: all hours for several groups; 4 hours
- *   growing by 1.75 per chunk for one group); groups x chunks <= 256.
+ *   `chunk` sets the hours per chunk: c > 0 equal chunks of c hours; -c, c
+ *   hours then the rest; 0, for several groups a third of the hours then the
+ *   rest (all groups' first chunks are copied before any group's second), for
+ *   one group 4 hours growing by 1.75 per chunk; groups x chunks <= 256.
  *   host_forc  [nstep][IBIS_FORC_COUNT][ld]  pinned HOST: hourly forcing
  *   forc       [nstep][IBIS_FORC_COUNT][ld]  DEVICE: where the forcing lands
  *   host_prog  [IBIS_PROG_COUNT][ld] pinned HOST, or NULL: the state after the

@@ -44,7 +44,7 @@ def test_host_step_rejects_bad_arguments(so):
     assert f(*args, 40, 32, 1, p, NUL, 0, 0, -1, NUL) == EINVAL      # ncell > ld
     assert f(*args, 30, 32, 1, p, NUL, 48, 0, -1, NUL) == EINVAL     # group not a multiple of 32
     assert f(*args, 30, 32, 1, p, NUL, -32, 0, -1, NUL) == EINVAL
-    assert f(*args, 30, 32, 1, p, NUL, 0, -1, -1, NUL) == EINVAL     # negative chunk
+    assert f(*args, 30, 32, 1, p, NUL, 0, -2 ** 31, -1, NUL) == EINVAL   # no such first chunk
     split = next(c["id"] for c in lib.configs() if c["form"] == "split")
     assert f(*args, 30, 32, 1, p, NUL, 0, 0, split, NUL) == EINVAL   # needs scratch
     assert f(*args, 30, 32, 1, p, NUL, 0, 0, 99, NUL) == EINVAL
