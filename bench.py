@@ -513,10 +513,9 @@ def run_ours(args):
     gen_out = torch.empty_like(forc)
 
     def e2e_daily_day():
-        d_daily.copy_(h_daily, non_blocking=True)
-        _forcing.hourly_forcing(d_daily, lat_d, n, jday0=172, seed=5, out=gen_out, stream=stream)
-        cols.run(gen_out, P, stream=stream)
-        h_prog.copy_(cols.prog, non_blocking=True)
+        # ibis_day_host_f32: per group of columns the daily weather in, the
+        # hourly forcing generated, the day stepped and the state out
+        cols.run_host_daily(h_daily, lat_d, P, 172, seed=5, host_prog=h_prog, stream=stream)
 
     e2e_daily_day()
     ms_e2e_daily = float(np.sum(timed(e2e_daily_day, args.steps))) / args.steps
@@ -594,6 +593,7 @@ def run_ours(args):
                                   "h2d_bytes_per_step": int(h_daily.numel() * 4),
                                   "d2h_bytes_per_step": int(h_prog.numel() * 4),
                                   "forcing_generation_ms": ms_gen,
+                                  "entry": "Columns.run_host_daily -> ibis_day_host_f32",
                                   "note": "daily weather in, hourly forcing generated on the GPU by the reference's "
                                           "diurnal algorithm (not the hourly generator of the workload above)"},
             "gpu_launches": args.steps * (1 if cfg_desc["form"] == "fused" else 2 * HOURS),

@@ -238,6 +238,53 @@ class Columns:
         _lib.check(rc, "ibis_step_host_f32")
         return self
 
+    def run_host_daily(self, host_daily: torch.Tensor, lat: torch.Tensor, params: StepParams, jday0: int,
+                       day0: int = 0, seed: int = 0, observed_fira: bool = False,
+                       host_prog: torch.Tensor | None = None, group: int = 0, stream=None):
+        """Advance the columns through the days of ``host_daily`` (a pinned host
+        tensor ``(nday, IBIS_DAILY_COUNT, ld)`` of daily weather), the hourly
+        forcing generated on the device as ``forcing.hourly_forcing`` generates
+        it (``lat``: ``(ld,)`` float32 degrees on the device), and copy the state
+        after the last hour to ``host_prog``: ``ibis_day_host_f32``, in groups of
+        columns whose copies and generation overlap the other groups' hours.
+        Asynchronous on ``stream``.  FP32 columns only."""
+        if self.dtype != torch.float32:
+            raise ValueError("run_host_daily runs FP32 columns")
+        if (host_daily.device.type != "cpu" or host_daily.dtype != torch.float32 or not host_daily.is_pinned()
+                or host_daily.dim() != 3 or host_daily.shape[1:] != (L.N_DAILY, self.ld)
+                or not host_daily.is_contiguous()):
+            raise ValueError(f"host daily weather must be a pinned contiguous (nday, {L.N_DAILY}, {self.ld}) float32 "
+                             "CPU tensor")
+        if lat.shape != (self.ld,) or lat.dtype != torch.float32 or lat.device != self.device:
+            raise ValueError(f"lat must be a ({self.ld},) float32 tensor on the columns' device")
+        if host_prog is not None and (host_prog.device.type != "cpu" or not host_prog.is_pinned()
+                                      or host_prog.shape != self.prog.shape or host_prog.dtype != self.dtype
+                                      or not host_prog.is_contiguous()):
+            raise ValueError("host_prog must be a pinned contiguous CPU tensor shaped like prog")
+        nday = host_daily.shape[0]
+        nh = int(round(86400.0 / params.dtime))
+        if getattr(self, "_host_daily", None) is None or self._host_daily.shape[0] < nday:
+            self._host_daily = torch.empty((nday, L.N_DAILY, self.ld), dtype=torch.float32, device=self.device)
+        if getattr(self, "_host_forc", None) is None or self._host_forc.shape[0] < nday * nh:
+            self._host_forc = torch.empty((nday * nh, L.N_FORC, self.ld), dtype=self.dtype, device=self.device)
+        cfg = self.launch_config(nday * nh)
+        if _lib.configs()[cfg]["form"] != "fused":
+            cfg = -1
+        flags = params.flags & ~FLAG_DIAG if self.diag is None else params.flags | FLAG_DIAG
+        if self.acc is None:
+            flags &= ~_ACC_FLAGS
+        p = params.to_c()
+        p.flags = flags
+        if stream is None:
+            stream = torch.cuda.current_stream(self.device)
+        rc = _lib.load().ibis_day_host_f32(_ptr(self.prog), _ptr(self.stat), _ptr(host_daily), _ptr(self._host_daily),
+                                           _ptr(lat), _ptr(self._host_forc), _ptr(self.diag), _ptr(self.acc),
+                                           _ptr(host_prog), self.ncell, self.ld, nday, int(jday0), int(day0),
+                                           int(seed) & 0xFFFFFFFF, 1 if observed_fira else 0, ctypes.byref(p),
+                                           _ptr(self.status), int(group), int(cfg), ctypes.c_void_p(stream.cuda_stream))
+        _lib.check(rc, "ibis_day_host_f32")
+        return self
+
     @staticmethod
     def chunk_schedule(nstep: int, chunk="auto"):
         """Hours per host-to-device chunk.  An integer gives equal chunks;

@@ -20,6 +20,10 @@ IBIS_SUN_CONFIGS(IBIS_EXTERN, 9)
 IBIS_X3_CONFIGS(IBIS_EXTERN_X3, 6)
 IBIS_X3_CONFIGS(IBIS_EXTERN_X3, 9)
 #undef IBIS_EXTERN_X3
+// the forcing generator of ibis_diurnal_f32.cu on a range of cells
+int diurnal(const float* daily, const float* lat, const float* sw_obs, const unsigned char* use, float* forc,
+            int ncell, int ld, int nday, int jday0, int day0, float dtime, unsigned int seed, unsigned int flags,
+            void* stream, const char* what, int cell0);
 }  // namespace ibis
 
 extern "C" int ibis_step_f32(float* prog, const float* stat, const float* forc, float* diag, float* acc, int ncell,
@@ -293,6 +297,91 @@ extern "C" int ibis_step_host_f32(float* prog, const float* stat, const float* h
     // the caller's stream continues after every queued group's hours and copies,
     // on failure too, so that nothing of this call is still running when the
     // caller's stream reaches its next work
+    cudaError_t j = cudaSuccess;
+    for (int g = 0; g < queued && j == cudaSuccess; ++g) j = cudaStreamWaitEvent(user, h.stepped[g], 0);
+    if (j == cudaSuccess) j = cudaEventRecord(h.out_done, h.d2h);
+    if (j == cudaSuccess) j = cudaStreamWaitEvent(user, h.out_done, 0);
+    if (what) return host_error(e, what);
+    if (rc) return rc;
+    if (j != cudaSuccess) return host_error(j, "stream join");
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Days from host daily weather: per group of columns, the group's days of
+// weather copied in (tens of bytes per cell-day), its hourly forcing generated
+// on the device, its hours stepped and its state copied out, the groups on the
+// library's streams so one group's generation and copies overlap the others'
+// hours.
+// ---------------------------------------------------------------------------
+extern "C" int ibis_day_host_f32(float* prog, const float* stat, const float* host_daily, float* daily,
+                                 const float* lat, float* forc, float* diag, float* acc, float* host_prog, int ncell,
+                                 int ld, int nday, int jday0, int day0, unsigned int seed, unsigned int dflags,
+                                 const IbisParams* params, int* status, int group, int config, void* stream) {
+    if (!prog || !stat || !host_daily || !daily || !lat || !forc || !params) return -EINVAL;
+    if (ncell < 0 || nday < 0 || ld < ncell || ld % 32 || group < 0 || group % 32) return -EINVAL;
+    if (config < -1 || config >= ibis::kNumConfigs || (config >= 0 && ibis::kConfigs[config].form != 0))
+        return -EINVAL;
+    if (day0 < 0 || jday0 < 1 || jday0 > 366 || (dflags & ~IBIS_DIURNAL_OBSERVED_FIRA)) return -EINVAL;
+    if (!(params->dtime > 0.0)) return -EINVAL;
+    const int nh = (int)(86400.0 / params->dtime);
+    if (nh < 1 || nh > 254 || (double)nh * params->dtime != 86400.0) return -EINVAL;
+    if (ncell == 0) return 0;
+    const int nstep = nday * nh;
+    const int cfg = config >= 0 ? config : (nstep >= ibis::kAccSmemMinSteps ? ibis::kLongFused : ibis::kDefaultFused);
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return -ENODEV;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) return -ENODEV;
+    if (group == 0) {
+        const int block = ibis::kConfigs[cfg].block;
+        const double wave = (double)sms * block * ibis::kConfigs[cfg].minb;
+        group = ncell > kHostGroupWaves * wave
+                    ? ((ncell + kHostAutoGroups - 1) / kHostAutoGroups + block - 1) / block * block
+                    : (ncell + 31) / 32 * 32;
+    }
+    const int min_group = ((ncell + kHostMaxGroups - 1) / kHostMaxGroups + 31) / 32 * 32;
+    if (group < min_group) group = min_group;
+    const int ngroup = (ncell + group - 1) / group;
+    std::lock_guard<std::mutex> lock(g_host_mu);
+    HostPipe& h = g_host[dev];
+    cudaError_t e = host_pipe_init(h);
+    if (e != cudaSuccess) return host_error(e, "stream setup");
+    cudaStream_t user = (cudaStream_t)stream;
+    if ((e = cudaEventRecord(h.start, user)) != cudaSuccess) return host_error(e, "event record");
+    e = cudaStreamWaitEvent(h.h2d, h.start, 0);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(h.d2h, h.start, 0);
+    for (int k = 0; k < kHostStreams && k < ngroup && e == cudaSuccess; ++k)
+        e = cudaStreamWaitEvent(h.comp[k], h.start, 0);
+    if (e != cudaSuccess) return host_error(e, "stream wait");
+    const size_t pitch = (size_t)ld * sizeof(float);
+    int rc = 0, queued = 0;
+    const char* what = nullptr;
+    for (int g = 0; g < ngroup && !rc && !what; ++g) {
+        const int c0 = g * group, n = ncell - c0 < group ? ncell - c0 : group;
+        cudaStream_t cs = h.comp[g % kHostStreams];
+        if (nday > 0) {
+            e = cudaMemcpy2DAsync(daily + c0, pitch, host_daily + c0, pitch, (size_t)n * sizeof(float),
+                                  (size_t)nday * IBIS_DAILY_COUNT, cudaMemcpyHostToDevice, h.h2d);
+            if (e == cudaSuccess) e = cudaEventRecord(h.landed[g], h.h2d);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(cs, h.landed[g], 0);
+            if (e != cudaSuccess) { what = "weather copy"; break; }
+            rc = ibis::diurnal(daily + c0, lat + c0, nullptr, nullptr, forc + c0, n, ld, nday, jday0, day0,
+                               (float)params->dtime, seed, dflags, cs, "ibis_day_host_f32", c0);
+            if (!rc)
+                rc = ibis::hourly_step<float>(prog + c0, stat + c0, forc + c0, diag ? diag + c0 : nullptr,
+                                              acc ? acc + c0 : nullptr, n, ld, nstep, params, status, cs, nullptr,
+                                              cfg, c0);
+        }
+        const cudaError_t r = cudaEventRecord(h.stepped[g], cs);
+        if (r != cudaSuccess) { what = "event record"; e = r; break; }
+        queued = g + 1;
+        if (rc || !host_prog) continue;
+        e = cudaStreamWaitEvent(h.d2h, h.stepped[g], 0);
+        if (e == cudaSuccess)
+            e = cudaMemcpy2DAsync(host_prog + c0, pitch, prog + c0, pitch, (size_t)n * sizeof(float), IBIS_PROG_COUNT,
+                                  cudaMemcpyDeviceToHost, h.d2h);
+        if (e != cudaSuccess) what = "state copy";
+    }
     cudaError_t j = cudaSuccess;
     for (int g = 0; g < queued && j == cudaSuccess; ++g) j = cudaStreamWaitEvent(user, h.stepped[g], 0);
     if (j == cudaSuccess) j = cudaEventRecord(h.out_done, h.d2h);

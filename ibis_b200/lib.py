@@ -76,6 +76,8 @@ SIGNATURES = {
     "ibis_wetland_features": (ctypes.c_int, [ctypes.POINTER(IbisWetlandBuilderC)] + [_V] * 4),
     "ibis_wetland_learned": (ctypes.c_int, [ctypes.POINTER(IbisForestC), _V] + [ctypes.c_int] * 2 + [_V] * 7
                              + [ctypes.c_int] + [_V] * 3),
+    "ibis_day_host_f32": (ctypes.c_int, [_V] * 9 + [ctypes.c_int] * 5 + [ctypes.c_uint] * 2 + [_P, _V]
+                          + [ctypes.c_int] * 2 + [_V]),
     "ibis_step_host_f32": (ctypes.c_int, [_V] * 7 + [ctypes.c_int] * 3 + [_P, _V] + [ctypes.c_int] * 3 + [_V]),
     "ibis_ensemble_f32": (ctypes.c_int, [_E, _P, ctypes.c_int, ctypes.c_void_p]),
     "ibis_ensemble_hours_f32": (ctypes.c_int, [_E, _P, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),

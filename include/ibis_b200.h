@@ -117,6 +117,27 @@ int ibis_step_host_f32(float* prog, const float* stat, const float* host_forc, f
                        float* host_prog, int ncell, int ld, int nstep, const IbisParams* params, int* status,
                        int group, int chunk, int config, void* stream);
 
+/* Days of the step from daily weather in HOST memory, the state read back to
+ * HOST memory: per group of columns (`group` as for ibis_step_host_f32), the
+ * group's daily weather copied in, its hourly forcing generated on the device
+ * (as ibis_diurnal_f32 generates it, the variates keyed by each cell's index
+ * in the caller's numbering, so the forcing equals one call over all cells),
+ * its nday * 86400/dtime hours stepped and its state copied out, on streams of
+ * the library's own so one group's work overlaps the others'.
+ *   host_daily [nday][IBIS_DAILY_COUNT][ld]  pinned HOST: daily weather
+ *   daily      [nday][IBIS_DAILY_COUNT][ld]  DEVICE: where it lands
+ *   lat        [ld] DEVICE: latitude (degrees)
+ *   forc       [nday * 86400/dtime][IBIS_FORC_COUNT][ld] DEVICE: the generated forcing
+ *   jday0, day0, seed, dflags as for ibis_diurnal_f32 (dtime from params);
+ *   other arguments as for ibis_step_host_f32.
+ * Replaces: _run_day_inner's days -- compute_precip_timing + diurnal
+ * (python-port/ibis/physics/weather.py:395-601) and timestep_body / _step_body
+ * (loops_gswp3.py:115-320) -- on host arrays. */
+int ibis_day_host_f32(float* prog, const float* stat, const float* host_daily, float* daily, const float* lat,
+                      float* forc, float* diag, float* acc, float* host_prog, int ncell, int ld, int nday, int jday0,
+                      int day0, unsigned int seed, unsigned int dflags, const IbisParams* params, int* status,
+                      int group, int config, void* stream);
+
 /* A calibration ensemble: nrun runs, each one parameter vector at one site
  * over its own record of hourly forcing.  Per-run buffers use ld_run, per-site
  * buffers ld_site (both multiples of 32, >= the count).

@@ -53,6 +53,18 @@ def test_host_step_rejects_bad_arguments(so):
     assert f(*args, 0, 32, 1, p, NUL, 0, 0, -1, NUL) == 0             # nothing to do
 
 
+def test_day_host_rejects_bad_arguments(so):
+    p = _p()
+    f = so.ibis_day_host_f32
+    a = (DEV, DEV, DEV, DEV, DEV, DEV, NUL, DEV, NUL)
+    assert f(*a, 30, 33, 1, 1, 0, 0, 0, p, NUL, 0, -1, NUL) == EINVAL          # ld not a multiple of 32
+    assert f(*a, 30, 32, 1, 0, 0, 0, 0, p, NUL, 0, -1, NUL) == EINVAL          # day of year 0
+    assert f(*a, 30, 32, 1, 1, 0, 0, 4, p, NUL, 0, -1, NUL) == EINVAL          # unknown generator flag
+    assert f(*a, 30, 32, 1, 1, 0, 0, 0, _p(dtime=7000.0), NUL, 0, -1, NUL) == EINVAL   # not a whole day of steps
+    assert f(DEV, DEV, NUL, DEV, DEV, DEV, NUL, DEV, NUL, 30, 32, 1, 1, 0, 0, 0, p, NUL, 0, -1, NUL) == EINVAL
+    assert f(*a, 0, 32, 1, 1, 0, 0, 0, p, NUL, 0, -1, NUL) == 0                # nothing to do
+
+
 def test_day_kernels_reject_bad_arguments(so):
     p, dp = _p(), ctypes.byref(DayParams().to_c())
     for f in (so.ibis_day_begin_f32, so.ibis_day_begin_f64):

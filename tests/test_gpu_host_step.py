@@ -68,3 +68,35 @@ def test_host_step_reports_cells_in_caller_numbering(cuda_lib):
     torch.cuda.synchronize()
     flagged, first = cols.nonfinite()
     assert flagged and first == bad
+
+
+@pytest.mark.parametrize("group,fira", [(0, False), (640, True), (4992, False)])
+def test_host_days_from_daily_weather_equal_the_device_path(cuda_lib, group, fira):
+    """``ibis_day_host_f32`` (``Columns.run_host_daily``): per group the daily
+    weather in, the forcing generated (variates keyed by the caller's cell
+    numbers), the days stepped and the state out -- equal to generating the
+    forcing over every cell (``forcing.hourly_forcing``) and one step launch,
+    bit for bit."""
+    from ibis_b200 import forcing as _forcing
+    prog, stat, forc, P = _workload()
+    rng = np.random.default_rng(4)
+    nday = 2
+    lat = rng.uniform(-60.0, 80.0, NCELL)
+    w = synth.make_daily_weather(rng, lat, nday)
+    ref = _columns(prog, stat)
+    lat_d = torch.zeros(ref.ld, dtype=torch.float32, device="cuda")
+    lat_d[:NCELL] = torch.from_numpy(lat.astype(np.float32)).cuda()
+    planes = _forcing.daily_planes(w, ref.ld)
+    f = _forcing.hourly_forcing(torch.from_numpy(planes).cuda(), lat_d, NCELL, jday0=100, day0=7, seed=11,
+                                observed_fira=fira)
+    ref.run(f, P)
+    cols = _columns(prog, stat)
+    h_prog = torch.zeros_like(cols.prog, device="cpu").pin_memory()
+    stream = torch.cuda.Stream()
+    cols.run_host_daily(torch.from_numpy(planes).pin_memory(), lat_d, P, 100, day0=7, seed=11, observed_fira=fira,
+                        host_prog=h_prog, group=group, stream=stream)
+    stream.synchronize()
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(cols.prog.cpu().numpy(), ref.prog.cpu().numpy())
+    np.testing.assert_array_equal(cols.acc.cpu().numpy(), ref.acc.cpu().numpy())
+    np.testing.assert_array_equal(h_prog.numpy()[:, :NCELL], ref.prog.cpu().numpy()[:, :NCELL])
