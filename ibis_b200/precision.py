@@ -121,14 +121,19 @@ def _oracle_chunk(task):
 
 
 def report(ncell: int = 1000, nhour: int = 8760, seed: int = 2024, chunk: int = 720, device="cuda",
-           oracle_cells: int = 0, legs=("f32", "f64", "f64_w32")) -> dict:
+           oracle_cells: int = 0, legs=("f32", "f64", "f64_w32"), params: StepParams | None = None) -> dict:
     """Run the legs on the first ``ncell`` columns for ``nhour`` hours; return the
     report (every leg against ``f64``; with ``oracle_cells`` also ``f64`` and
-    ``f32`` against the float64 oracle on the first ``oracle_cells`` columns)."""
+    ``f32`` against the float64 oracle on the first ``oracle_cells`` columns).
+    ``params``: the step's parameters (default: the defaults at 390 ppm CO2);
+    under temperature acclimation the columns get seeded acclimation states."""
+    from .params import FLAG_ACCLIM
     stat, lat, rng = population(ncell, seed)
     f0 = synth.make_forcing(rng, lat, min(chunk, nhour), start_doy=1)
     prog = synth.make_initial(rng, stat, {k: v[0] for k, v in f0.items()})
-    P = StepParams(co2conc=390.0e-6)
+    P = StepParams(co2conc=390.0e-6) if params is None else params.copy()
+    if P.flags & FLAG_ACCLIM:
+        stat = dict(stat, acclim_x=np.random.default_rng(seed + 1).uniform(-12.0, 28.0, ncell))
     P.flags = P.flags | FLAG_SOIL_MEANS
     P64 = P.copy()
     P64.flags = P64.flags & ~FLAG_KAHAN

@@ -81,3 +81,24 @@ def test_f64_kernel_tracks_oracle_for_a_week(cuda_lib):
     assert not bad, bad[:6]
     bad = compare(got, prog, 1e-3) + compare(cols.acc_host(compensated=False), acc, 1e-3)
     assert not bad, bad[:6]
+
+
+@pytest.fixture(scope="module")
+def release_year(cuda_lib):
+    from goldens import Case
+    from ibis_b200.params import FLAG_ACC, FLAG_KAHAN
+    P = Case("release").params.copy()
+    P.flags |= FLAG_ACC | FLAG_KAHAN
+    return precision.report(1000, 8760, legs=("f32", "f64"), params=P)
+
+
+def test_release_parameter_year(release_year):
+    """The same year under the release parameter file's switches (sunlit/shaded
+    canopies, vmax and slope mixing, the NPP split by capacity, per-PFT
+    temperature acclimation): the IBIS 3.0 FP32 kernels against their FP64
+    twins, every annual flux total within 1e-4 (measured: at most 8.7e-6,
+    runoff and sensible heat; GPP 2.2e-7)."""
+    r = release_year
+    assert not any(r["nonfinite"].values())
+    for flux, v in r["fluxes"].items():
+        assert v["total_rel"] < 1e-4, (flux, v)
