@@ -126,8 +126,9 @@ constexpr int kHostStreams = 16;    // compute streams the groups take in turn
 constexpr int kHostMaxGroups = 64;
 constexpr int kHostMaxPieces = 256; // (group, chunk of hours) pairs of one call
 // groups when the caller leaves the size to the library: at 95,333 cells x 24
-// hours a day from host to host took 3.86 ms in 20 groups, 3.94 ms in 16 and
-// 4.2 ms in 8 (the same day with its forcing already on the device: 3.66 ms)
+// hours, with whole days per group, a day from host to host took 3.86 ms in 20
+// groups, 3.94 ms in 16 and 4.2 ms in 8 (the same day with its forcing already
+// on the device: 3.66 ms on that GPU)
 constexpr int kHostAutoGroups = 20;
 // batches of more than this many waves of the launch configuration are cut
 // into groups, smaller ones into chunks of hours.  A day from host to host,
@@ -160,8 +161,8 @@ cudaError_t host_pipe_init(HostPipe& h) {
     return e;
 }
 
-int host_error(cudaError_t e, const char* what) {
-    fprintf(stderr, "ibis_step_host_f32: %s failed: %s\n", what, cudaGetErrorString(e));
+int host_error(cudaError_t e, const char* what, const char* entry = "ibis_step_host_f32") {
+    fprintf(stderr, "%s: %s failed: %s\n", entry, what, cudaGetErrorString(e));
     return -(int)e - 1000;
 }
 
@@ -345,14 +346,14 @@ extern "C" int ibis_day_host_f32(float* prog, const float* stat, const float* ho
     std::lock_guard<std::mutex> lock(g_host_mu);
     HostPipe& h = g_host[dev];
     cudaError_t e = host_pipe_init(h);
-    if (e != cudaSuccess) return host_error(e, "stream setup");
+    if (e != cudaSuccess) return host_error(e, "stream setup", "ibis_day_host_f32");
     cudaStream_t user = (cudaStream_t)stream;
-    if ((e = cudaEventRecord(h.start, user)) != cudaSuccess) return host_error(e, "event record");
+    if ((e = cudaEventRecord(h.start, user)) != cudaSuccess) return host_error(e, "event record", "ibis_day_host_f32");
     e = cudaStreamWaitEvent(h.h2d, h.start, 0);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(h.d2h, h.start, 0);
     for (int k = 0; k < kHostStreams && k < ngroup && e == cudaSuccess; ++k)
         e = cudaStreamWaitEvent(h.comp[k], h.start, 0);
-    if (e != cudaSuccess) return host_error(e, "stream wait");
+    if (e != cudaSuccess) return host_error(e, "stream wait", "ibis_day_host_f32");
     const size_t pitch = (size_t)ld * sizeof(float);
     int rc = 0, queued = 0;
     const char* what = nullptr;
@@ -386,8 +387,8 @@ extern "C" int ibis_day_host_f32(float* prog, const float* stat, const float* ho
     for (int g = 0; g < queued && j == cudaSuccess; ++g) j = cudaStreamWaitEvent(user, h.stepped[g], 0);
     if (j == cudaSuccess) j = cudaEventRecord(h.out_done, h.d2h);
     if (j == cudaSuccess) j = cudaStreamWaitEvent(user, h.out_done, 0);
-    if (what) return host_error(e, what);
+    if (what) return host_error(e, what, "ibis_day_host_f32");
     if (rc) return rc;
-    if (j != cudaSuccess) return host_error(j, "stream join");
+    if (j != cudaSuccess) return host_error(j, "stream join", "ibis_day_host_f32");
     return 0;
 }
