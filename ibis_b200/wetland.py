@@ -295,11 +295,11 @@ def run_month_learned(loop, daily: torch.Tensor, fb: FeatureBuilder, lw: Learned
         raise ValueError("the builder, the file and the FP32 columns must share the leading dimension")
     s = _stream(cols.device, stream)
     nacc = L.N_ACC
-    p_means = L.OFF["ACC"]["tsoi_mean"][0]
-    assert [L.OFF["ACC"][k][0] for k in ("wsoi_mean", "wisoi_mean", "tg_mean")] == [p_means + 6, p_means + 12,
-                                                                                     p_means + 18]
-    acc_planes = torch.tensor(list(range(p_means, p_means + 19)) + [L.OFF["ACC"]["aytrunof"][0],
-                                                                     L.OFF["ACC"]["aytdrain"][0]], device=cols.device)
+    # the month-mean planes in the builder's order (tsoi 6, wsoi 6, wisoi 6, tg), then runoff and drainage
+    mean_planes = [L.OFF["ACC"][k][0] + j for k in ("tsoi_mean", "wsoi_mean", "wisoi_mean", "tg_mean")
+                   for j in range(L.OFF["ACC"][k][1])]
+    acc_planes = torch.tensor(mean_planes + [L.OFF["ACC"]["aytrunof"][0], L.OFF["ACC"]["aytdrain"][0]],
+                              device=cols.device)
     day_planes = torch.tensor([L.OFF["DAYST"]["ayprcp"][0], L.OFF["DAYST"]["ayaet"][0]], device=cols.device)
     f_in = L.OFF["STAT"]["f_inund"][0]
     with torch.cuda.stream(s):
