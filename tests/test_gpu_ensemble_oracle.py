@@ -18,9 +18,13 @@ Tolerances (FP32 kernels against float64 after 48 hours): temperatures within
 ``T_ABS`` K, soil water within ``W_ABS``, and the day-loop sums within
 ``ACC_REL`` of the largest magnitude of their plane; a served request's per-year
 sums within ``SERVE_REL`` (they are differences of running totals at the year
-ends) -- about 10x the departures measured on these cases
+ends), runoff within ``SERVE_RUNOFF_REL`` (surface runoff switches on at
+saturation and puddle thresholds, so an hour's FP32 soil water can move its
+onset: measured 6.0e-5 with the default parameters and 6.1e-4 under the
+release switches, where the other sums stay within 1.4e-5) -- about 10x (runoff
+3x) the departures measured on these cases
 (``measured_errors``: temperatures 0.26 / 0.55 mK, soil water 1.6e-6, sums
-4e-6 / 3.2e-6, served sums 6e-5).
+4e-6 / 3.2e-6, served sums 1.4e-5, served runoff 6.1e-4).
 """
 import warnings
 
@@ -32,6 +36,7 @@ import oracle
 from ibis_b200 import ensemble as E
 from ibis_b200 import layout as L
 from ibis_b200 import serve as S
+from ibis_b200 import synth
 
 warnings.filterwarnings("ignore", category=RuntimeWarning)
 pytestmark = pytest.mark.gpu
@@ -39,7 +44,8 @@ pytestmark = pytest.mark.gpu
 T_ABS = 5e-3
 W_ABS = 2e-5
 ACC_REL = 5e-5
-SERVE_REL = 6e-4
+SERVE_REL = 2e-4
+SERVE_RUNOFF_REL = 2e-3
 TEMPS = ("tsoi", "tg", "tu", "ts", "tl", "t12", "t34", "tsno", "ti", "tsoi_deep")
 SUMS = ("aygpptot", "aynpptot", "adaet", "afsena", "aytrunof", "aytdrain", "ch4")
 
@@ -144,9 +150,13 @@ def measured_errors():
             "served": _served_vs_oracle()}
 
 
-def _served_vs_oracle():
+def _served_vs_oracle(params=None):
     year_hours = 48
-    lib = S.SiteLibrary(nsite=5, years=2, seed=4, year_hours=year_hours)
+    lib = S.SiteLibrary(nsite=5, years=2, seed=4, year_hours=year_hours, params=params)
+    if params is not None:
+        # per-site acclimation states for the release file's temperature acclimation
+        lib.spec.stat["acclim_x"] = np.random.default_rng(6).uniform(-12.0, 28.0, 5)
+        lib.stat.copy_(torch.from_numpy(synth.to_planes("STAT", lib.spec.stat, lib.ld_site)).to(lib.stat))
     rng = np.random.default_rng(8)
     req = S.Request(rid=0, sites=np.array([0, 2, 4]), years=2, vector=E.draw_vectors(rng, 1)[0], arrival=0.0)
     srv = S.Server(lib, budget_bytes=lib.nbytes + 64 * S.slot_bytes(2), epoch_hours=24)
@@ -155,13 +165,16 @@ def _served_vs_oracle():
     spec = lib.spec
     recs = lambda h: np.stack([spec.forc[spec.site_first[s] + h] for s in req.sites]).astype(np.float64)
     want = oracle_runs(spec, recs, [req.vector], req.sites, 2 * year_hours, year_hours=year_hours)[0][2]
-    err = 0.0
+    err, per = 0.0, {}
     for y in range(2):
         for k, f in enumerate(L.YEARLY):
             w = want[y][f.name] - (want[y - 1][f.name] if y else 0.0)
             scale = max(float(np.max(np.abs(w))), 1e-30)
-            err = max(err, float(np.max(np.abs(got[:, y, k] - w))) / scale)
-    return {"acc": err}
+            e = float(np.max(np.abs(got[:, y, k] - w))) / scale
+            per[f"{f.name}.{y}"] = e
+            if f.name != "aytrunof":
+                err = max(err, e)
+    return {"acc": err, "runoff": max(per["aytrunof.0"], per["aytrunof.1"]), "per_field": per}
 
 
 def test_ensemble_runs_match_oracle(cuda_lib):
@@ -205,4 +218,11 @@ def test_release_switches_change_ensemble_runs(cuda_lib):
 
 def test_served_request_matches_oracle(cuda_lib):
     e = _served_vs_oracle()
-    assert e["acc"] < SERVE_REL, e
+    assert e["acc"] < SERVE_REL and e["runoff"] < SERVE_RUNOFF_REL, e
+
+
+def test_served_request_under_release_switches_matches_oracle(cuda_lib):
+    """A request served under the release parameter file's switches (the
+    ensemble kernels with the IBIS 3.0 extensions) against the oracle."""
+    e = _served_vs_oracle(release_params())
+    assert e["acc"] < SERVE_REL and e["runoff"] < SERVE_RUNOFF_REL, e
