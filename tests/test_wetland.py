@@ -104,3 +104,23 @@ def test_learned_file_applies_to_its_own_cells_only(tmp_path):
     np.savez(tmp_path / "g.npz", **bad)
     with pytest.raises(ValueError):
         W.LearnedWetland(str(tmp_path / "g.npz"), I, J)
+
+
+def test_forest_arrays_check_the_trees():
+    """The host reads boosters into flat node arrays and refuses malformed or
+    unsupported ones before anything reaches a GPU."""
+    import json
+    from ibis_b200.wetland import forest_arrays
+    t0 = [("split", 0, 0.5, 1, 2, False), ("leaf", 0.125), ("leaf", -0.5)]
+    a = forest_arrays([booster_json([t0], base_score="[5E-1]", nfeat=45)])
+    assert a["tree_first"].tolist() == [0, 1] and a["node_first"].tolist() == [0, 3]
+    assert a["left"].tolist() == [1, -1, -1] and a["value"].tolist() == [0.5, 0.125, -0.5]
+    assert a["base_margin"].tolist() == [0.5] and a["transform"].tolist() == [0]
+    bad_child = json.loads(booster_json([t0], nfeat=45))
+    bad_child["learner"]["gradient_booster"]["model"]["trees"][0]["right_children"][0] = 7
+    bad_feat = json.loads(booster_json([[("split", 60, 0.5, 1, 2, False), ("leaf", 0.1), ("leaf", 0.2)]], nfeat=45))
+    for doc in (bad_child, bad_feat):
+        with pytest.raises(ValueError):
+            forest_arrays([json.dumps(doc)])
+    with pytest.raises(ValueError):
+        forest_arrays([booster_json([t0], objective="reg:gamma", nfeat=45)])
