@@ -34,6 +34,7 @@ UNITS = {
     "ibis_f32_inst_b.cu": F32_FLAGS,
     "ibis_f32_inst_c.cu": F32_FLAGS,
     "ibis_f32_inst_d.cu": F32_FLAGS,
+    "ibis_f32_inst_e.cu": F32_FLAGS,
     "ibis_x3_inst_a.cu": F32_FLAGS,
     "ibis_x3_inst_b.cu": F32_FLAGS,
     "ibis_x3_inst_c.cu": F32_FLAGS,

@@ -3,6 +3,7 @@
 #pragma once
 #include <errno.h>
 #include <math.h>
+#include <stdint.h>
 #include <stdio.h>
 #include <string.h>
 
@@ -16,15 +17,17 @@ namespace ibis {
 
 // Launch configurations.  form 0: one fused kernel per launch (all hours in
 // registers/shared memory); form 1: a surface kernel and a ground kernel per
-// hour.  block/minb are the block size and the minimum resident blocks per SM
-// promised to the compiler (__launch_bounds__), i.e. the register budget.
+// hour; form 2: the fused kernel with each hour's forcing brought into shared
+// memory by bulk copies while the hour before it runs.  block/minb are the
+// block size and the minimum resident blocks per SM promised to the compiler
+// (__launch_bounds__), i.e. the register budget.
 struct LaunchConfig {
     int form, block, minb, block2, minb2;
 };
 constexpr LaunchConfig kConfigs[] = {
     {0, 128, 2, 0, 0}, {0, 64, 4, 0, 0},  {0, 96, 2, 0, 0},    {0, 128, 3, 0, 0},
     {0, 160, 1, 0, 0}, {0, 192, 1, 0, 0}, {0, 224, 1, 0, 0},   {0, 256, 1, 0, 0},
-    {1, 128, 2, 128, 3}, {1, 256, 1, 256, 2}, {1, 128, 3, 128, 4}};
+    {1, 128, 2, 128, 3}, {1, 256, 1, 256, 2}, {1, 128, 3, 128, 4}, {2, 224, 1, 0, 0}};
 constexpr int kNumConfigs = sizeof(kConfigs) / sizeof(kConfigs[0]);
 constexpr int kDefaultFused = 0;
 constexpr int kLongFused = 6;      // ibis_step_f32's choice for launches of kAccSmemMinSteps hours or more
@@ -230,6 +233,187 @@ __global__ void __launch_bounds__(BLOCK, MINB) hourly_step_kernel(R* __restrict_
     }
 }
 
+// ---- Fused kernel with the forcing staged by the bulk-copy (TMA) engine (form 2)
+//
+// Each hour's forcing tile -- IBIS_FORC_COUNT planes x the block's cells, one
+// untiled cp.async.bulk per plane -- lands in shared memory while the block
+// computes the hour before it.  Thread 0 issues hour s+1 as soon as every live
+// thread of the block has copied hour s out of the buffer (the "empty"
+// mbarrier counts the live threads, the "full" mbarrier counts the bytes in);
+// the copy then has the whole of hour s to land.  One buffer is enough: the
+// threads read their 12 values at the top of the hour.  Every wait is bounded:
+// a wait that gives up sets the block's abort word (no copy is issued after it
+// and later waits return at once) and status[0] bit 2, and the block finishes
+// its hours on whatever the buffer holds; thread 0 then waits, again bounded,
+// for its last copy to land before it leaves.
+constexpr int kStageWaitLimit = 1 << 22;
+
+template <typename R, int BLOCK>
+struct ForcStage {
+    static_assert(BLOCK % 4 == 0, "a plane's tile must start on a 16-byte boundary");
+    static constexpr size_t data = (size_t)IBIS_FORC_COUNT * BLOCK * sizeof(R);
+    static constexpr size_t bytes = data + 32;  // + full, empty mbarriers, abort and last-issued words
+};
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* b, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(b)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(unsigned long long* b) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(b)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* b, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(b)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* b, unsigned parity) {
+    unsigned done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(smem_addr(b)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+// Wait for the phase of `b` with the given parity to complete: true when it
+// did, false when the block's abort word is set or kStageWaitLimit polls pass.
+__device__ __forceinline__ bool stage_wait(unsigned long long* b, unsigned parity, volatile int* abort_word) {
+    for (int k = 0; k < kStageWaitLimit; ++k) {
+        if (mbar_try_wait(b, parity)) return true;
+        if (*abort_word) return false;
+    }
+    return false;
+}
+
+// Issue hour `h`'s forcing tile into `buf`: plane p of the tile at buf[p * BLOCK].
+// `bytes` per plane is the live cells rounded up to 4 (16 bytes), which stays
+// inside a plane of ld >= ncell cells because ld and the tile start are
+// multiples of 4 cells.
+template <typename R, int BLOCK>
+__device__ __forceinline__ void stage_issue(R* buf, const R* __restrict__ src, int ld, unsigned bytes,
+                                            unsigned long long* full) {
+    mbar_arrive_expect_tx(full, bytes * IBIS_FORC_COUNT);
+#pragma unroll
+    for (int p = 0; p < IBIS_FORC_COUNT; ++p)
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                         smem_addr(buf + p * BLOCK)),
+                     "l"(src + (size_t)p * ld), "r"(bytes), "r"(smem_addr(full))
+                     : "memory");
+}
+
+template <typename R>
+__device__ __forceinline__ Forc<R> read_forc_tile(const R* t, int block) {
+    Forc<R> F;
+    auto g = [&](int plane) { return t[plane * block]; };
+    F.ta = g(IBIS_FORC_TA); F.qa = g(IBIS_FORC_QA); F.ua = g(IBIS_FORC_UA); F.ps = g(IBIS_FORC_PSURF);
+    F.cosz = g(IBIS_FORC_COSZEN);
+    F.sd[0] = g(IBIS_FORC_SOLAD); F.sd[1] = g(IBIS_FORC_SOLAD + 1);
+    F.si[0] = g(IBIS_FORC_SOLAI); F.si[1] = g(IBIS_FORC_SOLAI + 1);
+    F.fira = g(IBIS_FORC_FIRA); F.rain = g(IBIS_FORC_RAINA); F.snow = g(IBIS_FORC_SNOWA);
+    return F;
+}
+
+// The staged kernel's shared memory: column state, the on-chip accumulators,
+// then the forcing tile and its barriers (16-byte aligned).
+template <typename R, int BLOCK, int MINB>
+struct StagedSmem {
+    static constexpr size_t col = (size_t)BLOCK * sizeof(Col<R>);
+    static constexpr size_t acc = (size_t)BLOCK * 2 * kAccOnChip * sizeof(R);
+    static constexpr size_t stage_off = (col + acc + 15) / 16 * 16;
+    static constexpr size_t total = stage_off + ForcStage<R, BLOCK>::bytes;
+};
+
+// Callers guarantee: `forc` 16-byte aligned, forc_stride and ld multiples of 4
+// (launch_staged checks and otherwise runs the unstaged kernel).
+// Give up on the staged forcing: no further copies, later waits return at once.
+__device__ __forceinline__ void stage_give_up(volatile int* abort_word, int* status) {
+    *abort_word = 1;
+    if (status) atomicOr(status, 4);
+}
+
+template <typename R, int NT, bool SU, bool SL, int BLOCK, int MINB, bool X3>
+__global__ void __launch_bounds__(BLOCK, MINB) hourly_step_staged_kernel(
+    R* __restrict__ prog, const R* __restrict__ stat, const R* __restrict__ forc, R* __restrict__ diag,
+    R* __restrict__ acc, int ncell, int ld, int nstep, long long forc_stride, const DevParams<R> P,
+    int* __restrict__ status) {
+    static_assert(sizeof(R) == 4 && StateInSmem<R>::value, "the staged form is the FP32 shared-memory kernel");
+    static_assert(AccInSmem<R, BLOCK, MINB>::value, "the staged form keeps the accumulators on chip");
+    using SM = StagedSmem<R, BLOCK, MINB>;
+    static_assert((SM::total + 1024) * MINB <= 228 * 1024, "staged shared memory exceeds the SM");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    // fixed offsets from the shared-memory base, so none of them holds a register across the hour
+    R* const tile = reinterpret_cast<R*>(smem_raw + SM::stage_off);
+    unsigned long long* const full = reinterpret_cast<unsigned long long*>(smem_raw + SM::stage_off +
+                                                                           ForcStage<R, BLOCK>::data);
+    unsigned long long* const empty = full + 1;
+    volatile int* const abort_word = reinterpret_cast<volatile int*>(full + 2);
+    volatile int* const last_issued = abort_word + 1;
+    const int i0 = blockIdx.x * BLOCK;
+    if (threadIdx.x == 0) {
+        const int nlive = ncell - i0 < BLOCK ? ncell - i0 : BLOCK;
+        mbar_init(full, 1);
+        mbar_init(empty, (unsigned)nlive);
+        *abort_word = 0;
+        *last_issued = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();  // every thread of the block reaches this before any leaves
+    // bytes per plane: the block's live cells rounded up to 4 (16 bytes)
+    auto plane_bytes = [&]() {
+        const int nlive = ncell - i0 < BLOCK ? ncell - i0 : BLOCK;
+        return (unsigned)((nlive + 3) & ~3) * (unsigned)sizeof(R);
+    };
+    if (threadIdx.x == 0 && nstep > 0) stage_issue<R, BLOCK>(tile, forc + i0, ld, plane_bytes(), full);
+    const int i = i0 + threadIdx.x;
+    if (i >= ncell) return;
+    Col<R>& c = *(reinterpret_cast<Col<R>*>(smem_raw) + threadIdx.x);
+    load_col(c, prog + i, ld);
+    Stat<R> S{stat + i, ld};
+    Diag<R> D{diag ? diag + i : nullptr, ld};
+    R* const sacc = reinterpret_cast<R*>(smem_raw + SM::col) + threadIdx.x;
+    const bool kahan = (P.flags & IBIS_FLAG_KAHAN) != 0;
+    using AccT = Acc<R, BLOCK>;
+    AccT A{sacc, ld, kahan, true, acc ? acc + i : nullptr};
+    if (acc) acc_move<R, true>(acc + i, ld, sacc, BLOCK, P.flags);
+#pragma unroll 1
+    for (int s = 0; s < nstep; ++s) {
+        const unsigned parity = (unsigned)(s & 1);
+        if (!stage_wait(full, parity, abort_word)) stage_give_up(abort_word, status);
+        Forc<R> F = read_forc_tile(tile + threadIdx.x, BLOCK);
+        mbar_arrive(empty);
+        if (threadIdx.x == 0 && s + 1 < nstep && !*abort_word) {
+            if (stage_wait(empty, parity, abort_word)) {
+                stage_issue<R, BLOCK>(tile, forc + (size_t)(s + 1) * forc_stride + i0, ld, plane_bytes(), full);
+                *last_issued = s + 1;
+            } else {
+                stage_give_up(abort_word, status);
+            }
+        }
+        A.last = (s + 1 == nstep);
+        column_step<R, NT, SU, SL>(c, F, S, D, A, P, uniform_source<R, X3>(P));
+    }
+    if (acc) acc_move<R, false>(acc + i, ld, sacc, BLOCK, P.flags);
+    R sum = store_col(c, prog + i, ld);
+    if (threadIdx.x == 0 && *abort_word) {
+        // after a give-up the last copy may still be landing: let it finish
+        // (bounded) before the block's shared memory is released
+        volatile int never = 0;
+        stage_wait(full, (unsigned)(*last_issued & 1), &never);
+    }
+    if (status && !finite(sum)) {
+        atomicOr(status, 1);
+        atomicMin(status + 1, i + P.cell0);
+    }
+}
+
 // Two-kernel form of one hour: the surface phase writes the hand-off values to
 // `mid` (kMidCount planes), the ground phase reads them.  Both phases load the
 // column from `prog` and write back what they change.
@@ -426,6 +610,26 @@ cudaError_t launch_fused(R* prog, const R* stat, const R* forc, R* diag, R* acc,
     return cudaGetLastError();
 }
 
+// Form 2: the staged fused kernel.  A forcing buffer the bulk copies cannot
+// address (start not 16-byte aligned, hour or plane stride not a multiple of 4
+// cells) runs the unstaged kernel of the same block size instead: the results
+// are the same, only the loads differ.
+template <typename R, int NT, bool SU, bool SL, int BLOCK, int MINB, bool X3>
+cudaError_t launch_staged(R* prog, const R* stat, const R* forc, R* diag, R* acc, int ncell, int ld, int nstep,
+                          long long fstride, const DevParams<R>& P, int* status, cudaStream_t s) {
+    if ((reinterpret_cast<uintptr_t>(forc) & 15) != 0 || (fstride & 3) != 0 || (ld & 3) != 0)
+        return launch_fused<R, NT, SU, SL, BLOCK, MINB, true, X3>(prog, stat, forc, diag, acc, ncell, ld, nstep,
+                                                                  fstride, P, status, s);
+    using SM = StagedSmem<R, BLOCK, MINB>;
+    const int grid = (ncell + BLOCK - 1) / BLOCK;
+    auto k = hourly_step_staged_kernel<R, NT, SU, SL, BLOCK, MINB, X3>;
+    static unsigned long long fitted = 0;
+    cudaError_t e = fit_smem_once(fitted, k, BLOCK, SM::total, SM::total);
+    if (e != cudaSuccess) return e;
+    k<<<grid, BLOCK, SM::total, s>>>(prog, stat, forc, diag, acc, ncell, ld, nstep, fstride, P, status);
+    return cudaGetLastError();
+}
+
 template <typename R, int NT, bool SU, bool SL, int B1, int M1, int B2, int M2, bool X3>
 cudaError_t launch_split(R* prog, const R* stat, const R* forc, R* diag, R* acc, R* mid, int ncell, int ld,
                          int nstep, long long fstride, const DevParams<R>& P, int* status, cudaStream_t s) {
@@ -460,6 +664,9 @@ cudaError_t run_config(R* prog, const R* stat, const R* forc, R* diag, R* acc, R
         }
         return launch_fused<R, NT, SU, SL, C.block, C.minb, true, X3>(prog, stat, forc, diag, acc, ncell, ld, nstep,
                                                                       fs, P, status, s);
+    } else if constexpr (C.form == 2) {
+        return launch_staged<R, NT, SU, SL, C.block, C.minb, X3>(prog, stat, forc, diag, acc, ncell, ld, nstep, fs, P,
+                                                                 status, s);
     } else {
         return launch_split<R, NT, SU, SL, C.block, C.minb, C.block2, C.minb2, X3>(prog, stat, forc, diag, acc, mid,
                                                                                   ncell, ld, nstep, fs, P, status, s);
@@ -475,7 +682,7 @@ cudaError_t run_config(R* prog, const R* stat, const R* forc, R* diag, R* acc, R
 #define IBIS_F77_CONFIGS(X, NT)                                                                                \
     X(NT, false, false, 0) X(NT, false, false, 1) X(NT, false, false, 2) X(NT, false, false, 3)                \
     X(NT, false, false, 4) X(NT, false, false, 5) X(NT, false, false, 6) X(NT, false, false, 7)                \
-    X(NT, false, false, 8) X(NT, false, false, 9) X(NT, false, false, 10)
+    X(NT, false, false, 8) X(NT, false, false, 9) X(NT, false, false, 10) X(NT, false, false, 11)
 #define IBIS_SUN_CONFIGS(X, NT)                                                                                \
     X(NT, true, false, 0) X(NT, false, true, 0) X(NT, true, true, 0)                                           \
     X(NT, true, false, 8) X(NT, false, true, 8) X(NT, true, true, 8)
@@ -497,10 +704,10 @@ cudaError_t dispatch_config(int cfg, R* prog, const R* stat, const R* forc, R* d
         return run_config<R, NT, SU, SL, kDefaultFused, true>(IBIS_ARGS);
     } else if constexpr (X3) {
         if (cfg == kLongFused && SU == SL) return run_config<R, NT, SU, SL, kLongFused, true>(IBIS_ARGS);
-        if (kConfigs[cfg].form == 0) return run_config<R, NT, SU, SL, kDefaultFused, true>(IBIS_ARGS);
+        if (kConfigs[cfg].form != 1) return run_config<R, NT, SU, SL, kDefaultFused, true>(IBIS_ARGS);
         return run_config<R, NT, SU, SL, kDefaultSplit, true>(IBIS_ARGS);
     } else if constexpr (SU || SL) {
-        if (kConfigs[cfg].form == 0) return run_config<R, NT, SU, SL, kDefaultFused>(IBIS_ARGS);
+        if (kConfigs[cfg].form != 1) return run_config<R, NT, SU, SL, kDefaultFused>(IBIS_ARGS);
         return run_config<R, NT, SU, SL, kDefaultSplit>(IBIS_ARGS);
     } else {
         switch (cfg) {
@@ -514,6 +721,7 @@ cudaError_t dispatch_config(int cfg, R* prog, const R* stat, const R* forc, R* d
             case 8: return run_config<R, NT, SU, SL, 8>(IBIS_ARGS);
             case 9: return run_config<R, NT, SU, SL, 9>(IBIS_ARGS);
             case 10: return run_config<R, NT, SU, SL, 10>(IBIS_ARGS);
+            case 11: return run_config<R, NT, SU, SL, 11>(IBIS_ARGS);
             default: return run_config<R, NT, SU, SL, 0>(IBIS_ARGS);
         }
     }

@@ -205,7 +205,7 @@ extern "C" int ibis_step_host_f32(float* prog, const float* stat, const float* h
     if (!prog || !stat || !host_forc || !forc || !params) return -EINVAL;
     if (ncell < 0 || nstep < 0 || ld < ncell || ld % 32 || group < 0 || group % 32 || chunk < -(1 << 20))
         return -EINVAL;
-    if (config < -1 || config >= ibis::kNumConfigs || (config >= 0 && ibis::kConfigs[config].form != 0))
+    if (config < -1 || config >= ibis::kNumConfigs || (config >= 0 && ibis::kConfigs[config].form == 1))
         return -EINVAL;
     if (ncell == 0) return 0;
     const int cfg = config >= 0 ? config : (nstep >= ibis::kAccSmemMinSteps ? ibis::kLongFused : ibis::kDefaultFused);
@@ -321,7 +321,7 @@ extern "C" int ibis_day_host_f32(float* prog, const float* stat, const float* ho
                                  const IbisParams* params, int* status, int group, int config, void* stream) {
     if (!prog || !stat || !host_daily || !daily || !lat || !forc || !params) return -EINVAL;
     if (ncell < 0 || nday < 0 || ld < ncell || ld % 32 || group < 0 || group % 32) return -EINVAL;
-    if (config < -1 || config >= ibis::kNumConfigs || (config >= 0 && ibis::kConfigs[config].form != 0))
+    if (config < -1 || config >= ibis::kNumConfigs || (config >= 0 && ibis::kConfigs[config].form == 1))
         return -EINVAL;
     if (day0 < 0 || jday0 < 1 || jday0 > 366 || (dflags & ~IBIS_DIURNAL_OBSERVED_FIRA)) return -EINVAL;
     if (!(params->dtime > 0.0)) return -EINVAL;

@@ -104,7 +104,9 @@ _configs = None
 
 def configs():
     """List of dicts describing the launch configurations of the FP32 kernels
-    (read from the library once; the table is compiled in)."""
+    (read from the library once; the table is compiled in).  ``staged`` marks
+    the fused configuration whose hourly forcing tiles are brought into shared
+    memory by bulk copies."""
     global _configs
     if _configs is not None:
         return [dict(c) for c in _configs]
@@ -114,8 +116,8 @@ def configs():
         v = [ctypes.c_int() for _ in range(5)]
         check(L.ibis_config_info(i, *[ctypes.byref(x) for x in v]), "ibis_config_info")
         f, b, m, b2, m2 = (x.value for x in v)
-        out.append(dict(id=i, form="fused" if f == 0 else "split", block=b, min_blocks=m, block2=b2,
-                        min_blocks2=m2))
+        out.append(dict(id=i, form="split" if f == 1 else "fused", staged=f == 2, block=b, min_blocks=m,
+                        block2=b2, min_blocks2=m2))
     _configs = out
     return [dict(c) for c in out]
 

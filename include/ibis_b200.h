@@ -62,7 +62,12 @@ int ibis_step_config_f32(float* prog, const float* stat, const float* forc, floa
                          int config);
 
 /* Launch configurations: count, and the description of one
- * (form 0 = fused, 1 = two-kernel; block sizes and min resident blocks/SM). */
+ * (form 0 = fused, 1 = two-kernel, 2 = fused with each hour's forcing tile
+ * brought into shared memory by bulk copies while the hour before it runs;
+ * block sizes and min resident blocks/SM).  A form-2 launch whose forcing
+ * pointer is not 16-byte aligned runs the form-0 kernel of the same block
+ * size; one whose bounded wait for a copy gave up sets status[0] bit 2
+ * (value 4), and its results are not to be used. */
 int ibis_num_configs(void);
 int ibis_config_info(int config, int* form, int* block, int* min_blocks, int* block2, int* min_blocks2);
 
