@@ -4,6 +4,12 @@
 #pragma once
 #include "ibis_column.cuh"
 
+// 1: the FP32 kernels solve soil water in float for the hour's increments
+// (soil_water_increments); 0: in double on absolute contents (soil_water).
+#ifndef IBIS_SOILW_INCREMENTS
+#define IBIS_SOILW_INCREMENTS 1
+#endif
+
 namespace ibis {
 
 // Thomas algorithm (solvers.py:17-83) on N unknowns held in registers.
@@ -216,6 +222,106 @@ __device__ __forceinline__ void soil_water(double (&w)[NL], double& wpud, double
     wflo[0] = wflo[0] + fsq - fwpud;
 #pragma unroll
     for (int k = 0; k < NL; ++k) w[k] = wn[k];
+}
+
+// The FP32 kernels' soilh2o (soil_physics.py:196-373): the same implicit system
+// in float, solved for the hour's increments delta = w_new - w.  Its
+// right-hand side holds the flux divergence and the implicit terms applied to
+// the current profile, so float32 rounds relative to the hour's change where a
+// layer changes slowly, and relative to w where the implicit terms dominate
+// (wet, conductive layers), as the float32 state's own storage does.  The
+// saturation bound and the upward excess flux work on the increments too.
+template <typename R>
+__device__ __forceinline__ void soil_water_increments(float (&w)[NL], float& wpud, float (&wflo)[NL + 1],
+                                                      const float (&wisoi)[NL], const float (&poros)[NL],
+                                                      const float (&pflo)[NL], const Stat<R>& S, float fwtop,
+                                                      float fwpud, const DevParams<R>& P) {
+    const float dmin = 1e-9f;
+    const float dtime = P.dtime, rhow = P.rhow, eps = P.epsilon;
+    const bool consistent = (P.flags & IBIS_FLAG_H2O_CONSISTENT) != 0;
+    float e[NL + 1], f[NL + 1], g[NL + 1];
+    e[0] = f[0] = g[0] = 0.0f;
+    f[NL] = g[NL] = 0.0f;
+    float hyd_prev = S(IBIS_STAT_HYDRAUL, 0);
+    float suc_prev = S(IBIS_STAT_SUCTION, 0);
+    float bex_prev = S(IBIS_STAT_BEX, 0);
+#pragma unroll
+    for (int k = 1; k < NL; ++k) {
+        const float hyd = S(IBIS_STAT_HYDRAUL, k);
+        const float suc = S(IBIS_STAT_SUCTION, k);
+        const float bex = S(IBIS_STAT_BEX, k);
+        const float wp = P.sw32_wp[k], wm = P.sw32_wm[k];
+        const float a = wm * hyd_prev + wp * hyd;
+        const float b = wm * hyd_prev * suc_prev * bex_prev + wp * hyd * suc * bex;
+        const float zb = wm * bex_prev + wp * bex;
+        const int nb = (int)floorf(zb + 0.5f);
+        const int m = 2 * nb + 3;
+        const int nn = nb + 2;
+        const float ws = consistent ? wp * w[k - 1] + wm * w[k] : wm * w[k - 1] + wp * w[k];
+        const float wa = fminf(ws, 1.0f);
+        const float pw1 = ipow(wa, nn - 1);
+        float bwn1 = b * pw1;
+        float bwn = bwn1 * wa;
+        if (bwn < dmin) bwn1 = 0.0f;
+        bwn = fmaxf(bwn, dmin);
+        const float dw = (w[k] - w[k - 1]) * P.sw32_rhm[k];
+        const float wam1 = pw1 * pw1;                   // wa**(m-1) = (wa**(nn-1))**2
+        const float ek = (float)(m - 1) * a * (wam1 * wa) - (float)nn * bwn1 * wa * dw;
+        const float fk = (float)(-m) * a * wam1 + (float)nn * bwn1 * dw;
+        float zi = fmaxf(0.0f, 1.0f - fmaxf(wisoi[k - 1], wisoi[k]));
+        zi = zi * zi;
+        e[k] = zi * ek;
+        f[k] = zi * fk;
+        g[k] = zi * bwn;
+        hyd_prev = hyd; suc_prev = suc; bex_prev = bex;
+    }
+    {
+        const float wab = fminf(w[NL - 1], 1.0f);
+        const int mb = 2 * (int)floorf(bex_prev + 0.5f) + 3;
+        const float zi = fmaxf(0.0f, 1.0f - wisoi[NL - 1]);
+        e[NL] = (zi * zi) * (-hyd_prev * ipow(wab, mb) * P.bperm);
+    }
+    float lo[NL], di[NL], up[NL], r[NL], dl[NL];
+#pragma unroll
+    for (int k = 0; k < NL; ++k) {
+        const float dt = dtime / fmaxf(pflo[k] * P.hsoi[k], 1e-30f);
+        const float rhb = P.sw32_rhb[k];
+        float d1 = dt * (f[k] * P.sw32_c1[k] - g[k] * rhb);
+        float d2m, d3;                                  // d2m: the diagonal less its 1
+        if (k < NL - 1) {
+            const float rhp = P.sw32_rhp[k];
+            d2m = dt * (-f[k + 1] * P.sw32_c3[k] + f[k] * P.sw32_c5[k] + g[k + 1] * rhp + g[k] * rhb);
+            d3 = dt * (-f[k + 1] * P.sw32_c6[k] - g[k + 1] * rhp);
+        } else {
+            d2m = dt * (-f[k + 1] + f[k] * P.sw32_c5[k] + g[k] * rhb);
+            d3 = 0.0f;
+        }
+        float rk = dt * (e[k + 1] - e[k]) - d2m * w[k];
+        if (k == 0) {
+            d1 = 0.0f;
+            rk = rk + dt * (fwtop + fwpud) / rhow;
+        } else {
+            rk = rk - d1 * w[k - 1];
+        }
+        if (k < NL - 1) rk = rk - d3 * w[k + 1];
+        lo[k] = d1; di[k] = 1.0f + d2m; up[k] = d3; r[k] = rk;
+    }
+    thomas(lo, di, up, r, dl);
+    wflo[NL] = -rhow * e[NL];
+    float fsq = 0.0f;
+#pragma unroll
+    for (int k = NL - 1; k >= 0; --k) {
+        const float zz = rhow * poros[k] * fmaxf(eps, 1.0f - wisoi[k]) * P.hsoi[k];
+        float dwk = dl[k] + dtime * fsq / zz;           // w_new - w before the saturation bound
+        const float over = (w[k] - 1.0f) + dwk;         // w_new - 1
+        const float fsn = fmaxf(over, 0.0f) * zz / dtime;
+        if (over > 0.0f) dwk = 1.0f - w[k];
+        wflo[k] = wflo[k + 1] + dwk * zz / dtime;
+        w[k] = over > 0.0f ? 1.0f : w[k] + dwk;
+        fsq = fsn;
+    }
+    wpud = fmaxf(wpud + (fsq - fwpud) * dtime, 0.0f);
+    wflo[0] = wflo[0] + fsq - fwpud;
 }
 
 // ---------------------------------------------------------------------------

@@ -513,6 +513,12 @@ static DevParams<R> make_dev_params(const IbisParams& h) {
     }
     d.rdt64 = 1.0 / h.dtime;
     d.rrhow64 = 1.0 / h.rhow;
+    for (int k = 0; k < NL; ++k) {
+        d.sw32_wp[k] = (float)d.sw_wp[k]; d.sw32_wm[k] = (float)d.sw_wm[k];
+        d.sw32_rhm[k] = (float)d.sw_rhm[k]; d.sw32_rhb[k] = (float)d.sw_rhb[k]; d.sw32_rhp[k] = (float)d.sw_rhp[k];
+        d.sw32_c1[k] = (float)d.sw_c1[k]; d.sw32_c3[k] = (float)d.sw_c3[k];
+        d.sw32_c5[k] = (float)d.sw_c5[k]; d.sw32_c6[k] = (float)d.sw_c6[k];
+    }
     // respiration tables formed in float32 as the reference does (loops_gswp3.py:185-190)
     const float per_s = (float)(h.ndaypy * 86400.0), mol = (float)(1000.0 / 12.0);
     for (int j = 0; j < 12; ++j) {

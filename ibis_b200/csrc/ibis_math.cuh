@@ -66,6 +66,18 @@ __device__ __forceinline__ double ipow(double x, int n) {
     return any ? r : 1.0;
 }
 
+__device__ __forceinline__ float ipow(float x, int n) {
+    float r = 1.0f, b = x;
+    bool any = false;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        if (n & 1) { r = any ? r * b : b; any = true; }
+        n >>= 1;
+        if (n) b = b * b;
+    }
+    return any ? r : 1.0f;
+}
+
 // ---------------------------------------------------------------------------
 // Lowe (1977) saturation vapour pressure and its derivative, both branches
 // evaluated on clamped offsets (reference physics/thermo.py:38-174).

@@ -34,6 +34,10 @@ struct DevParams {
     double sw_rhm[6], sw_rhb[6], sw_rhp[6], sw_c1[6], sw_c3[6], sw_c5[6], sw_c6[6];
     double rdt64;      // 1 / dtime in double
     double rrhow64;    // 1 / rhow in double
+    // float copies of sw_wp, sw_wm and the multipliers, for the FP32 kernels'
+    // increment-form soil-water solve
+    float sw32_wp[6], sw32_wm[6], sw32_rhm[6], sw32_rhb[6], sw32_rhp[6], sw32_c1[6], sw32_c3[6], sw32_c5[6],
+        sw32_c6[6];
     R rwood_s[12], rroot_s[12], keep[12];  // float32-formed respiration rates (loops_gswp3.py:185-190)
     R ch4_w;           // float32(dtime / 86400)
     R rh_conv;         // float32(12e-3 * 86400)

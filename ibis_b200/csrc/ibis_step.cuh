@@ -539,9 +539,15 @@ __device__ __forceinline__ void ground_phase(Col<R>& c, const Forc<R>& F, const 
     }
     const R fhtop_soil = heatg_avg + raing_avg * P.ch2o * (traing_avg - tpt[0])
                        - grunof * P.ch2o * mx(P.tmelt - tpt[0], R(0.0));
-    // soil water, double (soil_physics.py:196-373)
+    // soil water (soil_physics.py:196-373): increment form in the FP32 kernels,
+    // double in the FP64 kernels
     R wnew[NL], wflo[NL + 1], wpud_h;
-    {
+    if constexpr (sizeof(R) == 4 && IBIS_SOILW_INCREMENTS) {
+#pragma unroll
+        for (int k = 0; k < NL; ++k) wnew[k] = wsw[k];
+        wpud_h = wpw;
+        soil_water_increments(wnew, wpud_h, wflo, wisw, poros, pflo, S, fwtop, fwpud, P);
+    } else {
         double w64[NL], i64[NL], p64[NL], pf64[NL], wf64[NL + 1];
 #pragma unroll
         for (int k = 0; k < NL; ++k) { w64[k] = wsw[k]; i64[k] = wisw[k]; p64[k] = poros[k]; pf64[k] = pflo[k]; }
