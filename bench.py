@@ -582,7 +582,7 @@ def run_ours(args):
                                 "achieved_gbs": _algorithmic_bytes(1) * args.ncell * HOURS / (ms_plain / 1e3) / 1e9},
             "e2e": {"value": cell_steps / (ms_e2e / 1e3), "unit": "cell-steps/s", "ms_per_step": ms_e2e,
                     "entry": "Columns.run_host -> ibis_step_host_f32",
-                    "group_cells": args.e2e_group or "auto (a twentieth of the columns in whole blocks; chunks of "
+                    "group_cells": args.e2e_group or "auto (a sixteenth of the columns in whole blocks; chunks of "
                                                      "hours up to 1.15 waves)",
                     "h2d_bytes_per_step": int(h_forc.numel() * 4), "d2h_bytes_per_step": int(h_prog.numel() * 4)},
             "e2e_hour_chunks": {"value": cell_steps / (ms_e2e_chunks / 1e3), "unit": "cell-steps/s",

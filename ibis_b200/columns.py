@@ -199,7 +199,7 @@ class Columns:
         ``(nstep, IBIS_FORC_COUNT, ld)``) and, with ``host_prog`` (a pinned host
         tensor shaped like ``prog``), copy the state after the last hour out:
         ``ibis_step_host_f32``, which overlaps the copies with the steps -- in
-        groups of ``group`` columns for batches of several waves (0: twenty
+        groups of ``group`` columns for batches of several waves (0: sixteen
         groups), each group's hours in chunks (``chunk`` hours each, ``-c``:
         ``c`` hours then the rest; 0: a third of the hours then the rest, or for
         a batch of about one wave 4 hours growing by 1.75).  Asynchronous on

@@ -125,11 +125,14 @@ namespace {
 constexpr int kHostStreams = 16;    // compute streams the groups take in turn
 constexpr int kHostMaxGroups = 64;
 constexpr int kHostMaxPieces = 256; // (group, chunk of hours) pairs of one call
-// groups when the caller leaves the size to the library: at 95,333 cells x 24
-// hours, with whole days per group, a day from host to host took 3.86 ms in 20
-// groups, 3.94 ms in 16 and 4.2 ms in 8 (the same day with its forcing already
-// on the device: 3.66 ms on that GPU)
-constexpr int kHostAutoGroups = 20;
+// groups when the caller leaves the size to ibis_step_host_f32: at 95,333
+// cells x 24 hours, each group's day in two chunks, a day from host to host
+// takes 3.17 ms in 16 groups, 3.19 in 12, 3.20 in 24 and 3.26 in 20 (median of
+// 4 interleaved rounds; the same day with its forcing already on the device:
+// 2.99 ms)
+constexpr int kHostAutoGroups = 16;
+// the same for ibis_day_host_f32 (forcing generated per group from daily weather)
+constexpr int kDayHostAutoGroups = 20;
 // batches of more than this many waves of the launch configuration are cut
 // into groups, smaller ones into chunks of hours.  A day from host to host,
 // groups / chunks: 1 wave (33,152 cells) 2.30 / 1.71 ms; 1.25 waves 2.37 /
@@ -337,7 +340,7 @@ extern "C" int ibis_day_host_f32(float* prog, const float* stat, const float* ho
         const int block = ibis::kConfigs[cfg].block;
         const double wave = (double)sms * block * ibis::kConfigs[cfg].minb;
         group = ncell > kHostGroupWaves * wave
-                    ? ((ncell + kHostAutoGroups - 1) / kHostAutoGroups + block - 1) / block * block
+                    ? ((ncell + kDayHostAutoGroups - 1) / kDayHostAutoGroups + block - 1) / block * block
                     : (ncell + 31) / 32 * 32;
     }
     const int min_group = ((ncell + kHostMaxGroups - 1) / kHostMaxGroups + 31) / 32 * 32;

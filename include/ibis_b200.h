@@ -94,7 +94,7 @@ int ibis_step_split_noalloc_f32(float* prog, const float* stat, const float* for
  * reference's timestep_body called on NumPy state, a day loop fed from files).
  * The copies overlap the steps on streams of the library's own:
  *   - a batch of more than 1.15 waves of the launch configuration is cut into
- *     groups of columns (`group` cells, a multiple of 32; 0 = a twentieth of
+ *     groups of columns (`group` cells, a multiple of 32; 0 = a sixteenth of
  *     ncell, rounded up to whole blocks of the launch configuration; raised
  *     so there are at most 64 groups), each
  *     group's forcing copied in, stepped and its state copied out while other
@@ -123,7 +123,8 @@ int ibis_step_host_f32(float* prog, const float* stat, const float* host_forc, f
                        int group, int chunk, int config, void* stream);
 
 /* Days of the step from daily weather in HOST memory, the state read back to
- * HOST memory: per group of columns (`group` as for ibis_step_host_f32), the
+ * HOST memory: per group of columns (`group` as for ibis_step_host_f32, but
+ * 0 = a twentieth of ncell in whole blocks), the
  * group's daily weather copied in, its hourly forcing generated on the device
  * (as ibis_diurnal_f32 generates it, the variates keyed by each cell's index
  * in the caller's numbering, so the forcing equals one call over all cells),

@@ -87,7 +87,7 @@ def test_unaligned_forcing_falls_back_to_the_unstaged_kernel(cuda_lib):
 
 
 def test_staged_through_the_host_pipeline(cuda_lib):
-    """ibis_step_host_f32 with the staged configuration: 20 groups of whole
+    """ibis_step_host_f32 with the staged configuration: groups of two
     blocks, each reading its forcing at its own offset, against the same
     configuration from device memory."""
     wl = synth.make_workload(224 * 40 + 17, 24, seed=replicas.replica_seed(1000, 0))
