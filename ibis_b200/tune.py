@@ -1,6 +1,7 @@
 """Autotuner for the launch configuration of the FP32 hourly-step kernels.
 
-A launch configuration fixes the form (one fused kernel per launch, or a
+A launch configuration fixes the form (one fused kernel per launch, the same
+with each hour's forcing tile staged into shared memory by bulk copies, or a
 surface kernel and a ground kernel per hour), the block size and the register
 budget (minimum resident blocks per SM).  Which is fastest depends on the batch:
 the number of columns sets how many waves of blocks fill the 148 SMs, and the
