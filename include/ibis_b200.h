@@ -56,6 +56,10 @@ int ibis_mid_planes(void);
  * (0 <= config < ibis_num_configs()): the form (fused or two-kernel), block
  * size and register budget.  `scratch` is required by two-kernel configs and
  * ignored by fused ones.  ibis_b200/tune.py times them and picks one per batch.
+ * Every configuration exists for the F77 canopy without the sunlit/shaded
+ * split; other flag sets have configurations 0 and 8 (and 6 for the IBIS 3.0
+ * kernels with both canopies of one kind), and any other fused (two-kernel)
+ * configuration runs as 0 (8) for them.
  * Replaces: timestep_body (loops.py:234) iterated by _step_body (loops_gswp3.py:115). */
 int ibis_step_config_f32(float* prog, const float* stat, const float* forc, float* diag, float* acc, float* scratch,
                          int ncell, int ld, int nstep, const IbisParams* params, int* status, void* stream,
