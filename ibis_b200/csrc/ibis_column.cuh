@@ -129,7 +129,7 @@ __device__ __forceinline__ TwoStr<R> two_stream(R cosz, R lai, R sai, R asd, R a
     R k = gdir / mx(cosz, R(0.01));
     R p = avmu * k;
     R sgn = (p >= q) ? R(1.0) : R(-1.0);
-    if (fabs((double)(p - q)) < (double)(R(0.001) * p)) p = (R(1.0) + sgn * R(0.001)) * p;
+    if (ab(p - q) < R(0.001) * p) p = (R(1.0) + sgn * R(0.001)) * p;
     R c0 = om * p;
     R d = c0 * betad;
     R f = c0 * (R(1.0) - betad);
@@ -318,7 +318,7 @@ __device__ __forceinline__ void wet_fraction(R tveg, R wliq, R wsno, R wliqmax, 
 template <typename R>
 __device__ __forceinline__ void mix2(R& xm, R& tm, R x1, R t1, R x2, R t2, R x3, R t3, R eps) {
     R s = x1 + x2 + x3;
-    bool ok = fabs((double)s) >= (double)eps;
+    bool ok = ab(s) >= eps;
     tm = ok ? (t1 * x1 + t2 * x2 + t3 * x3) / s : R(0.0);
     xm = ok ? s : R(0.0);
 }
@@ -667,7 +667,7 @@ template <typename R>
 __device__ __forceinline__ R weight_veg(R t, R ch, R wliq, R wsno, R prev, bool first, const DevParams<R>& P) {
     if (first) return R(1.0);
     R h = ch * (t - P.tmelt);
-    R z = mx(R(fabs((double)h)), P.epsilon);
+    R z = mx(ab(h), P.epsilon);
     R nw;
     if (h > P.epsilon + R(1.0e-8)) nw = R(1.0) - mn(R(1.0), P.hfus * wsno / z);
     else if (h < -P.epsilon - R(1.0e-8)) nw = R(1.0) - mn(R(1.0), P.hfus * wliq / z);

@@ -24,6 +24,8 @@ __device__ __forceinline__ float mx(float a, float b) { return fmaxf(a, b); }
 __device__ __forceinline__ double mx(double a, double b) { return fmax(a, b); }
 __device__ __forceinline__ float mn(float a, float b) { return fminf(a, b); }
 __device__ __forceinline__ double mn(double a, double b) { return fmin(a, b); }
+__device__ __forceinline__ float ab(float x) { return fabsf(x); }
+__device__ __forceinline__ double ab(double x) { return fabs(x); }
 __device__ __forceinline__ bool finite(float x) { return isfinite(x); }
 __device__ __forceinline__ bool finite(double x) { return isfinite(x); }
 
