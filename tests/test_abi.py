@@ -75,3 +75,18 @@ def test_wetland_layouts_match_ctypes(tmp_path, struct, cname):
     got = _c_layout(tmp_path, body)
     assert got[0] == ctypes.sizeof(E)
     assert got[1:] == [getattr(E, n).offset for n in names]
+
+
+def test_launch_configuration_table():
+    """The configuration table is read from the library without a GPU: the
+    default long configuration (6: fused, block 224, accumulators on chip), the
+    two-kernel ones, and the staged fused form (11) with the same block."""
+    cfgs = lib.configs()
+    assert len(cfgs) == lib.load().ibis_num_configs() == 12
+    assert cfgs[6]["form"] == "fused" and cfgs[6]["block"] == 224 and not cfgs[6]["staged"]
+    assert cfgs[11]["form"] == "fused" and cfgs[11]["staged"]
+    assert (cfgs[11]["block"], cfgs[11]["min_blocks"]) == (cfgs[6]["block"], cfgs[6]["min_blocks"])
+    assert [c["id"] for c in cfgs if c["form"] == "split"] == [8, 9, 10]
+    form = ctypes.c_int()
+    assert lib.load().ibis_config_info(11, ctypes.byref(form), None, None, None, None) == 0 and form.value == 2
+    assert lib.load().ibis_config_info(12, None, None, None, None, None) < 0
